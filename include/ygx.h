@@ -1,0 +1,221 @@
+/*
+ * ygx.h -- C ABI of libygx.so, the sm_100a CUDA implementation of the
+ * yggdrax tree pipeline (Morton encode + stable sort, Karras radix /
+ * fixed-depth builds, octree tables, node geometry, dual-tree traversal).
+ *
+ * Conventions
+ *  - Every array argument is a DEVICE pointer to caller-owned memory unless
+ *    the comment says "host".  Nothing here allocates device memory.
+ *  - Scratch memory is a caller-provided device workspace `ws` of at least
+ *    the bytes returned by the matching *_workspace_size function.  Its first
+ *    256 bytes hold a status word of YGX_FLAG_* bits that kernels OR into
+ *    instead of trapping; clear it with ygx_workspace_init and read it with
+ *    ygx_status_read.
+ *  - Index outputs use the "index dtype" of the reference (int64 by default,
+ *    int32 when index_bits == 32): arguments typed `void*` with an
+ *    `index_bits` parameter are arrays of that dtype.
+ *  - All work is enqueued on `stream`; functions synchronize the stream only
+ *    where their comment says so (to return data-dependent sizes).
+ *  - Return value: YGX_OK or one of the YGX_ERR_* codes below.
+ *
+ * Each entry point names the reference function (file:line in the yggdrax
+ * project) whose behaviour it provides.
+ */
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+typedef struct CUstream_st* cudaStream_t;
+
+enum {
+  YGX_OK = 0,
+  YGX_ERR_ARG = 1,             /* bad argument / workspace too small          */
+  YGX_ERR_CUDA = 2,            /* a CUDA runtime call or launch failed        */
+  YGX_ERR_TIMEOUT = 3,         /* a bounded device spin gave up               */
+  YGX_ERR_QUEUE_OVERFLOW = 4,  /* traversal wavefront capacity exceeded       */
+  YGX_ERR_FAR_OVERFLOW = 5,    /* far-list capacity exceeded                  */
+  YGX_ERR_NEAR_OVERFLOW = 6,   /* near-list capacity exceeded                 */
+  YGX_ERR_INT32_TOTAL = 7,     /* pair totals exceed the int32 range          */
+  YGX_ERR_MALFORMED = 8        /* topology inconsistent (tied Morton codes)   */
+};
+
+/* status-word bits (device side) */
+#define YGX_FLAG_TIMEOUT (1u << 0)
+#define YGX_FLAG_QUEUE_OVERFLOW (1u << 1)
+#define YGX_FLAG_FAR_OVERFLOW (1u << 2)
+#define YGX_FLAG_NEAR_OVERFLOW (1u << 3)
+#define YGX_FLAG_MALFORMED (1u << 4)
+#define YGX_FLAG_BAD_INPUT (1u << 5)
+
+/* traversal statistics words (host array of YGX_TSTAT_WORDS uint64) */
+#define YGX_TSTAT_WORDS 16
+#define YGX_TSTAT_FAR_TOTAL 0   /* directed far entries (sum of far counts)    */
+#define YGX_TSTAT_NEAR_TOTAL 1  /* directed near entries                       */
+#define YGX_TSTAT_MAX_FAR 2     /* largest far row                             */
+#define YGX_TSTAT_MAX_NEAR 3    /* largest near row                            */
+#define YGX_TSTAT_ACCEPT 4      /* accept decisions (canonical pairs)          */
+#define YGX_TSTAT_NEAR 5        /* near decisions                              */
+#define YGX_TSTAT_REFINE 6      /* refine decisions                            */
+#define YGX_TSTAT_MAX_WF 7      /* largest wavefront                           */
+#define YGX_TSTAT_GENS 8        /* wavefront generations                       */
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- workspace / status -------------------------------------------------- */
+
+/* Zeroes the status word and bookkeeping header of a workspace. */
+int ygx_workspace_init(void* ws, size_t ws_bytes, cudaStream_t stream);
+/* Copies the status word to host *host_flags; synchronizes the stream. */
+int ygx_status_read(const void* ws, uint32_t* host_flags, cudaStream_t stream);
+
+/* ---- L0: bounds, Morton codes, stable sort ------------------------------- */
+
+/* infer_bounds (yggdrax/bounds.py:11-33): bounds_out = [min x,y,z, max x,y,z]
+ * with the reference's padding.  ws: ygx_encode_sort_workspace_size(0). */
+int ygx_bounds(const float* positions, int64_t n, float* bounds_out, void* ws, size_t ws_bytes,
+               cudaStream_t stream);
+
+/* morton_encode_impl (yggdrax/morton.py:43-77): 63-bit codes of positions
+ * (n x 3 float32) in bounds (6 floats, device). */
+int ygx_morton_encode(const float* positions, int64_t n, const float* bounds, uint64_t* codes,
+                      cudaStream_t stream);
+
+size_t ygx_encode_sort_workspace_size(int64_t n);
+/* Fused infer_bounds (if bounds_in == NULL) + morton_encode_impl + the stable
+ * argsort of the codes (yggdrax/_tree_impl.py:397-402, yggdrax/tree.py:401-404):
+ * codes_sorted[k] = code of particle order[k], ascending, ties by index. */
+int ygx_encode_sort(const float* positions, int64_t n, const float* bounds_in, float* bounds_out,
+                    uint64_t* codes_sorted, uint32_t* order, void* ws, size_t ws_bytes,
+                    cudaStream_t stream);
+
+size_t ygx_sort_pairs_workspace_size(int64_t n);
+/* Stable LSD radix sort of (uint64 key, uint32 value) pairs on key bits
+ * [begin_bit, end_bit) -- the device equivalent of jnp.argsort(stable=True)
+ * used throughout the reference (values_in == NULL: value = input index). */
+int ygx_sort_pairs(const uint64_t* keys_in, const uint32_t* values_in, int64_t n, int begin_bit,
+                   int end_bit, uint64_t* keys_out, uint32_t* values_out, void* ws,
+                   size_t ws_bytes, cudaStream_t stream);
+
+/* reorder_particles_by_indices / inverse_permutation
+ * (yggdrax/_tree_impl.py:900-926): any output may be NULL. */
+int ygx_reorder(const float* positions, const float* masses, const uint32_t* order, int64_t n,
+                int index_bits, float* positions_sorted, float* masses_sorted,
+                void* particle_indices, void* inverse, cudaStream_t stream);
+
+/* ---- L1: leaf partitions -------------------------------------------------- */
+
+/* Fixed-size chunks of the sorted order (yggdrax/_tree_impl.py:404-406):
+ * L = ceil(n / leaf_size) leaves; leaf_codes = codes_sorted[start];
+ * leaf_depths (may be NULL) = -1. */
+int ygx_leaves_adaptive(const uint64_t* codes_sorted, int64_t n, int64_t leaf_size, int index_bits,
+                        void* leaf_starts, void* leaf_ends, uint64_t* leaf_codes,
+                        void* leaf_depths, cudaStream_t stream);
+
+/* _fixed_depth_leaf_partitions (yggdrax/_tree_impl.py:1373-1401), depth >= 1:
+ * 8^depth dense buckets, empty ones kept. */
+int ygx_leaves_fixed(const uint64_t* codes_sorted, int64_t n, int depth, int index_bits,
+                     void* leaf_starts, void* leaf_ends, uint64_t* leaf_codes, void* leaf_depths,
+                     cudaStream_t stream);
+
+size_t ygx_refine_workspace_size(int64_t num_buckets);
+/* _refine_leaf_partitions_by_aspect (yggdrax/_tree_impl.py:96-227), pass 1:
+ * per-bucket refined-leaf counts; the total lands at device *total_out. */
+int ygx_refine_count(const float* positions_sorted, const uint64_t* codes_sorted,
+                     const void* starts, const void* ends, const uint64_t* codes,
+                     const void* depths, int64_t L, int current_depth, int max_refine_levels,
+                     double aspect_threshold, int min_leaf_particles, int index_bits,
+                     int64_t* total_out, void* ws, size_t ws_bytes, cudaStream_t stream);
+/* pass 2 (same arguments and workspace): the refined leaves in (start, code)
+ * order. */
+int ygx_refine_emit(const float* positions_sorted, const uint64_t* codes_sorted,
+                    const void* starts, const void* ends, const uint64_t* codes,
+                    const void* depths, int64_t L, int current_depth, int max_refine_levels,
+                    double aspect_threshold, int min_leaf_particles, int index_bits,
+                    void* out_starts, void* out_ends, uint64_t* out_codes, void* out_depths,
+                    void* ws, size_t ws_bytes, cudaStream_t stream);
+
+/* ---- L1: Karras topology and levels --------------------------------------- */
+
+size_t ygx_topology_workspace_size(int64_t num_leaves);
+/* _build_tree_from_leaf_partitions (yggdrax/_tree_impl.py:1009-1355) for
+ * L >= 2 leaves, total = 2L - 1 nodes: parent, left/right children and leaf
+ * flags, node_ranges (total x 2, inclusive), node_level, level_offsets (65),
+ * nodes_by_level, num_levels (1) -- plus int32 copies used by the geometry
+ * and traversal kernels (left32/right32 span all nodes, -1 on leaves).
+ * *tree_flags_out (device word) gets YGX_FLAG_MALFORMED when tied leaf codes
+ * produced a parent array that disagrees with the child arrays. */
+int ygx_build_topology(const uint64_t* leaf_codes, const void* leaf_starts, const void* leaf_ends,
+                       int64_t L, int index_bits, void* parent, void* left, void* right,
+                       uint8_t* left_is_leaf, uint8_t* right_is_leaf, void* node_ranges,
+                       void* node_level, void* level_offsets, void* nodes_by_level,
+                       void* num_levels, int32_t* parent32, int32_t* left32, int32_t* right32,
+                       int32_t* level32, int32_t* nbl32, uint32_t* tree_flags_out, void* ws,
+                       size_t ws_bytes, cudaStream_t stream);
+
+/* ---- L1b: explicit octree tables ------------------------------------------ */
+
+size_t ygx_octree_workspace_size(int64_t num_leaves);
+/* build_explicit_octree_metadata (yggdrax/octree.py:479-550) over a radix
+ * topology of `total` nodes: M = 2L - 1 cell slots.  max_cell_depth bounds
+ * every leaf cell depth (<= 21) and sizes the address sort. */
+int ygx_octree_tables(const void* node_ranges, int64_t total, const uint64_t* morton_codes,
+                      int64_t n, const uint64_t* leaf_codes, const void* leaf_depths,
+                      int max_cell_depth, int index_bits, void* oct_parent, void* oct_children,
+                      void* oct_child_counts, uint8_t* oct_child_mask, uint8_t* oct_valid_mask,
+                      uint64_t* oct_node_codes, void* oct_node_depths, void* oct_node_ranges,
+                      void* oct_nodes_by_level, void* oct_level_offsets, void* oct_num_levels,
+                      uint8_t* oct_leaf_mask, void* oct_leaf_nodes, void* radix_node_to_oct,
+                      void* radix_leaf_to_oct, void* ws, size_t ws_bytes, cudaStream_t stream);
+
+/* ---- L2: node geometry ----------------------------------------------------- */
+
+size_t ygx_geometry_workspace_size(int64_t total);
+/* compute_tree_geometry (yggdrax/_geometry_impl.py:176-338): center (total x 3),
+ * half_extent (total x 3), radius, max_extent (float32).  use_morton selects
+ * Morton-cell leaf boxes; otherwise particle ranges with at most
+ * max_leaf_size particles per leaf (< 0: no cap). */
+int ygx_tree_geometry(const void* node_ranges, int64_t total, int index_bits,
+                      const int32_t* parent32, const int32_t* left32, const int32_t* right32,
+                      const int32_t* level32, const uint32_t* tree_flags,
+                      const float* positions_sorted, int64_t n, int use_morton,
+                      const float* bounds, const uint64_t* leaf_codes, const void* leaf_depths,
+                      int64_t max_leaf_size, float* center, float* half_extent, float* radius,
+                      float* max_extent, void* ws, size_t ws_bytes, cudaStream_t stream);
+
+/* ---- L3: dual-tree traversal ------------------------------------------------ */
+
+size_t ygx_traverse_workspace_size(int64_t total, int64_t num_leaves, int64_t wf_capacity);
+/* Count pass of build_interactions_and_neighbors
+ * (yggdrax/_interactions_impl.py:2600-2939 _dual_tree_walk_count_impl):
+ * mac 0 = "bh", 1 = "dehnen", 2 = "engblom".  stats_out / flags_out are HOST
+ * arrays (YGX_TSTAT_WORDS / 1 words).  Synchronizes the stream. */
+int ygx_traverse_count(const float* center, const float* radius, const float* max_extent,
+                       const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
+                       int64_t total, int64_t num_internal, int mac, float theta,
+                       float dehnen_radius_scale, int root, int64_t wf_capacity,
+                       uint64_t* stats_out, uint32_t* flags_out, void* ws, size_t ws_bytes,
+                       cudaStream_t stream);
+/* Fill pass (_dual_tree_walk_compact_fill_impl, :2942-3558) plus the offset
+ * tables of _result_to_interactions / _result_to_neighbors (:3561-3837). */
+int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta, int root,
+                      int64_t wf_capacity, int gens, const int32_t* nbl32,
+                      const void* tree_level_offsets, int num_levels, int index_bits,
+                      void* node_offsets, void* far_counts, void* level_offsets,
+                      void* near_offsets, void* near_counts, int32_t* far_src32,
+                      int32_t* near_nbr32, void* ws, size_t ws_bytes, cudaStream_t stream);
+/* Row finalize: canonical (ascending) order within each row, level-major
+ * far sources/targets/target_levels, leaf-ordered near neighbours, and
+ * optionally the dense neighbour_leaf_positions table (L x max_nbr). */
+int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capacity,
+                          const int32_t* level32, const int32_t* leafpos32, int index_bits,
+                          int32_t* far_src32, int32_t* near_nbr32, void* far_sources,
+                          void* far_targets, void* target_levels, void* neighbors,
+                          void* neighbor_leaf_positions, int64_t max_nbr, void* ws,
+                          size_t ws_bytes, cudaStream_t stream);
+int ygx_traverse_status(const void* ws, uint32_t* flags_out, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif

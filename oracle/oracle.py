@@ -1,0 +1,551 @@
+"""CPU oracle for the yggdrax tree pipeline -- TEST INFRASTRUCTURE ONLY.
+
+A restatement of the reference algorithm used to check the CUDA product
+(``yggdrax_b200``) bit for bit.  Only ``tests/``, ``__graft_entry__.smoke()``
+and the CPU-baseline legs of ``bench.py`` may import this module; the product
+never does.
+
+The heavy lifting lives in ``ygx_oracle.cpp`` (C++17 + OpenMP, compiled with
+``-ffp-contract=off``); this module holds the thin orchestration that mirrors
+the reference's public functions and returns numpy arrays:
+
+* ``infer_bounds`` -- ``yggdrax/bounds.py:11-33``
+* ``morton_encode`` -- ``yggdrax/morton.py:43-77``
+* ``build_tree`` / ``build_fixed_depth_tree`` -- ``yggdrax/_tree_impl.py:354-519``
+  and ``:1009-1401`` (Karras build, levels, fixed-depth buckets, refinement)
+* ``octree_metadata`` -- ``yggdrax/octree.py:168-550``
+* ``compute_tree_geometry`` -- ``yggdrax/_geometry_impl.py:176-338``
+* ``build_interactions_and_neighbors`` -- ``yggdrax/_interactions_impl.py``
+  (MAC 338-395, extents 993-1061, walk 1119-1905 / 2600-3558, result layouts
+  3561-3837), with rows in canonical ascending order.
+
+Parity status: the refinement helper is pinned against the reference's own
+NumPy function (golden fixtures in ``tests/golden``); the remaining stages are
+pinned against golden fixtures produced by running the reference's source in
+this container over a NumPy stand-in for ``jax.numpy`` (see
+``tests/golden/make_golden.py``).  Bit patterns that depend on XLA's own
+lowering (fp32 reduction order of ``linalg.norm``/``sum``, FMA contraction)
+follow IEEE evaluation in the written order and are documented as such.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SRC = os.path.join(_HERE, "ygx_oracle.cpp")
+_LIB_PATH = os.path.join(_HERE, "libygx_oracle.so")
+_lib = None
+
+MAX_TREE_LEVELS = 64
+_MAX_MORTON_LEVEL = 21
+_DEFAULT_MAX_NEIGHBORS = 2048
+
+
+def build(force: bool = False) -> str:
+    """Compile the C++ oracle into ``oracle/libygx_oracle.so``."""
+    if (
+        not force
+        and os.path.exists(_LIB_PATH)
+        and os.path.getmtime(_LIB_PATH) >= os.path.getmtime(_SRC)
+    ):
+        return _LIB_PATH
+    cmd = [
+        "g++", "-O3", "-std=c++17", "-fopenmp", "-ffp-contract=off", "-fno-fast-math",
+        "-fPIC", "-shared", _SRC, "-o", _LIB_PATH,
+    ]
+    subprocess.run(cmd, check=True)
+    return _LIB_PATH
+
+
+def _load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        build()
+    lib = ctypes.CDLL(_LIB_PATH)
+    P = ctypes.c_void_p
+    i64 = ctypes.c_int64
+    lib.ygo_walk.restype = ctypes.c_void_p
+    lib.ygo_walk.argtypes = [P, P, P, P, i64, i64, ctypes.c_float, ctypes.c_int, i64]
+    lib.ygo_walk_sizes.argtypes = [P, P]
+    lib.ygo_walk_lists.argtypes = [P, i64, P, P, i64, P, P, P, P, P, P, P]
+    lib.ygo_walk_free.argtypes = [P]
+    lib.ygo_refine.restype = i64
+    lib.ygo_refine.argtypes = [P, P, P, P, P, P, i64, ctypes.c_int, ctypes.c_int,
+                               ctypes.c_double, ctypes.c_int, i64, P, P, P, P]
+    lib.ygo_octree_metadata.restype = i64
+    lib.ygo_geometry.restype = ctypes.c_int
+    lib.ygo_geometry.argtypes = [P, i64, P, P, P, P, i64, ctypes.c_int, P, P, P, P, i64,
+                                 P, P, P, P]
+    lib.ygo_num_threads.restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def _p(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data) if a.size else ctypes.c_void_p(0)
+
+
+def num_threads() -> int:
+    return int(_load().ygo_num_threads())
+
+
+def set_num_threads(t: int) -> None:
+    _load().ygo_set_num_threads(ctypes.c_int(int(t)))
+
+
+# ---------------------------------------------------------------------------
+# L0 primitives
+
+
+def infer_bounds(positions: np.ndarray):
+    pos = np.ascontiguousarray(positions, dtype=np.float32)
+    mn = np.empty(3, np.float32)
+    mx = np.empty(3, np.float32)
+    _load().ygo_infer_bounds(_p(pos), ctypes.c_int64(pos.shape[0]), _p(mn), _p(mx))
+    return mn, mx
+
+
+def morton_encode(positions: np.ndarray, bounds) -> np.ndarray:
+    pos = np.ascontiguousarray(positions, dtype=np.float32)
+    bmin = np.ascontiguousarray(bounds[0], dtype=np.float32)
+    bmax = np.ascontiguousarray(bounds[1], dtype=np.float32)
+    codes = np.empty(pos.shape[0], np.uint64)
+    _load().ygo_morton_encode(_p(pos), ctypes.c_int64(pos.shape[0]), _p(bmin), _p(bmax),
+                              _p(codes))
+    return codes
+
+
+def stable_argsort_u64(keys: np.ndarray, key_bits: int = 64) -> np.ndarray:
+    keys = np.ascontiguousarray(keys, dtype=np.uint64)
+    out = np.empty(keys.shape[0], np.int64)
+    _load().ygo_stable_argsort_u64(_p(keys), ctypes.c_int64(keys.shape[0]),
+                                   ctypes.c_int(key_bits), _p(out))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# L1 tree build
+
+
+@dataclass
+class OracleTree:
+    """Field-for-field mirror of the reference ``RadixTree`` topology
+    (``_tree_impl.py:24-71``), optionally extended with the ``oct_*`` fields
+    of ``OctreeTopology`` (``octree.py:73-110``)."""
+
+    parent: np.ndarray
+    left_child: np.ndarray
+    right_child: np.ndarray
+    left_is_leaf: np.ndarray
+    right_is_leaf: np.ndarray
+    particle_indices: np.ndarray
+    morton_codes: np.ndarray
+    node_ranges: np.ndarray
+    num_particles: int
+    num_internal_nodes: int
+    node_level: np.ndarray
+    level_offsets: np.ndarray
+    nodes_by_level: np.ndarray
+    num_levels: int
+    bounds_min: np.ndarray
+    bounds_max: np.ndarray
+    leaf_codes: np.ndarray
+    leaf_depths: np.ndarray
+    use_morton_geometry: bool
+    leaf_size: Optional[int]
+    octree: Optional[dict] = None
+    positions_sorted: Optional[np.ndarray] = None
+    masses_sorted: Optional[np.ndarray] = None
+    inverse_permutation: Optional[np.ndarray] = None
+    extras: dict = field(default_factory=dict)
+
+
+def resolve_fixed_depth_level(num_particles: int, target: int, max_allowed_depth: int) -> int:
+    """``_tree_impl.py:1358-1370``."""
+    target = max(1, int(target))
+    if num_particles <= target:
+        return 0
+    target_leaves = math.ceil(num_particles / target)
+    depth = math.ceil(math.log(target_leaves, 8))
+    return int(min(depth, max_allowed_depth))
+
+
+def _tree_from_partitions(pos, mass, order, sorted_codes, starts, ends, bounds, *,
+                          leaf_size, use_morton, leaf_codes=None, leaf_depths=None,
+                          return_reordered=True) -> OracleTree:
+    """``_tree_impl.py:1009-1355`` (_build_tree_from_leaf_partitions)."""
+    lib = _load()
+    n = pos.shape[0]
+    L = int(starts.shape[0])
+    starts = np.ascontiguousarray(starts, np.int64)
+    ends = np.ascontiguousarray(ends, np.int64)
+    if leaf_codes is None:
+        leaf_codes = sorted_codes[np.clip(starts, 0, n - 1)]
+    leaf_codes = np.ascontiguousarray(leaf_codes, np.uint64)
+    if leaf_depths is None:
+        leaf_depths = np.full(L, -1, np.int64)
+    leaf_depths = np.ascontiguousarray(leaf_depths, np.int64)
+    if L == 1:
+        level_offsets = np.zeros(MAX_TREE_LEVELS + 1, np.int64)
+        level_offsets[1] = 1
+        t = OracleTree(
+            parent=np.array([-1], np.int64), left_child=np.zeros(0, np.int64),
+            right_child=np.zeros(0, np.int64), left_is_leaf=np.zeros(0, bool),
+            right_is_leaf=np.zeros(0, bool), particle_indices=order,
+            morton_codes=sorted_codes, node_ranges=np.array([[0, n - 1]], np.int64),
+            num_particles=n, num_internal_nodes=0, node_level=np.zeros(1, np.int64),
+            level_offsets=level_offsets, nodes_by_level=np.zeros(1, np.int64),
+            num_levels=1, bounds_min=bounds[0], bounds_max=bounds[1],
+            leaf_codes=leaf_codes, leaf_depths=leaf_depths,
+            use_morton_geometry=use_morton, leaf_size=leaf_size)
+    else:
+        total = 2 * L - 1
+        ni = L - 1
+        parent = np.empty(total, np.int64)
+        left = np.empty(ni, np.int64)
+        right = np.empty(ni, np.int64)
+        lil = np.empty(ni, np.uint8)
+        ril = np.empty(ni, np.uint8)
+        ranges = np.empty((total, 2), np.int64)
+        lib.ygo_karras(_p(leaf_codes), _p(starts), _p(ends), ctypes.c_int64(L), _p(parent),
+                       _p(left), _p(right), _p(lil), _p(ril), _p(ranges))
+        node_level = np.empty(total, np.int64)
+        level_offsets = np.empty(MAX_TREE_LEVELS + 1, np.int64)
+        nbl = np.empty(total, np.int64)
+        nl = np.zeros(1, np.int64)
+        lib.ygo_levels(_p(parent), ctypes.c_int64(total), _p(node_level), _p(level_offsets),
+                       _p(nbl), _p(nl))
+        t = OracleTree(
+            parent=parent, left_child=left, right_child=right,
+            left_is_leaf=lil.astype(bool), right_is_leaf=ril.astype(bool),
+            particle_indices=order, morton_codes=sorted_codes, node_ranges=ranges,
+            num_particles=n, num_internal_nodes=ni, node_level=node_level,
+            level_offsets=level_offsets, nodes_by_level=nbl, num_levels=int(nl[0]),
+            bounds_min=bounds[0], bounds_max=bounds[1], leaf_codes=leaf_codes,
+            leaf_depths=leaf_depths, use_morton_geometry=use_morton, leaf_size=leaf_size)
+    if return_reordered:
+        t.positions_sorted = pos[order]
+        t.masses_sorted = mass[order]
+        inv = np.empty(n, np.int64)
+        inv[order] = np.arange(n, dtype=np.int64)
+        t.inverse_permutation = inv
+    return t
+
+
+def _encode_and_sort(pos, bounds):
+    codes = morton_encode(pos, bounds)
+    order = stable_argsort_u64(codes, 63)
+    return codes, order, codes[order]
+
+
+def build_tree(positions, masses, bounds=None, *, leaf_size: int = 8,
+               return_reordered: bool = True) -> OracleTree:
+    """``tree.py:1412-1478`` -> ``_tree_impl.py:354-420``."""
+    pos = np.ascontiguousarray(positions, np.float32)
+    mass = np.ascontiguousarray(masses, np.float32)
+    n = pos.shape[0]
+    if n < 1:
+        raise ValueError("Need at least one particle")
+    if leaf_size < 1:
+        raise ValueError("leaf_size must be >= 1")
+    bounds = infer_bounds(pos) if bounds is None else (
+        np.asarray(bounds[0], np.float32), np.asarray(bounds[1], np.float32))
+    _, order, sc = _encode_and_sort(pos, bounds)
+    starts = np.arange(0, n, leaf_size, dtype=np.int64)
+    ends = np.minimum(starts + leaf_size, n)
+    return _tree_from_partitions(pos, mass, order, sc, starts, ends, bounds,
+                                 leaf_size=int(leaf_size), use_morton=False,
+                                 return_reordered=return_reordered)
+
+
+def fixed_depth_partitions(sorted_codes: np.ndarray, depth: int, n: int):
+    """``_tree_impl.py:1373-1401``."""
+    depth = max(0, int(depth))
+    if depth == 0:
+        return (np.array([0], np.int64), np.array([n], np.int64),
+                np.array([0], np.uint64), np.array([0], np.int64))
+    L = 1 << (3 * depth)
+    starts = np.empty(L, np.int64)
+    ends = np.empty(L, np.int64)
+    codes = np.empty(L, np.uint64)
+    depths = np.empty(L, np.int64)
+    _load().ygo_fixed_depth_partitions(_p(sorted_codes), ctypes.c_int64(n), ctypes.c_int(depth),
+                                       _p(starts), _p(ends), _p(codes), _p(depths))
+    return starts, ends, codes, depths
+
+
+def refine_partitions(pos_sorted, sorted_codes, starts, ends, codes, depths, current_depth,
+                      max_refine_levels=2, aspect_threshold=8.0, min_leaf_particles=2):
+    """``_tree_impl.py:96-227`` (_refine_leaf_partitions_by_aspect)."""
+    lib = _load()
+    pos_sorted = np.ascontiguousarray(pos_sorted, np.float32)
+    sorted_codes = np.ascontiguousarray(sorted_codes, np.uint64)
+    args = [np.ascontiguousarray(a, dt) for a, dt in
+            ((starts, np.int64), (ends, np.int64), (codes, np.uint64), (depths, np.int64))]
+    L = args[0].shape[0]
+    cap = 4 * L + 64
+    while True:
+        o = [np.empty(cap, np.int64), np.empty(cap, np.int64), np.empty(cap, np.uint64),
+             np.empty(cap, np.int64)]
+        m = lib.ygo_refine(_p(pos_sorted), _p(sorted_codes), *[_p(a) for a in args],
+                           ctypes.c_int64(L), ctypes.c_int(int(current_depth)),
+                           ctypes.c_int(int(max_refine_levels)),
+                           ctypes.c_double(float(aspect_threshold)),
+                           ctypes.c_int(int(min_leaf_particles)), ctypes.c_int64(cap),
+                           *[_p(a) for a in o])
+        if m <= cap:
+            return tuple(a[:m].copy() for a in o)
+        cap = int(m)
+
+
+def build_fixed_depth_tree(positions, masses, bounds=None, *, target_leaf_particles: int = 32,
+                           max_depth: Optional[int] = None, refine_local: bool = True,
+                           max_refine_levels: int = 2, aspect_threshold: float = 8.0,
+                           min_refined_leaf_particles: int = 2,
+                           return_reordered: bool = True) -> OracleTree:
+    """``tree.py:1628-1726`` -> ``_tree_impl.py:423-519``."""
+    pos = np.ascontiguousarray(positions, np.float32)
+    mass = np.ascontiguousarray(masses, np.float32)
+    n = pos.shape[0]
+    if n < 1:
+        raise ValueError("Need at least one particle")
+    if target_leaf_particles < 1:
+        raise ValueError("target_leaf_particles must be >= 1")
+    bounds = infer_bounds(pos) if bounds is None else (
+        np.asarray(bounds[0], np.float32), np.asarray(bounds[1], np.float32))
+    _, order, sc = _encode_and_sort(pos, bounds)
+    max_allowed = min(MAX_TREE_LEVELS - 1, _MAX_MORTON_LEVEL)
+    if max_depth is not None:
+        max_allowed = min(max_allowed, int(max_depth))
+    depth = resolve_fixed_depth_level(n, target_leaf_particles, max_allowed)
+    starts, ends, codes, depths = fixed_depth_partitions(sc, depth, n)
+    if refine_local:
+        starts, ends, codes, depths = refine_partitions(
+            pos[order], sc, starts, ends, codes, depths, depth, max_refine_levels,
+            aspect_threshold, min_refined_leaf_particles)
+    t = _tree_from_partitions(pos, mass, order, sc, starts, ends, bounds, leaf_size=None,
+                              use_morton=True, leaf_codes=codes, leaf_depths=depths,
+                              return_reordered=return_reordered)
+    t.extras["resolved_depth"] = depth
+    return t
+
+
+def octree_metadata(tree: OracleTree) -> dict:
+    """``octree.py:479-550`` (build_explicit_octree_metadata)."""
+    lib = _load()
+    total = tree.node_ranges.shape[0]
+    ni = (total - 1) // 2
+    L = total - ni
+    M = max(1, 2 * L - 1)
+    o = dict(
+        oct_parent=np.empty(M, np.int64), oct_children=np.empty((M, 8), np.int64),
+        oct_child_counts=np.empty(M, np.int64), oct_child_mask=np.empty((M, 8), np.uint8),
+        oct_valid_mask=np.empty(M, np.uint8), oct_node_codes=np.empty(M, np.uint64),
+        oct_node_depths=np.empty(M, np.int64), oct_node_ranges=np.empty((M, 2), np.int64),
+        oct_nodes_by_level=np.empty(M, np.int64), oct_level_offsets=np.empty(23, np.int64),
+        oct_num_levels=np.empty(1, np.int64), oct_leaf_mask=np.empty(M, np.uint8),
+        oct_leaf_nodes=np.empty(M, np.int64), radix_node_to_oct=np.empty(total, np.int64),
+        radix_leaf_to_oct=np.empty(L, np.int64))
+    ranges = np.ascontiguousarray(tree.node_ranges, np.int64)
+    codes = np.ascontiguousarray(tree.morton_codes, np.uint64)
+    lc = np.ascontiguousarray(tree.leaf_codes, np.uint64)
+    ld = np.ascontiguousarray(tree.leaf_depths, np.int64)
+    lib.ygo_octree_metadata(
+        _p(ranges), ctypes.c_int64(total), _p(codes), ctypes.c_int64(codes.shape[0]), _p(lc),
+        _p(ld), *[_p(o[k]) for k in (
+            "oct_parent", "oct_children", "oct_child_counts", "oct_child_mask",
+            "oct_valid_mask", "oct_node_codes", "oct_node_depths", "oct_node_ranges",
+            "oct_nodes_by_level", "oct_level_offsets", "oct_num_levels", "oct_leaf_mask",
+            "oct_leaf_nodes", "radix_node_to_oct", "radix_leaf_to_oct")])
+    for k in ("oct_child_mask", "oct_valid_mask", "oct_leaf_mask"):
+        o[k] = o[k].astype(bool)
+    o["oct_num_levels"] = int(o["oct_num_levels"][0])
+    return o
+
+
+def build_octree(positions, masses, bounds=None, *, leaf_size: int = 8,
+                 return_reordered: bool = True) -> OracleTree:
+    """``tree.py:1481-1549``: adaptive partition + explicit octree tables."""
+    t = build_tree(positions, masses, bounds, leaf_size=leaf_size,
+                   return_reordered=return_reordered)
+    t.octree = octree_metadata(t)
+    return t
+
+
+def build_fixed_depth_octree(positions, masses, bounds=None, **kw) -> OracleTree:
+    """``tree.py:1821-1879``."""
+    t = build_fixed_depth_tree(positions, masses, bounds, **kw)
+    t.octree = octree_metadata(t)
+    return t
+
+
+# ---------------------------------------------------------------------------
+# L2 geometry
+
+
+@dataclass
+class OracleGeometry:
+    center: np.ndarray
+    half_extent: np.ndarray
+    radius: np.ndarray
+    max_extent: np.ndarray
+
+
+def compute_tree_geometry(tree: OracleTree, positions_sorted: np.ndarray,
+                          max_leaf_size: Optional[int] = None) -> OracleGeometry:
+    """``geometry.py:17-75`` -> ``_geometry_impl.py:176-338``."""
+    lib = _load()
+    total = tree.node_ranges.shape[0]
+    if max_leaf_size is None and tree.leaf_size is not None:
+        max_leaf_size = int(tree.leaf_size)
+    cap = -1 if max_leaf_size is None else int(max_leaf_size)
+    pos = np.ascontiguousarray(positions_sorted, np.float32)
+    ranges = np.ascontiguousarray(tree.node_ranges, np.int64)
+    left = np.ascontiguousarray(tree.left_child, np.int64)
+    right = np.ascontiguousarray(tree.right_child, np.int64)
+    parent = np.ascontiguousarray(tree.parent, np.int64)
+    g = OracleGeometry(np.empty((total, 3), np.float32), np.empty((total, 3), np.float32),
+                       np.empty(total, np.float32), np.empty(total, np.float32))
+    rc = lib.ygo_geometry(_p(ranges), ctypes.c_int64(total), _p(left), _p(right), _p(parent),
+                          _p(pos), ctypes.c_int64(pos.shape[0]),
+                          ctypes.c_int(1 if tree.use_morton_geometry else 0),
+                          _p(np.asarray(tree.bounds_min, np.float32)),
+                          _p(np.asarray(tree.bounds_max, np.float32)),
+                          _p(np.ascontiguousarray(tree.leaf_codes, np.uint64)),
+                          _p(np.ascontiguousarray(tree.leaf_depths, np.int64)),
+                          ctypes.c_int64(cap), _p(g.center), _p(g.half_extent), _p(g.radius),
+                          _p(g.max_extent))
+    if rc != 0:
+        raise RuntimeError("geometry depth pass did not converge (cyclic parent array)")
+    return g
+
+
+# ---------------------------------------------------------------------------
+# L3 traversal
+
+
+def mac_extents(tree: OracleTree, geom: OracleGeometry, mac_type: str,
+                dehnen_radius_scale: float = 1.0) -> np.ndarray:
+    """``_interactions_impl.py:993-1061`` (_build_mac_extents).
+
+    Propagation and leaf depth padding only touch extents <= 0; with
+    ``half >= 1e-6`` every extent is positive, which this restatement
+    requires (it raises otherwise)."""
+    ext = np.asarray(geom.max_extent if mac_type == "bh" else geom.radius, np.float32)
+    if not np.all(ext > 0):
+        raise NotImplementedError("non-positive MAC extents are outside the restated path")
+    if mac_type == "dehnen":
+        ext = (np.float32(dehnen_radius_scale) * ext).astype(np.float32)
+    return np.ascontiguousarray(ext, np.float32)
+
+
+def leaf_ordering(tree: OracleTree):
+    """``_interactions_impl.py:1071-1103`` (_resolve_leaf_ordering)."""
+    total = tree.node_ranges.shape[0]
+    ni = tree.num_internal_nodes
+    L = total - ni
+    po = np.arange(ni, total, dtype=np.int64)
+    native = np.arange(L, dtype=np.int64)
+    if tree.octree is not None:
+        native = np.argsort(tree.octree["radix_leaf_to_oct"], kind="stable").astype(np.int64)
+    leaf_indices = po[native]
+    po_to_native = np.zeros(L, np.int64)
+    po_to_native[native] = np.arange(L, dtype=np.int64)
+    leaf_position = np.full(total, -1, np.int64)
+    leaf_position[leaf_indices] = np.arange(L, dtype=np.int64)
+    return leaf_indices, leaf_position, po, po_to_native
+
+
+_MAC_CODES = {"bh": 0, "dehnen": 1, "engblom": 2}
+
+
+def build_interactions_and_neighbors(tree: OracleTree, geom: OracleGeometry, theta: float = 0.5,
+                                     mac_type: str = "bh",
+                                     dehnen_radius_scale: float = 1.0) -> dict:
+    """Exact far/near lists of ``build_interactions_and_neighbors``
+    (``_interactions_impl.py:6031-6144``) with canonical row order."""
+    lib = _load()
+    total = tree.node_ranges.shape[0]
+    ni = tree.num_internal_nodes
+    L = total - ni
+    leaf_indices, leaf_position, po, po_to_native = leaf_ordering(tree)
+    out = dict(leaf_indices=leaf_indices, particle_order_leaf_indices=po,
+               particle_order_to_native_leaf=po_to_native)
+    theta_sq = np.float32(theta) * np.float32(theta)
+    if ni == 0:
+        out.update(far_counts=np.zeros(total, np.int64),
+                   offsets=np.zeros(total + 1, np.int64), sources=np.zeros(0, np.int64),
+                   targets=np.zeros(0, np.int64), near_counts=np.zeros(L, np.int64),
+                   near_offsets=np.zeros(L + 1, np.int64), neighbors=np.zeros(0, np.int64),
+                   accept_decisions=0, near_decisions=0, refine_decisions=0, max_wf=1,
+                   generations=0)
+        out["level_offsets"] = np.zeros(int(tree.num_levels) + 1, np.int64)
+        out["target_levels"] = np.zeros(0, np.int64)
+        return out
+    ext = mac_extents(tree, geom, mac_type, dehnen_radius_scale)
+    center = np.ascontiguousarray(geom.center, np.float32)
+    left = np.concatenate([tree.left_child, np.full(L, -1, np.int64)]).astype(np.int64)
+    right = np.concatenate([tree.right_child, np.full(L, -1, np.int64)]).astype(np.int64)
+    root = int(np.argmin(tree.parent))
+    h = lib.ygo_walk(_p(center), _p(ext), _p(left), _p(right), ctypes.c_int64(total),
+                     ctypes.c_int64(ni), ctypes.c_float(theta_sq), ctypes.c_int(_MAC_CODES[mac_type]),
+                     ctypes.c_int64(root))
+    try:
+        sizes = np.zeros(7, np.int64)
+        lib.ygo_walk_sizes(h, _p(sizes))
+        P, Q = int(sizes[0]), int(sizes[1])
+        far_counts = np.empty(total, np.int64)
+        offsets = np.empty(total + 1, np.int64)
+        sources = np.empty(2 * P, np.int64)
+        targets = np.empty(2 * P, np.int64)
+        near_counts = np.empty(L, np.int64)
+        near_offsets = np.empty(L + 1, np.int64)
+        neighbors = np.empty(2 * Q, np.int64)
+        nbl = np.ascontiguousarray(tree.nodes_by_level, np.int64)
+        lib.ygo_walk_lists(h, ctypes.c_int64(total), _p(nbl), _p(leaf_position),
+                           ctypes.c_int64(L), _p(far_counts), _p(offsets), _p(sources),
+                           _p(targets), _p(near_counts), _p(near_offsets), _p(neighbors))
+    finally:
+        lib.ygo_walk_free(h)
+    num_levels = int(tree.num_levels)
+    lvl_idx = np.asarray(tree.level_offsets[: num_levels + 1], np.int64)
+    counts_by_level = far_counts[nbl]
+    offsets_by_level = np.concatenate([[0], np.cumsum(counts_by_level)]).astype(np.int64)
+    out.update(
+        far_counts=far_counts, offsets=offsets, sources=sources, targets=targets,
+        level_offsets=offsets_by_level[lvl_idx] if P else np.zeros(num_levels + 1, np.int64),
+        target_levels=np.asarray(tree.node_level, np.int64)[targets],
+        near_counts=near_counts, near_offsets=near_offsets, neighbors=neighbors,
+        accept_decisions=int(sizes[2]), near_decisions=int(sizes[3]),
+        refine_decisions=int(sizes[4]), max_wf=int(sizes[5]), generations=int(sizes[6]))
+    if P == 0:
+        out["offsets"] = np.zeros(total + 1, np.int64)
+    return out
+
+
+def neighbor_leaf_positions(leaf_indices, near_offsets, near_counts, neighbors, total):
+    """Dense helper of ``_result_to_neighbors`` (``_interactions_impl.py:3658-3688``)."""
+    L = leaf_indices.shape[0]
+    if L == 0:
+        return np.zeros((0, 0), np.int64)
+    max_nbr = int(near_counts.max()) if L else 0
+    if max_nbr == 0:
+        return np.zeros((L, 0), np.int64)
+    lookup = np.full(total, -1, np.int64)
+    lookup[leaf_indices] = np.arange(L, dtype=np.int64)
+    k = np.arange(max_nbr, dtype=np.int64)
+    idx = near_offsets[:-1, None] + k[None, :]
+    valid = k[None, :] < near_counts[:, None]
+    safe = np.where(valid, idx, 0)
+    pos = lookup[neighbors[safe]] if neighbors.size else np.zeros_like(safe)
+    return np.where(valid, pos, -1)

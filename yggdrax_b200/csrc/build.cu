@@ -1,0 +1,617 @@
+// Tree build kernels (L1): reorder, leaf partitions (adaptive, fixed depth,
+// local aspect refinement), Karras LBVH topology and node levels.
+#include "scan.cuh"
+#include "sort.cuh"
+
+namespace ygx {
+namespace {
+
+// ---------------------------------------------------------------------------
+// _tree_impl.py:900-926 and :1047-1050: positions/masses gathered into Morton
+// order, particle_indices in the index dtype, inverse permutation scatter.
+__global__ void k_reorder(const float* __restrict__ pos, const float* __restrict__ mass,
+                          const uint32_t* __restrict__ order, int64_t n, int index_bits,
+                          float* __restrict__ pos_sorted, float* __restrict__ mass_sorted,
+                          void* __restrict__ particle_indices, void* __restrict__ inverse) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = order[k];
+    if (pos_sorted) {
+      pos_sorted[3 * k] = __ldg(pos + 3 * (int64_t)v);
+      pos_sorted[3 * k + 1] = __ldg(pos + 3 * (int64_t)v + 1);
+      pos_sorted[3 * k + 2] = __ldg(pos + 3 * (int64_t)v + 2);
+    }
+    if (mass_sorted) mass_sorted[k] = __ldg(mass + v);
+    if (particle_indices) store_idx(particle_indices, index_bits, k, v);
+    if (inverse) store_idx(inverse, index_bits, v, k);
+  }
+}
+
+// _tree_impl.py:405-406: fixed-size chunks of the sorted order.
+__global__ void k_leaves_adaptive(const uint64_t* __restrict__ codes, int64_t n, int64_t leaf_size,
+                                  int64_t L, int index_bits, void* starts, void* ends,
+                                  uint64_t* __restrict__ leaf_codes, void* depths) {
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < L;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    int64_t s = j * leaf_size;
+    int64_t e = s + leaf_size < n ? s + leaf_size : n;
+    store_idx(starts, index_bits, j, s);
+    store_idx(ends, index_bits, j, e);
+    leaf_codes[j] = codes[s];
+    if (depths) store_idx(depths, index_bits, j, -1);
+  }
+}
+
+__device__ __forceinline__ int64_t lower_bound_u64(const uint64_t* a, int64_t n, uint64_t q) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if (a[mid] < q) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// _tree_impl.py:1373-1401: dense 8^d buckets over the sorted codes.  Because
+// the codes are sorted, bucket b starts at lower_bound(b << shift); counts
+// and the exclusive scan of the reference follow from the bucket bounds.
+__global__ void k_leaves_fixed(const uint64_t* __restrict__ codes, int64_t n, int depth,
+                               int64_t L, int index_bits, void* starts, void* ends,
+                               uint64_t* __restrict__ leaf_codes, void* depths) {
+  const int shift = 63 - 3 * depth > 0 ? 63 - 3 * depth : 0;
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < L;
+       b += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = (uint64_t)b << shift;
+    int64_t s = lower_bound_u64(codes, n, lo);
+    int64_t e = b + 1 < L ? lower_bound_u64(codes, n, (uint64_t)(b + 1) << shift) : n;
+    store_idx(starts, index_bits, b, s);
+    store_idx(ends, index_bits, b, e);
+    leaf_codes[b] = lo;
+    store_idx(depths, index_bits, b, depth);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// _tree_impl.py:96-227 (_refine_leaf_partitions_by_aspect), one warp per
+// input bucket.  The reference walks a FIFO queue and finally orders leaves
+// by (start, code); within a bucket the emitted leaves tile its particle
+// range in increasing sub-octant order, so a depth-first walk that visits
+// sub-octants in increasing order emits them already in (start, code) order,
+// and buckets are emitted in bucket order.  The float64 aspect test, the
+// fp32 comparison of the 1e-12 floor and the 64 - 3*depth entry shift follow
+// the reference exactly.
+struct RefineItem {
+  int64_t s, e;
+  uint64_t code;
+  int32_t depth;
+  int32_t final_leaf;  // child with <= min_leaf particles: emitted as is
+};
+
+constexpr int kRefineStack = 64;
+
+template <bool kEmit>
+__global__ void k_refine(const float* __restrict__ pos_sorted, const uint64_t* __restrict__ codes,
+                         const void* starts, const void* ends, const uint64_t* __restrict__ bcodes,
+                         const void* bdepths, int64_t L, int current_depth,
+                         int max_refine_levels, double aspect_threshold, int min_leaf,
+                         int index_bits, int64_t* __restrict__ counts,
+                         const int64_t* __restrict__ offsets, void* o_starts, void* o_ends,
+                         uint64_t* __restrict__ o_codes, void* o_depths,
+                         uint32_t* __restrict__ status) {
+  __shared__ RefineItem s_stack[8][kRefineStack];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  RefineItem* stack = s_stack[wib];
+  for (int64_t b = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib; b < L; b += warps) {
+    int64_t emitted = 0;
+    const int64_t out_base = kEmit ? offsets[b] : 0;
+    if (lane == 0) {
+      stack[0].s = load_idx(starts, index_bits, b);
+      stack[0].e = load_idx(ends, index_bits, b);
+      stack[0].code = bcodes[b];
+      stack[0].depth = (int32_t)load_idx(bdepths, index_bits, b);
+      stack[0].final_leaf = 0;
+    }
+    int sp = 1;
+    __syncwarp();
+    while (sp > 0) {
+      const RefineItem it = stack[sp - 1];
+      __syncwarp();
+      --sp;
+      bool keep = it.final_leaf != 0 || it.e <= it.s;
+      int64_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      int64_t child_shift = -1;
+      if (!keep) {
+        float mn[3], mx[3];
+        unsigned nan = 0;
+        for (int a = 0; a < 3; ++a) { mn[a] = __int_as_float(0x7f800000); mx[a] = -__int_as_float(0x7f800000); }
+        for (int64_t p = it.s + lane; p < it.e; p += 32)
+          for (int a = 0; a < 3; ++a) {
+            float v = pos_sorted[3 * p + a];
+            if (v != v) nan |= 1u << a;
+            mn[a] = fminf(mn[a], v);
+            mx[a] = fmaxf(mx[a], v);
+          }
+        for (int off = 16; off > 0; off >>= 1) {
+          for (int a = 0; a < 3; ++a) {
+            mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], off));
+            mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], off));
+          }
+          nan |= __shfl_xor_sync(0xffffffffu, nan, off);
+        }
+        const float qnan = __int_as_float(0x7fc00000);
+        float ext[3];
+        for (int a = 0; a < 3; ++a) ext[a] = ((nan >> a) & 1) ? qnan : __fsub_rn(mx[a], mn[a]);
+        const float emin = fmin_nan(fmin_nan(ext[0], ext[1]), ext[2]);
+        const float emax = fmax_nan(fmax_nan(ext[0], ext[1]), ext[2]);
+        // max(emin, 1e-12) in Python compares in fp32 and keeps emin unless
+        // the floor is strictly larger; the ratio is taken in float64.
+        const double min_axis = (1e-12f > emin) ? 1e-12 : (double)emin;
+        const double aspect = (min_axis > 0.0) ? (double)emax / min_axis
+                                               : __longlong_as_double(0x7ff0000000000000ll);
+        const bool exceeded = (it.depth - current_depth) >= max_refine_levels;
+        int64_t entry_shift = 64 - (int64_t)it.depth * 3;
+        if (entry_shift < 0) entry_shift = 0;
+        child_shift = entry_shift - 3;
+        if (aspect <= aspect_threshold || exceeded || child_shift < 0) {
+          keep = true;
+        } else {
+          for (int64_t p = it.s + lane; p < it.e; p += 32) cnt[(codes[p] >> child_shift) & 7ull]++;
+          int nz = 0;
+          for (int k = 0; k < 8; ++k) {
+            int64_t c = cnt[k];
+            for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+            cnt[k] = c;
+            nz += c != 0;
+          }
+          if (nz <= 1) keep = true;
+        }
+      }
+      if (keep) {
+        if (kEmit && lane == 0) {
+          const int64_t o = out_base + emitted;
+          store_idx(o_starts, index_bits, o, it.s);
+          store_idx(o_ends, index_bits, o, it.e);
+          o_codes[o] = it.code;
+          store_idx(o_depths, index_bits, o, it.depth);
+        }
+        ++emitted;
+        continue;
+      }
+      // The children tile [s, e) in increasing sub order.  Push them in
+      // reverse so the lowest pops first; a refined child is expanded
+      // completely before its next sibling pops (depth-first pre-order).
+      int64_t child_off[8];
+      int64_t off = it.s;
+      for (int sub = 0; sub < 8; ++sub) { child_off[sub] = off; off += cnt[sub]; }
+      for (int sub = 7; sub >= 0; --sub) {
+        if (cnt[sub] == 0) continue;
+        if (sp >= kRefineStack) {
+          if (lane == 0) raise_flag(status, kFlagQueueOverflow);
+          continue;
+        }
+        if (lane == 0) {
+          RefineItem c;
+          c.s = child_off[sub];
+          c.e = child_off[sub] + cnt[sub];
+          c.code = it.code | ((uint64_t)sub << child_shift);
+          c.depth = it.depth + 1;
+          c.final_leaf = cnt[sub] <= min_leaf ? 1 : 0;
+          stack[sp] = c;
+        }
+        ++sp;
+      }
+      __syncwarp();
+    }
+    if (!kEmit && lane == 0) counts[b] = emitted;
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// _tree_impl.py:1115-1270: Karras (2012) topology over L >= 2 leaf codes.
+__device__ __forceinline__ int64_t kdelta(const uint64_t* __restrict__ c, int64_t L, int64_t i,
+                                          int64_t j, uint64_t ci) {
+  if (j < 0 || j >= L) return -1;
+  uint64_t cj = c[j];
+  if (ci == cj) return 64 + clz64((uint64_t)i ^ (uint64_t)j);
+  return clz64(ci ^ cj);
+}
+__device__ __forceinline__ int64_t lcp_codes(uint64_t a, uint64_t b) {
+  return a == b ? 64 : clz64(a ^ b);
+}
+
+__global__ void k_karras(const uint64_t* __restrict__ codes, const void* starts, const void* ends,
+                         int64_t L, int index_bits, void* left, void* right,
+                         uint8_t* __restrict__ lil, uint8_t* __restrict__ ril, void* ranges,
+                         int32_t* __restrict__ left32, int32_t* __restrict__ right32,
+                         int32_t* __restrict__ parent_claim) {
+  const int64_t ni = L - 1;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < L;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (i == ni) {
+      // Leaf ranges (one thread per leaf handled below).
+      continue;
+    }
+    const uint64_t ci = codes[i];
+    int64_t dp = kdelta(codes, L, i, i + 1, ci);
+    int64_t dm = kdelta(codes, L, i, i - 1, ci);
+    int64_t d = (dp - dm) > 0 ? 1 : ((dp - dm) < 0 ? -1 : 0);
+    if (i == 0 || d == 0) d = 1;
+    const int64_t dmin = kdelta(codes, L, i, i - d, ci);
+    int64_t span = 0;
+    for (int k = 30; k >= 0; --k) {
+      int64_t step = (int64_t)1 << k;
+      int64_t cand = i + (span + step) * d;
+      if (cand >= 0 && cand < L && kdelta(codes, L, i, cand, ci) > dmin) span += step;
+    }
+    const int64_t end = i + span * d;
+    const int64_t first = i < end ? i : end, last = i < end ? end : i;
+    store_idx(ranges, index_bits, 2 * i, load_idx(starts, index_bits, first));
+    store_idx(ranges, index_bits, 2 * i + 1, load_idx(ends, index_bits, last) - 1);
+    const uint64_t fc = codes[first];
+    const int64_t cp = lcp_codes(fc, codes[last]);
+    int64_t split = first;
+    for (int k = 30; k >= 0; --k) {
+      int64_t mid = split + ((int64_t)1 << k);
+      if (mid < last && lcp_codes(fc, codes[mid]) > cp) split = mid;
+    }
+    const bool ll = split == first, rl = split + 1 == last;
+    const int64_t lc = ll ? ni + first : split;
+    const int64_t rc = rl ? ni + last : split + 1;
+    lil[i] = ll;
+    ril[i] = rl;
+    store_idx(left, index_bits, i, lc);
+    store_idx(right, index_bits, i, rc);
+    left32[i] = (int32_t)lc;
+    right32[i] = (int32_t)rc;
+    // Serial-scatter semantics of parent.at[left].set / .at[right].set:
+    // any right claim beats every left claim, larger index wins within a side.
+    atomicMax(&parent_claim[lc], (int32_t)i);
+    atomicMax(&parent_claim[rc], (int32_t)(i + ni));
+  }
+}
+
+__global__ void k_leaf_ranges(const void* starts, const void* ends, int64_t L, int index_bits,
+                              void* ranges, int32_t* __restrict__ left32,
+                              int32_t* __restrict__ right32) {
+  const int64_t ni = L - 1;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < L;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    store_idx(ranges, index_bits, 2 * (ni + j), load_idx(starts, index_bits, j));
+    store_idx(ranges, index_bits, 2 * (ni + j) + 1, load_idx(ends, index_bits, j) - 1);
+    left32[ni + j] = -1;
+    right32[ni + j] = -1;
+  }
+}
+
+// Decode the claims into parent, and flag any internal node whose children
+// do not name it back (a malformed topology from tied codes).
+__global__ void k_parent_decode(const int32_t* __restrict__ claim, int64_t total, int64_t ni,
+                                int index_bits, void* parent, int32_t* __restrict__ parent32) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    int32_t c = claim[k];
+    int64_t p = c < 0 ? -1 : (c >= ni ? c - ni : c);
+    store_idx(parent, index_bits, k, p);
+    parent32[k] = (int32_t)p;
+  }
+}
+
+__global__ void k_check_wellformed(const int32_t* __restrict__ parent32,
+                                   const int32_t* __restrict__ left32,
+                                   const int32_t* __restrict__ right32, int64_t total, int64_t ni,
+                                   uint32_t* __restrict__ tree_flags) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    bool bad = (k == 0) ? parent32[0] != -1 : parent32[k] < 0;
+    if (k < ni) bad = bad || parent32[left32[k]] != (int32_t)k || parent32[right32[k]] != (int32_t)k;
+    if (bad) atomicOr(tree_flags, kFlagMalformed);
+  }
+}
+
+// _tree_impl.py:1272-1299: depth by synchronous pointer doubling.  Rounds
+// after the state stops changing are no-ops, so a round that sees the
+// previous round unchanged returns at once; `stop` records how many rounds
+// actually ran so the final state can be read from the right buffer.
+__global__ void k_depth_init(const int32_t* __restrict__ parent32, int64_t total,
+                             int32_t* __restrict__ sc, int32_t* __restrict__ d) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    int32_t p = parent32[k];
+    sc[k] = p < 0 ? (int32_t)k : p;
+    d[k] = p < 0 ? 0 : 1;
+  }
+}
+
+__global__ void k_depth_round(const int32_t* __restrict__ sc_in, const int32_t* __restrict__ d_in,
+                              int32_t* __restrict__ sc_out, int32_t* __restrict__ d_out,
+                              int64_t total, int round, uint32_t* __restrict__ changed,
+                              uint32_t* __restrict__ stop) {
+  if (round > 0 && ((volatile uint32_t*)changed)[round - 1] == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicMin(stop, (uint32_t)round);
+    return;
+  }
+  bool any = false;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    int32_t s = sc_in[k];
+    int32_t nd = d_in[k] + d_in[s];
+    int32_t ns = sc_in[s];
+    sc_out[k] = ns;
+    d_out[k] = nd;
+    any |= (ns != s) || (nd != d_in[k]);
+  }
+  if (__syncthreads_or(any) && threadIdx.x == 0) atomicOr(&changed[round], 1u);
+}
+
+// Final node levels (from whichever buffer holds the last state), the level
+// histogram over 64 bins and the 16-bit sort keys for nodes_by_level.
+__global__ void k_depth_finish(const int32_t* __restrict__ sc0, const int32_t* __restrict__ d0,
+                               const int32_t* __restrict__ sc1, const int32_t* __restrict__ d1,
+                               int64_t total, const uint32_t* __restrict__ stop, uint32_t rounds,
+                               int index_bits,
+                               void* node_level, int32_t* __restrict__ level32,
+                               uint64_t* __restrict__ level_keys, uint32_t* __restrict__ level_hist,
+                               int32_t* __restrict__ max_level, uint32_t* __restrict__ tree_flags) {
+  const uint32_t r = *stop < rounds ? *stop : rounds;
+  const int32_t* sc = (r & 1) ? sc1 : sc0;
+  const int32_t* d = (r & 1) ? d1 : d0;
+  __shared__ uint32_t s_hist[64];
+  if (threadIdx.x < 64) s_hist[threadIdx.x] = 0;
+  __syncthreads();
+  int32_t mx = 0;
+  bool detached = false;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    int32_t lv = d[k];
+    store_idx(node_level, index_bits, k, lv);
+    level32[k] = lv;
+    level_keys[k] = (uint64_t)(uint32_t)lv;
+    if (lv >= 0 && lv < 64) atomicAdd(&s_hist[lv], 1u);
+    mx = lv > mx ? lv : mx;
+    detached |= sc[k] != 0;
+  }
+  __syncthreads();
+  if (threadIdx.x < 64 && s_hist[threadIdx.x]) atomicAdd(&level_hist[threadIdx.x], s_hist[threadIdx.x]);
+  atomicMax(max_level, mx);
+  if (detached) atomicOr(tree_flags, kFlagMalformed);
+}
+
+__global__ void k_level_tables(const uint32_t* __restrict__ level_hist,
+                               const int32_t* __restrict__ max_level, int index_bits,
+                               void* level_offsets, void* num_levels) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    int64_t acc = 0;
+    store_idx(level_offsets, index_bits, 0, 0);
+    for (int l = 0; l < 64; ++l) {
+      acc += level_hist[l];
+      store_idx(level_offsets, index_bits, l + 1, acc);
+    }
+    int64_t nl = (int64_t)(*max_level) + 1;
+    nl = nl < 1 ? 1 : (nl > 64 ? 64 : nl);
+    store_idx(num_levels, index_bits, 0, nl);
+  }
+}
+
+__global__ void k_u32_to_index(const uint32_t* __restrict__ in, int64_t n, int index_bits,
+                               void* out, int32_t* __restrict__ out32) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    store_idx(out, index_bits, k, in[k]);
+    if (out32) out32[k] = (int32_t)in[k];
+  }
+}
+
+}  // namespace
+
+// Scratch layout of ygx_build_topology.
+struct TopoScratch {
+  uint32_t* status;
+  uint32_t* tree_flags;
+  int32_t* parent_claim;
+  int32_t* sc[2];
+  int32_t* d[2];
+  uint32_t* changed;
+  uint32_t* stop;
+  uint32_t* level_hist;
+  int32_t* max_level;
+  uint64_t* level_keys;
+  uint64_t* level_keys_sorted;
+  uint32_t* nbl_u32;
+  SortScratch sort;
+};
+
+static TopoScratch carve_topo(Arena& a, int64_t L) {
+  const int64_t total = L > 0 ? 2 * L - 1 : 1;
+  TopoScratch s;
+  s.status = a.take<uint32_t>(64);
+  s.tree_flags = a.take<uint32_t>(64);
+  s.changed = a.take<uint32_t>(128);
+  s.stop = a.take<uint32_t>(64);
+  s.level_hist = a.take<uint32_t>(64);
+  s.max_level = a.take<int32_t>(64);
+  s.parent_claim = a.take<int32_t>(total);
+  for (int b = 0; b < 2; ++b) { s.sc[b] = a.take<int32_t>(total); s.d[b] = a.take<int32_t>(total); }
+  s.level_keys = a.take<uint64_t>(total);
+  s.level_keys_sorted = a.take<uint64_t>(total);
+  s.nbl_u32 = a.take<uint32_t>(total);
+  s.sort = carve_sort_scratch(a, total, 2);
+  return s;
+}
+
+}  // namespace ygx
+
+extern "C" {
+
+int ygx_reorder(const float* positions, const float* masses, const uint32_t* order, int64_t n,
+                int index_bits, float* positions_sorted, float* masses_sorted,
+                void* particle_indices, void* inverse, cudaStream_t stream) {
+  if (n < 1 || !order || (index_bits != 32 && index_bits != 64)) return YGX_ERR_ARG;
+  ygx::k_reorder<<<ygx::grid_for(n, 256), 256, 0, stream>>>(
+      positions, masses, order, n, index_bits, positions_sorted, masses_sorted, particle_indices,
+      inverse);
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
+int ygx_leaves_adaptive(const uint64_t* codes_sorted, int64_t n, int64_t leaf_size, int index_bits,
+                        void* leaf_starts, void* leaf_ends, uint64_t* leaf_codes,
+                        void* leaf_depths, cudaStream_t stream) {
+  if (n < 1 || leaf_size < 1) return YGX_ERR_ARG;
+  const int64_t L = (n + leaf_size - 1) / leaf_size;
+  ygx::k_leaves_adaptive<<<ygx::grid_for(L, 256), 256, 0, stream>>>(
+      codes_sorted, n, leaf_size, L, index_bits, leaf_starts, leaf_ends, leaf_codes, leaf_depths);
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
+int ygx_leaves_fixed(const uint64_t* codes_sorted, int64_t n, int depth, int index_bits,
+                     void* leaf_starts, void* leaf_ends, uint64_t* leaf_codes, void* leaf_depths,
+                     cudaStream_t stream) {
+  if (n < 1 || depth < 1 || depth > 10) return YGX_ERR_ARG;
+  const int64_t L = (int64_t)1 << (3 * depth);
+  ygx::k_leaves_fixed<<<ygx::grid_for(L, 256), 256, 0, stream>>>(
+      codes_sorted, n, depth, L, index_bits, leaf_starts, leaf_ends, leaf_codes, leaf_depths);
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
+size_t ygx_refine_workspace_size(int64_t num_buckets) {
+  ygx::Arena a{nullptr, 0, 0};
+  a.take<uint32_t>(64);
+  a.take<int64_t>(num_buckets + 1);
+  a.take<int64_t>(num_buckets + 1);
+  a.take<int64_t>(ygx::scan_scratch_elems(num_buckets));
+  return a.used + 256;
+}
+
+// Pass 1: per-bucket output counts and their exclusive scan; the total
+// number of refined leaves is left at device address *total_out.
+int ygx_refine_count(const float* positions_sorted, const uint64_t* codes_sorted,
+                     const void* starts, const void* ends, const uint64_t* codes,
+                     const void* depths, int64_t L, int current_depth, int max_refine_levels,
+                     double aspect_threshold, int min_leaf_particles, int index_bits,
+                     int64_t* total_out, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (L < 1 || ws_bytes < ygx_refine_workspace_size(L)) return YGX_ERR_ARG;
+  ygx::Arena a{(char*)ws, 0, ws_bytes};
+  uint32_t* status = a.take<uint32_t>(64);
+  int64_t* counts = a.take<int64_t>(L + 1);
+  int64_t* offsets = a.take<int64_t>(L + 1);
+  int64_t* tmp = a.take<int64_t>(ygx::scan_scratch_elems(L));
+  const int warps_per_block = 8;
+  int grid = ygx::grid_for(L, warps_per_block, ygx::kNumSMs * 16);
+  ygx::k_refine<false><<<grid, 32 * warps_per_block, 0, stream>>>(
+      positions_sorted, codes_sorted, starts, ends, codes, depths, L, current_depth,
+      max_refine_levels, aspect_threshold, min_leaf_particles, index_bits, counts, nullptr,
+      nullptr, nullptr, nullptr, nullptr, status);
+  YGX_CHECK_LAUNCH();
+  int rc = ygx::exclusive_scan<int64_t>(counts, L, offsets, tmp, stream);
+  if (rc) return rc;
+  if (cudaMemcpyAsync(total_out, offsets + L, sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                      stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  return YGX_OK;
+}
+
+// Pass 2: emit the refined leaves (same arguments as pass 1, same workspace).
+int ygx_refine_emit(const float* positions_sorted, const uint64_t* codes_sorted,
+                    const void* starts, const void* ends, const uint64_t* codes,
+                    const void* depths, int64_t L, int current_depth, int max_refine_levels,
+                    double aspect_threshold, int min_leaf_particles, int index_bits,
+                    void* out_starts, void* out_ends, uint64_t* out_codes, void* out_depths,
+                    void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (L < 1 || ws_bytes < ygx_refine_workspace_size(L)) return YGX_ERR_ARG;
+  ygx::Arena a{(char*)ws, 0, ws_bytes};
+  uint32_t* status = a.take<uint32_t>(64);
+  a.take<int64_t>(L + 1);
+  int64_t* offsets = a.take<int64_t>(L + 1);
+  const int warps_per_block = 8;
+  int grid = ygx::grid_for(L, warps_per_block, ygx::kNumSMs * 16);
+  ygx::k_refine<true><<<grid, 32 * warps_per_block, 0, stream>>>(
+      positions_sorted, codes_sorted, starts, ends, codes, depths, L, current_depth,
+      max_refine_levels, aspect_threshold, min_leaf_particles, index_bits, nullptr, offsets,
+      out_starts, out_ends, out_codes, out_depths, status);
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
+size_t ygx_topology_workspace_size(int64_t num_leaves) {
+  ygx::Arena a{nullptr, 0, 0};
+  ygx::carve_topo(a, num_leaves);
+  return a.used + 256;
+}
+
+// Karras topology + levels for L >= 2 leaves (total = 2L - 1 nodes).
+// Outputs in the index dtype: parent (total), left/right (L-1), node_ranges
+// (total x 2), node_level (total), level_offsets (65), nodes_by_level
+// (total), num_levels (1); bool flags (L-1); int32 traversal copies
+// parent32/left32/right32/level32 (total, -1 children for leaves) and
+// nbl32 (total).  tree_flags_out (device, 1 word) receives kFlagMalformed
+// when the parent array and the child arrays disagree.
+int ygx_build_topology(const uint64_t* leaf_codes, const void* leaf_starts, const void* leaf_ends,
+                       int64_t L, int index_bits, void* parent, void* left, void* right,
+                       uint8_t* left_is_leaf, uint8_t* right_is_leaf, void* node_ranges,
+                       void* node_level, void* level_offsets, void* nodes_by_level,
+                       void* num_levels, int32_t* parent32, int32_t* left32, int32_t* right32,
+                       int32_t* level32, int32_t* nbl32, uint32_t* tree_flags_out, void* ws,
+                       size_t ws_bytes, cudaStream_t stream) {
+  if (L < 2 || (index_bits != 32 && index_bits != 64)) return YGX_ERR_ARG;
+  if ((2 * L - 1) >= (int64_t)INT32_MAX / 2) return YGX_ERR_ARG;
+  if (ws_bytes < ygx_topology_workspace_size(L)) return YGX_ERR_ARG;
+  ygx::Arena a{(char*)ws, 0, ws_bytes};
+  ygx::TopoScratch s = ygx::carve_topo(a, L);
+  const int64_t total = 2 * L - 1, ni = L - 1;
+  // flags, changed, stop, hist, max_level are contiguous: one memset.
+  if (cudaMemsetAsync(s.tree_flags, 0, (char*)(s.max_level + 64) - (char*)s.tree_flags, stream) !=
+      cudaSuccess)
+    return YGX_ERR_CUDA;
+  if (cudaMemsetAsync(s.stop, 0xFF, 64 * sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
+  if (cudaMemsetAsync(s.parent_claim, 0xFF, total * sizeof(int32_t), stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  ygx::k_karras<<<ygx::grid_for(L, 256), 256, 0, stream>>>(
+      leaf_codes, leaf_starts, leaf_ends, L, index_bits, left, right, left_is_leaf, right_is_leaf,
+      node_ranges, left32, right32, s.parent_claim);
+  YGX_CHECK_LAUNCH();
+  ygx::k_leaf_ranges<<<ygx::grid_for(L, 256), 256, 0, stream>>>(leaf_starts, leaf_ends, L,
+                                                                index_bits, node_ranges, left32,
+                                                                right32);
+  YGX_CHECK_LAUNCH();
+  ygx::k_parent_decode<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.parent_claim, total, ni,
+                                                                      index_bits, parent, parent32);
+  YGX_CHECK_LAUNCH();
+  ygx::k_check_wellformed<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      parent32, left32, right32, total, ni, s.tree_flags);
+  YGX_CHECK_LAUNCH();
+  // Levels by pointer doubling: bit_length(total) + 1 rounds.
+  int bl = 0;
+  while (((int64_t)1 << bl) <= total) ++bl;
+  const int rounds = bl + 1 > 1 ? bl + 1 : 1;
+  ygx::k_depth_init<<<ygx::grid_for(total, 256), 256, 0, stream>>>(parent32, total, s.sc[0], s.d[0]);
+  YGX_CHECK_LAUNCH();
+  for (int r = 0; r < rounds; ++r) {
+    ygx::k_depth_round<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+        s.sc[r & 1], s.d[r & 1], s.sc[(r + 1) & 1], s.d[(r + 1) & 1], total, r, s.changed, s.stop);
+    YGX_CHECK_LAUNCH();
+  }
+  ygx::k_depth_finish<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      s.sc[0], s.d[0], s.sc[1], s.d[1], total, s.stop, (uint32_t)rounds, index_bits, node_level,
+      level32, s.level_keys, s.level_hist, s.max_level, s.tree_flags);
+  YGX_CHECK_LAUNCH();
+  ygx::k_level_tables<<<1, 32, 0, stream>>>(s.level_hist, s.max_level, index_bits, level_offsets,
+                                            num_levels);
+  YGX_CHECK_LAUNCH();
+  // nodes_by_level: stable argsort of node_level (levels < 2^16).
+  int rc = ygx::onesweep_sort(s.level_keys, nullptr, total, 0, 16, s.level_keys_sorted, s.nbl_u32,
+                              s.sort, false, s.status, stream);
+  if (rc) return rc;
+  ygx::k_u32_to_index<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.nbl_u32, total, index_bits,
+                                                                     nodes_by_level, nbl32);
+  YGX_CHECK_LAUNCH();
+  if (tree_flags_out &&
+      cudaMemcpyAsync(tree_flags_out, s.tree_flags, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                      stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  return YGX_OK;
+}
+
+}  // extern "C"

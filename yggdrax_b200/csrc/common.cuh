@@ -1,0 +1,113 @@
+// Shared helpers for the yggdrax_b200 CUDA kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "../../include/ygx.h"
+
+namespace ygx {
+
+constexpr int kNumSMs = 148;
+
+// Device-side status word.  Kernels never trap: a bounded spin that gives up,
+// or a capacity that is exceeded, ORs a flag in here and the kernel returns.
+// Flags map one-to-one onto the YGX_ERR_* return codes.
+enum StatusFlag : uint32_t {
+  kFlagTimeout = 1u << 0,
+  kFlagQueueOverflow = 1u << 1,
+  kFlagFarOverflow = 1u << 2,
+  kFlagNearOverflow = 1u << 3,
+  kFlagMalformed = 1u << 4,
+  kFlagBadInput = 1u << 5,
+};
+
+// Iteration limit of every device-side spin (decoupled look-back).  A wait
+// this long means a producer did not make progress; the waiter records
+// kFlagTimeout and continues with what it has, so the launch always ends.
+#ifndef YGX_SPIN_LIMIT
+#define YGX_SPIN_LIMIT (1u << 22)
+#endif
+
+__device__ __forceinline__ void raise_flag(uint32_t* status, uint32_t f) {
+  if (status) atomicOr(status, f);
+}
+
+__device__ __forceinline__ int clz64(uint64_t x) { return x ? __clzll((long long)x) : 64; }
+
+// 21-bit spread / compact with the interleave masks of a 63-bit Morton code.
+__host__ __device__ __forceinline__ uint64_t spread3(uint64_t x) {
+  x &= 0x1FFFFFull;
+  x = (x | (x << 32)) & 0x1F00000000FFFFull;
+  x = (x | (x << 16)) & 0x1F0000FF0000FFull;
+  x = (x | (x << 8)) & 0x100F00F00F00F00Full;
+  x = (x | (x << 4)) & 0x10C30C30C30C30C3ull;
+  x = (x | (x << 2)) & 0x1249249249249249ull;
+  return x;
+}
+__host__ __device__ __forceinline__ uint64_t compact3(uint64_t x) {
+  x &= 0x1249249249249249ull;
+  x = (x | (x >> 2)) & 0x10C30C30C30C30C3ull;
+  x = (x | (x >> 4)) & 0x100F00F00F00F00Full;
+  x = (x | (x >> 8)) & 0x1F0000FF0000FFull;
+  x = (x | (x >> 16)) & 0x1F00000000FFFFull;
+  x = (x | (x >> 32)) & 0x1FFFFFull;
+  return x;
+}
+
+// uint64 shifts with the "shift >= 64 gives 0" rule of the reference's
+// uint64 arithmetic.
+__host__ __device__ __forceinline__ uint64_t shr64(uint64_t x, uint64_t s) { return s >= 64 ? 0 : (x >> s); }
+__host__ __device__ __forceinline__ uint64_t shl64(uint64_t x, uint64_t s) { return s >= 64 ? 0 : (x << s); }
+
+// NaN-propagating min / max (the reference's minimum / maximum).
+__device__ __forceinline__ float fmin_nan(float a, float b) {
+  return (a != a || b != b) ? __int_as_float(0x7fc00000) : fminf(a, b);
+}
+__device__ __forceinline__ float fmax_nan(float a, float b) {
+  return (a != a || b != b) ? __int_as_float(0x7fc00000) : fmaxf(a, b);
+}
+
+// Index outputs are INDEX_DTYPE: int64 by default, int32 on request.
+template <typename T>
+__device__ __forceinline__ void store_index(void* base, int64_t i, int64_t v) {
+  reinterpret_cast<T*>(base)[i] = static_cast<T>(v);
+}
+__device__ __forceinline__ void store_idx(void* base, int index_bits, int64_t i, int64_t v) {
+  if (index_bits == 32) reinterpret_cast<int32_t*>(base)[i] = (int32_t)v;
+  else reinterpret_cast<int64_t*>(base)[i] = v;
+}
+__device__ __forceinline__ int64_t load_idx(const void* base, int index_bits, int64_t i) {
+  if (index_bits == 32) return reinterpret_cast<const int32_t*>(base)[i];
+  return reinterpret_cast<const int64_t*>(base)[i];
+}
+
+inline int grid_for(int64_t n, int block, int max_blocks = kNumSMs * 16) {
+  int64_t g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > max_blocks) g = max_blocks;
+  return (int)g;
+}
+
+inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+
+// Bump allocator over a caller-provided workspace.
+struct Arena {
+  char* base;
+  size_t used;
+  size_t cap;
+  template <typename T>
+  T* take(size_t count) {
+    size_t off = align_up(used);
+    used = off + count * sizeof(T);
+    return base ? reinterpret_cast<T*>(base + off) : nullptr;
+  }
+};
+
+}  // namespace ygx
+
+#define YGX_CHECK_LAUNCH()                           \
+  do {                                               \
+    cudaError_t _e = cudaGetLastError();             \
+    if (_e != cudaSuccess) return YGX_ERR_CUDA;      \
+  } while (0)

@@ -1,0 +1,300 @@
+// Bounding box + 63-bit Morton encode + stable sort (L0 of the pipeline).
+//
+// Replaces infer_bounds (bounds.py:11-33), morton_encode_impl
+// (morton.py:43-77) and the stable argsort of the codes
+// (_tree_impl.py:401, tree.py:403).
+//
+// k_bbox reads the positions once with 16-byte loads and reduces min/max per
+// axis; its last CTA (arrival counter, no waiting) applies the reference's
+// padding.  k_encode reads the positions again (the second read is served
+// largely from L2 for inputs up to ~100 MB), writes the codes, and builds the
+// per-pass digit histograms of the following radix sort so the sort never
+// re-reads the keys for them.
+#include "sort.cuh"
+
+namespace ygx {
+namespace {
+
+constexpr int kBBoxThreads = 256;
+constexpr int kBBoxBlocks = kNumSMs * 4;
+
+struct Box {
+  float mn[3], mx[3];
+  unsigned nan;
+  __device__ void init() {
+    for (int a = 0; a < 3; ++a) { mn[a] = __int_as_float(0x7f800000); mx[a] = -__int_as_float(0x7f800000); }
+    nan = 0;
+  }
+  __device__ __forceinline__ void add(int a, float v) {
+    if (v != v) nan |= 1u << a;
+    mn[a] = fminf(mn[a], v);
+    mx[a] = fmaxf(mx[a], v);
+  }
+  __device__ void merge(const Box& o) {
+    for (int a = 0; a < 3; ++a) { mn[a] = fminf(mn[a], o.mn[a]); mx[a] = fmaxf(mx[a], o.mx[a]); }
+    nan |= o.nan;
+  }
+  __device__ void warp_reduce() {
+    for (int off = 16; off > 0; off >>= 1) {
+      for (int a = 0; a < 3; ++a) {
+        mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], off));
+        mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], off));
+      }
+      nan |= __shfl_xor_sync(0xffffffffu, nan, off);
+    }
+  }
+};
+
+// Four particles = twelve floats = three 16-byte words.
+__device__ __forceinline__ void load_chunk(const float* __restrict__ pos, int64_t c, bool vec,
+                                           float f[12]) {
+  if (vec) {
+    const float4* p4 = reinterpret_cast<const float4*>(pos) + 3 * c;
+    float4 a = __ldg(p4), b = __ldg(p4 + 1), d = __ldg(p4 + 2);
+    f[0] = a.x; f[1] = a.y; f[2] = a.z; f[3] = a.w;
+    f[4] = b.x; f[5] = b.y; f[6] = b.z; f[7] = b.w;
+    f[8] = d.x; f[9] = d.y; f[10] = d.z; f[11] = d.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 12; ++k) f[k] = __ldg(pos + 12 * c + k);
+  }
+}
+
+__global__ void __launch_bounds__(kBBoxThreads)
+    k_bbox(const float* __restrict__ pos, int64_t n, float* __restrict__ partials,
+           unsigned* __restrict__ arrivals, float* __restrict__ bounds_out) {
+  __shared__ Box s_box[kBBoxThreads / 32];
+  __shared__ bool s_last;
+  Box b;
+  b.init();
+  const bool vec = (reinterpret_cast<uintptr_t>(pos) & 15) == 0;
+  const int64_t chunks = n / 4;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < chunks;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    float f[12];
+    load_chunk(pos, c, vec, f);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) b.add(k % 3, f[k]);
+  }
+  if (blockIdx.x == 0)
+    for (int64_t i = chunks * 4 + threadIdx.x; i < n; i += blockDim.x)
+      for (int a = 0; a < 3; ++a) b.add(a, pos[3 * i + a]);
+  b.warp_reduce();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) s_box[warp] = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Box t = s_box[0];
+    for (int w = 1; w < kBBoxThreads / 32; ++w) t.merge(s_box[w]);
+    float* out = partials + 8 * blockIdx.x;
+    for (int a = 0; a < 3; ++a) { out[a] = t.mn[a]; out[3 + a] = t.mx[a]; }
+    out[6] = __uint_as_float(t.nan);
+    __threadfence();
+    unsigned ticket = atomicAdd(arrivals, 1u);
+    s_last = ticket == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  // Last CTA to arrive: reduce the per-CTA partials.
+  __threadfence();
+  Box t;
+  t.init();
+  for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+    const volatile float* p = partials + 8 * k;
+    Box o;
+    for (int a = 0; a < 3; ++a) { o.mn[a] = p[a]; o.mx[a] = p[3 + a]; }
+    o.nan = __float_as_uint(p[6]);
+    t.merge(o);
+  }
+  t.warp_reduce();
+  if (lane == 0) s_box[warp] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Box r = s_box[0];
+    for (int w = 1; w < kBBoxThreads / 32; ++w) r.merge(s_box[w]);
+    const float qnan = __int_as_float(0x7fc00000);
+    for (int a = 0; a < 3; ++a) {
+      float lo = (r.nan >> a) & 1 ? qnan : r.mn[a];
+      float hi = (r.nan >> a) & 1 ? qnan : r.mx[a];
+      // bounds.py:29-33: span * 0.05 (fp32), floor 1e-6, min - pad, max + pad
+      float span = __fsub_rn(hi, lo);
+      float pad = fmax_nan(__fmul_rn(span, 0.05f), 1e-6f);
+      bounds_out[a] = __fsub_rn(lo, pad);
+      bounds_out[3 + a] = __fadd_rn(hi, pad);
+    }
+    *arrivals = 0;  // ready for the next call
+  }
+}
+
+// morton.py:64-77 in fp32 with IEEE division and round-half-even.
+__device__ __forceinline__ uint64_t encode_one(float x, float y, float z, const float* mn,
+                                               const float* span) {
+  float v[3] = {x, y, z};
+  uint64_t q[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float norm = __fdiv_rn(__fsub_rn(v[a], mn[a]), span[a]);
+    norm = fminf(fmaxf(norm, 0.0f), 1.0f);  // NaN -> 0 (no integer image)
+    q[a] = __float2ull_rn(__fmul_rn(norm, 2097151.0f));
+  }
+  return spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+}
+
+constexpr int kEncodeThreads = 256;
+
+__global__ void __launch_bounds__(kEncodeThreads)
+    k_encode(const float* __restrict__ pos, int64_t n, const float* __restrict__ bounds,
+             uint64_t* __restrict__ codes, uint32_t* __restrict__ hist, int hist_passes) {
+  __shared__ uint32_t s_hist[8 * kSortRadix];
+  for (int i = threadIdx.x; i < hist_passes * kSortRadix; i += blockDim.x) s_hist[i] = 0;
+  __syncthreads();
+  float mn[3], span[3];
+  for (int a = 0; a < 3; ++a) {
+    mn[a] = bounds[a];
+    span[a] = __fsub_rn(bounds[3 + a], bounds[a]);
+  }
+  const bool vec = (reinterpret_cast<uintptr_t>(pos) & 15) == 0 &&
+                   (reinterpret_cast<uintptr_t>(codes) & 15) == 0;
+  const int64_t chunks = (n + 3) / 4;
+  const int64_t full = n / 4;
+  const int lane = threadIdx.x & 31;
+  // Every lane of a warp runs the same number of iterations so the
+  // warp-aggregated histogram updates below see a full warp.
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t start = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+  for (int64_t cw = start; cw < chunks; cw += stride) {
+    const int64_t c = cw + lane;
+    uint64_t code[4];
+    int valid = 0;
+    if (c < full) {
+      float f[12];
+      load_chunk(pos, c, vec, f);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) code[k] = encode_one(f[3 * k], f[3 * k + 1], f[3 * k + 2], mn, span);
+      valid = 4;
+      if (vec) {
+        ulonglong2* o = reinterpret_cast<ulonglong2*>(codes + 4 * c);
+        o[0] = make_ulonglong2(code[0], code[1]);
+        o[1] = make_ulonglong2(code[2], code[3]);
+      } else {
+        for (int k = 0; k < 4; ++k) codes[4 * c + k] = code[k];
+      }
+    } else if (c < chunks) {
+      for (int64_t i = 4 * c; i < n; ++i, ++valid) {
+        code[valid] = encode_one(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], mn, span);
+        codes[i] = code[valid];
+      }
+    }
+    if (hist_passes > 0) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        for (int p = 0; p < hist_passes; ++p) {
+          uint32_t d = k < valid ? (uint32_t)(code[k] >> (p * kSortRadixBits)) & (kSortRadix - 1)
+                                 : 0xFFFFu;
+          unsigned peers = __match_any_sync(0xffffffffu, d);
+          if (d != 0xFFFFu && lane == __ffs(peers) - 1)
+            atomicAdd(&s_hist[p * kSortRadix + d], (uint32_t)__popc(peers));
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < hist_passes * kSortRadix; i += blockDim.x)
+    if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
+}
+
+}  // namespace
+
+struct EncodeSortLayout {
+  uint32_t* status;
+  float* partials;
+  unsigned* arrivals;
+  SortScratch sort;
+};
+
+static EncodeSortLayout carve_encode_sort(Arena& a, int64_t n) {
+  EncodeSortLayout l;
+  l.status = a.take<uint32_t>(64);
+  l.partials = a.take<float>(8 * kBBoxBlocks);
+  l.arrivals = a.take<unsigned>(64);
+  l.sort = carve_sort_scratch(a, n);
+  return l;
+}
+
+}  // namespace ygx
+
+extern "C" {
+
+size_t ygx_encode_sort_workspace_size(int64_t n) {
+  ygx::Arena a{nullptr, 0, 0};
+  ygx::carve_encode_sort(a, n);
+  return a.used + 256;
+}
+
+int ygx_workspace_init(void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (!ws || ws_bytes < 512) return YGX_ERR_ARG;
+  return cudaMemsetAsync(ws, 0, 512, stream) == cudaSuccess ? YGX_OK : YGX_ERR_CUDA;
+}
+
+int ygx_status_read(const void* ws, uint32_t* host_flags, cudaStream_t stream) {
+  if (!ws || !host_flags) return YGX_ERR_ARG;
+  if (cudaMemcpyAsync(host_flags, ws, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
+      cudaSuccess)
+    return YGX_ERR_CUDA;
+  if (cudaStreamSynchronize(stream) != cudaSuccess) return YGX_ERR_CUDA;
+  return YGX_OK;
+}
+
+int ygx_bounds(const float* positions, int64_t n, float* bounds_out, void* ws, size_t ws_bytes,
+               cudaStream_t stream) {
+  if (n < 1 || !positions || !bounds_out || !ws) return YGX_ERR_ARG;
+  if (ws_bytes < ygx_encode_sort_workspace_size(0)) return YGX_ERR_ARG;
+  ygx::Arena a{(char*)ws, 0, ws_bytes};
+  ygx::EncodeSortLayout l = ygx::carve_encode_sort(a, 0);
+  if (cudaMemsetAsync(l.arrivals, 0, sizeof(unsigned), stream) != cudaSuccess) return YGX_ERR_CUDA;
+  int grid = ygx::grid_for((n + 3) / 4, ygx::kBBoxThreads, ygx::kBBoxBlocks);
+  ygx::k_bbox<<<grid, ygx::kBBoxThreads, 0, stream>>>(positions, n, l.partials, l.arrivals,
+                                                      bounds_out);
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
+int ygx_morton_encode(const float* positions, int64_t n, const float* bounds, uint64_t* codes,
+                      cudaStream_t stream) {
+  if (n < 0 || (n > 0 && (!positions || !bounds || !codes))) return YGX_ERR_ARG;
+  if (n == 0) return YGX_OK;
+  int grid = ygx::grid_for((n + 3) / 4, ygx::kEncodeThreads, ygx::kNumSMs * 8);
+  ygx::k_encode<<<grid, ygx::kEncodeThreads, 0, stream>>>(positions, n, bounds, codes, nullptr, 0);
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
+int ygx_encode_sort(const float* positions, int64_t n, const float* bounds_in, float* bounds_out,
+                    uint64_t* codes_sorted, uint32_t* order, void* ws, size_t ws_bytes,
+                    cudaStream_t stream) {
+  if (n < 1 || !positions || !bounds_out || !codes_sorted || !order || !ws) return YGX_ERR_ARG;
+  if (ws_bytes < ygx_encode_sort_workspace_size(n)) return YGX_ERR_ARG;
+  ygx::Arena a{(char*)ws, 0, ws_bytes};
+  ygx::EncodeSortLayout l = ygx::carve_encode_sort(a, n);
+  if (bounds_in) {
+    if (cudaMemcpyAsync(bounds_out, bounds_in, 6 * sizeof(float), cudaMemcpyDeviceToDevice,
+                        stream) != cudaSuccess)
+      return YGX_ERR_CUDA;
+  } else {
+    if (cudaMemsetAsync(l.arrivals, 0, sizeof(unsigned), stream) != cudaSuccess) return YGX_ERR_CUDA;
+    int grid = ygx::grid_for((n + 3) / 4, ygx::kBBoxThreads, ygx::kBBoxBlocks);
+    ygx::k_bbox<<<grid, ygx::kBBoxThreads, 0, stream>>>(positions, n, l.partials, l.arrivals,
+                                                        bounds_out);
+    YGX_CHECK_LAUNCH();
+  }
+  const int passes = ygx::sort_passes(0, 63);
+  if (ygx::sort_scratch_reset(l.sort, n, passes, stream) != cudaSuccess) return YGX_ERR_CUDA;
+  int grid = ygx::grid_for((n + 3) / 4, ygx::kEncodeThreads, ygx::kNumSMs * 8);
+  ygx::k_encode<<<grid, ygx::kEncodeThreads, 0, stream>>>(positions, n, bounds_out, codes_sorted,
+                                                          l.sort.hist, passes);
+  YGX_CHECK_LAUNCH();
+  return ygx::onesweep_sort(codes_sorted, nullptr, n, 0, 63, codes_sorted, order, l.sort, true,
+                            l.status, stream);
+}
+
+}  // extern "C"

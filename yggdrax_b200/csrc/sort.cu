@@ -1,0 +1,289 @@
+// Onesweep stable LSD radix sort (Adinets & Merrill 2022 style) for
+// sm_100a.  Each pass is one kernel: a CTA takes the next tile ticket, ranks
+// its 4096 keys stably with warp match-any multisplit, publishes its digit
+// counts, resolves its global digit offsets by decoupled look-back over the
+// preceding tiles (bounded spin), then scatters through shared memory so
+// global writes are contiguous within each digit run.
+#include "sort.cuh"
+
+namespace ygx {
+
+namespace {
+
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagInc = 2u << 30;
+constexpr uint32_t kCountMask = (1u << 30) - 1;
+
+__device__ __forceinline__ uint32_t ld_volatile_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_volatile_u32(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__global__ void k_histogram(const uint64_t* __restrict__ keys, int64_t n, int begin_bit,
+                            int passes, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s_hist[8 * kSortRadix];
+  for (int i = threadIdx.x; i < passes * kSortRadix; i += blockDim.x) s_hist[i] = 0;
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    hist_add_key(s_hist, keys[i], begin_bit, passes);
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * kSortRadix; i += blockDim.x)
+    if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
+}
+
+// One CTA per pass: exclusive scan of 256 digit counts.
+__global__ void k_hist_scan(const uint32_t* __restrict__ hist, uint32_t* __restrict__ offsets) {
+  __shared__ uint32_t s[kSortRadix];
+  const int p = blockIdx.x, t = threadIdx.x;
+  uint32_t v = hist[p * kSortRadix + t];
+  s[t] = v;
+  __syncthreads();
+  for (int off = 1; off < kSortRadix; off <<= 1) {
+    uint32_t add = t >= off ? s[t - off] : 0;
+    __syncthreads();
+    s[t] += add;
+    __syncthreads();
+  }
+  offsets[p * kSortRadix + t] = s[t] - v;
+}
+
+struct __align__(16) OnesweepSmem {
+  uint32_t warp_hist[kSortThreads / 32][kSortRadix];
+  uint32_t tile_start[kSortRadix];
+  uint32_t glob[kSortRadix];
+  uint32_t warp_tot[kSortThreads / 32];
+  uint32_t ticket;
+  uint64_t keys[kSortTile];
+  uint32_t vals[kSortTile];
+};
+
+template <bool kIotaValues>
+__global__ void __launch_bounds__(kSortThreads, 3)
+    k_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+               int64_t n, int shift, const uint32_t* __restrict__ digit_offsets,
+               uint32_t* __restrict__ lookback, uint32_t* __restrict__ ticket_counter,
+               uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
+               uint32_t* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  OnesweepSmem& sm = *reinterpret_cast<OnesweepSmem*>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  for (int i = tid; i < (kSortThreads / 32) * kSortRadix; i += kSortThreads)
+    (&sm.warp_hist[0][0])[i] = 0;
+  if (tid == 0) sm.ticket = atomicAdd(ticket_counter, 1u);
+  __syncthreads();
+  const uint32_t tile = sm.ticket;
+  const int64_t base = (int64_t)tile * kSortTile;
+  const int64_t wbase = base + (int64_t)warp * (kSortItems * 32);
+
+  uint64_t keys[kSortItems];
+  uint16_t rank[kSortItems];
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    int64_t idx = wbase + i * 32 + lane;
+    keys[i] = idx < n ? keys_in[idx] : ~0ull;
+  }
+  const unsigned lt_mask = (1u << lane) - 1u;
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    uint32_t d = (uint32_t)(keys[i] >> shift) & (kSortRadix - 1);
+    unsigned peers = __match_any_sync(0xffffffffu, d);
+    int leader = __ffs(peers) - 1;
+    uint32_t old = 0;
+    if (lane == leader) {
+      old = sm.warp_hist[warp][d];
+      sm.warp_hist[warp][d] = old + __popc(peers);
+    }
+    old = __shfl_sync(0xffffffffu, old, leader);
+    rank[i] = (uint16_t)(old + __popc(peers & lt_mask));
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // Thread t owns digit t: warp-exclusive prefixes and the tile total.
+  const int d = tid;
+  uint32_t total = 0;
+#pragma unroll
+  for (int w = 0; w < kSortThreads / 32; ++w) {
+    uint32_t c = sm.warp_hist[w][d];
+    sm.warp_hist[w][d] = total;
+    total += c;
+  }
+  // Publish this tile's digit count as early as possible.
+  uint32_t* my_lb = lookback + (size_t)tile * kSortRadix;
+  if (tile == 0) st_volatile_u32(&my_lb[d], kFlagInc | total);
+  else st_volatile_u32(&my_lb[d], kFlagAgg | total);
+
+  // Block exclusive scan of the digit totals -> tile-local digit starts.
+  uint32_t incl = total;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    uint32_t v = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += v;
+  }
+  if (lane == 31) sm.warp_tot[warp] = incl;
+  __syncthreads();
+  uint32_t wpre = 0;
+  for (int w = 0; w < warp; ++w) wpre += sm.warp_tot[w];
+  sm.tile_start[d] = wpre + incl - total;
+
+  // Decoupled look-back for digit d.
+  uint32_t excl = 0;
+  if (tile > 0) {
+    int64_t j = (int64_t)tile - 1;
+    while (j >= 0) {
+      const uint32_t* p = lookback + (size_t)j * kSortRadix + d;
+      uint32_t v = ld_volatile_u32(p);
+      uint32_t spins = 0;
+      while ((v & ~kCountMask) == 0 && spins < YGX_SPIN_LIMIT) {
+        __nanosleep(32);
+        v = ld_volatile_u32(p);
+        ++spins;
+      }
+      if ((v & ~kCountMask) == 0) {
+        raise_flag(status, kFlagTimeout);
+        break;
+      }
+      excl += v & kCountMask;
+      if ((v & ~kCountMask) == kFlagInc) break;
+      --j;
+    }
+    st_volatile_u32(&my_lb[d], kFlagInc | ((excl + total) & kCountMask));
+  }
+  sm.glob[d] = digit_offsets[d] + excl;
+  __syncthreads();
+
+  // Scatter into shared memory in tile-sorted order.
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    uint32_t dd = (uint32_t)(keys[i] >> shift) & (kSortRadix - 1);
+    uint32_t pos = sm.tile_start[dd] + sm.warp_hist[warp][dd] + rank[i];
+    int64_t idx = wbase + i * 32 + lane;
+    sm.keys[pos] = keys[i];
+    sm.vals[pos] = kIotaValues ? (uint32_t)idx : (idx < n ? vals_in[idx] : 0u);
+  }
+  __syncthreads();
+  const int64_t nvalid = n - base < kSortTile ? n - base : kSortTile;
+#pragma unroll 4
+  for (int k = tid; k < nvalid; k += kSortThreads) {
+    uint64_t key = sm.keys[k];
+    uint32_t dd = (uint32_t)(key >> shift) & (kSortRadix - 1);
+    uint32_t g = sm.glob[dd] + (uint32_t)k - sm.tile_start[dd];
+    if (g < (uint64_t)n) {
+      keys_out[g] = key;
+      vals_out[g] = sm.vals[k];
+    } else {
+      raise_flag(status, kFlagBadInput);  // inconsistent histogram: never write out of range
+    }
+  }
+}
+
+}  // namespace
+
+size_t onesweep_scratch_bytes(int64_t n, int max_passes) {
+  Arena a{nullptr, 0, 0};
+  carve_sort_scratch(a, n, max_passes);
+  return a.used + 256;
+}
+
+SortScratch carve_sort_scratch(Arena& a, int64_t n, int max_passes) {
+  SortScratch s;
+  const int64_t tiles = sort_tiles(n) > 0 ? sort_tiles(n) : 1;
+  // hist, lookback and counters are contiguous so one memset clears them.
+  s.hist = a.take<uint32_t>((size_t)max_passes * kSortRadix);
+  s.lookback = a.take<uint32_t>((size_t)max_passes * tiles * kSortRadix);
+  s.counters = a.take<uint32_t>(64);
+  s.offsets = a.take<uint32_t>((size_t)max_passes * kSortRadix);
+  s.keys_tmp = a.take<uint64_t>((size_t)(n > 0 ? n : 1));
+  s.vals_tmp = a.take<uint32_t>((size_t)(n > 0 ? n : 1));
+  return s;
+}
+
+cudaError_t sort_scratch_reset(const SortScratch& s, int64_t n, int passes, cudaStream_t st) {
+  (void)passes;
+  size_t bytes = (size_t)((char*)(s.counters + 64) - (char*)s.hist);
+  return cudaMemsetAsync(s.hist, 0, bytes, st);
+}
+
+int onesweep_sort(const uint64_t* keys_in, const uint32_t* vals_in, int64_t n, int begin_bit,
+                  int end_bit, uint64_t* keys_out, uint32_t* vals_out, const SortScratch& s,
+                  bool hist_ready, uint32_t* status, cudaStream_t st) {
+  if (n <= 0) return YGX_OK;
+  if (n >= (int64_t)kCountMask) return YGX_ERR_ARG;
+  if (begin_bit < 0 || end_bit > 64 || end_bit <= begin_bit) return YGX_ERR_ARG;
+  if (vals_in != nullptr && (const void*)vals_in == (const void*)vals_out) return YGX_ERR_ARG;
+  const int passes = sort_passes(begin_bit, end_bit);
+  if (passes > 8) return YGX_ERR_ARG;
+  const int64_t tiles = sort_tiles(n);
+  if (!hist_ready) {
+    if (sort_scratch_reset(s, n, passes, st) != cudaSuccess) return YGX_ERR_CUDA;
+    k_histogram<<<grid_for(n, 256, kNumSMs * 4), 256, 0, st>>>(keys_in, n, begin_bit, passes,
+                                                               s.hist);
+    YGX_CHECK_LAUNCH();
+  }
+  k_hist_scan<<<passes, kSortRadix, 0, st>>>(s.hist, s.offsets);
+  YGX_CHECK_LAUNCH();
+
+  const size_t smem = sizeof(OnesweepSmem);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(k_onesweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_onesweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_done = true;
+  }
+  const uint64_t* src_k = keys_in;
+  const uint32_t* src_v = vals_in;
+  for (int p = 0; p < passes; ++p) {
+    bool to_out = ((passes - 1 - p) % 2) == 0;
+    uint64_t* dk = to_out ? keys_out : s.keys_tmp;
+    uint32_t* dv = to_out ? vals_out : s.vals_tmp;
+    if (p == 0 && (const void*)src_k == (const void*)dk) {
+      // Input aliases this pass's destination: stage it in the other buffer.
+      uint64_t* stage = to_out ? s.keys_tmp : keys_out;
+      if (cudaMemcpyAsync(stage, src_k, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, st) !=
+          cudaSuccess)
+        return YGX_ERR_CUDA;
+      src_k = stage;
+    }
+    uint32_t* lb = s.lookback + (size_t)p * tiles * kSortRadix;
+    const uint32_t* offs = s.offsets + p * kSortRadix;
+    int shift = begin_bit + p * kSortRadixBits;
+    if (p == 0 && src_v == nullptr)
+      k_onesweep<true><<<(unsigned)tiles, kSortThreads, smem, st>>>(
+          src_k, nullptr, n, shift, offs, lb, s.counters + p, dk, dv, status);
+    else
+      k_onesweep<false><<<(unsigned)tiles, kSortThreads, smem, st>>>(
+          src_k, src_v, n, shift, offs, lb, s.counters + p, dk, dv, status);
+    YGX_CHECK_LAUNCH();
+    src_k = dk;
+    src_v = dv;
+  }
+  return YGX_OK;
+}
+
+}  // namespace ygx
+
+extern "C" {
+
+size_t ygx_sort_pairs_workspace_size(int64_t n) {
+  return 256 + ygx::onesweep_scratch_bytes(n);
+}
+
+int ygx_sort_pairs(const uint64_t* keys_in, const uint32_t* values_in, int64_t n, int begin_bit,
+                   int end_bit, uint64_t* keys_out, uint32_t* values_out, void* ws,
+                   size_t ws_bytes, cudaStream_t stream) {
+  if (n < 0 || (n > 0 && (!keys_in || !keys_out || !values_out || !ws))) return YGX_ERR_ARG;
+  if (ws_bytes < ygx_sort_pairs_workspace_size(n)) return YGX_ERR_ARG;
+  ygx::Arena a{(char*)ws, 0, ws_bytes};
+  uint32_t* status = a.take<uint32_t>(64);
+  ygx::SortScratch s = ygx::carve_sort_scratch(a, n);
+  return ygx::onesweep_sort(keys_in, values_in, n, begin_bit, end_bit, keys_out, values_out, s,
+                            false, status, stream);
+}
+
+}  // extern "C"

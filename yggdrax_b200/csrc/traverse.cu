@@ -1,0 +1,705 @@
+// Symmetric dual-tree traversal (L3): replaces the count walk and the
+// compact fill walk of build_interactions_and_neighbors
+// (_interactions_impl.py:2600-3558) and the result layouts of
+// _result_to_interactions / _result_to_neighbors (:3561-3837).
+//
+// The pair set is the reference's: a breadth-first refinement of canonical
+// (lo, hi) node pairs from (root, root).  Per pair: MAC
+// (_interactions_impl.py:338-395) in fp32 in the reference's operation order,
+// ACCEPT / NEAR / REFINE (:713-728), split rule on the canonical orientation
+// and child pairs (:1262-1310).  An accepted pair lands in both endpoints'
+// far rows, a near leaf pair in both leaves' near rows.
+//
+// Each BFS generation is one launch over the current wavefront; a warp
+// processes 32 pairs, aggregates its counter/cursor atomics per distinct
+// node with match-any, and pushes its child pairs with one atomic per warp.
+// The count pass sizes the rows; the fill pass writes each entry into its
+// row at an atomic cursor; the finalize pass sorts every row (canonical
+// order) and widens it into the level-major int64/int32 outputs.
+#include "scan.cuh"
+
+namespace ygx {
+namespace {
+
+struct __align__(16) NodeRec {
+  float4 c;  // center x, y, z; MAC extent
+  int4 k;    // left child, right child (-1 for leaves), leaf position (-1 internal), 0
+};
+
+enum WalkMode { kCount = 0, kFill = 1 };
+enum MacKind { kMacBH = 0, kMacDehnen = 1, kMacEngblom = 2 };
+
+// stats words (uint64): see ygx.h YGX_TSTAT_*
+enum {
+  kStatFarTotal = 0,
+  kStatNearTotal = 1,
+  kStatMaxFar = 2,
+  kStatMaxNear = 3,
+  kStatAccept = 4,
+  kStatNear = 5,
+  kStatRefine = 6,
+  kStatMaxWf = 7,
+  kStatGens = 8,
+  kStatWords = 16
+};
+
+__global__ void k_node_recs(const float* __restrict__ center, const float* __restrict__ radius,
+                            const float* __restrict__ max_extent, const int32_t* __restrict__ left32,
+                            const int32_t* __restrict__ right32, const int32_t* __restrict__ leafpos,
+                            int64_t total, int mac, float dehnen_scale, NodeRec* __restrict__ recs,
+                            uint32_t* __restrict__ status) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    // _build_mac_extents (_interactions_impl.py:993-1061): sphere radius for
+    // dehnen/engblom (scaled for dehnen), box max half-extent for bh.  The
+    // zero-extent propagation there never fires for positive extents.
+    float e = mac == kMacBH ? max_extent[k] : radius[k];
+    if (mac == kMacDehnen) e = __fmul_rn(dehnen_scale, e);
+    if (!(e > 0.0f)) raise_flag(status, kFlagBadInput);
+    NodeRec r;
+    r.c = make_float4(center[3 * k], center[3 * k + 1], center[3 * k + 2], e);
+    r.k = make_int4(left32[k], right32[k], leafpos[k], 0);
+    recs[k] = r;
+  }
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Adds 1 to cnt[key] for every lane with pred, one atomic per distinct key.
+__device__ __forceinline__ void agg_count(int32_t* cnt, int key, bool pred) {
+  unsigned m = __ballot_sync(0xffffffffu, pred);
+  if (pred) {
+    unsigned peers = __match_any_sync(m, key);
+    if ((peers & lanemask_lt()) == 0) atomicAdd(&cnt[key], __popc(peers));
+  }
+}
+// Returns a unique slot cursor[key]++ for every lane with pred.
+__device__ __forceinline__ int agg_slot(int32_t* cur, int key, bool pred) {
+  unsigned m = __ballot_sync(0xffffffffu, pred);
+  int slot = 0;
+  if (pred) {
+    unsigned peers = __match_any_sync(m, key);
+    int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (((int)(threadIdx.x & 31)) == leader) base = atomicAdd(&cur[key], __popc(peers));
+    base = __shfl_sync(m, base, leader);
+    slot = base + __popc(peers & lanemask_lt());
+  }
+  return slot;
+}
+
+template <int kMode, int kMac>
+__global__ void __launch_bounds__(256)
+    k_walk_gen(const NodeRec* __restrict__ nodes, int32_t ni, float theta_sq, float theta,
+               const int2* __restrict__ wf_in, int2* __restrict__ wf_out,
+               uint32_t* __restrict__ sizes, int gen, uint32_t cap, int32_t* __restrict__ far_cnt,
+               int32_t* __restrict__ near_cnt, const int64_t* __restrict__ far_off,
+               const int64_t* __restrict__ near_off, const int32_t* __restrict__ far_expect,
+               const int32_t* __restrict__ near_expect, int32_t* __restrict__ far_src,
+               int32_t* __restrict__ near_nbr, unsigned long long* __restrict__ stats,
+               uint32_t* __restrict__ status) {
+  // After an overflow the counter may exceed the buffer: never read past it.
+  const uint32_t size = sizes[gen] < cap ? sizes[gen] : cap;
+  if (size == 0) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = lanemask_lt();
+  unsigned long long n_acc = 0, n_near = 0, n_ref = 0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < size;
+       base += stride) {
+    const int64_t i = base + lane;
+    const bool valid = i < size;
+    int t = 0, s = 0;
+    if (valid) {
+      int2 p = wf_in[i];
+      t = p.x;
+      s = p.y;
+    }
+    NodeRec A, B;
+    if (valid) { A = nodes[t]; B = nodes[s]; }
+    bool acc = false, nearp = false, refine = false;
+    if (valid) {
+      const float dx = __fsub_rn(A.c.x, B.c.x);
+      const float dy = __fsub_rn(A.c.y, B.c.y);
+      const float dz = __fsub_rn(A.c.z, B.c.z);
+      float d2 = __fmul_rn(dx, dx);
+      d2 = __fadd_rn(d2, __fmul_rn(dy, dy));
+      d2 = __fadd_rn(d2, __fmul_rn(dz, dz));
+      const float et = A.c.w, es = B.c.w;
+      bool ok;
+      if (kMac == kMacEngblom) {
+        const float big = fmax_nan(et, es), small = fmin_nan(et, es);
+        const float lhs = __fadd_rn(big, __fmul_rn(theta, small));
+        ok = __fmul_rn(lhs, lhs) <= __fmul_rn(theta_sq, d2);
+      } else {
+        const float sum = __fadd_rn(et, es);
+        ok = __fmul_rn(sum, sum) <= __fmul_rn(theta_sq, d2);
+      }
+      const bool diff = t != s;
+      acc = diff && d2 > 0.0f && ok;
+      nearp = !acc && diff && t >= ni && s >= ni;
+      refine = !acc && !nearp;
+    }
+    n_acc += __popc(__ballot_sync(0xffffffffu, acc));
+    n_near += __popc(__ballot_sync(0xffffffffu, nearp));
+    n_ref += __popc(__ballot_sync(0xffffffffu, refine));
+
+    if (kMode == kCount) {
+      agg_count(far_cnt, t, acc);
+      agg_count(far_cnt, s, acc);
+      agg_count(near_cnt, A.k.z, nearp);
+      agg_count(near_cnt, B.k.z, nearp);
+    } else {
+      int st = agg_slot(far_cnt, t, acc);
+      if (acc) {
+        if (st < far_expect[t]) far_src[far_off[t] + st] = s;
+        else raise_flag(status, kFlagFarOverflow);
+      }
+      int ss = agg_slot(far_cnt, s, acc);
+      if (acc) {
+        if (ss < far_expect[s]) far_src[far_off[s] + ss] = t;
+        else raise_flag(status, kFlagFarOverflow);
+      }
+      const int lt_ = nearp ? A.k.z : 0, ls_ = nearp ? B.k.z : 0;
+      int nt = agg_slot(near_cnt, lt_, nearp);
+      if (nearp) {
+        if (nt < near_expect[lt_]) near_nbr[near_off[lt_] + nt] = s;
+        else raise_flag(status, kFlagNearOverflow);
+      }
+      int ns = agg_slot(near_cnt, ls_, nearp);
+      if (nearp) {
+        if (ns < near_expect[ls_]) near_nbr[near_off[ls_] + ns] = t;
+        else raise_flag(status, kFlagNearOverflow);
+      }
+    }
+
+    // Children of a refined pair (_interactions_impl.py:1262-1310).
+    int nc = 0;
+    int2 ch[4];
+    if (refine) {
+      const bool same = t == s;
+      const bool t_int = t < ni, s_int = s < ni;
+      const float et = A.c.w, es = B.c.w;
+      const bool split_t = t_int && (same || !s_int || et >= es);
+      const bool split_s = s_int && (same || !t_int || es > et);
+      auto mk = [](int a, int b) { return a < b ? make_int2(a, b) : make_int2(b, a); };
+      if (split_t && split_s) {
+        if (same) {
+          ch[0] = mk(A.k.x, A.k.x);
+          ch[1] = mk(A.k.x, A.k.y);
+          ch[2] = mk(A.k.y, A.k.y);
+          nc = 3;
+        } else {
+          ch[0] = mk(A.k.x, B.k.x);
+          ch[1] = mk(A.k.x, B.k.y);
+          ch[2] = mk(A.k.y, B.k.x);
+          ch[3] = mk(A.k.y, B.k.y);
+          nc = 4;
+        }
+      } else if (split_t) {
+        ch[0] = mk(A.k.x, s);
+        ch[1] = mk(A.k.y, s);
+        nc = 2;
+      } else if (split_s) {
+        ch[0] = mk(t, B.k.x);
+        ch[1] = mk(t, B.k.y);
+        nc = 2;
+      }
+    }
+    int incl = nc;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      int v = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= off) incl += v;
+    }
+    const int wtotal = __shfl_sync(0xffffffffu, incl, 31);
+    if (wtotal > 0) {
+      uint32_t wbase = 0;
+      if (lane == 31) wbase = atomicAdd(&sizes[gen + 1], (uint32_t)wtotal);
+      wbase = __shfl_sync(0xffffffffu, wbase, 31);
+      const uint32_t o = wbase + (uint32_t)(incl - nc);
+      for (int k = 0; k < nc; ++k) {
+        if (o + k < cap) wf_out[o + k] = ch[k];
+        else raise_flag(status, kFlagQueueOverflow);
+      }
+    }
+  }
+  (void)lt;
+  if (lane == 0) {
+    if (n_acc) atomicAdd(&stats[kStatAccept], n_acc);
+    if (n_near) atomicAdd(&stats[kStatNear], n_near);
+    if (n_ref) atomicAdd(&stats[kStatRefine], n_ref);
+  }
+}
+
+__global__ void k_seed(int2* wf, uint32_t* sizes, int root) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    wf[0] = make_int2(root, root);
+    sizes[0] = 1;
+  }
+}
+
+// Totals and maxima of the count pass; max wavefront and generations.
+__global__ void k_count_stats(const int32_t* __restrict__ far_cnt, int64_t total,
+                              const int32_t* __restrict__ near_cnt, int64_t L,
+                              const uint32_t* __restrict__ sizes, int max_gens,
+                              unsigned long long* __restrict__ stats) {
+  unsigned long long fsum = 0, nsum = 0, fmax = 0, nmax = 0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    unsigned long long v = (unsigned long long)far_cnt[k];
+    fsum += v;
+    fmax = v > fmax ? v : fmax;
+  }
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < L;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    unsigned long long v = (unsigned long long)near_cnt[k];
+    nsum += v;
+    nmax = v > nmax ? v : nmax;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    fsum += __shfl_xor_sync(0xffffffffu, fsum, off);
+    nsum += __shfl_xor_sync(0xffffffffu, nsum, off);
+    unsigned long long a = __shfl_xor_sync(0xffffffffu, fmax, off);
+    unsigned long long b = __shfl_xor_sync(0xffffffffu, nmax, off);
+    fmax = a > fmax ? a : fmax;
+    nmax = b > nmax ? b : nmax;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (fsum) atomicAdd(&stats[kStatFarTotal], fsum);
+    if (nsum) atomicAdd(&stats[kStatNearTotal], nsum);
+    atomicMax(&stats[kStatMaxFar], fmax);
+    atomicMax(&stats[kStatMaxNear], nmax);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long mw = 1, g = 0;
+    for (int k = 0; k <= max_gens; ++k) {
+      if (sizes[k] == 0) break;
+      g = k + 1;
+      if (k > 0 && sizes[k] > mw) mw = sizes[k];
+    }
+    stats[kStatMaxWf] = mw;
+    stats[kStatGens] = g;
+  }
+}
+
+// counts in nodes_by_level order (for the level-major far layout).
+__global__ void k_gather_counts(const int32_t* __restrict__ cnt, const int32_t* __restrict__ order,
+                                int64_t m, int32_t* __restrict__ out) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += (int64_t)gridDim.x * blockDim.x)
+    out[r] = cnt[order ? order[r] : r];
+}
+
+// node_offsets[nbl[r]] = obl[r]; far_off (int64, node-indexed) the same;
+// counts widened; level_offsets = obl[tree_level_offsets[l]].
+__global__ void k_far_offsets(const int64_t* __restrict__ obl, const int32_t* __restrict__ nbl,
+                              const int32_t* __restrict__ cnt, int64_t total, int index_bits,
+                              int64_t* __restrict__ far_off, void* node_offsets, void* counts_out,
+                              const void* tree_level_offsets, int num_levels,
+                              void* level_offsets_out) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= total;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    if (r == total) {
+      store_idx(node_offsets, index_bits, total, obl[total]);
+    } else {
+      const int32_t v = nbl[r];
+      far_off[v] = obl[r];
+      store_idx(node_offsets, index_bits, v, obl[r]);
+      store_idx(counts_out, index_bits, r, cnt[r]);
+    }
+    if (r <= num_levels) {
+      int64_t li = load_idx(tree_level_offsets, index_bits, r);
+      store_idx(level_offsets_out, index_bits, r, obl[li]);
+    }
+  }
+}
+
+__global__ void k_near_offsets(const int64_t* __restrict__ off, const int32_t* __restrict__ cnt,
+                               int64_t L, int index_bits, void* offsets_out, void* counts_out) {
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j <= L;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    store_idx(offsets_out, index_bits, j, off[j]);
+    if (j < L) store_idx(counts_out, index_bits, j, cnt[j]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row finalize: sort each row ascending and widen it.  The network is the
+// all-ascending ("mirrored") bitonic sort: for each block size k the first
+// step pairs i with i ^ (k - 1), later steps pair i with i ^ j.  Every
+// comparator puts the minimum at the lower index, so a row of any length n
+// sorts as if padded with +inf, and comparators whose upper index is >= n
+// are no-ops that can be skipped -- no padding storage is needed.
+// Rows up to kWarpRowCap entries: one warp in shared memory; up to
+// kBlockRowCap: one CTA in shared memory; longer: one CTA in place in
+// global memory.
+
+constexpr int kWarpRowCap = 256;
+constexpr int kBlockRowCap = 8192;
+
+template <bool kBlockSync>
+__device__ __forceinline__ void mirrored_bitonic(int32_t* a, int64_t n, int tid, int nthreads) {
+  int64_t np2 = 1;
+  while (np2 < n) np2 <<= 1;
+  for (int64_t k = 2; k <= np2; k <<= 1) {
+    for (int64_t j = k >> 1; j > 0; j >>= 1) {
+      const bool first = j == (k >> 1);
+      // np2 / 2 comparators per step; comparator c -> lower index i
+      for (int64_t c = tid; c < (np2 >> 1); c += nthreads) {
+        const int64_t i = ((c / j) * (2 * j)) + (c % j);  // bit j of i is clear
+        const int64_t p = first ? (i ^ (k - 1)) : (i | j);
+        const int64_t lo = i < p ? i : p, hi = i < p ? p : i;
+        if (hi < n) {
+          int32_t x = a[lo], y = a[hi];
+          if (x > y) { a[lo] = y; a[hi] = x; }
+        }
+      }
+      if (kBlockSync) __syncthreads(); else __syncwarp();
+    }
+  }
+}
+
+// Writes the sorted row: values (sources or neighbours) in the index dtype
+// and, for far rows, the target node and its level for every entry.
+__device__ __forceinline__ void emit_row(const int32_t* a, int64_t n, int64_t off, int index_bits,
+                                         void* vals_out, void* tgt_out, void* lvl_out, int32_t tgt,
+                                         int32_t lvl, int tid, int nthreads) {
+  for (int64_t k = tid; k < n; k += nthreads) {
+    store_idx(vals_out, index_bits, off + k, a[k]);
+    if (tgt_out) {
+      store_idx(tgt_out, index_bits, off + k, tgt);
+      store_idx(lvl_out, index_bits, off + k, lvl);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256)
+    k_rows_small(int64_t rows, const int64_t* __restrict__ row_off,
+                 const int32_t* __restrict__ row_cnt, const int32_t* __restrict__ row_level,
+                 const int32_t* __restrict__ raw, int index_bits, void* vals_out, void* tgt_out,
+                 void* lvl_out, int32_t* __restrict__ big_rows, uint32_t* __restrict__ n_big) {
+  __shared__ int32_t s_buf[8][kWarpRowCap];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t warps = (int64_t)gridDim.x * 8;
+  int32_t* a = s_buf[w];
+  for (int64_t r = (int64_t)blockIdx.x * 8 + w; r < rows; r += warps) {
+    const int64_t off = row_off[r];
+    const int64_t n = row_cnt[r];
+    if (n == 0) continue;
+    if (n > kWarpRowCap) {
+      if (lane == 0) big_rows[atomicAdd(n_big, 1u)] = (int32_t)r;
+      continue;
+    }
+    for (int k = lane; k < n; k += 32) a[k] = raw[off + k];
+    __syncwarp();
+    mirrored_bitonic<false>(a, n, lane, 32);
+    emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, (int32_t)r,
+             row_level ? row_level[r] : 0, lane, 32);
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(1024)
+    k_rows_big(const int32_t* __restrict__ big_rows, const uint32_t* __restrict__ n_big,
+               const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
+               const int32_t* __restrict__ row_level, int32_t* __restrict__ raw, int index_bits,
+               void* vals_out, void* tgt_out, void* lvl_out) {
+  __shared__ int32_t s_a[kBlockRowCap];
+  const uint32_t nb = *n_big;
+  for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+    const int32_t r = big_rows[b];
+    const int64_t off = row_off[r];
+    const int64_t n = row_cnt[r];
+    int32_t* a;
+    if (n <= kBlockRowCap) {
+      a = s_a;
+      for (int64_t k = threadIdx.x; k < n; k += blockDim.x) a[k] = raw[off + k];
+      __syncthreads();
+    } else {
+      a = raw + off;  // in place, global memory
+    }
+    mirrored_bitonic<true>(a, n, threadIdx.x, blockDim.x);
+    emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, r, row_level ? row_level[r] : 0,
+             threadIdx.x, blockDim.x);
+    __syncthreads();
+  }
+}
+
+// Dense neighbour leaf positions (L x max_nbr) of _result_to_neighbors.
+__global__ void k_neighbor_leaf_positions(const int64_t* __restrict__ near_off,
+                                          const int32_t* __restrict__ near_cnt, int64_t L,
+                                          const void* neighbors, int index_bits,
+                                          const int32_t* __restrict__ leafpos, int64_t max_nbr,
+                                          void* out) {
+  const int64_t total = L * max_nbr;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = e / max_nbr, k = e - j * max_nbr;
+    int64_t v = -1;
+    if (k < near_cnt[j]) v = leafpos[load_idx(neighbors, index_bits, near_off[j] + k)];
+    store_idx(out, index_bits, e, v);
+  }
+}
+
+}  // namespace
+
+struct TravScratch {
+  uint32_t* status;
+  unsigned long long* stats;
+  uint32_t* sizes;  // per generation
+  uint32_t* n_big;
+  NodeRec* recs;
+  int32_t* far_cnt;
+  int32_t* near_cnt;
+  int32_t* far_cur;
+  int32_t* near_cur;
+  int32_t* cnt_by_level;
+  int64_t* obl;
+  int64_t* far_off;
+  int64_t* near_off;
+  int64_t* scan_tmp;
+  int32_t* big_rows;
+  int2* wf[2];
+};
+
+constexpr int kMaxGens = 4096;
+
+static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap) {
+  TravScratch s;
+  s.status = a.take<uint32_t>(64);
+  s.stats = a.take<unsigned long long>(kStatWords);
+  s.sizes = a.take<uint32_t>(kMaxGens + 2);
+  s.n_big = a.take<uint32_t>(64);
+  s.recs = a.take<NodeRec>(total);
+  s.far_cnt = a.take<int32_t>(total);
+  s.near_cnt = a.take<int32_t>(L);
+  s.far_cur = a.take<int32_t>(total);
+  s.near_cur = a.take<int32_t>(L);
+  s.cnt_by_level = a.take<int32_t>(total);
+  s.obl = a.take<int64_t>(total + 1);
+  s.far_off = a.take<int64_t>(total + 1);
+  s.near_off = a.take<int64_t>(L + 1);
+  s.scan_tmp = a.take<int64_t>(scan_scratch_elems(total > L ? total : L));
+  s.big_rows = a.take<int32_t>(total > L ? total : L);
+  s.wf[0] = a.take<int2>(cap);
+  s.wf[1] = a.take<int2>(cap);
+  return s;
+}
+
+template <int kMode>
+static int launch_gen(int mac, const TravScratch& s, int32_t ni, float theta_sq, float theta,
+                      int gen, uint32_t cap, const int32_t* far_expect, const int32_t* near_expect,
+                      int32_t* far_src, int32_t* near_nbr, int32_t* fc, int32_t* nc,
+                      cudaStream_t st) {
+  const int grid = kNumSMs * 8;
+  const int2* in = s.wf[gen & 1];
+  int2* out = s.wf[(gen + 1) & 1];
+#define YGX_GEN(MAC)                                                                          \
+  k_walk_gen<kMode, MAC><<<grid, 256, 0, st>>>(s.recs, ni, theta_sq, theta, in, out, s.sizes, \
+                                               gen, cap, fc, nc, s.far_off, s.near_off,       \
+                                               far_expect, near_expect, far_src, near_nbr,    \
+                                               s.stats, s.status)
+  if (mac == kMacBH) YGX_GEN(kMacBH);
+  else if (mac == kMacDehnen) YGX_GEN(kMacDehnen);
+  else YGX_GEN(kMacEngblom);
+#undef YGX_GEN
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
+}  // namespace ygx
+
+extern "C" {
+
+size_t ygx_traverse_workspace_size(int64_t total, int64_t num_leaves, int64_t wf_capacity) {
+  ygx::Arena a{nullptr, 0, 0};
+  ygx::carve_trav(a, total, num_leaves, wf_capacity);
+  return a.used + 256;
+}
+
+static int trav_setup(ygx::TravScratch& s, void* ws, size_t ws_bytes, int64_t total, int64_t L,
+                      int64_t cap) {
+  if (ws_bytes < ygx_traverse_workspace_size(total, L, cap)) return YGX_ERR_ARG;
+  ygx::Arena a{(char*)ws, 0, ws_bytes};
+  s = ygx::carve_trav(a, total, L, cap);
+  return YGX_OK;
+}
+
+// Count pass.  Builds the per-node walk records (center + MAC extent +
+// children + leaf position), walks from (root, root) generation by
+// generation until the wavefront is empty (checked every 16 generations),
+// and copies to the host: stats_out[YGX_TSTAT_WORDS] (far/near totals and
+// maxima, decision counters, max wavefront, generations) and the status
+// flags.  leafpos32[node] is the near-row position of a leaf (-1 for
+// internal nodes).  Synchronizes the stream.
+int ygx_traverse_count(const float* center, const float* radius, const float* max_extent,
+                       const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
+                       int64_t total, int64_t num_internal, int mac, float theta,
+                       float dehnen_radius_scale, int root, int64_t wf_capacity,
+                       uint64_t* stats_out, uint32_t* flags_out, void* ws, size_t ws_bytes,
+                       cudaStream_t stream) {
+  if (total < 3 || num_internal < 1 || mac < 0 || mac > 2 || wf_capacity < 4 ||
+      wf_capacity > (int64_t)UINT32_MAX || !stats_out || !flags_out)
+    return YGX_ERR_ARG;
+  const int64_t L = total - num_internal;
+  ygx::TravScratch s;
+  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity);
+  if (rc) return rc;
+  // theta^2 in fp32 (jnp.asarray(theta, float32) ** 2) and its sqrt.
+  const float th = theta;
+  const float theta_sq = th * th;
+  const float theta_r = sqrtf(theta_sq);
+  if (cudaMemsetAsync(s.status, 0, (char*)(s.n_big + 64) - (char*)s.status, stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  if (cudaMemsetAsync(s.far_cnt, 0, sizeof(int32_t) * total, stream) != cudaSuccess ||
+      cudaMemsetAsync(s.near_cnt, 0, sizeof(int32_t) * L, stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  ygx::k_node_recs<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      center, radius, max_extent, left32, right32, leafpos32, total, mac, dehnen_radius_scale,
+      s.recs, s.status);
+  YGX_CHECK_LAUNCH();
+  ygx::k_seed<<<1, 32, 0, stream>>>(s.wf[0], s.sizes, root);
+  YGX_CHECK_LAUNCH();
+  int gen = 0;
+  const int chunk = 16;
+  while (true) {
+    for (int k = 0; k < chunk && gen < ygx::kMaxGens; ++k, ++gen) {
+      rc = ygx::launch_gen<ygx::kCount>(mac, s, (int32_t)num_internal, theta_sq, theta_r, gen,
+                                        (uint32_t)wf_capacity, nullptr, nullptr, nullptr, nullptr,
+                                        s.far_cnt, s.near_cnt, stream);
+      if (rc) return rc;
+    }
+    uint32_t probe = 0, flags = 0;
+    if (cudaMemcpyAsync(&probe, s.sizes + gen, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(&flags, s.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+      return YGX_ERR_CUDA;
+    if (probe == 0 || flags != 0) break;
+    if (gen >= ygx::kMaxGens) {
+      flags_out[0] = ygx::kFlagQueueOverflow;
+      return YGX_ERR_QUEUE_OVERFLOW;
+    }
+  }
+  ygx::k_count_stats<<<ygx::grid_for(total, 256, ygx::kNumSMs * 4), 256, 0, stream>>>(
+      s.far_cnt, total, s.near_cnt, L, s.sizes, gen, s.stats);
+  YGX_CHECK_LAUNCH();
+  if (cudaMemcpyAsync(stats_out, s.stats, sizeof(uint64_t) * YGX_TSTAT_WORDS,
+                      cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaMemcpyAsync(flags_out, s.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  return YGX_OK;
+}
+
+// Fill pass (after a successful count pass on the same workspace).
+// Writes the level-major far layout and the near CSR: node_offsets
+// (total+1), far_counts (total), level_offsets (num_levels+1), near_offsets
+// (L+1), near_counts (L) in the index dtype, and the raw rows far_src32
+// (far total) / near_nbr32 (near total) in walk order.  `gens` is the
+// generation count reported by the count pass.  Does not synchronize.
+int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta, int root,
+                      int64_t wf_capacity, int gens, const int32_t* nbl32,
+                      const void* tree_level_offsets, int num_levels, int index_bits,
+                      void* node_offsets, void* far_counts, void* level_offsets,
+                      void* near_offsets, void* near_counts, int32_t* far_src32,
+                      int32_t* near_nbr32, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (total < 3 || num_internal < 1 || gens < 0 || gens > ygx::kMaxGens ||
+      (index_bits != 32 && index_bits != 64))
+    return YGX_ERR_ARG;
+  const int64_t L = total - num_internal;
+  ygx::TravScratch s;
+  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity);
+  if (rc) return rc;
+  const float th = theta;
+  const float theta_sq = th * th;
+  const float theta_r = sqrtf(theta_sq);
+  ygx::k_gather_counts<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.far_cnt, nbl32, total,
+                                                                      s.cnt_by_level);
+  YGX_CHECK_LAUNCH();
+  rc = ygx::exclusive_scan<int32_t>(s.cnt_by_level, total, s.obl, s.scan_tmp, stream);
+  if (rc) return rc;
+  ygx::k_far_offsets<<<ygx::grid_for(total + 1, 256), 256, 0, stream>>>(
+      s.obl, nbl32, s.far_cnt, total, index_bits, s.far_off, node_offsets, far_counts,
+      tree_level_offsets, num_levels, level_offsets);
+  YGX_CHECK_LAUNCH();
+  rc = ygx::exclusive_scan<int32_t>(s.near_cnt, L, s.near_off, s.scan_tmp, stream);
+  if (rc) return rc;
+  ygx::k_near_offsets<<<ygx::grid_for(L + 1, 256), 256, 0, stream>>>(s.near_off, s.near_cnt, L,
+                                                                     index_bits, near_offsets,
+                                                                     near_counts);
+  YGX_CHECK_LAUNCH();
+  if (cudaMemsetAsync(s.far_cur, 0, sizeof(int32_t) * total, stream) != cudaSuccess ||
+      cudaMemsetAsync(s.near_cur, 0, sizeof(int32_t) * L, stream) != cudaSuccess ||
+      cudaMemsetAsync(s.sizes, 0, sizeof(uint32_t) * (ygx::kMaxGens + 2), stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  ygx::k_seed<<<1, 32, 0, stream>>>(s.wf[0], s.sizes, root);
+  YGX_CHECK_LAUNCH();
+  for (int gen = 0; gen < gens; ++gen) {
+    rc = ygx::launch_gen<ygx::kFill>(mac, s, (int32_t)num_internal, theta_sq, theta_r, gen,
+                                     (uint32_t)wf_capacity, s.far_cnt, s.near_cnt, far_src32,
+                                     near_nbr32, s.far_cur, s.near_cur, stream);
+    if (rc) return rc;
+  }
+  return YGX_OK;
+}
+
+// Finalize: canonical (ascending) order within every row, widened into the
+// index-dtype outputs: far sources / targets / target_levels in the
+// level-major layout, near neighbours in leaf order.  far_src32 and
+// near_nbr32 are sorted in place for rows longer than 8192.  If
+// neighbor_leaf_positions is non-null it receives the dense (L x max_nbr)
+// leaf-position table.  Does not synchronize.
+int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capacity,
+                          const int32_t* level32, const int32_t* leafpos32, int index_bits,
+                          int32_t* far_src32, int32_t* near_nbr32, void* far_sources,
+                          void* far_targets, void* target_levels, void* neighbors,
+                          void* neighbor_leaf_positions, int64_t max_nbr, void* ws,
+                          size_t ws_bytes, cudaStream_t stream) {
+  if (total < 3 || num_internal < 1 || (index_bits != 32 && index_bits != 64)) return YGX_ERR_ARG;
+  const int64_t L = total - num_internal;
+  ygx::TravScratch s;
+  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity);
+  if (rc) return rc;
+  const int grid_small = ygx::kNumSMs * 16;
+  // far rows
+  if (cudaMemsetAsync(s.n_big, 0, sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
+  ygx::k_rows_small<<<grid_small, 256, 0, stream>>>(total, s.far_off, s.far_cnt, level32, far_src32,
+                                                    index_bits, far_sources, far_targets,
+                                                    target_levels, s.big_rows, s.n_big);
+  YGX_CHECK_LAUNCH();
+  ygx::k_rows_big<<<ygx::kNumSMs, 1024, 0, stream>>>(s.big_rows, s.n_big, s.far_off, s.far_cnt,
+                                                     level32, far_src32, index_bits, far_sources,
+                                                     far_targets, target_levels);
+  YGX_CHECK_LAUNCH();
+  // near rows
+  if (cudaMemsetAsync(s.n_big, 0, sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
+  ygx::k_rows_small<<<grid_small, 256, 0, stream>>>(L, s.near_off, s.near_cnt, nullptr, near_nbr32,
+                                                    index_bits, neighbors, nullptr, nullptr,
+                                                    s.big_rows, s.n_big);
+  YGX_CHECK_LAUNCH();
+  ygx::k_rows_big<<<ygx::kNumSMs, 1024, 0, stream>>>(s.big_rows, s.n_big, s.near_off, s.near_cnt,
+                                                     nullptr, near_nbr32, index_bits, neighbors,
+                                                     nullptr, nullptr);
+  YGX_CHECK_LAUNCH();
+  if (neighbor_leaf_positions && max_nbr > 0) {
+    ygx::k_neighbor_leaf_positions<<<ygx::grid_for(L * max_nbr, 256), 256, 0, stream>>>(
+        s.near_off, s.near_cnt, L, neighbors, index_bits, leafpos32, max_nbr,
+        neighbor_leaf_positions);
+    YGX_CHECK_LAUNCH();
+  }
+  return YGX_OK;
+}
+
+int ygx_traverse_status(const void* ws, uint32_t* flags_out, cudaStream_t stream) {
+  return ygx_status_read(ws, flags_out, stream);
+}
+
+}  // extern "C"

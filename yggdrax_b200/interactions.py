@@ -1,0 +1,520 @@
+"""Dual-tree far/near interaction lists on the GPU.
+
+Mirrors ``build_interactions_and_neighbors`` (yggdrax/interactions.py:338-448,
+yggdrax/_interactions_impl.py:6031-6144) and its containers
+(``_interactions_impl.py:235-242, 416-424, 566-644``).  The walk, the row
+sizing and the level-major / CSR layouts run as sm_100a kernels
+(``ygx_traverse_count`` / ``_fill`` / ``_finalize``).
+
+Output contract: the same pair sets and layouts as the reference; within
+every row the entries are in ascending order (the reference's within-row
+order comes from an unstable sort and is unspecified).  Capacity arguments
+keep their meaning: with ``traversal_config`` / ``max_interactions_per_node``
+/ ``max_pair_queue`` the reference's padded walk would fail on the same
+inputs, so the same ``RuntimeError`` is raised; without them the exact
+count-then-fill path is used, as in the reference.
+"""
+
+from __future__ import annotations
+
+import logging
+import os
+from dataclasses import dataclass
+from typing import Callable, Literal, NamedTuple, Optional
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .dtypes import INDEX_BITS, INDEX_DTYPE
+from .tree import _dev_of, resolve_tree_topology
+
+logger = logging.getLogger(__name__)
+
+_DEFAULT_MAX_INTERACTIONS = 512
+_DEFAULT_MAX_NEIGHBORS = 2048
+DEFAULT_PAIR_QUEUE_MULTIPLIER = 128
+_DEFAULT_PAIR_BATCH = 32
+_AUTO_INTERACTION_MIN = 2048
+_AUTO_INTERACTION_MAX = 16384
+_AUTO_INTERACTION_SCALE = 4
+_INT32_MAX = (1 << 31) - 1
+
+MACType = Literal["bh", "engblom", "dehnen"]
+_MAC_CODES = {"bh": 0, "dehnen": 1, "engblom": 2}
+
+
+@dataclass(frozen=True)
+class DualTreeTraversalConfig:
+    """Fixed traversal parameters for the dual-tree walk (:235-242)."""
+
+    max_pair_queue: int
+    process_block: int
+    max_interactions_per_node: int
+    max_neighbors_per_leaf: int = _DEFAULT_MAX_NEIGHBORS
+
+
+_GLOBAL_DUAL_TREE_CONFIG: Optional[DualTreeTraversalConfig] = None
+
+
+def set_default_dual_tree_config(config: Optional[DualTreeTraversalConfig]) -> None:
+    """Module-level fallback configuration (:250-266)."""
+    if config is not None:
+        if config.max_pair_queue < 1:
+            raise ValueError("max_pair_queue must be >= 1")
+        if config.process_block < 1:
+            raise ValueError("process_block must be >= 1")
+        if config.max_interactions_per_node < 1:
+            raise ValueError("max_interactions_per_node must be >= 1")
+        if config.max_neighbors_per_leaf < 1:
+            raise ValueError("max_neighbors_per_leaf must be >= 1")
+    global _GLOBAL_DUAL_TREE_CONFIG
+    _GLOBAL_DUAL_TREE_CONFIG = config
+
+
+class DualTreeRetryEvent(NamedTuple):
+    attempt: int
+    queue_capacity: int
+    interaction_capacity: int
+    status: str
+    far_pair_count: int
+    near_pair_count: int
+
+
+class NodeInteractionList(NamedTuple):
+    """Far-field interactions in level-major order (:566-592)."""
+
+    offsets: torch.Tensor
+    sources: torch.Tensor
+    targets: torch.Tensor
+    counts: torch.Tensor
+    level_offsets: torch.Tensor
+    target_levels: torch.Tensor
+
+
+class NodeNeighborList(NamedTuple):
+    """Near-field neighbour CSR over leaves in native order (:595-609)."""
+
+    offsets: torch.Tensor
+    neighbors: torch.Tensor
+    leaf_indices: torch.Tensor
+    counts: torch.Tensor
+    particle_order_leaf_indices: torch.Tensor
+    particle_order_to_native_leaf: torch.Tensor
+    neighbor_leaf_positions: torch.Tensor
+    target_block_leaf_ids: torch.Tensor
+    target_block_source_leaf_ids: torch.Tensor
+    target_block_valid_mask: torch.Tensor
+    target_block_offsets: torch.Tensor
+    target_block_size: int
+
+
+class DualTreeWalkResult(NamedTuple):
+    """Raw walk payload (:612-631) in the exact count-then-fill layout."""
+
+    interaction_offsets: torch.Tensor
+    interaction_sources: torch.Tensor
+    interaction_targets: torch.Tensor
+    interaction_tags: torch.Tensor
+    interaction_counts: torch.Tensor
+    neighbor_offsets: torch.Tensor
+    neighbor_indices: torch.Tensor
+    neighbor_counts: torch.Tensor
+    leaf_indices: torch.Tensor
+    far_pair_count: torch.Tensor
+    near_pair_count: torch.Tensor
+    queue_overflow: torch.Tensor
+    far_overflow: torch.Tensor
+    near_overflow: torch.Tensor
+    accept_decisions: torch.Tensor
+    near_decisions: torch.Tensor
+    refine_decisions: torch.Tensor
+
+
+class CompactTaggedFarPairs(NamedTuple):
+    sources: torch.Tensor
+    targets: torch.Tensor
+    tags: torch.Tensor
+    far_pair_count: torch.Tensor
+
+
+# ---------------------------------------------------------------------------
+# Capacity ladders of the reference (used only to reproduce its errors)
+
+
+def _next_power_of_two(value: int) -> int:
+    value = max(1, int(value))
+    return 1 << (value - 1).bit_length()
+
+
+def _queue_candidates_bounded(*, max_capacity: int, process_block: int) -> list:
+    """:296-316."""
+    qmax = max(4, int(max_capacity))
+    base = min(max(1024, int(process_block) * 16), qmax)
+    cands = [base]
+    while cands[-1] < qmax:
+        nxt = min(qmax, cands[-1] * 2)
+        if nxt == cands[-1]:
+            break
+        cands.append(nxt)
+    return cands
+
+
+def _auto_pair_queue_candidates(total_nodes: int, num_internal: int) -> list:
+    """:450-485."""
+    conservative = DEFAULT_PAIR_QUEUE_MULTIPLIER * max(4, total_nodes)
+    start = min(max(4096, num_internal * 2), conservative)
+    if start >= conservative:
+        return [int(conservative)]
+    cands = []
+    cap = start
+    while cap < conservative:
+        cands.append(int(cap))
+        cap = max(cap * 2, cap + 1024)
+    cands.append(int(conservative))
+    return list(dict.fromkeys(cands))
+
+
+def _auto_interaction_capacity(total_nodes: int) -> int:
+    """:516-537."""
+    scaled = max(total_nodes // _AUTO_INTERACTION_SCALE, _AUTO_INTERACTION_MIN)
+    scaled = min(scaled, _AUTO_INTERACTION_MAX)
+    return int(min(_AUTO_INTERACTION_MAX, max(_AUTO_INTERACTION_MIN, _next_power_of_two(scaled))))
+
+
+_FAR_MSG = "Interaction list capacity exceeded; increase max_interactions_per_node and rebuild."
+_NEAR_MSG = "Neighbor list capacity exceeded; increase max_neighbors_per_leaf and rebuild."
+
+
+# ---------------------------------------------------------------------------
+
+
+def _leaf_ordering(topology, total: int, ni: int, dev):
+    """_resolve_leaf_ordering (:1071-1103): native leaf order (stable order
+    of radix_leaf_to_oct for octrees), leaf positions, inverse map."""
+    nl = total - ni
+    po = torch.arange(ni, total, dtype=INDEX_DTYPE, device=dev)
+    if hasattr(topology, "radix_leaf_to_oct"):
+        lib = L.lib()
+        keys = topology.radix_leaf_to_oct.to(torch.int64).contiguous().view(torch.uint64)
+        kout = torch.empty_like(keys)
+        native = torch.empty(nl, dtype=torch.int32, device=dev)
+        ws = L.workspace(lib.ygx_sort_pairs_workspace_size(nl), dev)
+        L.check(lib.ygx_sort_pairs(L.ptr(keys), None, nl, 0, 32, L.ptr(kout), L.ptr(native),
+                                   L.ptr(ws), ws.numel(), L.stream_handle(dev)),
+                "ygx_sort_pairs")
+        native = native.to(torch.int64)
+    else:
+        native = torch.arange(nl, dtype=torch.int64, device=dev)
+    leaf_indices = po[native]
+    po_to_native = torch.empty(nl, dtype=INDEX_DTYPE, device=dev)
+    po_to_native[native] = torch.arange(nl, dtype=INDEX_DTYPE, device=dev)
+    leafpos32 = torch.full((total,), -1, dtype=torch.int32, device=dev)
+    leafpos32[leaf_indices.long()] = torch.arange(nl, dtype=torch.int32, device=dev)
+    return leaf_indices, leafpos32, po, po_to_native
+
+
+def _target_blocks(counts, offsets, nbr_leaf_pos, L_count, dev):
+    """_build_target_blocks (:3690-3769); active only with
+    YGGDRAX_NEARFIELD_TARGET_BLOCK_SIZE > 0."""
+    raw = os.environ.get("YGGDRAX_NEARFIELD_TARGET_BLOCK_SIZE", "0")
+    try:
+        k = max(0, int(raw))
+    except Exception:
+        k = 0
+    z = lambda *s, dt=INDEX_DTYPE: torch.zeros(s, dtype=dt, device=dev)  # noqa: E731
+    if k <= 0 or L_count == 0:
+        return z(0), z(0, 0), z(0, 0, dt=torch.bool), z(L_count + 1), 0
+    max_nbr = int(nbr_leaf_pos.shape[1])
+    if max_nbr == 0:
+        return z(0), z(0, k), z(0, k, dt=torch.bool), z(L_count + 1), k
+    blocks = (counts + (k - 1)) // k
+    boff = torch.cat([z(1), torch.cumsum(blocks, 0).to(INDEX_DTYPE)])
+    nb = int(boff[-1].item())
+    if nb == 0:
+        return z(0), z(0, k), z(0, k, dt=torch.bool), boff, k
+    bid = torch.arange(nb, dtype=INDEX_DTYPE, device=dev)
+    tl = torch.searchsorted(boff[1:], bid, right=True)
+    local = bid - boff[tl]
+    es = offsets[tl] + local * k
+    stop = offsets[tl + 1]
+    eo = torch.arange(k, dtype=INDEX_DTYPE, device=dev)
+    eidx = es[:, None] + eo[None, :]
+    ev = eidx < stop[:, None]
+    lidx = local[:, None] * k + eo[None, :]
+    lv = lidx < max_nbr
+    safe = torch.where(ev & lv, lidx, torch.zeros_like(lidx))
+    src = nbr_leaf_pos[tl[:, None], safe]
+    sv = src >= 0
+    valid = ev & lv & sv
+    src = torch.where(valid, src, torch.zeros_like(src))
+    return tl.to(INDEX_DTYPE), src.to(INDEX_DTYPE), valid, boff, k
+
+
+@dataclass
+class _WalkOut:
+    far_counts: torch.Tensor
+    node_offsets: torch.Tensor
+    level_offsets: torch.Tensor
+    sources: torch.Tensor
+    targets: torch.Tensor
+    target_levels: torch.Tensor
+    near_counts: torch.Tensor
+    near_offsets: torch.Tensor
+    neighbors: torch.Tensor
+    neighbor_leaf_positions: torch.Tensor
+    leaf_indices: torch.Tensor
+    particle_order_leaf_indices: torch.Tensor
+    particle_order_to_native_leaf: torch.Tensor
+    stats: dict
+    num_levels: int
+
+
+def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_scale: float,
+              wf_capacity: Optional[int] = None) -> _WalkOut:
+    """Count -> scan -> fill -> finalize on the GPU."""
+    lib = L.lib()
+    total = int(topology.parent.shape[0])
+    ni = int(topology.left_child.shape[0])
+    nl = total - ni
+    dev = topology.parent.device
+    st = L.stream_handle(dev)
+    ib, idt = INDEX_BITS, INDEX_DTYPE
+    leaf_indices, leafpos32, po, po_to_native = _leaf_ordering(topology, total, ni, dev)
+    num_levels = int(topology.num_levels)
+    z = lambda *s: torch.zeros(s, dtype=idt, device=dev)  # noqa: E731
+    if ni == 0:
+        return _WalkOut(
+            far_counts=z(total), node_offsets=z(total + 1), level_offsets=z(num_levels + 1),
+            sources=z(0), targets=z(0), target_levels=z(0), near_counts=z(nl),
+            near_offsets=z(nl + 1), neighbors=z(0), neighbor_leaf_positions=z(nl, 0),
+            leaf_indices=leaf_indices, particle_order_leaf_indices=po,
+            particle_order_to_native_leaf=po_to_native,
+            stats=dict(far_total=0, near_total=0, max_far=0, max_near=0, accept=0, near=0,
+                       refine=0, max_wf=1, gens=0), num_levels=num_levels)
+    d = _dev_of(topology)
+    center = geometry.center.contiguous().float()
+    radius = geometry.radius.contiguous().float()
+    max_extent = geometry.max_extent.contiguous().float()
+    cap = int(wf_capacity) if wf_capacity else 32 * total + 65536
+    mac = _MAC_CODES[mac_type]
+    root = int(torch.argmin(d.parent32).item()) if bool(
+        (d.tree_flags != 0).any().item()) else 0
+    while True:
+        ws = L.workspace(lib.ygx_traverse_workspace_size(total, nl, cap), dev)
+        stats = np.zeros(L.TSTAT_WORDS, np.uint64)
+        flags = np.zeros(1, np.uint32)
+        rc = lib.ygx_traverse_count(
+            L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32), L.ptr(d.right32),
+            L.ptr(leafpos32), total, ni, mac, float(theta), float(dehnen_radius_scale), root,
+            cap, stats.ctypes.data, flags.ctypes.data, L.ptr(ws), ws.numel(), st)
+        f = int(flags[0])
+        if f & L.FLAG_QUEUE_OVERFLOW and cap < (1 << 32) - 1:
+            cap = min((1 << 32) - 1, cap * 4)
+            del ws
+            continue
+        L.check(rc, "ygx_traverse_count")
+        if f & L.FLAG_BAD_INPUT:
+            raise ValueError("MAC extents must be positive (geometry has zero or NaN extents)")
+        if f:
+            raise L.YgxError(f"traversal count pass reported flags {f:#x}")
+        break
+    s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
+    P, Q = s["far_total"], s["near_total"]
+    node_offsets = torch.empty(total + 1, dtype=idt, device=dev)
+    far_counts = torch.empty(total, dtype=idt, device=dev)
+    level_offsets = torch.empty(num_levels + 1, dtype=idt, device=dev)
+    near_offsets = torch.empty(nl + 1, dtype=idt, device=dev)
+    near_counts = torch.empty(nl, dtype=idt, device=dev)
+    far_src32 = torch.empty(max(P, 1), dtype=torch.int32, device=dev)
+    near_nbr32 = torch.empty(max(Q, 1), dtype=torch.int32, device=dev)
+    L.check(lib.ygx_traverse_fill(
+        total, ni, mac, float(theta), root, cap, s["gens"], L.ptr(d.nbl32),
+        L.ptr(topology.level_offsets), num_levels, ib, L.ptr(node_offsets), L.ptr(far_counts),
+        L.ptr(level_offsets), L.ptr(near_offsets), L.ptr(near_counts), L.ptr(far_src32),
+        L.ptr(near_nbr32), L.ptr(ws), ws.numel(), st), "ygx_traverse_fill")
+    sources = torch.empty(P, dtype=idt, device=dev)
+    targets = torch.empty(P, dtype=idt, device=dev)
+    target_levels = torch.empty(P, dtype=idt, device=dev)
+    neighbors = torch.empty(Q, dtype=idt, device=dev)
+    max_nbr = s["max_near"]
+    nlp = torch.empty((nl, max_nbr), dtype=idt, device=dev)
+    L.check(lib.ygx_traverse_finalize(
+        total, ni, cap, L.ptr(d.level32), L.ptr(leafpos32), ib, L.ptr(far_src32),
+        L.ptr(near_nbr32), L.ptr(sources), L.ptr(targets), L.ptr(target_levels),
+        L.ptr(neighbors), L.ptr(nlp) if max_nbr > 0 else None, max_nbr, L.ptr(ws), ws.numel(),
+        st), "ygx_traverse_finalize")
+    f = L.read_status(ws)
+    if f & (L.FLAG_FAR_OVERFLOW | L.FLAG_NEAR_OVERFLOW | L.FLAG_QUEUE_OVERFLOW):
+        raise L.YgxError(f"traversal fill pass disagreed with the count pass (flags {f:#x})")
+    if P == 0:
+        node_offsets = z(total + 1)
+        level_offsets = z(num_levels + 1)
+    return _WalkOut(far_counts=far_counts, node_offsets=node_offsets,
+                    level_offsets=level_offsets, sources=sources, targets=targets,
+                    target_levels=target_levels, near_counts=near_counts,
+                    near_offsets=near_offsets, neighbors=neighbors,
+                    neighbor_leaf_positions=nlp, leaf_indices=leaf_indices,
+                    particle_order_leaf_indices=po, particle_order_to_native_leaf=po_to_native,
+                    stats=s, num_levels=num_levels)
+
+
+def _check_capacities(w: _WalkOut, total: int, ni: int, *, max_interactions_per_node,
+                      max_neighbors_per_leaf, max_pair_queue, process_block,
+                      traversal_config) -> None:
+    """Raise where the reference's runner (_run_dual_tree_walk_raw,
+    :3840-4440) would raise on the same pair sets."""
+    s = w.stats
+    nl = total - ni
+    use_count_pass = (max_interactions_per_node is None and max_pair_queue is None
+                      and traversal_config is None)
+    if use_count_pass:
+        conservative = max(total * DEFAULT_PAIR_QUEUE_MULTIPLIER,
+                           _auto_pair_queue_candidates(total, ni)[-1])
+        if s["max_wf"] > conservative:
+            raise RuntimeError(
+                "Count-pass traversal wavefront overflowed its conservative buffer.")
+        if max(1, s["max_near"]) > max(1, _INT32_MAX // max(1, nl)):
+            raise RuntimeError(
+                "Suggested per-leaf neighbor capacity is too large to safely allocate on the "
+                "host (would overflow int32). Enable local refinement or pass explicit "
+                "capacities (max_neighbors_per_leaf / max_interactions_per_node).")
+        if s["far_total"] > _INT32_MAX or s["near_total"] > _INT32_MAX:
+            raise RuntimeError(
+                "Dual-tree traversal pair totals exceed signed int32 capacity; refine the tree "
+                "or use a lower-memory traversal strategy.")
+        return
+    config = traversal_config if traversal_config is not None else _GLOBAL_DUAL_TREE_CONFIG
+    auto = _auto_pair_queue_candidates(total, ni)
+    if config is not None:
+        K = int(config.max_interactions_per_node)
+        nbr_limit = int(config.max_neighbors_per_leaf)
+        queue = _queue_candidates_bounded(max_capacity=max(4, int(config.max_pair_queue)),
+                                          process_block=int(config.process_block))
+        queue += [c for c in auto if c > queue[-1]]
+        qmsg = "Pair queue capacity exceeded; increase max_pair_queue and rebuild."
+    else:
+        K = (int(max_interactions_per_node) if max_interactions_per_node is not None
+             else _auto_interaction_capacity(total))
+        if max_interactions_per_node is not None and max_interactions_per_node < 1:
+            raise ValueError("max_interactions_per_node must be >= 1")
+        nbr_limit = int(max_neighbors_per_leaf)
+        if max_pair_queue is not None:
+            queue = [max(4, int(max_pair_queue))]
+            qmsg = "Pair queue capacity exceeded; increase max_pair_queue and rebuild."
+        else:
+            queue = auto
+            qmsg = ("Pair queue capacity exceeded; pass a larger max_pair_queue value to "
+                    "override auto-scaling.")
+    if s["max_wf"] > queue[-1]:
+        raise RuntimeError(qmsg)
+    if s["max_far"] > K:
+        raise RuntimeError(_FAR_MSG)
+    hard_cap = max(1, _INT32_MAX // max(1, nl))
+    if s["max_near"] > max(min(max(1, nbr_limit), hard_cap), hard_cap):
+        raise RuntimeError(_NEAR_MSG)
+
+
+def build_interactions_and_neighbors(
+    tree,
+    geometry,
+    theta: float = 0.5,
+    max_interactions_per_node: Optional[int] = None,
+    max_neighbors_per_leaf: int = _DEFAULT_MAX_NEIGHBORS,
+    max_pair_queue: Optional[int] = None,
+    process_block: Optional[int] = None,
+    traversal_config: Optional[DualTreeTraversalConfig] = None,
+    retry_logger: Optional[Callable[[DualTreeRetryEvent], object]] = None,
+    mac_type: MACType = "bh",
+    dehnen_radius_scale: float = 1.0,
+    pair_policy=None,
+    policy_state: object = None,
+    *,
+    return_result: bool = False,
+    return_compact_far_pairs: bool = False,
+    return_interactions: bool = True,
+    return_grouped: bool = False,
+):
+    """Far-field interactions and near-field neighbour lists in one walk.
+
+    Same arguments, defaults and return conventions as the reference
+    (``(interactions, neighbors)`` plus, in this order, the raw result, the
+    compact far pairs and the grouped buffers when requested).  ``pair_policy``
+    and ``return_grouped`` are outside the GPU pipeline and raise."""
+    topology = resolve_tree_topology(tree)
+    if mac_type not in _MAC_CODES:
+        raise ValueError(f"Unknown mac_type: {mac_type}")
+    if float(dehnen_radius_scale) <= 0.0:
+        raise ValueError("dehnen_radius_scale must be > 0")
+    if pair_policy is not None:
+        raise NotImplementedError("pair_policy is outside the GPU traversal (default MAC only)")
+    if return_grouped and not return_interactions:
+        raise ValueError("grouped interaction return requires return_interactions=True")
+    if return_grouped:
+        raise NotImplementedError("grouped interaction buffers are outside the GPU pipeline")
+    if process_block is not None and process_block < 1:
+        raise ValueError("process_block must be >= 1")
+    del retry_logger, policy_state  # no retries happen on this path
+    total = int(topology.parent.shape[0])
+    ni = int(topology.left_child.shape[0])
+    w = _run_walk(topology, geometry, theta, mac_type, dehnen_radius_scale)
+    _check_capacities(w, total, ni, max_interactions_per_node=max_interactions_per_node,
+                      max_neighbors_per_leaf=max_neighbors_per_leaf,
+                      max_pair_queue=max_pair_queue, process_block=process_block,
+                      traversal_config=traversal_config)
+    dev = topology.parent.device
+    interactions = None
+    if return_interactions:
+        interactions = NodeInteractionList(
+            offsets=w.node_offsets, sources=w.sources, targets=w.targets, counts=w.far_counts,
+            level_offsets=w.level_offsets, target_levels=w.target_levels)
+    nl = total - ni
+    tb = _target_blocks(w.near_counts, w.near_offsets, w.neighbor_leaf_positions, nl, dev)
+    neighbors = NodeNeighborList(
+        offsets=w.near_offsets, neighbors=w.neighbors, leaf_indices=w.leaf_indices,
+        counts=w.near_counts, particle_order_leaf_indices=w.particle_order_leaf_indices,
+        particle_order_to_native_leaf=w.particle_order_to_native_leaf,
+        neighbor_leaf_positions=w.neighbor_leaf_positions, target_block_leaf_ids=tb[0],
+        target_block_source_leaf_ids=tb[1], target_block_valid_mask=tb[2],
+        target_block_offsets=tb[3], target_block_size=int(tb[4]))
+    out = [interactions, neighbors]
+    if return_result or return_compact_far_pairs:
+        # Exact count-then-fill layout: rows in node order.
+        idt = INDEX_DTYPE
+        counts = w.far_counts.to(torch.int64)
+        no = torch.zeros(total + 1, dtype=torch.int64, device=dev)
+        no[1:] = torch.cumsum(counts, 0)
+        P = int(w.sources.shape[0])
+        node = torch.repeat_interleave(torch.arange(total, device=dev), counts)
+        within = torch.arange(P, device=dev) - no[node]
+        src_pos = w.node_offsets.to(torch.int64)[node] + within
+        raw_src = w.sources[src_pos] if P else w.sources
+        raw_tgt = node.to(idt)
+        tags = torch.full((P,), -1, dtype=idt, device=dev)
+        fpc = torch.tensor(P, dtype=idt, device=dev)
+        if return_result:
+            s = w.stats
+            out.append(DualTreeWalkResult(
+                interaction_offsets=no.to(idt), interaction_sources=raw_src,
+                interaction_targets=raw_tgt, interaction_tags=tags,
+                interaction_counts=w.far_counts, neighbor_offsets=w.near_offsets,
+                neighbor_indices=w.neighbors, neighbor_counts=w.near_counts,
+                leaf_indices=w.leaf_indices, far_pair_count=fpc,
+                near_pair_count=torch.tensor(int(w.neighbors.shape[0]), dtype=idt, device=dev),
+                queue_overflow=torch.tensor(False, device=dev),
+                far_overflow=torch.tensor(False, device=dev),
+                near_overflow=torch.tensor(False, device=dev),
+                accept_decisions=torch.tensor(s["accept"], dtype=idt, device=dev),
+                near_decisions=torch.tensor(s["near"], dtype=idt, device=dev),
+                refine_decisions=torch.tensor(s["refine"], dtype=idt, device=dev)))
+        if return_compact_far_pairs:
+            out.append(CompactTaggedFarPairs(sources=raw_src, targets=raw_tgt, tags=tags,
+                                             far_pair_count=fpc))
+    return tuple(out)
+
+
+__all__ = [
+    "MACType", "DualTreeTraversalConfig", "DualTreeRetryEvent", "DualTreeWalkResult",
+    "NodeInteractionList", "NodeNeighborList", "CompactTaggedFarPairs",
+    "build_interactions_and_neighbors", "set_default_dual_tree_config",
+]
