@@ -1,0 +1,395 @@
+"""Benchmark: full tree pipeline (Morton -> sort -> build -> geometry -> lists).
+
+One step = ``build_tree`` (radix/LBVH, leaf 32) + ``compute_tree_geometry`` +
+``build_interactions_and_neighbors`` (dehnen, theta 0.6, exact count-then-
+fill lists) over N = 16,777,216 float32 Plummer particles (seed 4, scale
+radius 1, truncated at r = 20, equal masses).  The metric is particles/s of
+the whole step.
+
+* ``value``: inputs already resident in HBM, CUDA-event timed over K steps.
+* ``e2e``: the same step through the public API from pinned host buffers:
+  host->device copy of positions and masses and device->host copy of the
+  per-node far/near counts inside the timed region.
+* ``roofline``: the dominant kernel family (see ``--breakdown``) timed with
+  CUDA events inside this run, against the measured HBM copy bandwidth.
+* ``cpu_baseline``: the CPU restatement of the pipeline (OpenMP, all host
+  cores) on a bounded sample.
+* ``--impl reference``: that CPU implementation on the host cores as the
+  reference arm (the reference itself is JAX, which this image lacks).
+
+With ``--gpus N`` (torchrun, one rank per GPU) every rank runs its own
+replica: the path does not shard, so there is no collective; the value is
+the particles of all ranks over the slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+N_DEFAULT = 16_777_216
+LEAF = 32
+THETA = 0.6
+MAC = "dehnen"
+WORKLOAD = "plummer_16M_radix_leaf32_dehnen_theta0.6_two_pass"
+METRIC = "particles/s full build+traversal (Morton, sort, radix build, geometry, exact lists)"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx.append(float(f[2]))
+                except ValueError:
+                    continue
+                for name, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(name)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_pipeline(pos, mass):
+    """CPU restatement of one step (used for the CPU baseline only)."""
+    from oracle import oracle as O
+
+    t = O.build_tree(pos, mass, leaf_size=LEAF)
+    g = O.compute_tree_geometry(t, t.positions_sorted)
+    r = O.build_interactions_and_neighbors(t, g, theta=THETA, mac_type=MAC)
+    return t, r
+
+
+def cpu_baseline(sample_n: int, reps: int = 1):
+    from oracle import oracle as O
+    from yggdrax_b200 import inputs
+
+    O.build()
+    pos, mass = inputs.plummer(sample_n, 4)
+    cpu_pipeline(pos[:4096], mass[:4096])  # load + warm
+    best = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        cpu_pipeline(pos, mass)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return {"value": sample_n / best, "unit": "particles/s", "cores": O.num_threads(),
+            "kind": "port",
+            "sample": f"{sample_n} Plummer particles (seed 4), same step, wall clock, "
+                      f"best of {reps}"}
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    sample_n = args.cpu_sample
+    from oracle import oracle as O
+    from yggdrax_b200 import inputs
+
+    O.build()
+    pos, mass = inputs.plummer(sample_n, 4)
+    for _ in range(args.warmup):
+        cpu_pipeline(pos, mass)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cpu_pipeline(pos, mass)
+    dt = (time.perf_counter() - t0) / max(1, args.steps)
+    v = sample_n / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "particles/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+int64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_particles": sample_n, "parallelism": "cpu"},
+        "cpu_baseline": {"value": v, "unit": "particles/s", "cores": O.num_threads(),
+                         "kind": "port",
+                         "sample": f"{sample_n} Plummer particles (seed 4) per step; the "
+                                   "reference is JAX-only and JAX is not installed"},
+        "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--cpu-sample", type=int, default=1 << 20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--breakdown", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    import yggdrax_b200 as yb
+    from yggdrax_b200 import _lib as L
+    from yggdrax_b200 import build_ext, inputs
+
+    world, rank, local = _dist()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    build_ext.build()
+    lib = L.lib()
+
+    n = args.n
+    pos_np, mass_np = inputs.plummer(n, 4)
+    pos_h = torch.from_numpy(pos_np).pin_memory()
+    mass_h = torch.from_numpy(mass_np).pin_memory()
+    pos_d = pos_h.to(dev)
+    mass_d = mass_h.to(dev)
+
+    def step(P, M):
+        tree, ps = yb.build_tree(P, M, leaf_size=LEAF, return_reordered=True)[:2]
+        geom = yb.compute_tree_geometry(tree, ps)
+        inter, nbrs = yb.build_interactions_and_neighbors(tree, geom, theta=THETA, mac_type=MAC)
+        return tree, geom, inter, nbrs
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        out = step(pos_d, mass_d)
+    del out
+    barrier()
+
+    # -- device-resident timing ------------------------------------------------
+    launches0 = lib.ygx_launch_counter()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        barrier()
+        ev[0].record()
+        for _ in range(args.steps):
+            tree, geom, inter, nbrs = step(pos_d, mass_d)
+        ev[1].record()
+        barrier()
+    launches = lib.ygx_launch_counter() - launches0
+    t_dev = ev[0].elapsed_time(ev[1]) / 1e3 / args.steps
+    far_entries = int(inter.sources.numel())
+    near_entries = int(nbrs.neighbors.numel())
+    total_nodes = int(tree.parent.shape[0])
+    del tree, geom, inter, nbrs
+
+    # -- end to end through the public API from host buffers --------------------
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    d2h = 0
+    e0.record()
+    for _ in range(args.steps):
+        P = pos_h.to(dev, non_blocking=True)
+        M = mass_h.to(dev, non_blocking=True)
+        _, _, inter, nbrs = step(P, M)
+        fc = inter.counts.cpu()
+        nc = nbrs.counts.cpu()
+        d2h = fc.numel() * fc.element_size() + nc.numel() * nc.element_size()
+    e1.record()
+    barrier()
+    t_e2e = e0.elapsed_time(e1) / 1e3 / args.steps
+    h2d = pos_h.numel() * 4 + mass_h.numel() * 4
+    del inter, nbrs
+
+    # -- roofline of the dominant kernel family: the onesweep sort passes -------
+    codes = yb.morton_encode(pos_d, yb.infer_bounds(pos_d))
+    kout = torch.empty_like(codes)
+    vout = torch.empty(n, dtype=torch.int32, device=dev)
+    wsb = L.workspace(lib.ygx_sort_pairs_workspace_size(n), dev)
+    st = L.stream_handle(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def sort_once():
+        L.check(lib.ygx_sort_pairs(L.ptr(codes), None, n, 0, 63, L.ptr(kout), L.ptr(vout),
+                                   L.ptr(wsb), wsb.numel(), st), "ygx_sort_pairs")
+
+    for _ in range(3):
+        sort_once()
+    sort_ms = []
+    for _ in range(max(3, args.steps)):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        sort_once()
+        b.record()
+        torch.cuda.synchronize(dev)
+        sort_ms.append(a.elapsed_time(b))
+    passes = 8
+    sort_s = float(np.median(sort_ms)) / 1e3
+    # algorithmic bytes per onesweep pass: read key+value, write key+value
+    bytes_per_pass = 24.0 * n
+    achieved = bytes_per_pass / (sort_s / passes) / 1e9
+    peak, peak_kind = _peaks()
+    roofline = {"kernel": "k_onesweep (8 passes, 8-bit digits, key u64 + value u32)",
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": bytes_per_pass,
+                "launch_ms_avg": sort_s / passes * 1e3}
+
+    breakdown = None
+    if args.breakdown:
+        breakdown = stage_breakdown(pos_d, mass_d, dev)
+
+    # -- aggregate over ranks ---------------------------------------------------
+    t_max, te_max = t_dev, t_e2e
+    if world > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([t_dev, t_e2e], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max, te_max = float(tt[0]), float(tt[1])
+    if rank == 0:
+        cpu = None if args.no_cpu_baseline else cpu_baseline(args.cpu_sample)
+        line = {
+            "metric": METRIC, "value": world * n / t_max, "unit": "particles/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+int64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_particles": n, "leaf_size": LEAF,
+                       "mac": MAC, "theta": THETA, "total_nodes": total_nodes,
+                       "far_entries": far_entries, "near_entries": near_entries,
+                       "pairs_per_s": world * (far_entries + near_entries) / t_max,
+                       "l2": "inputs (268 MB) larger than L2; no flush between steps",
+                       "parallelism": f"replicas{world}"},
+            "e2e": {"value": world * n / te_max, "unit": "particles/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+        }
+        if breakdown is not None:
+            line["breakdown_ms"] = breakdown
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def stage_breakdown(pos_d, mass_d, dev):
+    """Per-stage CUDA-event times of one step (diagnostics)."""
+    import torch
+
+    import yggdrax_b200 as yb
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    marks = {}
+    torch.cuda.synchronize(dev)
+    a, b, c, d = ev(), ev(), ev(), ev()
+    a.record()
+    tree, ps = yb.build_tree(pos_d, mass_d, leaf_size=LEAF, return_reordered=True)[:2]
+    b.record()
+    geom = yb.compute_tree_geometry(tree, ps)
+    c.record()
+    yb.build_interactions_and_neighbors(tree, geom, theta=THETA, mac_type=MAC)
+    d.record()
+    torch.cuda.synchronize(dev)
+    marks["build"] = a.elapsed_time(b)
+    marks["geometry"] = b.elapsed_time(c)
+    marks["traversal"] = c.elapsed_time(d)
+    a, b = ev(), ev()
+    a.record()
+    yb.encode_and_sort(pos_d)
+    b.record()
+    torch.cuda.synchronize(dev)
+    marks["encode_sort"] = a.elapsed_time(b)
+    from yggdrax_b200 import interactions as I
+
+    marks["walk_stats"] = dict(I.LAST_WALK_STATS)
+    return marks
+
+
+if __name__ == "__main__":
+    sys.exit(main())

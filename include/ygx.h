@@ -69,6 +69,8 @@ extern "C" {
 int ygx_workspace_init(void* ws, size_t ws_bytes, cudaStream_t stream);
 /* Copies the status word to host *host_flags; synchronizes the stream. */
 int ygx_status_read(const void* ws, uint32_t* host_flags, cudaStream_t stream);
+/* Number of kernel launches this library has issued in this process. */
+uint64_t ygx_launch_counter(void);
 
 /* ---- L0: bounds, Morton codes, stable sort ------------------------------- */
 

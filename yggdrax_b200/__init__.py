@@ -19,6 +19,7 @@ from .interactions import (
     NodeNeighborList,
     build_interactions_and_neighbors,
     set_default_dual_tree_config,
+    set_dense_neighbor_budget,
 )
 from .morton import (
     encode_and_sort,

@@ -49,6 +49,7 @@ F64 = ctypes.c_double
 _SIGS = {
     "ygx_workspace_init": (I32, [P, SZ, P]),
     "ygx_status_read": (I32, [P, P, P]),
+    "ygx_launch_counter": (ctypes.c_uint64, []),
     "ygx_bounds": (I32, [P, I64, P, P, SZ, P]),
     "ygx_morton_encode": (I32, [P, I64, P, P, P]),
     "ygx_encode_sort_workspace_size": (SZ, [I64]),

@@ -106,8 +106,15 @@ struct Arena {
 
 }  // namespace ygx
 
+namespace ygx {
+// Host-side count of kernel launches issued by this library (all threads).
+void note_launch();
+}  // namespace ygx
+
+// Called right after every kernel launch: counts it and reports launch errors.
 #define YGX_CHECK_LAUNCH()                           \
   do {                                               \
+    ygx::note_launch();                              \
     cudaError_t _e = cudaGetLastError();             \
     if (_e != cudaSuccess) return YGX_ERR_CUDA;      \
   } while (0)

@@ -1,5 +1,14 @@
 #include "scan.cuh"
 
+#include <atomic>
+
+namespace ygx {
+static std::atomic<unsigned long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace ygx
+
+extern "C" uint64_t ygx_launch_counter(void) { return ygx::g_launches.load(); }
+
 namespace ygx {
 namespace {
 

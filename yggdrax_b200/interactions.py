@@ -182,6 +182,28 @@ def _auto_interaction_capacity(total_nodes: int) -> int:
     return int(min(_AUTO_INTERACTION_MAX, max(_AUTO_INTERACTION_MIN, _next_power_of_two(scaled))))
 
 
+_DENSE_BUDGET: Optional[int] = None
+LAST_WALK_STATS: dict = {}  # diagnostics of the most recent walk
+
+
+def set_dense_neighbor_budget(nbytes: Optional[int]) -> None:
+    """Byte budget of the dense ``neighbor_leaf_positions`` helper table
+    (``None``: a quarter of the device memory that is free at call time).
+    The table is ``(num_leaves, max_neighbours)``; when one sparse leaf is
+    near to nearly every other leaf it grows quadratically (terabytes for
+    16M-particle Plummer spheres), so above the budget an empty ``(L, 0)``
+    table is returned and the CSR ``offsets`` / ``neighbors`` stay exact."""
+    global _DENSE_BUDGET
+    _DENSE_BUDGET = None if nbytes is None else int(nbytes)
+
+
+def _dense_neighbor_budget(dev) -> int:
+    if _DENSE_BUDGET is not None:
+        return _DENSE_BUDGET
+    free, _ = torch.cuda.mem_get_info(dev)
+    return int(free // 4)
+
+
 _FAR_MSG = "Interaction list capacity exceeded; increase max_interactions_per_node and rebuild."
 _NEAR_MSG = "Neighbor list capacity exceeded; increase max_neighbors_per_leaf and rebuild."
 
@@ -320,6 +342,8 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
             raise L.YgxError(f"traversal count pass reported flags {f:#x}")
         break
     s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
+    LAST_WALK_STATS.clear()
+    LAST_WALK_STATS.update(s, wf_capacity=cap)
     P, Q = s["far_total"], s["near_total"]
     node_offsets = torch.empty(total + 1, dtype=idt, device=dev)
     far_counts = torch.empty(total, dtype=idt, device=dev)
@@ -338,6 +362,13 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     target_levels = torch.empty(P, dtype=idt, device=dev)
     neighbors = torch.empty(Q, dtype=idt, device=dev)
     max_nbr = s["max_near"]
+    dense_bytes = nl * max_nbr * (4 if ib == 32 else 8)
+    if dense_bytes > _dense_neighbor_budget(dev):
+        logger.warning(
+            "neighbor_leaf_positions would need %.1f GiB (%d leaves x %d neighbours); "
+            "returning an empty (L, 0) table -- raise the budget with "
+            "set_dense_neighbor_budget() to build it", dense_bytes / 2**30, nl, max_nbr)
+        max_nbr = 0
     nlp = torch.empty((nl, max_nbr), dtype=idt, device=dev)
     L.check(lib.ygx_traverse_finalize(
         total, ni, cap, L.ptr(d.level32), L.ptr(leafpos32), ib, L.ptr(far_src32),
@@ -517,4 +548,5 @@ __all__ = [
     "MACType", "DualTreeTraversalConfig", "DualTreeRetryEvent", "DualTreeWalkResult",
     "NodeInteractionList", "NodeNeighborList", "CompactTaggedFarPairs",
     "build_interactions_and_neighbors", "set_default_dual_tree_config",
+    "set_dense_neighbor_budget",
 ]
