@@ -258,3 +258,52 @@ def test_sort_pairs_is_stable(cuda_device):
         np.testing.assert_array_equal(vo.cpu().numpy(), want)
         np.testing.assert_array_equal(ko.cpu().numpy(), keys[want])
         assert L.read_status(ws) == 0
+
+
+def test_long_rows_match_oracle(cuda_device, oracle):
+    """Plummer halo leaves are near to every other leaf: rows of > 8192
+    entries take the bitmap ordering path."""
+    import yggdrax_b200 as yb
+    from yggdrax_b200 import inputs
+
+    pos, mass = inputs.plummer(300_000, 5)
+    P, M = _to_dev(pos, cuda_device), _to_dev(mass, cuda_device)
+    gt, ps = yb.build_tree(P, M, leaf_size=32, return_reordered=True)[:2]
+    gg = yb.compute_tree_geometry(gt, ps)
+    gi, gn = yb.build_interactions_and_neighbors(gt, gg, theta=0.6, mac_type="dehnen")
+    ot = oracle.build_tree(pos, mass, leaf_size=32)
+    og = oracle.compute_tree_geometry(ot, ot.positions_sorted)
+    r = oracle.build_interactions_and_neighbors(ot, og, theta=0.6, mac_type="dehnen")
+    assert r["near_counts"].max() > 8192
+    _compare_lists(gi, gn, r)
+
+
+def test_reference_count_pass_limit(cuda_device):
+    """The reference's count-pass sizing check (max near row vs
+    int32_max // L) raises on a 2M Plummer sphere; with the limits off the
+    exact lists are returned."""
+    import yggdrax_b200 as yb
+    from yggdrax_b200 import inputs
+
+    pos, mass = inputs.plummer(1 << 21, 6)
+    P, M = _to_dev(pos, cuda_device), _to_dev(mass, cuda_device)
+    gt, ps = yb.build_tree(P, M, leaf_size=32, return_reordered=True)[:2]
+    gg = yb.compute_tree_geometry(gt, ps)
+    with pytest.raises(RuntimeError, match="Suggested per-leaf neighbor capacity"):
+        yb.build_interactions_and_neighbors(gt, gg, theta=0.6, mac_type="dehnen")
+    yb.set_reference_limits(False)
+    try:
+        gi, gn = yb.build_interactions_and_neighbors(gt, gg, theta=0.6, mac_type="dehnen")
+    finally:
+        yb.set_reference_limits(True)
+    nl = gt.num_leaves
+    assert int(gn.counts.max()) > (2**31 - 1) // nl
+    assert int(gn.offsets[-1]) == int(gn.neighbors.numel())
+    # every row strictly ascending
+    nb = gn.neighbors.cpu().numpy()
+    off = gn.offsets.cpu().numpy()
+    d = np.diff(nb)
+    starts = off[1:-1]
+    mask = np.ones(d.shape[0], bool)
+    mask[starts[(starts > 0) & (starts <= d.shape[0])] - 1] = False
+    assert (d[mask] > 0).all()

@@ -20,6 +20,7 @@ from .interactions import (
     build_interactions_and_neighbors,
     set_default_dual_tree_config,
     set_dense_neighbor_budget,
+    set_reference_limits,
 )
 from .morton import (
     encode_and_sort,

@@ -404,28 +404,92 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Long rows: one CTA per row.  Up to kBlockRowCap entries sort in shared
+// memory.  Longer rows hold distinct node ids (a canonical pair is visited
+// once), so they are ordered by setting one bit per entry in a bitmap over
+// all node ids and reading the bitmap back in order; if the bit count shows
+// duplicates the row is sorted in place in global memory instead.
 __global__ void __launch_bounds__(1024)
     k_rows_big(const int32_t* __restrict__ big_rows, const uint32_t* __restrict__ n_big,
                const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
                const int32_t* __restrict__ row_level, int32_t* __restrict__ raw, int index_bits,
-               void* vals_out, void* tgt_out, void* lvl_out) {
+               void* vals_out, void* tgt_out, void* lvl_out, uint32_t* __restrict__ bitmaps,
+               int64_t universe) {
   __shared__ int32_t s_a[kBlockRowCap];
+  __shared__ int64_t s_warp[32];
+  __shared__ int64_t s_total;
   const uint32_t nb = *n_big;
+  const int64_t words = (universe + 31) / 32;
+  uint32_t* bm = bitmaps + (int64_t)blockIdx.x * words;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
   for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
     const int32_t r = big_rows[b];
     const int64_t off = row_off[r];
     const int64_t n = row_cnt[r];
-    int32_t* a;
+    const int32_t lvl = row_level ? row_level[r] : 0;
     if (n <= kBlockRowCap) {
-      a = s_a;
-      for (int64_t k = threadIdx.x; k < n; k += blockDim.x) a[k] = raw[off + k];
+      for (int64_t k = tid; k < n; k += nt) s_a[k] = raw[off + k];
       __syncthreads();
-    } else {
-      a = raw + off;  // in place, global memory
+      mirrored_bitonic<true>(s_a, n, tid, nt);
+      emit_row(s_a, n, off, index_bits, vals_out, tgt_out, lvl_out, r, lvl, tid, nt);
+      __syncthreads();
+      continue;
     }
-    mirrored_bitonic<true>(a, n, threadIdx.x, blockDim.x);
-    emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, r, row_level ? row_level[r] : 0,
-             threadIdx.x, blockDim.x);
+    for (int64_t w = tid; w < words; w += nt) bm[w] = 0u;
+    __syncthreads();
+    for (int64_t k = tid; k < n; k += nt) {
+      const int32_t v = raw[off + k];
+      atomicOr(&bm[v >> 5], 1u << (v & 31));
+    }
+    __syncthreads();
+    // Thread t owns words [t*chunk, (t+1)*chunk): count, scan, emit.
+    const int64_t chunk = (words + nt - 1) / nt;
+    const int64_t w0 = (int64_t)tid * chunk;
+    const int64_t w1 = w0 + chunk < words ? w0 + chunk : words;
+    int64_t mine = 0;
+    for (int64_t w = w0; w < w1; ++w) mine += __popc(__ldcg(bm + w));
+    int64_t incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+      int64_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      int64_t wv = lane < (nt >> 5) ? s_warp[lane] : 0;
+      int64_t wi = wv;
+      for (int o = 1; o < 32; o <<= 1) {
+        int64_t v = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += v;
+      }
+      if (lane < (nt >> 5)) s_warp[lane] = wi - wv;
+      if (lane == 31) s_total = wi;
+    }
+    __syncthreads();
+    const bool distinct = s_total == n;
+    if (distinct) {
+      int64_t pos = off + s_warp[warp] + incl - mine;
+      for (int64_t w = w0; w < w1; ++w) {
+        uint32_t bits = __ldcg(bm + w);
+        while (bits) {
+          const int bit = __ffs(bits) - 1;
+          bits &= bits - 1;
+          const int64_t v = w * 32 + bit;
+          store_idx(vals_out, index_bits, pos, v);
+          if (tgt_out) {
+            store_idx(tgt_out, index_bits, pos, r);
+            store_idx(lvl_out, index_bits, pos, lvl);
+          }
+          ++pos;
+        }
+      }
+    }
+    __syncthreads();
+    if (!distinct) {
+      int32_t* a = raw + off;  // repeated entries: sort in place in global memory
+      mirrored_bitonic<true>(a, n, tid, nt);
+      emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, r, lvl, tid, nt);
+    }
     __syncthreads();
   }
 }
@@ -464,6 +528,7 @@ struct TravScratch {
   int64_t* near_off;
   int64_t* scan_tmp;
   int32_t* big_rows;
+  uint32_t* bitmaps;
   int2* wf[2];
 };
 
@@ -486,6 +551,7 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap) {
   s.near_off = a.take<int64_t>(L + 1);
   s.scan_tmp = a.take<int64_t>(scan_scratch_elems(total > L ? total : L));
   s.big_rows = a.take<int32_t>(total > L ? total : L);
+  s.bitmaps = a.take<uint32_t>((size_t)kNumSMs * ((total + 31) / 32));
   s.wf[0] = a.take<int2>(cap);
   s.wf[1] = a.take<int2>(cap);
   return s;
@@ -677,7 +743,7 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
   YGX_CHECK_LAUNCH();
   ygx::k_rows_big<<<ygx::kNumSMs, 1024, 0, stream>>>(s.big_rows, s.n_big, s.far_off, s.far_cnt,
                                                      level32, far_src32, index_bits, far_sources,
-                                                     far_targets, target_levels);
+                                                     far_targets, target_levels, s.bitmaps, total);
   YGX_CHECK_LAUNCH();
   // near rows
   if (cudaMemsetAsync(s.n_big, 0, sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
@@ -687,7 +753,7 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
   YGX_CHECK_LAUNCH();
   ygx::k_rows_big<<<ygx::kNumSMs, 1024, 0, stream>>>(s.big_rows, s.n_big, s.near_off, s.near_cnt,
                                                      nullptr, near_nbr32, index_bits, neighbors,
-                                                     nullptr, nullptr);
+                                                     nullptr, nullptr, s.bitmaps, total);
   YGX_CHECK_LAUNCH();
   if (neighbor_leaf_positions && max_nbr > 0) {
     ygx::k_neighbor_leaf_positions<<<ygx::grid_for(L * max_nbr, 256), 256, 0, stream>>>(

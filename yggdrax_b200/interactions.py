@@ -182,6 +182,26 @@ def _auto_interaction_capacity(total_nodes: int) -> int:
     return int(min(_AUTO_INTERACTION_MAX, max(_AUTO_INTERACTION_MIN, _next_power_of_two(scaled))))
 
 
+_REFERENCE_LIMITS = os.environ.get("YGGDRAX_B200_REFERENCE_LIMITS", "1").strip().lower() not in (
+    "0", "false", "no", "off")
+
+
+def set_reference_limits(enabled: bool) -> None:
+    """Raise where the reference raises (default) or not.
+
+    The reference sizes dense host/device buffers from the walk's counts and
+    refuses to run when they would not fit: in count-then-fill mode it raises
+    when the longest near row exceeds ``int32_max // num_leaves``
+    (``_interactions_impl.py:4170-4187``), which every Plummer sphere above
+    ~1.5M particles at leaf 32 triggers because its outermost halo leaf is near
+    to every other leaf.  This implementation needs no dense buffers to
+    produce the exact lists, so with ``enabled=False`` those checks are
+    skipped and the lists are returned.  Environment:
+    ``YGGDRAX_B200_REFERENCE_LIMITS=0``."""
+    global _REFERENCE_LIMITS
+    _REFERENCE_LIMITS = bool(enabled)
+
+
 _DENSE_BUDGET: Optional[int] = None
 LAST_WALK_STATS: dict = {}  # diagnostics of the most recent walk
 
@@ -489,10 +509,11 @@ def build_interactions_and_neighbors(
     total = int(topology.parent.shape[0])
     ni = int(topology.left_child.shape[0])
     w = _run_walk(topology, geometry, theta, mac_type, dehnen_radius_scale)
-    _check_capacities(w, total, ni, max_interactions_per_node=max_interactions_per_node,
-                      max_neighbors_per_leaf=max_neighbors_per_leaf,
-                      max_pair_queue=max_pair_queue, process_block=process_block,
-                      traversal_config=traversal_config)
+    if _REFERENCE_LIMITS:
+        _check_capacities(w, total, ni, max_interactions_per_node=max_interactions_per_node,
+                          max_neighbors_per_leaf=max_neighbors_per_leaf,
+                          max_pair_queue=max_pair_queue, process_block=process_block,
+                          traversal_config=traversal_config)
     dev = topology.parent.device
     interactions = None
     if return_interactions:
@@ -548,5 +569,5 @@ __all__ = [
     "MACType", "DualTreeTraversalConfig", "DualTreeRetryEvent", "DualTreeWalkResult",
     "NodeInteractionList", "NodeNeighborList", "CompactTaggedFarPairs",
     "build_interactions_and_neighbors", "set_default_dual_tree_config",
-    "set_dense_neighbor_budget",
+    "set_dense_neighbor_budget", "set_reference_limits",
 ]
