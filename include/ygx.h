@@ -36,7 +36,8 @@ enum {
   YGX_ERR_FAR_OVERFLOW = 5,    /* far-list capacity exceeded                  */
   YGX_ERR_NEAR_OVERFLOW = 6,   /* near-list capacity exceeded                 */
   YGX_ERR_INT32_TOTAL = 7,     /* pair totals exceed the int32 range          */
-  YGX_ERR_MALFORMED = 8        /* topology inconsistent (tied Morton codes)   */
+  YGX_ERR_MALFORMED = 8,       /* topology inconsistent (tied Morton codes)   */
+  YGX_ERR_TOO_LARGE = 9        /* size above a fixed maximum                  */
 };
 
 /* status-word bits (device side) */
@@ -99,6 +100,20 @@ size_t ygx_sort_pairs_workspace_size(int64_t n);
 int ygx_sort_pairs(const uint64_t* keys_in, const uint32_t* values_in, int64_t n, int begin_bit,
                    int end_bit, uint64_t* keys_out, uint32_t* values_out, void* ws,
                    size_t ws_bytes, cudaStream_t stream);
+
+/* Same sort as ygx_sort_pairs, for callers that cannot allocate device
+ * memory where they sort (e.g. an XLA custom-call handler without a scratch
+ * request, whose framework has preallocated the GPU's memory pool): the
+ * scratch lives in a 4 MiB array inside libygx.so that every GPU using the
+ * library keeps until the process exits.  At most 262,144 keys per call;
+ * larger n returns YGX_ERR_TOO_LARGE.  Nothing is allocated.  The first call
+ * on a device looks up the array's device address (make it before any
+ * stream capture, with the stream's device current).  All calls share the
+ * array: calls that overlap on the GPU race, so order them on one stream.
+ * No counterpart in the reference (it has no allocation-free sort entry). */
+int ygx_sort_pairs_noalloc(const uint64_t* keys_in, const uint32_t* values_in, int64_t n,
+                           int begin_bit, int end_bit, uint64_t* keys_out, uint32_t* values_out,
+                           cudaStream_t stream);
 
 /* reorder_particles_by_indices / inverse_permutation
  * (yggdrax/_tree_impl.py:900-926): any output may be NULL. */

@@ -26,6 +26,7 @@ ERROR_NAMES = {
     6: "YGX_ERR_NEAR_OVERFLOW",
     7: "YGX_ERR_INT32_TOTAL",
     8: "YGX_ERR_MALFORMED",
+    9: "YGX_ERR_TOO_LARGE",
 }
 FLAG_TIMEOUT = 1 << 0
 FLAG_QUEUE_OVERFLOW = 1 << 1
@@ -56,6 +57,7 @@ _SIGS = {
     "ygx_encode_sort": (I32, [P, I64, P, P, P, P, P, SZ, P]),
     "ygx_sort_pairs_workspace_size": (SZ, [I64]),
     "ygx_sort_pairs": (I32, [P, P, I64, I32, I32, P, P, P, SZ, P]),
+    "ygx_sort_pairs_noalloc": (I32, [P, P, I64, I32, I32, P, P, P]),
     "ygx_reorder": (I32, [P, P, P, I64, I32, P, P, P, P, P]),
     "ygx_leaves_adaptive": (I32, [P, I64, I64, I32, P, P, P, P, P]),
     "ygx_leaves_fixed": (I32, [P, I64, I32, I32, P, P, P, P, P]),
