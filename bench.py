@@ -370,6 +370,9 @@ def stage_breakdown(pos_d, mass_d, dev):
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     marks = {}
+    from yggdrax_b200 import interactions as I
+
+    I._TIMING = True
     torch.cuda.synchronize(dev)
     a, b, c, d = ev(), ev(), ev(), ev()
     a.record()

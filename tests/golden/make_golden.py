@@ -1,0 +1,186 @@
+"""Generate golden fixtures by running the reference yggdrax source.
+
+Run in a container that has the reference checkout (default
+/root/reference/yggdrax) but no JAX: the reference modules are imported over
+``jaxshim`` (NumPy with JAX's indexing / scatter / search semantics) and
+executed on small seeded inputs.  The outputs are written as ``*.npz`` next
+to this script and are what ``tests/test_golden.py`` checks the oracle
+against.  Within-row order of the interaction / neighbour lists is
+unspecified in the reference (unstable argsort), so rows are stored sorted.
+
+Usage: python tests/golden/make_golden.py [reference_package_dir]
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import jaxshim  # noqa: E402
+
+TREE_FIELDS = ["parent", "left_child", "right_child", "left_is_leaf", "right_is_leaf",
+               "particle_indices", "morton_codes", "node_ranges", "node_level", "level_offsets",
+               "nodes_by_level", "num_levels", "bounds_min", "bounds_max", "leaf_codes",
+               "leaf_depths"]
+OCT_FIELDS = ["oct_parent", "oct_children", "oct_child_counts", "oct_child_mask",
+              "oct_valid_mask", "oct_node_codes", "oct_node_depths", "oct_node_ranges",
+              "oct_nodes_by_level", "oct_level_offsets", "oct_num_levels", "oct_leaf_mask",
+              "oct_leaf_nodes", "radix_node_to_oct", "radix_leaf_to_oct"]
+
+
+def _rows_sorted(offsets, counts, vals):
+    out = np.array(vals, copy=True)
+    for s, c in zip(np.asarray(offsets)[: len(counts)], np.asarray(counts)):
+        if c > 1:
+            out[s: s + c] = np.sort(out[s: s + c])
+    return out
+
+
+def _inputs():
+    rng = np.random.default_rng(2024)
+    uni = rng.uniform(-1, 1, (300, 3)).astype(np.float32)
+    # Plummer-like radial profile (small)
+    x = rng.uniform(0, 1, 400)
+    r = 1.0 / np.sqrt(x ** (-2.0 / 3.0) - 1.0)
+    r = np.minimum(r, 20.0)
+    d = rng.normal(size=(400, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    plum = (r[:, None] * d).astype(np.float32)
+    cl = np.concatenate([rng.normal(c, s, (200, 3)) for c, s in
+                         [((-3, 0, 1), 0.05), ((2, 2, -1), 0.3), ((0, -2, 2), 0.02)]])
+    clumps = cl.astype(np.float32)
+    col = np.array([[float(i), 0.0, 0.0] for i in range(128)], np.float32)
+    dup = np.zeros((16, 3), np.float32)
+    return dict(uniform300=uni, plummer400=plum, clumps600=clumps, collinear128=col, dup16=dup)
+
+
+def main(root: str) -> None:
+    m = jaxshim.load_reference(root)
+    jnp = sys.modules["jax.numpy"]
+    ti, oc, gi, ii, bd, mo = (m["_tree_impl"], m["octree"], m["_geometry_impl"],
+                              m["_interactions_impl"], m["bounds"], m["morton"])
+    inputs = _inputs()
+    col_bounds = (np.array([-10.0, -1.0, -1.0], np.float32), np.array([10.0, 1.0, 1.0], np.float32))
+
+    def save(name, **arrs):
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"),
+                            **{k: np.asarray(v) for k, v in arrs.items()})
+        print("wrote", name, len(arrs), "arrays")
+
+    def tree_arrays(prefix, t):
+        out = {}
+        for f in TREE_FIELDS:
+            out[f"{prefix}{f}"] = np.asarray(getattr(t, f))
+        out[f"{prefix}num_internal_nodes"] = np.asarray(int(t.num_internal_nodes))
+        return out
+
+    def geometry_arrays(prefix, g):
+        return {f"{prefix}center": g.center, f"{prefix}half_extent": g.half_extent,
+                f"{prefix}radius": g.radius, f"{prefix}max_extent": g.max_extent}
+
+    def walk_arrays(prefix, topo, g, theta, mac, cfg=None):
+        kw = {} if cfg is None else {"traversal_config": cfg}
+        inter, nbr = ii.build_interactions_and_neighbors(topo, g, theta=theta, mac_type=mac, **kw)
+        return {
+            f"{prefix}far_offsets": inter.offsets, f"{prefix}far_counts": inter.counts,
+            f"{prefix}far_sources": _rows_sorted(inter.offsets, inter.counts, inter.sources),
+            f"{prefix}far_targets": inter.targets,
+            f"{prefix}far_level_offsets": inter.level_offsets,
+            f"{prefix}far_target_levels": inter.target_levels,
+            f"{prefix}near_offsets": nbr.offsets, f"{prefix}near_counts": nbr.counts,
+            f"{prefix}near_neighbors": _rows_sorted(nbr.offsets, nbr.counts, nbr.neighbors),
+            f"{prefix}near_leaf_indices": nbr.leaf_indices,
+            f"{prefix}near_po_to_native": nbr.particle_order_to_native_leaf,
+        }
+
+    # -- L0: bounds, Morton codes, stable order ---------------------------------
+    arrs = {}
+    for name in ("uniform300", "plummer400", "clumps600"):
+        p = jnp.asarray(inputs[name])
+        b = bd.infer_bounds(p)
+        c = mo.morton_encode_impl(p, b)
+        arrs[f"{name}_pos"] = inputs[name]
+        arrs[f"{name}_bmin"], arrs[f"{name}_bmax"] = b
+        arrs[f"{name}_codes"] = c
+        arrs[f"{name}_order"] = jnp.argsort(c, stable=True)
+    p = jnp.asarray(inputs["collinear128"])
+    arrs["collinear128_pos"] = inputs["collinear128"]
+    arrs["collinear128_codes"] = mo.morton_encode_impl(p, (jnp.asarray(col_bounds[0]),
+                                                          jnp.asarray(col_bounds[1])))
+    save("morton", **arrs)
+
+    # -- L1/L2/L3 on adaptive trees ---------------------------------------------
+    for name, leaf in (("uniform300", 4), ("uniform300", 1), ("plummer400", 8), ("dup16", 1),
+                       ("dup16", 4)):
+        pos = inputs[name]
+        mass = np.linspace(0.5, 1.5, pos.shape[0]).astype(np.float32)
+        p, ms = jnp.asarray(pos), jnp.asarray(mass)
+        b = bd.infer_bounds(p)
+        t, ps, msrt, inv = ti.build_tree(p, ms, b, leaf_size=leaf, return_reordered=True)
+        out = dict(pos=pos, mass=mass, positions_sorted=ps, masses_sorted=msrt, inverse=inv)
+        out.update(tree_arrays("", t))
+        g = gi.compute_tree_geometry(t, ps, max_leaf_size=leaf)
+        out.update(geometry_arrays("geom_", g))
+        aug = oc.augment_radix_topology_with_octree(t)
+        for f in OCT_FIELDS:
+            out[f] = np.asarray(getattr(aug, f))
+        if name != "dup16" and leaf > 1:
+            for theta, mac in ((0.6, "dehnen"), (0.5, "bh"), (0.5, "engblom")):
+                out.update(walk_arrays(f"walk_{mac}_", t, g, theta, mac))
+            out.update(walk_arrays("walkoct_dehnen_", aug, g, 0.6, "dehnen"))
+            cfg = ii.DualTreeTraversalConfig(max_pair_queue=4096, process_block=64,
+                                             max_interactions_per_node=256,
+                                             max_neighbors_per_leaf=256)
+            out.update(walk_arrays("padded_dehnen_", t, g, 0.6, "dehnen", cfg))
+        save(f"adaptive_{name}_leaf{leaf}", **out)
+
+    # -- fixed depth (+ local refinement) ---------------------------------------
+    for name, target, bounds in (("clumps600", 8, None), ("collinear128", 8, col_bounds),
+                                 ("plummer400", 4, None)):
+        pos = inputs[name]
+        mass = np.linspace(0.5, 1.5, pos.shape[0]).astype(np.float32)
+        p, ms = jnp.asarray(pos), jnp.asarray(mass)
+        b = bd.infer_bounds(p) if bounds is None else (jnp.asarray(bounds[0]),
+                                                       jnp.asarray(bounds[1]))
+        for refine in (True, False):
+            t, ps, msrt, inv = ti.build_fixed_depth_tree(
+                p, ms, b, target_leaf_particles=target, refine_local=refine,
+                return_reordered=True)
+            out = dict(pos=pos, mass=mass, positions_sorted=ps, masses_sorted=msrt, inverse=inv,
+                       bmin_in=np.asarray(b[0]), bmax_in=np.asarray(b[1]))
+            out.update(tree_arrays("", t))
+            g = gi.compute_tree_geometry(t, ps)
+            out.update(geometry_arrays("geom_", g))
+            aug = oc.augment_radix_topology_with_octree(t)
+            for f in OCT_FIELDS:
+                out[f] = np.asarray(getattr(aug, f))
+            if name != "collinear128":
+                out.update(walk_arrays("walkoct_dehnen_", aug, g, 0.6, "dehnen"))
+            save(f"fixed_{name}_t{target}_{'refine' if refine else 'plain'}", **out)
+
+    # -- refinement helper on its own (pure NumPy in the reference) --------------
+    rng = np.random.default_rng(5)
+    pts = np.concatenate([rng.normal(0, [1.0, 0.01, 0.01], (300, 3)),
+                          rng.normal(0.5, [0.02, 0.5, 0.02], (300, 3))]).astype(np.float32)
+    p = jnp.asarray(pts)
+    b = bd.infer_bounds(p)
+    codes = np.asarray(mo.morton_encode_impl(p, b))
+    order = np.argsort(codes, kind="stable")
+    sc = codes[order]
+    for depth in (1, 2):
+        starts, ends, lc, ld = (np.asarray(a) for a in ti._fixed_depth_leaf_partitions(
+            jnp.asarray(sc), depth, pts.shape[0]))
+        r = ti._refine_leaf_partitions_by_aspect(pts[order], sc, starts.astype(np.int64),
+                                                 ends.astype(np.int64), lc.astype(np.uint64),
+                                                 ld.astype(np.int64), depth)
+        save(f"refine_d{depth}", pos_sorted=pts[order], sorted_codes=sc, starts=starts,
+             ends=ends, codes=lc, depths=ld, out_starts=r[0], out_ends=r[1], out_codes=r[2],
+             out_depths=r[3])
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/yggdrax")

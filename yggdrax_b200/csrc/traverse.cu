@@ -92,8 +92,11 @@ __device__ __forceinline__ int agg_slot(int32_t* cur, int key, bool pred) {
   return slot;
 }
 
+constexpr int kWalkThreads = 512;
+constexpr int kStage = 8192;  // staged child pairs per CTA (64 KB)
+
 template <int kMode, int kMac>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kWalkThreads, 2)
     k_walk_gen(const NodeRec* __restrict__ nodes, int32_t ni, float theta_sq, float theta,
                const int2* __restrict__ wf_in, int2* __restrict__ wf_out,
                uint32_t* __restrict__ sizes, int gen, uint32_t cap, int32_t* __restrict__ far_cnt,
@@ -102,16 +105,42 @@ __global__ void __launch_bounds__(256)
                const int32_t* __restrict__ near_expect, int32_t* __restrict__ far_src,
                int32_t* __restrict__ near_nbr, unsigned long long* __restrict__ stats,
                uint32_t* __restrict__ status) {
+  extern __shared__ int2 s_stage[];  // kStage entries (dynamic shared memory)
+  __shared__ uint32_t s_cnt, s_base, s_need_flush;
   // After an overflow the counter may exceed the buffer: never read past it.
   const uint32_t size = sizes[gen] < cap ? sizes[gen] : cap;
   if (size == 0) return;
   const int lane = threadIdx.x & 31;
-  const unsigned lt = lanemask_lt();
+  if (threadIdx.x == 0) s_cnt = 0;
   unsigned long long n_acc = 0, n_near = 0, n_ref = 0;
+
+  // Child pairs of the CTA's pairs collect in shared memory and leave in
+  // contiguous chunks, one global reservation per chunk.
+  auto flush = [&]() {
+    __syncthreads();
+    const uint32_t cnt = s_cnt;
+    if (cnt > 0) {
+      if (threadIdx.x == 0) s_base = atomicAdd(&sizes[gen + 1], cnt);
+      __syncthreads();
+      const uint32_t base0 = s_base;
+      for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) {
+        if (base0 + k < cap) wf_out[base0 + k] = s_stage[k];
+        else raise_flag(status, kFlagQueueOverflow);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) s_cnt = 0;
+    }
+    __syncthreads();
+  };
+
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < size;
-       base += stride) {
-    const int64_t i = base + lane;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < size; base += stride) {
+    // Block-uniform decision: read the count between barriers.
+    __syncthreads();
+    if (threadIdx.x == 0) s_need_flush = s_cnt > (uint32_t)(kStage - 4 * kWalkThreads);
+    __syncthreads();
+    if (s_need_flush) flush();
+    const int64_t i = base + threadIdx.x;
     const bool valid = i < size;
     int t = 0, s = 0;
     if (valid) {
@@ -120,6 +149,9 @@ __global__ void __launch_bounds__(256)
       s = p.y;
     }
     NodeRec A, B;
+    A.c = make_float4(0.f, 0.f, 0.f, 0.f);
+    A.k = make_int4(-1, -1, 0, 0);
+    B = A;
     if (valid) { A = nodes[t]; B = nodes[s]; }
     bool acc = false, nearp = false, refine = false;
     if (valid) {
@@ -219,16 +251,13 @@ __global__ void __launch_bounds__(256)
     const int wtotal = __shfl_sync(0xffffffffu, incl, 31);
     if (wtotal > 0) {
       uint32_t wbase = 0;
-      if (lane == 31) wbase = atomicAdd(&sizes[gen + 1], (uint32_t)wtotal);
+      if (lane == 31) wbase = atomicAdd(&s_cnt, (uint32_t)wtotal);
       wbase = __shfl_sync(0xffffffffu, wbase, 31);
       const uint32_t o = wbase + (uint32_t)(incl - nc);
-      for (int k = 0; k < nc; ++k) {
-        if (o + k < cap) wf_out[o + k] = ch[k];
-        else raise_flag(status, kFlagQueueOverflow);
-      }
+      for (int k = 0; k < nc; ++k) s_stage[o + k] = ch[k];
     }
   }
-  (void)lt;
+  flush();
   if (lane == 0) {
     if (n_acc) atomicAdd(&stats[kStatAccept], n_acc);
     if (n_near) atomicAdd(&stats[kStatNear], n_near);
@@ -339,8 +368,9 @@ __global__ void k_near_offsets(const int64_t* __restrict__ off, const int32_t* _
 // kBlockRowCap: one CTA in shared memory; longer: one CTA in place in
 // global memory.
 
-constexpr int kWarpRowCap = 256;
-constexpr int kBlockRowCap = 8192;
+constexpr int kWarpRowCap = 1024;   // one warp, 4 KB of shared memory
+constexpr int kBlockRowCap = 16384; // one CTA, 64 KB of shared memory
+constexpr int kBigThreads = 512;
 
 template <bool kBlockSync>
 __device__ __forceinline__ void mirrored_bitonic(int32_t* a, int64_t n, int tid, int nthreads) {
@@ -409,13 +439,13 @@ __global__ void __launch_bounds__(256)
 // once), so they are ordered by setting one bit per entry in a bitmap over
 // all node ids and reading the bitmap back in order; if the bit count shows
 // duplicates the row is sorted in place in global memory instead.
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(kBigThreads)
     k_rows_big(const int32_t* __restrict__ big_rows, const uint32_t* __restrict__ n_big,
                const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
                const int32_t* __restrict__ row_level, int32_t* __restrict__ raw, int index_bits,
                void* vals_out, void* tgt_out, void* lvl_out, uint32_t* __restrict__ bitmaps,
                int64_t universe) {
-  __shared__ int32_t s_a[kBlockRowCap];
+  extern __shared__ int32_t s_a[];  // kBlockRowCap entries (dynamic shared memory)
   __shared__ int64_t s_warp[32];
   __shared__ int64_t s_total;
   const uint32_t nb = *n_big;
@@ -533,6 +563,7 @@ struct TravScratch {
 };
 
 constexpr int kMaxGens = 4096;
+constexpr int kBigGrid = kNumSMs * 3;
 
 static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap) {
   TravScratch s;
@@ -551,7 +582,7 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap) {
   s.near_off = a.take<int64_t>(L + 1);
   s.scan_tmp = a.take<int64_t>(scan_scratch_elems(total > L ? total : L));
   s.big_rows = a.take<int32_t>(total > L ? total : L);
-  s.bitmaps = a.take<uint32_t>((size_t)kNumSMs * ((total + 31) / 32));
+  s.bitmaps = a.take<uint32_t>((size_t)kBigGrid * ((total + 31) / 32));
   s.wf[0] = a.take<int2>(cap);
   s.wf[1] = a.take<int2>(cap);
   return s;
@@ -562,11 +593,19 @@ static int launch_gen(int mac, const TravScratch& s, int32_t ni, float theta_sq,
                       int gen, uint32_t cap, const int32_t* far_expect, const int32_t* near_expect,
                       int32_t* far_src, int32_t* near_nbr, int32_t* fc, int32_t* nc,
                       cudaStream_t st) {
-  const int grid = kNumSMs * 8;
+  const int grid = kNumSMs * 2;
   const int2* in = s.wf[gen & 1];
   int2* out = s.wf[(gen + 1) & 1];
+  const size_t smem = sizeof(int2) * kStage;
+  static bool attr_done[2] = {false, false};
+  if (!attr_done[kMode]) {
+    cudaFuncSetAttribute(k_walk_gen<kMode, kMacBH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_walk_gen<kMode, kMacDehnen>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_walk_gen<kMode, kMacEngblom>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_done[kMode] = true;
+  }
 #define YGX_GEN(MAC)                                                                          \
-  k_walk_gen<kMode, MAC><<<grid, 256, 0, st>>>(s.recs, ni, theta_sq, theta, in, out, s.sizes, \
+  k_walk_gen<kMode, MAC><<<grid, kWalkThreads, smem, st>>>(s.recs, ni, theta_sq, theta, in, out, s.sizes, \
                                                gen, cap, fc, nc, s.far_off, s.near_off,       \
                                                far_expect, near_expect, far_src, near_nbr,    \
                                                s.stats, s.status)
@@ -735,13 +774,19 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
   int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity);
   if (rc) return rc;
   const int grid_small = ygx::kNumSMs * 16;
+  const size_t big_smem = sizeof(int32_t) * ygx::kBlockRowCap;
+  static bool big_attr = false;
+  if (!big_attr) {
+    cudaFuncSetAttribute(ygx::k_rows_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem);
+    big_attr = true;
+  }
   // far rows
   if (cudaMemsetAsync(s.n_big, 0, sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
   ygx::k_rows_small<<<grid_small, 256, 0, stream>>>(total, s.far_off, s.far_cnt, level32, far_src32,
                                                     index_bits, far_sources, far_targets,
                                                     target_levels, s.big_rows, s.n_big);
   YGX_CHECK_LAUNCH();
-  ygx::k_rows_big<<<ygx::kNumSMs, 1024, 0, stream>>>(s.big_rows, s.n_big, s.far_off, s.far_cnt,
+  ygx::k_rows_big<<<ygx::kBigGrid, ygx::kBigThreads, big_smem, stream>>>(s.big_rows, s.n_big, s.far_off, s.far_cnt,
                                                      level32, far_src32, index_bits, far_sources,
                                                      far_targets, target_levels, s.bitmaps, total);
   YGX_CHECK_LAUNCH();
@@ -751,7 +796,7 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
                                                     index_bits, neighbors, nullptr, nullptr,
                                                     s.big_rows, s.n_big);
   YGX_CHECK_LAUNCH();
-  ygx::k_rows_big<<<ygx::kNumSMs, 1024, 0, stream>>>(s.big_rows, s.n_big, s.near_off, s.near_cnt,
+  ygx::k_rows_big<<<ygx::kBigGrid, ygx::kBigThreads, big_smem, stream>>>(s.big_rows, s.n_big, s.near_off, s.near_cnt,
                                                      nullptr, near_nbr32, index_bits, neighbors,
                                                      nullptr, nullptr, s.bitmaps, total);
   YGX_CHECK_LAUNCH();

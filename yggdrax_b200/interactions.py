@@ -204,6 +204,7 @@ def set_reference_limits(enabled: bool) -> None:
 
 _DENSE_BUDGET: Optional[int] = None
 LAST_WALK_STATS: dict = {}  # diagnostics of the most recent walk
+_TIMING = os.environ.get("YGGDRAX_B200_TIMING", "0") == "1"  # per-pass CUDA-event times
 
 
 def set_dense_neighbor_budget(nbytes: Optional[int]) -> None:
@@ -335,6 +336,10 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
             stats=dict(far_total=0, near_total=0, max_far=0, max_near=0, accept=0, near=0,
                        refine=0, max_wf=1, gens=0), num_levels=num_levels)
     d = _dev_of(topology)
+    timing = _TIMING
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(4)] if timing else None
+    if timing:
+        evs[0].record()
     center = geometry.center.contiguous().float()
     radius = geometry.radius.contiguous().float()
     max_extent = geometry.max_extent.contiguous().float()
@@ -361,6 +366,8 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
         if f:
             raise L.YgxError(f"traversal count pass reported flags {f:#x}")
         break
+    if timing:
+        evs[1].record()
     s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
     LAST_WALK_STATS.clear()
     LAST_WALK_STATS.update(s, wf_capacity=cap)
@@ -377,6 +384,8 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
         L.ptr(topology.level_offsets), num_levels, ib, L.ptr(node_offsets), L.ptr(far_counts),
         L.ptr(level_offsets), L.ptr(near_offsets), L.ptr(near_counts), L.ptr(far_src32),
         L.ptr(near_nbr32), L.ptr(ws), ws.numel(), st), "ygx_traverse_fill")
+    if timing:
+        evs[2].record()
     sources = torch.empty(P, dtype=idt, device=dev)
     targets = torch.empty(P, dtype=idt, device=dev)
     target_levels = torch.empty(P, dtype=idt, device=dev)
@@ -395,6 +404,12 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
         L.ptr(near_nbr32), L.ptr(sources), L.ptr(targets), L.ptr(target_levels),
         L.ptr(neighbors), L.ptr(nlp) if max_nbr > 0 else None, max_nbr, L.ptr(ws), ws.numel(),
         st), "ygx_traverse_finalize")
+    if timing:
+        evs[3].record()
+        torch.cuda.synchronize(dev)
+        LAST_WALK_STATS.update(count_ms=evs[0].elapsed_time(evs[1]),
+                               fill_ms=evs[1].elapsed_time(evs[2]),
+                               finalize_ms=evs[2].elapsed_time(evs[3]))
     f = L.read_status(ws)
     if f & (L.FLAG_FAR_OVERFLOW | L.FLAG_NEAR_OVERFLOW | L.FLAG_QUEUE_OVERFLOW):
         raise L.YgxError(f"traversal fill pass disagreed with the count pass (flags {f:#x})")
