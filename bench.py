@@ -380,8 +380,16 @@ def stage_breakdown(pos_d, mass_d, dev):
     b.record()
     geom = yb.compute_tree_geometry(tree, ps)
     c.record()
-    yb.build_interactions_and_neighbors(tree, geom, theta=THETA, mac_type=MAC)
+    inter, nbrs = yb.build_interactions_and_neighbors(tree, geom, theta=THETA, mac_type=MAC)
     d.record()
+    hist = {}
+    for name, cnt in (("far", inter.counts), ("near", nbrs.counts)):
+        c64 = cnt.to(torch.int64)
+        edges = [0, 32, 256, 1024, 16384, 1 << 40]
+        hist[name] = {f"<={edges[k + 1]}": [int(((c64 > edges[k]) & (c64 <= edges[k + 1])).sum()),
+                                           int(c64[(c64 > edges[k]) & (c64 <= edges[k + 1])].sum())]
+                      for k in range(len(edges) - 1)}
+    marks["row_histogram_rows_entries"] = hist
     torch.cuda.synchronize(dev)
     marks["build"] = a.elapsed_time(b)
     marks["geometry"] = b.elapsed_time(c)

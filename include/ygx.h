@@ -217,7 +217,8 @@ int ygx_traverse_count(const float* center, const float* radius, const float* ma
 /* Fill pass (_dual_tree_walk_compact_fill_impl, :2942-3558) plus the offset
  * tables of _result_to_interactions / _result_to_neighbors (:3561-3837). */
 int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta, int root,
-                      int64_t wf_capacity, int gens, const int32_t* nbl32,
+                      int64_t wf_capacity, int gens, int64_t far_total, int64_t near_total,
+                      const int32_t* nbl32,
                       const void* tree_level_offsets, int num_levels, int index_bits,
                       void* node_offsets, void* far_counts, void* level_offsets,
                       void* near_offsets, void* near_counts, int32_t* far_src32,

@@ -75,8 +75,8 @@ _SIGS = {
     "ygx_traverse_workspace_size": (SZ, [I64, I64, I64]),
     "ygx_traverse_count": (I32, [P, P, P, P, P, P, I64, I64, I32, F32, F32, I32, I64, P, P, P,
                                  SZ, P]),
-    "ygx_traverse_fill": (I32, [I64, I64, I32, F32, I32, I64, I32, P, P, I32, I32, P, P, P, P,
-                                P, P, P, P, SZ, P]),
+    "ygx_traverse_fill": (I32, [I64, I64, I32, F32, I32, I64, I32, I64, I64, P, P, I32, I32, P,
+                                P, P, P, P, P, P, P, SZ, P]),
     "ygx_traverse_finalize": (I32, [I64, I64, I64, P, P, I32, P, P, P, P, P, P, P, I64, P, SZ,
                                     P]),
 }

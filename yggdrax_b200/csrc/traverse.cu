@@ -92,17 +92,34 @@ __device__ __forceinline__ int agg_slot(int32_t* cur, int key, bool pred) {
   return slot;
 }
 
-constexpr int kWalkThreads = 512;
-constexpr int kStage = 8192;  // staged child pairs per CTA (64 KB)
+constexpr int kWalkThreads = 256;
+constexpr int kStage = 4096;  // staged child pairs per CTA (32 KB)
+constexpr int kWalkBlocksPerSM = 5;
+
+// Returns a unique absolute position pos[key]++ for every lane with pred.
+__device__ __forceinline__ unsigned long long agg_pos(unsigned long long* pos, int key,
+                                                      bool pred) {
+  unsigned m = __ballot_sync(0xffffffffu, pred);
+  unsigned long long p = 0;
+  if (pred) {
+    unsigned peers = __match_any_sync(m, key);
+    int leader = __ffs(peers) - 1;
+    unsigned long long base = 0;
+    if (((int)(threadIdx.x & 31)) == leader) base = atomicAdd(&pos[key], (unsigned long long)__popc(peers));
+    base = __shfl_sync(m, base, leader);
+    p = base + __popc(peers & lanemask_lt());
+  }
+  return p;
+}
 
 template <int kMode, int kMac>
-__global__ void __launch_bounds__(kWalkThreads, 2)
+__global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
     k_walk_gen(const NodeRec* __restrict__ nodes, int32_t ni, float theta_sq, float theta,
                const int2* __restrict__ wf_in, int2* __restrict__ wf_out,
                uint32_t* __restrict__ sizes, int gen, uint32_t cap, int32_t* __restrict__ far_cnt,
-               int32_t* __restrict__ near_cnt, const int64_t* __restrict__ far_off,
-               const int64_t* __restrict__ near_off, const int32_t* __restrict__ far_expect,
-               const int32_t* __restrict__ near_expect, int32_t* __restrict__ far_src,
+               int32_t* __restrict__ near_cnt, unsigned long long* __restrict__ far_pos,
+               unsigned long long* __restrict__ near_pos, unsigned long long far_total,
+               unsigned long long near_total, int32_t* __restrict__ far_src,
                int32_t* __restrict__ near_nbr, unsigned long long* __restrict__ stats,
                uint32_t* __restrict__ status) {
   extern __shared__ int2 s_stage[];  // kStage entries (dynamic shared memory)
@@ -186,26 +203,21 @@ __global__ void __launch_bounds__(kWalkThreads, 2)
       agg_count(near_cnt, A.k.z, nearp);
       agg_count(near_cnt, B.k.z, nearp);
     } else {
-      int st = agg_slot(far_cnt, t, acc);
+      // Cursors start at each row's offset, so the aggregated atomic yields
+      // the write position; k_check_cursors verifies every row ended exactly
+      // at its end.  A cursor that runs past the total is never written.
+      const unsigned long long pt = agg_pos(far_pos, t, acc);
+      const unsigned long long ps = agg_pos(far_pos, s, acc);
       if (acc) {
-        if (st < far_expect[t]) far_src[far_off[t] + st] = s;
-        else raise_flag(status, kFlagFarOverflow);
-      }
-      int ss = agg_slot(far_cnt, s, acc);
-      if (acc) {
-        if (ss < far_expect[s]) far_src[far_off[s] + ss] = t;
-        else raise_flag(status, kFlagFarOverflow);
+        if (pt < far_total) far_src[pt] = s; else raise_flag(status, kFlagFarOverflow);
+        if (ps < far_total) far_src[ps] = t; else raise_flag(status, kFlagFarOverflow);
       }
       const int lt_ = nearp ? A.k.z : 0, ls_ = nearp ? B.k.z : 0;
-      int nt = agg_slot(near_cnt, lt_, nearp);
+      const unsigned long long qt = agg_pos(near_pos, lt_, nearp);
+      const unsigned long long qs = agg_pos(near_pos, ls_, nearp);
       if (nearp) {
-        if (nt < near_expect[lt_]) near_nbr[near_off[lt_] + nt] = s;
-        else raise_flag(status, kFlagNearOverflow);
-      }
-      int ns = agg_slot(near_cnt, ls_, nearp);
-      if (nearp) {
-        if (ns < near_expect[ls_]) near_nbr[near_off[ls_] + ns] = t;
-        else raise_flag(status, kFlagNearOverflow);
+        if (qt < near_total) near_nbr[qt] = s; else raise_flag(status, kFlagNearOverflow);
+        if (qs < near_total) near_nbr[qs] = t; else raise_flag(status, kFlagNearOverflow);
       }
     }
 
@@ -262,6 +274,34 @@ __global__ void __launch_bounds__(kWalkThreads, 2)
     if (n_acc) atomicAdd(&stats[kStatAccept], n_acc);
     if (n_near) atomicAdd(&stats[kStatNear], n_near);
     if (n_ref) atomicAdd(&stats[kStatRefine], n_ref);
+  }
+}
+
+__global__ void k_init_cursors(const int64_t* __restrict__ far_off, int64_t total,
+                               unsigned long long* __restrict__ far_pos,
+                               const int64_t* __restrict__ near_off, int64_t L,
+                               unsigned long long* __restrict__ near_pos) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    far_pos[k] = (unsigned long long)far_off[k];
+    if (k < L) near_pos[k] = (unsigned long long)near_off[k];
+  }
+}
+
+// Every cursor must end exactly at its row's end (fill == count).
+__global__ void k_check_cursors(const int64_t* __restrict__ far_off,
+                                const int32_t* __restrict__ far_cnt,
+                                const unsigned long long* __restrict__ far_pos, int64_t total,
+                                const int64_t* __restrict__ near_off,
+                                const int32_t* __restrict__ near_cnt,
+                                const unsigned long long* __restrict__ near_pos, int64_t L,
+                                uint32_t* __restrict__ status) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    if (far_pos[k] != (unsigned long long)(far_off[k] + far_cnt[k]))
+      raise_flag(status, kFlagFarOverflow);
+    if (k < L && near_pos[k] != (unsigned long long)(near_off[k] + near_cnt[k]))
+      raise_flag(status, kFlagNearOverflow);
   }
 }
 
@@ -381,7 +421,8 @@ __device__ __forceinline__ void mirrored_bitonic(int32_t* a, int64_t n, int tid,
       const bool first = j == (k >> 1);
       // np2 / 2 comparators per step; comparator c -> lower index i
       for (int64_t c = tid; c < (np2 >> 1); c += nthreads) {
-        const int64_t i = ((c / j) * (2 * j)) + (c % j);  // bit j of i is clear
+        // j is a power of two: insert a zero bit at position log2(j).
+        const int64_t i = ((c & ~(j - 1)) << 1) | (c & (j - 1));
         const int64_t p = first ? (i ^ (k - 1)) : (i | j);
         const int64_t lo = i < p ? i : p, hi = i < p ? p : i;
         if (hi < n) {
@@ -408,29 +449,120 @@ __device__ __forceinline__ void emit_row(const int32_t* a, int64_t n, int64_t of
   }
 }
 
-__global__ void __launch_bounds__(256)
+// One warp sorts a row of up to 32*R entries held in registers in the
+// "blocked" layout: lane l holds elements l*R .. l*R+R-1.  Loads and stores
+// stay coalesced through a padded shared-memory transpose (row stride R+1,
+// conflict-free both ways).  With this layout the bitonic steps with
+// partner distance j < R are compare-exchanges between registers of one
+// lane and only the steps with j >= R exchange across lanes (shuffles).
+// The row is padded with INT32_MAX to 32*R entries.
+template <int R>
+__device__ __forceinline__ void warp_sort_row(const int32_t* __restrict__ raw, int64_t off,
+                                              int n, int index_bits, void* vals_out,
+                                              void* tgt_out, void* lvl_out, int32_t tgt,
+                                              int32_t lvl, int lane, int32_t* __restrict__ sm) {
+  constexpr int S = R + 1;
+  constexpr int LOGR = R == 1 ? 0 : R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : R == 16 ? 4 : 5;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int e = r * 32 + lane;
+    sm[(e >> LOGR) * S + (e & (R - 1))] = e < n ? raw[off + e] : INT32_MAX;
+  }
+  __syncwarp();
+  int32_t v[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = sm[lane * S + r];
+#pragma unroll
+  for (int k = 2; k <= 32 * R; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j < R) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if ((r & j) == 0) {
+            const int pr = r | j;
+            const bool up = (((lane << LOGR) + r) & k) == 0;
+            const int32_t x = v[r], y = v[pr];
+            const int32_t mn = x < y ? x : y, mx = x < y ? y : x;
+            v[r] = up ? mn : mx;
+            v[pr] = up ? mx : mn;
+          }
+        }
+      } else {
+        const int lj = j >> LOGR;
+        const bool lower = (lane & lj) == 0;
+        const bool up = ((lane << LOGR) & k) == 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int32_t y = __shfl_xor_sync(0xffffffffu, v[r], lj);
+          const int32_t mn = v[r] < y ? v[r] : y, mx = v[r] < y ? y : v[r];
+          v[r] = (lower == up) ? mn : mx;
+        }
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < R; ++r) sm[lane * S + r] = v[r];
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int e = r * 32 + lane;
+    if (e < n) {
+      const int32_t x = sm[(e >> LOGR) * S + (e & (R - 1))];
+      store_idx(vals_out, index_bits, off + e, x);
+      if (tgt_out) {
+        store_idx(tgt_out, index_bits, off + e, tgt);
+        store_idx(lvl_out, index_bits, off + e, lvl);
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// Rows of 513..1024 entries (32 registers per lane) run in their own kernel
+// so the <= 512 case keeps a smaller register budget and more warps.
+__global__ void __launch_bounds__(256, 2)
+    k_rows_mid(const int32_t* __restrict__ mid_rows, const uint32_t* __restrict__ n_mid,
+               const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
+               const int32_t* __restrict__ row_level, const int32_t* __restrict__ raw,
+               int index_bits, void* vals_out, void* tgt_out, void* lvl_out) {
+  __shared__ int32_t s_rows[8][32 * 33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int32_t* sm = s_rows[w];
+  const uint32_t nm = *n_mid;
+  for (uint32_t b = blockIdx.x * 8 + w; b < nm; b += gridDim.x * 8) {
+    const int32_t r = mid_rows[b];
+    warp_sort_row<32>(raw, row_off[r], row_cnt[r], index_bits, vals_out, tgt_out, lvl_out, r,
+                      row_level ? row_level[r] : 0, lane, sm);
+  }
+}
+
+__global__ void __launch_bounds__(256, 3)
     k_rows_small(int64_t rows, const int64_t* __restrict__ row_off,
                  const int32_t* __restrict__ row_cnt, const int32_t* __restrict__ row_level,
                  const int32_t* __restrict__ raw, int index_bits, void* vals_out, void* tgt_out,
-                 void* lvl_out, int32_t* __restrict__ big_rows, uint32_t* __restrict__ n_big) {
-  __shared__ int32_t s_buf[8][kWarpRowCap];
+                 void* lvl_out, int32_t* __restrict__ big_rows, uint32_t* __restrict__ n_big,
+                 int32_t* __restrict__ mid_rows, uint32_t* __restrict__ n_mid) {
+  __shared__ int32_t s_rows[8][32 * 17];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int32_t* sm = s_rows[w];
   const int64_t warps = (int64_t)gridDim.x * 8;
-  int32_t* a = s_buf[w];
   for (int64_t r = (int64_t)blockIdx.x * 8 + w; r < rows; r += warps) {
     const int64_t off = row_off[r];
-    const int64_t n = row_cnt[r];
+    const int n = row_cnt[r];
     if (n == 0) continue;
     if (n > kWarpRowCap) {
       if (lane == 0) big_rows[atomicAdd(n_big, 1u)] = (int32_t)r;
       continue;
     }
-    for (int k = lane; k < n; k += 32) a[k] = raw[off + k];
-    __syncwarp();
-    mirrored_bitonic<false>(a, n, lane, 32);
-    emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, (int32_t)r,
-             row_level ? row_level[r] : 0, lane, 32);
-    __syncwarp();
+    const int32_t tgt = (int32_t)r, lvl = row_level ? row_level[r] : 0;
+    if (n <= 32) warp_sort_row<1>(raw, off, n, index_bits, vals_out, tgt_out, lvl_out, tgt, lvl, lane, sm);
+    else if (n <= 64) warp_sort_row<2>(raw, off, n, index_bits, vals_out, tgt_out, lvl_out, tgt, lvl, lane, sm);
+    else if (n <= 128) warp_sort_row<4>(raw, off, n, index_bits, vals_out, tgt_out, lvl_out, tgt, lvl, lane, sm);
+    else if (n <= 256) warp_sort_row<8>(raw, off, n, index_bits, vals_out, tgt_out, lvl_out, tgt, lvl, lane, sm);
+    else if (n <= 512) warp_sort_row<16>(raw, off, n, index_bits, vals_out, tgt_out, lvl_out, tgt, lvl, lane, sm);
+    else if (lane == 0) mid_rows[atomicAdd(n_mid, 1u)] = (int32_t)r;
   }
 }
 
@@ -550,14 +682,15 @@ struct TravScratch {
   NodeRec* recs;
   int32_t* far_cnt;
   int32_t* near_cnt;
-  int32_t* far_cur;
-  int32_t* near_cur;
   int32_t* cnt_by_level;
   int64_t* obl;
   int64_t* far_off;
   int64_t* near_off;
+  unsigned long long* far_pos;
+  unsigned long long* near_pos;
   int64_t* scan_tmp;
   int32_t* big_rows;
+  int32_t* mid_rows;
   uint32_t* bitmaps;
   int2* wf[2];
 };
@@ -574,14 +707,15 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap) {
   s.recs = a.take<NodeRec>(total);
   s.far_cnt = a.take<int32_t>(total);
   s.near_cnt = a.take<int32_t>(L);
-  s.far_cur = a.take<int32_t>(total);
-  s.near_cur = a.take<int32_t>(L);
   s.cnt_by_level = a.take<int32_t>(total);
   s.obl = a.take<int64_t>(total + 1);
   s.far_off = a.take<int64_t>(total + 1);
   s.near_off = a.take<int64_t>(L + 1);
+  s.far_pos = a.take<unsigned long long>(total);
+  s.near_pos = a.take<unsigned long long>(L);
   s.scan_tmp = a.take<int64_t>(scan_scratch_elems(total > L ? total : L));
   s.big_rows = a.take<int32_t>(total > L ? total : L);
+  s.mid_rows = a.take<int32_t>(total > L ? total : L);
   s.bitmaps = a.take<uint32_t>((size_t)kBigGrid * ((total + 31) / 32));
   s.wf[0] = a.take<int2>(cap);
   s.wf[1] = a.take<int2>(cap);
@@ -590,10 +724,10 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap) {
 
 template <int kMode>
 static int launch_gen(int mac, const TravScratch& s, int32_t ni, float theta_sq, float theta,
-                      int gen, uint32_t cap, const int32_t* far_expect, const int32_t* near_expect,
-                      int32_t* far_src, int32_t* near_nbr, int32_t* fc, int32_t* nc,
-                      cudaStream_t st) {
-  const int grid = kNumSMs * 2;
+                      int gen, uint32_t cap, unsigned long long far_total,
+                      unsigned long long near_total, int32_t* far_src, int32_t* near_nbr,
+                      int32_t* fc, int32_t* nc, cudaStream_t st) {
+  const int grid = kNumSMs * kWalkBlocksPerSM;
   const int2* in = s.wf[gen & 1];
   int2* out = s.wf[(gen + 1) & 1];
   const size_t smem = sizeof(int2) * kStage;
@@ -606,8 +740,8 @@ static int launch_gen(int mac, const TravScratch& s, int32_t ni, float theta_sq,
   }
 #define YGX_GEN(MAC)                                                                          \
   k_walk_gen<kMode, MAC><<<grid, kWalkThreads, smem, st>>>(s.recs, ni, theta_sq, theta, in, out, s.sizes, \
-                                               gen, cap, fc, nc, s.far_off, s.near_off,       \
-                                               far_expect, near_expect, far_src, near_nbr,    \
+                                               gen, cap, fc, nc, s.far_pos, s.near_pos,       \
+                                               far_total, near_total, far_src, near_nbr,      \
                                                s.stats, s.status)
   if (mac == kMacBH) YGX_GEN(kMacBH);
   else if (mac == kMacDehnen) YGX_GEN(kMacDehnen);
@@ -675,7 +809,7 @@ int ygx_traverse_count(const float* center, const float* radius, const float* ma
   while (true) {
     for (int k = 0; k < chunk && gen < ygx::kMaxGens; ++k, ++gen) {
       rc = ygx::launch_gen<ygx::kCount>(mac, s, (int32_t)num_internal, theta_sq, theta_r, gen,
-                                        (uint32_t)wf_capacity, nullptr, nullptr, nullptr, nullptr,
+                                        (uint32_t)wf_capacity, 0ull, 0ull, nullptr, nullptr,
                                         s.far_cnt, s.near_cnt, stream);
       if (rc) return rc;
     }
@@ -711,7 +845,8 @@ int ygx_traverse_count(const float* center, const float* radius, const float* ma
 // (far total) / near_nbr32 (near total) in walk order.  `gens` is the
 // generation count reported by the count pass.  Does not synchronize.
 int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta, int root,
-                      int64_t wf_capacity, int gens, const int32_t* nbl32,
+                      int64_t wf_capacity, int gens, int64_t far_total, int64_t near_total,
+                      const int32_t* nbl32,
                       const void* tree_level_offsets, int num_levels, int index_bits,
                       void* node_offsets, void* far_counts, void* level_offsets,
                       void* near_offsets, void* near_counts, int32_t* far_src32,
@@ -726,6 +861,8 @@ int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta,
   const float th = theta;
   const float theta_sq = th * th;
   const float theta_r = sqrtf(theta_sq);
+  const unsigned long long far_total_u = (unsigned long long)far_total;
+  const unsigned long long near_total_u = (unsigned long long)near_total;
   ygx::k_gather_counts<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.far_cnt, nbl32, total,
                                                                       s.cnt_by_level);
   YGX_CHECK_LAUNCH();
@@ -741,18 +878,22 @@ int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta,
                                                                      index_bits, near_offsets,
                                                                      near_counts);
   YGX_CHECK_LAUNCH();
-  if (cudaMemsetAsync(s.far_cur, 0, sizeof(int32_t) * total, stream) != cudaSuccess ||
-      cudaMemsetAsync(s.near_cur, 0, sizeof(int32_t) * L, stream) != cudaSuccess ||
-      cudaMemsetAsync(s.sizes, 0, sizeof(uint32_t) * (ygx::kMaxGens + 2), stream) != cudaSuccess)
+  if (cudaMemsetAsync(s.sizes, 0, sizeof(uint32_t) * (ygx::kMaxGens + 2), stream) != cudaSuccess)
     return YGX_ERR_CUDA;
+  ygx::k_init_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.far_off, total, s.far_pos,
+                                                                     s.near_off, L, s.near_pos);
+  YGX_CHECK_LAUNCH();
   ygx::k_seed<<<1, 32, 0, stream>>>(s.wf[0], s.sizes, root);
   YGX_CHECK_LAUNCH();
   for (int gen = 0; gen < gens; ++gen) {
     rc = ygx::launch_gen<ygx::kFill>(mac, s, (int32_t)num_internal, theta_sq, theta_r, gen,
-                                     (uint32_t)wf_capacity, s.far_cnt, s.near_cnt, far_src32,
-                                     near_nbr32, s.far_cur, s.near_cur, stream);
+                                     (uint32_t)wf_capacity, far_total_u, near_total_u, far_src32,
+                                     near_nbr32, nullptr, nullptr, stream);
     if (rc) return rc;
   }
+  ygx::k_check_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      s.far_off, s.far_cnt, s.far_pos, total, s.near_off, s.near_cnt, s.near_pos, L, s.status);
+  YGX_CHECK_LAUNCH();
   return YGX_OK;
 }
 
@@ -781,20 +922,29 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
     big_attr = true;
   }
   // far rows
-  if (cudaMemsetAsync(s.n_big, 0, sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
+  if (cudaMemsetAsync(s.n_big, 0, 2 * sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
   ygx::k_rows_small<<<grid_small, 256, 0, stream>>>(total, s.far_off, s.far_cnt, level32, far_src32,
                                                     index_bits, far_sources, far_targets,
-                                                    target_levels, s.big_rows, s.n_big);
+                                                    target_levels, s.big_rows, s.n_big,
+                                                    s.mid_rows, s.n_big + 1);
+  YGX_CHECK_LAUNCH();
+  ygx::k_rows_mid<<<grid_small, 256, 0, stream>>>(s.mid_rows, s.n_big + 1, s.far_off, s.far_cnt,
+                                                  level32, far_src32, index_bits, far_sources,
+                                                  far_targets, target_levels);
   YGX_CHECK_LAUNCH();
   ygx::k_rows_big<<<ygx::kBigGrid, ygx::kBigThreads, big_smem, stream>>>(s.big_rows, s.n_big, s.far_off, s.far_cnt,
                                                      level32, far_src32, index_bits, far_sources,
                                                      far_targets, target_levels, s.bitmaps, total);
   YGX_CHECK_LAUNCH();
   // near rows
-  if (cudaMemsetAsync(s.n_big, 0, sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
+  if (cudaMemsetAsync(s.n_big, 0, 2 * sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
   ygx::k_rows_small<<<grid_small, 256, 0, stream>>>(L, s.near_off, s.near_cnt, nullptr, near_nbr32,
                                                     index_bits, neighbors, nullptr, nullptr,
-                                                    s.big_rows, s.n_big);
+                                                    s.big_rows, s.n_big, s.mid_rows, s.n_big + 1);
+  YGX_CHECK_LAUNCH();
+  ygx::k_rows_mid<<<grid_small, 256, 0, stream>>>(s.mid_rows, s.n_big + 1, s.near_off, s.near_cnt,
+                                                  nullptr, near_nbr32, index_bits, neighbors,
+                                                  nullptr, nullptr);
   YGX_CHECK_LAUNCH();
   ygx::k_rows_big<<<ygx::kBigGrid, ygx::kBigThreads, big_smem, stream>>>(s.big_rows, s.n_big, s.near_off, s.near_cnt,
                                                      nullptr, near_nbr32, index_bits, neighbors,

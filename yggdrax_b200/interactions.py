@@ -380,7 +380,7 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     far_src32 = torch.empty(max(P, 1), dtype=torch.int32, device=dev)
     near_nbr32 = torch.empty(max(Q, 1), dtype=torch.int32, device=dev)
     L.check(lib.ygx_traverse_fill(
-        total, ni, mac, float(theta), root, cap, s["gens"], L.ptr(d.nbl32),
+        total, ni, mac, float(theta), root, cap, s["gens"], P, Q, L.ptr(d.nbl32),
         L.ptr(topology.level_offsets), num_levels, ib, L.ptr(node_offsets), L.ptr(far_counts),
         L.ptr(level_offsets), L.ptr(near_offsets), L.ptr(near_counts), L.ptr(far_src32),
         L.ptr(near_nbr32), L.ptr(ws), ws.numel(), st), "ygx_traverse_fill")
