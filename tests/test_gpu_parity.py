@@ -307,3 +307,26 @@ def test_reference_count_pass_limit(cuda_device):
     mask = np.ones(d.shape[0], bool)
     mask[starts[(starts > 0) & (starts <= d.shape[0])] - 1] = False
     assert (d[mask] > 0).all()
+
+
+def test_wavefront_overflow_retries_with_larger_capacity(cuda_device):
+    """A wavefront capacity far below the walk's peak makes the count pass
+    report a queue overflow; the walk is re-run with a larger wavefront and
+    returns the same lists as a walk that never overflowed."""
+    import yggdrax_b200 as yb
+    from yggdrax_b200 import inputs
+    from yggdrax_b200.interactions import LAST_WALK_STATS, _run_walk
+
+    pos, mass = inputs.uniform_cube(1 << 20, 3)
+    P, M = _to_dev(pos, cuda_device), _to_dev(mass, cuda_device)
+    gt, ps = yb.build_tree(P, M, leaf_size=8, return_reordered=True)[:2]
+    gg = yb.compute_tree_geometry(gt, ps)
+    a = _run_walk(gt, gg, 0.6, "dehnen", 1.0)
+    peak = LAST_WALK_STATS["max_wf"]
+    assert peak > 2_000_000
+    b = _run_walk(gt, gg, 0.6, "dehnen", 1.0, wf_capacity=4)
+    assert LAST_WALK_STATS["wf_capacity"] > 4
+    assert LAST_WALK_STATS["max_wf"] == peak
+    for f in ("far_counts", "node_offsets", "level_offsets", "sources", "targets",
+              "near_counts", "near_offsets", "neighbors"):
+        np.testing.assert_array_equal(_np(getattr(a, f)), _np(getattr(b, f)), err_msg=f)

@@ -77,26 +77,8 @@ __device__ __forceinline__ void agg_count(int32_t* cnt, int key, bool pred) {
     if ((peers & lanemask_lt()) == 0) atomicAdd(&cnt[key], __popc(peers));
   }
 }
-// Returns a unique slot cursor[key]++ for every lane with pred.
-__device__ __forceinline__ int agg_slot(int32_t* cur, int key, bool pred) {
-  unsigned m = __ballot_sync(0xffffffffu, pred);
-  int slot = 0;
-  if (pred) {
-    unsigned peers = __match_any_sync(m, key);
-    int leader = __ffs(peers) - 1;
-    int base = 0;
-    if (((int)(threadIdx.x & 31)) == leader) base = atomicAdd(&cur[key], __popc(peers));
-    base = __shfl_sync(m, base, leader);
-    slot = base + __popc(peers & lanemask_lt());
-  }
-  return slot;
-}
-
-constexpr int kWalkThreads = 256;
-constexpr int kStage = 4096;  // staged child pairs per CTA (32 KB)
-constexpr int kWalkBlocksPerSM = 5;
-
-// Returns a unique absolute position pos[key]++ for every lane with pred.
+// Returns a unique absolute position pos[key]++ for every lane with pred,
+// one atomic per distinct key in the warp.
 __device__ __forceinline__ unsigned long long agg_pos(unsigned long long* pos, int key,
                                                       bool pred) {
   unsigned m = __ballot_sync(0xffffffffu, pred);
@@ -105,73 +87,122 @@ __device__ __forceinline__ unsigned long long agg_pos(unsigned long long* pos, i
     unsigned peers = __match_any_sync(m, key);
     int leader = __ffs(peers) - 1;
     unsigned long long base = 0;
-    if (((int)(threadIdx.x & 31)) == leader) base = atomicAdd(&pos[key], (unsigned long long)__popc(peers));
+    if (((int)(threadIdx.x & 31)) == leader)
+      base = atomicAdd(&pos[key], (unsigned long long)__popc(peers));
     base = __shfl_sync(m, base, leader);
     p = base + __popc(peers & lanemask_lt());
   }
   return p;
 }
 
+constexpr int kWalkThreads = 256;
+constexpr int kWalkBlocksPerSM = 6;
+constexpr int kWalkGrid = kNumSMs * kWalkBlocksPerSM;  // fixed across generations
+
+// One BFS generation.  The wavefront of generation g is split into
+// kWalkGrid regions, one per CTA of generation g-1, each holding cnt_in[r]
+// pairs at wf_in[r * R ...].  A CTA maps a global input index to (region,
+// offset) through the prefix sum of cnt_in kept in shared memory.  Input is
+// taken in 32-pair warp chunks interleaved across CTAs (chunk c goes to CTA
+// c mod G), and a CTA appends child pairs to its own output region in a
+// fixed order (iteration, warp, lane) with one barrier per iteration, so
+// the wavefront of every generation is the same in the count and the fill
+// pass: a fill pass cannot overflow where its count pass did not.
 template <int kMode, int kMac>
 __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
-    k_walk_gen(const NodeRec* __restrict__ nodes, int32_t ni, float theta_sq, float theta,
+    k_walk_gen(const NodeRec* __restrict__ nodes, int32_t ni, int32_t total_nodes,
+               float theta_sq, float theta,
                const int2* __restrict__ wf_in, int2* __restrict__ wf_out,
-               uint32_t* __restrict__ sizes, int gen, uint32_t cap, int32_t* __restrict__ far_cnt,
+               const uint32_t* __restrict__ cnt_in, uint32_t* __restrict__ cnt_out, uint32_t R,
+               uint32_t* __restrict__ sizes, int gen, int32_t* __restrict__ far_cnt,
                int32_t* __restrict__ near_cnt, unsigned long long* __restrict__ far_pos,
                unsigned long long* __restrict__ near_pos, unsigned long long far_total,
                unsigned long long near_total, int32_t* __restrict__ far_src,
                int32_t* __restrict__ near_nbr, unsigned long long* __restrict__ stats,
                uint32_t* __restrict__ status) {
-  extern __shared__ int2 s_stage[];  // kStage entries (dynamic shared memory)
-  __shared__ uint32_t s_cnt, s_base, s_need_flush;
-  // After an overflow the counter may exceed the buffer: never read past it.
-  const uint32_t size = sizes[gen] < cap ? sizes[gen] : cap;
-  if (size == 0) return;
-  const int lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) s_cnt = 0;
+  constexpr int kWarps = kWalkThreads / 32;
+  __shared__ uint32_t s_prefix[kWalkGrid + 1];
+  __shared__ uint32_t s_wsum[kWarps];
+  __shared__ uint32_t s_wt[2][kWarps];
+  const int G = gridDim.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // Exclusive prefix of the input region counts (G <= kWalkGrid).
+  {
+    constexpr int kPer = (kWalkGrid + kWalkThreads - 1) / kWalkThreads;
+    uint32_t v[kPer];
+    uint32_t mine = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int r = tid * kPer + k;
+      v[k] = r < G ? cnt_in[r] : 0u;
+      mine += v[k];
+    }
+    uint32_t incl = mine;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= off) incl += o;
+    }
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    uint32_t wpre = 0;
+    for (int w = 0; w < warp; ++w) wpre += s_wsum[w];
+    uint32_t run = wpre + incl - mine;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int r = tid * kPer + k;
+      if (r < G) s_prefix[r] = run;
+      run += v[k];
+    }
+    if (tid == kWalkThreads - 1) s_prefix[G] = run;
+    __syncthreads();
+  }
+  const uint32_t total_in = s_prefix[G];
+  if (total_in == 0) {
+    if (tid == 0) cnt_out[blockIdx.x] = 0;
+    return;
+  }
+  int2* my_out = wf_out + (size_t)blockIdx.x * R;
   unsigned long long n_acc = 0, n_near = 0, n_ref = 0;
-
-  // Child pairs of the CTA's pairs collect in shared memory and leave in
-  // contiguous chunks, one global reservation per chunk.
-  auto flush = [&]() {
-    __syncthreads();
-    const uint32_t cnt = s_cnt;
-    if (cnt > 0) {
-      if (threadIdx.x == 0) s_base = atomicAdd(&sizes[gen + 1], cnt);
-      __syncthreads();
-      const uint32_t base0 = s_base;
-      for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) {
-        if (base0 + k < cap) wf_out[base0 + k] = s_stage[k];
-        else raise_flag(status, kFlagQueueOverflow);
+  unsigned long long cta_base = 0;  // block-uniform: pairs appended so far
+  int buf = 0;
+  for (int64_t k = 0;; ++k, buf ^= 1) {
+    const int64_t chunk0 = k * kWarps * G + blockIdx.x;  // warp 0's chunk
+    if (chunk0 * 32 >= (int64_t)total_in) break;         // block-uniform
+    const int64_t wbase = (chunk0 + (int64_t)warp * G) * 32;
+    const int64_t i = wbase + lane;
+    const bool valid = i < (int64_t)total_in;
+    int t = 0, sv = 0;
+    if (wbase < (int64_t)total_in) {
+      // Region of the warp's first index (last r with prefix[r] <= wbase),
+      // then each lane steps past the regions its own index has left.
+      int r = 0, hi = G;
+      while (hi - r > 1) {
+        const int mid = (r + hi) >> 1;
+        if (s_prefix[mid] <= (uint32_t)wbase) r = mid; else hi = mid;
       }
-      __syncthreads();
-      if (threadIdx.x == 0) s_cnt = 0;
+      if (valid) {
+        while (r + 1 < G && s_prefix[r + 1] <= (uint32_t)i) ++r;
+        const int2 p = wf_in[(size_t)r * R + ((uint32_t)i - s_prefix[r])];
+        t = p.x;
+        sv = p.y;
+      }
     }
-    __syncthreads();
-  };
-
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < size; base += stride) {
-    // Block-uniform decision: read the count between barriers.
-    __syncthreads();
-    if (threadIdx.x == 0) s_need_flush = s_cnt > (uint32_t)(kStage - 4 * kWalkThreads);
-    __syncthreads();
-    if (s_need_flush) flush();
-    const int64_t i = base + threadIdx.x;
-    const bool valid = i < size;
-    int t = 0, s = 0;
-    if (valid) {
-      int2 p = wf_in[i];
-      t = p.x;
-      s = p.y;
-    }
+    const bool in_range = (unsigned)t < (unsigned)total_nodes &&
+                          (unsigned)sv < (unsigned)total_nodes;
+    if (valid && !in_range) raise_flag(status, kFlagBadInput);
+    const bool live = valid && in_range;
     NodeRec A, B;
-    A.c = make_float4(0.f, 0.f, 0.f, 0.f);
-    A.k = make_int4(-1, -1, 0, 0);
-    B = A;
-    if (valid) { A = nodes[t]; B = nodes[s]; }
+    if (live) {
+      A = nodes[t];
+      B = nodes[sv];
+    } else {
+      A.c = make_float4(0.f, 0.f, 0.f, 0.f);
+      A.k = make_int4(-1, -1, 0, 0);
+      B = A;
+    }
     bool acc = false, nearp = false, refine = false;
-    if (valid) {
+    if (live) {
       const float dx = __fsub_rn(A.c.x, B.c.x);
       const float dy = __fsub_rn(A.c.y, B.c.y);
       const float dz = __fsub_rn(A.c.z, B.c.z);
@@ -188,9 +219,9 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
         const float sum = __fadd_rn(et, es);
         ok = __fmul_rn(sum, sum) <= __fmul_rn(theta_sq, d2);
       }
-      const bool diff = t != s;
+      const bool diff = t != sv;
       acc = diff && d2 > 0.0f && ok;
-      nearp = !acc && diff && t >= ni && s >= ni;
+      nearp = !acc && diff && t >= ni && sv >= ni;
       refine = !acc && !nearp;
     }
     n_acc += __popc(__ballot_sync(0xffffffffu, acc));
@@ -199,58 +230,58 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
 
     if (kMode == kCount) {
       agg_count(far_cnt, t, acc);
-      agg_count(far_cnt, s, acc);
+      agg_count(far_cnt, sv, acc);
       agg_count(near_cnt, A.k.z, nearp);
       agg_count(near_cnt, B.k.z, nearp);
     } else {
       // Cursors start at each row's offset, so the aggregated atomic yields
-      // the write position; k_check_cursors verifies every row ended exactly
-      // at its end.  A cursor that runs past the total is never written.
+      // the write position; k_check_cursors verifies every row ended
+      // exactly at its end.  Nothing past the total is written.
       const unsigned long long pt = agg_pos(far_pos, t, acc);
-      const unsigned long long ps = agg_pos(far_pos, s, acc);
+      const unsigned long long ps = agg_pos(far_pos, sv, acc);
       if (acc) {
-        if (pt < far_total) far_src[pt] = s; else raise_flag(status, kFlagFarOverflow);
+        if (pt < far_total) far_src[pt] = sv; else raise_flag(status, kFlagFarOverflow);
         if (ps < far_total) far_src[ps] = t; else raise_flag(status, kFlagFarOverflow);
       }
       const int lt_ = nearp ? A.k.z : 0, ls_ = nearp ? B.k.z : 0;
       const unsigned long long qt = agg_pos(near_pos, lt_, nearp);
       const unsigned long long qs = agg_pos(near_pos, ls_, nearp);
       if (nearp) {
-        if (qt < near_total) near_nbr[qt] = s; else raise_flag(status, kFlagNearOverflow);
+        if (qt < near_total) near_nbr[qt] = sv; else raise_flag(status, kFlagNearOverflow);
         if (qs < near_total) near_nbr[qs] = t; else raise_flag(status, kFlagNearOverflow);
       }
     }
 
     // Children of a refined pair (_interactions_impl.py:1262-1310).
     int nc = 0;
-    int2 ch[4];
+    int2 c0 = make_int2(0, 0), c1 = c0, c2 = c0, c3 = c0;
     if (refine) {
-      const bool same = t == s;
-      const bool t_int = t < ni, s_int = s < ni;
+      const bool same = t == sv;
+      const bool t_int = t < ni, s_int = sv < ni;
       const float et = A.c.w, es = B.c.w;
       const bool split_t = t_int && (same || !s_int || et >= es);
       const bool split_s = s_int && (same || !t_int || es > et);
       auto mk = [](int a, int b) { return a < b ? make_int2(a, b) : make_int2(b, a); };
       if (split_t && split_s) {
         if (same) {
-          ch[0] = mk(A.k.x, A.k.x);
-          ch[1] = mk(A.k.x, A.k.y);
-          ch[2] = mk(A.k.y, A.k.y);
+          c0 = mk(A.k.x, A.k.x);
+          c1 = mk(A.k.x, A.k.y);
+          c2 = mk(A.k.y, A.k.y);
           nc = 3;
         } else {
-          ch[0] = mk(A.k.x, B.k.x);
-          ch[1] = mk(A.k.x, B.k.y);
-          ch[2] = mk(A.k.y, B.k.x);
-          ch[3] = mk(A.k.y, B.k.y);
+          c0 = mk(A.k.x, B.k.x);
+          c1 = mk(A.k.x, B.k.y);
+          c2 = mk(A.k.y, B.k.x);
+          c3 = mk(A.k.y, B.k.y);
           nc = 4;
         }
       } else if (split_t) {
-        ch[0] = mk(A.k.x, s);
-        ch[1] = mk(A.k.y, s);
+        c0 = mk(A.k.x, sv);
+        c1 = mk(A.k.y, sv);
         nc = 2;
       } else if (split_s) {
-        ch[0] = mk(t, B.k.x);
-        ch[1] = mk(t, B.k.y);
+        c0 = mk(t, B.k.x);
+        c1 = mk(t, B.k.y);
         nc = 2;
       }
     }
@@ -260,16 +291,39 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
       int v = __shfl_up_sync(0xffffffffu, incl, off);
       if (lane >= off) incl += v;
     }
-    const int wtotal = __shfl_sync(0xffffffffu, incl, 31);
-    if (wtotal > 0) {
-      uint32_t wbase = 0;
-      if (lane == 31) wbase = atomicAdd(&s_cnt, (uint32_t)wtotal);
-      wbase = __shfl_sync(0xffffffffu, wbase, 31);
-      const uint32_t o = wbase + (uint32_t)(incl - nc);
-      for (int k = 0; k < nc; ++k) s_stage[o + k] = ch[k];
+    if (lane == 31) s_wt[buf][warp] = (uint32_t)incl;
+    __syncthreads();
+    uint32_t pre = 0, sum = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t v = s_wt[buf][w];
+      pre += w < warp ? v : 0u;
+      sum += v;
     }
+    // Every child that fits is written, so the first min(total, R) slots of
+    // the region are always filled.
+    const unsigned long long at = cta_base + pre + (uint32_t)(incl - nc);
+    if (nc > 0) {
+      if (at + (unsigned long long)nc <= R) {
+        int2* o = my_out + at;
+        o[0] = c0;
+        if (nc > 1) o[1] = c1;
+        if (nc > 2) o[2] = c2;
+        if (nc > 3) o[3] = c3;
+      } else {
+        if (at + 0 < R) my_out[at + 0] = c0;
+        if (nc > 1 && at + 1 < R) my_out[at + 1] = c1;
+        if (nc > 2 && at + 2 < R) my_out[at + 2] = c2;
+        raise_flag(status, kFlagQueueOverflow);
+      }
+    }
+    cta_base += sum;
   }
-  flush();
+  if (tid == 0) {
+    const uint32_t c = cta_base < R ? (uint32_t)cta_base : R;
+    cnt_out[blockIdx.x] = c;
+    if (c) atomicAdd(&sizes[gen + 1], c);
+  }
   if (lane == 0) {
     if (n_acc) atomicAdd(&stats[kStatAccept], n_acc);
     if (n_near) atomicAdd(&stats[kStatNear], n_near);
@@ -305,8 +359,10 @@ __global__ void k_check_cursors(const int64_t* __restrict__ far_off,
   }
 }
 
-__global__ void k_seed(int2* wf, uint32_t* sizes, int root) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
+__global__ void k_seed(int2* wf, uint32_t* cnt, uint32_t* sizes, int root) {
+  // generation 0: one pair (root, root) in region 0, all other regions empty
+  for (int r = threadIdx.x; r < kWalkGrid; r += blockDim.x) cnt[r] = r == 0 ? 1u : 0u;
+  if (threadIdx.x == 0) {
     wf[0] = make_int2(root, root);
     sizes[0] = 1;
   }
@@ -413,20 +469,22 @@ constexpr int kBlockRowCap = 16384; // one CTA, 64 KB of shared memory
 constexpr int kBigThreads = 512;
 
 template <bool kBlockSync>
-__device__ __forceinline__ void mirrored_bitonic(int32_t* a, int64_t n, int tid, int nthreads) {
-  int64_t np2 = 1;
+__device__ __forceinline__ void mirrored_bitonic(int32_t* a, int64_t n64, int tid, int nthreads) {
+  // Row lengths stay below 2^31 (they are counts of one node's partners).
+  const int32_t n = (int32_t)n64;
+  int32_t np2 = 1;
   while (np2 < n) np2 <<= 1;
-  for (int64_t k = 2; k <= np2; k <<= 1) {
-    for (int64_t j = k >> 1; j > 0; j >>= 1) {
+  for (int32_t k = 2; k <= np2; k <<= 1) {
+    for (int32_t j = k >> 1; j > 0; j >>= 1) {
       const bool first = j == (k >> 1);
       // np2 / 2 comparators per step; comparator c -> lower index i
-      for (int64_t c = tid; c < (np2 >> 1); c += nthreads) {
+      for (int32_t c = tid; c < (np2 >> 1); c += nthreads) {
         // j is a power of two: insert a zero bit at position log2(j).
-        const int64_t i = ((c & ~(j - 1)) << 1) | (c & (j - 1));
-        const int64_t p = first ? (i ^ (k - 1)) : (i | j);
-        const int64_t lo = i < p ? i : p, hi = i < p ? p : i;
+        const int32_t i = ((c & ~(j - 1)) << 1) | (c & (j - 1));
+        const int32_t p = first ? (i ^ (k - 1)) : (i | j);
+        const int32_t lo = i < p ? i : p, hi = i < p ? p : i;
         if (hi < n) {
-          int32_t x = a[lo], y = a[hi];
+          const int32_t x = a[lo], y = a[hi];
           if (x > y) { a[lo] = y; a[hi] = x; }
         }
       }
@@ -520,49 +578,53 @@ __device__ __forceinline__ void warp_sort_row(const int32_t* __restrict__ raw, i
   __syncwarp();
 }
 
-// Rows of 513..1024 entries (32 registers per lane) run in their own kernel
-// so the <= 512 case keeps a smaller register budget and more warps.
-__global__ void __launch_bounds__(256, 2)
-    k_rows_mid(const int32_t* __restrict__ mid_rows, const uint32_t* __restrict__ n_mid,
-               const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
-               const int32_t* __restrict__ row_level, const int32_t* __restrict__ raw,
-               int index_bits, void* vals_out, void* tgt_out, void* lvl_out) {
-  __shared__ int32_t s_rows[8][32 * 33];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int32_t* sm = s_rows[w];
-  const uint32_t nm = *n_mid;
-  for (uint32_t b = blockIdx.x * 8 + w; b < nm; b += gridDim.x * 8) {
-    const int32_t r = mid_rows[b];
-    warp_sort_row<32>(raw, row_off[r], row_cnt[r], index_bits, vals_out, tgt_out, lvl_out, r,
-                      row_level ? row_level[r] : 0, lane, sm);
-  }
-}
+// Rows are bucketed by size class first; each class runs in its own kernel
+// with a single register-network instantiation (one instantiation per
+// kernel keeps the instruction footprint small).  Class c holds rows of
+// 32*2^(c-1) < n <= 32*2^c entries (c = 0: n <= 32); longer rows go to the
+// CTA kernel.
+constexpr int kRowClasses = 6;  // R = 1, 2, 4, 8, 16, 32
 
-__global__ void __launch_bounds__(256, 3)
-    k_rows_small(int64_t rows, const int64_t* __restrict__ row_off,
-                 const int32_t* __restrict__ row_cnt, const int32_t* __restrict__ row_level,
-                 const int32_t* __restrict__ raw, int index_bits, void* vals_out, void* tgt_out,
-                 void* lvl_out, int32_t* __restrict__ big_rows, uint32_t* __restrict__ n_big,
-                 int32_t* __restrict__ mid_rows, uint32_t* __restrict__ n_mid) {
-  __shared__ int32_t s_rows[8][32 * 17];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int32_t* sm = s_rows[w];
-  const int64_t warps = (int64_t)gridDim.x * 8;
-  for (int64_t r = (int64_t)blockIdx.x * 8 + w; r < rows; r += warps) {
-    const int64_t off = row_off[r];
+__global__ void k_rows_classify(int64_t rows, const int32_t* __restrict__ row_cnt,
+                                int32_t* __restrict__ lists, int64_t list_stride,
+                                uint32_t* __restrict__ list_n, int32_t* __restrict__ big_rows,
+                                uint32_t* __restrict__ n_big) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows;
+       r += (int64_t)gridDim.x * blockDim.x) {
     const int n = row_cnt[r];
     if (n == 0) continue;
     if (n > kWarpRowCap) {
-      if (lane == 0) big_rows[atomicAdd(n_big, 1u)] = (int32_t)r;
+      big_rows[atomicAdd(n_big, 1u)] = (int32_t)r;
       continue;
     }
-    const int32_t tgt = (int32_t)r, lvl = row_level ? row_level[r] : 0;
-    if (n <= 32) warp_sort_row<1>(raw, off, n, index_bits, vals_out, tgt_out, lvl_out, tgt, lvl, lane, sm);
-    else if (n <= 64) warp_sort_row<2>(raw, off, n, index_bits, vals_out, tgt_out, lvl_out, tgt, lvl, lane, sm);
-    else if (n <= 128) warp_sort_row<4>(raw, off, n, index_bits, vals_out, tgt_out, lvl_out, tgt, lvl, lane, sm);
-    else if (n <= 256) warp_sort_row<8>(raw, off, n, index_bits, vals_out, tgt_out, lvl_out, tgt, lvl, lane, sm);
-    else if (n <= 512) warp_sort_row<16>(raw, off, n, index_bits, vals_out, tgt_out, lvl_out, tgt, lvl, lane, sm);
-    else if (lane == 0) mid_rows[atomicAdd(n_mid, 1u)] = (int32_t)r;
+    int c = 0;
+    while ((32 << c) < n) ++c;
+    // warp-aggregated append per class
+    const unsigned m = __activemask();
+    const unsigned peers = __match_any_sync(m, c);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&list_n[c], (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    unsigned lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    lists[c * list_stride + base + __popc(peers & lt)] = (int32_t)r;
+  }
+}
+
+template <int R>
+__global__ void __launch_bounds__(256, R >= 32 ? 2 : (R >= 16 ? 3 : 4))
+    k_rows_class(const int32_t* __restrict__ list, const uint32_t* __restrict__ list_n,
+                 const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
+                 const int32_t* __restrict__ row_level, const int32_t* __restrict__ raw,
+                 int index_bits, void* vals_out, void* tgt_out, void* lvl_out) {
+  __shared__ int32_t s_rows[8][32 * (R + 1)];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t nm = *list_n;
+  for (uint32_t b = blockIdx.x * 8 + w; b < nm; b += gridDim.x * 8) {
+    const int32_t r = list[b];
+    warp_sort_row<R>(raw, row_off[r], row_cnt[r], index_bits, vals_out, tgt_out, lvl_out, r,
+                     row_level ? row_level[r] : 0, lane, s_rows[w]);
   }
 }
 
@@ -571,7 +633,7 @@ __global__ void __launch_bounds__(256, 3)
 // once), so they are ordered by setting one bit per entry in a bitmap over
 // all node ids and reading the bitmap back in order; if the bit count shows
 // duplicates the row is sorted in place in global memory instead.
-__global__ void __launch_bounds__(kBigThreads)
+__global__ void __launch_bounds__(kBigThreads, 3)
     k_rows_big(const int32_t* __restrict__ big_rows, const uint32_t* __restrict__ n_big,
                const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
                const int32_t* __restrict__ row_level, int32_t* __restrict__ raw, int index_bits,
@@ -690,12 +752,20 @@ struct TravScratch {
   unsigned long long* near_pos;
   int64_t* scan_tmp;
   int32_t* big_rows;
-  int32_t* mid_rows;
+  int32_t* class_rows;  // kRowClasses lists of max(total, L) rows
   uint32_t* bitmaps;
   int2* wf[2];
+  uint32_t* region_cnt[2];
 };
 
 constexpr int kMaxGens = 4096;
+// Every CTA of a generation appends at most 4 x kWalkThreads pairs per input
+// chunk; a region of at least that size keeps small walks from overflowing.
+constexpr int64_t kMinRegion = 4 * kWalkThreads;
+static int64_t region_capacity(int64_t cap) {
+  const int64_t r = cap / kWalkGrid;
+  return r < kMinRegion ? kMinRegion : r;
+}
 constexpr int kBigGrid = kNumSMs * 3;
 
 static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap) {
@@ -703,7 +773,7 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap) {
   s.status = a.take<uint32_t>(64);
   s.stats = a.take<unsigned long long>(kStatWords);
   s.sizes = a.take<uint32_t>(kMaxGens + 2);
-  s.n_big = a.take<uint32_t>(64);
+  s.n_big = a.take<uint32_t>(64);  // [0] long rows, [1..6] class counts
   s.recs = a.take<NodeRec>(total);
   s.far_cnt = a.take<int32_t>(total);
   s.near_cnt = a.take<int32_t>(L);
@@ -715,34 +785,31 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap) {
   s.near_pos = a.take<unsigned long long>(L);
   s.scan_tmp = a.take<int64_t>(scan_scratch_elems(total > L ? total : L));
   s.big_rows = a.take<int32_t>(total > L ? total : L);
-  s.mid_rows = a.take<int32_t>(total > L ? total : L);
+  s.class_rows = a.take<int32_t>((size_t)kRowClasses * (total > L ? total : L));
   s.bitmaps = a.take<uint32_t>((size_t)kBigGrid * ((total + 31) / 32));
-  s.wf[0] = a.take<int2>(cap);
-  s.wf[1] = a.take<int2>(cap);
+  s.wf[0] = a.take<int2>(region_capacity(cap) * kWalkGrid);
+  s.wf[1] = a.take<int2>(region_capacity(cap) * kWalkGrid);
+  s.region_cnt[0] = a.take<uint32_t>(kWalkGrid);
+  s.region_cnt[1] = a.take<uint32_t>(kWalkGrid);
   return s;
 }
 
 template <int kMode>
-static int launch_gen(int mac, const TravScratch& s, int32_t ni, float theta_sq, float theta,
+static int launch_gen(int mac, const TravScratch& s, int32_t ni, int32_t total_nodes,
+                      float theta_sq, float theta,
                       int gen, uint32_t cap, unsigned long long far_total,
                       unsigned long long near_total, int32_t* far_src, int32_t* near_nbr,
                       int32_t* fc, int32_t* nc, cudaStream_t st) {
-  const int grid = kNumSMs * kWalkBlocksPerSM;
   const int2* in = s.wf[gen & 1];
   int2* out = s.wf[(gen + 1) & 1];
-  const size_t smem = sizeof(int2) * kStage;
-  static bool attr_done[2] = {false, false};
-  if (!attr_done[kMode]) {
-    cudaFuncSetAttribute(k_walk_gen<kMode, kMacBH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_walk_gen<kMode, kMacDehnen>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_walk_gen<kMode, kMacEngblom>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_done[kMode] = true;
-  }
+  const uint32_t* cin = s.region_cnt[gen & 1];
+  uint32_t* cout = s.region_cnt[(gen + 1) & 1];
+  const uint32_t R = (uint32_t)region_capacity(cap);
 #define YGX_GEN(MAC)                                                                          \
-  k_walk_gen<kMode, MAC><<<grid, kWalkThreads, smem, st>>>(s.recs, ni, theta_sq, theta, in, out, s.sizes, \
-                                               gen, cap, fc, nc, s.far_pos, s.near_pos,       \
-                                               far_total, near_total, far_src, near_nbr,      \
-                                               s.stats, s.status)
+  k_walk_gen<kMode, MAC><<<kWalkGrid, kWalkThreads, 0, st>>>(                                 \
+      s.recs, ni, total_nodes, theta_sq, theta, in, out, cin, cout, R, s.sizes, gen, fc, nc,   \
+      s.far_pos,                                                                              \
+      s.near_pos, far_total, near_total, far_src, near_nbr, s.stats, s.status)
   if (mac == kMacBH) YGX_GEN(kMacBH);
   else if (mac == kMacDehnen) YGX_GEN(kMacDehnen);
   else YGX_GEN(kMacEngblom);
@@ -782,7 +849,7 @@ int ygx_traverse_count(const float* center, const float* radius, const float* ma
                        float dehnen_radius_scale, int root, int64_t wf_capacity,
                        uint64_t* stats_out, uint32_t* flags_out, void* ws, size_t ws_bytes,
                        cudaStream_t stream) {
-  if (total < 3 || num_internal < 1 || mac < 0 || mac > 2 || wf_capacity < 4 ||
+  if (total < 3 || total > INT32_MAX || num_internal < 1 || mac < 0 || mac > 2 || wf_capacity < 4 ||
       wf_capacity > (int64_t)UINT32_MAX || !stats_out || !flags_out)
     return YGX_ERR_ARG;
   const int64_t L = total - num_internal;
@@ -802,13 +869,13 @@ int ygx_traverse_count(const float* center, const float* radius, const float* ma
       center, radius, max_extent, left32, right32, leafpos32, total, mac, dehnen_radius_scale,
       s.recs, s.status);
   YGX_CHECK_LAUNCH();
-  ygx::k_seed<<<1, 32, 0, stream>>>(s.wf[0], s.sizes, root);
+  ygx::k_seed<<<1, 256, 0, stream>>>(s.wf[0], s.region_cnt[0], s.sizes, root);
   YGX_CHECK_LAUNCH();
   int gen = 0;
   const int chunk = 16;
   while (true) {
     for (int k = 0; k < chunk && gen < ygx::kMaxGens; ++k, ++gen) {
-      rc = ygx::launch_gen<ygx::kCount>(mac, s, (int32_t)num_internal, theta_sq, theta_r, gen,
+      rc = ygx::launch_gen<ygx::kCount>(mac, s, (int32_t)num_internal, (int32_t)total, theta_sq, theta_r, gen,
                                         (uint32_t)wf_capacity, 0ull, 0ull, nullptr, nullptr,
                                         s.far_cnt, s.near_cnt, stream);
       if (rc) return rc;
@@ -851,7 +918,7 @@ int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta,
                       void* node_offsets, void* far_counts, void* level_offsets,
                       void* near_offsets, void* near_counts, int32_t* far_src32,
                       int32_t* near_nbr32, void* ws, size_t ws_bytes, cudaStream_t stream) {
-  if (total < 3 || num_internal < 1 || gens < 0 || gens > ygx::kMaxGens ||
+  if (total < 3 || total > INT32_MAX || num_internal < 1 || gens < 0 || gens > ygx::kMaxGens ||
       (index_bits != 32 && index_bits != 64))
     return YGX_ERR_ARG;
   const int64_t L = total - num_internal;
@@ -883,10 +950,10 @@ int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta,
   ygx::k_init_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.far_off, total, s.far_pos,
                                                                      s.near_off, L, s.near_pos);
   YGX_CHECK_LAUNCH();
-  ygx::k_seed<<<1, 32, 0, stream>>>(s.wf[0], s.sizes, root);
+  ygx::k_seed<<<1, 256, 0, stream>>>(s.wf[0], s.region_cnt[0], s.sizes, root);
   YGX_CHECK_LAUNCH();
   for (int gen = 0; gen < gens; ++gen) {
-    rc = ygx::launch_gen<ygx::kFill>(mac, s, (int32_t)num_internal, theta_sq, theta_r, gen,
+    rc = ygx::launch_gen<ygx::kFill>(mac, s, (int32_t)num_internal, (int32_t)total, theta_sq, theta_r, gen,
                                      (uint32_t)wf_capacity, far_total_u, near_total_u, far_src32,
                                      near_nbr32, nullptr, nullptr, stream);
     if (rc) return rc;
@@ -921,35 +988,30 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
     cudaFuncSetAttribute(ygx::k_rows_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem);
     big_attr = true;
   }
-  // far rows
-  if (cudaMemsetAsync(s.n_big, 0, 2 * sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
-  ygx::k_rows_small<<<grid_small, 256, 0, stream>>>(total, s.far_off, s.far_cnt, level32, far_src32,
-                                                    index_bits, far_sources, far_targets,
-                                                    target_levels, s.big_rows, s.n_big,
-                                                    s.mid_rows, s.n_big + 1);
+  const int64_t stride = total > L ? total : L;
+  auto rows_pass = [&](int64_t rows, const int64_t* off, const int32_t* cnt, const int32_t* lvl,
+                       int32_t* raw, void* vals, void* tgts, void* lvls) -> int {
+    if (cudaMemsetAsync(s.n_big, 0, 8 * sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
+    ygx::k_rows_classify<<<ygx::grid_for(rows, 256), 256, 0, stream>>>(
+        rows, cnt, s.class_rows, stride, s.n_big + 1, s.big_rows, s.n_big);
+    YGX_CHECK_LAUNCH();
+#define YGX_ROWS(C, R)                                                                       \
+  ygx::k_rows_class<R><<<grid_small, 256, 0, stream>>>(s.class_rows + (C) * stride,            \
+                                                       s.n_big + 1 + (C), off, cnt, lvl, raw, \
+                                                       index_bits, vals, tgts, lvls);         \
   YGX_CHECK_LAUNCH();
-  ygx::k_rows_mid<<<grid_small, 256, 0, stream>>>(s.mid_rows, s.n_big + 1, s.far_off, s.far_cnt,
-                                                  level32, far_src32, index_bits, far_sources,
-                                                  far_targets, target_levels);
-  YGX_CHECK_LAUNCH();
-  ygx::k_rows_big<<<ygx::kBigGrid, ygx::kBigThreads, big_smem, stream>>>(s.big_rows, s.n_big, s.far_off, s.far_cnt,
-                                                     level32, far_src32, index_bits, far_sources,
-                                                     far_targets, target_levels, s.bitmaps, total);
-  YGX_CHECK_LAUNCH();
-  // near rows
-  if (cudaMemsetAsync(s.n_big, 0, 2 * sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
-  ygx::k_rows_small<<<grid_small, 256, 0, stream>>>(L, s.near_off, s.near_cnt, nullptr, near_nbr32,
-                                                    index_bits, neighbors, nullptr, nullptr,
-                                                    s.big_rows, s.n_big, s.mid_rows, s.n_big + 1);
-  YGX_CHECK_LAUNCH();
-  ygx::k_rows_mid<<<grid_small, 256, 0, stream>>>(s.mid_rows, s.n_big + 1, s.near_off, s.near_cnt,
-                                                  nullptr, near_nbr32, index_bits, neighbors,
-                                                  nullptr, nullptr);
-  YGX_CHECK_LAUNCH();
-  ygx::k_rows_big<<<ygx::kBigGrid, ygx::kBigThreads, big_smem, stream>>>(s.big_rows, s.n_big, s.near_off, s.near_cnt,
-                                                     nullptr, near_nbr32, index_bits, neighbors,
-                                                     nullptr, nullptr, s.bitmaps, total);
-  YGX_CHECK_LAUNCH();
+    YGX_ROWS(0, 1) YGX_ROWS(1, 2) YGX_ROWS(2, 4) YGX_ROWS(3, 8) YGX_ROWS(4, 16) YGX_ROWS(5, 32)
+#undef YGX_ROWS
+    ygx::k_rows_big<<<ygx::kBigGrid, ygx::kBigThreads, big_smem, stream>>>(
+        s.big_rows, s.n_big, off, cnt, lvl, raw, index_bits, vals, tgts, lvls, s.bitmaps, total);
+    YGX_CHECK_LAUNCH();
+    return YGX_OK;
+  };
+  int rc2 = rows_pass(total, s.far_off, s.far_cnt, level32, far_src32, far_sources, far_targets,
+                      target_levels);
+  if (rc2) return rc2;
+  rc2 = rows_pass(L, s.near_off, s.near_cnt, nullptr, near_nbr32, neighbors, nullptr, nullptr);
+  if (rc2) return rc2;
   if (neighbor_leaf_positions && max_nbr > 0) {
     ygx::k_neighbor_leaf_positions<<<ygx::grid_for(L * max_nbr, 256), 256, 0, stream>>>(
         s.near_off, s.near_cnt, L, neighbors, index_bits, leafpos32, max_nbr,
