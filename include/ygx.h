@@ -47,6 +47,7 @@ enum {
 #define YGX_FLAG_NEAR_OVERFLOW (1u << 3)
 #define YGX_FLAG_MALFORMED (1u << 4)
 #define YGX_FLAG_BAD_INPUT (1u << 5)
+#define YGX_FLAG_LOG_OVERFLOW (1u << 6)
 
 /* traversal statistics words (host array of YGX_TSTAT_WORDS uint64) */
 #define YGX_TSTAT_WORDS 16
@@ -59,6 +60,8 @@ enum {
 #define YGX_TSTAT_REFINE 6      /* refine decisions                            */
 #define YGX_TSTAT_MAX_WF 7      /* largest wavefront                           */
 #define YGX_TSTAT_GENS 8        /* wavefront generations                       */
+#define YGX_TSTAT_WF_NEED 9     /* wf_capacity that would have fit             */
+#define YGX_TSTAT_LOG_NEED 10   /* log_capacity that would have fit            */
 
 #ifdef __cplusplus
 extern "C" {
@@ -203,22 +206,32 @@ int ygx_tree_geometry(const void* node_ranges, int64_t total, int index_bits,
 
 /* ---- L3: dual-tree traversal ------------------------------------------------ */
 
-size_t ygx_traverse_workspace_size(int64_t total, int64_t num_leaves, int64_t wf_capacity);
-/* Count pass of build_interactions_and_neighbors
- * (yggdrax/_interactions_impl.py:2600-2939 _dual_tree_walk_count_impl):
+/* wf_capacity: wavefront pairs over all walk regions; log_capacity: logged
+ * (accepted or near) pairs over all log regions.  The walk reports in
+ * YGX_TSTAT_WF_NEED / YGX_TSTAT_LOG_NEED the capacities that would have fit. */
+size_t ygx_traverse_workspace_size(int64_t total, int64_t num_leaves, int64_t wf_capacity,
+                                   int64_t log_capacity);
+/* The walk of build_interactions_and_neighbors: the count walk
+ * (yggdrax/_interactions_impl.py:2600-2939 _dual_tree_walk_count_impl) and
+ * the pair enumeration of the fill walk (:2942-3558) in one pass; every
+ * accepted / near pair is logged once for ygx_traverse_fill.
  * mac 0 = "bh", 1 = "dehnen", 2 = "engblom".  stats_out / flags_out are HOST
- * arrays (YGX_TSTAT_WORDS / 1 words).  Synchronizes the stream. */
-int ygx_traverse_count(const float* center, const float* radius, const float* max_extent,
-                       const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
-                       int64_t total, int64_t num_internal, int mac, float theta,
-                       float dehnen_radius_scale, int root, int64_t wf_capacity,
-                       uint64_t* stats_out, uint32_t* flags_out, void* ws, size_t ws_bytes,
-                       cudaStream_t stream);
-/* Fill pass (_dual_tree_walk_compact_fill_impl, :2942-3558) plus the offset
- * tables of _result_to_interactions / _result_to_neighbors (:3561-3837). */
-int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta, int root,
-                      int64_t wf_capacity, int gens, int64_t far_total, int64_t near_total,
-                      const int32_t* nbl32,
+ * arrays (YGX_TSTAT_WORDS / 1 words).  YGX_FLAG_QUEUE_OVERFLOW or
+ * YGX_FLAG_LOG_OVERFLOW in *flags_out: re-run with larger capacities (the
+ * walk is deterministic; the reported log need is exact).  Synchronizes the
+ * stream. */
+int ygx_traverse_walk(const float* center, const float* radius, const float* max_extent,
+                      const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
+                      int64_t total, int64_t num_internal, int mac, float theta,
+                      float dehnen_radius_scale, int root, int64_t wf_capacity,
+                      int64_t log_capacity, uint64_t* stats_out, uint32_t* flags_out, void* ws,
+                      size_t ws_bytes, cudaStream_t stream);
+/* Row layout of the fill walk (_dual_tree_walk_compact_fill_impl,
+ * :2942-3558) and the offset tables of _result_to_interactions /
+ * _result_to_neighbors (:3561-3837), from the walk's counts and pair log. */
+int ygx_traverse_fill(int64_t total, int64_t num_internal, int64_t wf_capacity,
+                      int64_t log_capacity, int64_t far_total, int64_t near_total,
+                      const int32_t* nbl32, const int32_t* leafpos32,
                       const void* tree_level_offsets, int num_levels, int index_bits,
                       void* node_offsets, void* far_counts, void* level_offsets,
                       void* near_offsets, void* near_counts, int32_t* far_src32,
@@ -227,7 +240,7 @@ int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta,
  * far sources/targets/target_levels, leaf-ordered near neighbours, and
  * optionally the dense neighbour_leaf_positions table (L x max_nbr). */
 int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capacity,
-                          const int32_t* level32, const int32_t* leafpos32, int index_bits,
+                          int64_t log_capacity, const int32_t* level32, const int32_t* leafpos32, int index_bits,
                           int32_t* far_src32, int32_t* near_nbr32, void* far_sources,
                           void* far_targets, void* target_levels, void* neighbors,
                           void* neighbor_leaf_positions, int64_t max_nbr, void* ws,

@@ -16,7 +16,7 @@ def _declared():
 
 def test_header_declares_entry_points():
     names = _declared()
-    assert "ygx_encode_sort" in names and "ygx_traverse_count" in names
+    assert "ygx_encode_sort" in names and "ygx_traverse_walk" in names
     assert len(names) >= 20
 
 
@@ -40,7 +40,7 @@ def test_workspace_size_queries_run_without_gpu():
         assert lib.ygx_encode_sort_workspace_size(n) > 0
         assert lib.ygx_sort_pairs_workspace_size(n) > 0
     assert lib.ygx_topology_workspace_size(1024) > lib.ygx_topology_workspace_size(2)
-    assert lib.ygx_traverse_workspace_size(2047, 1024, 1 << 16) > (1 << 16) * 16
+    assert lib.ygx_traverse_workspace_size(2047, 1024, 1 << 16, 1 << 16) > (1 << 16) * 24
 
 
 def test_product_does_not_import_oracle():

@@ -34,10 +34,11 @@ FLAG_FAR_OVERFLOW = 1 << 2
 FLAG_NEAR_OVERFLOW = 1 << 3
 FLAG_MALFORMED = 1 << 4
 FLAG_BAD_INPUT = 1 << 5
+FLAG_LOG_OVERFLOW = 1 << 6
 
 TSTAT_WORDS = 16
 TSTAT = dict(far_total=0, near_total=1, max_far=2, max_near=3, accept=4, near=5, refine=6,
-             max_wf=7, gens=8)
+             max_wf=7, gens=8, wf_need=9, log_need=10)
 
 P = ctypes.c_void_p
 I64 = ctypes.c_int64
@@ -72,12 +73,12 @@ _SIGS = {
     "ygx_geometry_workspace_size": (SZ, [I64]),
     "ygx_tree_geometry": (I32, [P, I64, I32, P, P, P, P, P, P, I64, I32, P, P, P, I64, P, P,
                                 P, P, P, SZ, P]),
-    "ygx_traverse_workspace_size": (SZ, [I64, I64, I64]),
-    "ygx_traverse_count": (I32, [P, P, P, P, P, P, I64, I64, I32, F32, F32, I32, I64, P, P, P,
-                                 SZ, P]),
-    "ygx_traverse_fill": (I32, [I64, I64, I32, F32, I32, I64, I32, I64, I64, P, P, I32, I32, P,
-                                P, P, P, P, P, P, P, SZ, P]),
-    "ygx_traverse_finalize": (I32, [I64, I64, I64, P, P, I32, P, P, P, P, P, P, P, I64, P, SZ,
+    "ygx_traverse_workspace_size": (SZ, [I64, I64, I64, I64]),
+    "ygx_traverse_walk": (I32, [P, P, P, P, P, P, I64, I64, I32, F32, F32, I32, I64, I64, P, P,
+                                P, SZ, P]),
+    "ygx_traverse_fill": (I32, [I64, I64, I64, I64, I64, I64, P, P, P, I32, I32, P, P, P, P, P,
+                                P, P, P, SZ, P]),
+    "ygx_traverse_finalize": (I32, [I64, I64, I64, I64, P, P, I32, P, P, P, P, P, P, P, I64, P, SZ,
                                     P]),
 }
 

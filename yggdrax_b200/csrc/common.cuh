@@ -20,6 +20,7 @@ enum StatusFlag : uint32_t {
   kFlagNearOverflow = 1u << 3,
   kFlagMalformed = 1u << 4,
   kFlagBadInput = 1u << 5,
+  kFlagLogOverflow = 1u << 6,
 };
 
 // Iteration limit of every device-side spin (decoupled look-back).  A wait

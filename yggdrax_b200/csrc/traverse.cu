@@ -10,12 +10,14 @@
 // and child pairs (:1262-1310).  An accepted pair lands in both endpoints'
 // far rows, a near leaf pair in both leaves' near rows.
 //
-// Each BFS generation is one launch over the current wavefront; a warp
-// processes 32 pairs, aggregates its counter/cursor atomics per distinct
-// node with match-any, and pushes its child pairs with one atomic per warp.
-// The count pass sizes the rows; the fill pass writes each entry into its
-// row at an atomic cursor; the finalize pass sorts every row (canonical
-// order) and widens it into the level-major int64/int32 outputs.
+// Each BFS generation is one launch over the current wavefront.  One walk
+// does all the pair work: it counts every far / near row entry (per-node
+// counters, one atomic per distinct node per warp via match-any) and logs
+// every accepted or near pair once, as (lo, hi | near-bit), in the CTA's own
+// region of a pair log.  A scan of the counts gives the row offsets; a
+// scatter pass reads the log back coalesced and writes each pair into both
+// endpoints' rows at atomic cursors; the finalize pass sorts every row
+// (canonical order) and widens it into the level-major int64/int32 outputs.
 #include "scan.cuh"
 
 namespace ygx {
@@ -26,7 +28,6 @@ struct __align__(16) NodeRec {
   int4 k;    // left child, right child (-1 for leaves), leaf position (-1 internal), 0
 };
 
-enum WalkMode { kCount = 0, kFill = 1 };
 enum MacKind { kMacBH = 0, kMacDehnen = 1, kMacEngblom = 2 };
 
 // stats words (uint64): see ygx.h YGX_TSTAT_*
@@ -40,6 +41,8 @@ enum {
   kStatRefine = 6,
   kStatMaxWf = 7,
   kStatGens = 8,
+  kStatWfNeed = 9,
+  kStatLogNeed = 10,
   kStatWords = 16
 };
 
@@ -104,22 +107,22 @@ constexpr int kWalkGrid = kNumSMs * kWalkBlocksPerSM;  // fixed across generatio
 // pairs at wf_in[r * R ...].  A CTA maps a global input index to (region,
 // offset) through the prefix sum of cnt_in kept in shared memory.  Input is
 // taken in 32-pair warp chunks interleaved across CTAs (chunk c goes to CTA
-// c mod G), and a CTA appends child pairs to its own output region in a
-// fixed order (iteration, warp, lane) with one barrier per iteration, so
-// the wavefront of every generation is the same in the count and the fill
-// pass: a fill pass cannot overflow where its count pass did not.
-template <int kMode, int kMac>
+// c mod G), and a CTA appends child pairs to its own wavefront region and
+// accepted / near pairs to its own log region (which grows over all
+// generations, log_cnt[b] entries so far) in a fixed order (iteration,
+// warp, lane) with one barrier per iteration.  The walk is therefore
+// deterministic, and the entries a region would have needed are counted
+// even past its end, so one re-run with the reported sizes always fits.
+template <int kMac>
 __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
     k_walk_gen(const NodeRec* __restrict__ nodes, int32_t ni, int32_t total_nodes,
                float theta_sq, float theta,
                const int2* __restrict__ wf_in, int2* __restrict__ wf_out,
                const uint32_t* __restrict__ cnt_in, uint32_t* __restrict__ cnt_out, uint32_t R,
                uint32_t* __restrict__ sizes, int gen, int32_t* __restrict__ far_cnt,
-               int32_t* __restrict__ near_cnt, unsigned long long* __restrict__ far_pos,
-               unsigned long long* __restrict__ near_pos, unsigned long long far_total,
-               unsigned long long near_total, int32_t* __restrict__ far_src,
-               int32_t* __restrict__ near_nbr, unsigned long long* __restrict__ stats,
-               uint32_t* __restrict__ status) {
+               int32_t* __restrict__ near_cnt, int2* __restrict__ log,
+               unsigned long long* __restrict__ log_cnt, unsigned long long LR,
+               unsigned long long* __restrict__ stats, uint32_t* __restrict__ status) {
   constexpr int kWarps = kWalkThreads / 32;
   __shared__ uint32_t s_prefix[kWalkGrid + 1];
   __shared__ uint32_t s_wsum[kWarps];
@@ -165,6 +168,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
   int2* my_out = wf_out + (size_t)blockIdx.x * R;
   unsigned long long n_acc = 0, n_near = 0, n_ref = 0;
   unsigned long long cta_base = 0;  // block-uniform: pairs appended so far
+  unsigned long long log_base = log_cnt[blockIdx.x];  // block-uniform
   int buf = 0;
   for (int64_t k = 0;; ++k, buf ^= 1) {
     const int64_t chunk0 = k * kWarps * G + blockIdx.x;  // warp 0's chunk
@@ -228,29 +232,10 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
     n_near += __popc(__ballot_sync(0xffffffffu, nearp));
     n_ref += __popc(__ballot_sync(0xffffffffu, refine));
 
-    if (kMode == kCount) {
-      agg_count(far_cnt, t, acc);
-      agg_count(far_cnt, sv, acc);
-      agg_count(near_cnt, A.k.z, nearp);
-      agg_count(near_cnt, B.k.z, nearp);
-    } else {
-      // Cursors start at each row's offset, so the aggregated atomic yields
-      // the write position; k_check_cursors verifies every row ended
-      // exactly at its end.  Nothing past the total is written.
-      const unsigned long long pt = agg_pos(far_pos, t, acc);
-      const unsigned long long ps = agg_pos(far_pos, sv, acc);
-      if (acc) {
-        if (pt < far_total) far_src[pt] = sv; else raise_flag(status, kFlagFarOverflow);
-        if (ps < far_total) far_src[ps] = t; else raise_flag(status, kFlagFarOverflow);
-      }
-      const int lt_ = nearp ? A.k.z : 0, ls_ = nearp ? B.k.z : 0;
-      const unsigned long long qt = agg_pos(near_pos, lt_, nearp);
-      const unsigned long long qs = agg_pos(near_pos, ls_, nearp);
-      if (nearp) {
-        if (qt < near_total) near_nbr[qt] = sv; else raise_flag(status, kFlagNearOverflow);
-        if (qs < near_total) near_nbr[qs] = t; else raise_flag(status, kFlagNearOverflow);
-      }
-    }
+    agg_count(far_cnt, t, acc);
+    agg_count(far_cnt, sv, acc);
+    agg_count(near_cnt, A.k.z, nearp);
+    agg_count(near_cnt, B.k.z, nearp);
 
     // Children of a refined pair (_interactions_impl.py:1262-1310).
     int nc = 0;
@@ -291,7 +276,10 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
       int v = __shfl_up_sync(0xffffffffu, incl, off);
       if (lane >= off) incl += v;
     }
-    if (lane == 31) s_wt[buf][warp] = (uint32_t)incl;
+    const bool lg = acc || nearp;
+    const unsigned lmask = __ballot_sync(0xffffffffu, lg);
+    // children (<= 128 per warp) in the low half, log entries in the high
+    if (lane == 31) s_wt[buf][warp] = (uint32_t)incl | ((uint32_t)__popc(lmask) << 16);
     __syncthreads();
     uint32_t pre = 0, sum = 0;
 #pragma unroll
@@ -300,6 +288,16 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
       pre += w < warp ? v : 0u;
       sum += v;
     }
+    if (lg) {
+      const unsigned long long la = log_base + (pre >> 16) + __popc(lmask & lanemask_lt());
+      if (la < LR)
+        log[(size_t)blockIdx.x * LR + la] = make_int2(t, sv | (nearp ? (int)0x80000000u : 0));
+      else
+        raise_flag(status, kFlagLogOverflow);
+    }
+    log_base += sum >> 16;
+    sum &= 0xffffu;
+    pre &= 0xffffu;
     // Every child that fits is written, so the first min(total, R) slots of
     // the region are always filled.
     const unsigned long long at = cta_base + pre + (uint32_t)(incl - nc);
@@ -323,6 +321,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
     const uint32_t c = cta_base < R ? (uint32_t)cta_base : R;
     cnt_out[blockIdx.x] = c;
     if (c) atomicAdd(&sizes[gen + 1], c);
+    log_cnt[blockIdx.x] = log_base;
+    atomicMax(&stats[kStatWfNeed], cta_base);
   }
   if (lane == 0) {
     if (n_acc) atomicAdd(&stats[kStatAccept], n_acc);
@@ -339,6 +339,50 @@ __global__ void k_init_cursors(const int64_t* __restrict__ far_off, int64_t tota
        k += (int64_t)gridDim.x * blockDim.x) {
     far_pos[k] = (unsigned long long)far_off[k];
     if (k < L) near_pos[k] = (unsigned long long)near_off[k];
+  }
+}
+
+// Scatter pass: CTA b reads its log region back in order and writes each
+// pair into both endpoints' rows.  Cursors start at each row's offset, so
+// the aggregated atomic yields the write position; k_check_cursors then
+// verifies every row ended exactly at its end.  Nothing past the totals is
+// written.
+__global__ void __launch_bounds__(256)
+    k_log_scatter(const int2* __restrict__ log, const unsigned long long* __restrict__ log_cnt,
+                  unsigned long long LR, const int32_t* __restrict__ leafpos,
+                  unsigned long long* __restrict__ far_pos,
+                  unsigned long long* __restrict__ near_pos, unsigned long long far_total,
+                  unsigned long long near_total, int32_t* __restrict__ far_src,
+                  int32_t* __restrict__ near_nbr, uint32_t* __restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  for (int b = blockIdx.x; b < kWalkGrid; b += gridDim.x) {
+    const unsigned long long n = log_cnt[b] < LR ? log_cnt[b] : LR;
+    const int2* src = log + (size_t)b * LR;
+    for (unsigned long long base = threadIdx.x & ~31u; base < n; base += blockDim.x) {
+      const unsigned long long i = base + lane;
+      int t = 0, sv = 0;
+      bool far = false, nearp = false;
+      if (i < n) {
+        const int2 e = src[i];
+        t = e.x;
+        sv = e.y & 0x7fffffff;
+        nearp = e.y < 0;
+        far = !nearp;
+      }
+      const unsigned long long pt = agg_pos(far_pos, t, far);
+      const unsigned long long ps = agg_pos(far_pos, sv, far);
+      if (far) {
+        if (pt < far_total) far_src[pt] = sv; else raise_flag(status, kFlagFarOverflow);
+        if (ps < far_total) far_src[ps] = t; else raise_flag(status, kFlagFarOverflow);
+      }
+      const int lt = nearp ? leafpos[t] : 0, ls = nearp ? leafpos[sv] : 0;
+      const unsigned long long qt = agg_pos(near_pos, lt, nearp);
+      const unsigned long long qs = agg_pos(near_pos, ls, nearp);
+      if (nearp) {
+        if (qt < near_total) near_nbr[qt] = sv; else raise_flag(status, kFlagNearOverflow);
+        if (qs < near_total) near_nbr[qs] = t; else raise_flag(status, kFlagNearOverflow);
+      }
+    }
   }
 }
 
@@ -372,6 +416,7 @@ __global__ void k_seed(int2* wf, uint32_t* cnt, uint32_t* sizes, int root) {
 __global__ void k_count_stats(const int32_t* __restrict__ far_cnt, int64_t total,
                               const int32_t* __restrict__ near_cnt, int64_t L,
                               const uint32_t* __restrict__ sizes, int max_gens,
+                              const unsigned long long* __restrict__ log_cnt,
                               unsigned long long* __restrict__ stats) {
   unsigned long long fsum = 0, nsum = 0, fmax = 0, nmax = 0;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
@@ -409,6 +454,11 @@ __global__ void k_count_stats(const int32_t* __restrict__ far_cnt, int64_t total
     }
     stats[kStatMaxWf] = mw;
     stats[kStatGens] = g;
+    // capacities (in total entries over all regions) that would have fit
+    unsigned long long ln = 0;
+    for (int b = 0; b < kWalkGrid; ++b) ln = log_cnt[b] > ln ? log_cnt[b] : ln;
+    stats[kStatLogNeed] = ln * kWalkGrid;
+    stats[kStatWfNeed] = stats[kStatWfNeed] * kWalkGrid;
   }
 }
 
@@ -756,6 +806,9 @@ struct TravScratch {
   uint32_t* bitmaps;
   int2* wf[2];
   uint32_t* region_cnt[2];
+  unsigned long long* log_cnt;
+  int2* log;
+  unsigned long long log_region;
 };
 
 constexpr int kMaxGens = 4096;
@@ -768,7 +821,13 @@ static int64_t region_capacity(int64_t cap) {
 }
 constexpr int kBigGrid = kNumSMs * 3;
 
-static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap) {
+// Entries per CTA log region for a total log capacity.
+static int64_t log_region_capacity(int64_t log_cap) {
+  const int64_t r = (log_cap + kWalkGrid - 1) / kWalkGrid;
+  return r < 1 ? 1 : r;
+}
+
+static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap, int64_t log_cap) {
   TravScratch s;
   s.status = a.take<uint32_t>(64);
   s.stats = a.take<unsigned long long>(kStatWords);
@@ -791,25 +850,23 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap) {
   s.wf[1] = a.take<int2>(region_capacity(cap) * kWalkGrid);
   s.region_cnt[0] = a.take<uint32_t>(kWalkGrid);
   s.region_cnt[1] = a.take<uint32_t>(kWalkGrid);
+  s.log_cnt = a.take<unsigned long long>(kWalkGrid);
+  s.log_region = (unsigned long long)log_region_capacity(log_cap);
+  s.log = a.take<int2>((size_t)s.log_region * kWalkGrid);
   return s;
 }
 
-template <int kMode>
 static int launch_gen(int mac, const TravScratch& s, int32_t ni, int32_t total_nodes,
-                      float theta_sq, float theta,
-                      int gen, uint32_t cap, unsigned long long far_total,
-                      unsigned long long near_total, int32_t* far_src, int32_t* near_nbr,
-                      int32_t* fc, int32_t* nc, cudaStream_t st) {
+                      float theta_sq, float theta, int gen, uint32_t cap, cudaStream_t st) {
   const int2* in = s.wf[gen & 1];
   int2* out = s.wf[(gen + 1) & 1];
   const uint32_t* cin = s.region_cnt[gen & 1];
   uint32_t* cout = s.region_cnt[(gen + 1) & 1];
   const uint32_t R = (uint32_t)region_capacity(cap);
-#define YGX_GEN(MAC)                                                                          \
-  k_walk_gen<kMode, MAC><<<kWalkGrid, kWalkThreads, 0, st>>>(                                 \
-      s.recs, ni, total_nodes, theta_sq, theta, in, out, cin, cout, R, s.sizes, gen, fc, nc,   \
-      s.far_pos,                                                                              \
-      s.near_pos, far_total, near_total, far_src, near_nbr, s.stats, s.status)
+#define YGX_GEN(MAC)                                                                        \
+  k_walk_gen<MAC><<<kWalkGrid, kWalkThreads, 0, st>>>(                                      \
+      s.recs, ni, total_nodes, theta_sq, theta, in, out, cin, cout, R, s.sizes, gen,        \
+      s.far_cnt, s.near_cnt, s.log, s.log_cnt, s.log_region, s.stats, s.status)
   if (mac == kMacBH) YGX_GEN(kMacBH);
   else if (mac == kMacDehnen) YGX_GEN(kMacDehnen);
   else YGX_GEN(kMacEngblom);
@@ -822,39 +879,43 @@ static int launch_gen(int mac, const TravScratch& s, int32_t ni, int32_t total_n
 
 extern "C" {
 
-size_t ygx_traverse_workspace_size(int64_t total, int64_t num_leaves, int64_t wf_capacity) {
+size_t ygx_traverse_workspace_size(int64_t total, int64_t num_leaves, int64_t wf_capacity,
+                                   int64_t log_capacity) {
   ygx::Arena a{nullptr, 0, 0};
-  ygx::carve_trav(a, total, num_leaves, wf_capacity);
+  ygx::carve_trav(a, total, num_leaves, wf_capacity, log_capacity);
   return a.used + 256;
 }
 
 static int trav_setup(ygx::TravScratch& s, void* ws, size_t ws_bytes, int64_t total, int64_t L,
-                      int64_t cap) {
-  if (ws_bytes < ygx_traverse_workspace_size(total, L, cap)) return YGX_ERR_ARG;
+                      int64_t cap, int64_t log_cap) {
+  if (cap < 4 || cap > (int64_t)UINT32_MAX || log_cap < 1) return YGX_ERR_ARG;
+  if (ws_bytes < ygx_traverse_workspace_size(total, L, cap, log_cap)) return YGX_ERR_ARG;
   ygx::Arena a{(char*)ws, 0, ws_bytes};
-  s = ygx::carve_trav(a, total, L, cap);
+  s = ygx::carve_trav(a, total, L, cap, log_cap);
   return YGX_OK;
 }
 
-// Count pass.  Builds the per-node walk records (center + MAC extent +
+// The walk.  Builds the per-node walk records (center + MAC extent +
 // children + leaf position), walks from (root, root) generation by
 // generation until the wavefront is empty (checked every 16 generations),
-// and copies to the host: stats_out[YGX_TSTAT_WORDS] (far/near totals and
-// maxima, decision counters, max wavefront, generations) and the status
-// flags.  leafpos32[node] is the near-row position of a leaf (-1 for
-// internal nodes).  Synchronizes the stream.
-int ygx_traverse_count(const float* center, const float* radius, const float* max_extent,
-                       const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
-                       int64_t total, int64_t num_internal, int mac, float theta,
-                       float dehnen_radius_scale, int root, int64_t wf_capacity,
-                       uint64_t* stats_out, uint32_t* flags_out, void* ws, size_t ws_bytes,
-                       cudaStream_t stream) {
-  if (total < 3 || total > INT32_MAX || num_internal < 1 || mac < 0 || mac > 2 || wf_capacity < 4 ||
-      wf_capacity > (int64_t)UINT32_MAX || !stats_out || !flags_out)
+// counting every far / near row entry and logging every accepted / near
+// pair, and copies to the host: stats_out[YGX_TSTAT_WORDS] (far/near totals
+// and maxima, decision counters, max wavefront, generations, and the
+// wavefront / log capacities that would have fit) and the status flags.
+// leafpos32[node] is the near-row position of a leaf (-1 for internal
+// nodes).  Synchronizes the stream.
+int ygx_traverse_walk(const float* center, const float* radius, const float* max_extent,
+                      const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
+                      int64_t total, int64_t num_internal, int mac, float theta,
+                      float dehnen_radius_scale, int root, int64_t wf_capacity,
+                      int64_t log_capacity, uint64_t* stats_out, uint32_t* flags_out, void* ws,
+                      size_t ws_bytes, cudaStream_t stream) {
+  if (total < 3 || total > INT32_MAX || num_internal < 1 || mac < 0 || mac > 2 ||
+      root < 0 || root >= total || !stats_out || !flags_out)
     return YGX_ERR_ARG;
   const int64_t L = total - num_internal;
   ygx::TravScratch s;
-  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity);
+  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity, log_capacity);
   if (rc) return rc;
   // theta^2 in fp32 (jnp.asarray(theta, float32) ** 2) and its sqrt.
   const float th = theta;
@@ -863,7 +924,9 @@ int ygx_traverse_count(const float* center, const float* radius, const float* ma
   if (cudaMemsetAsync(s.status, 0, (char*)(s.n_big + 64) - (char*)s.status, stream) != cudaSuccess)
     return YGX_ERR_CUDA;
   if (cudaMemsetAsync(s.far_cnt, 0, sizeof(int32_t) * total, stream) != cudaSuccess ||
-      cudaMemsetAsync(s.near_cnt, 0, sizeof(int32_t) * L, stream) != cudaSuccess)
+      cudaMemsetAsync(s.near_cnt, 0, sizeof(int32_t) * L, stream) != cudaSuccess ||
+      cudaMemsetAsync(s.log_cnt, 0, sizeof(unsigned long long) * ygx::kWalkGrid, stream) !=
+          cudaSuccess)
     return YGX_ERR_CUDA;
   ygx::k_node_recs<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
       center, radius, max_extent, left32, right32, leafpos32, total, mac, dehnen_radius_scale,
@@ -875,26 +938,27 @@ int ygx_traverse_count(const float* center, const float* radius, const float* ma
   const int chunk = 16;
   while (true) {
     for (int k = 0; k < chunk && gen < ygx::kMaxGens; ++k, ++gen) {
-      rc = ygx::launch_gen<ygx::kCount>(mac, s, (int32_t)num_internal, (int32_t)total, theta_sq, theta_r, gen,
-                                        (uint32_t)wf_capacity, 0ull, 0ull, nullptr, nullptr,
-                                        s.far_cnt, s.near_cnt, stream);
+      rc = ygx::launch_gen(mac, s, (int32_t)num_internal, (int32_t)total, theta_sq, theta_r, gen,
+                           (uint32_t)wf_capacity, stream);
       if (rc) return rc;
     }
     uint32_t probe = 0, flags = 0;
-    if (cudaMemcpyAsync(&probe, s.sizes + gen, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
-            cudaSuccess ||
+    if (cudaMemcpyAsync(&probe, s.sizes + gen, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                        stream) != cudaSuccess ||
         cudaMemcpyAsync(&flags, s.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
             cudaSuccess ||
         cudaStreamSynchronize(stream) != cudaSuccess)
       return YGX_ERR_CUDA;
-    if (probe == 0 || flags != 0) break;
+    // A wavefront overflow ends the walk at once; a log overflow does not
+    // (the walk goes on counting, so the log need it reports is exact).
+    if (probe == 0 || (flags & ~(uint32_t)ygx::kFlagLogOverflow) != 0) break;
     if (gen >= ygx::kMaxGens) {
       flags_out[0] = ygx::kFlagQueueOverflow;
       return YGX_ERR_QUEUE_OVERFLOW;
     }
   }
   ygx::k_count_stats<<<ygx::grid_for(total, 256, ygx::kNumSMs * 4), 256, 0, stream>>>(
-      s.far_cnt, total, s.near_cnt, L, s.sizes, gen, s.stats);
+      s.far_cnt, total, s.near_cnt, L, s.sizes, gen, s.log_cnt, s.stats);
   YGX_CHECK_LAUNCH();
   if (cudaMemcpyAsync(stats_out, s.stats, sizeof(uint64_t) * YGX_TSTAT_WORDS,
                       cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
@@ -905,31 +969,25 @@ int ygx_traverse_count(const float* center, const float* radius, const float* ma
   return YGX_OK;
 }
 
-// Fill pass (after a successful count pass on the same workspace).
-// Writes the level-major far layout and the near CSR: node_offsets
-// (total+1), far_counts (total), level_offsets (num_levels+1), near_offsets
-// (L+1), near_counts (L) in the index dtype, and the raw rows far_src32
-// (far total) / near_nbr32 (near total) in walk order.  `gens` is the
-// generation count reported by the count pass.  Does not synchronize.
-int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta, int root,
-                      int64_t wf_capacity, int gens, int64_t far_total, int64_t near_total,
-                      const int32_t* nbl32,
+// Fill (after a walk without overflow on the same workspace).  Writes the
+// level-major far layout and the near CSR: node_offsets (total+1),
+// far_counts (total), level_offsets (num_levels+1), near_offsets (L+1),
+// near_counts (L) in the index dtype, and the raw rows far_src32 (far
+// total) / near_nbr32 (near total) in log order.  Does not synchronize.
+int ygx_traverse_fill(int64_t total, int64_t num_internal, int64_t wf_capacity,
+                      int64_t log_capacity, int64_t far_total, int64_t near_total,
+                      const int32_t* nbl32, const int32_t* leafpos32,
                       const void* tree_level_offsets, int num_levels, int index_bits,
                       void* node_offsets, void* far_counts, void* level_offsets,
                       void* near_offsets, void* near_counts, int32_t* far_src32,
                       int32_t* near_nbr32, void* ws, size_t ws_bytes, cudaStream_t stream) {
-  if (total < 3 || total > INT32_MAX || num_internal < 1 || gens < 0 || gens > ygx::kMaxGens ||
+  if (total < 3 || total > INT32_MAX || num_internal < 1 || far_total < 0 || near_total < 0 ||
       (index_bits != 32 && index_bits != 64))
     return YGX_ERR_ARG;
   const int64_t L = total - num_internal;
   ygx::TravScratch s;
-  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity);
+  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity, log_capacity);
   if (rc) return rc;
-  const float th = theta;
-  const float theta_sq = th * th;
-  const float theta_r = sqrtf(theta_sq);
-  const unsigned long long far_total_u = (unsigned long long)far_total;
-  const unsigned long long near_total_u = (unsigned long long)near_total;
   ygx::k_gather_counts<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.far_cnt, nbl32, total,
                                                                       s.cnt_by_level);
   YGX_CHECK_LAUNCH();
@@ -945,19 +1003,14 @@ int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta,
                                                                      index_bits, near_offsets,
                                                                      near_counts);
   YGX_CHECK_LAUNCH();
-  if (cudaMemsetAsync(s.sizes, 0, sizeof(uint32_t) * (ygx::kMaxGens + 2), stream) != cudaSuccess)
-    return YGX_ERR_CUDA;
   ygx::k_init_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.far_off, total, s.far_pos,
                                                                      s.near_off, L, s.near_pos);
   YGX_CHECK_LAUNCH();
-  ygx::k_seed<<<1, 256, 0, stream>>>(s.wf[0], s.region_cnt[0], s.sizes, root);
+  ygx::k_log_scatter<<<ygx::kWalkGrid, 256, 0, stream>>>(
+      s.log, s.log_cnt, s.log_region, leafpos32, s.far_pos, s.near_pos,
+      (unsigned long long)far_total, (unsigned long long)near_total, far_src32, near_nbr32,
+      s.status);
   YGX_CHECK_LAUNCH();
-  for (int gen = 0; gen < gens; ++gen) {
-    rc = ygx::launch_gen<ygx::kFill>(mac, s, (int32_t)num_internal, (int32_t)total, theta_sq, theta_r, gen,
-                                     (uint32_t)wf_capacity, far_total_u, near_total_u, far_src32,
-                                     near_nbr32, nullptr, nullptr, stream);
-    if (rc) return rc;
-  }
   ygx::k_check_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
       s.far_off, s.far_cnt, s.far_pos, total, s.near_off, s.near_cnt, s.near_pos, L, s.status);
   YGX_CHECK_LAUNCH();
@@ -971,7 +1024,7 @@ int ygx_traverse_fill(int64_t total, int64_t num_internal, int mac, float theta,
 // neighbor_leaf_positions is non-null it receives the dense (L x max_nbr)
 // leaf-position table.  Does not synchronize.
 int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capacity,
-                          const int32_t* level32, const int32_t* leafpos32, int index_bits,
+                          int64_t log_capacity, const int32_t* level32, const int32_t* leafpos32, int index_bits,
                           int32_t* far_src32, int32_t* near_nbr32, void* far_sources,
                           void* far_targets, void* target_levels, void* neighbors,
                           void* neighbor_leaf_positions, int64_t max_nbr, void* ws,
@@ -979,7 +1032,7 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
   if (total < 3 || num_internal < 1 || (index_bits != 32 && index_bits != 64)) return YGX_ERR_ARG;
   const int64_t L = total - num_internal;
   ygx::TravScratch s;
-  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity);
+  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity, log_capacity);
   if (rc) return rc;
   const int grid_small = ygx::kNumSMs * 16;
   const size_t big_smem = sizeof(int32_t) * ygx::kBlockRowCap;

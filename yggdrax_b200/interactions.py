@@ -4,7 +4,7 @@ Mirrors ``build_interactions_and_neighbors`` (yggdrax/interactions.py:338-448,
 yggdrax/_interactions_impl.py:6031-6144) and its containers
 (``_interactions_impl.py:235-242, 416-424, 566-644``).  The walk, the row
 sizing and the level-major / CSR layouts run as sm_100a kernels
-(``ygx_traverse_count`` / ``_fill`` / ``_finalize``).
+(``ygx_traverse_walk`` / ``_fill`` / ``_finalize``).
 
 Output contract: the same pair sets and layouts as the reference; within
 every row the entries are in ascending order (the reference's within-row
@@ -204,6 +204,11 @@ def set_reference_limits(enabled: bool) -> None:
 
 _DENSE_BUDGET: Optional[int] = None
 LAST_WALK_STATS: dict = {}  # diagnostics of the most recent walk
+# Capacity hints per (mac, theta): wavefront and pair-log entries per tree
+# node that the last walk needed.  The next walk starts from them (with
+# head-room) so a repeated workload sizes its buffers right the first time;
+# a walk that overflows is re-run with the sizes it reports.
+_CAPACITY_HINTS: dict = {}
 _TIMING = os.environ.get("YGGDRAX_B200_TIMING", "0") == "1"  # per-pass CUDA-event times
 
 
@@ -315,7 +320,7 @@ class _WalkOut:
 
 def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_scale: float,
               wf_capacity: Optional[int] = None) -> _WalkOut:
-    """Count -> scan -> fill -> finalize on the GPU."""
+    """Walk (counts + pair log) -> scan -> fill (scatter) -> finalize on the GPU."""
     lib = L.lib()
     total = int(topology.parent.shape[0])
     ni = int(topology.left_child.shape[0])
@@ -343,34 +348,47 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     center = geometry.center.contiguous().float()
     radius = geometry.radius.contiguous().float()
     max_extent = geometry.max_extent.contiguous().float()
-    cap = int(wf_capacity) if wf_capacity else 32 * total + 65536
+    hint_wf, hint_log = _CAPACITY_HINTS.get((mac_type, float(theta)), (0.0, 0.0))
+    cap = int(wf_capacity) if wf_capacity else max(32 * total + 65536, int(1.25 * hint_wf * total))
+    log_cap = max(8 * total + 65536, int(1.1 * hint_log * total))
+    cap = min(cap, (1 << 32) - 1)
     mac = _MAC_CODES[mac_type]
     root = int(torch.argmin(d.parent32).item()) if bool(
         (d.tree_flags != 0).any().item()) else 0
     while True:
-        ws = L.workspace(lib.ygx_traverse_workspace_size(total, nl, cap), dev)
+        ws = L.workspace(lib.ygx_traverse_workspace_size(total, nl, cap, log_cap), dev)
         stats = np.zeros(L.TSTAT_WORDS, np.uint64)
         flags = np.zeros(1, np.uint32)
-        rc = lib.ygx_traverse_count(
+        rc = lib.ygx_traverse_walk(
             L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32), L.ptr(d.right32),
             L.ptr(leafpos32), total, ni, mac, float(theta), float(dehnen_radius_scale), root,
-            cap, stats.ctypes.data, flags.ctypes.data, L.ptr(ws), ws.numel(), st)
+            cap, log_cap, stats.ctypes.data, flags.ctypes.data, L.ptr(ws), ws.numel(), st)
         f = int(flags[0])
-        if f & L.FLAG_QUEUE_OVERFLOW and cap < (1 << 32) - 1:
-            cap = min((1 << 32) - 1, cap * 4)
+        if f & (L.FLAG_QUEUE_OVERFLOW | L.FLAG_LOG_OVERFLOW) and rc == 0:
+            if f & L.FLAG_QUEUE_OVERFLOW:
+                if cap >= (1 << 32) - 1:
+                    raise L.YgxError("traversal wavefront exceeds 2^32 pairs")
+                # the needs a truncated walk reports are lower bounds only
+                cap = min((1 << 32) - 1, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
+                log_cap = max(log_cap, int(stats[L.TSTAT["log_need"]]))
+            else:
+                log_cap = int(stats[L.TSTAT["log_need"]])
             del ws
             continue
-        L.check(rc, "ygx_traverse_count")
+        L.check(rc, "ygx_traverse_walk")
         if f & L.FLAG_BAD_INPUT:
             raise ValueError("MAC extents must be positive (geometry has zero or NaN extents)")
         if f:
-            raise L.YgxError(f"traversal count pass reported flags {f:#x}")
+            raise L.YgxError(f"traversal walk reported flags {f:#x}")
         break
+    if not wf_capacity:
+        _CAPACITY_HINTS[(mac_type, float(theta))] = (
+            int(stats[L.TSTAT["wf_need"]]) / total, int(stats[L.TSTAT["log_need"]]) / total)
     if timing:
         evs[1].record()
     s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
     LAST_WALK_STATS.clear()
-    LAST_WALK_STATS.update(s, wf_capacity=cap)
+    LAST_WALK_STATS.update(s, wf_capacity=cap, log_capacity=log_cap)
     P, Q = s["far_total"], s["near_total"]
     node_offsets = torch.empty(total + 1, dtype=idt, device=dev)
     far_counts = torch.empty(total, dtype=idt, device=dev)
@@ -380,7 +398,7 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     far_src32 = torch.empty(max(P, 1), dtype=torch.int32, device=dev)
     near_nbr32 = torch.empty(max(Q, 1), dtype=torch.int32, device=dev)
     L.check(lib.ygx_traverse_fill(
-        total, ni, mac, float(theta), root, cap, s["gens"], P, Q, L.ptr(d.nbl32),
+        total, ni, cap, log_cap, P, Q, L.ptr(d.nbl32), L.ptr(leafpos32),
         L.ptr(topology.level_offsets), num_levels, ib, L.ptr(node_offsets), L.ptr(far_counts),
         L.ptr(level_offsets), L.ptr(near_offsets), L.ptr(near_counts), L.ptr(far_src32),
         L.ptr(near_nbr32), L.ptr(ws), ws.numel(), st), "ygx_traverse_fill")
@@ -400,14 +418,14 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
         max_nbr = 0
     nlp = torch.empty((nl, max_nbr), dtype=idt, device=dev)
     L.check(lib.ygx_traverse_finalize(
-        total, ni, cap, L.ptr(d.level32), L.ptr(leafpos32), ib, L.ptr(far_src32),
+        total, ni, cap, log_cap, L.ptr(d.level32), L.ptr(leafpos32), ib, L.ptr(far_src32),
         L.ptr(near_nbr32), L.ptr(sources), L.ptr(targets), L.ptr(target_levels),
         L.ptr(neighbors), L.ptr(nlp) if max_nbr > 0 else None, max_nbr, L.ptr(ws), ws.numel(),
         st), "ygx_traverse_finalize")
     if timing:
         evs[3].record()
         torch.cuda.synchronize(dev)
-        LAST_WALK_STATS.update(count_ms=evs[0].elapsed_time(evs[1]),
+        LAST_WALK_STATS.update(walk_ms=evs[0].elapsed_time(evs[1]),
                                fill_ms=evs[1].elapsed_time(evs[2]),
                                finalize_ms=evs[2].elapsed_time(evs[3]))
     f = L.read_status(ws)
