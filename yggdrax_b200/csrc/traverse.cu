@@ -644,7 +644,10 @@ __global__ void k_rows_classify(int64_t rows, const int32_t* __restrict__ row_cn
     const int n = row_cnt[r];
     if (n == 0) continue;
     if (n > kWarpRowCap) {
-      big_rows[atomicAdd(n_big, 1u)] = (int32_t)r;
+      // rows longer than kBlockRowCap from the front, the others from the
+      // back: the long-row kernel takes the longest first
+      if (n > kBlockRowCap) big_rows[atomicAdd(&n_big[0], 1u)] = (int32_t)r;
+      else big_rows[list_stride - 1 - atomicAdd(&n_big[8], 1u)] = (int32_t)r;
       continue;
     }
     int c = 0;
@@ -678,91 +681,244 @@ __global__ void __launch_bounds__(256, R >= 32 ? 2 : (R >= 16 ? 3 : 4))
   }
 }
 
-// Long rows: one CTA per row.  Up to kBlockRowCap entries sort in shared
-// memory.  Longer rows hold distinct node ids (a canonical pair is visited
-// once), so they are ordered by setting one bit per entry in a bitmap over
-// all node ids and reading the bitmap back in order; if the bit count shows
-// duplicates the row is sorted in place in global memory instead.
+// Position of the r-th (0-based) set bit of w (r < popc(w)), by halving.
+__device__ __forceinline__ int select_bit(uint32_t w, int r) {
+  int base = 0;
+  int c = __popc(w & 0xffffu);
+  if (r >= c) { r -= c; w >>= 16; base += 16; }
+  c = __popc(w & 0xffu);
+  if (r >= c) { r -= c; w >>= 8; base += 8; }
+  c = __popc(w & 0xfu);
+  if (r >= c) { r -= c; w >>= 4; base += 4; }
+  c = __popc(w & 0x3u);
+  if (r >= c) { r -= c; w >>= 2; base += 2; }
+  return base + (r >= (int)(w & 1u) ? 1 : 0);
+}
+
+constexpr int kSumWords = 1024;  // summary bits: bitmaps up to 1024 * 32 words (2^20 values)
+
+// Exclusive prefix over the block (one value per thread, kBigThreads
+// threads); returns the prefix and leaves the total in *total.
+__device__ __forceinline__ int64_t block_excl_scan(int64_t v, int64_t* s_tmp, int64_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t u = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += u;
+  }
+  if (lane == 31) s_tmp[warp] = incl;
+  __syncthreads();
+  int64_t wpre = 0, tot = 0;
+  for (int w = 0; w < (kBigThreads >> 5); ++w) {
+    const int64_t t = s_tmp[w];
+    wpre += w < warp ? t : 0;
+    tot += t;
+  }
+  *total = tot;
+  __syncthreads();  // s_tmp may be reused right after
+  return wpre + incl - v;
+}
+
+// Long rows (> kWarpRowCap entries): one CTA per row, rows taken from a
+// work counter longest first.  A row holds distinct node ids (a canonical
+// pair is visited once), so it is ordered through a two-level bitmap over
+// its value range [min, max]: one bit per value (in shared memory when the
+// range fits kBlockRowCap words, else in this CTA's global bitmap) and one
+// summary bit per non-empty bitmap word.  The summary gives the non-empty
+// words in order (written over the row's raw entries, which are no longer
+// needed), and warps then walk chunks of 32 such words, finding the q-th
+// set bit for q = lane, lane + 32, ... so the output writes are coalesced.
+// The cost is O(n + range / 1024) per row, and only the words that were set
+// are cleared again.  Repeated entries (seen when a bit was already set) or
+// ranges beyond the summary send the row to a bitonic network instead (in
+// shared memory up to kBlockRowCap entries, else in place in global memory).
 __global__ void __launch_bounds__(kBigThreads, 3)
-    k_rows_big(const int32_t* __restrict__ big_rows, const uint32_t* __restrict__ n_big,
-               const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
-               const int32_t* __restrict__ row_level, int32_t* __restrict__ raw, int index_bits,
-               void* vals_out, void* tgt_out, void* lvl_out, uint32_t* __restrict__ bitmaps,
-               int64_t universe) {
-  extern __shared__ int32_t s_a[];  // kBlockRowCap entries (dynamic shared memory)
-  __shared__ int64_t s_warp[32];
-  __shared__ int64_t s_total;
-  const uint32_t nb = *n_big;
-  const int64_t words = (universe + 31) / 32;
-  uint32_t* bm = bitmaps + (int64_t)blockIdx.x * words;
+    k_rows_big(const int32_t* __restrict__ big_rows, uint32_t* __restrict__ n_big,
+               int64_t list_cap, const int64_t* __restrict__ row_off,
+               const int32_t* __restrict__ row_cnt, const int32_t* __restrict__ row_level,
+               int32_t* __restrict__ raw, int index_bits, void* vals_out, void* tgt_out,
+               void* lvl_out, uint32_t* __restrict__ bitmaps, int64_t universe) {
+  extern __shared__ uint32_t s_dyn[];  // kBlockRowCap words: bitmap, or a row to sort
+  __shared__ uint32_t s_sum[kSumWords];
+  __shared__ int32_t s_cc[kSumWords];  // per-chunk counts, then bases (< n < 2^31)
+  __shared__ int64_t s_tmp[32];
+  __shared__ int32_t s_min[32], s_max[32];
+  __shared__ uint32_t s_item;
+  __shared__ int s_dup;
+  const uint32_t n_long = n_big[0], n_mid = n_big[8];
+  const int64_t gwords = (universe + 31) / 32;
+  uint32_t* gbm = bitmaps + (int64_t)blockIdx.x * gwords;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-  for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
-    const int32_t r = big_rows[b];
+  const int nwarps = nt >> 5;
+  for (int w = tid; w < kBlockRowCap; w += nt) s_dyn[w] = 0u;
+  for (int w = tid; w < kSumWords; w += nt) s_sum[w] = 0u;
+  if (gwords > kBlockRowCap)
+    for (int64_t w = tid; w < gwords; w += nt) gbm[w] = 0u;
+  __syncthreads();
+  while (true) {
+    if (tid == 0) {
+      s_item = atomicAdd(&n_big[9], 1u);
+      s_dup = 0;
+    }
+    __syncthreads();
+    const uint32_t b = s_item;
+    if (b >= n_long + n_mid) break;
+    const int32_t r = b < n_long ? big_rows[b] : big_rows[list_cap - 1 - (b - n_long)];
     const int64_t off = row_off[r];
     const int64_t n = row_cnt[r];
     const int32_t lvl = row_level ? row_level[r] : 0;
-    if (n <= kBlockRowCap) {
-      for (int64_t k = tid; k < n; k += nt) s_a[k] = raw[off + k];
-      __syncthreads();
-      mirrored_bitonic<true>(s_a, n, tid, nt);
-      emit_row(s_a, n, off, index_bits, vals_out, tgt_out, lvl_out, r, lvl, tid, nt);
-      __syncthreads();
-      continue;
-    }
-    for (int64_t w = tid; w < words; w += nt) bm[w] = 0u;
-    __syncthreads();
+    int32_t vmin = INT32_MAX, vmax = INT32_MIN;
     for (int64_t k = tid; k < n; k += nt) {
       const int32_t v = raw[off + k];
-      atomicOr(&bm[v >> 5], 1u << (v & 31));
+      vmin = v < vmin ? v : vmin;
+      vmax = v > vmax ? v : vmax;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      vmin = min(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+      vmax = max(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    }
+    if (lane == 0) {
+      s_min[warp] = vmin;
+      s_max[warp] = vmax;
     }
     __syncthreads();
-    // Thread t owns words [t*chunk, (t+1)*chunk): count, scan, emit.
-    const int64_t chunk = (words + nt - 1) / nt;
-    const int64_t w0 = (int64_t)tid * chunk;
-    const int64_t w1 = w0 + chunk < words ? w0 + chunk : words;
-    int64_t mine = 0;
-    for (int64_t w = w0; w < w1; ++w) mine += __popc(__ldcg(bm + w));
-    int64_t incl = mine;
-    for (int o = 1; o < 32; o <<= 1) {
-      int64_t v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += v;
+    vmin = s_min[0];
+    vmax = s_max[0];
+    for (int w = 1; w < nwarps; ++w) {
+      vmin = min(vmin, s_min[w]);
+      vmax = max(vmax, s_max[w]);
     }
-    if (lane == 31) s_warp[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-      int64_t wv = lane < (nt >> 5) ? s_warp[lane] : 0;
-      int64_t wi = wv;
-      for (int o = 1; o < 32; o <<= 1) {
-        int64_t v = __shfl_up_sync(0xffffffffu, wi, o);
-        if (lane >= o) wi += v;
+    const int64_t words = ((int64_t)vmax - vmin + 1 + 31) >> 5;
+    const int64_t swords = (words + 31) >> 5;
+    bool sorted = false;
+    if (swords <= kSumWords) {
+      uint32_t* bm = words <= kBlockRowCap ? s_dyn : gbm;
+      bool dup = false;
+      for (int64_t k = tid; k < n; k += nt) {
+        const uint32_t v = (uint32_t)(raw[off + k] - vmin);
+        const uint32_t bit = 1u << (v & 31);
+        if (atomicOr(&bm[v >> 5], bit) & bit) dup = true;
+        atomicOr(&s_sum[v >> 10], 1u << ((v >> 5) & 31));
       }
-      if (lane < (nt >> 5)) s_warp[lane] = wi - wv;
-      if (lane == 31) s_total = wi;
-    }
-    __syncthreads();
-    const bool distinct = s_total == n;
-    if (distinct) {
-      int64_t pos = off + s_warp[warp] + incl - mine;
-      for (int64_t w = w0; w < w1; ++w) {
-        uint32_t bits = __ldcg(bm + w);
-        while (bits) {
-          const int bit = __ffs(bits) - 1;
-          bits &= bits - 1;
-          const int64_t v = w * 32 + bit;
-          store_idx(vals_out, index_bits, pos, v);
-          if (tgt_out) {
-            store_idx(tgt_out, index_bits, pos, r);
-            store_idx(lvl_out, index_bits, pos, lvl);
-          }
-          ++pos;
+      if (dup) s_dup = 1;
+      __syncthreads();
+      if (s_dup) {
+        // undo the bits; the row goes to the bitonic network
+        for (int64_t k = tid; k < n; k += nt) {
+          const uint32_t v = (uint32_t)(raw[off + k] - vmin);
+          bm[v >> 5] = 0u;
         }
+        for (int64_t w = tid; w < swords; w += nt) s_sum[w] = 0u;
+        __syncthreads();
+      } else {
+        // Non-empty words in ascending order -> raw[off, off + m).
+        constexpr int kSumPer = kSumWords / kBigThreads;
+        int64_t c = 0;
+#pragma unroll
+        for (int k = 0; k < kSumPer; ++k) {
+          const int64_t sw = (int64_t)tid * kSumPer + k;
+          c += sw < swords ? __popc(s_sum[sw]) : 0;
+        }
+        int64_t m;
+        int64_t base = block_excl_scan(c, s_tmp, &m);
+#pragma unroll
+        for (int k = 0; k < kSumPer; ++k) {
+          const int64_t sw = (int64_t)tid * kSumPer + k;
+          uint32_t bits = sw < swords ? s_sum[sw] : 0u;
+          while (bits) {
+            const int bit = __ffs(bits) - 1;
+            bits &= bits - 1;
+            raw[off + base++] = (int32_t)(sw * 32 + bit);
+          }
+        }
+        __syncthreads();
+        // bits per chunk of 32 listed words
+        const int64_t nch = (m + 31) >> 5;
+        for (int64_t ch = warp; ch < nch; ch += nwarps) {
+          const int64_t j = ch * 32 + lane;
+          int cnt = j < m ? __popc(bm[raw[off + j]]) : 0;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+          if (lane == 0) s_cc[ch] = cnt;
+        }
+        __syncthreads();
+        {
+          int64_t cv[kSumPer];
+          int64_t mine = 0;
+#pragma unroll
+          for (int k = 0; k < kSumPer; ++k) {
+            const int64_t ch = (int64_t)tid * kSumPer + k;
+            cv[k] = ch < nch ? s_cc[ch] : 0;
+            mine += cv[k];
+          }
+          int64_t tot;
+          int64_t run = block_excl_scan(mine, s_tmp, &tot);
+#pragma unroll
+          for (int k = 0; k < kSumPer; ++k) {
+            const int64_t ch = (int64_t)tid * kSumPer + k;
+            if (ch < nch) s_cc[ch] = (int32_t)run;
+            run += cv[k];
+          }
+        }
+        __syncthreads();
+        for (int64_t ch = warp; ch < nch; ch += nwarps) {
+          const int64_t j = ch * 32 + lane;
+          const int32_t wi = j < m ? raw[off + j] : 0;
+          const uint32_t word = j < m ? bm[wi] : 0u;
+          const int c1 = __popc(word);
+          int incl = c1;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+          }
+          const int T = __shfl_sync(0xffffffffu, incl, 31);
+          const int64_t pos = off + s_cc[ch];
+          for (int q0 = 0; q0 < T; q0 += 32) {
+            const int q = q0 + lane;
+            // lo = listed words whose inclusive count is <= q (lo <= 31)
+            int lo = 0;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+              const int v = __shfl_sync(0xffffffffu, incl, lo + step - 1);
+              if (v <= q) lo += step;
+            }
+            const uint32_t wsel = __shfl_sync(0xffffffffu, word, lo);
+            const int ex = __shfl_sync(0xffffffffu, incl - c1, lo);
+            const int32_t wsi = __shfl_sync(0xffffffffu, wi, lo);
+            if (q < T) {
+              const int32_t v = vmin + wsi * 32 + select_bit(wsel, q - ex);
+              store_idx(vals_out, index_bits, pos + q, v);
+              if (tgt_out) {
+                store_idx(tgt_out, index_bits, pos + q, r);
+                store_idx(lvl_out, index_bits, pos + q, lvl);
+              }
+            }
+          }
+        }
+        __syncthreads();
+        for (int64_t j = tid; j < m; j += nt) bm[raw[off + j]] = 0u;
+        for (int64_t w = tid; w < swords; w += nt) s_sum[w] = 0u;
+        __syncthreads();
+        sorted = true;
       }
     }
-    __syncthreads();
-    if (!distinct) {
-      int32_t* a = raw + off;  // repeated entries: sort in place in global memory
-      mirrored_bitonic<true>(a, n, tid, nt);
-      emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, r, lvl, tid, nt);
+    if (!sorted) {
+      if (n <= kBlockRowCap) {
+        int32_t* a = reinterpret_cast<int32_t*>(s_dyn);
+        for (int64_t k = tid; k < n; k += nt) a[k] = raw[off + k];
+        __syncthreads();
+        mirrored_bitonic<true>(a, n, tid, nt);
+        emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, r, lvl, tid, nt);
+        __syncthreads();
+        for (int64_t k = tid; k < n; k += nt) s_dyn[k] = 0u;  // bitmap stays zero
+      } else {
+        int32_t* a = raw + off;
+        mirrored_bitonic<true>(a, n, tid, nt);
+        emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, r, lvl, tid, nt);
+      }
     }
     __syncthreads();
   }
@@ -832,7 +988,8 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap, i
   s.status = a.take<uint32_t>(64);
   s.stats = a.take<unsigned long long>(kStatWords);
   s.sizes = a.take<uint32_t>(kMaxGens + 2);
-  s.n_big = a.take<uint32_t>(64);  // [0] long rows, [1..6] class counts
+  // [0] rows > kBlockRowCap, [1..6] class counts, [8] other long rows, [9] work counter
+  s.n_big = a.take<uint32_t>(64);
   s.recs = a.take<NodeRec>(total);
   s.far_cnt = a.take<int32_t>(total);
   s.near_cnt = a.take<int32_t>(L);
@@ -1044,7 +1201,7 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
   const int64_t stride = total > L ? total : L;
   auto rows_pass = [&](int64_t rows, const int64_t* off, const int32_t* cnt, const int32_t* lvl,
                        int32_t* raw, void* vals, void* tgts, void* lvls) -> int {
-    if (cudaMemsetAsync(s.n_big, 0, 8 * sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
+    if (cudaMemsetAsync(s.n_big, 0, 16 * sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
     ygx::k_rows_classify<<<ygx::grid_for(rows, 256), 256, 0, stream>>>(
         rows, cnt, s.class_rows, stride, s.n_big + 1, s.big_rows, s.n_big);
     YGX_CHECK_LAUNCH();
@@ -1056,7 +1213,8 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
     YGX_ROWS(0, 1) YGX_ROWS(1, 2) YGX_ROWS(2, 4) YGX_ROWS(3, 8) YGX_ROWS(4, 16) YGX_ROWS(5, 32)
 #undef YGX_ROWS
     ygx::k_rows_big<<<ygx::kBigGrid, ygx::kBigThreads, big_smem, stream>>>(
-        s.big_rows, s.n_big, off, cnt, lvl, raw, index_bits, vals, tgts, lvls, s.bitmaps, total);
+        s.big_rows, s.n_big, stride, off, cnt, lvl, raw, index_bits, vals, tgts, lvls, s.bitmaps,
+        total);
     YGX_CHECK_LAUNCH();
     return YGX_OK;
   };
