@@ -14,7 +14,8 @@ from typing import Optional
 import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libygx.so")
+# YGGDRAX_B200_LIBRARY names another build of the same library (same ABI).
+LIB_PATH = os.environ.get("YGGDRAX_B200_LIBRARY") or os.path.join(_HERE, "libygx.so")
 
 YGX_OK = 0
 ERROR_NAMES = {

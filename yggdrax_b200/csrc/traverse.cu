@@ -12,7 +12,7 @@
 //
 // Each BFS generation is one launch over the current wavefront.  One walk
 // does all the pair work: it counts every far / near row entry (per-node
-// counters, one atomic per distinct node per warp via match-any) and logs
+// counters) and logs
 // every accepted or near pair once, as (lo, hi | near-bit), in the CTA's own
 // region of a pair log.  A scan of the counts gives the row offsets; a
 // scatter pass reads the log back coalesced and writes each pair into both
@@ -72,14 +72,6 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
-// Adds 1 to cnt[key] for every lane with pred, one atomic per distinct key.
-__device__ __forceinline__ void agg_count(int32_t* cnt, int key, bool pred) {
-  unsigned m = __ballot_sync(0xffffffffu, pred);
-  if (pred) {
-    unsigned peers = __match_any_sync(m, key);
-    if ((peers & lanemask_lt()) == 0) atomicAdd(&cnt[key], __popc(peers));
-  }
-}
 // Returns a unique absolute position pos[key]++ for every lane with pred,
 // one atomic per distinct key in the warp.
 __device__ __forceinline__ unsigned long long agg_pos(unsigned long long* pos, int key,
@@ -228,14 +220,19 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
       nearp = !acc && diff && t >= ni && sv >= ni;
       refine = !acc && !nearp;
     }
-    n_acc += __popc(__ballot_sync(0xffffffffu, acc));
-    n_near += __popc(__ballot_sync(0xffffffffu, nearp));
-    n_ref += __popc(__ballot_sync(0xffffffffu, refine));
-
-    agg_count(far_cnt, t, acc);
-    agg_count(far_cnt, sv, acc);
-    agg_count(near_cnt, A.k.z, nearp);
-    agg_count(near_cnt, B.k.z, nearp);
+    n_acc += acc;
+    n_near += nearp;
+    n_ref += refine;
+    // Row counts: plain fire-and-forget atomics (aggregating equal keys in
+    // the warp with match-any first measured slower here).
+    if (acc) {
+      atomicAdd(&far_cnt[t], 1);
+      atomicAdd(&far_cnt[sv], 1);
+    }
+    if (nearp) {
+      atomicAdd(&near_cnt[A.k.z], 1);
+      atomicAdd(&near_cnt[B.k.z], 1);
+    }
 
     // Children of a refined pair (_interactions_impl.py:1262-1310).
     int nc = 0;
@@ -323,6 +320,11 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
     if (c) atomicAdd(&sizes[gen + 1], c);
     log_cnt[blockIdx.x] = log_base;
     atomicMax(&stats[kStatWfNeed], cta_base);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    n_acc += __shfl_xor_sync(0xffffffffu, n_acc, o);
+    n_near += __shfl_xor_sync(0xffffffffu, n_near, o);
+    n_ref += __shfl_xor_sync(0xffffffffu, n_ref, o);
   }
   if (lane == 0) {
     if (n_acc) atomicAdd(&stats[kStatAccept], n_acc);
