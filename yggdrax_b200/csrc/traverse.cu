@@ -93,6 +93,8 @@ __device__ __forceinline__ unsigned long long agg_pos(unsigned long long* pos, i
 constexpr int kWalkThreads = 256;
 constexpr int kWalkBlocksPerSM = 6;
 constexpr int kWalkGrid = kNumSMs * kWalkBlocksPerSM;  // fixed across generations
+constexpr int kCoarse = 4096;  // coarse index buckets of a walk generation
+static_assert(kWalkGrid < 65536, "coarse index holds region ids as uint16");
 
 // One BFS generation.  The wavefront of generation g is split into
 // kWalkGrid regions, one per CTA of generation g-1, each holding cnt_in[r]
@@ -117,6 +119,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
                unsigned long long* __restrict__ stats, uint32_t* __restrict__ status) {
   constexpr int kWarps = kWalkThreads / 32;
   __shared__ uint32_t s_prefix[kWalkGrid + 1];
+  __shared__ uint16_t s_coarse[kCoarse];
   __shared__ uint32_t s_wsum[kWarps];
   __shared__ uint32_t s_wt[2][kWarps];
   const int G = gridDim.x;
@@ -157,32 +160,41 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
     if (tid == 0) cnt_out[blockIdx.x] = 0;
     return;
   }
+  // Coarse index: s_coarse[j] = region holding index j << shift (buckets of
+  // 2^shift indices, at most kCoarse of them), so a lookup starts at most a
+  // bucket's worth of regions before its target.
+  int shift = 0;
+  while (((total_in - 1) >> shift) >= (uint32_t)kCoarse) ++shift;
+  for (int r = tid; r < G; r += kWalkThreads) {
+    const uint32_t mask = (1u << shift) - 1;
+    const uint32_t j0 = (uint32_t)(((uint64_t)s_prefix[r] + mask) >> shift);
+    const uint32_t j1 = (uint32_t)(((uint64_t)s_prefix[r + 1] + mask) >> shift);
+    for (uint32_t j = j0; j < j1; ++j) s_coarse[j] = (uint16_t)r;
+  }
+  __syncthreads();
   int2* my_out = wf_out + (size_t)blockIdx.x * R;
   unsigned long long n_acc = 0, n_near = 0, n_ref = 0;
   unsigned long long cta_base = 0;  // block-uniform: pairs appended so far
   unsigned long long log_base = log_cnt[blockIdx.x];  // block-uniform
+  const uint32_t nchunks = (total_in + 31) >> 5;
+  const uint32_t cstride = (uint32_t)kWarps * G;
   int buf = 0;
-  for (int64_t k = 0;; ++k, buf ^= 1) {
-    const int64_t chunk0 = k * kWarps * G + blockIdx.x;  // warp 0's chunk
-    if (chunk0 * 32 >= (int64_t)total_in) break;         // block-uniform
-    const int64_t wbase = (chunk0 + (int64_t)warp * G) * 32;
-    const int64_t i = wbase + lane;
-    const bool valid = i < (int64_t)total_in;
+  for (uint32_t chunk0 = blockIdx.x; chunk0 < nchunks; chunk0 += cstride, buf ^= 1) {
+    // chunk0 is warp 0's chunk (block-uniform loop); this warp takes chunk
+    const uint32_t chunk = chunk0 + warp * G;
+    const bool wvalid = chunk < nchunks;
+    const uint32_t wbase = chunk << 5;
+    const uint32_t i = wbase + lane;
+    const bool valid = wvalid && i < total_in;
     int t = 0, sv = 0;
-    if (wbase < (int64_t)total_in) {
-      // Region of the warp's first index (last r with prefix[r] <= wbase),
-      // then each lane steps past the regions its own index has left.
-      int r = 0, hi = G;
-      while (hi - r > 1) {
-        const int mid = (r + hi) >> 1;
-        if (s_prefix[mid] <= (uint32_t)wbase) r = mid; else hi = mid;
-      }
-      if (valid) {
-        while (r + 1 < G && s_prefix[r + 1] <= (uint32_t)i) ++r;
-        const int2 p = wf_in[(size_t)r * R + ((uint32_t)i - s_prefix[r])];
-        t = p.x;
-        sv = p.y;
-      }
+    if (valid) {
+      // Region of i: from the coarse index of the warp's first index, step
+      // past the regions that end at or before i.
+      int r = s_coarse[wbase >> shift];
+      while (r + 1 < G && s_prefix[r + 1] <= i) ++r;
+      const int2 p = wf_in[(size_t)r * R + (i - s_prefix[r])];
+      t = p.x;
+      sv = p.y;
     }
     const bool in_range = (unsigned)t < (unsigned)total_nodes &&
                           (unsigned)sv < (unsigned)total_nodes;
@@ -1047,7 +1059,7 @@ size_t ygx_traverse_workspace_size(int64_t total, int64_t num_leaves, int64_t wf
 
 static int trav_setup(ygx::TravScratch& s, void* ws, size_t ws_bytes, int64_t total, int64_t L,
                       int64_t cap, int64_t log_cap) {
-  if (cap < 4 || cap > (int64_t)UINT32_MAX || log_cap < 1) return YGX_ERR_ARG;
+  if (cap < 4 || cap > (int64_t)UINT32_MAX - 4096 || log_cap < 1) return YGX_ERR_ARG;
   if (ws_bytes < ygx_traverse_workspace_size(total, L, cap, log_cap)) return YGX_ERR_ARG;
   ygx::Arena a{(char*)ws, 0, ws_bytes};
   s = ygx::carve_trav(a, total, L, cap, log_cap);
