@@ -39,6 +39,9 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 N_DEFAULT = 16_777_216
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_onesweep launch
+# (ncu, keys = Morton codes of the Plummer input), by key count.
+SORT_PASS_DRAM_BYTES: dict = {16_777_216: 361_430_000}
 LEAF = 32
 THETA = 0.6
 MAC = "dehnen"
@@ -77,7 +80,14 @@ class ClockSampler:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
-        time.sleep(0.3)
+        # nvidia-smi's start-up (driver / NVML initialisation) must not overlap
+        # the timed region: wait for its first sample line.
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < 10.0:
+            if os.path.getsize(self.path) > 0 or self.proc.poll() is not None:
+                break
+            time.sleep(0.05)
+        time.sleep(0.1)
         return self
 
     def __exit__(self, *a):
@@ -187,6 +197,52 @@ def run_reference(args):
     return 0
 
 
+def sort_roofline(codes, dev, reps: int) -> dict:
+    """The build's HBM-bound kernel: the onesweep LSD sort of the Morton codes
+    (key u64 + value u32, 8-bit digits over 63 bits = 8 passes), timed with
+    CUDA events on its own stream, L2 flushed (256 MB write) before every
+    sort.  Algorithmic bytes per pass: read key + value, write key + value
+    (24 B per key)."""
+    import torch
+
+    from yggdrax_b200 import _lib as L
+
+    lib = L.lib()
+    n = int(codes.numel())
+    kout = torch.empty_like(codes)
+    vout = torch.empty(n, dtype=torch.int32, device=dev)
+    wsb = L.workspace(lib.ygx_sort_pairs_workspace_size(n), dev)
+    st = L.stream_handle(dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def sort_once():
+        L.check(lib.ygx_sort_pairs(L.ptr(codes), None, n, 0, 63, L.ptr(kout), L.ptr(vout),
+                                   L.ptr(wsb), wsb.numel(), st), "ygx_sort_pairs")
+
+    for _ in range(3):
+        sort_once()
+    sort_ms = []
+    for _ in range(reps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sort_once()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        sort_ms.append(a.elapsed_time(b))
+    passes = 8
+    sort_s = float(np.median(sort_ms)) / 1e3
+    bytes_per_pass = 24.0 * n
+    achieved = bytes_per_pass / (sort_s / passes) / 1e9
+    peak, peak_kind = _peaks()
+    return {"kernel": "k_onesweep (8 passes, 8-bit digits, key u64 + value u32)",
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": SORT_PASS_DRAM_BYTES.get(n), "algorithmic_bytes_per_launch": bytes_per_pass,
+            "launch_ms_avg": sort_s / passes * 1e3, "n_keys": n}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -197,6 +253,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--breakdown", action="store_true")
+    ap.add_argument("--roofline-only", action="store_true",
+                    help="time only the sort roofline leg (for profiling it)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -226,6 +284,12 @@ def main():
 
     n = args.n
     pos_np, mass_np = inputs.plummer(n, 4)
+    if args.roofline_only:
+        P = torch.from_numpy(pos_np).to(dev)
+        r = sort_roofline(yb.morton_encode(P, yb.infer_bounds(P)), dev, max(3, args.steps))
+        if rank == 0:
+            print(json.dumps({"roofline": r}), flush=True)
+        return 0
     pos_h = torch.from_numpy(pos_np).pin_memory()
     mass_h = torch.from_numpy(mass_np).pin_memory()
     pos_d = pos_h.to(dev)
@@ -284,40 +348,8 @@ def main():
     h2d = pos_h.numel() * 4 + mass_h.numel() * 4
     del inter, nbrs
 
-    # -- roofline of the dominant kernel family: the onesweep sort passes -------
-    codes = yb.morton_encode(pos_d, yb.infer_bounds(pos_d))
-    kout = torch.empty_like(codes)
-    vout = torch.empty(n, dtype=torch.int32, device=dev)
-    wsb = L.workspace(lib.ygx_sort_pairs_workspace_size(n), dev)
-    st = L.stream_handle(dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-
-    def sort_once():
-        L.check(lib.ygx_sort_pairs(L.ptr(codes), None, n, 0, 63, L.ptr(kout), L.ptr(vout),
-                                   L.ptr(wsb), wsb.numel(), st), "ygx_sort_pairs")
-
-    for _ in range(3):
-        sort_once()
-    sort_ms = []
-    for _ in range(max(3, args.steps)):
-        flush.zero_()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        sort_once()
-        b.record()
-        torch.cuda.synchronize(dev)
-        sort_ms.append(a.elapsed_time(b))
-    passes = 8
-    sort_s = float(np.median(sort_ms)) / 1e3
-    # algorithmic bytes per onesweep pass: read key+value, write key+value
-    bytes_per_pass = 24.0 * n
-    achieved = bytes_per_pass / (sort_s / passes) / 1e9
-    peak, peak_kind = _peaks()
-    roofline = {"kernel": "k_onesweep (8 passes, 8-bit digits, key u64 + value u32)",
-                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                "algorithmic_bytes_per_launch": bytes_per_pass,
-                "launch_ms_avg": sort_s / passes * 1e3}
+    roofline = sort_roofline(yb.morton_encode(pos_d, yb.infer_bounds(pos_d)), dev,
+                             max(3, args.steps))
 
     breakdown = None
     if args.breakdown:

@@ -1,9 +1,10 @@
 // Onesweep stable LSD radix sort (Adinets & Merrill 2022 style) for
-// sm_100a.  Each pass is one kernel: a CTA takes the next tile ticket, ranks
-// its 4096 keys stably with warp match-any multisplit, publishes its digit
-// counts, resolves its global digit offsets by decoupled look-back over the
-// preceding tiles (bounded spin), then scatters through shared memory so
-// global writes are contiguous within each digit run.
+// sm_100a.  Each pass is one kernel: a CTA takes the next tile ticket,
+// counts its 4096 keys' digits, publishes the counts, resolves its global
+// digit offsets by decoupled look-back over the preceding tiles (bounded
+// spin), ranks its keys stably with a ballot multisplit, then scatters
+// through shared memory so global writes are contiguous within each digit
+// run.
 #include "sort.cuh"
 
 namespace ygx {
@@ -63,7 +64,7 @@ struct __align__(16) OnesweepSmem {
 };
 
 template <bool kIotaValues>
-__global__ void __launch_bounds__(kSortThreads, 3)
+__global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
     k_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                int64_t n, int shift, const uint32_t* __restrict__ digit_offsets,
                uint32_t* __restrict__ lookback, uint32_t* __restrict__ ticket_counter,
@@ -75,6 +76,8 @@ __global__ void __launch_bounds__(kSortThreads, 3)
 
   for (int i = tid; i < (kSortThreads / 32) * kSortRadix; i += kSortThreads)
     (&sm.warp_hist[0][0])[i] = 0;
+  __shared__ uint32_t s_cnt[kSortRadix];
+  if (tid < kSortRadix) s_cnt[tid] = 0;
   if (tid == 0) sm.ticket = atomicAdd(ticket_counter, 1u);
   __syncthreads();
   const uint32_t tile = sm.ticket;
@@ -82,42 +85,116 @@ __global__ void __launch_bounds__(kSortThreads, 3)
   const int64_t wbase = base + (int64_t)warp * (kSortItems * 32);
 
   uint64_t keys[kSortItems];
+  uint32_t vals[kSortItems];
   uint16_t rank[kSortItems];
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
     int64_t idx = wbase + i * 32 + lane;
     keys[i] = idx < n ? keys_in[idx] : ~0ull;
   }
+  // Early counts: the tile's digit histogram first, so its aggregate is
+  // published and its look-back resolved before the (longer) ranking --
+  // successors then find an inclusive prefix sooner.
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i)
+    atomicAdd(&s_cnt[(uint32_t)(keys[i] >> shift) & (kSortRadix - 1)], 1u);
+  __syncthreads();
+  const int d = tid;
+  uint32_t total = s_cnt[d];
+  uint32_t* my_lb = lookback + (size_t)tile * kSortRadix;
+  if (tile == 0) st_volatile_u32(&my_lb[d], kFlagInc | total);
+  else st_volatile_u32(&my_lb[d], kFlagAgg | total);
+  // Decoupled look-back for digit d, kLookback predecessors per step: their
+  // words are read together (independent loads) and resolved in order; only
+  // a predecessor that has published nothing yet is waited for (bounded).
+  uint32_t excl = 0;
+  if (tile > 0) {
+    constexpr int kLookback = 8;
+    int64_t j = (int64_t)tile - 1;
+    bool done = false, timed_out = false;
+    while (!done && !timed_out) {
+      uint32_t v[kLookback];
+#pragma unroll
+      for (int k = 0; k < kLookback; ++k)
+        v[k] = j - k >= 0 ? ld_volatile_u32(lookback + (size_t)(j - k) * kSortRadix + d)
+                          : kFlagInc;  // before tile 0: inclusive zero
+#pragma unroll
+      for (int k = 0; k < kLookback; ++k) {
+        if (done || timed_out) continue;
+        uint32_t w = v[k];
+        if ((w & ~kCountMask) == 0) {
+          const uint32_t* p = lookback + (size_t)(j - k) * kSortRadix + d;
+          uint32_t spins = 0;
+          while ((w & ~kCountMask) == 0 && spins < YGX_SPIN_LIMIT) {
+            __nanosleep(32);
+            w = ld_volatile_u32(p);
+            ++spins;
+          }
+          if ((w & ~kCountMask) == 0) {
+            timed_out = true;
+            continue;
+          }
+        }
+        excl += w & kCountMask;
+        if ((w & ~kCountMask) == kFlagInc) done = true;
+      }
+      j -= kLookback;
+    }
+    if (timed_out) raise_flag(status, kFlagTimeout);
+    st_volatile_u32(&my_lb[d], kFlagInc | ((excl + total) & kCountMask));
+  }
+  sm.glob[d] = digit_offsets[d] + excl;
+  // Stable warp multisplit, kRankGroup items at a time: the peer mask of
+  // every item (lanes holding the same digit) from one ballot per digit bit
+  // (match-any measured slower here), then one shared-memory atomic per
+  // distinct digit (issued back to back; atomics of one warp on one counter
+  // apply in program order, so earlier items get lower ranks), then the
+  // shuffles.
   const unsigned lt_mask = (1u << lane) - 1u;
+  constexpr int kRankGroup = 4;
+#pragma unroll
+  for (int g = 0; g < kSortItems; g += kRankGroup) {
+    unsigned peers[kRankGroup];
+    uint32_t dg[kRankGroup], old[kRankGroup];
+#pragma unroll
+    for (int u = 0; u < kRankGroup; ++u) {
+      dg[u] = (uint32_t)(keys[g + u] >> shift) & (kSortRadix - 1);
+      unsigned pm = 0xffffffffu;
+#pragma unroll
+      for (int b = 0; b < kSortRadixBits; ++b) {
+        const unsigned bb = __ballot_sync(0xffffffffu, (dg[u] >> b) & 1u);
+        pm &= ((dg[u] >> b) & 1u) ? bb : ~bb;
+      }
+      peers[u] = pm;
+    }
+#pragma unroll
+    for (int u = 0; u < kRankGroup; ++u) {
+      old[u] = 0;
+      if (lane == __ffs(peers[u]) - 1)
+        old[u] = atomicAdd(&sm.warp_hist[warp][dg[u]], (uint32_t)__popc(peers[u]));
+    }
+#pragma unroll
+    for (int u = 0; u < kRankGroup; ++u) {
+      const uint32_t o = __shfl_sync(0xffffffffu, old[u], __ffs(peers[u]) - 1);
+      rank[g + u] = (uint16_t)(o + __popc(peers[u] & lt_mask));
+    }
+  }
+  // values travel with the keys; loading them here overlaps the look-back
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
-    uint32_t d = (uint32_t)(keys[i] >> shift) & (kSortRadix - 1);
-    unsigned peers = __match_any_sync(0xffffffffu, d);
-    int leader = __ffs(peers) - 1;
-    uint32_t old = 0;
-    if (lane == leader) {
-      old = sm.warp_hist[warp][d];
-      sm.warp_hist[warp][d] = old + __popc(peers);
-    }
-    old = __shfl_sync(0xffffffffu, old, leader);
-    rank[i] = (uint16_t)(old + __popc(peers & lt_mask));
-    __syncwarp();
+    int64_t idx = wbase + i * 32 + lane;
+    vals[i] = kIotaValues ? (uint32_t)idx : (idx < n ? vals_in[idx] : 0u);
   }
   __syncthreads();
 
   // Thread t owns digit t: warp-exclusive prefixes and the tile total.
-  const int d = tid;
-  uint32_t total = 0;
+  total = 0;
 #pragma unroll
   for (int w = 0; w < kSortThreads / 32; ++w) {
     uint32_t c = sm.warp_hist[w][d];
     sm.warp_hist[w][d] = total;
     total += c;
   }
-  // Publish this tile's digit count as early as possible.
-  uint32_t* my_lb = lookback + (size_t)tile * kSortRadix;
-  if (tile == 0) st_volatile_u32(&my_lb[d], kFlagInc | total);
-  else st_volatile_u32(&my_lb[d], kFlagAgg | total);
 
   // Block exclusive scan of the digit totals -> tile-local digit starts.
   uint32_t incl = total;
@@ -132,30 +209,6 @@ __global__ void __launch_bounds__(kSortThreads, 3)
   for (int w = 0; w < warp; ++w) wpre += sm.warp_tot[w];
   sm.tile_start[d] = wpre + incl - total;
 
-  // Decoupled look-back for digit d.
-  uint32_t excl = 0;
-  if (tile > 0) {
-    int64_t j = (int64_t)tile - 1;
-    while (j >= 0) {
-      const uint32_t* p = lookback + (size_t)j * kSortRadix + d;
-      uint32_t v = ld_volatile_u32(p);
-      uint32_t spins = 0;
-      while ((v & ~kCountMask) == 0 && spins < YGX_SPIN_LIMIT) {
-        __nanosleep(32);
-        v = ld_volatile_u32(p);
-        ++spins;
-      }
-      if ((v & ~kCountMask) == 0) {
-        raise_flag(status, kFlagTimeout);
-        break;
-      }
-      excl += v & kCountMask;
-      if ((v & ~kCountMask) == kFlagInc) break;
-      --j;
-    }
-    st_volatile_u32(&my_lb[d], kFlagInc | ((excl + total) & kCountMask));
-  }
-  sm.glob[d] = digit_offsets[d] + excl;
   __syncthreads();
 
   // Scatter into shared memory in tile-sorted order.
@@ -163,9 +216,8 @@ __global__ void __launch_bounds__(kSortThreads, 3)
   for (int i = 0; i < kSortItems; ++i) {
     uint32_t dd = (uint32_t)(keys[i] >> shift) & (kSortRadix - 1);
     uint32_t pos = sm.tile_start[dd] + sm.warp_hist[warp][dd] + rank[i];
-    int64_t idx = wbase + i * 32 + lane;
     sm.keys[pos] = keys[i];
-    sm.vals[pos] = kIotaValues ? (uint32_t)idx : (idx < n ? vals_in[idx] : 0u);
+    sm.vals[pos] = vals[i];
   }
   __syncthreads();
   const int64_t nvalid = n - base < kSortTile ? n - base : kSortTile;

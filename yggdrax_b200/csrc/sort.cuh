@@ -10,6 +10,8 @@ constexpr int kSortRadix = 1 << kSortRadixBits;
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+constexpr int kSortBlocksPerSM = 3;                   // onesweep CTAs resident per SM
+static_assert(kSortThreads == kSortRadix, "onesweep: thread t owns digit t");
 
 inline int sort_passes(int begin_bit, int end_bit) {
   return (end_bit - begin_bit + kSortRadixBits - 1) / kSortRadixBits;
