@@ -44,6 +44,14 @@ __device__ __forceinline__ void ld_box(const float* __restrict__ mn, const float
   }
 }
 
+// Arrival on a parent: release this thread's box writes, acquire the
+// sibling's (one acq_rel atomic instead of a fence on either side).
+__device__ __forceinline__ int arrive_acq_rel(int32_t* p) {
+  int old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(p) : "memory");
+  return old;
+}
+
 __device__ void climb(int64_t node, const int32_t* __restrict__ parent32,
                       const int32_t* __restrict__ left32, const int32_t* __restrict__ right32,
                       float* __restrict__ mn, float* __restrict__ mx, int32_t* __restrict__ arrive,
@@ -51,9 +59,7 @@ __device__ void climb(int64_t node, const int32_t* __restrict__ parent32,
                       float* __restrict__ radius, float* __restrict__ max_extent) {
   int64_t p = parent32[node];
   while (p >= 0) {
-    __threadfence();
-    if (atomicAdd(&arrive[p], 1) == 0) return;  // sibling not finished yet
-    __threadfence();
+    if (arrive_acq_rel(&arrive[p]) == 0) return;  // sibling not finished yet
     const int64_t l = left32[p], r = right32[p];
     float llo[3], lhi[3], rlo[3], rhi[3], lo[3], hi[3];
     ld_box(mn, mx, l, llo, lhi);
@@ -70,7 +76,9 @@ __device__ void climb(int64_t node, const int32_t* __restrict__ parent32,
   }
 }
 
-// Leaf boxes from particle ranges; one warp per leaf, then lane 0 climbs.
+// Leaf boxes from particle ranges.  A warp reduces 32 leaves one after the
+// other (coalesced particle loads, shuffle reductions); lane j keeps leaf j's
+// box, and then all 32 lanes climb at once.
 __global__ void k_leaf_ranges_refit(const void* ranges, int64_t ni, int64_t L, int index_bits,
                                     const float* __restrict__ pos, int64_t cap, bool empty_inf,
                                     const int32_t* __restrict__ parent32,
@@ -83,40 +91,52 @@ __global__ void k_leaf_ranges_refit(const void* ranges, int64_t ni, int64_t L, i
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const float big = empty_inf ? __int_as_float(0x7f800000) : 3.402823466e38f;
-  for (int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < L; j += warps) {
-    const int64_t node = ni + j;
-    const int64_t s = load_idx(ranges, index_bits, 2 * node);
-    int64_t c = load_idx(ranges, index_bits, 2 * node + 1) - s + 1;
-    if (cap >= 0 && c > cap) c = cap;
-    float lo[3] = {big, big, big}, hi[3] = {-big, -big, -big};
-    unsigned nan = 0;
-    for (int64_t k = lane; k < c; k += 32) {
-      const float* p = pos + 3 * (s + k);
+  const float qnan = __int_as_float(0x7fc00000);
+  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32;
+       base < L; base += warps * 32) {
+    float my_lo[3] = {0.f, 0.f, 0.f}, my_hi[3] = {0.f, 0.f, 0.f};
+    const int nl = L - base < 32 ? (int)(L - base) : 32;
+    for (int jj = 0; jj < nl; ++jj) {
+      const int64_t node = ni + base + jj;
+      const int64_t s = load_idx(ranges, index_bits, 2 * node);
+      int64_t c = load_idx(ranges, index_bits, 2 * node + 1) - s + 1;
+      if (cap >= 0 && c > cap) c = cap;
+      float lo[3] = {big, big, big}, hi[3] = {-big, -big, -big};
+      unsigned nan = 0;
+      for (int64_t k = lane; k < c; k += 32) {
+        const float* p = pos + 3 * (s + k);
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        float v = __ldg(p + a);
-        if (v != v) nan |= 1u << a;
-        lo[a] = fminf(lo[a], v);
-        hi[a] = fmaxf(hi[a], v);
+        for (int a = 0; a < 3; ++a) {
+          float v = __ldg(p + a);
+          if (v != v) nan |= 1u << a;
+          lo[a] = fminf(lo[a], v);
+          hi[a] = fmaxf(hi[a], v);
+        }
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
+          hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
+        }
+        nan |= __shfl_xor_sync(0xffffffffu, nan, off);
+      }
+      if (lane == jj) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          my_lo[a] = (nan >> a) & 1 ? qnan : lo[a];
+          my_hi[a] = (nan >> a) & 1 ? qnan : hi[a];
+        }
       }
     }
-    for (int off = 16; off > 0; off >>= 1) {
+    if (lane < nl) {
+      const int64_t node = ni + base + lane;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
-        hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
+        __stcg(mn + 3 * node + a, my_lo[a]);
+        __stcg(mx + 3 * node + a, my_hi[a]);
       }
-      nan |= __shfl_xor_sync(0xffffffffu, nan, off);
-    }
-    if (lane == 0) {
-      const float qnan = __int_as_float(0x7fc00000);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        if ((nan >> a) & 1) { lo[a] = qnan; hi[a] = qnan; }
-        __stcg(mn + 3 * node + a, lo[a]);
-        __stcg(mx + 3 * node + a, hi[a]);
-      }
-      finalize_node(node, lo, hi, center, half, radius, max_extent);
+      finalize_node(node, my_lo, my_hi, center, half, radius, max_extent);
       if (climb_ok) climb(node, parent32, left32, right32, mn, mx, arrive, center, half, radius,
                           max_extent);
     }
@@ -259,7 +279,8 @@ int ygx_tree_geometry(const void* node_ranges, int64_t total, int index_bits,
         s.arrive, tree_flags, center, half_extent, radius, max_extent);
   } else {
     const int warps = 8;
-    ygx::k_leaf_ranges_refit<<<ygx::grid_for(L, warps, ygx::kNumSMs * 32), warps * 32, 0, stream>>>(
+    ygx::k_leaf_ranges_refit<<<ygx::grid_for((L + 31) / 32, warps, ygx::kNumSMs * 16), warps * 32, 0,
+                               stream>>>(
         node_ranges, ni, L, index_bits, positions_sorted, max_leaf_size, max_leaf_size == 0,
         parent32, left32, right32, s.mn, s.mx, s.arrive, tree_flags, center, half_extent, radius,
         max_extent);
