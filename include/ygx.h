@@ -220,10 +220,12 @@ size_t ygx_traverse_workspace_size(int64_t total, int64_t num_leaves, int64_t wf
  * YGX_FLAG_LOG_OVERFLOW in *flags_out: re-run with larger capacities (the
  * walk is deterministic; the reported log need is exact).  Synchronizes the
  * stream. */
+#define YGX_WALK_LOG 0   /* one walk: row counts + a log of accepted / near pairs */
+#define YGX_WALK_COUNT 1 /* plain two-pass mode, first walk: row counts only     */
 int ygx_traverse_walk(const float* center, const float* radius, const float* max_extent,
                       const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
                       int64_t total, int64_t num_internal, int mac, float theta,
-                      float dehnen_radius_scale, int root, int64_t wf_capacity,
+                      float dehnen_radius_scale, int root, int mode, int64_t wf_capacity,
                       int64_t log_capacity, uint64_t* stats_out, uint32_t* flags_out, void* ws,
                       size_t ws_bytes, cudaStream_t stream);
 /* Row layout of the fill walk (_dual_tree_walk_compact_fill_impl,
@@ -236,6 +238,18 @@ int ygx_traverse_fill(int64_t total, int64_t num_internal, int64_t wf_capacity,
                       void* node_offsets, void* far_counts, void* level_offsets,
                       void* near_offsets, void* near_counts, int32_t* far_src32,
                       int32_t* near_nbr32, void* ws, size_t ws_bytes, cudaStream_t stream);
+/* Plain two-pass mode, second walk (the reference's count-then-fill,
+ * _dual_tree_walk_compact_fill_impl :2942-3558): after ygx_traverse_walk with
+ * YGX_WALK_COUNT on the same workspace, the offset tables as in
+ * ygx_traverse_fill and the raw rows written by walking the `gens`
+ * generations again (entries at atomic row cursors). */
+int ygx_traverse_fill_walk(int64_t total, int64_t num_internal, int mac, float theta, int root,
+                           int64_t wf_capacity, int64_t log_capacity, int gens,
+                           int64_t far_total, int64_t near_total, const int32_t* nbl32,
+                           const void* tree_level_offsets, int num_levels, int index_bits,
+                           void* node_offsets, void* far_counts, void* level_offsets,
+                           void* near_offsets, void* near_counts, int32_t* far_src32,
+                           int32_t* near_nbr32, void* ws, size_t ws_bytes, cudaStream_t stream);
 /* Row finalize: canonical (ascending) order within each row, level-major
  * far sources/targets/target_levels, leaf-ordered near neighbours, and
  * optionally the dense neighbour_leaf_positions table (L x max_nbr). */

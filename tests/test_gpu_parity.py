@@ -330,3 +330,25 @@ def test_wavefront_overflow_retries_with_larger_capacity(cuda_device):
     for f in ("far_counts", "node_offsets", "level_offsets", "sources", "targets",
               "near_counts", "near_offsets", "neighbors"):
         np.testing.assert_array_equal(_np(getattr(a, f)), _np(getattr(b, f)), err_msg=f)
+
+
+@pytest.mark.parametrize("mode", ["two_pass", "log"])
+def test_traversal_modes_give_identical_lists(cuda_device, oracle, mode):
+    """The plain two-pass schedule (count walk, then a fill walk) and the
+    one-walk pair log return the same lists as the oracle."""
+    import yggdrax_b200 as yb
+    from yggdrax_b200 import inputs
+
+    pos, mass = inputs.plummer(200_000, 11)
+    P, M = _to_dev(pos, cuda_device), _to_dev(mass, cuda_device)
+    gt, ps = yb.build_tree(P, M, leaf_size=16, return_reordered=True)[:2]
+    gg = yb.compute_tree_geometry(gt, ps)
+    yb.set_traversal_mode(mode)
+    try:
+        gi, gn = yb.build_interactions_and_neighbors(gt, gg, theta=0.5, mac_type="bh")
+    finally:
+        yb.set_traversal_mode("log")
+    ot = oracle.build_tree(pos, mass, leaf_size=16)
+    og = oracle.compute_tree_geometry(ot, ot.positions_sorted)
+    r = oracle.build_interactions_and_neighbors(ot, og, theta=0.5, mac_type="bh")
+    _compare_lists(gi, gn, r)

@@ -21,6 +21,7 @@ from .interactions import (
     set_default_dual_tree_config,
     set_dense_neighbor_budget,
     set_reference_limits,
+    set_traversal_mode,
 )
 from .morton import (
     encode_and_sort,

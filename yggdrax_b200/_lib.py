@@ -36,6 +36,8 @@ FLAG_NEAR_OVERFLOW = 1 << 3
 FLAG_MALFORMED = 1 << 4
 FLAG_BAD_INPUT = 1 << 5
 FLAG_LOG_OVERFLOW = 1 << 6
+WALK_LOG = 0
+WALK_COUNT = 1
 
 TSTAT_WORDS = 16
 TSTAT = dict(far_total=0, near_total=1, max_far=2, max_near=3, accept=4, near=5, refine=6,
@@ -75,8 +77,10 @@ _SIGS = {
     "ygx_tree_geometry": (I32, [P, I64, I32, P, P, P, P, P, P, I64, I32, P, P, P, I64, P, P,
                                 P, P, P, SZ, P]),
     "ygx_traverse_workspace_size": (SZ, [I64, I64, I64, I64]),
-    "ygx_traverse_walk": (I32, [P, P, P, P, P, P, I64, I64, I32, F32, F32, I32, I64, I64, P, P,
-                                P, SZ, P]),
+    "ygx_traverse_walk": (I32, [P, P, P, P, P, P, I64, I64, I32, F32, F32, I32, I32, I64, I64,
+                                P, P, P, SZ, P]),
+    "ygx_traverse_fill_walk": (I32, [I64, I64, I32, F32, I32, I64, I64, I32, I64, I64, P, P, I32,
+                                     I32, P, P, P, P, P, P, P, P, SZ, P]),
     "ygx_traverse_fill": (I32, [I64, I64, I64, I64, I64, I64, P, P, P, I32, I32, P, P, P, P, P,
                                 P, P, P, SZ, P]),
     "ygx_traverse_finalize": (I32, [I64, I64, I64, I64, P, P, I32, P, P, P, P, P, P, P, I64, P, SZ,

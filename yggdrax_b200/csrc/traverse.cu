@@ -96,6 +96,27 @@ constexpr int kWalkGrid = kNumSMs * kWalkBlocksPerSM;  // fixed across generatio
 constexpr int kCoarse = 4096;  // coarse index buckets of a walk generation
 static_assert(kWalkGrid < 65536, "coarse index holds region ids as uint16");
 
+// What a walk does with its accepted / near pairs:
+//  kWalkLog   count row entries and log each pair once (then k_log_scatter);
+//  kWalkCount count row entries only (first walk of the plain two-pass mode);
+//  kWalkFill  write both directed entries into the exact rows at atomic
+//             cursors (second walk of the plain two-pass mode);
+//  kWalkPred  write them into rows of predicted capacity (cursor < row end),
+//             logging each directed entry that does not fit as (row key, value)
+//             with far rows keyed by node and near rows by total + leaf position.
+enum WalkMode { kWalkLog = 0, kWalkCount = 1, kWalkFill = 2, kWalkPred = 3 };
+
+struct RowSink {
+  unsigned long long* far_pos;         // cursors (fill / predicted)
+  unsigned long long* near_pos;
+  const unsigned long long* far_end;   // predicted: row ends
+  const unsigned long long* near_end;
+  int32_t* far_src;                    // raw rows
+  int32_t* near_nbr;
+  unsigned long long far_total;        // fill: buffer sizes
+  unsigned long long near_total;
+};
+
 // One BFS generation.  The wavefront of generation g is split into
 // kWalkGrid regions, one per CTA of generation g-1, each holding cnt_in[r]
 // pairs at wf_in[r * R ...].  A CTA maps a global input index to (region,
@@ -107,7 +128,7 @@ static_assert(kWalkGrid < 65536, "coarse index holds region ids as uint16");
 // warp, lane) with one barrier per iteration.  The walk is therefore
 // deterministic, and the entries a region would have needed are counted
 // even past its end, so one re-run with the reported sizes always fits.
-template <int kMac>
+template <int kMode, int kMac>
 __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
     k_walk_gen(const NodeRec* __restrict__ nodes, int32_t ni, int32_t total_nodes,
                float theta_sq, float theta,
@@ -115,7 +136,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
                const uint32_t* __restrict__ cnt_in, uint32_t* __restrict__ cnt_out, uint32_t R,
                uint32_t* __restrict__ sizes, int gen, int32_t* __restrict__ far_cnt,
                int32_t* __restrict__ near_cnt, int2* __restrict__ log,
-               unsigned long long* __restrict__ log_cnt, unsigned long long LR,
+               unsigned long long* __restrict__ log_cnt, unsigned long long LR, RowSink sink,
                unsigned long long* __restrict__ stats, uint32_t* __restrict__ status) {
   constexpr int kWarps = kWalkThreads / 32;
   __shared__ uint32_t s_prefix[kWalkGrid + 1];
@@ -235,15 +256,53 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
     n_acc += acc;
     n_near += nearp;
     n_ref += refine;
-    // Row counts: plain fire-and-forget atomics (aggregating equal keys in
-    // the warp with match-any first measured slower here).
-    if (acc) {
-      atomicAdd(&far_cnt[t], 1);
-      atomicAdd(&far_cnt[sv], 1);
-    }
-    if (nearp) {
-      atomicAdd(&near_cnt[A.k.z], 1);
-      atomicAdd(&near_cnt[B.k.z], 1);
+    int lc = 0;  // log entries of this lane
+    int2 le0 = make_int2(0, 0), le1 = le0;
+    if (kMode == kWalkLog || kMode == kWalkCount) {
+      // Row counts: plain fire-and-forget atomics (aggregating equal keys in
+      // the warp with match-any first measured slower here).
+      if (acc) {
+        atomicAdd(&far_cnt[t], 1);
+        atomicAdd(&far_cnt[sv], 1);
+      }
+      if (nearp) {
+        atomicAdd(&near_cnt[A.k.z], 1);
+        atomicAdd(&near_cnt[B.k.z], 1);
+      }
+      if (kMode == kWalkLog && (acc || nearp)) {
+        lc = 1;
+        le0 = make_int2(t, sv | (nearp ? (int)0x80000000u : 0));
+      }
+    } else if (acc || nearp) {
+      const int rt = acc ? t : A.k.z, rs = acc ? sv : B.k.z;
+      unsigned long long* cur = acc ? sink.far_pos : sink.near_pos;
+      int32_t* dst = acc ? sink.far_src : sink.near_nbr;
+      const unsigned long long pt = atomicAdd(&cur[rt], 1ull);
+      const unsigned long long ps = atomicAdd(&cur[rs], 1ull);
+      if (kMode == kWalkFill) {
+        const unsigned long long lim = acc ? sink.far_total : sink.near_total;
+        const uint32_t fl = acc ? kFlagFarOverflow : kFlagNearOverflow;
+        if (pt < lim) dst[pt] = sv; else raise_flag(status, fl);
+        if (ps < lim) dst[ps] = t; else raise_flag(status, fl);
+      } else {
+        const unsigned long long* end = acc ? sink.far_end : sink.near_end;
+        const int kt = acc ? t : total_nodes + rt, ks = acc ? sv : total_nodes + rs;
+        if (pt < end[rt]) {
+          dst[pt] = sv;
+        } else {
+          le0 = make_int2(kt, sv);
+          lc = 1;
+        }
+        if (ps < end[rs]) {
+          dst[ps] = t;
+        } else if (lc == 0) {
+          le0 = make_int2(ks, t);
+          lc = 1;
+        } else {
+          le1 = make_int2(ks, t);
+          lc = 2;
+        }
+      }
     }
 
     // Children of a refined pair (_interactions_impl.py:1262-1310).
@@ -279,16 +338,16 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
         nc = 2;
       }
     }
-    int incl = nc;
+    // warp scan of (children | log entries << 8): <= 128 and <= 64 per warp
+    int incl = nc | (lc << 8);
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
       int v = __shfl_up_sync(0xffffffffu, incl, off);
       if (lane >= off) incl += v;
     }
-    const bool lg = acc || nearp;
-    const unsigned lmask = __ballot_sync(0xffffffffu, lg);
-    // children (<= 128 per warp) in the low half, log entries in the high
-    if (lane == 31) s_wt[buf][warp] = (uint32_t)incl | ((uint32_t)__popc(lmask) << 16);
+    // children (<= 1024 per CTA) in the low half, log entries in the high
+    if (lane == 31)
+      s_wt[buf][warp] = (uint32_t)(incl & 0xff) | ((uint32_t)(incl >> 8) << 16);
     __syncthreads();
     uint32_t pre = 0, sum = 0;
 #pragma unroll
@@ -297,19 +356,20 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
       pre += w < warp ? v : 0u;
       sum += v;
     }
-    if (lg) {
-      const unsigned long long la = log_base + (pre >> 16) + __popc(lmask & lanemask_lt());
-      if (la < LR)
-        log[(size_t)blockIdx.x * LR + la] = make_int2(t, sv | (nearp ? (int)0x80000000u : 0));
-      else
-        raise_flag(status, kFlagLogOverflow);
+    if (lc > 0) {
+      const unsigned long long la = log_base + (pre >> 16) + (uint32_t)((incl >> 8) - lc);
+      int2* lp = log + (size_t)blockIdx.x * LR;
+      if (la < LR) lp[la] = le0; else raise_flag(status, kFlagLogOverflow);
+      if (lc > 1) {
+        if (la + 1 < LR) lp[la + 1] = le1; else raise_flag(status, kFlagLogOverflow);
+      }
     }
     log_base += sum >> 16;
     sum &= 0xffffu;
     pre &= 0xffffu;
     // Every child that fits is written, so the first min(total, R) slots of
     // the region are always filled.
-    const unsigned long long at = cta_base + pre + (uint32_t)(incl - nc);
+    const unsigned long long at = cta_base + pre + (uint32_t)((incl & 0xff) - nc);
     if (nc > 0) {
       if (at + (unsigned long long)nc <= R) {
         int2* o = my_out + at;
@@ -1027,23 +1087,108 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap, i
   return s;
 }
 
-static int launch_gen(int mac, const TravScratch& s, int32_t ni, int32_t total_nodes,
-                      float theta_sq, float theta, int gen, uint32_t cap, cudaStream_t st) {
+static int launch_gen(int mode, int mac, const TravScratch& s, int32_t ni, int32_t total_nodes,
+                      float theta_sq, float theta, int gen, uint32_t cap, const RowSink& sink,
+                      cudaStream_t st) {
   const int2* in = s.wf[gen & 1];
   int2* out = s.wf[(gen + 1) & 1];
   const uint32_t* cin = s.region_cnt[gen & 1];
   uint32_t* cout = s.region_cnt[(gen + 1) & 1];
   const uint32_t R = (uint32_t)region_capacity(cap);
-#define YGX_GEN(MAC)                                                                        \
-  k_walk_gen<MAC><<<kWalkGrid, kWalkThreads, 0, st>>>(                                      \
+#define YGX_GEN(MODE, MAC)                                                                  \
+  k_walk_gen<MODE, MAC><<<kWalkGrid, kWalkThreads, 0, st>>>(                                \
       s.recs, ni, total_nodes, theta_sq, theta, in, out, cin, cout, R, s.sizes, gen,        \
-      s.far_cnt, s.near_cnt, s.log, s.log_cnt, s.log_region, s.stats, s.status)
-  if (mac == kMacBH) YGX_GEN(kMacBH);
-  else if (mac == kMacDehnen) YGX_GEN(kMacDehnen);
-  else YGX_GEN(kMacEngblom);
+      s.far_cnt, s.near_cnt, s.log, s.log_cnt, s.log_region, sink, s.stats, s.status)
+#define YGX_GEN_MAC(MODE)                     \
+  if (mac == kMacBH) YGX_GEN(MODE, kMacBH);   \
+  else if (mac == kMacDehnen) YGX_GEN(MODE, kMacDehnen); \
+  else YGX_GEN(MODE, kMacEngblom);
+  switch (mode) {
+    case kWalkLog: YGX_GEN_MAC(kWalkLog) break;
+    case kWalkCount: YGX_GEN_MAC(kWalkCount) break;
+    case kWalkFill: YGX_GEN_MAC(kWalkFill) break;
+    case kWalkPred: YGX_GEN_MAC(kWalkPred) break;
+    default: return YGX_ERR_ARG;
+  }
+#undef YGX_GEN_MAC
 #undef YGX_GEN
   YGX_CHECK_LAUNCH();
   return YGX_OK;
+}
+
+// Seeds (root, root) and launches the generations.  With fixed_gens < 0 the
+// wavefront size is probed every 16 generations until it is empty (or a
+// wavefront overflow is flagged); otherwise exactly fixed_gens generations
+// run (a repeat of a walk whose length is known).  *gens_out = launched.
+static int run_gens(int mode, int mac, const TravScratch& s, int32_t ni, int32_t total,
+                    float theta_sq, float theta_r, int root, uint32_t cap, const RowSink& sink,
+                    int fixed_gens, int* gens_out, cudaStream_t stream) {
+  k_seed<<<1, 256, 0, stream>>>(s.wf[0], s.region_cnt[0], s.sizes, root);
+  YGX_CHECK_LAUNCH();
+  int gen = 0, rc = YGX_OK;
+  if (fixed_gens >= 0) {
+    for (; gen < fixed_gens; ++gen) {
+      rc = launch_gen(mode, mac, s, ni, total, theta_sq, theta_r, gen, cap, sink, stream);
+      if (rc) return rc;
+    }
+    *gens_out = gen;
+    return YGX_OK;
+  }
+  const int chunk = 16;
+  while (true) {
+    for (int k = 0; k < chunk && gen < kMaxGens; ++k, ++gen) {
+      rc = launch_gen(mode, mac, s, ni, total, theta_sq, theta_r, gen, cap, sink, stream);
+      if (rc) return rc;
+    }
+    uint32_t probe = 0, flags = 0;
+    if (cudaMemcpyAsync(&probe, s.sizes + gen, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                        stream) != cudaSuccess ||
+        cudaMemcpyAsync(&flags, s.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+      return YGX_ERR_CUDA;
+    // A wavefront overflow ends the walk at once; a log overflow does not
+    // (the walk goes on counting, so the log need it reports is exact).
+    if (probe == 0 || (flags & ~(uint32_t)kFlagLogOverflow) != 0) break;
+    if (gen >= kMaxGens) {
+      *gens_out = gen;
+      return YGX_ERR_QUEUE_OVERFLOW;
+    }
+  }
+  *gens_out = gen;
+  return YGX_OK;
+}
+
+// Row offsets from the counts in the workspace: level-major far offsets and
+// the index-dtype offset / count tables, leaf-order near offsets.
+static int row_offsets(const TravScratch& s, int64_t total, int64_t L, const int32_t* nbl32,
+                       const void* tree_level_offsets, int num_levels, int index_bits,
+                       void* node_offsets, void* far_counts, void* level_offsets,
+                       void* near_offsets, void* near_counts, cudaStream_t stream) {
+  k_gather_counts<<<grid_for(total, 256), 256, 0, stream>>>(s.far_cnt, nbl32, total,
+                                                            s.cnt_by_level);
+  YGX_CHECK_LAUNCH();
+  int rc = exclusive_scan<int32_t>(s.cnt_by_level, total, s.obl, s.scan_tmp, stream);
+  if (rc) return rc;
+  k_far_offsets<<<grid_for(total + 1, 256), 256, 0, stream>>>(
+      s.obl, nbl32, s.far_cnt, total, index_bits, s.far_off, node_offsets, far_counts,
+      tree_level_offsets, num_levels, level_offsets);
+  YGX_CHECK_LAUNCH();
+  rc = exclusive_scan<int32_t>(s.near_cnt, L, s.near_off, s.scan_tmp, stream);
+  if (rc) return rc;
+  k_near_offsets<<<grid_for(L + 1, 256), 256, 0, stream>>>(s.near_off, s.near_cnt, L,
+                                                           index_bits, near_offsets, near_counts);
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
+static RowSink no_sink() {
+  RowSink k;
+  k.far_pos = k.near_pos = nullptr;
+  k.far_end = k.near_end = nullptr;
+  k.far_src = k.near_nbr = nullptr;
+  k.far_total = k.near_total = 0;
+  return k;
 }
 
 }  // namespace ygx
@@ -1078,11 +1223,12 @@ static int trav_setup(ygx::TravScratch& s, void* ws, size_t ws_bytes, int64_t to
 int ygx_traverse_walk(const float* center, const float* radius, const float* max_extent,
                       const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
                       int64_t total, int64_t num_internal, int mac, float theta,
-                      float dehnen_radius_scale, int root, int64_t wf_capacity,
+                      float dehnen_radius_scale, int root, int mode, int64_t wf_capacity,
                       int64_t log_capacity, uint64_t* stats_out, uint32_t* flags_out, void* ws,
                       size_t ws_bytes, cudaStream_t stream) {
   if (total < 3 || total > INT32_MAX || num_internal < 1 || mac < 0 || mac > 2 ||
-      root < 0 || root >= total || !stats_out || !flags_out)
+      root < 0 || root >= total || !stats_out || !flags_out ||
+      (mode != YGX_WALK_LOG && mode != YGX_WALK_COUNT))
     return YGX_ERR_ARG;
   const int64_t L = total - num_internal;
   ygx::TravScratch s;
@@ -1103,31 +1249,12 @@ int ygx_traverse_walk(const float* center, const float* radius, const float* max
       center, radius, max_extent, left32, right32, leafpos32, total, mac, dehnen_radius_scale,
       s.recs, s.status);
   YGX_CHECK_LAUNCH();
-  ygx::k_seed<<<1, 256, 0, stream>>>(s.wf[0], s.region_cnt[0], s.sizes, root);
-  YGX_CHECK_LAUNCH();
   int gen = 0;
-  const int chunk = 16;
-  while (true) {
-    for (int k = 0; k < chunk && gen < ygx::kMaxGens; ++k, ++gen) {
-      rc = ygx::launch_gen(mac, s, (int32_t)num_internal, (int32_t)total, theta_sq, theta_r, gen,
-                           (uint32_t)wf_capacity, stream);
-      if (rc) return rc;
-    }
-    uint32_t probe = 0, flags = 0;
-    if (cudaMemcpyAsync(&probe, s.sizes + gen, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                        stream) != cudaSuccess ||
-        cudaMemcpyAsync(&flags, s.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
-            cudaSuccess ||
-        cudaStreamSynchronize(stream) != cudaSuccess)
-      return YGX_ERR_CUDA;
-    // A wavefront overflow ends the walk at once; a log overflow does not
-    // (the walk goes on counting, so the log need it reports is exact).
-    if (probe == 0 || (flags & ~(uint32_t)ygx::kFlagLogOverflow) != 0) break;
-    if (gen >= ygx::kMaxGens) {
-      flags_out[0] = ygx::kFlagQueueOverflow;
-      return YGX_ERR_QUEUE_OVERFLOW;
-    }
-  }
+  rc = ygx::run_gens(mode == YGX_WALK_LOG ? ygx::kWalkLog : ygx::kWalkCount, mac, s,
+                     (int32_t)num_internal, (int32_t)total, theta_sq, theta_r, root,
+                     (uint32_t)wf_capacity, ygx::no_sink(), -1, &gen, stream);
+  if (rc == YGX_ERR_QUEUE_OVERFLOW) flags_out[0] = ygx::kFlagQueueOverflow;
+  if (rc) return rc;
   ygx::k_count_stats<<<ygx::grid_for(total, 256, ygx::kNumSMs * 4), 256, 0, stream>>>(
       s.far_cnt, total, s.near_cnt, L, s.sizes, gen, s.log_cnt, s.stats);
   YGX_CHECK_LAUNCH();
@@ -1159,21 +1286,10 @@ int ygx_traverse_fill(int64_t total, int64_t num_internal, int64_t wf_capacity,
   ygx::TravScratch s;
   int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity, log_capacity);
   if (rc) return rc;
-  ygx::k_gather_counts<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.far_cnt, nbl32, total,
-                                                                      s.cnt_by_level);
-  YGX_CHECK_LAUNCH();
-  rc = ygx::exclusive_scan<int32_t>(s.cnt_by_level, total, s.obl, s.scan_tmp, stream);
+  rc = ygx::row_offsets(s, total, L, nbl32, tree_level_offsets, num_levels, index_bits,
+                        node_offsets, far_counts, level_offsets, near_offsets, near_counts,
+                        stream);
   if (rc) return rc;
-  ygx::k_far_offsets<<<ygx::grid_for(total + 1, 256), 256, 0, stream>>>(
-      s.obl, nbl32, s.far_cnt, total, index_bits, s.far_off, node_offsets, far_counts,
-      tree_level_offsets, num_levels, level_offsets);
-  YGX_CHECK_LAUNCH();
-  rc = ygx::exclusive_scan<int32_t>(s.near_cnt, L, s.near_off, s.scan_tmp, stream);
-  if (rc) return rc;
-  ygx::k_near_offsets<<<ygx::grid_for(L + 1, 256), 256, 0, stream>>>(s.near_off, s.near_cnt, L,
-                                                                     index_bits, near_offsets,
-                                                                     near_counts);
-  YGX_CHECK_LAUNCH();
   ygx::k_init_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.far_off, total, s.far_pos,
                                                                      s.near_off, L, s.near_pos);
   YGX_CHECK_LAUNCH();
@@ -1182,6 +1298,55 @@ int ygx_traverse_fill(int64_t total, int64_t num_internal, int64_t wf_capacity,
       (unsigned long long)far_total, (unsigned long long)near_total, far_src32, near_nbr32,
       s.status);
   YGX_CHECK_LAUNCH();
+  ygx::k_check_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      s.far_off, s.far_cnt, s.far_pos, total, s.near_off, s.near_cnt, s.near_pos, L, s.status);
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
+// Second walk of the plain two-pass mode (after ygx_traverse_walk with
+// YGX_WALK_COUNT on the same workspace): the offset tables as in
+// ygx_traverse_fill, then the same `gens` generations again, each directed
+// entry written at its row's atomic cursor, and every cursor checked
+// against its row end.  Does not synchronize.
+int ygx_traverse_fill_walk(int64_t total, int64_t num_internal, int mac, float theta, int root,
+                           int64_t wf_capacity, int64_t log_capacity, int gens,
+                           int64_t far_total, int64_t near_total, const int32_t* nbl32,
+                           const void* tree_level_offsets, int num_levels, int index_bits,
+                           void* node_offsets, void* far_counts, void* level_offsets,
+                           void* near_offsets, void* near_counts, int32_t* far_src32,
+                           int32_t* near_nbr32, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (total < 3 || total > INT32_MAX || num_internal < 1 || mac < 0 || mac > 2 || root < 0 ||
+      root >= total || gens < 0 || gens > ygx::kMaxGens || far_total < 0 || near_total < 0 ||
+      (index_bits != 32 && index_bits != 64))
+    return YGX_ERR_ARG;
+  const int64_t L = total - num_internal;
+  ygx::TravScratch s;
+  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity, log_capacity);
+  if (rc) return rc;
+  const float th = theta;
+  const float theta_sq = th * th;
+  const float theta_r = sqrtf(theta_sq);
+  rc = ygx::row_offsets(s, total, L, nbl32, tree_level_offsets, num_levels, index_bits,
+                        node_offsets, far_counts, level_offsets, near_offsets, near_counts,
+                        stream);
+  if (rc) return rc;
+  if (cudaMemsetAsync(s.sizes, 0, sizeof(uint32_t) * (ygx::kMaxGens + 2), stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  ygx::k_init_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.far_off, total, s.far_pos,
+                                                                     s.near_off, L, s.near_pos);
+  YGX_CHECK_LAUNCH();
+  ygx::RowSink sink = ygx::no_sink();
+  sink.far_pos = s.far_pos;
+  sink.near_pos = s.near_pos;
+  sink.far_src = far_src32;
+  sink.near_nbr = near_nbr32;
+  sink.far_total = (unsigned long long)far_total;
+  sink.near_total = (unsigned long long)near_total;
+  int ran = 0;
+  rc = ygx::run_gens(ygx::kWalkFill, mac, s, (int32_t)num_internal, (int32_t)total, theta_sq,
+                     theta_r, root, (uint32_t)wf_capacity, sink, gens, &ran, stream);
+  if (rc) return rc;
   ygx::k_check_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
       s.far_off, s.far_cnt, s.far_pos, total, s.near_off, s.near_cnt, s.near_pos, L, s.status);
   YGX_CHECK_LAUNCH();

@@ -210,6 +210,23 @@ LAST_WALK_STATS: dict = {}  # diagnostics of the most recent walk
 # a walk that overflows is re-run with the sizes it reports.
 _CAPACITY_HINTS: dict = {}
 _TIMING = os.environ.get("YGGDRAX_B200_TIMING", "0") == "1"  # per-pass CUDA-event times
+TRAVERSAL_MODES = ("log", "two_pass")
+_TRAVERSAL_MODE = os.environ.get("YGGDRAX_B200_TRAVERSAL_MODE", "log")
+
+
+def set_traversal_mode(mode: str) -> None:
+    """How the exact lists are produced (all modes return identical lists):
+
+    * ``"log"`` (default): one walk that counts row entries and logs every
+      accepted / near pair once, then a scatter of the log into the rows;
+    * ``"two_pass"``: the reference's plain count-then-fill schedule, two
+      walks (counts, then entries written at row cursors).
+
+    Environment: ``YGGDRAX_B200_TRAVERSAL_MODE``."""
+    global _TRAVERSAL_MODE
+    if mode not in TRAVERSAL_MODES:
+        raise ValueError(f"traversal mode must be one of {TRAVERSAL_MODES}, got {mode!r}")
+    _TRAVERSAL_MODE = mode
 
 
 def set_dense_neighbor_budget(nbytes: Optional[int]) -> None:
@@ -348,9 +365,13 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     center = geometry.center.contiguous().float()
     radius = geometry.radius.contiguous().float()
     max_extent = geometry.max_extent.contiguous().float()
+    mode = _TRAVERSAL_MODE
+    if mode not in TRAVERSAL_MODES:
+        raise ValueError(f"traversal mode must be one of {TRAVERSAL_MODES}, got {mode!r}")
+    walk_mode = L.WALK_LOG if mode == "log" else L.WALK_COUNT
     hint_wf, hint_log = _CAPACITY_HINTS.get((mac_type, float(theta)), (0.0, 0.0))
     cap = int(wf_capacity) if wf_capacity else max(32 * total + 65536, int(1.25 * hint_wf * total))
-    log_cap = max(8 * total + 65536, int(1.1 * hint_log * total))
+    log_cap = max(8 * total + 65536, int(1.1 * hint_log * total)) if walk_mode == L.WALK_LOG else 1
     cap = min(cap, (1 << 32) - 1)
     mac = _MAC_CODES[mac_type]
     root = int(torch.argmin(d.parent32).item()) if bool(
@@ -362,7 +383,8 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
         rc = lib.ygx_traverse_walk(
             L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32), L.ptr(d.right32),
             L.ptr(leafpos32), total, ni, mac, float(theta), float(dehnen_radius_scale), root,
-            cap, log_cap, stats.ctypes.data, flags.ctypes.data, L.ptr(ws), ws.numel(), st)
+            walk_mode, cap, log_cap, stats.ctypes.data, flags.ctypes.data, L.ptr(ws),
+            ws.numel(), st)
         f = int(flags[0])
         if f & (L.FLAG_QUEUE_OVERFLOW | L.FLAG_LOG_OVERFLOW) and rc == 0:
             if f & L.FLAG_QUEUE_OVERFLOW:
@@ -382,13 +404,15 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
             raise L.YgxError(f"traversal walk reported flags {f:#x}")
         break
     if not wf_capacity:
+        prev = _CAPACITY_HINTS.get((mac_type, float(theta)), (0.0, 0.0))
+        log_need = int(stats[L.TSTAT["log_need"]]) / total if walk_mode == L.WALK_LOG else prev[1]
         _CAPACITY_HINTS[(mac_type, float(theta))] = (
-            int(stats[L.TSTAT["wf_need"]]) / total, int(stats[L.TSTAT["log_need"]]) / total)
+            int(stats[L.TSTAT["wf_need"]]) / total, log_need)
     if timing:
         evs[1].record()
     s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
     LAST_WALK_STATS.clear()
-    LAST_WALK_STATS.update(s, wf_capacity=cap, log_capacity=log_cap)
+    LAST_WALK_STATS.update(s, wf_capacity=cap, log_capacity=log_cap, mode=mode)
     P, Q = s["far_total"], s["near_total"]
     node_offsets = torch.empty(total + 1, dtype=idt, device=dev)
     far_counts = torch.empty(total, dtype=idt, device=dev)
@@ -397,11 +421,19 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     near_counts = torch.empty(nl, dtype=idt, device=dev)
     far_src32 = torch.empty(max(P, 1), dtype=torch.int32, device=dev)
     near_nbr32 = torch.empty(max(Q, 1), dtype=torch.int32, device=dev)
-    L.check(lib.ygx_traverse_fill(
-        total, ni, cap, log_cap, P, Q, L.ptr(d.nbl32), L.ptr(leafpos32),
-        L.ptr(topology.level_offsets), num_levels, ib, L.ptr(node_offsets), L.ptr(far_counts),
-        L.ptr(level_offsets), L.ptr(near_offsets), L.ptr(near_counts), L.ptr(far_src32),
-        L.ptr(near_nbr32), L.ptr(ws), ws.numel(), st), "ygx_traverse_fill")
+    if walk_mode == L.WALK_LOG:
+        L.check(lib.ygx_traverse_fill(
+            total, ni, cap, log_cap, P, Q, L.ptr(d.nbl32), L.ptr(leafpos32),
+            L.ptr(topology.level_offsets), num_levels, ib, L.ptr(node_offsets),
+            L.ptr(far_counts), L.ptr(level_offsets), L.ptr(near_offsets), L.ptr(near_counts),
+            L.ptr(far_src32), L.ptr(near_nbr32), L.ptr(ws), ws.numel(), st), "ygx_traverse_fill")
+    else:
+        L.check(lib.ygx_traverse_fill_walk(
+            total, ni, mac, float(theta), root, cap, log_cap, s["gens"], P, Q, L.ptr(d.nbl32),
+            L.ptr(topology.level_offsets), num_levels, ib, L.ptr(node_offsets),
+            L.ptr(far_counts), L.ptr(level_offsets), L.ptr(near_offsets), L.ptr(near_counts),
+            L.ptr(far_src32), L.ptr(near_nbr32), L.ptr(ws), ws.numel(), st),
+            "ygx_traverse_fill_walk")
     if timing:
         evs[2].record()
     sources = torch.empty(P, dtype=idt, device=dev)
