@@ -62,6 +62,10 @@ enum {
 #define YGX_TSTAT_GENS 8        /* wavefront generations                       */
 #define YGX_TSTAT_WF_NEED 9     /* wf_capacity that would have fit             */
 #define YGX_TSTAT_LOG_NEED 10   /* log_capacity that would have fit            */
+#define YGX_TSTAT_OVF_ROWS 11   /* predicted walk: rows past their capacity    */
+#define YGX_TSTAT_OVF_ENTRIES 12 /* predicted walk: entries past the capacities */
+#define YGX_TSTAT_EXT_FAR 13    /* predicted walk: far extension entries       */
+#define YGX_TSTAT_EXT_NEAR 14   /* predicted walk: near extension entries      */
 
 #ifdef __cplusplus
 extern "C" {
@@ -250,15 +254,94 @@ int ygx_traverse_fill_walk(int64_t total, int64_t num_internal, int mac, float t
                            void* node_offsets, void* far_counts, void* level_offsets,
                            void* near_offsets, void* near_counts, int32_t* far_src32,
                            int32_t* near_nbr32, void* ws, size_t ws_bytes, cudaStream_t stream);
+/* Learned one-pass mode (no counterpart in the reference; it replaces the
+ * count walk of count-then-fill, _interactions_impl.py:2600-2939, by the
+ * capacities of ygx_predict_caps and stays exact by completing every row
+ * that outgrew its capacity):
+ * 1. ygx_traverse_pad_offsets: padded row offsets into the workspace;
+ *    sums_out (host, 2 words) = padded far / near totals.
+ * 2. ygx_traverse_walk_predicted: one walk writing the raw rows (buffers of
+ *    at least the padded totals); entries past a row's capacity are logged.
+ * 3. ygx_traverse_fill_predicted: offset tables, overflowed rows moved to the
+ *    extension area (raw buffers of padded total + YGX_TSTAT_EXT_* entries)
+ *    and completed; far_raw_off / near_raw_off receive the raw row starts for
+ *    ygx_traverse_finalize. */
+int ygx_traverse_pad_offsets(int64_t total, int64_t num_internal, int64_t wf_capacity,
+                             int64_t log_capacity, const int32_t* far_cap32,
+                             const int32_t* near_cap32, uint64_t* sums_out, void* ws,
+                             size_t ws_bytes, cudaStream_t stream);
+int ygx_traverse_walk_predicted(const float* center, const float* radius,
+                                const float* max_extent, const int32_t* left32,
+                                const int32_t* right32, const int32_t* leafpos32, int64_t total,
+                                int64_t num_internal, int mac, float theta,
+                                float dehnen_radius_scale, int root, int64_t wf_capacity,
+                                int64_t log_capacity, const int32_t* far_cap32,
+                                const int32_t* near_cap32, int32_t* far_raw32,
+                                int32_t* near_raw32, uint64_t* stats_out, uint32_t* flags_out,
+                                void* ws, size_t ws_bytes, cudaStream_t stream);
+int ygx_traverse_fill_predicted(int64_t total, int64_t num_internal, int64_t wf_capacity,
+                                int64_t log_capacity, const int32_t* far_cap32,
+                                const int32_t* near_cap32, int64_t far_raw_cap,
+                                int64_t near_raw_cap, const int32_t* nbl32,
+                                const void* tree_level_offsets, int num_levels, int index_bits,
+                                void* node_offsets, void* far_counts, void* level_offsets,
+                                void* near_offsets, void* near_counts, int32_t* far_raw32,
+                                int32_t* near_raw32, int64_t* far_raw_off, int64_t* near_raw_off,
+                                void* ws, size_t ws_bytes, cudaStream_t stream);
 /* Row finalize: canonical (ascending) order within each row, level-major
  * far sources/targets/target_levels, leaf-ordered near neighbours, and
- * optionally the dense neighbour_leaf_positions table (L x max_nbr). */
+ * optionally the dense neighbour_leaf_positions table (L x max_nbr).
+ * far_raw_off / near_raw_off (device int64 per row, may be null) say where
+ * each raw row starts when the raw rows are not at the output offsets (the
+ * predicted walk's padded rows). */
 int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capacity,
-                          int64_t log_capacity, const int32_t* level32, const int32_t* leafpos32, int index_bits,
-                          int32_t* far_src32, int32_t* near_nbr32, void* far_sources,
+                          int64_t log_capacity, const int32_t* level32, const int32_t* leafpos32,
+                          int index_bits, int32_t* far_src32, int32_t* near_nbr32,
+                          const int64_t* far_raw_off, const int64_t* near_raw_off,
+                          void* far_sources,
                           void* far_targets, void* target_levels, void* neighbors,
                           void* neighbor_leaf_positions, int64_t max_nbr, void* ws,
                           size_t ws_bytes, cudaStream_t stream);
+/* ---- learned row-capacity predictor (no counterpart in the reference) -----
+ * A per-node MLP (YGX_MLP_INPUTS -> 64 -> 64 -> 2, ReLU, fp32) that predicts
+ * log2(1 + far row length) and log2(1 + near row length) from the node's
+ * geometry, so the one-pass predicted walk can size its rows without the
+ * count walk of count-then-fill (_interactions_impl.py:2600-2939).
+ * Parameters: one float array of YGX_MLP_PARAMS (W1 [in x 64], b1, W2
+ * [64 x 64], b2, W3 [64 x 2], b3; row-major). */
+#define YGX_MLP_INPUTS 12
+#define YGX_MLP_PARAMS 5122
+int ygx_mlp_param_count(void);
+size_t ygx_mlp_workspace_size(int64_t batch);
+/* features[k * YGX_MLP_INPUTS + i] of every node (node_ranges inclusive,
+ * index dtype).  mac as in ygx_traverse_walk. */
+int ygx_node_features(const float* center, const float* radius, const float* max_extent,
+                      const int32_t* level32, const int32_t* parent32, int64_t total,
+                      int64_t num_internal, const void* node_ranges, int index_bits, int root,
+                      float theta, int mac, float* features, cudaStream_t stream);
+/* out[k * 2 + j] = MLP(features[k]). */
+int ygx_mlp_forward(const float* params, const float* features, int64_t n, float* out,
+                    cudaStream_t stream);
+/* Masked mean-squared-error gradients of one batch (targets / mask [batch x 2]);
+ * grads_out (YGX_MLP_PARAMS floats) and loss_out (1 float) are device
+ * pointers, either may be null. */
+int ygx_mlp_gradients(const float* params, const float* features, const float* targets,
+                      const float* mask, int64_t batch, float* grads_out, float* loss_out,
+                      void* ws, size_t ws_bytes, cudaStream_t stream);
+/* One Adam step (step >= 1, betas 0.9 / 0.999) on a batch. */
+int ygx_mlp_train_step(float* params, float* adam_m, float* adam_v, int step, float lr,
+                       const float* features, const float* targets, const float* mask,
+                       int64_t batch, float* loss_out, void* ws, size_t ws_bytes,
+                       cudaStream_t stream);
+/* Row capacities: far_cap32[node] and near_cap32[leaf position] =
+ * ceil(2^(prediction + slack) - 1) + add. */
+int ygx_predict_caps(const float* center, const float* radius, const float* max_extent,
+                     const int32_t* level32, const int32_t* parent32, const int32_t* leafpos32,
+                     int64_t total, int64_t num_internal, const void* node_ranges, int index_bits,
+                     int root, float theta, int mac, const float* params, float slack_far,
+                     float slack_near, int32_t add, int32_t* far_cap32, int32_t* near_cap32,
+                     cudaStream_t stream);
+
 int ygx_traverse_status(const void* ws, uint32_t* flags_out, cudaStream_t stream);
 
 #ifdef __cplusplus

@@ -1,0 +1,153 @@
+"""The learned capacity predictor on the GPU: its training kernels against the
+float64 NumPy reference (gradients, forward), its features against NumPy,
+that training lowers the loss, and that the learned one-pass traversal
+returns exactly the oracle's lists -- with the shipped weights, with a random
+predictor and with capacities so tight that most rows overflow."""
+
+import numpy as np
+import pytest
+
+from mlp_ref import forward as ref_forward
+from mlp_ref import loss_and_grad
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a, dev):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def _batch(seed, n):
+    from yggdrax_b200 import predictor
+
+    rng = np.random.default_rng(seed)
+    p = predictor.init_params(seed).astype(np.float32)
+    p += rng.normal(0, 0.02, p.shape).astype(np.float32)  # non-zero biases
+    X = rng.normal(0, 1, (n, predictor.N_INPUTS)).astype(np.float32)
+    Y = rng.normal(0, 2, (n, 2)).astype(np.float32)
+    M = (rng.uniform(size=(n, 2)) > 0.25).astype(np.float32)
+    return p, X, Y, M
+
+
+def test_mlp_gradients_match_reference(cuda_device):
+    from yggdrax_b200 import predictor
+
+    p, X, Y, M = _batch(1, 3000)
+    loss, g = predictor.gradients(_t(p, cuda_device), _t(X, cuda_device), _t(Y, cuda_device),
+                                  _t(M, cuda_device))
+    ref_loss, ref_g = loss_and_grad(p.astype(np.float64), X.astype(np.float64), Y, M)
+    g = g.cpu().numpy().astype(np.float64)
+    # fp32 kernels vs the float64 reference
+    assert abs(loss - ref_loss) <= 1e-4 * abs(ref_loss)
+    scale = np.abs(ref_g).max()
+    np.testing.assert_allclose(g, ref_g, rtol=1e-3, atol=1e-5 * scale)
+
+
+def test_mlp_forward_matches_reference(cuda_device):
+    from yggdrax_b200 import predictor
+
+    p, X, _, _ = _batch(2, 5000)
+    out = predictor.forward(_t(p, cuda_device), _t(X, cuda_device)).cpu().numpy()
+    ref, _ = ref_forward(p.astype(np.float64), X.astype(np.float64))
+    np.testing.assert_allclose(out, ref, rtol=1e-4, atol=1e-4)
+
+
+def test_training_lowers_the_loss(cuda_device):
+    from yggdrax_b200 import predictor
+
+    rng = np.random.default_rng(3)
+    X = rng.normal(0, 1, (20000, predictor.N_INPUTS)).astype(np.float32)
+    Y = np.stack([np.sin(X[:, 0]) + X[:, 1] ** 2, np.abs(X[:, 2]) - X[:, 3]], 1).astype(np.float32)
+    M = np.ones_like(Y)
+    Xd, Yd, Md = _t(X, cuda_device), _t(Y, cuda_device), _t(M, cuda_device)
+    p0 = predictor.init_params(0)
+    loss0, _ = predictor.gradients(_t(p0, cuda_device), Xd, Yd, Md)
+    p = predictor.train(Xd, Yd, Md, steps=400, batch=4096, lr=3e-3, lr_end=3e-4, params=p0)
+    loss1, _ = predictor.gradients(p, Xd, Yd, Md)
+    assert loss1 < 0.1 * loss0, (loss0, loss1)
+
+
+def test_node_features_match_numpy(cuda_device):
+    import yggdrax_b200 as yb
+    from yggdrax_b200 import inputs, predictor
+    from yggdrax_b200.tree import _dev_of
+
+    pos, mass = inputs.plummer(50_000, 21)
+    P, M = _t(pos, cuda_device), _t(mass, cuda_device)
+    t, ps = yb.build_tree(P, M, leaf_size=16, return_reordered=True)[:2]
+    g = yb.compute_tree_geometry(t, ps)
+    X = predictor.node_features(t, g, 0.6, "dehnen").cpu().numpy()
+    c = g.center.cpu().numpy().astype(np.float64)
+    r = g.radius.cpu().numpy().astype(np.float64)
+    e = g.max_extent.cpu().numpy().astype(np.float64)
+    d = _dev_of(t)
+    lvl = d.level32.cpu().numpy()
+    par = d.parent32.cpu().numpy()
+    rng_ = t.node_ranges.cpu().numpy()
+    ni = int(t.left_child.shape[0])
+    root = 0
+    dist = np.linalg.norm(c - c[root], axis=1)
+    cnt = np.maximum(rng_[:, 1] - rng_[:, 0] + 1, 1)
+    parr = np.where(par >= 0, par, np.arange(par.size))
+    nleaves = r.size - ni
+    ref = np.stack([np.log2(r / r[root]), np.log2(e / e[root]), lvl / 16.0,
+                    (np.arange(r.size) >= ni).astype(np.float64), np.log2(cnt) / 8.0,
+                    np.log2(r[parr] / r[root]), np.log2(dist / r[root] + 1e-3),
+                    np.log2(r / (dist + 1e-3 * r[root])), np.full(r.size, 0.6),
+                    np.zeros(r.size), np.full(r.size, np.log2(nleaves) * 0.05),
+                    np.log2(cnt / cnt[parr])], 1)
+    np.testing.assert_allclose(X, ref, rtol=1e-4, atol=1e-4)
+
+
+def _learned_lists(cuda_device, oracle, params=None, cal=None, n=120_000, seed=31):
+    import yggdrax_b200 as yb
+    from test_gpu_parity import _compare_lists
+    from yggdrax_b200 import inputs, predictor
+    from yggdrax_b200.interactions import LAST_WALK_STATS
+
+    pos, mass = inputs.plummer(n, seed)
+    P, M = _t(pos, cuda_device), _t(mass, cuda_device)
+    t, ps = yb.build_tree(P, M, leaf_size=16, return_reordered=True)[:2]
+    g = yb.compute_tree_geometry(t, ps)
+    if params is not None:
+        predictor.set_predictor(params, cal)
+    yb.set_traversal_mode("learned")
+    try:
+        gi, gn = yb.build_interactions_and_neighbors(t, g, theta=0.6, mac_type="dehnen")
+        stats = dict(LAST_WALK_STATS)
+    finally:
+        yb.set_traversal_mode("log")
+        predictor.set_predictor(None)
+    ot = oracle.build_tree(pos, mass, leaf_size=16)
+    og = oracle.compute_tree_geometry(ot, ot.positions_sorted)
+    r = oracle.build_interactions_and_neighbors(ot, og, theta=0.6, mac_type="dehnen")
+    _compare_lists(gi, gn, r)
+    return stats
+
+
+def test_learned_mode_exact_with_shipped_weights(cuda_device, oracle):
+    stats = _learned_lists(cuda_device, oracle)
+    assert stats["mode"] == "learned"
+    # the shipped predictor sizes nearly every row right
+    assert stats["overflow_row_fraction"] < 0.2
+    assert stats["over_allocation"] < 8.0
+
+
+def test_learned_mode_exact_when_most_rows_overflow(cuda_device, oracle):
+    """A random predictor with negative slack: most rows outgrow their
+    capacity and are completed from the log."""
+    from yggdrax_b200 import predictor
+
+    stats = _learned_lists(cuda_device, oracle, predictor.init_params(7),
+                           dict(slack_far=-6.0, slack_near=-6.0, add=1))
+    assert stats["ovf_rows"] > 0 and stats["overflow_row_fraction"] > 0.3
+
+
+def test_learned_mode_exact_with_generous_capacities(cuda_device, oracle):
+    from yggdrax_b200 import predictor
+
+    stats = _learned_lists(cuda_device, oracle, predictor.init_params(8),
+                           dict(slack_far=12.0, slack_near=12.0, add=64), n=40_000)
+    assert stats["ovf_rows"] == 0

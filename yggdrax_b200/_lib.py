@@ -41,7 +41,8 @@ WALK_COUNT = 1
 
 TSTAT_WORDS = 16
 TSTAT = dict(far_total=0, near_total=1, max_far=2, max_near=3, accept=4, near=5, refine=6,
-             max_wf=7, gens=8, wf_need=9, log_need=10)
+             max_wf=7, gens=8, wf_need=9, log_need=10, ovf_rows=11, ovf_entries=12,
+             ext_far=13, ext_near=14)
 
 P = ctypes.c_void_p
 I64 = ctypes.c_int64
@@ -83,7 +84,21 @@ _SIGS = {
                                      I32, P, P, P, P, P, P, P, P, SZ, P]),
     "ygx_traverse_fill": (I32, [I64, I64, I64, I64, I64, I64, P, P, P, I32, I32, P, P, P, P, P,
                                 P, P, P, SZ, P]),
-    "ygx_traverse_finalize": (I32, [I64, I64, I64, I64, P, P, I32, P, P, P, P, P, P, P, I64, P, SZ,
+    "ygx_traverse_pad_offsets": (I32, [I64, I64, I64, I64, P, P, P, P, SZ, P]),
+    "ygx_traverse_walk_predicted": (I32, [P, P, P, P, P, P, I64, I64, I32, F32, F32, I32, I64,
+                                          I64, P, P, P, P, P, P, P, SZ, P]),
+    "ygx_traverse_fill_predicted": (I32, [I64, I64, I64, I64, P, P, I64, I64, P, P, I32, I32, P,
+                                          P, P, P, P, P, P, P, P, P, SZ, P]),
+    "ygx_mlp_param_count": (I32, []),
+    "ygx_mlp_workspace_size": (SZ, [I64]),
+    "ygx_node_features": (I32, [P, P, P, P, P, I64, I64, P, I32, I32, F32, I32, P, P]),
+    "ygx_mlp_forward": (I32, [P, P, I64, P, P]),
+    "ygx_mlp_gradients": (I32, [P, P, P, P, I64, P, P, P, SZ, P]),
+    "ygx_mlp_train_step": (I32, [P, P, P, I32, F32, P, P, P, I64, P, P, SZ, P]),
+    "ygx_predict_caps": (I32, [P, P, P, P, P, P, I64, I64, P, I32, I32, F32, I32, P, F32, F32,
+                               I32, P, P, P]),
+    "ygx_traverse_finalize": (I32, [I64, I64, I64, I64, P, P, I32, P, P, P, P, P, P, P, P, P, I64,
+                                    P, SZ,
                                     P]),
 }
 

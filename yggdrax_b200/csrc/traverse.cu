@@ -43,6 +43,10 @@ enum {
   kStatGens = 8,
   kStatWfNeed = 9,
   kStatLogNeed = 10,
+  kStatOvfRows = 11,
+  kStatOvfEntries = 12,
+  kStatExtFar = 13,
+  kStatExtNear = 14,
   kStatWords = 16
 };
 
@@ -460,6 +464,140 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---- predicted mode ----------------------------------------------------------
+
+__global__ void k_pad_ends(const int64_t* __restrict__ pad, const int32_t* __restrict__ cap,
+                           int64_t n, unsigned long long* __restrict__ end,
+                           unsigned long long* __restrict__ pos) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    end[k] = (unsigned long long)(pad[k] + cap[k]);
+    pos[k] = (unsigned long long)pad[k];
+  }
+}
+
+// Exact row lengths from the cursors of the predicted walk; rows that
+// outgrew their capacity get their full length in ext_cnt (they move to the
+// extension area), the others 0.
+__global__ void k_pred_counts(const unsigned long long* __restrict__ pos,
+                              const int64_t* __restrict__ pad, const int32_t* __restrict__ cap,
+                              int64_t n, int32_t* __restrict__ cnt, int32_t* __restrict__ ext_cnt,
+                              unsigned long long* __restrict__ stats, int ext_word) {
+  unsigned long long rows = 0, entries = 0, ext = 0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = (int64_t)pos[k] - pad[k];
+    cnt[k] = (int32_t)c;
+    const bool over = c > cap[k];
+    ext_cnt[k] = over ? (int32_t)c : 0;
+    if (over) {
+      ++rows;
+      entries += (unsigned long long)(c - cap[k]);
+      ext += (unsigned long long)c;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    rows += __shfl_xor_sync(0xffffffffu, rows, o);
+    entries += __shfl_xor_sync(0xffffffffu, entries, o);
+    ext += __shfl_xor_sync(0xffffffffu, ext, o);
+  }
+  if ((threadIdx.x & 31) == 0 && rows) {
+    atomicAdd(&stats[kStatOvfRows], rows);
+    atomicAdd(&stats[kStatOvfEntries], entries);
+    atomicAdd(&stats[ext_word], ext);
+  }
+}
+
+// Read offsets of the raw rows: the padded row, or for a row that outgrew
+// its capacity a fresh place in the extension area (after all padded rows)
+// that will hold its first cap entries (k_relocate_copy) followed by the
+// entries the walk logged (appended at the cursor left at ext + cap).  Rows
+// that move are listed for the copy.
+__global__ void k_relocate_mark(const int64_t* __restrict__ pad, const int32_t* __restrict__ cap,
+                                const int32_t* __restrict__ ext_cnt,
+                                const int64_t* __restrict__ ext_off, int64_t n, int64_t raw_cap,
+                                unsigned long long* __restrict__ pos,
+                                int64_t* __restrict__ raw_off, int32_t* __restrict__ moved,
+                                uint32_t* __restrict__ n_moved, uint32_t* __restrict__ status,
+                                uint32_t overflow_flag) {
+  const int64_t ext_base = pad[n];
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    if (ext_cnt[k] == 0) {
+      raw_off[k] = pad[k];
+      continue;
+    }
+    const int64_t dst = ext_base + ext_off[k];
+    if (dst + ext_cnt[k] > raw_cap) {
+      raise_flag(status, overflow_flag);
+      raw_off[k] = pad[k];
+      continue;
+    }
+    raw_off[k] = dst;
+    pos[k] = (unsigned long long)(dst + cap[k]);
+    moved[atomicAdd(n_moved, 1u)] = (int32_t)k;
+  }
+}
+
+// One CTA per moved row copies its first cap entries to the extension area.
+__global__ void __launch_bounds__(256)
+    k_relocate_copy(const int32_t* __restrict__ moved, const uint32_t* __restrict__ n_moved,
+                    const int64_t* __restrict__ pad, const int32_t* __restrict__ cap,
+                    const int64_t* __restrict__ raw_off, int32_t* __restrict__ raw) {
+  const uint32_t nm = *n_moved;
+  for (uint32_t b = blockIdx.x; b < nm; b += gridDim.x) {
+    const int32_t k = moved[b];
+    const int64_t src = pad[k], dst = raw_off[k];
+    for (int64_t e = threadIdx.x; e < cap[k]; e += blockDim.x) raw[dst + e] = raw[src + e];
+  }
+}
+
+// Logged overflow entries (row key, value) -> their rows' extension tails.
+__global__ void k_ovf_scatter(const int2* __restrict__ log,
+                              const unsigned long long* __restrict__ log_cnt,
+                              unsigned long long LR, int32_t total,
+                              unsigned long long* __restrict__ far_pos,
+                              unsigned long long* __restrict__ near_pos,
+                              int32_t* __restrict__ far_raw, int32_t* __restrict__ near_raw,
+                              const int64_t* __restrict__ far_end,
+                              const int64_t* __restrict__ near_end,
+                              uint32_t* __restrict__ status) {
+  for (int b = blockIdx.x; b < kWalkGrid; b += gridDim.x) {
+    const unsigned long long n = log_cnt[b] < LR ? log_cnt[b] : LR;
+    const int2* src = log + (size_t)b * LR;
+    for (unsigned long long i = threadIdx.x; i < n; i += blockDim.x) {
+      const int2 e = src[i];
+      if (e.x < total) {
+        const unsigned long long p = atomicAdd(&far_pos[e.x], 1ull);
+        if ((long long)p < far_end[e.x]) far_raw[p] = e.y;
+        else raise_flag(status, kFlagFarOverflow);
+      } else {
+        const int r = e.x - total;
+        const unsigned long long p = atomicAdd(&near_pos[r], 1ull);
+        if ((long long)p < near_end[r]) near_raw[p] = e.y;
+        else raise_flag(status, kFlagNearOverflow);
+      }
+    }
+  }
+}
+
+// Row end for the extension tails: raw_off + count.
+__global__ void k_raw_ends(const int64_t* __restrict__ raw_off, const int32_t* __restrict__ cnt,
+                           int64_t n, int64_t* __restrict__ end) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x)
+    end[k] = raw_off[k] + cnt[k];
+}
+
+// Every relocated row's cursor must end at its row end.
+__global__ void k_check_ext(const unsigned long long* __restrict__ pos,
+                            const int64_t* __restrict__ end, const int32_t* __restrict__ ext_cnt,
+                            int64_t n, uint32_t* __restrict__ status, uint32_t flag) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x)
+    if (ext_cnt[k] && (long long)pos[k] != end[k]) raise_flag(status, flag);
+}
+
 // Every cursor must end exactly at its row's end (fill == count).
 __global__ void k_check_cursors(const int64_t* __restrict__ far_off,
                                 const int32_t* __restrict__ far_cnt,
@@ -639,7 +777,8 @@ __device__ __forceinline__ void emit_row(const int32_t* a, int64_t n, int64_t of
 // lane and only the steps with j >= R exchange across lanes (shuffles).
 // The row is padded with INT32_MAX to 32*R entries.
 template <int R>
-__device__ __forceinline__ void warp_sort_row(const int32_t* __restrict__ raw, int64_t off,
+__device__ __forceinline__ void warp_sort_row(const int32_t* __restrict__ raw, int64_t roff,
+                                              int64_t off,
                                               int n, int index_bits, void* vals_out,
                                               void* tgt_out, void* lvl_out, int32_t tgt,
                                               int32_t lvl, int lane, int32_t* __restrict__ sm) {
@@ -648,7 +787,7 @@ __device__ __forceinline__ void warp_sort_row(const int32_t* __restrict__ raw, i
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int e = r * 32 + lane;
-    sm[(e >> LOGR) * S + (e & (R - 1))] = e < n ? raw[off + e] : INT32_MAX;
+    sm[(e >> LOGR) * S + (e & (R - 1))] = e < n ? raw[roff + e] : INT32_MAX;
   }
   __syncwarp();
   int32_t v[R];
@@ -744,13 +883,15 @@ __global__ void __launch_bounds__(256, R >= 32 ? 2 : (R >= 16 ? 3 : 4))
     k_rows_class(const int32_t* __restrict__ list, const uint32_t* __restrict__ list_n,
                  const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
                  const int32_t* __restrict__ row_level, const int32_t* __restrict__ raw,
-                 int index_bits, void* vals_out, void* tgt_out, void* lvl_out) {
+                 const int64_t* __restrict__ raw_off, int index_bits, void* vals_out,
+                 void* tgt_out, void* lvl_out) {
   __shared__ int32_t s_rows[8][32 * (R + 1)];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t nm = *list_n;
   for (uint32_t b = blockIdx.x * 8 + w; b < nm; b += gridDim.x * 8) {
     const int32_t r = list[b];
-    warp_sort_row<R>(raw, row_off[r], row_cnt[r], index_bits, vals_out, tgt_out, lvl_out, r,
+    warp_sort_row<R>(raw, raw_off ? raw_off[r] : row_off[r], row_off[r], row_cnt[r],
+                     index_bits, vals_out, tgt_out, lvl_out, r,
                      row_level ? row_level[r] : 0, lane, s_rows[w]);
   }
 }
@@ -811,8 +952,9 @@ __global__ void __launch_bounds__(kBigThreads, 3)
     k_rows_big(const int32_t* __restrict__ big_rows, uint32_t* __restrict__ n_big,
                int64_t list_cap, const int64_t* __restrict__ row_off,
                const int32_t* __restrict__ row_cnt, const int32_t* __restrict__ row_level,
-               int32_t* __restrict__ raw, int index_bits, void* vals_out, void* tgt_out,
-               void* lvl_out, uint32_t* __restrict__ bitmaps, int64_t universe) {
+               int32_t* __restrict__ raw, const int64_t* __restrict__ raw_off, int index_bits,
+               void* vals_out, void* tgt_out, void* lvl_out, uint32_t* __restrict__ bitmaps,
+               int64_t universe) {
   extern __shared__ uint32_t s_dyn[];  // kBlockRowCap words: bitmap, or a row to sort
   __shared__ uint32_t s_sum[kSumWords];
   __shared__ int32_t s_cc[kSumWords];  // per-chunk counts, then bases (< n < 2^31)
@@ -840,11 +982,12 @@ __global__ void __launch_bounds__(kBigThreads, 3)
     if (b >= n_long + n_mid) break;
     const int32_t r = b < n_long ? big_rows[b] : big_rows[list_cap - 1 - (b - n_long)];
     const int64_t off = row_off[r];
+    const int64_t roff = raw_off ? raw_off[r] : off;  // where the raw row is read
     const int64_t n = row_cnt[r];
     const int32_t lvl = row_level ? row_level[r] : 0;
     int32_t vmin = INT32_MAX, vmax = INT32_MIN;
     for (int64_t k = tid; k < n; k += nt) {
-      const int32_t v = raw[off + k];
+      const int32_t v = raw[roff + k];
       vmin = v < vmin ? v : vmin;
       vmax = v > vmax ? v : vmax;
     }
@@ -871,7 +1014,7 @@ __global__ void __launch_bounds__(kBigThreads, 3)
       uint32_t* bm = words <= kBlockRowCap ? s_dyn : gbm;
       bool dup = false;
       for (int64_t k = tid; k < n; k += nt) {
-        const uint32_t v = (uint32_t)(raw[off + k] - vmin);
+        const uint32_t v = (uint32_t)(raw[roff + k] - vmin);
         const uint32_t bit = 1u << (v & 31);
         if (atomicOr(&bm[v >> 5], bit) & bit) dup = true;
         atomicOr(&s_sum[v >> 10], 1u << ((v >> 5) & 31));
@@ -881,13 +1024,13 @@ __global__ void __launch_bounds__(kBigThreads, 3)
       if (s_dup) {
         // undo the bits; the row goes to the bitonic network
         for (int64_t k = tid; k < n; k += nt) {
-          const uint32_t v = (uint32_t)(raw[off + k] - vmin);
+          const uint32_t v = (uint32_t)(raw[roff + k] - vmin);
           bm[v >> 5] = 0u;
         }
         for (int64_t w = tid; w < swords; w += nt) s_sum[w] = 0u;
         __syncthreads();
       } else {
-        // Non-empty words in ascending order -> raw[off, off + m).
+        // Non-empty words in ascending order -> raw[roff, roff + m).
         constexpr int kSumPer = kSumWords / kBigThreads;
         int64_t c = 0;
 #pragma unroll
@@ -904,7 +1047,7 @@ __global__ void __launch_bounds__(kBigThreads, 3)
           while (bits) {
             const int bit = __ffs(bits) - 1;
             bits &= bits - 1;
-            raw[off + base++] = (int32_t)(sw * 32 + bit);
+            raw[roff + base++] = (int32_t)(sw * 32 + bit);
           }
         }
         __syncthreads();
@@ -912,7 +1055,7 @@ __global__ void __launch_bounds__(kBigThreads, 3)
         const int64_t nch = (m + 31) >> 5;
         for (int64_t ch = warp; ch < nch; ch += nwarps) {
           const int64_t j = ch * 32 + lane;
-          int cnt = j < m ? __popc(bm[raw[off + j]]) : 0;
+          int cnt = j < m ? __popc(bm[raw[roff + j]]) : 0;
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
           if (lane == 0) s_cc[ch] = cnt;
@@ -939,7 +1082,7 @@ __global__ void __launch_bounds__(kBigThreads, 3)
         __syncthreads();
         for (int64_t ch = warp; ch < nch; ch += nwarps) {
           const int64_t j = ch * 32 + lane;
-          const int32_t wi = j < m ? raw[off + j] : 0;
+          const int32_t wi = j < m ? raw[roff + j] : 0;
           const uint32_t word = j < m ? bm[wi] : 0u;
           const int c1 = __popc(word);
           int incl = c1;
@@ -973,7 +1116,7 @@ __global__ void __launch_bounds__(kBigThreads, 3)
           }
         }
         __syncthreads();
-        for (int64_t j = tid; j < m; j += nt) bm[raw[off + j]] = 0u;
+        for (int64_t j = tid; j < m; j += nt) bm[raw[roff + j]] = 0u;
         for (int64_t w = tid; w < swords; w += nt) s_sum[w] = 0u;
         __syncthreads();
         sorted = true;
@@ -982,14 +1125,14 @@ __global__ void __launch_bounds__(kBigThreads, 3)
     if (!sorted) {
       if (n <= kBlockRowCap) {
         int32_t* a = reinterpret_cast<int32_t*>(s_dyn);
-        for (int64_t k = tid; k < n; k += nt) a[k] = raw[off + k];
+        for (int64_t k = tid; k < n; k += nt) a[k] = raw[roff + k];
         __syncthreads();
         mirrored_bitonic<true>(a, n, tid, nt);
         emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, r, lvl, tid, nt);
         __syncthreads();
         for (int64_t k = tid; k < n; k += nt) s_dyn[k] = 0u;  // bitmap stays zero
       } else {
-        int32_t* a = raw + off;
+        int32_t* a = raw + roff;
         mirrored_bitonic<true>(a, n, tid, nt);
         emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, r, lvl, tid, nt);
       }
@@ -1039,6 +1182,19 @@ struct TravScratch {
   unsigned long long* log_cnt;
   int2* log;
   unsigned long long log_region;
+  // predicted mode
+  int64_t* pad_far;   // total + 1
+  int64_t* pad_near;  // L + 1
+  unsigned long long* end_far;
+  unsigned long long* end_near;
+  int32_t* ext_far_cnt;
+  int32_t* ext_near_cnt;
+  int64_t* ext_far_off;   // total + 1
+  int64_t* ext_near_off;  // L + 1
+  int64_t* raw_off_far;
+  int64_t* raw_off_near;
+  int64_t* raw_end_far;
+  int64_t* raw_end_near;
 };
 
 constexpr int kMaxGens = 4096;
@@ -1084,6 +1240,18 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap, i
   s.log_cnt = a.take<unsigned long long>(kWalkGrid);
   s.log_region = (unsigned long long)log_region_capacity(log_cap);
   s.log = a.take<int2>((size_t)s.log_region * kWalkGrid);
+  s.pad_far = a.take<int64_t>(total + 1);
+  s.pad_near = a.take<int64_t>(L + 1);
+  s.end_far = a.take<unsigned long long>(total);
+  s.end_near = a.take<unsigned long long>(L);
+  s.ext_far_cnt = a.take<int32_t>(total);
+  s.ext_near_cnt = a.take<int32_t>(L);
+  s.ext_far_off = a.take<int64_t>(total + 1);
+  s.ext_near_off = a.take<int64_t>(L + 1);
+  s.raw_off_far = a.take<int64_t>(total);
+  s.raw_off_near = a.take<int64_t>(L);
+  s.raw_end_far = a.take<int64_t>(total);
+  s.raw_end_near = a.take<int64_t>(L);
   return s;
 }
 
@@ -1353,6 +1521,186 @@ int ygx_traverse_fill_walk(int64_t total, int64_t num_internal, int mac, float t
   return YGX_OK;
 }
 
+// ---- predicted (learned one-pass) mode ---------------------------------------
+
+// Padded row offsets from predicted capacities (far_cap32[node],
+// near_cap32[leaf position]) into the workspace; sums_out (host, 2 words)
+// gets the padded totals, which the raw row buffers must hold at least.
+// Synchronizes the stream.
+int ygx_traverse_pad_offsets(int64_t total, int64_t num_internal, int64_t wf_capacity,
+                             int64_t log_capacity, const int32_t* far_cap32,
+                             const int32_t* near_cap32, uint64_t* sums_out, void* ws,
+                             size_t ws_bytes, cudaStream_t stream) {
+  if (total < 3 || num_internal < 1 || !far_cap32 || !near_cap32 || !sums_out) return YGX_ERR_ARG;
+  const int64_t L = total - num_internal;
+  ygx::TravScratch s;
+  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity, log_capacity);
+  if (rc) return rc;
+  if ((rc = ygx::exclusive_scan<int32_t>(far_cap32, total, s.pad_far, s.scan_tmp, stream)))
+    return rc;
+  if ((rc = ygx::exclusive_scan<int32_t>(near_cap32, L, s.pad_near, s.scan_tmp, stream)))
+    return rc;
+  int64_t sums[2];
+  if (cudaMemcpyAsync(&sums[0], s.pad_far + total, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                      stream) != cudaSuccess ||
+      cudaMemcpyAsync(&sums[1], s.pad_near + L, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                      stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  sums_out[0] = (uint64_t)sums[0];
+  sums_out[1] = (uint64_t)sums[1];
+  return YGX_OK;
+}
+
+// One-pass walk into the padded rows set up by ygx_traverse_pad_offsets on
+// the same workspace (far_cap32 / near_cap32 are the same capacities).
+// Entries past a row's capacity go to the pair log.  Afterwards the
+// workspace holds the exact row lengths; stats_out adds YGX_TSTAT_OVF_ROWS /
+// _OVF_ENTRIES (rows that outgrew their capacity, entries past it) and
+// _EXT_FAR / _EXT_NEAR (extension space ygx_traverse_fill_predicted needs
+// beyond the padded totals).  Flags as in ygx_traverse_walk.  Synchronizes.
+int ygx_traverse_walk_predicted(const float* center, const float* radius,
+                                const float* max_extent, const int32_t* left32,
+                                const int32_t* right32, const int32_t* leafpos32, int64_t total,
+                                int64_t num_internal, int mac, float theta,
+                                float dehnen_radius_scale, int root, int64_t wf_capacity,
+                                int64_t log_capacity, const int32_t* far_cap32,
+                                const int32_t* near_cap32, int32_t* far_raw32,
+                                int32_t* near_raw32, uint64_t* stats_out, uint32_t* flags_out,
+                                void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (total < 3 || 2 * total > INT32_MAX || num_internal < 1 || mac < 0 || mac > 2 || root < 0 ||
+      root >= total || !far_cap32 || !near_cap32 || !far_raw32 || !near_raw32 || !stats_out ||
+      !flags_out)
+    return YGX_ERR_ARG;
+  const int64_t L = total - num_internal;
+  ygx::TravScratch s;
+  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity, log_capacity);
+  if (rc) return rc;
+  const float th = theta;
+  const float theta_sq = th * th;
+  const float theta_r = sqrtf(theta_sq);
+  if (cudaMemsetAsync(s.status, 0, (char*)(s.n_big + 64) - (char*)s.status, stream) !=
+          cudaSuccess ||
+      cudaMemsetAsync(s.log_cnt, 0, sizeof(unsigned long long) * ygx::kWalkGrid, stream) !=
+          cudaSuccess)
+    return YGX_ERR_CUDA;
+  ygx::k_node_recs<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      center, radius, max_extent, left32, right32, leafpos32, total, mac, dehnen_radius_scale,
+      s.recs, s.status);
+  YGX_CHECK_LAUNCH();
+  ygx::k_pad_ends<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.pad_far, far_cap32, total,
+                                                                 s.end_far, s.far_pos);
+  YGX_CHECK_LAUNCH();
+  ygx::k_pad_ends<<<ygx::grid_for(L, 256), 256, 0, stream>>>(s.pad_near, near_cap32, L,
+                                                             s.end_near, s.near_pos);
+  YGX_CHECK_LAUNCH();
+  ygx::RowSink sink = ygx::no_sink();
+  sink.far_pos = s.far_pos;
+  sink.near_pos = s.near_pos;
+  sink.far_end = s.end_far;
+  sink.near_end = s.end_near;
+  sink.far_src = far_raw32;
+  sink.near_nbr = near_raw32;
+  int gen = 0;
+  rc = ygx::run_gens(ygx::kWalkPred, mac, s, (int32_t)num_internal, (int32_t)total, theta_sq,
+                     theta_r, root, (uint32_t)wf_capacity, sink, -1, &gen, stream);
+  if (rc == YGX_ERR_QUEUE_OVERFLOW) flags_out[0] = ygx::kFlagQueueOverflow;
+  if (rc) return rc;
+  ygx::k_pred_counts<<<ygx::grid_for(total, 256, ygx::kNumSMs * 4), 256, 0, stream>>>(
+      s.far_pos, s.pad_far, far_cap32, total, s.far_cnt, s.ext_far_cnt, s.stats,
+      ygx::kStatExtFar);
+  YGX_CHECK_LAUNCH();
+  ygx::k_pred_counts<<<ygx::grid_for(L, 256, ygx::kNumSMs * 4), 256, 0, stream>>>(
+      s.near_pos, s.pad_near, near_cap32, L, s.near_cnt, s.ext_near_cnt, s.stats,
+      ygx::kStatExtNear);
+  YGX_CHECK_LAUNCH();
+  ygx::k_count_stats<<<ygx::grid_for(total, 256, ygx::kNumSMs * 4), 256, 0, stream>>>(
+      s.far_cnt, total, s.near_cnt, L, s.sizes, gen, s.log_cnt, s.stats);
+  YGX_CHECK_LAUNCH();
+  if (cudaMemcpyAsync(stats_out, s.stats, sizeof(uint64_t) * YGX_TSTAT_WORDS,
+                      cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaMemcpyAsync(flags_out, s.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  return YGX_OK;
+}
+
+// After ygx_traverse_walk_predicted without overflow flags: the offset
+// tables as in ygx_traverse_fill; rows that outgrew their capacity moved to
+// the extension area behind the padded rows (raw buffers of far_raw_cap /
+// near_raw_cap entries, at least padded total + YGX_TSTAT_EXT_*) and
+// completed from the log; far_raw_off / near_raw_off (device int64 per row)
+// receive where each raw row starts, for ygx_traverse_finalize.  Does not
+// synchronize.
+int ygx_traverse_fill_predicted(int64_t total, int64_t num_internal, int64_t wf_capacity,
+                                int64_t log_capacity, const int32_t* far_cap32,
+                                const int32_t* near_cap32, int64_t far_raw_cap,
+                                int64_t near_raw_cap, const int32_t* nbl32,
+                                const void* tree_level_offsets, int num_levels, int index_bits,
+                                void* node_offsets, void* far_counts, void* level_offsets,
+                                void* near_offsets, void* near_counts, int32_t* far_raw32,
+                                int32_t* near_raw32, int64_t* far_raw_off, int64_t* near_raw_off,
+                                void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (total < 3 || 2 * total > INT32_MAX || num_internal < 1 || !far_cap32 || !near_cap32 ||
+      !far_raw32 || !near_raw32 || !far_raw_off || !near_raw_off ||
+      (index_bits != 32 && index_bits != 64))
+    return YGX_ERR_ARG;
+  const int64_t L = total - num_internal;
+  ygx::TravScratch s;
+  int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity, log_capacity);
+  if (rc) return rc;
+  rc = ygx::row_offsets(s, total, L, nbl32, tree_level_offsets, num_levels, index_bits,
+                        node_offsets, far_counts, level_offsets, near_offsets, near_counts,
+                        stream);
+  if (rc) return rc;
+  if ((rc = ygx::exclusive_scan<int32_t>(s.ext_far_cnt, total, s.ext_far_off, s.scan_tmp, stream)))
+    return rc;
+  if ((rc = ygx::exclusive_scan<int32_t>(s.ext_near_cnt, L, s.ext_near_off, s.scan_tmp, stream)))
+    return rc;
+  // moved-row lists: far rows in big_rows, near rows in class_rows (both
+  // hold max(total, L) entries and are free until the finalize); counters
+  // in n_big[10] / n_big[11]
+  if (cudaMemsetAsync(s.n_big + 10, 0, 2 * sizeof(uint32_t), stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  ygx::k_relocate_mark<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      s.pad_far, far_cap32, s.ext_far_cnt, s.ext_far_off, total, far_raw_cap, s.far_pos,
+      s.raw_off_far, s.big_rows, s.n_big + 10, s.status, ygx::kFlagFarOverflow);
+  YGX_CHECK_LAUNCH();
+  ygx::k_relocate_mark<<<ygx::grid_for(L, 256), 256, 0, stream>>>(
+      s.pad_near, near_cap32, s.ext_near_cnt, s.ext_near_off, L, near_raw_cap, s.near_pos,
+      s.raw_off_near, s.class_rows, s.n_big + 11, s.status, ygx::kFlagNearOverflow);
+  YGX_CHECK_LAUNCH();
+  ygx::k_relocate_copy<<<ygx::kNumSMs * 8, 256, 0, stream>>>(s.big_rows, s.n_big + 10, s.pad_far,
+                                                            far_cap32, s.raw_off_far, far_raw32);
+  YGX_CHECK_LAUNCH();
+  ygx::k_relocate_copy<<<ygx::kNumSMs * 8, 256, 0, stream>>>(
+      s.class_rows, s.n_big + 11, s.pad_near, near_cap32, s.raw_off_near, near_raw32);
+  YGX_CHECK_LAUNCH();
+  ygx::k_raw_ends<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.raw_off_far, s.far_cnt, total,
+                                                                 s.raw_end_far);
+  YGX_CHECK_LAUNCH();
+  ygx::k_raw_ends<<<ygx::grid_for(L, 256), 256, 0, stream>>>(s.raw_off_near, s.near_cnt, L,
+                                                             s.raw_end_near);
+  YGX_CHECK_LAUNCH();
+  ygx::k_ovf_scatter<<<ygx::kWalkGrid, 256, 0, stream>>>(
+      s.log, s.log_cnt, s.log_region, (int32_t)total, s.far_pos, s.near_pos, far_raw32,
+      near_raw32, s.raw_end_far, s.raw_end_near, s.status);
+  YGX_CHECK_LAUNCH();
+  ygx::k_check_ext<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      s.far_pos, s.raw_end_far, s.ext_far_cnt, total, s.status, ygx::kFlagFarOverflow);
+  YGX_CHECK_LAUNCH();
+  ygx::k_check_ext<<<ygx::grid_for(L, 256), 256, 0, stream>>>(
+      s.near_pos, s.raw_end_near, s.ext_near_cnt, L, s.status, ygx::kFlagNearOverflow);
+  YGX_CHECK_LAUNCH();
+  if (cudaMemcpyAsync(far_raw_off, s.raw_off_far, sizeof(int64_t) * total,
+                      cudaMemcpyDeviceToDevice, stream) != cudaSuccess ||
+      cudaMemcpyAsync(near_raw_off, s.raw_off_near, sizeof(int64_t) * L,
+                      cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  return YGX_OK;
+}
+
 // Finalize: canonical (ascending) order within every row, widened into the
 // index-dtype outputs: far sources / targets / target_levels in the
 // level-major layout, near neighbours in leaf order.  far_src32 and
@@ -1360,8 +1708,10 @@ int ygx_traverse_fill_walk(int64_t total, int64_t num_internal, int mac, float t
 // neighbor_leaf_positions is non-null it receives the dense (L x max_nbr)
 // leaf-position table.  Does not synchronize.
 int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capacity,
-                          int64_t log_capacity, const int32_t* level32, const int32_t* leafpos32, int index_bits,
-                          int32_t* far_src32, int32_t* near_nbr32, void* far_sources,
+                          int64_t log_capacity, const int32_t* level32, const int32_t* leafpos32,
+                          int index_bits, int32_t* far_src32, int32_t* near_nbr32,
+                          const int64_t* far_raw_off, const int64_t* near_raw_off,
+                          void* far_sources,
                           void* far_targets, void* target_levels, void* neighbors,
                           void* neighbor_leaf_positions, int64_t max_nbr, void* ws,
                           size_t ws_bytes, cudaStream_t stream) {
@@ -1379,7 +1729,8 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
   }
   const int64_t stride = total > L ? total : L;
   auto rows_pass = [&](int64_t rows, const int64_t* off, const int32_t* cnt, const int32_t* lvl,
-                       int32_t* raw, void* vals, void* tgts, void* lvls) -> int {
+                       int32_t* raw, const int64_t* roff, void* vals, void* tgts,
+                       void* lvls) -> int {
     if (cudaMemsetAsync(s.n_big, 0, 16 * sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
     ygx::k_rows_classify<<<ygx::grid_for(rows, 256), 256, 0, stream>>>(
         rows, cnt, s.class_rows, stride, s.n_big + 1, s.big_rows, s.n_big);
@@ -1387,20 +1738,21 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
 #define YGX_ROWS(C, R)                                                                       \
   ygx::k_rows_class<R><<<grid_small, 256, 0, stream>>>(s.class_rows + (C) * stride,            \
                                                        s.n_big + 1 + (C), off, cnt, lvl, raw, \
-                                                       index_bits, vals, tgts, lvls);         \
+                                                       roff, index_bits, vals, tgts, lvls);   \
   YGX_CHECK_LAUNCH();
     YGX_ROWS(0, 1) YGX_ROWS(1, 2) YGX_ROWS(2, 4) YGX_ROWS(3, 8) YGX_ROWS(4, 16) YGX_ROWS(5, 32)
 #undef YGX_ROWS
     ygx::k_rows_big<<<ygx::kBigGrid, ygx::kBigThreads, big_smem, stream>>>(
-        s.big_rows, s.n_big, stride, off, cnt, lvl, raw, index_bits, vals, tgts, lvls, s.bitmaps,
-        total);
+        s.big_rows, s.n_big, stride, off, cnt, lvl, raw, roff, index_bits, vals, tgts, lvls,
+        s.bitmaps, total);
     YGX_CHECK_LAUNCH();
     return YGX_OK;
   };
-  int rc2 = rows_pass(total, s.far_off, s.far_cnt, level32, far_src32, far_sources, far_targets,
-                      target_levels);
+  int rc2 = rows_pass(total, s.far_off, s.far_cnt, level32, far_src32, far_raw_off, far_sources,
+                      far_targets, target_levels);
   if (rc2) return rc2;
-  rc2 = rows_pass(L, s.near_off, s.near_cnt, nullptr, near_nbr32, neighbors, nullptr, nullptr);
+  rc2 = rows_pass(L, s.near_off, s.near_cnt, nullptr, near_nbr32, near_raw_off, neighbors,
+                  nullptr, nullptr);
   if (rc2) return rc2;
   if (neighbor_leaf_positions && max_nbr > 0) {
     ygx::k_neighbor_leaf_positions<<<ygx::grid_for(L * max_nbr, 256), 256, 0, stream>>>(

@@ -210,7 +210,7 @@ LAST_WALK_STATS: dict = {}  # diagnostics of the most recent walk
 # a walk that overflows is re-run with the sizes it reports.
 _CAPACITY_HINTS: dict = {}
 _TIMING = os.environ.get("YGGDRAX_B200_TIMING", "0") == "1"  # per-pass CUDA-event times
-TRAVERSAL_MODES = ("log", "two_pass")
+TRAVERSAL_MODES = ("log", "two_pass", "learned")
 _TRAVERSAL_MODE = os.environ.get("YGGDRAX_B200_TRAVERSAL_MODE", "log")
 
 
@@ -220,7 +220,10 @@ def set_traversal_mode(mode: str) -> None:
     * ``"log"`` (default): one walk that counts row entries and logs every
       accepted / near pair once, then a scatter of the log into the rows;
     * ``"two_pass"``: the reference's plain count-then-fill schedule, two
-      walks (counts, then entries written at row cursors).
+      walks (counts, then entries written at row cursors);
+    * ``"learned"``: one walk writing straight into rows sized by the learned
+      capacity predictor (``yggdrax_b200.predictor``); rows that outgrow
+      their prediction are completed from a log.
 
     Environment: ``YGGDRAX_B200_TRAVERSAL_MODE``."""
     global _TRAVERSAL_MODE
@@ -335,6 +338,113 @@ class _WalkOut:
     num_levels: int
 
 
+# Learned mode, per (mac, theta): the overflow log capacity and the far /
+# near extension entries (per tree node) that the last predicted walk
+# needed, to size the next walk's log and extension room.
+_LEARNED_HINTS: dict = {}
+
+
+def _learned_walk_fill(topology, d, total, ni, nl, num_levels, center, radius, max_extent,
+                       leafpos32, theta, mac_type, mac, dehnen_radius_scale, root, wf_capacity,
+                       timing, evs):
+    """Predicted capacities -> padded offsets -> one walk into the padded rows
+    -> offsets, overflowed rows completed.  Re-runs the (deterministic) walk
+    with the sizes it reports when the wavefront, the overflow log or the
+    extension room was too small."""
+    from .predictor import default_predictor
+
+    lib = L.lib()
+    dev = topology.parent.device
+    st = L.stream_handle(dev)
+    ib, idt = INDEX_BITS, INDEX_DTYPE
+    params, cal = default_predictor(dev)
+    far_cap = torch.empty(total, dtype=torch.int32, device=dev)
+    near_cap = torch.empty(nl, dtype=torch.int32, device=dev)
+    L.check(lib.ygx_predict_caps(
+        L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.level32), L.ptr(d.parent32),
+        L.ptr(leafpos32), total, ni, L.ptr(topology.node_ranges.contiguous()), ib, root,
+        float(theta), mac, L.ptr(params), float(cal["slack_far"]), float(cal["slack_near"]),
+        int(cal["add"]), L.ptr(far_cap), L.ptr(near_cap), st), "ygx_predict_caps")
+    key = (mac_type, float(theta))
+    hint_wf, _ = _CAPACITY_HINTS.get(key, (0.0, 0.0))
+    cap = int(wf_capacity) if wf_capacity else max(32 * total + 65536, int(1.25 * hint_wf * total))
+    cap = min(cap, (1 << 32) - 1)
+    h_ovf, h_ext_far, h_ext_near = _LEARNED_HINTS.get(key, (0.0, 0.0, 0.0))
+    log_cap = max(65536, int(1.25 * h_ovf * total))
+    extra = [int(1.25 * h_ext_far * total), int(1.25 * h_ext_near * total)]
+    while True:
+        ws = L.workspace(lib.ygx_traverse_workspace_size(total, nl, cap, log_cap), dev)
+        sums = np.zeros(2, np.uint64)
+        L.check(lib.ygx_traverse_pad_offsets(total, ni, cap, log_cap, L.ptr(far_cap),
+                                             L.ptr(near_cap), sums.ctypes.data, L.ptr(ws),
+                                             ws.numel(), st), "ygx_traverse_pad_offsets")
+        pf, pn = int(sums[0]), int(sums[1])
+        fr = pf + max(extra[0], pf // 16 + 4096)
+        nr = pn + max(extra[1], pn // 16 + 4096)
+        far_raw = torch.empty(fr, dtype=torch.int32, device=dev)
+        near_raw = torch.empty(nr, dtype=torch.int32, device=dev)
+        stats = np.zeros(L.TSTAT_WORDS, np.uint64)
+        flags = np.zeros(1, np.uint32)
+        rc = lib.ygx_traverse_walk_predicted(
+            L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32), L.ptr(d.right32),
+            L.ptr(leafpos32), total, ni, mac, float(theta), float(dehnen_radius_scale), root,
+            cap, log_cap, L.ptr(far_cap), L.ptr(near_cap), L.ptr(far_raw), L.ptr(near_raw),
+            stats.ctypes.data, flags.ctypes.data, L.ptr(ws), ws.numel(), st)
+        f = int(flags[0])
+        if f & (L.FLAG_QUEUE_OVERFLOW | L.FLAG_LOG_OVERFLOW) and rc == 0:
+            if f & L.FLAG_QUEUE_OVERFLOW:
+                if cap >= (1 << 32) - 1:
+                    raise L.YgxError("traversal wavefront exceeds 2^32 pairs")
+                cap = min((1 << 32) - 1, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
+                log_cap = max(log_cap, int(stats[L.TSTAT["log_need"]]))
+            else:
+                log_cap = int(stats[L.TSTAT["log_need"]])
+            del ws, far_raw, near_raw
+            continue
+        L.check(rc, "ygx_traverse_walk_predicted")
+        if f & L.FLAG_BAD_INPUT:
+            raise ValueError("MAC extents must be positive (geometry has zero or NaN extents)")
+        if f:
+            raise L.YgxError(f"traversal walk reported flags {f:#x}")
+        ef, en = int(stats[L.TSTAT["ext_far"]]), int(stats[L.TSTAT["ext_near"]])
+        if pf + ef > fr or pn + en > nr:
+            extra = [ef, en]  # the walk is deterministic: the re-run needs exactly this
+            del ws, far_raw, near_raw
+            continue
+        break
+    if not wf_capacity:
+        _CAPACITY_HINTS[key] = (int(stats[L.TSTAT["wf_need"]]) / total,
+                                _CAPACITY_HINTS.get(key, (0.0, 0.0))[1])
+        _LEARNED_HINTS[key] = (int(stats[L.TSTAT["log_need"]]) / total,
+                               int(stats[L.TSTAT["ext_far"]]) / total,
+                               int(stats[L.TSTAT["ext_near"]]) / total)
+    if timing:
+        evs[1].record()
+    s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
+    LAST_WALK_STATS.clear()
+    entries = max(1, s["far_total"] + s["near_total"])
+    LAST_WALK_STATS.update(
+        s, wf_capacity=cap, log_capacity=log_cap, mode="learned", padded_far=pf,
+        padded_near=pn, over_allocation=(pf + pn) / entries,
+        overflow_row_fraction=s["ovf_rows"] / max(1, total + nl),
+        overflow_entry_fraction=s["ovf_entries"] / entries)
+    node_offsets = torch.empty(total + 1, dtype=idt, device=dev)
+    far_counts = torch.empty(total, dtype=idt, device=dev)
+    level_offsets = torch.empty(num_levels + 1, dtype=idt, device=dev)
+    near_offsets = torch.empty(nl + 1, dtype=idt, device=dev)
+    near_counts = torch.empty(nl, dtype=idt, device=dev)
+    far_raw_off = torch.empty(total, dtype=torch.int64, device=dev)
+    near_raw_off = torch.empty(max(nl, 1), dtype=torch.int64, device=dev)
+    L.check(lib.ygx_traverse_fill_predicted(
+        total, ni, cap, log_cap, L.ptr(far_cap), L.ptr(near_cap), fr, nr, L.ptr(d.nbl32),
+        L.ptr(topology.level_offsets), num_levels, ib, L.ptr(node_offsets), L.ptr(far_counts),
+        L.ptr(level_offsets), L.ptr(near_offsets), L.ptr(near_counts), L.ptr(far_raw),
+        L.ptr(near_raw), L.ptr(far_raw_off), L.ptr(near_raw_off), L.ptr(ws), ws.numel(), st),
+        "ygx_traverse_fill_predicted")
+    return (ws, cap, log_cap, s, far_raw, near_raw, far_raw_off, near_raw_off, node_offsets,
+            far_counts, level_offsets, near_offsets, near_counts)
+
+
 def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_scale: float,
               wf_capacity: Optional[int] = None) -> _WalkOut:
     """Walk (counts + pair log) -> scan -> fill (scatter) -> finalize on the GPU."""
@@ -368,72 +478,85 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     mode = _TRAVERSAL_MODE
     if mode not in TRAVERSAL_MODES:
         raise ValueError(f"traversal mode must be one of {TRAVERSAL_MODES}, got {mode!r}")
-    walk_mode = L.WALK_LOG if mode == "log" else L.WALK_COUNT
-    hint_wf, hint_log = _CAPACITY_HINTS.get((mac_type, float(theta)), (0.0, 0.0))
-    cap = int(wf_capacity) if wf_capacity else max(32 * total + 65536, int(1.25 * hint_wf * total))
-    log_cap = max(8 * total + 65536, int(1.1 * hint_log * total)) if walk_mode == L.WALK_LOG else 1
-    cap = min(cap, (1 << 32) - 1)
     mac = _MAC_CODES[mac_type]
     root = int(torch.argmin(d.parent32).item()) if bool(
         (d.tree_flags != 0).any().item()) else 0
-    while True:
-        ws = L.workspace(lib.ygx_traverse_workspace_size(total, nl, cap, log_cap), dev)
-        stats = np.zeros(L.TSTAT_WORDS, np.uint64)
-        flags = np.zeros(1, np.uint32)
-        rc = lib.ygx_traverse_walk(
-            L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32), L.ptr(d.right32),
-            L.ptr(leafpos32), total, ni, mac, float(theta), float(dehnen_radius_scale), root,
-            walk_mode, cap, log_cap, stats.ctypes.data, flags.ctypes.data, L.ptr(ws),
-            ws.numel(), st)
-        f = int(flags[0])
-        if f & (L.FLAG_QUEUE_OVERFLOW | L.FLAG_LOG_OVERFLOW) and rc == 0:
-            if f & L.FLAG_QUEUE_OVERFLOW:
-                if cap >= (1 << 32) - 1:
-                    raise L.YgxError("traversal wavefront exceeds 2^32 pairs")
-                # the needs a truncated walk reports are lower bounds only
-                cap = min((1 << 32) - 1, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
-                log_cap = max(log_cap, int(stats[L.TSTAT["log_need"]]))
-            else:
-                log_cap = int(stats[L.TSTAT["log_need"]])
-            del ws
-            continue
-        L.check(rc, "ygx_traverse_walk")
-        if f & L.FLAG_BAD_INPUT:
-            raise ValueError("MAC extents must be positive (geometry has zero or NaN extents)")
-        if f:
-            raise L.YgxError(f"traversal walk reported flags {f:#x}")
-        break
-    if not wf_capacity:
-        prev = _CAPACITY_HINTS.get((mac_type, float(theta)), (0.0, 0.0))
-        log_need = int(stats[L.TSTAT["log_need"]]) / total if walk_mode == L.WALK_LOG else prev[1]
-        _CAPACITY_HINTS[(mac_type, float(theta))] = (
-            int(stats[L.TSTAT["wf_need"]]) / total, log_need)
-    if timing:
-        evs[1].record()
-    s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
-    LAST_WALK_STATS.clear()
-    LAST_WALK_STATS.update(s, wf_capacity=cap, log_capacity=log_cap, mode=mode)
-    P, Q = s["far_total"], s["near_total"]
-    node_offsets = torch.empty(total + 1, dtype=idt, device=dev)
-    far_counts = torch.empty(total, dtype=idt, device=dev)
-    level_offsets = torch.empty(num_levels + 1, dtype=idt, device=dev)
-    near_offsets = torch.empty(nl + 1, dtype=idt, device=dev)
-    near_counts = torch.empty(nl, dtype=idt, device=dev)
-    far_src32 = torch.empty(max(P, 1), dtype=torch.int32, device=dev)
-    near_nbr32 = torch.empty(max(Q, 1), dtype=torch.int32, device=dev)
-    if walk_mode == L.WALK_LOG:
-        L.check(lib.ygx_traverse_fill(
-            total, ni, cap, log_cap, P, Q, L.ptr(d.nbl32), L.ptr(leafpos32),
-            L.ptr(topology.level_offsets), num_levels, ib, L.ptr(node_offsets),
-            L.ptr(far_counts), L.ptr(level_offsets), L.ptr(near_offsets), L.ptr(near_counts),
-            L.ptr(far_src32), L.ptr(near_nbr32), L.ptr(ws), ws.numel(), st), "ygx_traverse_fill")
+    far_raw_off = near_raw_off = None
+    if mode == "learned":
+        (ws, cap, log_cap, s, far_src32, near_nbr32, far_raw_off, near_raw_off, node_offsets,
+         far_counts, level_offsets, near_offsets, near_counts) = _learned_walk_fill(
+            topology, d, total, ni, nl, num_levels, center, radius, max_extent, leafpos32,
+            theta, mac_type, mac, dehnen_radius_scale, root, wf_capacity, timing, evs)
+        P, Q = s["far_total"], s["near_total"]
     else:
-        L.check(lib.ygx_traverse_fill_walk(
-            total, ni, mac, float(theta), root, cap, log_cap, s["gens"], P, Q, L.ptr(d.nbl32),
-            L.ptr(topology.level_offsets), num_levels, ib, L.ptr(node_offsets),
-            L.ptr(far_counts), L.ptr(level_offsets), L.ptr(near_offsets), L.ptr(near_counts),
-            L.ptr(far_src32), L.ptr(near_nbr32), L.ptr(ws), ws.numel(), st),
-            "ygx_traverse_fill_walk")
+        walk_mode = L.WALK_LOG if mode == "log" else L.WALK_COUNT
+        hint_wf, hint_log = _CAPACITY_HINTS.get((mac_type, float(theta)), (0.0, 0.0))
+        cap = int(wf_capacity) if wf_capacity else max(32 * total + 65536,
+                                                       int(1.25 * hint_wf * total))
+        log_cap = (max(8 * total + 65536, int(1.1 * hint_log * total))
+                   if walk_mode == L.WALK_LOG else 1)
+        cap = min(cap, (1 << 32) - 1)
+        while True:
+            ws = L.workspace(lib.ygx_traverse_workspace_size(total, nl, cap, log_cap), dev)
+            stats = np.zeros(L.TSTAT_WORDS, np.uint64)
+            flags = np.zeros(1, np.uint32)
+            rc = lib.ygx_traverse_walk(
+                L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32),
+                L.ptr(d.right32), L.ptr(leafpos32), total, ni, mac, float(theta),
+                float(dehnen_radius_scale), root, walk_mode, cap, log_cap, stats.ctypes.data,
+                flags.ctypes.data, L.ptr(ws), ws.numel(), st)
+            f = int(flags[0])
+            if f & (L.FLAG_QUEUE_OVERFLOW | L.FLAG_LOG_OVERFLOW) and rc == 0:
+                if f & L.FLAG_QUEUE_OVERFLOW:
+                    if cap >= (1 << 32) - 1:
+                        raise L.YgxError("traversal wavefront exceeds 2^32 pairs")
+                    # the needs a truncated walk reports are lower bounds only
+                    cap = min((1 << 32) - 1, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
+                    log_cap = max(log_cap, int(stats[L.TSTAT["log_need"]]))
+                else:
+                    log_cap = int(stats[L.TSTAT["log_need"]])
+                del ws
+                continue
+            L.check(rc, "ygx_traverse_walk")
+            if f & L.FLAG_BAD_INPUT:
+                raise ValueError("MAC extents must be positive (geometry has zero or NaN extents)")
+            if f:
+                raise L.YgxError(f"traversal walk reported flags {f:#x}")
+            break
+        if not wf_capacity:
+            prev = _CAPACITY_HINTS.get((mac_type, float(theta)), (0.0, 0.0))
+            log_need = (int(stats[L.TSTAT["log_need"]]) / total
+                        if walk_mode == L.WALK_LOG else prev[1])
+            _CAPACITY_HINTS[(mac_type, float(theta))] = (
+                int(stats[L.TSTAT["wf_need"]]) / total, log_need)
+        if timing:
+            evs[1].record()
+        s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
+        LAST_WALK_STATS.clear()
+        LAST_WALK_STATS.update(s, wf_capacity=cap, log_capacity=log_cap, mode=mode)
+        P, Q = s["far_total"], s["near_total"]
+        node_offsets = torch.empty(total + 1, dtype=idt, device=dev)
+        far_counts = torch.empty(total, dtype=idt, device=dev)
+        level_offsets = torch.empty(num_levels + 1, dtype=idt, device=dev)
+        near_offsets = torch.empty(nl + 1, dtype=idt, device=dev)
+        near_counts = torch.empty(nl, dtype=idt, device=dev)
+        far_src32 = torch.empty(max(P, 1), dtype=torch.int32, device=dev)
+        near_nbr32 = torch.empty(max(Q, 1), dtype=torch.int32, device=dev)
+        if walk_mode == L.WALK_LOG:
+            L.check(lib.ygx_traverse_fill(
+                total, ni, cap, log_cap, P, Q, L.ptr(d.nbl32), L.ptr(leafpos32),
+                L.ptr(topology.level_offsets), num_levels, ib, L.ptr(node_offsets),
+                L.ptr(far_counts), L.ptr(level_offsets), L.ptr(near_offsets), L.ptr(near_counts),
+                L.ptr(far_src32), L.ptr(near_nbr32), L.ptr(ws), ws.numel(), st),
+                "ygx_traverse_fill")
+        else:
+            L.check(lib.ygx_traverse_fill_walk(
+                total, ni, mac, float(theta), root, cap, log_cap, s["gens"], P, Q,
+                L.ptr(d.nbl32),
+                L.ptr(topology.level_offsets), num_levels, ib, L.ptr(node_offsets),
+                L.ptr(far_counts), L.ptr(level_offsets), L.ptr(near_offsets), L.ptr(near_counts),
+                L.ptr(far_src32), L.ptr(near_nbr32), L.ptr(ws), ws.numel(), st),
+                "ygx_traverse_fill_walk")
     if timing:
         evs[2].record()
     sources = torch.empty(P, dtype=idt, device=dev)
@@ -451,7 +574,9 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     nlp = torch.empty((nl, max_nbr), dtype=idt, device=dev)
     L.check(lib.ygx_traverse_finalize(
         total, ni, cap, log_cap, L.ptr(d.level32), L.ptr(leafpos32), ib, L.ptr(far_src32),
-        L.ptr(near_nbr32), L.ptr(sources), L.ptr(targets), L.ptr(target_levels),
+        L.ptr(near_nbr32), L.ptr(far_raw_off) if far_raw_off is not None else None,
+        L.ptr(near_raw_off) if near_raw_off is not None else None, L.ptr(sources), L.ptr(targets),
+        L.ptr(target_levels),
         L.ptr(neighbors), L.ptr(nlp) if max_nbr > 0 else None, max_nbr, L.ptr(ws), ws.numel(),
         st), "ygx_traverse_finalize")
     if timing:
