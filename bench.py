@@ -10,8 +10,14 @@ the whole step.
 * ``e2e``: the same step through the public API from pinned host buffers:
   host->device copy of positions and masses and device->host copy of the
   per-node far/near counts inside the timed region.
-* ``roofline``: the dominant kernel family (see ``--breakdown``) timed with
-  CUDA events inside this run, against the measured HBM copy bandwidth.
+* ``roofline``: the build's HBM-bound kernel (the onesweep sort passes)
+  timed with CUDA events inside this run, against the measured HBM copy
+  bandwidth; the traversal is latency bound and is reported as pairs/s.
+* ``modes``: the same step with each traversal schedule (all return the same
+  exact lists): ``log`` (one walk + pair log, the default and ``value``),
+  ``two_pass`` (the reference's count walk + fill walk) and ``learned`` (one
+  walk into rows sized by the learned capacity predictor, with its overflow
+  and over-allocation figures).
 * ``cpu_baseline``: the CPU restatement of the pipeline (OpenMP, all host
   cores) on a bounded sample.
 * ``--impl reference``: that CPU implementation on the host cores as the
@@ -253,6 +259,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--breakdown", action="store_true")
+    ap.add_argument("--no-modes", action="store_true",
+                    help="skip timing the two-pass and learned traversal schedules")
     ap.add_argument("--roofline-only", action="store_true",
                     help="time only the sort roofline leg (for profiling it)")
     args = ap.parse_args()
@@ -351,6 +359,11 @@ def main():
     roofline = sort_roofline(yb.morton_encode(pos_d, yb.infer_bounds(pos_d)), dev,
                              max(3, args.steps))
 
+    # -- the same step with the other traversal schedules (same exact lists) ----
+    modes = {"log": {"ms_per_step": t_dev * 1e3, "value": n / t_dev}}
+    if not args.no_modes:
+        modes.update(mode_timings(step, pos_d, mass_d, n, args.steps, barrier))
+
     breakdown = None
     if args.breakdown:
         breakdown = stage_breakdown(pos_d, mass_d, dev)
@@ -375,13 +388,14 @@ def main():
                        "far_entries": far_entries, "near_entries": near_entries,
                        "pairs_per_s": world * (far_entries + near_entries) / t_max,
                        "l2": "inputs (268 MB) larger than L2; no flush between steps",
-                       "parallelism": f"replicas{world}"},
+                       "traversal_mode": "log", "parallelism": f"replicas{world}"},
             "e2e": {"value": world * n / te_max, "unit": "particles/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
+            "modes": modes,
         }
         if breakdown is not None:
             line["breakdown_ms"] = breakdown
@@ -392,6 +406,40 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def mode_timings(step, pos_d, mass_d, n, steps, barrier) -> dict:
+    """Device time of the step with the plain two-pass traversal (count walk +
+    fill walk, the reference's schedule) and with the learned one-pass
+    traversal (rows sized by the capacity predictor), inputs resident."""
+    import torch
+
+    import yggdrax_b200 as yb
+    from yggdrax_b200.interactions import LAST_WALK_STATS
+
+    out = {}
+    for mode in ("two_pass", "learned"):
+        yb.set_traversal_mode(mode)
+        try:
+            for _ in range(2):  # capacity hints of this schedule
+                step(pos_d, mass_d)
+            barrier()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(steps):
+                step(pos_d, mass_d)
+            b.record()
+            barrier()
+            ms = a.elapsed_time(b) / steps
+            rec = {"ms_per_step": ms, "value": n / (ms / 1e3)}
+            if mode == "learned":
+                rec["predictor"] = {k: LAST_WALK_STATS.get(k) for k in (
+                    "over_allocation", "overflow_row_fraction", "overflow_entry_fraction",
+                    "ovf_rows", "padded_far", "padded_near")}
+            out[mode] = rec
+        finally:
+            yb.set_traversal_mode("log")
+    return out
 
 
 def stage_breakdown(pos_d, mass_d, dev):

@@ -222,16 +222,18 @@ size_t ygx_traverse_workspace_size(int64_t total, int64_t num_leaves, int64_t wf
  * mac 0 = "bh", 1 = "dehnen", 2 = "engblom".  stats_out / flags_out are HOST
  * arrays (YGX_TSTAT_WORDS / 1 words).  YGX_FLAG_QUEUE_OVERFLOW or
  * YGX_FLAG_LOG_OVERFLOW in *flags_out: re-run with larger capacities (the
- * walk is deterministic; the reported log need is exact).  Synchronizes the
- * stream. */
+ * walk is deterministic; the reported log need is exact).  gens_hint > 0:
+ * the expected number of generations (a previous walk's YGX_TSTAT_GENS);
+ * the wavefront is first checked after that many, then every 16.
+ * Synchronizes the stream. */
 #define YGX_WALK_LOG 0   /* one walk: row counts + a log of accepted / near pairs */
 #define YGX_WALK_COUNT 1 /* plain two-pass mode, first walk: row counts only     */
 int ygx_traverse_walk(const float* center, const float* radius, const float* max_extent,
                       const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
                       int64_t total, int64_t num_internal, int mac, float theta,
-                      float dehnen_radius_scale, int root, int mode, int64_t wf_capacity,
-                      int64_t log_capacity, uint64_t* stats_out, uint32_t* flags_out, void* ws,
-                      size_t ws_bytes, cudaStream_t stream);
+                      float dehnen_radius_scale, int root, int mode, int gens_hint,
+                      int64_t wf_capacity, int64_t log_capacity, uint64_t* stats_out,
+                      uint32_t* flags_out, void* ws, size_t ws_bytes, cudaStream_t stream);
 /* Row layout of the fill walk (_dual_tree_walk_compact_fill_impl,
  * :2942-3558) and the offset tables of _result_to_interactions /
  * _result_to_neighbors (:3561-3837), from the walk's counts and pair log. */
@@ -274,8 +276,9 @@ int ygx_traverse_walk_predicted(const float* center, const float* radius,
                                 const float* max_extent, const int32_t* left32,
                                 const int32_t* right32, const int32_t* leafpos32, int64_t total,
                                 int64_t num_internal, int mac, float theta,
-                                float dehnen_radius_scale, int root, int64_t wf_capacity,
-                                int64_t log_capacity, const int32_t* far_cap32,
+                                float dehnen_radius_scale, int root, int gens_hint,
+                                int64_t wf_capacity, int64_t log_capacity,
+                                const int32_t* far_cap32,
                                 const int32_t* near_cap32, int32_t* far_raw32,
                                 int32_t* near_raw32, uint64_t* stats_out, uint32_t* flags_out,
                                 void* ws, size_t ws_bytes, cudaStream_t stream);

@@ -78,15 +78,15 @@ _SIGS = {
     "ygx_tree_geometry": (I32, [P, I64, I32, P, P, P, P, P, P, I64, I32, P, P, P, I64, P, P,
                                 P, P, P, SZ, P]),
     "ygx_traverse_workspace_size": (SZ, [I64, I64, I64, I64]),
-    "ygx_traverse_walk": (I32, [P, P, P, P, P, P, I64, I64, I32, F32, F32, I32, I32, I64, I64,
-                                P, P, P, SZ, P]),
+    "ygx_traverse_walk": (I32, [P, P, P, P, P, P, I64, I64, I32, F32, F32, I32, I32, I32, I64,
+                                I64, P, P, P, SZ, P]),
     "ygx_traverse_fill_walk": (I32, [I64, I64, I32, F32, I32, I64, I64, I32, I64, I64, P, P, I32,
                                      I32, P, P, P, P, P, P, P, P, SZ, P]),
     "ygx_traverse_fill": (I32, [I64, I64, I64, I64, I64, I64, P, P, P, I32, I32, P, P, P, P, P,
                                 P, P, P, SZ, P]),
     "ygx_traverse_pad_offsets": (I32, [I64, I64, I64, I64, P, P, P, P, SZ, P]),
-    "ygx_traverse_walk_predicted": (I32, [P, P, P, P, P, P, I64, I64, I32, F32, F32, I32, I64,
-                                          I64, P, P, P, P, P, P, P, SZ, P]),
+    "ygx_traverse_walk_predicted": (I32, [P, P, P, P, P, P, I64, I64, I32, F32, F32, I32, I32,
+                                          I64, I64, P, P, P, P, P, P, P, SZ, P]),
     "ygx_traverse_fill_predicted": (I32, [I64, I64, I64, I64, P, P, I64, I64, P, P, I32, I32, P,
                                           P, P, P, P, P, P, P, P, P, SZ, P]),
     "ygx_mlp_param_count": (I32, []),

@@ -1290,7 +1290,7 @@ static int launch_gen(int mode, int mac, const TravScratch& s, int32_t ni, int32
 // run (a repeat of a walk whose length is known).  *gens_out = launched.
 static int run_gens(int mode, int mac, const TravScratch& s, int32_t ni, int32_t total,
                     float theta_sq, float theta_r, int root, uint32_t cap, const RowSink& sink,
-                    int fixed_gens, int* gens_out, cudaStream_t stream) {
+                    int fixed_gens, int gens_hint, int* gens_out, cudaStream_t stream) {
   k_seed<<<1, 256, 0, stream>>>(s.wf[0], s.region_cnt[0], s.sizes, root);
   YGX_CHECK_LAUNCH();
   int gen = 0, rc = YGX_OK;
@@ -1302,12 +1302,16 @@ static int run_gens(int mode, int mac, const TravScratch& s, int32_t ni, int32_t
     *gens_out = gen;
     return YGX_OK;
   }
-  const int chunk = 16;
+  // The first probe comes after gens_hint generations (the length of a
+  // previous walk of the same kind, so usually the only probe), later ones
+  // every 16.
+  int chunk = gens_hint > 0 ? gens_hint : 16;
   while (true) {
     for (int k = 0; k < chunk && gen < kMaxGens; ++k, ++gen) {
       rc = launch_gen(mode, mac, s, ni, total, theta_sq, theta_r, gen, cap, sink, stream);
       if (rc) return rc;
     }
+    chunk = 16;
     uint32_t probe = 0, flags = 0;
     if (cudaMemcpyAsync(&probe, s.sizes + gen, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                         stream) != cudaSuccess ||
@@ -1391,9 +1395,9 @@ static int trav_setup(ygx::TravScratch& s, void* ws, size_t ws_bytes, int64_t to
 int ygx_traverse_walk(const float* center, const float* radius, const float* max_extent,
                       const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
                       int64_t total, int64_t num_internal, int mac, float theta,
-                      float dehnen_radius_scale, int root, int mode, int64_t wf_capacity,
-                      int64_t log_capacity, uint64_t* stats_out, uint32_t* flags_out, void* ws,
-                      size_t ws_bytes, cudaStream_t stream) {
+                      float dehnen_radius_scale, int root, int mode, int gens_hint,
+                      int64_t wf_capacity, int64_t log_capacity, uint64_t* stats_out,
+                      uint32_t* flags_out, void* ws, size_t ws_bytes, cudaStream_t stream) {
   if (total < 3 || total > INT32_MAX || num_internal < 1 || mac < 0 || mac > 2 ||
       root < 0 || root >= total || !stats_out || !flags_out ||
       (mode != YGX_WALK_LOG && mode != YGX_WALK_COUNT))
@@ -1420,7 +1424,7 @@ int ygx_traverse_walk(const float* center, const float* radius, const float* max
   int gen = 0;
   rc = ygx::run_gens(mode == YGX_WALK_LOG ? ygx::kWalkLog : ygx::kWalkCount, mac, s,
                      (int32_t)num_internal, (int32_t)total, theta_sq, theta_r, root,
-                     (uint32_t)wf_capacity, ygx::no_sink(), -1, &gen, stream);
+                     (uint32_t)wf_capacity, ygx::no_sink(), -1, gens_hint, &gen, stream);
   if (rc == YGX_ERR_QUEUE_OVERFLOW) flags_out[0] = ygx::kFlagQueueOverflow;
   if (rc) return rc;
   ygx::k_count_stats<<<ygx::grid_for(total, 256, ygx::kNumSMs * 4), 256, 0, stream>>>(
@@ -1513,7 +1517,7 @@ int ygx_traverse_fill_walk(int64_t total, int64_t num_internal, int mac, float t
   sink.near_total = (unsigned long long)near_total;
   int ran = 0;
   rc = ygx::run_gens(ygx::kWalkFill, mac, s, (int32_t)num_internal, (int32_t)total, theta_sq,
-                     theta_r, root, (uint32_t)wf_capacity, sink, gens, &ran, stream);
+                     theta_r, root, (uint32_t)wf_capacity, sink, gens, 0, &ran, stream);
   if (rc) return rc;
   ygx::k_check_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
       s.far_off, s.far_cnt, s.far_pos, total, s.near_off, s.near_cnt, s.near_pos, L, s.status);
@@ -1563,8 +1567,9 @@ int ygx_traverse_walk_predicted(const float* center, const float* radius,
                                 const float* max_extent, const int32_t* left32,
                                 const int32_t* right32, const int32_t* leafpos32, int64_t total,
                                 int64_t num_internal, int mac, float theta,
-                                float dehnen_radius_scale, int root, int64_t wf_capacity,
-                                int64_t log_capacity, const int32_t* far_cap32,
+                                float dehnen_radius_scale, int root, int gens_hint,
+                                int64_t wf_capacity, int64_t log_capacity,
+                                const int32_t* far_cap32,
                                 const int32_t* near_cap32, int32_t* far_raw32,
                                 int32_t* near_raw32, uint64_t* stats_out, uint32_t* flags_out,
                                 void* ws, size_t ws_bytes, cudaStream_t stream) {
@@ -1603,7 +1608,7 @@ int ygx_traverse_walk_predicted(const float* center, const float* radius,
   sink.near_nbr = near_raw32;
   int gen = 0;
   rc = ygx::run_gens(ygx::kWalkPred, mac, s, (int32_t)num_internal, (int32_t)total, theta_sq,
-                     theta_r, root, (uint32_t)wf_capacity, sink, -1, &gen, stream);
+                     theta_r, root, (uint32_t)wf_capacity, sink, -1, gens_hint, &gen, stream);
   if (rc == YGX_ERR_QUEUE_OVERFLOW) flags_out[0] = ygx::kFlagQueueOverflow;
   if (rc) return rc;
   ygx::k_pred_counts<<<ygx::grid_for(total, 256, ygx::kNumSMs * 4), 256, 0, stream>>>(

@@ -9,7 +9,7 @@ import torch
 
 from . import _lib as L
 from .dtypes import INDEX_BITS
-from .tree import _dev_of, resolve_tree_topology
+from .tree import _dev_of, _host_of, resolve_tree_topology
 
 
 class TreeGeometry(NamedTuple):
@@ -51,8 +51,7 @@ def compute_tree_geometry(tree, positions_sorted: torch.Tensor, *,
     if max_leaf_size is None and getattr(topology, "leaf_size", None) is not None:
         max_leaf_size = int(topology.leaf_size)
     cap = -1 if max_leaf_size is None else int(max_leaf_size)
-    use_morton = bool(topology.use_morton_geometry.item()) if torch.is_tensor(
-        topology.use_morton_geometry) else bool(topology.use_morton_geometry)
+    use_morton = _host_of(topology).use_morton
     d = _dev_of(topology)
     dev = pos.device
     lib = L.lib()

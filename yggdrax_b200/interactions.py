@@ -27,7 +27,7 @@ import torch
 
 from . import _lib as L
 from .dtypes import INDEX_BITS, INDEX_DTYPE
-from .tree import _dev_of, resolve_tree_topology
+from .tree import _dev_of, _host_of, resolve_tree_topology
 
 logger = logging.getLogger(__name__)
 
@@ -209,6 +209,9 @@ LAST_WALK_STATS: dict = {}  # diagnostics of the most recent walk
 # head-room) so a repeated workload sizes its buffers right the first time;
 # a walk that overflows is re-run with the sizes it reports.
 _CAPACITY_HINTS: dict = {}
+# Generations of the last walk per (mac, theta): the walk checks its wavefront
+# first after that many (one host sync instead of one per 16 generations).
+_GENS_HINTS: dict = {}
 _TIMING = os.environ.get("YGGDRAX_B200_TIMING", "0") == "1"  # per-pass CUDA-event times
 TRAVERSAL_MODES = ("log", "two_pass", "learned")
 _TRAVERSAL_MODE = os.environ.get("YGGDRAX_B200_TRAVERSAL_MODE", "log")
@@ -255,6 +258,14 @@ _NEAR_MSG = "Neighbor list capacity exceeded; increase max_neighbors_per_leaf an
 
 
 # ---------------------------------------------------------------------------
+
+
+def _root_of(topology, d) -> int:
+    """Node 0 unless tied leaf codes made the topology malformed (then the
+    node without a parent, as the reference's walk starts there)."""
+    if not _host_of(topology).malformed:
+        return 0
+    return int(torch.argmin(d.parent32).item())
 
 
 def _leaf_ordering(topology, total: int, ni: int, dev):
@@ -388,7 +399,8 @@ def _learned_walk_fill(topology, d, total, ni, nl, num_levels, center, radius, m
         rc = lib.ygx_traverse_walk_predicted(
             L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32), L.ptr(d.right32),
             L.ptr(leafpos32), total, ni, mac, float(theta), float(dehnen_radius_scale), root,
-            cap, log_cap, L.ptr(far_cap), L.ptr(near_cap), L.ptr(far_raw), L.ptr(near_raw),
+            _GENS_HINTS.get(key, 0), cap, log_cap, L.ptr(far_cap), L.ptr(near_cap),
+            L.ptr(far_raw), L.ptr(near_raw),
             stats.ctypes.data, flags.ctypes.data, L.ptr(ws), ws.numel(), st)
         f = int(flags[0])
         if f & (L.FLAG_QUEUE_OVERFLOW | L.FLAG_LOG_OVERFLOW) and rc == 0:
@@ -418,6 +430,7 @@ def _learned_walk_fill(topology, d, total, ni, nl, num_levels, center, radius, m
         _LEARNED_HINTS[key] = (int(stats[L.TSTAT["log_need"]]) / total,
                                int(stats[L.TSTAT["ext_far"]]) / total,
                                int(stats[L.TSTAT["ext_near"]]) / total)
+    _GENS_HINTS[key] = int(stats[L.TSTAT["gens"]])
     if timing:
         evs[1].record()
     s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
@@ -456,7 +469,7 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     st = L.stream_handle(dev)
     ib, idt = INDEX_BITS, INDEX_DTYPE
     leaf_indices, leafpos32, po, po_to_native = _leaf_ordering(topology, total, ni, dev)
-    num_levels = int(topology.num_levels)
+    num_levels = _host_of(topology).num_levels
     z = lambda *s: torch.zeros(s, dtype=idt, device=dev)  # noqa: E731
     if ni == 0:
         return _WalkOut(
@@ -479,8 +492,7 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     if mode not in TRAVERSAL_MODES:
         raise ValueError(f"traversal mode must be one of {TRAVERSAL_MODES}, got {mode!r}")
     mac = _MAC_CODES[mac_type]
-    root = int(torch.argmin(d.parent32).item()) if bool(
-        (d.tree_flags != 0).any().item()) else 0
+    root = _root_of(topology, d)
     far_raw_off = near_raw_off = None
     if mode == "learned":
         (ws, cap, log_cap, s, far_src32, near_nbr32, far_raw_off, near_raw_off, node_offsets,
@@ -503,7 +515,8 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
             rc = lib.ygx_traverse_walk(
                 L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32),
                 L.ptr(d.right32), L.ptr(leafpos32), total, ni, mac, float(theta),
-                float(dehnen_radius_scale), root, walk_mode, cap, log_cap, stats.ctypes.data,
+                float(dehnen_radius_scale), root, walk_mode,
+                _GENS_HINTS.get((mac_type, float(theta)), 0), cap, log_cap, stats.ctypes.data,
                 flags.ctypes.data, L.ptr(ws), ws.numel(), st)
             f = int(flags[0])
             if f & (L.FLAG_QUEUE_OVERFLOW | L.FLAG_LOG_OVERFLOW) and rc == 0:
@@ -529,6 +542,7 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
                         if walk_mode == L.WALK_LOG else prev[1])
             _CAPACITY_HINTS[(mac_type, float(theta))] = (
                 int(stats[L.TSTAT["wf_need"]]) / total, log_need)
+        _GENS_HINTS[(mac_type, float(theta))] = int(stats[L.TSTAT["gens"]])
         if timing:
             evs[1].record()
         s = {k: int(stats[v]) for k, v in L.TSTAT.items()}

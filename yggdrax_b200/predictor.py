@@ -105,6 +105,7 @@ def init_params(seed: int = 0) -> np.ndarray:
 
 def node_features(topology, geometry, theta: float, mac_type: str) -> torch.Tensor:
     """(total, N_INPUTS) float32 features of every node (on the device)."""
+    from .interactions import _root_of
     from .tree import _dev_of
 
     lib = L.lib()
@@ -112,7 +113,7 @@ def node_features(topology, geometry, theta: float, mac_type: str) -> torch.Tens
     total = int(topology.parent.shape[0])
     ni = int(topology.left_child.shape[0])
     dev = topology.parent.device
-    root = _root_of(d)
+    root = _root_of(topology, d)
     X = torch.empty((total, N_INPUTS), dtype=torch.float32, device=dev)
     L.check(lib.ygx_node_features(
         L.ptr(geometry.center.contiguous().float()), L.ptr(geometry.radius.contiguous().float()),
@@ -122,8 +123,6 @@ def node_features(topology, geometry, theta: float, mac_type: str) -> torch.Tens
     return X
 
 
-def _root_of(d) -> int:
-    return int(torch.argmin(d.parent32).item()) if bool((d.tree_flags != 0).any().item()) else 0
 
 
 def forward(params: torch.Tensor, X: torch.Tensor) -> torch.Tensor:

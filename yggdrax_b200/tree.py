@@ -132,6 +132,34 @@ class DeviceTopology:
     bounds: torch.Tensor  # float32[6]
 
 
+@dataclass(frozen=True)
+class HostTopologyInfo:
+    """Host copies of the few scalars the later stages branch on, read back
+    once when the tree is built (so geometry and traversal need no sync)."""
+
+    malformed: bool     # tied leaf codes produced a non-standard topology
+    num_levels: int
+    use_morton: bool    # geometry from Morton cells (fixed depth)
+
+
+def _host_of(topology) -> HostTopologyInfo:
+    """The host info of a topology (read back now if it was not recorded)."""
+    h = getattr(topology, "_host", None)
+    if h is not None:
+        return h
+    d = _dev_of(topology)
+    um = topology.use_morton_geometry
+    h = HostTopologyInfo(
+        malformed=bool((d.tree_flags.cpu()[0] & L.FLAG_MALFORMED) != 0),
+        num_levels=int(topology.num_levels),
+        use_morton=bool(um.item()) if torch.is_tensor(um) else bool(um))
+    try:
+        object.__setattr__(topology, "_host", h)
+    except Exception:
+        pass
+    return h
+
+
 def _dev_of(topology) -> DeviceTopology:
     """The int32 device copies of a topology (rebuilt if absent)."""
     d = getattr(topology, "_dev", None)
@@ -380,7 +408,8 @@ def _build(positions, masses, bounds, *, build_mode: str, leaf_size: int = 8,
             nodes_by_level=torch.zeros(1, dtype=idt, device=dev),
             num_levels=torch.ones((), dtype=idt, device=dev), bounds_min=bmin, bounds_max=bmax,
             leaf_codes=lcodes, leaf_depths=ldepths,
-            use_morton_geometry=torch.tensor(use_morton, device=dev), leaf_size=tree_leaf_size)
+            use_morton_geometry=torch.full((), use_morton, dtype=torch.bool, device=dev),
+            leaf_size=tree_leaf_size)
         m1 = torch.full((1,), -1, dtype=torch.int32, device=dev)
         topo._dev = DeviceTopology(parent32=m1, left32=m1.clone(), right32=m1.clone(),
                                    level32=torch.zeros(1, dtype=torch.int32, device=dev),
@@ -416,11 +445,17 @@ def _build(positions, masses, bounds, *, build_mode: str, leaf_size: int = 8,
             num_particles=n, num_internal_nodes=ni, node_level=node_level,
             level_offsets=level_offsets, nodes_by_level=nbl, num_levels=num_levels,
             bounds_min=bmin, bounds_max=bmax, leaf_codes=lcodes, leaf_depths=ldepths,
-            use_morton_geometry=torch.tensor(use_morton, device=dev), leaf_size=tree_leaf_size)
+            use_morton_geometry=torch.full((), use_morton, dtype=torch.bool, device=dev),
+            leaf_size=tree_leaf_size)
         topo._dev = DeviceTopology(parent32=parent32, left32=left32, right32=right32,
                                    level32=level32, nbl32=nbl32, tree_flags=flags,
                                    bounds=bounds_dev)
     topo._max_cell_depth = max_cell_depth
+    # one read-back for the flags and the level count
+    hv = torch.cat([topo._dev.tree_flags.to(torch.int64).reshape(1),
+                    topo.num_levels.to(torch.int64).reshape(1)]).cpu()
+    topo._host = HostTopologyInfo(malformed=bool(int(hv[0]) & L.FLAG_MALFORMED),
+                                  num_levels=int(hv[1]), use_morton=bool(use_morton))
     return topo, pos_sorted, mass_sorted, inv
 
 
@@ -457,6 +492,7 @@ def augment_radix_topology_with_octree(topology) -> OctreeTopology:
     base = tuple(getattr(topology, name) for name in _RadixFields._fields)
     out = OctreeTopology(*base, *(o[k] for k in _OctreeFields._fields[len(_RadixFields._fields):]))
     out._dev = _dev_of(topology)
+    out._host = _host_of(topology)
     out._max_cell_depth = depth_hint
     return out
 
@@ -805,7 +841,7 @@ def get_nodes_by_level(tree) -> torch.Tensor:
 
 
 def get_num_levels(tree) -> int:
-    return int(resolve_tree_topology(tree).num_levels)
+    return _host_of(resolve_tree_topology(tree)).num_levels
 
 
 __all__ = [
