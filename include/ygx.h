@@ -296,11 +296,14 @@ int ygx_traverse_fill_predicted(int64_t total, int64_t num_internal, int64_t wf_
  * optionally the dense neighbour_leaf_positions table (L x max_nbr).
  * far_raw_off / near_raw_off (device int64 per row, may be null) say where
  * each raw row starts when the raw rows are not at the output offsets (the
- * predicted walk's padded rows). */
+ * predicted walk's padded rows); far_row_base / near_row_base (int32 per
+ * row, may be null) are subtracted from every node id written for the row
+ * (the batched forest writes each set's lists in its local node ids). */
 int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capacity,
                           int64_t log_capacity, const int32_t* level32, const int32_t* leafpos32,
                           int index_bits, int32_t* far_src32, int32_t* near_nbr32,
                           const int64_t* far_raw_off, const int64_t* near_raw_off,
+                          const int32_t* far_row_base, const int32_t* near_row_base,
                           void* far_sources,
                           void* far_targets, void* target_levels, void* neighbors,
                           void* neighbor_leaf_positions, int64_t max_nbr, void* ws,
@@ -344,6 +347,78 @@ int ygx_predict_caps(const float* center, const float* radius, const float* max_
                      int root, float theta, int mac, const float* params, float slack_far,
                      float slack_near, int32_t add, int32_t* far_cap32, int32_t* near_cap32,
                      cudaStream_t stream);
+
+/* ---- batched sets (no counterpart in the reference: many independent point
+ * sets, stored back to back, built and walked together; every set's slice of
+ * every output equals what the single-set entry points give for it) --------
+ * Set s = points offsets[s] .. offsets[s+1] (device int64, S + 1), S <= 65536.
+ * The forest: set s has L_s leaves at global leaf positions leaf_off[s] ..
+ * leaf_off[s+1] and 2 L_s - 1 nodes at global node ids NO_s = 2 leaf_off[s] - s,
+ * in the per-tree layout (internal nodes first). */
+size_t ygx_batch_encode_sort_workspace_size(int64_t n);
+/* infer_bounds / morton_encode_impl / the stable argsort
+ * (bounds.py:11-33, morton.py:43-77, _tree_impl.py:401) of every set:
+ * bounds_out (S x 6), codes_sorted and order_out (global input index) in
+ * (set, code, index) order, seg_sorted_out (may be null) the set of each. */
+int ygx_batch_encode_sort(const float* positions, int64_t n, const int64_t* offsets, int64_t S,
+                          float* bounds_out, uint64_t* codes_sorted, uint32_t* order_out,
+                          int32_t* seg_sorted_out, void* ws, size_t ws_bytes,
+                          cudaStream_t stream);
+/* _tree_impl.py:1047-1050, :900-910 per set (local particle_indices / inverse). */
+int ygx_batch_reorder(const float* positions, const float* masses, const uint32_t* order,
+                      const int32_t* seg_sorted, const int64_t* offsets, int64_t n, int index_bits,
+                      float* positions_sorted, float* masses_sorted, void* particle_indices,
+                      void* inverse, cudaStream_t stream);
+size_t ygx_batch_leaf_offsets_workspace_size(int64_t S);
+/* leaf_off (device, S + 1) = exclusive scan of ceil(n_s / leaf_size);
+ * *total_leaves_out (host).  Synchronizes the stream. */
+int ygx_batch_leaf_offsets(const int64_t* offsets, int64_t S, int64_t leaf_size,
+                           int64_t* leaf_off, int64_t* total_leaves_out, void* ws,
+                           size_t ws_bytes, cudaStream_t stream);
+/* _tree_impl.py:405-406 per set; leaf_seg = set of each global leaf. */
+int ygx_batch_leaves(const uint64_t* codes_sorted, const int64_t* offsets, const int64_t* leaf_off,
+                     int64_t S, int64_t total_leaves, int64_t leaf_size, int index_bits,
+                     void* leaf_starts, void* leaf_ends, uint64_t* leaf_codes, void* leaf_depths,
+                     int32_t* leaf_seg, cudaStream_t stream);
+size_t ygx_batch_topology_workspace_size(int64_t total_leaves, int64_t S);
+/* _build_tree_from_leaf_partitions (_tree_impl.py:1009-1355) for every set:
+ * per-set arrays with local values (parent / node_ranges / node_level /
+ * nodes_by_level: 2 total_leaves - S; left / right / flags: total_leaves - S;
+ * level_offsets S x 65; num_levels S), int32 copies with global node ids,
+ * node_seg32 / leafpos32 / node_base32 (per node), leaf_base32 (per leaf),
+ * seg_flags (S) and their union tree_flags_out. */
+int ygx_batch_build_topology(const uint64_t* leaf_codes, const void* leaf_starts,
+                             const void* leaf_ends, const int64_t* leaf_off,
+                             const int32_t* leaf_seg, int64_t S, int64_t total_leaves,
+                             int index_bits, void* parent, void* left, void* right,
+                             uint8_t* left_is_leaf, uint8_t* right_is_leaf, void* node_ranges,
+                             void* node_level, void* level_offsets, void* nodes_by_level,
+                             void* num_levels, int32_t* parent32, int32_t* left32,
+                             int32_t* right32, int32_t* level32, int32_t* nbl32,
+                             int32_t* node_seg32, int32_t* leafpos32, int32_t* node_base32,
+                             int32_t* leaf_base32, uint32_t* seg_flags, uint32_t* tree_flags_out,
+                             void* ws, size_t ws_bytes, cudaStream_t stream);
+/* compute_tree_geometry (_geometry_impl.py:176-338) for every tree of the
+ * forest (particle ranges; workspace ygx_geometry_workspace_size(total)). */
+int ygx_batch_tree_geometry(const void* node_ranges, int64_t total, int64_t S,
+                            const int64_t* leaf_off, const int32_t* leaf_seg,
+                            int64_t total_leaves, const int64_t* offsets, int index_bits,
+                            const int32_t* parent32, const int32_t* left32,
+                            const int32_t* right32, const int32_t* level32,
+                            const uint32_t* seg_flags, const float* positions_sorted,
+                            int64_t max_leaf_size, float* center, float* half_extent,
+                            float* radius, float* max_extent, void* ws, size_t ws_bytes,
+                            cudaStream_t stream);
+/* ygx_traverse_walk (YGX_WALK_LOG) over all trees of the forest at once;
+ * ygx_traverse_fill / ygx_traverse_finalize (with the node / leaf bases as
+ * row bases) follow on the same workspace. */
+int ygx_batch_traverse_walk(const float* center, const float* radius, const float* max_extent,
+                            const int32_t* left32, const int32_t* right32,
+                            const int32_t* leafpos32, const int32_t* parent32, int64_t total,
+                            const int64_t* leaf_off, int64_t S, const uint32_t* seg_flags,
+                            int mac, float theta, float dehnen_radius_scale, int gens_hint,
+                            int64_t wf_capacity, int64_t log_capacity, uint64_t* stats_out,
+                            uint32_t* flags_out, void* ws, size_t ws_bytes, cudaStream_t stream);
 
 int ygx_traverse_status(const void* ws, uint32_t* flags_out, cudaStream_t stream);
 

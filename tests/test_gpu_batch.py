@@ -1,0 +1,90 @@
+"""Batched point sets on the GPU: every set's slice of the batched build,
+geometry and lists equals (bit for bit) what the single-set path returns for
+that set alone -- uneven sizes, single-leaf sets, sets with many identical
+points (tied leaf codes) and collinear sets included."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOPO_FIELDS = ["parent", "left_child", "right_child", "left_is_leaf", "right_is_leaf",
+               "particle_indices", "morton_codes", "node_ranges", "node_level", "level_offsets",
+               "nodes_by_level", "num_levels", "bounds_min", "bounds_max", "leaf_codes",
+               "leaf_depths"]
+FAR_FIELDS = ["offsets", "sources", "targets", "counts", "level_offsets", "target_levels"]
+NEAR_FIELDS = ["offsets", "neighbors", "leaf_indices", "counts", "particle_order_leaf_indices",
+               "particle_order_to_native_leaf", "neighbor_leaf_positions"]
+
+
+def _sets(seed=5):
+    from yggdrax_b200 import inputs
+
+    rng = np.random.default_rng(seed)
+    sets = []
+    sizes = [1, 3, 16, 17, 33, 250, 1000, 4097] + list(rng.integers(2, 3000, 24))
+    for k, n in enumerate(sizes):
+        if k % 2:
+            p, m = inputs.plummer(int(n), 100 + k)
+        else:
+            p, m = inputs.uniform_cube(int(n), 100 + k)
+        sets.append((p, m))
+    dup = np.zeros((80, 3), np.float32)
+    dup[40:] = rng.uniform(-1, 1, (40, 3))
+    sets.append((dup, np.ones(80, np.float32)))                       # tied codes
+    sets.append((np.zeros((50, 3), np.float32), np.ones(50, np.float32)))  # all identical
+    col = np.stack([np.arange(300, dtype=np.float32), np.zeros(300, np.float32),
+                    np.zeros(300, np.float32)], 1)
+    sets.append((col, np.ones(300, np.float32)))
+    return sets
+
+
+def _eq(name, a, b):
+    a = a.detach().cpu().numpy() if hasattr(a, "detach") else np.asarray(a)
+    b = b.detach().cpu().numpy() if hasattr(b, "detach") else np.asarray(b)
+    assert a.shape == b.shape, f"{name}: {a.shape} vs {b.shape}"
+    if a.dtype.kind == "f":
+        assert np.array_equal(a.view(np.uint32), b.astype(a.dtype).view(np.uint32)), name
+    else:
+        assert np.array_equal(a.astype(np.int64) if a.dtype != np.uint64 else a,
+                              b.astype(np.int64) if b.dtype != np.uint64 else b), name
+
+
+@pytest.mark.parametrize("leaf", [16, 1])
+def test_batched_sets_match_single_set_path(cuda_device, leaf):
+    import torch
+
+    import yggdrax_b200 as yb
+    from yggdrax_b200 import batch as B
+
+    sets = _sets()
+    pos = np.concatenate([p for p, _ in sets])
+    mass = np.concatenate([m for _, m in sets])
+    off = np.concatenate([[0], np.cumsum([len(p) for p, _ in sets])]).astype(np.int64)
+    P = torch.from_numpy(pos).to(cuda_device)
+    M = torch.from_numpy(mass).to(cuda_device)
+    bt = B.build_trees_batched(P, M, off, leaf_size=leaf)
+    bg = B.compute_tree_geometry_batched(bt)
+    bi = B.build_interactions_and_neighbors_batched(bt, bg, theta=0.6, mac_type="dehnen")
+    for i, (p, m) in enumerate(sets):
+        pi, mi = torch.from_numpy(p).to(cuda_device), torch.from_numpy(m).to(cuda_device)
+        t, ps, ms, inv = yb.build_tree(pi, mi, leaf_size=leaf, return_reordered=True)[:4]
+        tb = bt.tree(i)
+        for f in TOPO_FIELDS:
+            _eq(f"set {i} {f}", getattr(tb, f), getattr(t, f))
+        a, b = int(off[i]), int(off[i + 1])
+        _eq(f"set {i} positions_sorted", bt.positions_sorted[a:b], ps)
+        _eq(f"set {i} masses_sorted", bt.masses_sorted[a:b], ms)
+        _eq(f"set {i} inverse", bt.inverse_permutation[a:b], inv)
+        g = yb.compute_tree_geometry(t, ps)
+        gb = bg.geometry(bt, i)
+        for f in ("center", "half_extent", "radius", "max_extent"):
+            _eq(f"set {i} {f}", getattr(gb, f), getattr(g, f))
+        if int(t.num_internal_nodes) == 0:
+            continue
+        fi, ni_ = yb.build_interactions_and_neighbors(t, g, theta=0.6, mac_type="dehnen")
+        fb, nb = bi.lists(bt, i)
+        for f in FAR_FIELDS:
+            _eq(f"set {i} far.{f}", getattr(fb, f), getattr(fi, f))
+        for f in NEAR_FIELDS:
+            _eq(f"set {i} near.{f}", getattr(nb, f), getattr(ni_, f))

@@ -97,9 +97,20 @@ _SIGS = {
     "ygx_mlp_train_step": (I32, [P, P, P, I32, F32, P, P, P, I64, P, P, SZ, P]),
     "ygx_predict_caps": (I32, [P, P, P, P, P, P, I64, I64, P, I32, I32, F32, I32, P, F32, F32,
                                I32, P, P, P]),
-    "ygx_traverse_finalize": (I32, [I64, I64, I64, I64, P, P, I32, P, P, P, P, P, P, P, P, P, I64,
-                                    P, SZ,
-                                    P]),
+    "ygx_traverse_finalize": (I32, [I64, I64, I64, I64, P, P, I32, P, P, P, P, P, P, P, P, P, P,
+                                    P, I64, P, SZ, P]),
+    "ygx_batch_encode_sort_workspace_size": (SZ, [I64]),
+    "ygx_batch_encode_sort": (I32, [P, I64, P, I64, P, P, P, P, P, SZ, P]),
+    "ygx_batch_reorder": (I32, [P, P, P, P, P, I64, I32, P, P, P, P, P]),
+    "ygx_batch_leaf_offsets_workspace_size": (SZ, [I64]),
+    "ygx_batch_leaf_offsets": (I32, [P, I64, I64, P, P, P, SZ, P]),
+    "ygx_batch_leaves": (I32, [P, P, P, I64, I64, I64, I32, P, P, P, P, P, P]),
+    "ygx_batch_topology_workspace_size": (SZ, [I64, I64]),
+    "ygx_batch_build_topology": (I32, [P, P, P, P, P, I64, I64, I32] + [P] * 22 + [SZ, P]),
+    "ygx_batch_tree_geometry": (I32, [P, I64, I64, P, P, I64, P, I32, P, P, P, P, P, P, I64, P, P,
+                                      P, P, P, SZ, P]),
+    "ygx_batch_traverse_walk": (I32, [P, P, P, P, P, P, P, I64, P, I64, P, I32, F32, F32, I32,
+                                      I64, I64, P, P, P, SZ, P]),
 }
 
 _lib: Optional[ctypes.CDLL] = None

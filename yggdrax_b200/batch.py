@@ -1,0 +1,393 @@
+"""Batched point sets: many independent trees built, measured and walked
+together.
+
+Sets are stored back to back in one position / mass array and described by
+``offsets`` (``S + 1`` entries, set ``s`` = points ``offsets[s] ..
+offsets[s+1]``).  Every stage runs once for all sets: Morton codes with each
+set's own bounds, one stable sort by (set, code), the Karras forest (set
+``s`` at global node ids ``2 * leaf_off[s] - s`` in the per-tree layout),
+bottom-up geometry over the forest, and one dual-tree walk whose first
+wavefront holds the root pair of every set.  The per-set accessors return
+exactly what the single-set functions (``build_tree``,
+``compute_tree_geometry``, ``build_interactions_and_neighbors``) return for
+that set alone: local node ids, the set's own offsets.
+
+This has no counterpart in the reference, which builds one set per call.
+Adaptive radix trees only (``leaf_size`` partitions).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .dtypes import INDEX_BITS, INDEX_DTYPE
+from .geometry import TreeGeometry
+from .interactions import (_CAPACITY_HINTS, _MAC_CODES, NodeInteractionList, NodeNeighborList,
+                           _dense_neighbor_budget)
+from .tree import MAX_TREE_LEVELS, RadixTreeTopology
+
+_GENS_HINTS_BATCH: dict = {}
+
+
+@dataclass
+class BatchedTrees:
+    """The forest of S radix trees (packed per-set arrays, local values)."""
+
+    offsets: torch.Tensor            # (S+1,) int64, device
+    leaf_off: torch.Tensor           # (S+1,) int64, device
+    leaf_size: int
+    positions_sorted: torch.Tensor   # (n, 3)
+    masses_sorted: torch.Tensor      # (n,)
+    inverse_permutation: torch.Tensor
+    particle_indices: torch.Tensor   # (n,) local to each set
+    morton_codes: torch.Tensor       # (n,) uint64, sets' sorted codes
+    bounds: torch.Tensor             # (S, 6)
+    leaf_starts: torch.Tensor
+    leaf_ends: torch.Tensor
+    leaf_codes: torch.Tensor
+    leaf_depths: torch.Tensor
+    parent: torch.Tensor             # (total,) local parent
+    left_child: torch.Tensor         # (total_leaves - S,)
+    right_child: torch.Tensor
+    left_is_leaf: torch.Tensor
+    right_is_leaf: torch.Tensor
+    node_ranges: torch.Tensor        # (total, 2) local particle ranges
+    node_level: torch.Tensor
+    level_offsets: torch.Tensor      # (S, 65)
+    nodes_by_level: torch.Tensor     # (total,) local ids
+    num_levels: torch.Tensor         # (S,)
+    # int32 device copies with global node ids
+    parent32: torch.Tensor = field(repr=False, default=None)
+    left32: torch.Tensor = field(repr=False, default=None)
+    right32: torch.Tensor = field(repr=False, default=None)
+    level32: torch.Tensor = field(repr=False, default=None)
+    nbl32: torch.Tensor = field(repr=False, default=None)
+    node_seg32: torch.Tensor = field(repr=False, default=None)
+    leaf_seg32: torch.Tensor = field(repr=False, default=None)
+    leafpos32: torch.Tensor = field(repr=False, default=None)
+    node_base32: torch.Tensor = field(repr=False, default=None)
+    leaf_base32: torch.Tensor = field(repr=False, default=None)
+    seg_flags: torch.Tensor = field(repr=False, default=None)
+    # host copies for slicing
+    offsets_host: np.ndarray = field(repr=False, default=None)
+    leaf_off_host: np.ndarray = field(repr=False, default=None)
+
+    @property
+    def num_sets(self) -> int:
+        return int(self.offsets_host.shape[0]) - 1
+
+    @property
+    def total_leaves(self) -> int:
+        return int(self.leaf_off_host[-1])
+
+    @property
+    def total_nodes(self) -> int:
+        return 2 * self.total_leaves - self.num_sets
+
+    def node_block(self, i: int):
+        a, b = int(self.leaf_off_host[i]), int(self.leaf_off_host[i + 1])
+        return 2 * a - i, 2 * (b - a) - 1
+
+    def tree(self, i: int) -> RadixTreeTopology:
+        """Set i's topology, as build_tree gives it for that set alone."""
+        a, b = int(self.leaf_off_host[i]), int(self.leaf_off_host[i + 1])
+        p0, p1 = int(self.offsets_host[i]), int(self.offsets_host[i + 1])
+        no, tot = self.node_block(i)
+        io = a - i
+        dev = self.parent.device
+        t = RadixTreeTopology(
+            parent=self.parent[no:no + tot], left_child=self.left_child[io:io + b - a - 1],
+            right_child=self.right_child[io:io + b - a - 1],
+            left_is_leaf=self.left_is_leaf[io:io + b - a - 1],
+            right_is_leaf=self.right_is_leaf[io:io + b - a - 1],
+            particle_indices=self.particle_indices[p0:p1], morton_codes=self.morton_codes[p0:p1],
+            node_ranges=self.node_ranges[no:no + tot], num_particles=p1 - p0,
+            num_internal_nodes=b - a - 1, node_level=self.node_level[no:no + tot],
+            level_offsets=self.level_offsets[i], nodes_by_level=self.nodes_by_level[no:no + tot],
+            num_levels=self.num_levels[i], bounds_min=self.bounds[i, :3],
+            bounds_max=self.bounds[i, 3:], leaf_codes=self.leaf_codes[a:b],
+            leaf_depths=self.leaf_depths[a:b],
+            use_morton_geometry=torch.zeros((), dtype=torch.bool, device=dev),
+            leaf_size=self.leaf_size)
+        return t
+
+
+def build_trees_batched(positions: torch.Tensor, masses: torch.Tensor, offsets,
+                        *, leaf_size: int = 16) -> BatchedTrees:
+    """Adaptive radix trees (``build_tree(..., leaf_size)``) of S point sets."""
+    lib = L.lib()
+    if leaf_size < 1:
+        raise ValueError("leaf_size must be >= 1")
+    dev = positions.device
+    st = L.stream_handle(dev)
+    ib, idt = INDEX_BITS, INDEX_DTYPE
+    pos = positions.contiguous().float()
+    mass = masses.contiguous().float()
+    n = int(pos.shape[0])
+    off_host = np.asarray(offsets.cpu() if torch.is_tensor(offsets) else offsets, dtype=np.int64)
+    S = int(off_host.shape[0]) - 1
+    if S < 1 or S > (1 << 16):
+        raise ValueError("between 1 and 65536 sets are supported")
+    if off_host[0] != 0 or off_host[-1] != n or np.any(np.diff(off_host) < 1):
+        raise ValueError("offsets must start at 0, end at len(positions) and give every set "
+                         ">= 1 point")
+    off = torch.from_numpy(off_host).to(dev)
+    ws = L.workspace(lib.ygx_batch_encode_sort_workspace_size(n), dev)
+    bounds = torch.empty((S, 6), dtype=torch.float32, device=dev)
+    codes = torch.empty(n, dtype=torch.uint64, device=dev)
+    order = torch.empty(n, dtype=torch.int32, device=dev)
+    seg_sorted = torch.empty(n, dtype=torch.int32, device=dev)
+    L.check(lib.ygx_batch_encode_sort(L.ptr(pos), n, L.ptr(off), S, L.ptr(bounds), L.ptr(codes),
+                                      L.ptr(order), L.ptr(seg_sorted), L.ptr(ws), ws.numel(), st),
+            "ygx_batch_encode_sort")
+    pos_s = torch.empty_like(pos)
+    mass_s = torch.empty_like(mass)
+    pidx = torch.empty(n, dtype=idt, device=dev)
+    inv = torch.empty(n, dtype=idt, device=dev)
+    L.check(lib.ygx_batch_reorder(L.ptr(pos), L.ptr(mass), L.ptr(order), L.ptr(seg_sorted),
+                                  L.ptr(off), n, ib, L.ptr(pos_s), L.ptr(mass_s), L.ptr(pidx),
+                                  L.ptr(inv), st), "ygx_batch_reorder")
+    leaf_off = torch.empty(S + 1, dtype=torch.int64, device=dev)
+    wsl = L.workspace(lib.ygx_batch_leaf_offsets_workspace_size(S), dev)
+    ltot = np.zeros(1, np.int64)
+    L.check(lib.ygx_batch_leaf_offsets(L.ptr(off), S, int(leaf_size), L.ptr(leaf_off),
+                                       ltot.ctypes.data, L.ptr(wsl), wsl.numel(), st),
+            "ygx_batch_leaf_offsets")
+    Lt = int(ltot[0])
+    starts = torch.empty(Lt, dtype=idt, device=dev)
+    ends = torch.empty(Lt, dtype=idt, device=dev)
+    lcodes = torch.empty(Lt, dtype=torch.uint64, device=dev)
+    ldepths = torch.empty(Lt, dtype=idt, device=dev)
+    leaf_seg = torch.empty(Lt, dtype=torch.int32, device=dev)
+    L.check(lib.ygx_batch_leaves(L.ptr(codes), L.ptr(off), L.ptr(leaf_off), S, Lt, int(leaf_size),
+                                 ib, L.ptr(starts), L.ptr(ends), L.ptr(lcodes), L.ptr(ldepths),
+                                 L.ptr(leaf_seg), st), "ygx_batch_leaves")
+    total, ni = 2 * Lt - S, Lt - S
+    e = lambda k, dt=idt: torch.empty(k, dtype=dt, device=dev)  # noqa: E731
+    i32 = torch.int32
+    out = dict(parent=e(total), left=e(max(ni, 0)), right=e(max(ni, 0)),
+               lil=e(max(ni, 0), torch.bool), ril=e(max(ni, 0), torch.bool),
+               ranges=torch.empty((total, 2), dtype=idt, device=dev), node_level=e(total),
+               level_offsets=torch.empty((S, MAX_TREE_LEVELS + 1), dtype=idt, device=dev),
+               nbl=e(total), num_levels=e(S), parent32=e(total, i32), left32=e(total, i32),
+               right32=e(total, i32), level32=e(total, i32), nbl32=e(total, i32),
+               node_seg32=e(total, i32), leafpos32=e(total, i32), node_base32=e(total, i32),
+               leaf_base32=e(Lt, i32), seg_flags=e(S, i32), tree_flags=e(1, i32))
+    wst = L.workspace(lib.ygx_batch_topology_workspace_size(Lt, S), dev)
+    L.check(lib.ygx_batch_build_topology(
+        L.ptr(lcodes), L.ptr(starts), L.ptr(ends), L.ptr(leaf_off), L.ptr(leaf_seg), S, Lt, ib,
+        *[L.ptr(out[k]) for k in ("parent", "left", "right", "lil", "ril", "ranges", "node_level",
+                                  "level_offsets", "nbl", "num_levels", "parent32", "left32",
+                                  "right32", "level32", "nbl32", "node_seg32", "leafpos32",
+                                  "node_base32", "leaf_base32", "seg_flags", "tree_flags")],
+        L.ptr(wst), wst.numel(), st), "ygx_batch_build_topology")
+    return BatchedTrees(
+        offsets=off, leaf_off=leaf_off, leaf_size=int(leaf_size), positions_sorted=pos_s,
+        masses_sorted=mass_s, inverse_permutation=inv, particle_indices=pidx,
+        morton_codes=codes, bounds=bounds, leaf_starts=starts, leaf_ends=ends, leaf_codes=lcodes,
+        leaf_depths=ldepths, parent=out["parent"], left_child=out["left"],
+        right_child=out["right"], left_is_leaf=out["lil"], right_is_leaf=out["ril"],
+        node_ranges=out["ranges"], node_level=out["node_level"],
+        level_offsets=out["level_offsets"], nodes_by_level=out["nbl"],
+        num_levels=out["num_levels"], parent32=out["parent32"], left32=out["left32"],
+        right32=out["right32"], level32=out["level32"], nbl32=out["nbl32"],
+        node_seg32=out["node_seg32"], leaf_seg32=leaf_seg, leafpos32=out["leafpos32"],
+        node_base32=out["node_base32"], leaf_base32=out["leaf_base32"],
+        seg_flags=out["seg_flags"].view(torch.int32), offsets_host=off_host,
+        leaf_off_host=leaf_off.cpu().numpy())
+
+
+@dataclass
+class BatchedGeometry:
+    center: torch.Tensor
+    half_extent: torch.Tensor
+    radius: torch.Tensor
+    max_extent: torch.Tensor
+
+    def geometry(self, batch: BatchedTrees, i: int) -> TreeGeometry:
+        no, tot = batch.node_block(i)
+        return TreeGeometry(center=self.center[no:no + tot],
+                            half_extent=self.half_extent[no:no + tot],
+                            radius=self.radius[no:no + tot],
+                            max_extent=self.max_extent[no:no + tot])
+
+
+def compute_tree_geometry_batched(batch: BatchedTrees) -> BatchedGeometry:
+    """``compute_tree_geometry(tree_s, positions_sorted_s, max_leaf_size=leaf_size)``
+    for every set."""
+    lib = L.lib()
+    dev = batch.parent.device
+    total = batch.total_nodes
+    g = BatchedGeometry(center=torch.empty((total, 3), dtype=torch.float32, device=dev),
+                        half_extent=torch.empty((total, 3), dtype=torch.float32, device=dev),
+                        radius=torch.empty(total, dtype=torch.float32, device=dev),
+                        max_extent=torch.empty(total, dtype=torch.float32, device=dev))
+    ws = L.workspace(lib.ygx_geometry_workspace_size(total), dev)
+    L.check(lib.ygx_batch_tree_geometry(
+        L.ptr(batch.node_ranges), total, batch.num_sets, L.ptr(batch.leaf_off),
+        L.ptr(batch.leaf_seg32), batch.total_leaves, L.ptr(batch.offsets), INDEX_BITS,
+        L.ptr(batch.parent32), L.ptr(batch.left32), L.ptr(batch.right32), L.ptr(batch.level32),
+        L.ptr(batch.seg_flags), L.ptr(batch.positions_sorted), int(batch.leaf_size),
+        L.ptr(g.center), L.ptr(g.half_extent), L.ptr(g.radius), L.ptr(g.max_extent), L.ptr(ws),
+        ws.numel(), L.stream_handle(dev)), "ygx_batch_tree_geometry")
+    return g
+
+
+@dataclass
+class BatchedInteractions:
+    """Far / near lists of every set, packed: far rows in level-major order
+    set after set, near rows leaf by leaf; node ids local to each set."""
+
+    node_offsets: torch.Tensor   # (total+1,) global row starts, node-indexed
+    far_counts: torch.Tensor
+    sources: torch.Tensor
+    targets: torch.Tensor
+    target_levels: torch.Tensor
+    near_offsets: torch.Tensor   # (total_leaves+1,)
+    near_counts: torch.Tensor
+    neighbors: torch.Tensor
+    stats: dict
+
+    def lists(self, batch: BatchedTrees, i: int):
+        """(NodeInteractionList, NodeNeighborList) of set i, as
+        build_interactions_and_neighbors gives them for that set alone."""
+        no, tot = batch.node_block(i)
+        a, b = int(batch.leaf_off_host[i]), int(batch.leaf_off_host[i + 1])
+        nl, ni = b - a, b - a - 1
+        dev = self.node_offsets.device
+        idt = self.node_offsets.dtype
+        total = batch.total_nodes
+        nbl = batch.nbl32
+
+        def row_start(x):  # start of the x-th node in level-major order
+            return int(self.node_offsets[int(nbl[x])]) if x < total else int(self.node_offsets[-1])
+
+        f0, f1 = row_start(no), row_start(no + tot)
+        offsets = torch.cat([self.node_offsets[no:no + tot] - f0,
+                             torch.tensor([f1 - f0], dtype=idt, device=dev)])
+        nlev = int(batch.num_levels[i])
+        lo = batch.level_offsets[i].cpu().numpy()
+        level_offsets = torch.tensor([row_start(no + int(lo[l])) - f0 for l in range(nlev + 1)],
+                                     dtype=idt, device=dev)
+        far = NodeInteractionList(
+            offsets=offsets, sources=self.sources[f0:f1], targets=self.targets[f0:f1],
+            counts=self.far_counts[no:no + tot], level_offsets=level_offsets,
+            target_levels=self.target_levels[f0:f1])
+        n0, n1 = int(self.near_offsets[a]), int(self.near_offsets[b])
+        nb = self.neighbors[n0:n1]
+        cnt = self.near_counts[a:b]
+        max_nbr = int(cnt.max()) if nl > 0 else 0
+        nlp = torch.full((nl, max_nbr), -1, dtype=idt, device=dev)
+        if max_nbr > 0 and nl * max_nbr * (4 if INDEX_BITS == 32 else 8) <= \
+                _dense_neighbor_budget(dev):
+            rows = torch.repeat_interleave(torch.arange(nl, device=dev), cnt.long())
+            starts = (self.near_offsets[a:b] - n0).long()
+            cols = torch.arange(n1 - n0, device=dev) - starts[rows]
+            nlp[rows, cols] = nb - ni
+        elif max_nbr > 0:
+            nlp = torch.empty((nl, 0), dtype=idt, device=dev)
+        ar = torch.arange(nl, dtype=idt, device=dev)
+        near = NodeNeighborList(
+            offsets=self.near_offsets[a:b + 1] - n0, neighbors=nb,
+            leaf_indices=ar + ni, counts=cnt, particle_order_leaf_indices=ar + ni,
+            particle_order_to_native_leaf=ar, neighbor_leaf_positions=nlp,
+            target_block_leaf_ids=torch.empty(0, dtype=idt, device=dev),
+            target_block_source_leaf_ids=torch.empty(0, dtype=idt, device=dev),
+            target_block_valid_mask=torch.empty(0, dtype=torch.bool, device=dev),
+            target_block_offsets=torch.zeros(1, dtype=idt, device=dev), target_block_size=0)
+        return far, near
+
+
+def build_interactions_and_neighbors_batched(batch: BatchedTrees, geometry: BatchedGeometry, *,
+                                             theta: float = 0.5, mac_type: str = "bh",
+                                             dehnen_radius_scale: float = 1.0
+                                             ) -> BatchedInteractions:
+    """The exact far / near lists (count-then-fill semantics, no capacities)
+    of every set, from one walk over the whole forest."""
+    if mac_type not in _MAC_CODES:
+        raise ValueError(f"Unknown mac_type '{mac_type}'")
+    if float(dehnen_radius_scale) <= 0.0:
+        raise ValueError("dehnen_radius_scale must be > 0")
+    lib = L.lib()
+    dev = batch.parent.device
+    st = L.stream_handle(dev)
+    ib, idt = INDEX_BITS, INDEX_DTYPE
+    total, Lt, S = batch.total_nodes, batch.total_leaves, batch.num_sets
+    ni = Lt - S
+    mac = _MAC_CODES[mac_type]
+    center = geometry.center.contiguous()
+    radius = geometry.radius.contiguous()
+    max_extent = geometry.max_extent.contiguous()
+    z = lambda *s: torch.zeros(s, dtype=idt, device=dev)  # noqa: E731
+    if ni == 0 or total < 3:  # every set is a single leaf: no pairs
+        return BatchedInteractions(
+            node_offsets=z(total + 1), far_counts=z(total), sources=z(0), targets=z(0),
+            target_levels=z(0), near_offsets=z(Lt + 1), near_counts=z(Lt), neighbors=z(0),
+            stats={})
+    key = ("batch", mac_type, float(theta))
+    hint_wf, hint_log = _CAPACITY_HINTS.get(key, (0.0, 0.0))
+    cap = min((1 << 32) - 4097, max(32 * total + 65536, int(1.25 * hint_wf * total)))
+    log_cap = max(8 * total + 65536, int(1.1 * hint_log * total))
+    while True:
+        ws = L.workspace(lib.ygx_traverse_workspace_size(total, Lt, cap, log_cap), dev)
+        stats = np.zeros(L.TSTAT_WORDS, np.uint64)
+        flags = np.zeros(1, np.uint32)
+        rc = lib.ygx_batch_traverse_walk(
+            L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(batch.left32),
+            L.ptr(batch.right32), L.ptr(batch.leafpos32), L.ptr(batch.parent32), total,
+            L.ptr(batch.leaf_off), S, L.ptr(batch.seg_flags), mac, float(theta),
+            float(dehnen_radius_scale), _GENS_HINTS_BATCH.get(key, 0), cap, log_cap,
+            stats.ctypes.data, flags.ctypes.data, L.ptr(ws), ws.numel(), st)
+        f = int(flags[0])
+        if f & (L.FLAG_QUEUE_OVERFLOW | L.FLAG_LOG_OVERFLOW) and rc == 0:
+            if f & L.FLAG_QUEUE_OVERFLOW:
+                cap = min((1 << 32) - 4097, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
+                log_cap = max(log_cap, int(stats[L.TSTAT["log_need"]]))
+            else:
+                log_cap = int(stats[L.TSTAT["log_need"]])
+            continue
+        L.check(rc, "ygx_batch_traverse_walk")
+        if f & L.FLAG_BAD_INPUT:
+            raise ValueError("MAC extents must be positive (geometry has zero or NaN extents)")
+        if f:
+            raise L.YgxError(f"traversal walk reported flags {f:#x}")
+        break
+    _CAPACITY_HINTS[key] = (int(stats[L.TSTAT["wf_need"]]) / total,
+                            int(stats[L.TSTAT["log_need"]]) / total)
+    _GENS_HINTS_BATCH[key] = int(stats[L.TSTAT["gens"]])
+    s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
+    P, Q = s["far_total"], s["near_total"]
+    node_offsets = torch.empty(total + 1, dtype=idt, device=dev)
+    far_counts = torch.empty(total, dtype=idt, device=dev)
+    level_dummy = torch.zeros(2, dtype=idt, device=dev)
+    level_out = torch.empty(2, dtype=idt, device=dev)
+    near_offsets = torch.empty(Lt + 1, dtype=idt, device=dev)
+    near_counts = torch.empty(Lt, dtype=idt, device=dev)
+    far_src32 = torch.empty(max(P, 1), dtype=torch.int32, device=dev)
+    near_nbr32 = torch.empty(max(Q, 1), dtype=torch.int32, device=dev)
+    L.check(lib.ygx_traverse_fill(
+        total, ni, cap, log_cap, P, Q, L.ptr(batch.nbl32), L.ptr(batch.leafpos32),
+        L.ptr(level_dummy), 0, ib, L.ptr(node_offsets), L.ptr(far_counts), L.ptr(level_out),
+        L.ptr(near_offsets), L.ptr(near_counts), L.ptr(far_src32), L.ptr(near_nbr32), L.ptr(ws),
+        ws.numel(), st), "ygx_traverse_fill")
+    sources = torch.empty(P, dtype=idt, device=dev)
+    targets = torch.empty(P, dtype=idt, device=dev)
+    target_levels = torch.empty(P, dtype=idt, device=dev)
+    neighbors = torch.empty(Q, dtype=idt, device=dev)
+    L.check(lib.ygx_traverse_finalize(
+        total, ni, cap, log_cap, L.ptr(batch.level32), L.ptr(batch.leafpos32), ib,
+        L.ptr(far_src32), L.ptr(near_nbr32), None, None, L.ptr(batch.node_base32),
+        L.ptr(batch.leaf_base32), L.ptr(sources), L.ptr(targets), L.ptr(target_levels),
+        L.ptr(neighbors), None, 0, L.ptr(ws), ws.numel(), st), "ygx_traverse_finalize")
+    f = L.read_status(ws)
+    if f & (L.FLAG_FAR_OVERFLOW | L.FLAG_NEAR_OVERFLOW | L.FLAG_QUEUE_OVERFLOW):
+        raise L.YgxError(f"traversal fill disagreed with the walk (flags {f:#x})")
+    return BatchedInteractions(
+        node_offsets=node_offsets, far_counts=far_counts, sources=sources, targets=targets,
+        target_levels=target_levels, near_offsets=near_offsets, near_counts=near_counts,
+        neighbors=neighbors, stats=s)

@@ -1,6 +1,7 @@
 // Tree build kernels (L1): reorder, leaf partitions (adaptive, fixed depth,
 // local aspect refinement), Karras LBVH topology and node levels.
 #include "scan.cuh"
+#include "karras.cuh"
 #include "sort.cuh"
 
 namespace ygx {
@@ -207,68 +208,16 @@ __global__ void k_refine(const float* __restrict__ pos_sorted, const uint64_t* _
   }
 }
 
-// ---------------------------------------------------------------------------
-// _tree_impl.py:1115-1270: Karras (2012) topology over L >= 2 leaf codes.
-__device__ __forceinline__ int64_t kdelta(const uint64_t* __restrict__ c, int64_t L, int64_t i,
-                                          int64_t j, uint64_t ci) {
-  if (j < 0 || j >= L) return -1;
-  uint64_t cj = c[j];
-  if (ci == cj) return 64 + clz64((uint64_t)i ^ (uint64_t)j);
-  return clz64(ci ^ cj);
-}
-__device__ __forceinline__ int64_t lcp_codes(uint64_t a, uint64_t b) {
-  return a == b ? 64 : clz64(a ^ b);
-}
-
 __global__ void k_karras(const uint64_t* __restrict__ codes, const void* starts, const void* ends,
                          int64_t L, int index_bits, void* left, void* right,
                          uint8_t* __restrict__ lil, uint8_t* __restrict__ ril, void* ranges,
                          int32_t* __restrict__ left32, int32_t* __restrict__ right32,
                          int32_t* __restrict__ parent_claim) {
   const int64_t ni = L - 1;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < L;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    if (i == ni) {
-      // Leaf ranges (one thread per leaf handled below).
-      continue;
-    }
-    const uint64_t ci = codes[i];
-    int64_t dp = kdelta(codes, L, i, i + 1, ci);
-    int64_t dm = kdelta(codes, L, i, i - 1, ci);
-    int64_t d = (dp - dm) > 0 ? 1 : ((dp - dm) < 0 ? -1 : 0);
-    if (i == 0 || d == 0) d = 1;
-    const int64_t dmin = kdelta(codes, L, i, i - d, ci);
-    int64_t span = 0;
-    for (int k = 30; k >= 0; --k) {
-      int64_t step = (int64_t)1 << k;
-      int64_t cand = i + (span + step) * d;
-      if (cand >= 0 && cand < L && kdelta(codes, L, i, cand, ci) > dmin) span += step;
-    }
-    const int64_t end = i + span * d;
-    const int64_t first = i < end ? i : end, last = i < end ? end : i;
-    store_idx(ranges, index_bits, 2 * i, load_idx(starts, index_bits, first));
-    store_idx(ranges, index_bits, 2 * i + 1, load_idx(ends, index_bits, last) - 1);
-    const uint64_t fc = codes[first];
-    const int64_t cp = lcp_codes(fc, codes[last]);
-    int64_t split = first;
-    for (int k = 30; k >= 0; --k) {
-      int64_t mid = split + ((int64_t)1 << k);
-      if (mid < last && lcp_codes(fc, codes[mid]) > cp) split = mid;
-    }
-    const bool ll = split == first, rl = split + 1 == last;
-    const int64_t lc = ll ? ni + first : split;
-    const int64_t rc = rl ? ni + last : split + 1;
-    lil[i] = ll;
-    ril[i] = rl;
-    store_idx(left, index_bits, i, lc);
-    store_idx(right, index_bits, i, rc);
-    left32[i] = (int32_t)lc;
-    right32[i] = (int32_t)rc;
-    // Serial-scatter semantics of parent.at[left].set / .at[right].set:
-    // any right claim beats every left claim, larger index wins within a side.
-    atomicMax(&parent_claim[lc], (int32_t)i);
-    atomicMax(&parent_claim[rc], (int32_t)(i + ni));
-  }
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ni;
+       i += (int64_t)gridDim.x * blockDim.x)
+    karras_node(codes, starts, ends, L, i, index_bits, left, right, lil, ril, ranges, left32,
+                right32, parent_claim, 0);
 }
 
 __global__ void k_leaf_ranges(const void* starts, const void* ends, int64_t L, int index_bits,
@@ -399,6 +348,221 @@ __global__ void k_u32_to_index(const uint32_t* __restrict__ in, int64_t n, int i
        k += (int64_t)gridDim.x * blockDim.x) {
     store_idx(out, index_bits, k, in[k]);
     if (out32) out32[k] = (int32_t)in[k];
+  }
+}
+
+// ---- batched sets: a forest of per-set trees --------------------------------
+// Set s has L_s leaves at global leaf positions [leaf_off[s], leaf_off[s+1])
+// and its 2 L_s - 1 nodes at global node ids [NO_s, NO_s + 2 L_s - 1) with
+// NO_s = 2 leaf_off[s] - s, in the reference's per-tree layout (internal
+// nodes first).  Per-set output arrays hold local values (what build_tree
+// gives for that set alone); the int32 copies hold global node ids.
+
+__device__ __forceinline__ int64_t seg_search(const int64_t* __restrict__ off, int64_t S,
+                                              int64_t g) {
+  int64_t lo = 0, hi = S;  // last s with off[s] <= g
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (off[mid] <= g) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Per-set reorder: positions / masses gathered into the sets' sorted order,
+// particle_indices and the inverse permutation local to each set.
+__global__ void k_seg_reorder(const float* __restrict__ pos, const float* __restrict__ mass,
+                              const uint32_t* __restrict__ order,
+                              const int32_t* __restrict__ seg_sorted,
+                              const int64_t* __restrict__ off, int64_t n, int index_bits,
+                              float* __restrict__ pos_sorted, float* __restrict__ mass_sorted,
+                              void* particle_indices, void* inverse) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = order[k];
+    const int64_t base = off[seg_sorted[k]];
+    pos_sorted[3 * k] = __ldg(pos + 3 * (int64_t)v);
+    pos_sorted[3 * k + 1] = __ldg(pos + 3 * (int64_t)v + 1);
+    pos_sorted[3 * k + 2] = __ldg(pos + 3 * (int64_t)v + 2);
+    if (mass_sorted) mass_sorted[k] = __ldg(mass + v);
+    if (particle_indices) store_idx(particle_indices, index_bits, k, (int64_t)v - base);
+    if (inverse) store_idx(inverse, index_bits, v, k - base);
+  }
+}
+
+__global__ void k_seg_leaf_counts(const int64_t* __restrict__ off, int64_t S, int64_t leaf,
+                                  int32_t* __restrict__ cnt) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < S;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t n = off[s + 1] - off[s];
+    cnt[s] = (int32_t)((n + leaf - 1) / leaf);
+  }
+}
+
+// _tree_impl.py:405-406 per set: fixed-size chunks of the set's sorted order.
+__global__ void k_seg_leaves(const uint64_t* __restrict__ codes, const int64_t* __restrict__ off,
+                             const int64_t* __restrict__ leaf_off, int64_t S, int64_t Ltot,
+                             int64_t leaf, int index_bits, void* starts, void* ends,
+                             uint64_t* __restrict__ leaf_codes, void* depths,
+                             int32_t* __restrict__ leaf_seg) {
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < Ltot;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t sg = seg_search(leaf_off, S, g);
+    const int64_t j = g - leaf_off[sg], n = off[sg + 1] - off[sg];
+    const int64_t b = j * leaf, e = b + leaf < n ? b + leaf : n;
+    store_idx(starts, index_bits, g, b);
+    store_idx(ends, index_bits, g, e);
+    leaf_codes[g] = codes[off[sg] + b];
+    if (depths) store_idx(depths, index_bits, g, -1);
+    leaf_seg[g] = (int32_t)sg;
+  }
+}
+
+__device__ __forceinline__ void* idx_ptr(void* base, int index_bits, int64_t k) {
+  return (char*)base + k * (index_bits == 32 ? 4 : 8);
+}
+__device__ __forceinline__ const void* idx_ptr(const void* base, int index_bits, int64_t k) {
+  return (const char*)base + k * (index_bits == 32 ? 4 : 8);
+}
+
+// One thread per global leaf position: the internal node of that position
+// (if any) through karras_node on the set's slice, the leaf node's range,
+// and the set id of both nodes.
+__global__ void k_seg_karras(const uint64_t* __restrict__ codes, const void* starts,
+                             const void* ends, const int64_t* __restrict__ leaf_off,
+                             const int32_t* __restrict__ leaf_seg, int64_t Ltot, int index_bits,
+                             void* left, void* right, uint8_t* __restrict__ lil,
+                             uint8_t* __restrict__ ril, void* ranges,
+                             int32_t* __restrict__ left32, int32_t* __restrict__ right32,
+                             int32_t* __restrict__ parent_claim,
+                             int32_t* __restrict__ node_seg, int32_t* __restrict__ leafpos32,
+                             int32_t* __restrict__ node_base, int32_t* __restrict__ leaf_base) {
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < Ltot;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t sg = leaf_seg[g];
+    const int64_t a = leaf_off[sg], Ls = leaf_off[sg + 1] - a, j = g - a;
+    const int64_t NO = 2 * a - sg, IO = a - sg;
+    if (j < Ls - 1) {
+      karras_node(codes + a, idx_ptr(starts, index_bits, a), idx_ptr(ends, index_bits, a), Ls, j,
+                  index_bits, idx_ptr(left, index_bits, IO), idx_ptr(right, index_bits, IO),
+                  lil + IO, ril + IO, idx_ptr(ranges, index_bits, 2 * NO), left32 + NO,
+                  right32 + NO, parent_claim + NO, NO);
+      node_seg[NO + j] = sg;
+      leafpos32[NO + j] = -1;
+      node_base[NO + j] = (int32_t)NO;
+    }
+    const int64_t node = NO + Ls - 1 + j;
+    leafpos32[node] = (int32_t)g;  // near rows: the sets' leaves back to back
+    node_base[node] = (int32_t)NO;
+    leaf_base[g] = (int32_t)NO;
+    store_idx(ranges, index_bits, 2 * node, load_idx(starts, index_bits, g));
+    store_idx(ranges, index_bits, 2 * node + 1, load_idx(ends, index_bits, g) - 1);
+    left32[node] = -1;
+    right32[node] = -1;
+    node_seg[node] = sg;
+  }
+}
+
+__global__ void k_seg_parent_decode(const int32_t* __restrict__ claim,
+                                    const int32_t* __restrict__ node_seg,
+                                    const int64_t* __restrict__ leaf_off, int64_t total,
+                                    int index_bits, void* parent, int32_t* __restrict__ parent32) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t sg = node_seg[k];
+    const int64_t a = leaf_off[sg], Ls = leaf_off[sg + 1] - a, NO = 2 * a - sg, ni = Ls - 1;
+    const int32_t c = claim[k];
+    const int64_t p = c < 0 ? -1 : (c >= ni ? c - ni : c);
+    store_idx(parent, index_bits, k, p);
+    parent32[k] = p < 0 ? -1 : (int32_t)(NO + p);
+  }
+}
+
+__global__ void k_seg_check_wellformed(const int32_t* __restrict__ parent32,
+                                       const int32_t* __restrict__ left32,
+                                       const int32_t* __restrict__ right32,
+                                       const int32_t* __restrict__ node_seg,
+                                       const int64_t* __restrict__ leaf_off, int64_t total,
+                                       uint32_t* __restrict__ seg_flags,
+                                       uint32_t* __restrict__ tree_flags) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t sg = node_seg[k];
+    const int64_t a = leaf_off[sg], Ls = leaf_off[sg + 1] - a, NO = 2 * a - sg;
+    const int64_t x = k - NO;
+    bool bad = x == 0 ? parent32[k] != -1 : parent32[k] < 0;
+    if (x < Ls - 1)
+      bad = bad || parent32[left32[k]] != (int32_t)k || parent32[right32[k]] != (int32_t)k;
+    if (bad) {
+      atomicOr(&seg_flags[sg], kFlagMalformed);
+      atomicOr(tree_flags, kFlagMalformed);
+    }
+  }
+}
+
+// Levels of the forest (pointer doubling ran over all sets at once), the
+// per-set level histograms and maxima, and (set, level) sort keys.  A node
+// whose root is not its set's node 0 marks its set malformed.
+__global__ void k_seg_depth_finish(const int32_t* __restrict__ sc0, const int32_t* __restrict__ d0,
+                                   const int32_t* __restrict__ sc1, const int32_t* __restrict__ d1,
+                                   int64_t total, const uint32_t* __restrict__ stop,
+                                   uint32_t rounds, const int32_t* __restrict__ node_seg,
+                                   const int64_t* __restrict__ leaf_off, int index_bits,
+                                   void* node_level, int32_t* __restrict__ level32,
+                                   uint64_t* __restrict__ level_keys,
+                                   uint32_t* __restrict__ seg_hist,
+                                   int32_t* __restrict__ seg_max, uint32_t* __restrict__ seg_flags,
+                                   uint32_t* __restrict__ tree_flags) {
+  const uint32_t r = *stop < rounds ? *stop : rounds;
+  const int32_t* sc = (r & 1) ? sc1 : sc0;
+  const int32_t* d = (r & 1) ? d1 : d0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t sg = node_seg[k];
+    const int64_t NO = 2 * leaf_off[sg] - sg;
+    const int32_t lv = d[k];
+    store_idx(node_level, index_bits, k, lv);
+    level32[k] = lv;
+    const uint32_t klv = lv < 0 ? 0u : (lv > 0xFFFF ? 0xFFFFu : (uint32_t)lv);
+    level_keys[k] = ((uint64_t)(uint32_t)sg << 16) | klv;
+    if (lv >= 0 && lv < 64) atomicAdd(&seg_hist[(int64_t)sg * 64 + lv], 1u);
+    atomicMax(&seg_max[sg], lv);
+    if (sc[k] != (int32_t)NO) {
+      atomicOr(&seg_flags[sg], kFlagMalformed);
+      atomicOr(tree_flags, kFlagMalformed);
+    }
+  }
+}
+
+__global__ void k_seg_level_tables(const uint32_t* __restrict__ seg_hist,
+                                   const int32_t* __restrict__ seg_max,
+                                   const int64_t* __restrict__ leaf_off, int64_t S,
+                                   int index_bits, void* level_offsets, void* num_levels) {
+  for (int64_t sg = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; sg < S;
+       sg += (int64_t)gridDim.x * blockDim.x) {
+    // a one-leaf tree has the reference's literal table (_tree_impl.py:1052-1110)
+    const bool single = leaf_off[sg + 1] - leaf_off[sg] == 1;
+    int64_t acc = 0;
+    store_idx(level_offsets, index_bits, sg * 65, 0);
+    for (int l = 0; l < 64; ++l) {
+      acc += seg_hist[sg * 64 + l];
+      store_idx(level_offsets, index_bits, sg * 65 + l + 1, single ? (l == 0 ? 1 : 0) : acc);
+    }
+    int64_t nl = (int64_t)seg_max[sg] + 1;
+    nl = nl < 1 ? 1 : (nl > 64 ? 64 : nl);
+    store_idx(num_levels, index_bits, sg, nl);
+  }
+}
+
+// nodes_by_level per set: local ids in the index dtype, global ids in nbl32.
+__global__ void k_seg_nbl(const uint32_t* __restrict__ ids, const int32_t* __restrict__ node_seg,
+                          const int64_t* __restrict__ leaf_off, int64_t total, int index_bits,
+                          void* nbl, int32_t* __restrict__ nbl32) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t id = ids[k];
+    const int32_t sg = node_seg[id];
+    store_idx(nbl, index_bits, k, (int64_t)id - (2 * leaf_off[sg] - sg));
+    nbl32[k] = (int32_t)id;
   }
 }
 
@@ -606,6 +770,182 @@ int ygx_build_topology(const uint64_t* leaf_codes, const void* leaf_starts, cons
   if (rc) return rc;
   ygx::k_u32_to_index<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.nbl_u32, total, index_bits,
                                                                      nodes_by_level, nbl32);
+  YGX_CHECK_LAUNCH();
+  if (tree_flags_out &&
+      cudaMemcpyAsync(tree_flags_out, s.tree_flags, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                      stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  return YGX_OK;
+}
+
+
+// ---- batched sets -------------------------------------------------------------
+
+// Leaf offsets of S sets (leaf_off: S + 1 int64, device): ceil(n_s /
+// leaf_size) adaptive leaves per set.  *total_leaves_out (host) = their sum.
+// Synchronizes the stream.
+int ygx_batch_leaf_offsets(const int64_t* offsets, int64_t S, int64_t leaf_size,
+                           int64_t* leaf_off, int64_t* total_leaves_out, void* ws,
+                           size_t ws_bytes, cudaStream_t stream) {
+  if (S < 1 || leaf_size < 1 || !offsets || !leaf_off || !total_leaves_out) return YGX_ERR_ARG;
+  ygx::Arena a{(char*)ws, 0, ws_bytes};
+  int32_t* cnt = a.take<int32_t>(S);
+  int64_t* tmp = a.take<int64_t>(ygx::scan_scratch_elems(S));
+  if (a.used > ws_bytes) return YGX_ERR_ARG;
+  ygx::k_seg_leaf_counts<<<ygx::grid_for(S, 256), 256, 0, stream>>>(offsets, S, leaf_size, cnt);
+  YGX_CHECK_LAUNCH();
+  int rc = ygx::exclusive_scan<int32_t>(cnt, S, leaf_off, tmp, stream);
+  if (rc) return rc;
+  if (cudaMemcpyAsync(total_leaves_out, leaf_off + S, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                      stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  return YGX_OK;
+}
+
+size_t ygx_batch_leaf_offsets_workspace_size(int64_t S) {
+  ygx::Arena a{nullptr, 0, 0};
+  a.take<int32_t>(S > 0 ? S : 1);
+  a.take<int64_t>(ygx::scan_scratch_elems(S > 0 ? S : 1));
+  return a.used + 256;
+}
+
+// Positions / masses in the sets' sorted order (ygx_batch_encode_sort's
+// order and seg_sorted), particle_indices and inverse local to each set.
+int ygx_batch_reorder(const float* positions, const float* masses, const uint32_t* order,
+                      const int32_t* seg_sorted, const int64_t* offsets, int64_t n, int index_bits,
+                      float* positions_sorted, float* masses_sorted, void* particle_indices,
+                      void* inverse, cudaStream_t stream) {
+  if (n < 1 || !positions || !order || !seg_sorted || !offsets || !positions_sorted ||
+      (index_bits != 32 && index_bits != 64))
+    return YGX_ERR_ARG;
+  ygx::k_seg_reorder<<<ygx::grid_for(n, 256), 256, 0, stream>>>(
+      positions, masses, order, seg_sorted, offsets, n, index_bits, positions_sorted,
+      masses_sorted, particle_indices, inverse);
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
+// Leaf partitions of every set (local particle ranges [start, end), leaf
+// codes, depths -1) and leaf_seg (int32, set of each global leaf).
+int ygx_batch_leaves(const uint64_t* codes_sorted, const int64_t* offsets, const int64_t* leaf_off,
+                     int64_t S, int64_t total_leaves, int64_t leaf_size, int index_bits,
+                     void* leaf_starts, void* leaf_ends, uint64_t* leaf_codes, void* leaf_depths,
+                     int32_t* leaf_seg, cudaStream_t stream) {
+  if (S < 1 || total_leaves < S || leaf_size < 1 || (index_bits != 32 && index_bits != 64))
+    return YGX_ERR_ARG;
+  ygx::k_seg_leaves<<<ygx::grid_for(total_leaves, 256), 256, 0, stream>>>(
+      codes_sorted, offsets, leaf_off, S, total_leaves, leaf_size, index_bits, leaf_starts,
+      leaf_ends, leaf_codes, leaf_depths, leaf_seg);
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
+static ygx::TopoScratch carve_seg_topo(ygx::Arena& a, int64_t total, int64_t S,
+                                       uint32_t** seg_hist, int32_t** seg_max,
+                                       int32_t** node_seg_tmp) {
+  ygx::TopoScratch s;
+  s.status = a.take<uint32_t>(64);
+  s.tree_flags = a.take<uint32_t>(64);
+  s.changed = a.take<uint32_t>(128);
+  s.stop = a.take<uint32_t>(64);
+  s.level_hist = a.take<uint32_t>(64);
+  s.max_level = a.take<int32_t>(64);
+  *seg_hist = a.take<uint32_t>((size_t)S * 64);
+  *seg_max = a.take<int32_t>(S);
+  s.parent_claim = a.take<int32_t>(total);
+  for (int b = 0; b < 2; ++b) { s.sc[b] = a.take<int32_t>(total); s.d[b] = a.take<int32_t>(total); }
+  s.level_keys = a.take<uint64_t>(total);
+  s.level_keys_sorted = a.take<uint64_t>(total);
+  s.nbl_u32 = a.take<uint32_t>(total);
+  *node_seg_tmp = nullptr;
+  s.sort = ygx::carve_sort_scratch(a, total, 4);
+  return s;
+}
+
+size_t ygx_batch_topology_workspace_size(int64_t total_leaves, int64_t S) {
+  ygx::Arena a{nullptr, 0, 0};
+  uint32_t* h;
+  int32_t* m;
+  int32_t* t;
+  const int64_t total = total_leaves > S ? 2 * total_leaves - S : 1;
+  carve_seg_topo(a, total, S > 0 ? S : 1, &h, &m, &t);
+  return a.used + 256;
+}
+
+// The forest of S Karras trees (set s: leaves leaf_off[s] .. leaf_off[s+1],
+// nodes at NO_s = 2 leaf_off[s] - s; total = 2 total_leaves - S).  Per-set
+// outputs hold local values as ygx_build_topology gives them for the set
+// alone: parent / node_ranges / node_level / nodes_by_level (total), left /
+// right / flags (total_leaves - S), level_offsets (S x 65), num_levels (S).
+// parent32 / left32 / right32 / nbl32 hold global node ids, node_seg32 the
+// set of every node, leafpos32 the near-row position of every leaf (the
+// sets' leaves back to back; -1 for internal nodes), node_base32 / leaf_base32
+// the first node id of the set of every node / leaf, seg_flags (S)
+// YGX_FLAG_MALFORMED per set and tree_flags_out (1 word) their union.
+int ygx_batch_build_topology(const uint64_t* leaf_codes, const void* leaf_starts,
+                             const void* leaf_ends, const int64_t* leaf_off,
+                             const int32_t* leaf_seg, int64_t S, int64_t total_leaves,
+                             int index_bits, void* parent, void* left, void* right,
+                             uint8_t* left_is_leaf, uint8_t* right_is_leaf, void* node_ranges,
+                             void* node_level, void* level_offsets, void* nodes_by_level,
+                             void* num_levels, int32_t* parent32, int32_t* left32,
+                             int32_t* right32, int32_t* level32, int32_t* nbl32,
+                             int32_t* node_seg32, int32_t* leafpos32, int32_t* node_base32,
+                             int32_t* leaf_base32, uint32_t* seg_flags, uint32_t* tree_flags_out,
+                             void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (S < 1 || S > (1 << 16) || total_leaves < S || (index_bits != 32 && index_bits != 64))
+    return YGX_ERR_ARG;
+  const int64_t total = 2 * total_leaves - S;
+  if (total >= (int64_t)INT32_MAX / 2) return YGX_ERR_ARG;
+  if (ws_bytes < ygx_batch_topology_workspace_size(total_leaves, S)) return YGX_ERR_ARG;
+  ygx::Arena a{(char*)ws, 0, ws_bytes};
+  uint32_t* seg_hist;
+  int32_t* seg_max;
+  int32_t* unused;
+  ygx::TopoScratch s = carve_seg_topo(a, total, S, &seg_hist, &seg_max, &unused);
+  // flags, changed, stop, hist, max_level, seg_hist, seg_max are contiguous
+  if (cudaMemsetAsync(s.tree_flags, 0, (char*)(seg_max + S) - (char*)s.tree_flags, stream) !=
+          cudaSuccess ||
+      cudaMemsetAsync(s.stop, 0xFF, 64 * sizeof(uint32_t), stream) != cudaSuccess ||
+      cudaMemsetAsync(s.parent_claim, 0xFF, total * sizeof(int32_t), stream) != cudaSuccess ||
+      cudaMemsetAsync(seg_flags, 0, S * sizeof(uint32_t), stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  ygx::k_seg_karras<<<ygx::grid_for(total_leaves, 256), 256, 0, stream>>>(
+      leaf_codes, leaf_starts, leaf_ends, leaf_off, leaf_seg, total_leaves, index_bits, left,
+      right, left_is_leaf, right_is_leaf, node_ranges, left32, right32, s.parent_claim,
+      node_seg32, leafpos32, node_base32, leaf_base32);
+  YGX_CHECK_LAUNCH();
+  ygx::k_seg_parent_decode<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      s.parent_claim, node_seg32, leaf_off, total, index_bits, parent, parent32);
+  YGX_CHECK_LAUNCH();
+  ygx::k_seg_check_wellformed<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      parent32, left32, right32, node_seg32, leaf_off, total, seg_flags, s.tree_flags);
+  YGX_CHECK_LAUNCH();
+  int bl = 0;
+  while (((int64_t)1 << bl) <= total) ++bl;
+  const int rounds = bl + 1;
+  ygx::k_depth_init<<<ygx::grid_for(total, 256), 256, 0, stream>>>(parent32, total, s.sc[0], s.d[0]);
+  YGX_CHECK_LAUNCH();
+  for (int r = 0; r < rounds; ++r) {
+    ygx::k_depth_round<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+        s.sc[r & 1], s.d[r & 1], s.sc[(r + 1) & 1], s.d[(r + 1) & 1], total, r, s.changed, s.stop);
+    YGX_CHECK_LAUNCH();
+  }
+  ygx::k_seg_depth_finish<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      s.sc[0], s.d[0], s.sc[1], s.d[1], total, s.stop, (uint32_t)rounds, node_seg32, leaf_off,
+      index_bits, node_level, level32, s.level_keys, seg_hist, seg_max, seg_flags, s.tree_flags);
+  YGX_CHECK_LAUNCH();
+  ygx::k_seg_level_tables<<<ygx::grid_for(S, 128), 128, 0, stream>>>(
+      seg_hist, seg_max, leaf_off, S, index_bits, level_offsets, num_levels);
+  YGX_CHECK_LAUNCH();
+  // nodes_by_level: stable sort by (set, level); sets < 2^16, levels < 2^16
+  int rc = ygx::onesweep_sort(s.level_keys, nullptr, total, 0, 32, s.level_keys_sorted, s.nbl_u32,
+                              s.sort, false, s.status, stream);
+  if (rc) return rc;
+  ygx::k_seg_nbl<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.nbl_u32, node_seg32, leaf_off,
+                                                                total, index_bits,
+                                                                nodes_by_level, nbl32);
   YGX_CHECK_LAUNCH();
   if (tree_flags_out &&
       cudaMemcpyAsync(tree_flags_out, s.tree_flags, sizeof(uint32_t), cudaMemcpyDeviceToDevice,

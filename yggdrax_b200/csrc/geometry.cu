@@ -225,6 +225,134 @@ __global__ void __launch_bounds__(1024)
   }
 }
 
+// ---- batched sets (a forest: set s at nodes NO_s = 2 leaf_off[s] - s) ------
+
+// k_leaf_ranges_refit over the leaves of all sets: a warp reduces 32 leaves
+// (global leaf positions) one after the other, then every lane climbs its
+// set's tree.  Particle ranges are local to the set (offset off[s]).
+__global__ void k_seg_leaf_refit(const void* ranges, const int64_t* __restrict__ leaf_off,
+                                 const int32_t* __restrict__ leaf_seg,
+                                 const int64_t* __restrict__ off, int64_t Ltot, int index_bits,
+                                 const float* __restrict__ pos, int64_t cap, bool empty_inf,
+                                 const int32_t* __restrict__ parent32,
+                                 const int32_t* __restrict__ left32,
+                                 const int32_t* __restrict__ right32, float* __restrict__ mn,
+                                 float* __restrict__ mx, int32_t* __restrict__ arrive,
+                                 const uint32_t* __restrict__ seg_flags, float* center,
+                                 float* half, float* radius, float* max_extent) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const float big = empty_inf ? __int_as_float(0x7f800000) : 3.402823466e38f;
+  const float qnan = __int_as_float(0x7fc00000);
+  for (int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32;
+       base < Ltot; base += warps * 32) {
+    float my_lo[3] = {0.f, 0.f, 0.f}, my_hi[3] = {0.f, 0.f, 0.f};
+    int64_t my_node = -1;
+    int32_t my_seg = 0;
+    const int nl = Ltot - base < 32 ? (int)(Ltot - base) : 32;
+    for (int jj = 0; jj < nl; ++jj) {
+      const int64_t g = base + jj;
+      const int32_t sg = leaf_seg[g];
+      const int64_t a = leaf_off[sg], Ls = leaf_off[sg + 1] - a;
+      const int64_t node = 2 * a - sg + Ls - 1 + (g - a);
+      const int64_t s0 = load_idx(ranges, index_bits, 2 * node);
+      int64_t c = load_idx(ranges, index_bits, 2 * node + 1) - s0 + 1;
+      if (cap >= 0 && c > cap) c = cap;
+      const int64_t pb = off[sg] + s0;
+      float lo[3] = {big, big, big}, hi[3] = {-big, -big, -big};
+      unsigned nan = 0;
+      for (int64_t k = lane; k < c; k += 32) {
+        const float* p = pos + 3 * (pb + k);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          float v = __ldg(p + q);
+          if (v != v) nan |= 1u << q;
+          lo[q] = fminf(lo[q], v);
+          hi[q] = fmaxf(hi[q], v);
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          lo[q] = fminf(lo[q], __shfl_xor_sync(0xffffffffu, lo[q], o));
+          hi[q] = fmaxf(hi[q], __shfl_xor_sync(0xffffffffu, hi[q], o));
+        }
+        nan |= __shfl_xor_sync(0xffffffffu, nan, o);
+      }
+      if (lane == jj) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          my_lo[q] = (nan >> q) & 1 ? qnan : lo[q];
+          my_hi[q] = (nan >> q) & 1 ? qnan : hi[q];
+        }
+        my_node = node;
+        my_seg = sg;
+      }
+    }
+    if (lane < nl) {
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        __stcg(mn + 3 * my_node + q, my_lo[q]);
+        __stcg(mx + 3 * my_node + q, my_hi[q]);
+      }
+      finalize_node(my_node, my_lo, my_hi, center, half, radius, max_extent);
+      if (!(seg_flags[my_seg] & kFlagMalformed))
+        climb(my_node, parent32, left32, right32, mn, mx, arrive, center, half, radius,
+              max_extent);
+    }
+  }
+}
+
+// k_serial_refit per malformed set: one CTA per set (others return).
+__global__ void __launch_bounds__(1024)
+    k_seg_serial_refit(const int64_t* __restrict__ leaf_off, int64_t S,
+                       const int32_t* __restrict__ level32, const int32_t* __restrict__ left32,
+                       const int32_t* __restrict__ right32, float* __restrict__ mn,
+                       float* __restrict__ mx, float* __restrict__ tmp,
+                       const uint32_t* __restrict__ seg_flags, float* center, float* half,
+                       float* radius, float* max_extent) {
+  __shared__ int s_max;
+  for (int64_t sg = blockIdx.x; sg < S; sg += gridDim.x) {
+    if (!(seg_flags[sg] & kFlagMalformed)) continue;
+    const int64_t a = leaf_off[sg], Ls = leaf_off[sg + 1] - a, NO = 2 * a - sg;
+    const int64_t ni = Ls - 1, total = 2 * Ls - 1;
+    if (threadIdx.x == 0) s_max = 0;
+    __syncthreads();
+    int mxl = 0;
+    for (int64_t k = threadIdx.x; k < total; k += blockDim.x) mxl = max(mxl, level32[NO + k]);
+    atomicMax(&s_max, mxl);
+    for (int64_t k = threadIdx.x; k < ni; k += blockDim.x)
+      for (int q = 0; q < 3; ++q) { mn[3 * (NO + k) + q] = 0.0f; mx[3 * (NO + k) + q] = 0.0f; }
+    __syncthreads();
+    const int maxd = s_max;
+    for (int level = maxd - 1; level >= 0; --level) {
+      for (int64_t i = NO + threadIdx.x; i < NO + ni; i += blockDim.x) {
+        if (level32[i] != level) continue;
+        const int64_t l = left32[i], r = right32[i];
+        for (int q = 0; q < 3; ++q) {
+          tmp[6 * i + q] = fmin_nan(mn[3 * l + q], mn[3 * r + q]);
+          tmp[6 * i + 3 + q] = fmax_nan(mx[3 * l + q], mx[3 * r + q]);
+        }
+      }
+      __syncthreads();
+      for (int64_t i = NO + threadIdx.x; i < NO + ni; i += blockDim.x) {
+        if (level32[i] != level) continue;
+        for (int q = 0; q < 3; ++q) {
+          mn[3 * i + q] = tmp[6 * i + q];
+          mx[3 * i + q] = tmp[6 * i + 3 + q];
+        }
+      }
+      __syncthreads();
+    }
+    for (int64_t k = NO + threadIdx.x; k < NO + ni; k += blockDim.x) {
+      float lo[3], hi[3];
+      for (int q = 0; q < 3; ++q) { lo[q] = mn[3 * k + q]; hi[q] = mx[3 * k + q]; }
+      finalize_node(k, lo, hi, center, half, radius, max_extent);
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace
 
 struct GeoScratch {
@@ -292,6 +420,39 @@ int ygx_tree_geometry(const void* node_ranges, int64_t total, int index_bits,
                                                 max_extent);
     YGX_CHECK_LAUNCH();
   }
+  return YGX_OK;
+}
+
+// Geometry of every tree of a batched forest (ygx_batch_build_topology):
+// leaf boxes from the sets' particle ranges in positions_sorted (set s at
+// offsets[s]), at most max_leaf_size particles per leaf; total = 2
+// total_leaves - S nodes.
+int ygx_batch_tree_geometry(const void* node_ranges, int64_t total, int64_t S,
+                            const int64_t* leaf_off, const int32_t* leaf_seg,
+                            int64_t total_leaves, const int64_t* offsets, int index_bits,
+                            const int32_t* parent32, const int32_t* left32,
+                            const int32_t* right32, const int32_t* level32,
+                            const uint32_t* seg_flags, const float* positions_sorted,
+                            int64_t max_leaf_size, float* center, float* half_extent,
+                            float* radius, float* max_extent, void* ws, size_t ws_bytes,
+                            cudaStream_t stream) {
+  if (total < 1 || S < 1 || total != 2 * total_leaves - S || (index_bits != 32 && index_bits != 64))
+    return YGX_ERR_ARG;
+  if (ws_bytes < ygx_geometry_workspace_size(total)) return YGX_ERR_ARG;
+  ygx::Arena a{(char*)ws, 0, ws_bytes};
+  ygx::GeoScratch s = ygx::carve_geo(a, total);
+  if (cudaMemsetAsync(s.arrive, 0, sizeof(int32_t) * total, stream) != cudaSuccess) return YGX_ERR_CUDA;
+  const int warps = 8;
+  ygx::k_seg_leaf_refit<<<ygx::grid_for((total_leaves + 31) / 32, warps, ygx::kNumSMs * 16),
+                          warps * 32, 0, stream>>>(
+      node_ranges, leaf_off, leaf_seg, offsets, total_leaves, index_bits, positions_sorted,
+      max_leaf_size, max_leaf_size == 0, parent32, left32, right32, s.mn, s.mx, s.arrive,
+      seg_flags, center, half_extent, radius, max_extent);
+  YGX_CHECK_LAUNCH();
+  ygx::k_seg_serial_refit<<<(unsigned)(S < 1024 ? S : 1024), 1024, 0, stream>>>(
+      leaf_off, S, level32, left32, right32, s.mn, s.mx, s.tmp, seg_flags, center, half_extent,
+      radius, max_extent);
+  YGX_CHECK_LAUNCH();
   return YGX_OK;
 }
 

@@ -10,6 +10,7 @@
 // largely from L2 for inputs up to ~100 MB), writes the codes, and builds the
 // per-pass digit histograms of the following radix sort so the sort never
 // re-reads the keys for them.
+#include "morton.cuh"
 #include "sort.cuh"
 
 namespace ygx {
@@ -126,20 +127,6 @@ __global__ void __launch_bounds__(kBBoxThreads)
   }
 }
 
-// morton.py:64-77 in fp32 with IEEE division and round-half-even.
-__device__ __forceinline__ uint64_t encode_one(float x, float y, float z, const float* mn,
-                                               const float* span) {
-  float v[3] = {x, y, z};
-  uint64_t q[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    float norm = __fdiv_rn(__fsub_rn(v[a], mn[a]), span[a]);
-    norm = fminf(fmaxf(norm, 0.0f), 1.0f);  // NaN -> 0 (no integer image)
-    q[a] = __float2ull_rn(__fmul_rn(norm, 2097151.0f));
-  }
-  return spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
-}
-
 constexpr int kEncodeThreads = 256;
 
 __global__ void __launch_bounds__(kEncodeThreads)
@@ -203,6 +190,93 @@ __global__ void __launch_bounds__(kEncodeThreads)
     if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
 }
 
+// ---- batched sets (segments [off[s], off[s+1]) of one position array) ---------
+
+// Bounds of every set: one CTA per set, the same reduction and padding as
+// k_bbox (bounds.py:29-33), and the set id of every point.
+__global__ void __launch_bounds__(kBBoxThreads)
+    k_seg_bbox(const float* __restrict__ pos, const int64_t* __restrict__ off, int64_t S,
+               float* __restrict__ bounds_out, int32_t* __restrict__ seg_of) {
+  __shared__ Box s_box[kBBoxThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t sg = blockIdx.x; sg < S; sg += gridDim.x) {
+    const int64_t b = off[sg], e = off[sg + 1];
+    Box bx;
+    bx.init();
+    for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+      for (int a = 0; a < 3; ++a) bx.add(a, pos[3 * i + a]);
+      seg_of[i] = (int32_t)sg;
+    }
+    bx.warp_reduce();
+    if (lane == 0) s_box[warp] = bx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      Box r = s_box[0];
+      for (int w = 1; w < kBBoxThreads / 32; ++w) r.merge(s_box[w]);
+      const float qnan = __int_as_float(0x7fc00000);
+      for (int a = 0; a < 3; ++a) {
+        float lo = (r.nan >> a) & 1 ? qnan : r.mn[a];
+        float hi = (r.nan >> a) & 1 ? qnan : r.mx[a];
+        float span = __fsub_rn(hi, lo);
+        float pad = fmax_nan(__fmul_rn(span, 0.05f), 1e-6f);
+        bounds_out[6 * sg + a] = __fsub_rn(lo, pad);
+        bounds_out[6 * sg + 3 + a] = __fadd_rn(hi, pad);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Codes of every point with its set's bounds, plus the digit histograms of
+// the 8 code passes of the sort.
+__global__ void __launch_bounds__(kEncodeThreads)
+    k_seg_encode(const float* __restrict__ pos, int64_t n, const int32_t* __restrict__ seg_of,
+                 const float* __restrict__ bounds, uint64_t* __restrict__ codes,
+                 uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s_hist[8 * kSortRadix];
+  for (int i = threadIdx.x; i < 8 * kSortRadix; i += blockDim.x) s_hist[i] = 0;
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float* bd = bounds + 6 * seg_of[i];
+    float mn[3], span[3];
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = bd[a];
+      span[a] = __fsub_rn(bd[3 + a], bd[a]);
+    }
+    const uint64_t c = encode_one(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], mn, span);
+    codes[i] = c;
+    for (int p = 0; p < 8; ++p)
+      atomicAdd(&s_hist[p * kSortRadix + ((uint32_t)(c >> (p * kSortRadixBits)) & (kSortRadix - 1))],
+                1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 8 * kSortRadix; i += blockDim.x)
+    if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
+}
+
+__global__ void k_u64_to_i32(const uint64_t* __restrict__ in, int64_t n, int32_t* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (int32_t)in[i];
+}
+
+// Sort keys of the second (stable, by set) sort: the set of each point in
+// the code order.
+__global__ void k_seg_keys(const uint32_t* __restrict__ perm, const int32_t* __restrict__ seg_of,
+                           int64_t n, uint64_t* __restrict__ keys) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    keys[i] = (uint64_t)(uint32_t)seg_of[perm[i]];
+}
+
+__global__ void k_gather_codes(const uint64_t* __restrict__ codes, const uint32_t* __restrict__ perm,
+                               int64_t n, uint64_t* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = codes[perm[i]];
+}
+
 }  // namespace
 
 struct EncodeSortLayout {
@@ -221,9 +295,84 @@ static EncodeSortLayout carve_encode_sort(Arena& a, int64_t n) {
   return l;
 }
 
+struct BatchEncodeLayout {
+  uint32_t* status;
+  int32_t* seg_of;
+  uint64_t* codes;
+  uint32_t* perm_code;
+  uint64_t* seg_keys;
+  uint64_t* seg_sorted;
+  SortScratch sort;
+};
+
+static BatchEncodeLayout carve_batch_encode(Arena& a, int64_t n) {
+  BatchEncodeLayout l;
+  const int64_t m = n > 0 ? n : 1;
+  l.status = a.take<uint32_t>(64);
+  l.seg_of = a.take<int32_t>(m);
+  l.codes = a.take<uint64_t>(m);
+  l.perm_code = a.take<uint32_t>(m);
+  l.seg_keys = a.take<uint64_t>(m);
+  l.seg_sorted = a.take<uint64_t>(m);
+  l.sort = carve_sort_scratch(a, n);
+  return l;
+}
+
 }  // namespace ygx
 
 extern "C" {
+
+size_t ygx_batch_encode_sort_workspace_size(int64_t n) {
+  ygx::Arena a{nullptr, 0, 0};
+  ygx::carve_batch_encode(a, n);
+  return a.used + 256;
+}
+
+// Batched bounds + Morton codes + stable order of S point sets stored back to
+// back (set s = positions[offsets[s] .. offsets[s+1]), offsets on the
+// device): per set what infer_bounds / morton_encode_impl / the stable
+// argsort of _tree_impl.py:401 give for that set alone.  bounds_out (S x 6:
+// min xyz, max xyz), codes_sorted (n) in (set, code, original index) order,
+// order_out (n) the global input index of each sorted point, seg_sorted_out
+// (n, int32, may be null) its set.
+int ygx_batch_encode_sort(const float* positions, int64_t n, const int64_t* offsets, int64_t S,
+                          float* bounds_out, uint64_t* codes_sorted, uint32_t* order_out,
+                          int32_t* seg_sorted_out, void* ws, size_t ws_bytes,
+                          cudaStream_t stream) {
+  if (n < 1 || S < 1 || S > (int64_t)1 << 16 || n >= (int64_t)UINT32_MAX || !positions ||
+      !offsets || !bounds_out || !codes_sorted || !order_out || !ws)
+    return YGX_ERR_ARG;
+  if (ws_bytes < ygx_batch_encode_sort_workspace_size(n)) return YGX_ERR_ARG;
+  ygx::Arena a{(char*)ws, 0, ws_bytes};
+  ygx::BatchEncodeLayout l = ygx::carve_batch_encode(a, n);
+  if (cudaMemsetAsync(l.status, 0, 64 * sizeof(uint32_t), stream) != cudaSuccess ||
+      ygx::sort_scratch_reset(l.sort, n, 8, stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  ygx::k_seg_bbox<<<(unsigned)(S < 65535 ? S : 65535), ygx::kBBoxThreads, 0, stream>>>(
+      positions, offsets, S, bounds_out, l.seg_of);
+  YGX_CHECK_LAUNCH();
+  ygx::k_seg_encode<<<ygx::grid_for(n, ygx::kEncodeThreads), ygx::kEncodeThreads, 0, stream>>>(
+      positions, n, l.seg_of, bounds_out, l.codes, l.sort.hist);
+  YGX_CHECK_LAUNCH();
+  // stable by code (63 bits), then stable by set (16 bits): (set, code, index)
+  int rc = ygx::onesweep_sort(l.codes, nullptr, n, 0, 63, codes_sorted, l.perm_code, l.sort, true,
+                              l.status, stream);
+  if (rc) return rc;
+  ygx::k_seg_keys<<<ygx::grid_for(n, 256), 256, 0, stream>>>(l.perm_code, l.seg_of, n,
+                                                             l.seg_keys);
+  YGX_CHECK_LAUNCH();
+  rc = ygx::onesweep_sort(l.seg_keys, l.perm_code, n, 0, 16, l.seg_sorted, order_out, l.sort,
+                          false, l.status, stream);
+  if (rc) return rc;
+  ygx::k_gather_codes<<<ygx::grid_for(n, 256), 256, 0, stream>>>(l.codes, order_out, n,
+                                                                 codes_sorted);
+  YGX_CHECK_LAUNCH();
+  if (seg_sorted_out) {
+    ygx::k_u64_to_i32<<<ygx::grid_for(n, 256), 256, 0, stream>>>(l.seg_sorted, n, seg_sorted_out);
+    YGX_CHECK_LAUNCH();
+  }
+  return YGX_OK;
+}
 
 size_t ygx_encode_sort_workspace_size(int64_t n) {
   ygx::Arena a{nullptr, 0, 0};

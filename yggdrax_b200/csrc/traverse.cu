@@ -254,7 +254,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
       }
       const bool diff = t != sv;
       acc = diff && d2 > 0.0f && ok;
-      nearp = !acc && diff && t >= ni && sv >= ni;
+      // leaves carry -1 children (node records), in a single tree and a forest
+      nearp = !acc && diff && A.k.x < 0 && B.k.x < 0;
       refine = !acc && !nearp;
     }
     n_acc += acc;
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSM)
     int2 c0 = make_int2(0, 0), c1 = c0, c2 = c0, c3 = c0;
     if (refine) {
       const bool same = t == sv;
-      const bool t_int = t < ni, s_int = sv < ni;
+      const bool t_int = A.k.x >= 0, s_int = B.k.x >= 0;
       const float et = A.c.w, es = B.c.w;
       const bool split_t = t_int && (same || !s_int || et >= es);
       const bool split_s = s_int && (same || !t_int || es > et);
@@ -624,6 +625,33 @@ __global__ void k_seed(int2* wf, uint32_t* cnt, uint32_t* sizes, int root) {
   }
 }
 
+// Generation 0 of a forest walk: (root_s, root_s) for every set, spread
+// over the regions round-robin.  root_s = 2 leaf_off[s] - s, or for a set
+// flagged malformed its first node without a parent (the reference starts
+// its walk at argmin(parent)).
+__global__ void k_seed_forest(int2* wf, uint32_t* cnt, uint32_t* sizes, uint32_t R,
+                              const int64_t* __restrict__ leaf_off, int64_t S,
+                              const int32_t* __restrict__ parent32,
+                              const uint32_t* __restrict__ seg_flags,
+                              uint32_t* __restrict__ status) {
+  for (int r = threadIdx.x; r < kWalkGrid; r += blockDim.x) {
+    const int64_t c = S > r ? (S - r + kWalkGrid - 1) / kWalkGrid : 0;
+    cnt[r] = c <= R ? (uint32_t)c : R;
+    if (c > R) raise_flag(status, kFlagQueueOverflow);
+  }
+  for (int64_t sg = threadIdx.x; sg < S; sg += blockDim.x) {
+    const int64_t a = leaf_off[sg], Ls = leaf_off[sg + 1] - a, NO = 2 * a - sg;
+    int64_t root = NO;
+    if (seg_flags && (seg_flags[sg] & kFlagMalformed)) {
+      for (int64_t k = NO; k < NO + 2 * Ls - 1; ++k)
+        if (parent32[k] < 0) { root = k; break; }
+    }
+    const int64_t r = sg % kWalkGrid, k = sg / kWalkGrid;
+    if (k < R) wf[(size_t)r * R + k] = make_int2((int)root, (int)root);
+  }
+  if (threadIdx.x == 0) sizes[0] = (uint32_t)S;
+}
+
 // Totals and maxima of the count pass; max wavefront and generations.
 __global__ void k_count_stats(const int32_t* __restrict__ far_cnt, int64_t total,
                               const int32_t* __restrict__ near_cnt, int64_t L,
@@ -759,9 +787,10 @@ __device__ __forceinline__ void mirrored_bitonic(int32_t* a, int64_t n64, int ti
 // and, for far rows, the target node and its level for every entry.
 __device__ __forceinline__ void emit_row(const int32_t* a, int64_t n, int64_t off, int index_bits,
                                          void* vals_out, void* tgt_out, void* lvl_out, int32_t tgt,
+                                         int32_t vbase,
                                          int32_t lvl, int tid, int nthreads) {
   for (int64_t k = tid; k < n; k += nthreads) {
-    store_idx(vals_out, index_bits, off + k, a[k]);
+    store_idx(vals_out, index_bits, off + k, a[k] - vbase);
     if (tgt_out) {
       store_idx(tgt_out, index_bits, off + k, tgt);
       store_idx(lvl_out, index_bits, off + k, lvl);
@@ -781,7 +810,8 @@ __device__ __forceinline__ void warp_sort_row(const int32_t* __restrict__ raw, i
                                               int64_t off,
                                               int n, int index_bits, void* vals_out,
                                               void* tgt_out, void* lvl_out, int32_t tgt,
-                                              int32_t lvl, int lane, int32_t* __restrict__ sm) {
+                                              int32_t vbase, int32_t lvl, int lane,
+                                              int32_t* __restrict__ sm) {
   constexpr int S = R + 1;
   constexpr int LOGR = R == 1 ? 0 : R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : R == 16 ? 4 : 5;
 #pragma unroll
@@ -831,7 +861,7 @@ __device__ __forceinline__ void warp_sort_row(const int32_t* __restrict__ raw, i
     const int e = r * 32 + lane;
     if (e < n) {
       const int32_t x = sm[(e >> LOGR) * S + (e & (R - 1))];
-      store_idx(vals_out, index_bits, off + e, x);
+      store_idx(vals_out, index_bits, off + e, x - vbase);
       if (tgt_out) {
         store_idx(tgt_out, index_bits, off + e, tgt);
         store_idx(lvl_out, index_bits, off + e, lvl);
@@ -883,15 +913,16 @@ __global__ void __launch_bounds__(256, R >= 32 ? 2 : (R >= 16 ? 3 : 4))
     k_rows_class(const int32_t* __restrict__ list, const uint32_t* __restrict__ list_n,
                  const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
                  const int32_t* __restrict__ row_level, const int32_t* __restrict__ raw,
-                 const int64_t* __restrict__ raw_off, int index_bits, void* vals_out,
-                 void* tgt_out, void* lvl_out) {
+                 const int64_t* __restrict__ raw_off, const int32_t* __restrict__ row_base,
+                 int index_bits, void* vals_out, void* tgt_out, void* lvl_out) {
   __shared__ int32_t s_rows[8][32 * (R + 1)];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t nm = *list_n;
   for (uint32_t b = blockIdx.x * 8 + w; b < nm; b += gridDim.x * 8) {
     const int32_t r = list[b];
+    const int32_t vbase = row_base ? row_base[r] : 0;
     warp_sort_row<R>(raw, raw_off ? raw_off[r] : row_off[r], row_off[r], row_cnt[r],
-                     index_bits, vals_out, tgt_out, lvl_out, r,
+                     index_bits, vals_out, tgt_out, lvl_out, r - vbase, vbase,
                      row_level ? row_level[r] : 0, lane, s_rows[w]);
   }
 }
@@ -952,9 +983,9 @@ __global__ void __launch_bounds__(kBigThreads, 3)
     k_rows_big(const int32_t* __restrict__ big_rows, uint32_t* __restrict__ n_big,
                int64_t list_cap, const int64_t* __restrict__ row_off,
                const int32_t* __restrict__ row_cnt, const int32_t* __restrict__ row_level,
-               int32_t* __restrict__ raw, const int64_t* __restrict__ raw_off, int index_bits,
-               void* vals_out, void* tgt_out, void* lvl_out, uint32_t* __restrict__ bitmaps,
-               int64_t universe) {
+               int32_t* __restrict__ raw, const int64_t* __restrict__ raw_off,
+               const int32_t* __restrict__ row_base, int index_bits, void* vals_out,
+               void* tgt_out, void* lvl_out, uint32_t* __restrict__ bitmaps, int64_t universe) {
   extern __shared__ uint32_t s_dyn[];  // kBlockRowCap words: bitmap, or a row to sort
   __shared__ uint32_t s_sum[kSumWords];
   __shared__ int32_t s_cc[kSumWords];  // per-chunk counts, then bases (< n < 2^31)
@@ -983,6 +1014,7 @@ __global__ void __launch_bounds__(kBigThreads, 3)
     const int32_t r = b < n_long ? big_rows[b] : big_rows[list_cap - 1 - (b - n_long)];
     const int64_t off = row_off[r];
     const int64_t roff = raw_off ? raw_off[r] : off;  // where the raw row is read
+    const int32_t vbase = row_base ? row_base[r] : 0;   // ids written relative to it
     const int64_t n = row_cnt[r];
     const int32_t lvl = row_level ? row_level[r] : 0;
     int32_t vmin = INT32_MAX, vmax = INT32_MIN;
@@ -1107,9 +1139,9 @@ __global__ void __launch_bounds__(kBigThreads, 3)
             const int32_t wsi = __shfl_sync(0xffffffffu, wi, lo);
             if (q < T) {
               const int32_t v = vmin + wsi * 32 + select_bit(wsel, q - ex);
-              store_idx(vals_out, index_bits, pos + q, v);
+              store_idx(vals_out, index_bits, pos + q, v - vbase);
               if (tgt_out) {
-                store_idx(tgt_out, index_bits, pos + q, r);
+                store_idx(tgt_out, index_bits, pos + q, r - vbase);
                 store_idx(lvl_out, index_bits, pos + q, lvl);
               }
             }
@@ -1128,13 +1160,13 @@ __global__ void __launch_bounds__(kBigThreads, 3)
         for (int64_t k = tid; k < n; k += nt) a[k] = raw[roff + k];
         __syncthreads();
         mirrored_bitonic<true>(a, n, tid, nt);
-        emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, r, lvl, tid, nt);
+        emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, r - vbase, vbase, lvl, tid, nt);
         __syncthreads();
         for (int64_t k = tid; k < n; k += nt) s_dyn[k] = 0u;  // bitmap stays zero
       } else {
         int32_t* a = raw + roff;
         mirrored_bitonic<true>(a, n, tid, nt);
-        emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, r, lvl, tid, nt);
+        emit_row(a, n, off, index_bits, vals_out, tgt_out, lvl_out, r - vbase, vbase, lvl, tid, nt);
       }
     }
     __syncthreads();
@@ -1288,10 +1320,25 @@ static int launch_gen(int mode, int mac, const TravScratch& s, int32_t ni, int32
 // wavefront size is probed every 16 generations until it is empty (or a
 // wavefront overflow is flagged); otherwise exactly fixed_gens generations
 // run (a repeat of a walk whose length is known).  *gens_out = launched.
+// The roots: one (root) or a forest (leaf_off != nullptr).
+struct Roots {
+  int root;
+  const int64_t* leaf_off;
+  int64_t S;
+  const int32_t* parent32;
+  const uint32_t* seg_flags;
+};
+
 static int run_gens(int mode, int mac, const TravScratch& s, int32_t ni, int32_t total,
-                    float theta_sq, float theta_r, int root, uint32_t cap, const RowSink& sink,
-                    int fixed_gens, int gens_hint, int* gens_out, cudaStream_t stream) {
-  k_seed<<<1, 256, 0, stream>>>(s.wf[0], s.region_cnt[0], s.sizes, root);
+                    float theta_sq, float theta_r, const Roots& roots, uint32_t cap,
+                    const RowSink& sink, int fixed_gens, int gens_hint, int* gens_out,
+                    cudaStream_t stream) {
+  if (roots.leaf_off)
+    k_seed_forest<<<1, 256, 0, stream>>>(s.wf[0], s.region_cnt[0], s.sizes,
+                                         (uint32_t)region_capacity(cap), roots.leaf_off,
+                                         roots.S, roots.parent32, roots.seg_flags, s.status);
+  else
+    k_seed<<<1, 256, 0, stream>>>(s.wf[0], s.region_cnt[0], s.sizes, roots.root);
   YGX_CHECK_LAUNCH();
   int gen = 0, rc = YGX_OK;
   if (fixed_gens >= 0) {
@@ -1392,16 +1439,12 @@ static int trav_setup(ygx::TravScratch& s, void* ws, size_t ws_bytes, int64_t to
 // wavefront / log capacities that would have fit) and the status flags.
 // leafpos32[node] is the near-row position of a leaf (-1 for internal
 // nodes).  Synchronizes the stream.
-int ygx_traverse_walk(const float* center, const float* radius, const float* max_extent,
-                      const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
-                      int64_t total, int64_t num_internal, int mac, float theta,
-                      float dehnen_radius_scale, int root, int mode, int gens_hint,
-                      int64_t wf_capacity, int64_t log_capacity, uint64_t* stats_out,
-                      uint32_t* flags_out, void* ws, size_t ws_bytes, cudaStream_t stream) {
-  if (total < 3 || total > INT32_MAX || num_internal < 1 || mac < 0 || mac > 2 ||
-      root < 0 || root >= total || !stats_out || !flags_out ||
-      (mode != YGX_WALK_LOG && mode != YGX_WALK_COUNT))
-    return YGX_ERR_ARG;
+static int walk_impl(const float* center, const float* radius, const float* max_extent,
+                     const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
+                     int64_t total, int64_t num_internal, int mac, float theta,
+                     float dehnen_radius_scale, const ygx::Roots& roots, int mode, int gens_hint,
+                     int64_t wf_capacity, int64_t log_capacity, uint64_t* stats_out,
+                     uint32_t* flags_out, void* ws, size_t ws_bytes, cudaStream_t stream) {
   const int64_t L = total - num_internal;
   ygx::TravScratch s;
   int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity, log_capacity);
@@ -1423,7 +1466,7 @@ int ygx_traverse_walk(const float* center, const float* radius, const float* max
   YGX_CHECK_LAUNCH();
   int gen = 0;
   rc = ygx::run_gens(mode == YGX_WALK_LOG ? ygx::kWalkLog : ygx::kWalkCount, mac, s,
-                     (int32_t)num_internal, (int32_t)total, theta_sq, theta_r, root,
+                     (int32_t)num_internal, (int32_t)total, theta_sq, theta_r, roots,
                      (uint32_t)wf_capacity, ygx::no_sink(), -1, gens_hint, &gen, stream);
   if (rc == YGX_ERR_QUEUE_OVERFLOW) flags_out[0] = ygx::kFlagQueueOverflow;
   if (rc) return rc;
@@ -1437,6 +1480,45 @@ int ygx_traverse_walk(const float* center, const float* radius, const float* max
       cudaStreamSynchronize(stream) != cudaSuccess)
     return YGX_ERR_CUDA;
   return YGX_OK;
+}
+
+int ygx_traverse_walk(const float* center, const float* radius, const float* max_extent,
+                      const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
+                      int64_t total, int64_t num_internal, int mac, float theta,
+                      float dehnen_radius_scale, int root, int mode, int gens_hint,
+                      int64_t wf_capacity, int64_t log_capacity, uint64_t* stats_out,
+                      uint32_t* flags_out, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (total < 3 || total > INT32_MAX || num_internal < 1 || mac < 0 || mac > 2 ||
+      root < 0 || root >= total || !stats_out || !flags_out ||
+      (mode != YGX_WALK_LOG && mode != YGX_WALK_COUNT))
+    return YGX_ERR_ARG;
+  return walk_impl(center, radius, max_extent, left32, right32, leafpos32, total, num_internal,
+                   mac, theta, dehnen_radius_scale, ygx::Roots{root, nullptr, 0, nullptr, nullptr},
+                   mode, gens_hint, wf_capacity, log_capacity, stats_out, flags_out, ws, ws_bytes,
+                   stream);
+}
+
+// The walk over a forest of S trees (ygx_batch_build_topology: set s at
+// nodes 2 leaf_off[s] - s, leafpos32 / left32 / right32 / parent32 with
+// global ids), all sets in one wavefront from (root_s, root_s); the
+// counts, pair log and stats as ygx_traverse_walk (YGX_WALK_LOG mode), so
+// ygx_traverse_fill / ygx_traverse_finalize follow on the same workspace
+// with total = all nodes and num_internal = total_leaves - S.
+int ygx_batch_traverse_walk(const float* center, const float* radius, const float* max_extent,
+                            const int32_t* left32, const int32_t* right32,
+                            const int32_t* leafpos32, const int32_t* parent32, int64_t total,
+                            const int64_t* leaf_off, int64_t S, const uint32_t* seg_flags,
+                            int mac, float theta, float dehnen_radius_scale, int gens_hint,
+                            int64_t wf_capacity, int64_t log_capacity, uint64_t* stats_out,
+                            uint32_t* flags_out, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (total < 1 || total > INT32_MAX || S < 1 || !leaf_off || !parent32 || mac < 0 || mac > 2 ||
+      !stats_out || !flags_out)
+    return YGX_ERR_ARG;
+  const int64_t total_leaves = (total + S) / 2;
+  return walk_impl(center, radius, max_extent, left32, right32, leafpos32, total,
+                   total_leaves - S, mac, theta, dehnen_radius_scale,
+                   ygx::Roots{0, leaf_off, S, parent32, seg_flags}, YGX_WALK_LOG, gens_hint,
+                   wf_capacity, log_capacity, stats_out, flags_out, ws, ws_bytes, stream);
 }
 
 // Fill (after a walk without overflow on the same workspace).  Writes the
@@ -1517,7 +1599,8 @@ int ygx_traverse_fill_walk(int64_t total, int64_t num_internal, int mac, float t
   sink.near_total = (unsigned long long)near_total;
   int ran = 0;
   rc = ygx::run_gens(ygx::kWalkFill, mac, s, (int32_t)num_internal, (int32_t)total, theta_sq,
-                     theta_r, root, (uint32_t)wf_capacity, sink, gens, 0, &ran, stream);
+                     theta_r, ygx::Roots{root, nullptr, 0, nullptr, nullptr},
+                     (uint32_t)wf_capacity, sink, gens, 0, &ran, stream);
   if (rc) return rc;
   ygx::k_check_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
       s.far_off, s.far_cnt, s.far_pos, total, s.near_off, s.near_cnt, s.near_pos, L, s.status);
@@ -1608,7 +1691,8 @@ int ygx_traverse_walk_predicted(const float* center, const float* radius,
   sink.near_nbr = near_raw32;
   int gen = 0;
   rc = ygx::run_gens(ygx::kWalkPred, mac, s, (int32_t)num_internal, (int32_t)total, theta_sq,
-                     theta_r, root, (uint32_t)wf_capacity, sink, -1, gens_hint, &gen, stream);
+                     theta_r, ygx::Roots{root, nullptr, 0, nullptr, nullptr},
+                     (uint32_t)wf_capacity, sink, -1, gens_hint, &gen, stream);
   if (rc == YGX_ERR_QUEUE_OVERFLOW) flags_out[0] = ygx::kFlagQueueOverflow;
   if (rc) return rc;
   ygx::k_pred_counts<<<ygx::grid_for(total, 256, ygx::kNumSMs * 4), 256, 0, stream>>>(
@@ -1716,6 +1800,7 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
                           int64_t log_capacity, const int32_t* level32, const int32_t* leafpos32,
                           int index_bits, int32_t* far_src32, int32_t* near_nbr32,
                           const int64_t* far_raw_off, const int64_t* near_raw_off,
+                          const int32_t* far_row_base, const int32_t* near_row_base,
                           void* far_sources,
                           void* far_targets, void* target_levels, void* neighbors,
                           void* neighbor_leaf_positions, int64_t max_nbr, void* ws,
@@ -1734,8 +1819,8 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
   }
   const int64_t stride = total > L ? total : L;
   auto rows_pass = [&](int64_t rows, const int64_t* off, const int32_t* cnt, const int32_t* lvl,
-                       int32_t* raw, const int64_t* roff, void* vals, void* tgts,
-                       void* lvls) -> int {
+                       int32_t* raw, const int64_t* roff, const int32_t* rbase, void* vals,
+                       void* tgts, void* lvls) -> int {
     if (cudaMemsetAsync(s.n_big, 0, 16 * sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
     ygx::k_rows_classify<<<ygx::grid_for(rows, 256), 256, 0, stream>>>(
         rows, cnt, s.class_rows, stride, s.n_big + 1, s.big_rows, s.n_big);
@@ -1743,21 +1828,22 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
 #define YGX_ROWS(C, R)                                                                       \
   ygx::k_rows_class<R><<<grid_small, 256, 0, stream>>>(s.class_rows + (C) * stride,            \
                                                        s.n_big + 1 + (C), off, cnt, lvl, raw, \
-                                                       roff, index_bits, vals, tgts, lvls);   \
+                                                       roff, rbase, index_bits, vals, tgts,   \
+                                                       lvls);                                 \
   YGX_CHECK_LAUNCH();
     YGX_ROWS(0, 1) YGX_ROWS(1, 2) YGX_ROWS(2, 4) YGX_ROWS(3, 8) YGX_ROWS(4, 16) YGX_ROWS(5, 32)
 #undef YGX_ROWS
     ygx::k_rows_big<<<ygx::kBigGrid, ygx::kBigThreads, big_smem, stream>>>(
-        s.big_rows, s.n_big, stride, off, cnt, lvl, raw, roff, index_bits, vals, tgts, lvls,
+        s.big_rows, s.n_big, stride, off, cnt, lvl, raw, roff, rbase, index_bits, vals, tgts, lvls,
         s.bitmaps, total);
     YGX_CHECK_LAUNCH();
     return YGX_OK;
   };
-  int rc2 = rows_pass(total, s.far_off, s.far_cnt, level32, far_src32, far_raw_off, far_sources,
-                      far_targets, target_levels);
+  int rc2 = rows_pass(total, s.far_off, s.far_cnt, level32, far_src32, far_raw_off,
+                      far_row_base, far_sources, far_targets, target_levels);
   if (rc2) return rc2;
-  rc2 = rows_pass(L, s.near_off, s.near_cnt, nullptr, near_nbr32, near_raw_off, neighbors,
-                  nullptr, nullptr);
+  rc2 = rows_pass(L, s.near_off, s.near_cnt, nullptr, near_nbr32, near_raw_off, near_row_base,
+                  neighbors, nullptr, nullptr);
   if (rc2) return rc2;
   if (neighbor_leaf_positions && max_nbr > 0) {
     ygx::k_neighbor_leaf_positions<<<ygx::grid_for(L * max_nbr, 256), 256, 0, stream>>>(

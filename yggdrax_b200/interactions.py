@@ -589,7 +589,8 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     L.check(lib.ygx_traverse_finalize(
         total, ni, cap, log_cap, L.ptr(d.level32), L.ptr(leafpos32), ib, L.ptr(far_src32),
         L.ptr(near_nbr32), L.ptr(far_raw_off) if far_raw_off is not None else None,
-        L.ptr(near_raw_off) if near_raw_off is not None else None, L.ptr(sources), L.ptr(targets),
+        L.ptr(near_raw_off) if near_raw_off is not None else None, None, None,
+        L.ptr(sources), L.ptr(targets),
         L.ptr(target_levels),
         L.ptr(neighbors), L.ptr(nlp) if max_nbr > 0 else None, max_nbr, L.ptr(ws), ws.numel(),
         st), "ygx_traverse_finalize")
