@@ -51,7 +51,7 @@ SORT_PASS_DRAM_BYTES: dict = {16_777_216: 361_430_000}
 LEAF = 32
 THETA = 0.6
 MAC = "dehnen"
-WORKLOAD = "plummer_16M_radix_leaf32_dehnen_theta0.6_two_pass"
+WORKLOAD = "plummer_16M_radix_leaf32_dehnen_theta0.6_exact_lists"
 METRIC = "particles/s full build+traversal (Morton, sort, radix build, geometry, exact lists)"
 
 
@@ -261,6 +261,8 @@ def main():
     ap.add_argument("--breakdown", action="store_true")
     ap.add_argument("--no-modes", action="store_true",
                     help="skip timing the two-pass and learned traversal schedules")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip timing the batched workload (4096 uneven point sets)")
     ap.add_argument("--roofline-only", action="store_true",
                     help="time only the sort roofline leg (for profiling it)")
     args = ap.parse_args()
@@ -364,6 +366,10 @@ def main():
     if not args.no_modes:
         modes.update(mode_timings(step, pos_d, mass_d, n, args.steps, barrier))
 
+    batched = None
+    if not args.no_batched:  # every rank (barriers inside)
+        batched = batched_timing(dev, args.steps, barrier)
+
     breakdown = None
     if args.breakdown:
         breakdown = stage_breakdown(pos_d, mass_d, dev)
@@ -396,6 +402,7 @@ def main():
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
             "modes": modes,
+            "batched": batched,
         }
         if breakdown is not None:
             line["breakdown_ms"] = breakdown
@@ -440,6 +447,79 @@ def mode_timings(step, pos_d, mass_d, n, steps, barrier) -> dict:
         finally:
             yb.set_traversal_mode("log")
     return out
+
+
+def batched_timing(dev, steps, barrier, sets: int = 4096, loop_sample: int = 64) -> dict:
+    """Device time of the batched workload: 4096 independent point sets,
+    sizes log-uniform in [256, 65536] (about 48M points), half uniform cube,
+    half Plummer, unit masses, seed 3; radix leaf 16, dehnen theta 0.6.  One
+    step = the batched build, geometry and exact lists of every set, one
+    launch per stage.  Beside it, the single-set API called set by set on
+    ``loop_sample`` sets, scaled to all sets by point count."""
+    import torch
+
+    import yggdrax_b200 as yb
+    from yggdrax_b200 import _lib as L
+    from yggdrax_b200 import batch as B
+    from yggdrax_b200 import inputs
+
+    pos, mass, off = inputs.batched_sets(sets, 3)
+    P = torch.from_numpy(pos).to(dev)
+    M = torch.from_numpy(mass).to(dev)
+    lib = L.lib()
+
+    def step():
+        bt = B.build_trees_batched(P, M, off, leaf_size=16)
+        bg = B.compute_tree_geometry_batched(bt)
+        bi = B.build_interactions_and_neighbors_batched(bt, bg, theta=THETA, mac_type=MAC)
+        return bt, bi
+
+    for _ in range(3):
+        bt, bi = step()
+    del bt, bi
+    barrier()
+    l0 = lib.ygx_launch_counter()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        bt, bi = step()
+    b.record()
+    barrier()
+    ms = a.elapsed_time(b) / steps
+    launches = (lib.ygx_launch_counter() - l0) / steps
+    far, near = int(bi.sources.numel()), int(bi.neighbors.numel())
+    nodes = bt.total_nodes
+    del bt, bi
+
+    # the single-set API, set by set, on a sample of sets
+    rng = np.random.default_rng(0)
+    pick = np.sort(rng.choice(sets, size=min(loop_sample, sets), replace=False))
+    views = [(P[off[i]:off[i + 1]], M[off[i]:off[i + 1]]) for i in pick]
+
+    def loop():
+        for p, m in views:
+            t, ps = yb.build_tree(p, m, leaf_size=16, return_reordered=True)[:2]
+            g = yb.compute_tree_geometry(t, ps)
+            if int(t.num_internal_nodes) > 0:
+                yb.build_interactions_and_neighbors(t, g, theta=THETA, mac_type=MAC)
+
+    loop()
+    barrier()
+    a.record()
+    loop()
+    b.record()
+    barrier()
+    sample_pts = int(sum(off[i + 1] - off[i] for i in pick))
+    loop_ms = a.elapsed_time(b) * float(off[-1]) / sample_pts
+    n = int(off[-1])
+    return {"workload": "4096_sets_loguniform_256_65536_cube_plummer_radix_leaf16_dehnen_theta0.6",
+            "n_sets": sets, "n_particles": n, "total_nodes": nodes, "ms_per_step": ms,
+            "value": n / (ms / 1e3), "unit": "particles/s", "far_entries": far,
+            "near_entries": near, "pairs_per_s": (far + near) / (ms / 1e3),
+            "gpu_launches_per_step": launches,
+            "single_set_loop": {"ms_estimate": loop_ms, "sample_sets": len(pick),
+                                "sample_particles": sample_pts,
+                                "speedup_of_batched": loop_ms / ms}}
 
 
 def stage_breakdown(pos_d, mass_d, dev):

@@ -151,3 +151,50 @@ def test_learned_mode_exact_with_generous_capacities(cuda_device, oracle):
     stats = _learned_lists(cuda_device, oracle, predictor.init_params(8),
                            dict(slack_far=12.0, slack_near=12.0, add=64), n=40_000)
     assert stats["ovf_rows"] == 0
+
+
+def _constant_predictor(Y, M):
+    """The method without the network: every node gets the same prediction
+    (the mean target of each output), weights zero."""
+    from yggdrax_b200 import predictor
+
+    p = np.zeros(predictor.N_PARAMS, np.float32)
+    for j in range(2):
+        sel = M[:, j] > 0
+        p[-2 + j] = float(Y[sel, j].mean())
+    return p
+
+
+def test_trained_network_gains_over_a_constant_capacity(cuda_device, oracle):
+    """What the trained network buys over the same one-pass method without
+    it.  The baseline gives every node the same predicted length (per list
+    kind), with its slack fitted on the evaluation system's own exact row
+    lengths so that it overflows on no more rows than the shipped network
+    does; the network needs far less padding for that overflow rate.  Both
+    runs return exactly the oracle's lists."""
+    import yggdrax_b200 as yb
+    from yggdrax_b200 import inputs, predictor
+    from yggdrax_b200.interactions import _leaf_ordering
+
+    dev, n, seed = cuda_device, 200_000, 41
+    trained, cal = predictor.load_weights()
+    st = _learned_lists(dev, oracle, trained, dict(cal), n=n, seed=seed)
+    # exact row lengths of the same system, from the plain path
+    pos, mass = inputs.plummer(n, seed)
+    t, ps = yb.build_tree(_t(pos, dev), _t(mass, dev), leaf_size=16, return_reordered=True)[:2]
+    g = yb.compute_tree_geometry(t, ps)
+    fi, nb = yb.build_interactions_and_neighbors(t, g, theta=0.6, mac_type="dehnen")
+    total, ni = int(t.parent.shape[0]), int(t.left_child.shape[0])
+    _, leafpos32, _, _ = _leaf_ordering(t, total, ni, dev)
+    Y, Mk = predictor.targets_of(t, fi.counts, nb.counts, leafpos32)
+    pc = _constant_predictor(Y.cpu().numpy(), Mk.cpu().numpy())
+    X = predictor.node_features(t, g, 0.6, "dehnen")
+    q = 1.0 - max(st["overflow_row_fraction"], 1e-3) / 2
+    cal_c = predictor.calibrate(predictor.forward(_t(pc, dev), X), Y, Mk, quantile=q,
+                                add=int(cal["add"]))
+    sc = _learned_lists(dev, oracle, pc, dict(cal_c), n=n, seed=seed)
+    print(f"trained: over-allocation {st['over_allocation']:.2f}, overflow rows "
+          f"{st['overflow_row_fraction']:.4f}; constant: over-allocation "
+          f"{sc['over_allocation']:.2f}, overflow rows {sc['overflow_row_fraction']:.4f}")
+    assert sc["overflow_row_fraction"] <= st["overflow_row_fraction"] + 1e-3
+    assert st["over_allocation"] < 0.5 * sc["over_allocation"]

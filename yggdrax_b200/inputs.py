@@ -68,4 +68,24 @@ def plummer_clumps(n: int, seed: int = 2, *, clumps: int = 64, box: float = 10.0
     return pos.astype(np.float32), mass.astype(np.float32)
 
 
-__all__ = ["uniform_cube", "plummer", "plummer_clumps"]
+def batched_sets(sets: int = 4096, seed: int = 3, *, lo: int = 256, hi: int = 65536):
+    """Independent point sets of uneven size, stored back to back: set sizes
+    ``floor(exp(U[ln lo, ln hi]))``, even-numbered sets uniform in [-1, 1]^3,
+    odd-numbered sets Plummer spheres (a = 1, r <= 20); unit masses.
+    Returns ``(positions (N, 3), masses (N,), offsets (sets + 1,) int64)``."""
+    rng = _rng(seed)
+    sizes = np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi), size=sets))).astype(np.int64)
+    sizes = np.maximum(sizes, 1)
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    pos = np.empty((int(offsets[-1]), 3), np.float32)
+    for s in range(sets):
+        n = int(sizes[s])
+        if s % 2 == 0:
+            p = rng.uniform(-1.0, 1.0, size=(n, 3))
+        else:
+            p = _plummer_radii(rng, n, 1.0, 20.0)[:, None] * _directions(rng, n)
+        pos[offsets[s]:offsets[s + 1]] = p
+    return pos, np.ones(pos.shape[0], np.float32), offsets
+
+
+__all__ = ["uniform_cube", "plummer", "plummer_clumps", "batched_sets"]

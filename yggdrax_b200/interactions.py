@@ -203,6 +203,7 @@ def set_reference_limits(enabled: bool) -> None:
 
 
 _DENSE_BUDGET: Optional[int] = None
+_DENSE_WARNED: set = set()
 LAST_WALK_STATS: dict = {}  # diagnostics of the most recent walk
 # Capacity hints per (mac, theta): wavefront and pair-log entries per tree
 # node that the last walk needed.  The next walk starts from them (with
@@ -580,10 +581,12 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     max_nbr = s["max_near"]
     dense_bytes = nl * max_nbr * (4 if ib == 32 else 8)
     if dense_bytes > _dense_neighbor_budget(dev):
-        logger.warning(
-            "neighbor_leaf_positions would need %.1f GiB (%d leaves x %d neighbours); "
-            "returning an empty (L, 0) table -- raise the budget with "
-            "set_dense_neighbor_budget() to build it", dense_bytes / 2**30, nl, max_nbr)
+        if (nl, max_nbr) not in _DENSE_WARNED:  # once per table shape
+            _DENSE_WARNED.add((nl, max_nbr))
+            logger.warning(
+                "neighbor_leaf_positions would need %.1f GiB (%d leaves x %d neighbours); "
+                "returning an empty (L, 0) table -- raise the budget with "
+                "set_dense_neighbor_budget() to build it", dense_bytes / 2**30, nl, max_nbr)
         max_nbr = 0
     nlp = torch.empty((nl, max_nbr), dtype=idt, device=dev)
     L.check(lib.ygx_traverse_finalize(
