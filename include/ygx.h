@@ -49,6 +49,13 @@ enum {
 #define YGX_FLAG_BAD_INPUT (1u << 5)
 #define YGX_FLAG_LOG_OVERFLOW (1u << 6)
 
+/* launch-shape knobs (ygx_tune_set / ygx_tune_get); chosen by the autotuner */
+#define YGX_TUNE_SORT_RANK 0   /* onesweep ranking: 0 ballots, 1 peer tables, 2 by skew */
+#define YGX_TUNE_SORT_SKEW 1   /* policy 2 threshold: max digit share x 256 (1..256)    */
+#define YGX_TUNE_WALK_BLOCKS 2 /* walk CTAs per SM (2..6)                              */
+#define YGX_TUNE_REFIT_WARPS 3 /* warps per CTA of the leaf refit (2, 4, 8)            */
+#define YGX_TUNE_ROW_GRID 4    /* CTAs per SM of the short-row finalize (4..32, pow2)  */
+
 /* traversal statistics words (host array of YGX_TSTAT_WORDS uint64) */
 #define YGX_TSTAT_WORDS 16
 #define YGX_TSTAT_FAR_TOTAL 0   /* directed far entries (sum of far counts)    */
@@ -79,6 +86,11 @@ int ygx_workspace_init(void* ws, size_t ws_bytes, cudaStream_t stream);
 int ygx_status_read(const void* ws, uint32_t* host_flags, cudaStream_t stream);
 /* Number of kernel launches this library has issued in this process. */
 uint64_t ygx_launch_counter(void);
+/* Launch-shape knobs (YGX_TUNE_*), process-wide.  No reference counterpart:
+ * the reference tunes nothing at run time.  An illegal value is rejected with
+ * YGX_ERR_ARG and leaves the knob unchanged.  Results never depend on a knob. */
+int ygx_tune_set(int knob, int value);
+int ygx_tune_get(int knob, int* value);
 
 /* ---- L0: bounds, Morton codes, stable sort ------------------------------- */
 

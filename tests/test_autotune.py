@@ -1,0 +1,66 @@
+"""The autotuner's host logic on the CPU: the knob table in the library
+(set / get, illegal values rejected), the JSON cache, and the search picking
+the cheapest setting of a synthetic cost model."""
+
+import pytest
+
+
+@pytest.fixture
+def tune_mod(monkeypatch, tmp_path):
+    from yggdrax_b200 import _lib as L
+    from yggdrax_b200 import autotune
+
+    try:
+        L.lib()
+    except Exception as e:  # pragma: no cover - library not built
+        pytest.skip(f"libygx.so not loadable: {e}")
+    monkeypatch.setenv("YGGDRAX_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    saved = autotune.current()
+    yield autotune
+    autotune.apply(saved)
+
+
+def test_knob_table_roundtrip(tune_mod):
+    from yggdrax_b200 import _lib as L
+
+    tune_mod.apply({"walk_blocks": 4, "row_grid": 8, "sort_rank": 2, "sort_skew": 100})
+    cur = tune_mod.current()
+    assert cur["walk_blocks"] == 4 and cur["row_grid"] == 8
+    assert cur["sort_rank"] == 2 and cur["sort_skew"] == 100
+    for knob, bad in (("walk_blocks", 1), ("walk_blocks", 7), ("refit_warps", 3),
+                      ("row_grid", 12), ("sort_rank", 3), ("sort_skew", 0), ("sort_skew", 257)):
+        with pytest.raises(ValueError):
+            tune_mod.apply({knob: bad})
+        assert tune_mod.current()[knob] == cur[knob]
+    with pytest.raises(ValueError):
+        tune_mod.apply({"no_such_knob": 1})
+    assert L.lib().ygx_tune_get(99, None) == 1
+
+
+def test_search_finds_cheapest_setting(tune_mod, monkeypatch):
+    # synthetic cost: best at walk_blocks=4, refit_warps=2, row_grid=32
+    def cost():
+        c = tune_mod.current()
+        return (10.0 + abs(c["walk_blocks"] - 4) + (c["refit_warps"] != 2) * 0.5
+                + (32 - c["row_grid"]) * 0.01)
+
+    monkeypatch.setattr(tune_mod, "time_ms", lambda fn, dev, reps=3, warmup=1: cost())
+    tune_mod.apply({"walk_blocks": 6, "refit_warps": 8, "row_grid": 16})
+    log = []
+    best = tune_mod.tune(lambda: None, None, log=log)
+    assert (best["walk_blocks"], best["refit_warps"], best["row_grid"]) == (4, 2, 32)
+    assert tune_mod.current() == best
+    assert len(log) == 1 + 3 + 2 + 3
+
+
+def test_cache_roundtrip(tune_mod, monkeypatch):
+    calls = []
+    monkeypatch.setattr(tune_mod, "tune",
+                        lambda step, dev, **kw: calls.append(1) or dict(tune_mod.current(),
+                                                                        walk_blocks=3))
+    cfg = tune_mod.tuned("dev|kind|n2^20|leaf=16", lambda: None, None)
+    assert cfg["walk_blocks"] == 3 and len(calls) == 1
+    tune_mod.apply({"walk_blocks": 6})
+    cfg2 = tune_mod.tuned("dev|kind|n2^20|leaf=16", lambda: None, None)
+    assert cfg2["walk_blocks"] == 3 and len(calls) == 1  # from the cache
+    assert tune_mod.current()["walk_blocks"] == 3

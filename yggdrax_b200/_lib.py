@@ -37,6 +37,7 @@ FLAG_MALFORMED = 1 << 4
 FLAG_BAD_INPUT = 1 << 5
 FLAG_LOG_OVERFLOW = 1 << 6
 WALK_LOG = 0
+TUNE = dict(sort_rank=0, sort_skew=1, walk_blocks=2, refit_warps=3, row_grid=4)
 WALK_COUNT = 1
 
 TSTAT_WORDS = 16
@@ -56,6 +57,8 @@ _SIGS = {
     "ygx_workspace_init": (I32, [P, SZ, P]),
     "ygx_status_read": (I32, [P, P, P]),
     "ygx_launch_counter": (ctypes.c_uint64, []),
+    "ygx_tune_set": (I32, [I32, I32]),
+    "ygx_tune_get": (I32, [I32, P]),
     "ygx_bounds": (I32, [P, I64, P, P, SZ, P]),
     "ygx_morton_encode": (I32, [P, I64, P, P, P]),
     "ygx_encode_sort_workspace_size": (SZ, [I64]),

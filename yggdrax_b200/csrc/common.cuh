@@ -10,6 +10,17 @@ namespace ygx {
 
 constexpr int kNumSMs = 148;
 
+// Launch-shape knobs (set through ygx_tune_set; defaults are the measured
+// best on B200 for the 16M-particle Plummer pipeline).
+struct Tune {
+  int sort_rank_policy = 2;    // onesweep ranking: 0 ballots, 1 peer tables, 2 by digit skew
+  int sort_skew_q8 = 32;       // policy 2: peer tables while max digit share <= q8 / 256
+  int walk_blocks_per_sm = 6;  // walk CTAs per SM (<= kWalkBlocksPerSM)
+  int refit_warps = 8;         // warps per CTA of the leaf refit
+  int row_grid_per_sm = 16;    // CTAs per SM of the short-row finalize kernels
+};
+extern Tune g_tune;
+
 // Device-side status word.  Kernels never trap: a bounded spin that gives up,
 // or a capacity that is exceeded, ORs a flag in here and the kernel returns.
 // Flags map one-to-one onto the YGX_ERR_* return codes.

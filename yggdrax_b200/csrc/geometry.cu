@@ -406,7 +406,7 @@ int ygx_tree_geometry(const void* node_ranges, int64_t total, int index_bits,
         leaf_codes, leaf_depths, ni, L, index_bits, bounds, parent32, left32, right32, s.mn, s.mx,
         s.arrive, tree_flags, center, half_extent, radius, max_extent);
   } else {
-    const int warps = 8;
+    const int warps = ygx::g_tune.refit_warps;
     ygx::k_leaf_ranges_refit<<<ygx::grid_for((L + 31) / 32, warps, ygx::kNumSMs * 16), warps * 32, 0,
                                stream>>>(
         node_ranges, ni, L, index_bits, positions_sorted, max_leaf_size, max_leaf_size == 0,
@@ -442,7 +442,7 @@ int ygx_batch_tree_geometry(const void* node_ranges, int64_t total, int64_t S,
   ygx::Arena a{(char*)ws, 0, ws_bytes};
   ygx::GeoScratch s = ygx::carve_geo(a, total);
   if (cudaMemsetAsync(s.arrive, 0, sizeof(int32_t) * total, stream) != cudaSuccess) return YGX_ERR_CUDA;
-  const int warps = 8;
+  const int warps = ygx::g_tune.refit_warps;
   ygx::k_seg_leaf_refit<<<ygx::grid_for((total_leaves + 31) / 32, warps, ygx::kNumSMs * 16),
                           warps * 32, 0, stream>>>(
       node_ranges, leaf_off, leaf_seg, offsets, total_leaves, index_bits, positions_sorted,

@@ -37,11 +37,20 @@ __global__ void k_histogram(const uint64_t* __restrict__ keys, int64_t n, int be
     if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
 }
 
-// One CTA per pass: exclusive scan of 256 digit counts.
-__global__ void k_hist_scan(const uint32_t* __restrict__ hist, uint32_t* __restrict__ offsets) {
+// One CTA per pass: exclusive scan of 256 digit counts, and the pass's
+// ranking method (rank_mode[p]): policy 0 = ballots, 1 = peer tables,
+// 2 = peer tables unless one digit holds more than skew_q8 / 256 of the keys
+// (many lanes of a warp then share a digit and the peer-table atomics
+// serialise on it).
+__global__ void k_hist_scan(const uint32_t* __restrict__ hist, uint32_t* __restrict__ offsets,
+                            uint32_t* __restrict__ rank_mode, int policy, int skew_q8) {
   __shared__ uint32_t s[kSortRadix];
+  __shared__ uint32_t s_max;
   const int p = blockIdx.x, t = threadIdx.x;
   uint32_t v = hist[p * kSortRadix + t];
+  if (t == 0) s_max = 0;
+  __syncthreads();
+  atomicMax(&s_max, v);
   s[t] = v;
   __syncthreads();
   for (int off = 1; off < kSortRadix; off <<= 1) {
@@ -51,7 +60,14 @@ __global__ void k_hist_scan(const uint32_t* __restrict__ hist, uint32_t* __restr
     __syncthreads();
   }
   offsets[p * kSortRadix + t] = s[t] - v;
+  if (t == kSortRadix - 1) {
+    const uint64_t tot = s[t];
+    rank_mode[p] = policy == 2 ? ((uint64_t)s_max * 256u <= tot * (uint64_t)skew_q8 ? 1u : 0u)
+                               : (uint32_t)policy;
+  }
 }
+
+constexpr int kPeerWords = (kSortThreads / 32) * 2 * kSortRadix;  // peer tables, in keys[]
 
 struct __align__(16) OnesweepSmem {
   uint32_t warp_hist[kSortThreads / 32][kSortRadix];
@@ -59,9 +75,12 @@ struct __align__(16) OnesweepSmem {
   uint32_t glob[kSortRadix];
   uint32_t warp_tot[kSortThreads / 32];
   uint32_t ticket;
-  uint64_t keys[kSortTile];
+  alignas(16) uint64_t keys[kSortTile];  // 16-byte aligned: zeroed with uint4 stores
   uint32_t vals[kSortTile];
 };
+static_assert(offsetof(OnesweepSmem, keys) % 16 == 0, "key staging area is 16-byte aligned");
+static_assert(kPeerWords * sizeof(uint32_t) <= kSortTile * sizeof(uint64_t),
+              "peer tables fit in the key staging area");
 
 template <bool kIotaValues>
 __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
@@ -69,13 +88,18 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
                int64_t n, int shift, const uint32_t* __restrict__ digit_offsets,
                uint32_t* __restrict__ lookback, uint32_t* __restrict__ ticket_counter,
                uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
-               uint32_t* __restrict__ status) {
+               const uint32_t* __restrict__ rank_mode, uint32_t* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   OnesweepSmem& sm = *reinterpret_cast<OnesweepSmem*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool peer_tables = *rank_mode != 0;  // uniform over the grid
 
   for (int i = tid; i < (kSortThreads / 32) * kSortRadix; i += kSortThreads)
     (&sm.warp_hist[0][0])[i] = 0;
+  if (peer_tables) {  // two zeroed 256-word tables per warp, in the (idle) key staging area
+    uint4* z = reinterpret_cast<uint4*>(sm.keys);
+    for (int i = tid; i < kPeerWords / 4; i += kSortThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
   __shared__ uint32_t s_cnt[kSortRadix];
   if (tid < kSortRadix) s_cnt[tid] = 0;
   if (tid == 0) sm.ticket = atomicAdd(ticket_counter, 1u);
@@ -152,6 +176,30 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
   // shuffles.
   const unsigned lt_mask = (1u << lane) - 1u;
   constexpr int kRankGroup = 4;
+  if (peer_tables) {
+    // Peer-table multisplit: every lane ORs its lane bit into its digit's
+    // word of a per-warp table, reads back the word (its peer mask) and the
+    // warp's running count of that digit; the highest peer advances the
+    // count and clears the word.  Two tables alternate so a clear never
+    // races the next item's ORs.  Earlier items, then lower lanes, rank first.
+    uint32_t* tb0 = reinterpret_cast<uint32_t*>(sm.keys) + warp * (2 * kSortRadix);
+    uint32_t* wh = sm.warp_hist[warp];
+#pragma unroll
+    for (int i = 0; i < kSortItems; ++i) {
+      uint32_t* tb = tb0 + (i & 1) * kSortRadix;
+      const uint32_t dg = (uint32_t)(keys[i] >> shift) & (kSortRadix - 1);
+      atomicOr(&tb[dg], 1u << lane);
+      __syncwarp();
+      const unsigned pm = tb[dg];
+      const uint32_t before = wh[dg];
+      __syncwarp();
+      rank[i] = (uint16_t)(before + __popc(pm & lt_mask));
+      if ((pm >> lane) == 1u) {
+        wh[dg] = before + __popc(pm);
+        tb[dg] = 0u;
+      }
+    }
+  } else {
 #pragma unroll
   for (int g = 0; g < kSortItems; g += kRankGroup) {
     unsigned peers[kRankGroup];
@@ -178,6 +226,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
       const uint32_t o = __shfl_sync(0xffffffffu, old[u], __ffs(peers[u]) - 1);
       rank[g + u] = (uint16_t)(o + __popc(peers[u] & lt_mask));
     }
+  }
   }
   // values travel with the keys; loading them here overlaps the look-back
 #pragma unroll
@@ -251,6 +300,7 @@ SortScratch carve_sort_scratch(Arena& a, int64_t n, int max_passes) {
   s.lookback = a.take<uint32_t>((size_t)max_passes * tiles * kSortRadix);
   s.counters = a.take<uint32_t>(64);
   s.offsets = a.take<uint32_t>((size_t)max_passes * kSortRadix);
+  s.rank_mode = a.take<uint32_t>(64);
   s.keys_tmp = a.take<uint64_t>((size_t)(n > 0 ? n : 1));
   s.vals_tmp = a.take<uint32_t>((size_t)(n > 0 ? n : 1));
   return s;
@@ -278,7 +328,8 @@ int onesweep_sort(const uint64_t* keys_in, const uint32_t* vals_in, int64_t n, i
                                                                s.hist);
     YGX_CHECK_LAUNCH();
   }
-  k_hist_scan<<<passes, kSortRadix, 0, st>>>(s.hist, s.offsets);
+  k_hist_scan<<<passes, kSortRadix, 0, st>>>(s.hist, s.offsets, s.rank_mode,
+                                             g_tune.sort_rank_policy, g_tune.sort_skew_q8);
   YGX_CHECK_LAUNCH();
 
   const size_t smem = sizeof(OnesweepSmem);
@@ -307,10 +358,10 @@ int onesweep_sort(const uint64_t* keys_in, const uint32_t* vals_in, int64_t n, i
     int shift = begin_bit + p * kSortRadixBits;
     if (p == 0 && src_v == nullptr)
       k_onesweep<true><<<(unsigned)tiles, kSortThreads, smem, st>>>(
-          src_k, nullptr, n, shift, offs, lb, s.counters + p, dk, dv, status);
+          src_k, nullptr, n, shift, offs, lb, s.counters + p, dk, dv, s.rank_mode + p, status);
     else
       k_onesweep<false><<<(unsigned)tiles, kSortThreads, smem, st>>>(
-          src_k, src_v, n, shift, offs, lb, s.counters + p, dk, dv, status);
+          src_k, src_v, n, shift, offs, lb, s.counters + p, dk, dv, s.rank_mode + p, status);
     YGX_CHECK_LAUNCH();
     src_k = dk;
     src_v = dv;

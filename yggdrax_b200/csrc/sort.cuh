@@ -25,6 +25,7 @@ size_t onesweep_scratch_bytes(int64_t n, int max_passes = 8);
 struct SortScratch {
   uint32_t* hist;       // [passes][256] digit counts
   uint32_t* offsets;    // [passes][256] exclusive digit offsets
+  uint32_t* rank_mode;  // [passes] ranking method of each pass (k_hist_scan)
   uint32_t* lookback;   // [passes][tiles][256]
   uint32_t* counters;   // [passes] tile tickets
   uint64_t* keys_tmp;   // [n]

@@ -629,13 +629,14 @@ __global__ void k_seed(int2* wf, uint32_t* cnt, uint32_t* sizes, int root) {
 // over the regions round-robin.  root_s = 2 leaf_off[s] - s, or for a set
 // flagged malformed its first node without a parent (the reference starts
 // its walk at argmin(parent)).
-__global__ void k_seed_forest(int2* wf, uint32_t* cnt, uint32_t* sizes, uint32_t R,
+__global__ void k_seed_forest(int2* wf, uint32_t* cnt, uint32_t* sizes, uint32_t R, int G,
                               const int64_t* __restrict__ leaf_off, int64_t S,
                               const int32_t* __restrict__ parent32,
                               const uint32_t* __restrict__ seg_flags,
                               uint32_t* __restrict__ status) {
+  // regions 0 .. G-1 (G = the walk's grid) hold the seeds, the rest stay empty
   for (int r = threadIdx.x; r < kWalkGrid; r += blockDim.x) {
-    const int64_t c = S > r ? (S - r + kWalkGrid - 1) / kWalkGrid : 0;
+    const int64_t c = r < G && S > r ? (S - r + G - 1) / G : 0;
     cnt[r] = c <= R ? (uint32_t)c : R;
     if (c > R) raise_flag(status, kFlagQueueOverflow);
   }
@@ -646,7 +647,7 @@ __global__ void k_seed_forest(int2* wf, uint32_t* cnt, uint32_t* sizes, uint32_t
       for (int64_t k = NO; k < NO + 2 * Ls - 1; ++k)
         if (parent32[k] < 0) { root = k; break; }
     }
-    const int64_t r = sg % kWalkGrid, k = sg / kWalkGrid;
+    const int64_t r = sg % G, k = sg / G;
     if (k < R) wf[(size_t)r * R + k] = make_int2((int)root, (int)root);
   }
   if (threadIdx.x == 0) sizes[0] = (uint32_t)S;
@@ -1287,6 +1288,15 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap, i
   return s;
 }
 
+// CTAs of every walk generation: a knob, at most kWalkGrid (the number of
+// wavefront / log regions the workspace holds; regions past the grid stay
+// empty).
+static int walk_grid() {
+  int b = g_tune.walk_blocks_per_sm;
+  b = b < 1 ? 1 : (b > kWalkBlocksPerSM ? kWalkBlocksPerSM : b);
+  return kNumSMs * b;
+}
+
 static int launch_gen(int mode, int mac, const TravScratch& s, int32_t ni, int32_t total_nodes,
                       float theta_sq, float theta, int gen, uint32_t cap, const RowSink& sink,
                       cudaStream_t st) {
@@ -1296,7 +1306,7 @@ static int launch_gen(int mode, int mac, const TravScratch& s, int32_t ni, int32
   uint32_t* cout = s.region_cnt[(gen + 1) & 1];
   const uint32_t R = (uint32_t)region_capacity(cap);
 #define YGX_GEN(MODE, MAC)                                                                  \
-  k_walk_gen<MODE, MAC><<<kWalkGrid, kWalkThreads, 0, st>>>(                                \
+  k_walk_gen<MODE, MAC><<<walk_grid(), kWalkThreads, 0, st>>>(                              \
       s.recs, ni, total_nodes, theta_sq, theta, in, out, cin, cout, R, s.sizes, gen,        \
       s.far_cnt, s.near_cnt, s.log, s.log_cnt, s.log_region, sink, s.stats, s.status)
 #define YGX_GEN_MAC(MODE)                     \
@@ -1335,7 +1345,8 @@ static int run_gens(int mode, int mac, const TravScratch& s, int32_t ni, int32_t
                     cudaStream_t stream) {
   if (roots.leaf_off)
     k_seed_forest<<<1, 256, 0, stream>>>(s.wf[0], s.region_cnt[0], s.sizes,
-                                         (uint32_t)region_capacity(cap), roots.leaf_off,
+                                         (uint32_t)region_capacity(cap), walk_grid(),
+                                         roots.leaf_off,
                                          roots.S, roots.parent32, roots.seg_flags, s.status);
   else
     k_seed<<<1, 256, 0, stream>>>(s.wf[0], s.region_cnt[0], s.sizes, roots.root);
@@ -1810,7 +1821,7 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
   ygx::TravScratch s;
   int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity, log_capacity);
   if (rc) return rc;
-  const int grid_small = ygx::kNumSMs * 16;
+  const int grid_small = ygx::kNumSMs * ygx::g_tune.row_grid_per_sm;
   const size_t big_smem = sizeof(int32_t) * ygx::kBlockRowCap;
   static bool big_attr = false;
   if (!big_attr) {
