@@ -491,6 +491,23 @@ def batched_timing(dev, steps, barrier, sets: int = 4096, loop_sample: int = 64)
     nodes = bt.total_nodes
     del bt, bi
 
+    # the same step replayed from a captured CUDA graph (inputs copied into
+    # the graph's buffers, one status read-back per step)
+    pipe = B.BatchedPipeline(off, leaf_size=16, theta=THETA, mac_type=MAC, device=dev)
+    pipe(P, M)  # ordinary path + capture
+    for _ in range(2):
+        pipe(P, M)
+    barrier()
+    a.record()
+    replayed = True
+    for _ in range(steps):
+        pipe(P, M)
+        replayed = replayed and pipe.last_replayed
+    b.record()
+    barrier()
+    graph_ms = a.elapsed_time(b) / steps
+    del pipe
+
     # the single-set API, set by set, on a sample of sets
     rng = np.random.default_rng(0)
     pick = np.sort(rng.choice(sets, size=min(loop_sample, sets), replace=False))
@@ -517,6 +534,8 @@ def batched_timing(dev, steps, barrier, sets: int = 4096, loop_sample: int = 64)
             "value": n / (ms / 1e3), "unit": "particles/s", "far_entries": far,
             "near_entries": near, "pairs_per_s": (far + near) / (ms / 1e3),
             "gpu_launches_per_step": launches,
+            "cuda_graph": {"ms_per_step": graph_ms, "value": n / (graph_ms / 1e3),
+                           "all_steps_replayed": replayed},
             "single_set_loop": {"ms_estimate": loop_ms, "sample_sets": len(pick),
                                 "sample_particles": sample_pts,
                                 "speedup_of_batched": loop_ms / ms}}

@@ -432,6 +432,29 @@ int ygx_batch_traverse_walk(const float* center, const float* radius, const floa
                             int64_t wf_capacity, int64_t log_capacity, uint64_t* stats_out,
                             uint32_t* flags_out, void* ws, size_t ws_bytes, cudaStream_t stream);
 
+/* The batched walk + fill + finalize in one call with every size fixed by
+ * the caller (exactly `gens` generations; wavefront / log capacities;
+ * far_capacity / near_capacity output entries) and no host synchronization
+ * or copy, so that a CUDA graph can capture it.  What does not fit is
+ * flagged in the workspace status (rows then left empty); read the flags and
+ * the statistics with ygx_traverse_stats_read.  No reference counterpart. */
+int ygx_batch_traverse_lists(
+    const float* center, const float* radius, const float* max_extent, const int32_t* left32,
+    const int32_t* right32, const int32_t* leafpos32, const int32_t* parent32,
+    const int32_t* nbl32, const int32_t* level32, const int32_t* node_base32,
+    const int32_t* leaf_base32, int64_t total, const int64_t* leaf_off, int64_t S,
+    const uint32_t* seg_flags, int mac, float theta, float dehnen_radius_scale, int gens,
+    int64_t wf_capacity, int64_t log_capacity, int64_t far_capacity, int64_t near_capacity,
+    int index_bits, void* node_offsets, void* far_counts, void* near_offsets, void* near_counts,
+    int32_t* far_src32, int32_t* near_nbr32, void* sources, void* targets, void* target_levels,
+    void* neighbors, void* ws, size_t ws_bytes, cudaStream_t stream);
+
+/* Statistics words (YGX_TSTAT_*) and status flags of a traversal workspace,
+ * copied to the host; synchronizes the stream. */
+int ygx_traverse_stats_read(int64_t total, int64_t num_leaves, int64_t wf_capacity,
+                            int64_t log_capacity, const void* ws, size_t ws_bytes,
+                            uint64_t* stats_out, uint32_t* flags_out, cudaStream_t stream);
+
 int ygx_traverse_status(const void* ws, uint32_t* flags_out, cudaStream_t stream);
 
 #ifdef __cplusplus

@@ -88,3 +88,57 @@ def test_batched_sets_match_single_set_path(cuda_device, leaf):
             _eq(f"set {i} far.{f}", getattr(fb, f), getattr(fi, f))
         for f in NEAR_FIELDS:
             _eq(f"set {i} near.{f}", getattr(nb, f), getattr(ni_, f))
+
+
+def _flat(bt, bg, bi):
+    return [x.detach().cpu().numpy().copy() for x in (
+        bt.particle_indices, bt.morton_codes, bt.parent, bt.node_ranges, bt.nodes_by_level,
+        bt.inverse_permutation, bg.center, bg.radius, bi.node_offsets, bi.far_counts,
+        bi.sources, bi.targets, bi.target_levels, bi.near_offsets, bi.neighbors)]
+
+
+def test_graph_pipeline_replays_equal_the_ordinary_path(cuda_device):
+    """BatchedPipeline: the captured graph's replays return exactly what the
+    ordinary batched functions return for the same inputs -- on the inputs it
+    was captured with, on new positions, and (through a re-capture) on inputs
+    whose lists outgrow the captured sizes."""
+    import torch
+
+    from yggdrax_b200 import batch as B
+    from yggdrax_b200 import inputs
+
+    pos, mass, off = inputs.batched_sets(48, 11, lo=16, hi=5000)
+    P = torch.from_numpy(pos).to(cuda_device)
+    M = torch.from_numpy(mass).to(cuda_device)
+
+    def ordinary(p):
+        bt = B.build_trees_batched(p, M, off, leaf_size=16)
+        bg = B.compute_tree_geometry_batched(bt)
+        bi = B.build_interactions_and_neighbors_batched(bt, bg, theta=0.6, mac_type="dehnen")
+        return _flat(bt, bg, bi)
+
+    pipe = B.BatchedPipeline(off, leaf_size=16, theta=0.6, mac_type="dehnen", margin=1.2,
+                             device=cuda_device)
+    first = _flat(*pipe(P, M))
+    assert not pipe.last_replayed and pipe.captures == 1
+    ref = ordinary(P)
+    for a, b in zip(first, ref):
+        assert np.array_equal(a, b)
+    for step in range(3):  # new positions each call, same layout
+        g = torch.Generator(device=cuda_device)
+        g.manual_seed(step)
+        P2 = (P * (1.0 + 0.02 * torch.rand(P.shape, device=cuda_device, generator=g))).contiguous()
+        got = _flat(*pipe(P2, M))
+        assert pipe.last_replayed
+        for k, (a, b) in enumerate(zip(got, ordinary(P2))):
+            assert np.array_equal(a, b), (step, k)
+    # a pipeline whose capacities are too small on purpose: every replay
+    # overflows, is flagged, and the call falls back to the ordinary path
+    small = B.BatchedPipeline(off, leaf_size=16, theta=0.6, mac_type="dehnen", margin=0.5,
+                              device=cuda_device)
+    small(P, M)
+    for k in range(2):
+        got = _flat(*small(P, M))
+        assert not small.last_replayed and small.captures == 2 + k
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b)

@@ -117,18 +117,35 @@ class BatchedTrees:
         return t
 
 
-def build_trees_batched(positions: torch.Tensor, masses: torch.Tensor, offsets,
-                        *, leaf_size: int = 16) -> BatchedTrees:
-    """Adaptive radix trees (``build_tree(..., leaf_size)``) of S point sets."""
-    lib = L.lib()
+@dataclass
+class BatchLayout:
+    """Set and leaf offsets of a batch: host copies and device copies.  Leaf
+    counts depend only on the set sizes (ceil(n_s / leaf_size) adaptive
+    leaves per set), so the whole layout is known before any kernel runs."""
+
+    offsets_host: np.ndarray
+    leaf_off_host: np.ndarray
+    offsets: torch.Tensor
+    leaf_off: torch.Tensor
+    leaf_size: int
+
+    @property
+    def num_sets(self) -> int:
+        return int(self.offsets_host.shape[0]) - 1
+
+    @property
+    def num_points(self) -> int:
+        return int(self.offsets_host[-1])
+
+    @property
+    def total_leaves(self) -> int:
+        return int(self.leaf_off_host[-1])
+
+
+def batch_layout(offsets, n: int, leaf_size: int, dev) -> BatchLayout:
+    """Validated layout of S sets over n points (``offsets``: S + 1 entries)."""
     if leaf_size < 1:
         raise ValueError("leaf_size must be >= 1")
-    dev = positions.device
-    st = L.stream_handle(dev)
-    ib, idt = INDEX_BITS, INDEX_DTYPE
-    pos = positions.contiguous().float()
-    mass = masses.contiguous().float()
-    n = int(pos.shape[0])
     off_host = np.asarray(offsets.cpu() if torch.is_tensor(offsets) else offsets, dtype=np.int64)
     S = int(off_host.shape[0]) - 1
     if S < 1 or S > (1 << 16):
@@ -136,7 +153,32 @@ def build_trees_batched(positions: torch.Tensor, masses: torch.Tensor, offsets,
     if off_host[0] != 0 or off_host[-1] != n or np.any(np.diff(off_host) < 1):
         raise ValueError("offsets must start at 0, end at len(positions) and give every set "
                          ">= 1 point")
-    off = torch.from_numpy(off_host).to(dev)
+    leaves = (np.diff(off_host) + leaf_size - 1) // leaf_size
+    leaf_off_host = np.concatenate([[0], np.cumsum(leaves)]).astype(np.int64)
+    return BatchLayout(offsets_host=off_host, leaf_off_host=leaf_off_host,
+                       offsets=torch.from_numpy(off_host).to(dev),
+                       leaf_off=torch.from_numpy(leaf_off_host).to(dev), leaf_size=int(leaf_size))
+
+
+def build_trees_batched(positions: torch.Tensor, masses: torch.Tensor, offsets,
+                        *, leaf_size: int = 16) -> BatchedTrees:
+    """Adaptive radix trees (``build_tree(..., leaf_size)``) of S point sets."""
+    lay = batch_layout(offsets, int(positions.shape[0]), leaf_size, positions.device)
+    return _build_on_layout(positions, masses, lay)
+
+
+def _build_on_layout(positions: torch.Tensor, masses: torch.Tensor,
+                     lay: BatchLayout) -> BatchedTrees:
+    """The batched build on a known layout: kernel launches only, no host
+    synchronization (so a CUDA graph can capture it)."""
+    lib = L.lib()
+    dev = positions.device
+    st = L.stream_handle(dev)
+    ib, idt = INDEX_BITS, INDEX_DTYPE
+    pos = positions.contiguous().float()
+    mass = masses.contiguous().float()
+    n = int(pos.shape[0])
+    S, off, off_host, leaf_size = lay.num_sets, lay.offsets, lay.offsets_host, lay.leaf_size
     ws = L.workspace(lib.ygx_batch_encode_sort_workspace_size(n), dev)
     bounds = torch.empty((S, 6), dtype=torch.float32, device=dev)
     codes = torch.empty(n, dtype=torch.uint64, device=dev)
@@ -152,13 +194,8 @@ def build_trees_batched(positions: torch.Tensor, masses: torch.Tensor, offsets,
     L.check(lib.ygx_batch_reorder(L.ptr(pos), L.ptr(mass), L.ptr(order), L.ptr(seg_sorted),
                                   L.ptr(off), n, ib, L.ptr(pos_s), L.ptr(mass_s), L.ptr(pidx),
                                   L.ptr(inv), st), "ygx_batch_reorder")
-    leaf_off = torch.empty(S + 1, dtype=torch.int64, device=dev)
-    wsl = L.workspace(lib.ygx_batch_leaf_offsets_workspace_size(S), dev)
-    ltot = np.zeros(1, np.int64)
-    L.check(lib.ygx_batch_leaf_offsets(L.ptr(off), S, int(leaf_size), L.ptr(leaf_off),
-                                       ltot.ctypes.data, L.ptr(wsl), wsl.numel(), st),
-            "ygx_batch_leaf_offsets")
-    Lt = int(ltot[0])
+    leaf_off = lay.leaf_off
+    Lt = lay.total_leaves
     starts = torch.empty(Lt, dtype=idt, device=dev)
     ends = torch.empty(Lt, dtype=idt, device=dev)
     lcodes = torch.empty(Lt, dtype=torch.uint64, device=dev)
@@ -199,7 +236,7 @@ def build_trees_batched(positions: torch.Tensor, masses: torch.Tensor, offsets,
         node_seg32=out["node_seg32"], leaf_seg32=leaf_seg, leafpos32=out["leafpos32"],
         node_base32=out["node_base32"], leaf_base32=out["leaf_base32"],
         seg_flags=out["seg_flags"].view(torch.int32), offsets_host=off_host,
-        leaf_off_host=leaf_off.cpu().numpy())
+        leaf_off_host=lay.leaf_off_host)
 
 
 @dataclass
@@ -391,3 +428,157 @@ def build_interactions_and_neighbors_batched(batch: BatchedTrees, geometry: Batc
         node_offsets=node_offsets, far_counts=far_counts, sources=sources, targets=targets,
         target_levels=target_levels, near_offsets=near_offsets, near_counts=near_counts,
         neighbors=neighbors, stats=s)
+
+
+def _lists_fixed(batch: BatchedTrees, geometry: BatchedGeometry, mac: int, theta: float,
+                 scale: float, sizes: dict):
+    """Batched lists with every size fixed in ``sizes`` (gens, wf, log, far,
+    near capacities): one library call, no host synchronization.  Returns
+    the full-capacity outputs and the workspace holding the statistics."""
+    lib = L.lib()
+    dev = batch.parent.device
+    idt = INDEX_DTYPE
+    total, Lt, S = batch.total_nodes, batch.total_leaves, batch.num_sets
+    ws = L.workspace(lib.ygx_traverse_workspace_size(total, Lt, sizes["wf"], sizes["log"]), dev)
+    e = lambda k, dt=idt: torch.empty(k, dtype=dt, device=dev)  # noqa: E731
+    o = dict(node_offsets=e(total + 1), far_counts=e(total), near_offsets=e(Lt + 1),
+             near_counts=e(Lt), far_src32=e(sizes["far"], torch.int32),
+             near_nbr32=e(sizes["near"], torch.int32), sources=e(sizes["far"]),
+             targets=e(sizes["far"]), target_levels=e(sizes["far"]), neighbors=e(sizes["near"]))
+    L.check(lib.ygx_batch_traverse_lists(
+        L.ptr(geometry.center), L.ptr(geometry.radius), L.ptr(geometry.max_extent),
+        L.ptr(batch.left32), L.ptr(batch.right32), L.ptr(batch.leafpos32), L.ptr(batch.parent32),
+        L.ptr(batch.nbl32), L.ptr(batch.level32), L.ptr(batch.node_base32),
+        L.ptr(batch.leaf_base32), total, L.ptr(batch.leaf_off), S, L.ptr(batch.seg_flags), mac,
+        float(theta), float(scale), int(sizes["gens"]), int(sizes["wf"]), int(sizes["log"]),
+        int(sizes["far"]), int(sizes["near"]), INDEX_BITS,
+        *[L.ptr(o[k]) for k in ("node_offsets", "far_counts", "near_offsets", "near_counts",
+                                "far_src32", "near_nbr32", "sources", "targets",
+                                "target_levels", "neighbors")],
+        L.ptr(ws), ws.numel(), L.stream_handle(dev)), "ygx_batch_traverse_lists")
+    return o, ws
+
+
+class BatchedPipeline:
+    """Build, geometry and exact lists of a batch with a FIXED layout (the
+    same set sizes every call, new positions), captured once in a CUDA graph
+    and replayed.
+
+    The first call runs the ordinary batched functions and records what the
+    walk needed (generations, wavefront / log capacities, list totals); it
+    then allocates every buffer with ``margin`` head-room and captures the
+    whole pipeline -- about 150 kernel launches, no host synchronization --
+    in one graph.  Later calls copy the inputs into the graph's input
+    buffers, replay it and read back one small status block (one host
+    synchronization per call).  If a replay did not fit (the flags say which
+    size), that call's result comes from the ordinary path and the graph is
+    captured again with the new sizes, so results are always the exact
+    lists.
+
+    The returned objects are views of the graph's buffers: the next call
+    overwrites them (copy what must be kept).  ``last_replayed`` tells
+    whether the last call came from the graph."""
+
+    def __init__(self, offsets, *, leaf_size: int = 16, theta: float = 0.5,
+                 mac_type: str = "bh", dehnen_radius_scale: float = 1.0,
+                 margin: float = 1.25, device=None):
+        if mac_type not in _MAC_CODES:
+            raise ValueError(f"Unknown mac_type '{mac_type}'")
+        if float(dehnen_radius_scale) <= 0.0:
+            raise ValueError("dehnen_radius_scale must be > 0")
+        self.device = torch.device(device) if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+        off = np.asarray(offsets.cpu() if torch.is_tensor(offsets) else offsets, dtype=np.int64)
+        self.layout = batch_layout(off, int(off[-1]), leaf_size, self.device)
+        self.theta, self.mac_type = float(theta), mac_type
+        self.scale, self.margin = float(dehnen_radius_scale), float(margin)
+        self.graph = None
+        self.sizes = None
+        self.captures = 0
+        self.last_replayed = False
+
+    # -- the ordinary path, which also measures the sizes ---------------------
+    def _eager(self, positions, masses):
+        bt = _build_on_layout(positions, masses, self.layout)
+        bg = compute_tree_geometry_batched(bt)
+        bi = build_interactions_and_neighbors_batched(
+            bt, bg, theta=self.theta, mac_type=self.mac_type,
+            dehnen_radius_scale=self.scale)
+        st = bi.stats
+        if st:
+            m = self.margin
+            self.sizes = dict(
+                gens=int(st["gens"]) + 4,
+                wf=max(32 * bt.total_nodes + 65536, int(m * st["wf_need"])),
+                log=max(8 * bt.total_nodes + 65536, int(m * st["log_need"])),
+                far=max(1024, int(m * st["far_total"])),
+                near=max(1024, int(m * st["near_total"])))
+        return bt, bg, bi
+
+    def _body(self):
+        bt = _build_on_layout(self.pos, self.mass, self.layout)
+        bg = compute_tree_geometry_batched(bt)
+        o, ws = _lists_fixed(bt, bg, _MAC_CODES[self.mac_type], self.theta, self.scale,
+                             self.sizes)
+        return bt, bg, o, ws
+
+    def _capture(self):
+        lay = self.layout
+        self.pos = torch.empty((lay.num_points, 3), dtype=torch.float32, device=self.device)
+        self.mass = torch.empty(lay.num_points, dtype=torch.float32, device=self.device)
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):  # warm-up off the capture, as CUDA graphs require
+            self._body()
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.out = self._body()
+        self.graph = g
+        self.captures += 1
+
+    def _views(self, stats):
+        bt, bg, o, ws = self.out
+        P, Q = int(stats["far_total"]), int(stats["near_total"])
+        bi = BatchedInteractions(
+            node_offsets=o["node_offsets"], far_counts=o["far_counts"],
+            sources=o["sources"][:P], targets=o["targets"][:P],
+            target_levels=o["target_levels"][:P], near_offsets=o["near_offsets"],
+            near_counts=o["near_counts"], neighbors=o["neighbors"][:Q], stats=stats)
+        return bt, bg, bi
+
+    def __call__(self, positions: torch.Tensor, masses: torch.Tensor):
+        """(BatchedTrees, BatchedGeometry, BatchedInteractions) of this call."""
+        lay = self.layout
+        if tuple(positions.shape) != (lay.num_points, 3) or masses.shape[0] != lay.num_points:
+            raise ValueError("positions / masses do not match the pipeline's layout")
+        if self.graph is None:
+            res = self._eager(positions, masses)
+            self.last_replayed = False
+            if self.sizes is not None:
+                self._capture()
+            return res
+        self.pos.copy_(positions)
+        self.mass.copy_(masses)
+        self.graph.replay()
+        bt = self.out[0]
+        total, Lt = bt.total_nodes, bt.total_leaves
+        stats = np.zeros(L.TSTAT_WORDS, np.uint64)
+        flags = np.zeros(1, np.uint32)
+        ws = self.out[3]
+        L.check(L.lib().ygx_traverse_stats_read(
+            total, Lt, self.sizes["wf"], self.sizes["log"], L.ptr(ws), ws.numel(),
+            stats.ctypes.data, flags.ctypes.data, L.stream_handle(self.device)),
+            "ygx_traverse_stats_read")
+        s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
+        if int(flags[0]) & L.FLAG_BAD_INPUT:
+            raise ValueError("MAC extents must be positive (geometry has zero or NaN extents)")
+        if int(flags[0]):  # a size did not fit: the ordinary path, then re-capture
+            self.graph, self.out = None, None
+            res = self._eager(positions, masses)
+            self._capture()
+            self.last_replayed = False
+            return res
+        self.last_replayed = True
+        return self._views(s)

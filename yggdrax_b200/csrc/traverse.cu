@@ -432,7 +432,9 @@ __global__ void __launch_bounds__(256)
                   unsigned long long* __restrict__ far_pos,
                   unsigned long long* __restrict__ near_pos, unsigned long long far_total,
                   unsigned long long near_total, int32_t* __restrict__ far_src,
-                  int32_t* __restrict__ near_nbr, uint32_t* __restrict__ status) {
+                  int32_t* __restrict__ near_nbr, uint32_t* __restrict__ status,
+                  uint32_t skip_mask) {
+  if (*status & skip_mask) return;  // flagged before the scatter: write nothing
   const int lane = threadIdx.x & 31;
   for (int b = blockIdx.x; b < kWalkGrid; b += gridDim.x) {
     const unsigned long long n = log_cnt[b] < LR ? log_cnt[b] : LR;
@@ -713,6 +715,32 @@ __global__ void k_gather_counts(const int32_t* __restrict__ cnt, const int32_t* 
 
 // node_offsets[nbl[r]] = obl[r]; far_off (int64, node-indexed) the same;
 // counts widened; level_offsets = obl[tree_level_offsets[l]].
+// After a walk of a fixed number of generations (no host probe): flags what
+// the caller's fixed sizes cannot hold -- a wavefront still non-empty after
+// the last generation, directed totals above the output capacities -- and
+// k_zero_counts_if then zeroes every row count, so the offset, scatter and
+// finalize stages that follow write nothing.
+__global__ void k_guard_totals(const uint32_t* __restrict__ sizes, int gens,
+                               const unsigned long long* __restrict__ stats,
+                               unsigned long long far_cap, unsigned long long near_cap,
+                               uint32_t* __restrict__ status) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  if (sizes[gens] != 0) raise_flag(status, kFlagQueueOverflow);
+  if (stats[kStatFarTotal] > far_cap) raise_flag(status, kFlagFarOverflow);
+  if (stats[kStatNearTotal] > near_cap) raise_flag(status, kFlagNearOverflow);
+}
+
+__global__ void k_zero_counts_if(const uint32_t* __restrict__ status, uint32_t mask,
+                                 int32_t* __restrict__ far_cnt, int64_t total,
+                                 int32_t* __restrict__ near_cnt, int64_t L) {
+  if ((*status & mask) == 0) return;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    far_cnt[k] = 0;
+    if (k < L) near_cnt[k] = 0;
+  }
+}
+
 __global__ void k_far_offsets(const int64_t* __restrict__ obl, const int32_t* __restrict__ nbl,
                               const int32_t* __restrict__ cnt, int64_t total, int index_bits,
                               int64_t* __restrict__ far_off, void* node_offsets, void* counts_out,
@@ -1561,7 +1589,7 @@ int ygx_traverse_fill(int64_t total, int64_t num_internal, int64_t wf_capacity,
   ygx::k_log_scatter<<<ygx::kWalkGrid, 256, 0, stream>>>(
       s.log, s.log_cnt, s.log_region, leafpos32, s.far_pos, s.near_pos,
       (unsigned long long)far_total, (unsigned long long)near_total, far_src32, near_nbr32,
-      s.status);
+      s.status, 0u);
   YGX_CHECK_LAUNCH();
   ygx::k_check_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
       s.far_off, s.far_cnt, s.far_pos, total, s.near_off, s.near_cnt, s.near_pos, L, s.status);
@@ -1807,6 +1835,14 @@ int ygx_traverse_fill_predicted(int64_t total, int64_t num_internal, int64_t wf_
 // near_nbr32 are sorted in place for rows longer than 8192.  If
 // neighbor_leaf_positions is non-null it receives the dense (L x max_nbr)
 // leaf-position table.  Does not synchronize.
+static int finalize_impl(const ygx::TravScratch& s, int64_t total, int64_t L,
+                         const int32_t* level32, const int32_t* leafpos32, int index_bits,
+                         int32_t* far_src32, int32_t* near_nbr32, const int64_t* far_raw_off,
+                         const int64_t* near_raw_off, const int32_t* far_row_base,
+                         const int32_t* near_row_base, void* far_sources, void* far_targets,
+                         void* target_levels, void* neighbors, void* neighbor_leaf_positions,
+                         int64_t max_nbr, cudaStream_t stream);
+
 int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capacity,
                           int64_t log_capacity, const int32_t* level32, const int32_t* leafpos32,
                           int index_bits, int32_t* far_src32, int32_t* near_nbr32,
@@ -1821,6 +1857,19 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
   ygx::TravScratch s;
   int rc = trav_setup(s, ws, ws_bytes, total, L, wf_capacity, log_capacity);
   if (rc) return rc;
+  return finalize_impl(s, total, L, level32, leafpos32, index_bits, far_src32, near_nbr32,
+                       far_raw_off, near_raw_off, far_row_base, near_row_base, far_sources,
+                       far_targets, target_levels, neighbors, neighbor_leaf_positions, max_nbr,
+                       stream);
+}
+
+static int finalize_impl(const ygx::TravScratch& s, int64_t total, int64_t L,
+                         const int32_t* level32, const int32_t* leafpos32, int index_bits,
+                         int32_t* far_src32, int32_t* near_nbr32, const int64_t* far_raw_off,
+                         const int64_t* near_raw_off, const int32_t* far_row_base,
+                         const int32_t* near_row_base, void* far_sources, void* far_targets,
+                         void* target_levels, void* neighbors, void* neighbor_leaf_positions,
+                         int64_t max_nbr, cudaStream_t stream) {
   const int grid_small = ygx::kNumSMs * ygx::g_tune.row_grid_per_sm;
   const size_t big_smem = sizeof(int32_t) * ygx::kBlockRowCap;
   static bool big_attr = false;
@@ -1867,6 +1916,110 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
 
 int ygx_traverse_status(const void* ws, uint32_t* flags_out, cudaStream_t stream) {
   return ygx_status_read(ws, flags_out, stream);
+}
+
+// The batched walk, fill and finalize of ygx_batch_traverse_walk +
+// ygx_traverse_fill + ygx_traverse_finalize in one call that never
+// synchronizes or copies to the host, so it can be captured in a CUDA graph
+// and replayed: every size is the caller's -- exactly `gens` walk
+// generations, the wavefront / log capacities, and far_capacity /
+// near_capacity entries in the output lists (far_src32 / sources / targets /
+// target_levels hold far_capacity, near_nbr32 / neighbors near_capacity).
+// A walk that does not fit (wavefront left after the last generation, a
+// wavefront or log region overflow, totals above the capacities) sets its
+// flag in the workspace status word and the lists are left unwritten (all
+// row counts zero); ygx_traverse_stats_read afterwards returns the flags and
+// the statistics (totals, generations, the capacities that would have
+// fitted), from which the caller re-sizes.  Rows are written with node ids
+// local to each set (minus node_base32 / leaf_base32).  No reference
+// counterpart (the reference builds one tree per call and sizes on the
+// host).
+int ygx_batch_traverse_lists(
+    const float* center, const float* radius, const float* max_extent, const int32_t* left32,
+    const int32_t* right32, const int32_t* leafpos32, const int32_t* parent32,
+    const int32_t* nbl32, const int32_t* level32, const int32_t* node_base32,
+    const int32_t* leaf_base32, int64_t total, const int64_t* leaf_off, int64_t S,
+    const uint32_t* seg_flags, int mac, float theta, float dehnen_radius_scale, int gens,
+    int64_t wf_capacity, int64_t log_capacity, int64_t far_capacity, int64_t near_capacity,
+    int index_bits, void* node_offsets, void* far_counts, void* near_offsets, void* near_counts,
+    int32_t* far_src32, int32_t* near_nbr32, void* sources, void* targets, void* target_levels,
+    void* neighbors, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (total < 3 || total > INT32_MAX || S < 1 || !leaf_off || !parent32 || mac < 0 || mac > 2 ||
+      gens < 1 || gens > ygx::kMaxGens || far_capacity < 1 || near_capacity < 1 ||
+      (index_bits != 32 && index_bits != 64) || !far_src32 || !near_nbr32 || !sources ||
+      !targets || !target_levels || !neighbors)
+    return YGX_ERR_ARG;
+  const int64_t Lt = (total + S) / 2, ni = Lt - S;
+  if (ni < 1 || 2 * Lt - S != total) return YGX_ERR_ARG;
+  ygx::TravScratch s;
+  int rc = trav_setup(s, ws, ws_bytes, total, Lt, wf_capacity, log_capacity);
+  if (rc) return rc;
+  const float th = theta;
+  const float theta_sq = th * th;
+  const float theta_r = sqrtf(theta_sq);
+  if (cudaMemsetAsync(s.status, 0, (char*)(s.n_big + 64) - (char*)s.status, stream) != cudaSuccess ||
+      cudaMemsetAsync(s.far_cnt, 0, sizeof(int32_t) * total, stream) != cudaSuccess ||
+      cudaMemsetAsync(s.near_cnt, 0, sizeof(int32_t) * Lt, stream) != cudaSuccess ||
+      cudaMemsetAsync(s.log_cnt, 0, sizeof(unsigned long long) * ygx::kWalkGrid, stream) !=
+          cudaSuccess)
+    return YGX_ERR_CUDA;
+  ygx::k_node_recs<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      center, radius, max_extent, left32, right32, leafpos32, total, mac, dehnen_radius_scale,
+      s.recs, s.status);
+  YGX_CHECK_LAUNCH();
+  int ran = 0;
+  rc = ygx::run_gens(ygx::kWalkLog, mac, s, (int32_t)ni, (int32_t)total, theta_sq, theta_r,
+                     ygx::Roots{0, leaf_off, S, parent32, seg_flags}, (uint32_t)wf_capacity,
+                     ygx::no_sink(), gens, 0, &ran, stream);
+  if (rc) return rc;
+  ygx::k_count_stats<<<ygx::grid_for(total, 256, ygx::kNumSMs * 4), 256, 0, stream>>>(
+      s.far_cnt, total, s.near_cnt, Lt, s.sizes, gens, s.log_cnt, s.stats);
+  YGX_CHECK_LAUNCH();
+  ygx::k_guard_totals<<<1, 32, 0, stream>>>(s.sizes, gens, s.stats,
+                                            (unsigned long long)far_capacity,
+                                            (unsigned long long)near_capacity, s.status);
+  YGX_CHECK_LAUNCH();
+  const uint32_t stop = ygx::kFlagQueueOverflow | ygx::kFlagLogOverflow | ygx::kFlagFarOverflow |
+                        ygx::kFlagNearOverflow | ygx::kFlagBadInput | ygx::kFlagTimeout;
+  ygx::k_zero_counts_if<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.status, stop, s.far_cnt,
+                                                                       total, s.near_cnt, Lt);
+  YGX_CHECK_LAUNCH();
+  rc = ygx::row_offsets(s, total, Lt, nbl32, nullptr, -1, index_bits, node_offsets, far_counts,
+                        nullptr, near_offsets, near_counts, stream);
+  if (rc) return rc;
+  ygx::k_init_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(s.far_off, total, s.far_pos,
+                                                                     s.near_off, Lt, s.near_pos);
+  YGX_CHECK_LAUNCH();
+  ygx::k_log_scatter<<<ygx::kWalkGrid, 256, 0, stream>>>(
+      s.log, s.log_cnt, s.log_region, leafpos32, s.far_pos, s.near_pos,
+      (unsigned long long)far_capacity, (unsigned long long)near_capacity, far_src32, near_nbr32,
+      s.status, stop);
+  YGX_CHECK_LAUNCH();
+  ygx::k_check_cursors<<<ygx::grid_for(total, 256), 256, 0, stream>>>(
+      s.far_off, s.far_cnt, s.far_pos, total, s.near_off, s.near_cnt, s.near_pos, Lt, s.status);
+  YGX_CHECK_LAUNCH();
+  return finalize_impl(s, total, Lt, level32, leafpos32, index_bits, far_src32, near_nbr32,
+                       nullptr, nullptr, node_base32, leaf_base32, sources, targets,
+                       target_levels, neighbors, nullptr, 0, stream);
+}
+
+// Copies the statistics words (YGX_TSTAT_*) and the status flags of a
+// traversal workspace to the host; synchronizes the stream.
+int ygx_traverse_stats_read(int64_t total, int64_t num_leaves, int64_t wf_capacity,
+                            int64_t log_capacity, const void* ws, size_t ws_bytes,
+                            uint64_t* stats_out, uint32_t* flags_out, cudaStream_t stream) {
+  if (!stats_out || !flags_out) return YGX_ERR_ARG;
+  ygx::TravScratch s;
+  int rc = trav_setup(s, const_cast<void*>(ws), ws_bytes, total, num_leaves, wf_capacity,
+                      log_capacity);
+  if (rc) return rc;
+  if (cudaMemcpyAsync(stats_out, s.stats, sizeof(uint64_t) * YGX_TSTAT_WORDS,
+                      cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaMemcpyAsync(flags_out, s.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  return YGX_OK;
 }
 
 }  // extern "C"
