@@ -261,6 +261,8 @@ def main():
     ap.add_argument("--breakdown", action="store_true")
     ap.add_argument("--no-modes", action="store_true",
                     help="skip timing the two-pass and learned traversal schedules")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch shapes (skip the autotuner)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip timing the batched workload (4096 uneven point sets)")
     ap.add_argument("--roofline-only", action="store_true",
@@ -322,6 +324,23 @@ def main():
         out = step(pos_d, mass_d)
     del out
     barrier()
+
+    # launch shapes chosen by the autotuner on this workload (sort knobs on
+    # its Morton codes, the rest on the whole step); untimed
+    tuning = None
+    if not args.no_tune:
+        from yggdrax_b200 import autotune
+
+        tlog: list = []
+        codes = yb.morton_encode(pos_d, yb.infer_bounds(pos_d))
+        chosen = autotune.tune(lambda: step(pos_d, mass_d), dev, codes=codes, log=tlog)
+        del codes
+        tuning = {"chosen": chosen, "measured": len(tlog),
+                  "step_ms_range": [min(r["ms"] for r in tlog if r["stage"] == "step"),
+                                    max(r["ms"] for r in tlog if r["stage"] == "step")],
+                  "sort_ms_range": [min(r["ms"] for r in tlog if r["stage"] == "sort"),
+                                    max(r["ms"] for r in tlog if r["stage"] == "sort")]}
+        barrier()
 
     # -- device-resident timing ------------------------------------------------
     launches0 = lib.ygx_launch_counter()
@@ -394,7 +413,8 @@ def main():
                        "far_entries": far_entries, "near_entries": near_entries,
                        "pairs_per_s": world * (far_entries + near_entries) / t_max,
                        "l2": "inputs (268 MB) larger than L2; no flush between steps",
-                       "traversal_mode": "log", "parallelism": f"replicas{world}"},
+                       "traversal_mode": "log", "parallelism": f"replicas{world}",
+                       "autotune": tuning},
             "e2e": {"value": world * n / te_max, "unit": "particles/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline,
@@ -478,6 +498,11 @@ def batched_timing(dev, steps, barrier, sets: int = 4096, loop_sample: int = 64)
         bt, bi = step()
     del bt, bi
     barrier()
+    from yggdrax_b200 import autotune
+
+    tlog: list = []
+    chosen = autotune.tune(step, dev, log=tlog)
+    barrier()
     l0 = lib.ygx_launch_counter()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
@@ -534,6 +559,7 @@ def batched_timing(dev, steps, barrier, sets: int = 4096, loop_sample: int = 64)
             "value": n / (ms / 1e3), "unit": "particles/s", "far_entries": far,
             "near_entries": near, "pairs_per_s": (far + near) / (ms / 1e3),
             "gpu_launches_per_step": launches,
+            "autotune": {"chosen": chosen, "measured": len(tlog)},
             "cuda_graph": {"ms_per_step": graph_ms, "value": n / (graph_ms / 1e3),
                            "all_steps_replayed": replayed},
             "single_set_loop": {"ms_estimate": loop_ms, "sample_sets": len(pick),
