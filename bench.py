@@ -462,7 +462,7 @@ def mode_timings(step, pos_d, mass_d, n, steps, barrier) -> dict:
             if mode == "learned":
                 rec["predictor"] = {k: LAST_WALK_STATS.get(k) for k in (
                     "over_allocation", "overflow_row_fraction", "overflow_entry_fraction",
-                    "ovf_rows", "padded_far", "padded_near")}
+                    "ovf_rows", "padded_far", "padded_near", "walk_runs")}
             out[mode] = rec
         finally:
             yb.set_traversal_mode("log")

@@ -386,7 +386,10 @@ def build_interactions_and_neighbors_batched(batch: BatchedTrees, geometry: Batc
                 cap = min((1 << 32) - 4097, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
                 log_cap = max(log_cap, int(stats[L.TSTAT["log_need"]]))
             else:
-                log_cap = int(stats[L.TSTAT["log_need"]])
+                # the reported need fits the re-run; head-room spares another
+                # re-run when the next inputs need a little more
+                log_cap = max(int(1.15 * int(stats[L.TSTAT["log_need"]])),
+                              log_cap + log_cap // 4)
             continue
         L.check(rc, "ygx_batch_traverse_walk")
         if f & L.FLAG_BAD_INPUT:
@@ -394,8 +397,9 @@ def build_interactions_and_neighbors_batched(batch: BatchedTrees, geometry: Batc
         if f:
             raise L.YgxError(f"traversal walk reported flags {f:#x}")
         break
-    _CAPACITY_HINTS[key] = (int(stats[L.TSTAT["wf_need"]]) / total,
-                            int(stats[L.TSTAT["log_need"]]) / total)
+    pw, pl = _CAPACITY_HINTS.get(key, (0.0, 0.0))  # hints only grow
+    _CAPACITY_HINTS[key] = (max(pw, int(stats[L.TSTAT["wf_need"]]) / total),
+                            max(pl, int(stats[L.TSTAT["log_need"]]) / total))
     _GENS_HINTS_BATCH[key] = int(stats[L.TSTAT["gens"]])
     s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
     P, Q = s["far_total"], s["near_total"]

@@ -360,9 +360,9 @@ def _learned_walk_fill(topology, d, total, ni, nl, num_levels, center, radius, m
                        leafpos32, theta, mac_type, mac, dehnen_radius_scale, root, wf_capacity,
                        timing, evs):
     """Predicted capacities -> padded offsets -> one walk into the padded rows
-    -> offsets, overflowed rows completed.  Re-runs the (deterministic) walk
-    with the sizes it reports when the wavefront, the overflow log or the
-    extension room was too small."""
+    -> offsets, overflowed rows completed.  Re-runs the walk with the sizes
+    it reports when the wavefront, the overflow log or the extension room was
+    too small."""
     from .predictor import default_predictor
 
     lib = L.lib()
@@ -384,7 +384,9 @@ def _learned_walk_fill(topology, d, total, ni, nl, num_levels, center, radius, m
     h_ovf, h_ext_far, h_ext_near = _LEARNED_HINTS.get(key, (0.0, 0.0, 0.0))
     log_cap = max(65536, int(1.25 * h_ovf * total))
     extra = [int(1.25 * h_ext_far * total), int(1.25 * h_ext_near * total)]
+    runs = 0
     while True:
+        runs += 1
         ws = L.workspace(lib.ygx_traverse_workspace_size(total, nl, cap, log_cap), dev)
         sums = np.zeros(2, np.uint64)
         L.check(lib.ygx_traverse_pad_offsets(total, ni, cap, log_cap, L.ptr(far_cap),
@@ -411,7 +413,10 @@ def _learned_walk_fill(topology, d, total, ni, nl, num_levels, center, radius, m
                 cap = min((1 << 32) - 1, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
                 log_cap = max(log_cap, int(stats[L.TSTAT["log_need"]]))
             else:
-                log_cap = int(stats[L.TSTAT["log_need"]])
+                # the reported need fits the re-run; head-room spares another
+                # re-run when the next inputs need a little more
+                log_cap = max(int(1.15 * int(stats[L.TSTAT["log_need"]])),
+                              log_cap + log_cap // 4)
             del ws, far_raw, near_raw
             continue
         L.check(rc, "ygx_traverse_walk_predicted")
@@ -426,9 +431,12 @@ def _learned_walk_fill(topology, d, total, ni, nl, num_levels, center, radius, m
             continue
         break
     if not wf_capacity:
-        _CAPACITY_HINTS[key] = (int(stats[L.TSTAT["wf_need"]]) / total,
-                                _CAPACITY_HINTS.get(key, (0.0, 0.0))[1])
-        _LEARNED_HINTS[key] = (int(stats[L.TSTAT["log_need"]]) / total,
+        # hints only grow: inputs that alternate between sizes then do not
+        # re-run the walk
+        pw, pl = _CAPACITY_HINTS.get(key, (0.0, 0.0))
+        _CAPACITY_HINTS[key] = (max(pw, int(stats[L.TSTAT["wf_need"]]) / total), pl)
+        po = _LEARNED_HINTS.get(key, (0.0, 0.0, 0.0))
+        _LEARNED_HINTS[key] = (max(po[0], int(stats[L.TSTAT["log_need"]]) / total),
                                int(stats[L.TSTAT["ext_far"]]) / total,
                                int(stats[L.TSTAT["ext_near"]]) / total)
     _GENS_HINTS[key] = int(stats[L.TSTAT["gens"]])
@@ -438,7 +446,7 @@ def _learned_walk_fill(topology, d, total, ni, nl, num_levels, center, radius, m
     LAST_WALK_STATS.clear()
     entries = max(1, s["far_total"] + s["near_total"])
     LAST_WALK_STATS.update(
-        s, wf_capacity=cap, log_capacity=log_cap, mode="learned", padded_far=pf,
+        s, wf_capacity=cap, log_capacity=log_cap, mode="learned", walk_runs=runs, padded_far=pf,
         padded_near=pn, over_allocation=(pf + pn) / entries,
         overflow_row_fraction=s["ovf_rows"] / max(1, total + nl),
         overflow_entry_fraction=s["ovf_entries"] / entries)
@@ -509,7 +517,9 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
         log_cap = (max(8 * total + 65536, int(1.1 * hint_log * total))
                    if walk_mode == L.WALK_LOG else 1)
         cap = min(cap, (1 << 32) - 1)
+        runs = 0
         while True:
+            runs += 1
             ws = L.workspace(lib.ygx_traverse_workspace_size(total, nl, cap, log_cap), dev)
             stats = np.zeros(L.TSTAT_WORDS, np.uint64)
             flags = np.zeros(1, np.uint32)
@@ -528,7 +538,10 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
                     cap = min((1 << 32) - 1, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
                     log_cap = max(log_cap, int(stats[L.TSTAT["log_need"]]))
                 else:
-                    log_cap = int(stats[L.TSTAT["log_need"]])
+                    # the reported need fits the re-run; head-room spares another
+                    # re-run when the next inputs need a little more
+                    log_cap = max(int(1.15 * int(stats[L.TSTAT["log_need"]])),
+                                  log_cap + log_cap // 4)
                 del ws
                 continue
             L.check(rc, "ygx_traverse_walk")
@@ -538,17 +551,19 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
                 raise L.YgxError(f"traversal walk reported flags {f:#x}")
             break
         if not wf_capacity:
+            # hints only grow (inputs that alternate do not re-run the walk)
             prev = _CAPACITY_HINTS.get((mac_type, float(theta)), (0.0, 0.0))
-            log_need = (int(stats[L.TSTAT["log_need"]]) / total
+            log_need = (max(prev[1], int(stats[L.TSTAT["log_need"]]) / total)
                         if walk_mode == L.WALK_LOG else prev[1])
             _CAPACITY_HINTS[(mac_type, float(theta))] = (
-                int(stats[L.TSTAT["wf_need"]]) / total, log_need)
+                max(prev[0], int(stats[L.TSTAT["wf_need"]]) / total), log_need)
         _GENS_HINTS[(mac_type, float(theta))] = int(stats[L.TSTAT["gens"]])
         if timing:
             evs[1].record()
         s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
         LAST_WALK_STATS.clear()
-        LAST_WALK_STATS.update(s, wf_capacity=cap, log_capacity=log_cap, mode=mode)
+        LAST_WALK_STATS.update(s, wf_capacity=cap, log_capacity=log_cap, mode=mode,
+                               walk_runs=runs)
         P, Q = s["far_total"], s["near_total"]
         node_offsets = torch.empty(total + 1, dtype=idt, device=dev)
         far_counts = torch.empty(total, dtype=idt, device=dev)
