@@ -457,6 +457,25 @@ int ygx_traverse_stats_read(int64_t total, int64_t num_leaves, int64_t wf_capaci
 
 int ygx_traverse_status(const void* ws, uint32_t* flags_out, cudaStream_t stream);
 
+/* dual_tree_walk_mutual (yggdrax/_interactions_impl.py:6357-6560): the
+ * symmetric walk that emits every unordered node pair once.  left_full /
+ * right_full: children of all `total` nodes (-1 on leaves) in the index dtype;
+ * centers (total x 3) and radii (total) are the caller's MAC inputs (accept
+ * when theta * |c_b - c_a| > r_a + r_b, strict).  far_a/far_b (far_cap) and
+ * near_a/near_b (near_cap) receive the canonical pairs (a < b) in the
+ * reference's breadth-first emission order, -1 past the end.  counts_out[2]
+ * (host) = far and near pairs the lists would hold (counted past the
+ * capacities); flags_out (host): bit 0 far, bit 1 near, bit 2 wavefront
+ * (max_pair_queue) overflow -- the walk stops after the generation that set
+ * one, like the reference.  Synchronizes once per generation. */
+size_t ygx_mutual_walk_workspace_size(int64_t total, int64_t max_pair_queue);
+int ygx_mutual_walk(const void* left_full, const void* right_full, int index_bits,
+                    const float* centers, const float* radii, int64_t total, float theta,
+                    int64_t root, int64_t max_pair_queue, int64_t far_cap, int64_t near_cap,
+                    void* far_a, void* far_b, void* near_a, void* near_b, int64_t* counts_out,
+                    uint32_t* flags_out, int* gens_out, void* ws, size_t ws_bytes,
+                    cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -549,3 +549,77 @@ def neighbor_leaf_positions(leaf_indices, near_offsets, near_counts, neighbors, 
     safe = np.where(valid, idx, 0)
     pos = lookup[neighbors[safe]] if neighbors.size else np.zeros_like(safe)
     return np.where(valid, pos, -1)
+
+
+def dual_tree_walk_mutual(left_full, right_full, centers, radii, theta, root, *,
+                          max_pair_queue: int, far_cap: int, near_cap: int) -> dict:
+    """Restatement of ``dual_tree_walk_mutual`` (_interactions_impl.py:6357-6560)
+    in NumPy, generation by generation: fp32 MAC ``theta^2 * d^2 > (r_a +
+    r_b)^2`` with ``d`` = centers[b] - centers[a] summed in written order
+    (:6480-6486), accept / near / refine (:6487-6494), ``_flat_append``
+    (:6339-6354) for the far and near lists, split rule (:6503-6506),
+    children in ``_count_refine_pairs_single`` order (:174-221) canonicalised
+    and compacted in wavefront order (:6524-6545)."""
+    left = np.asarray(left_full, np.int64)
+    right = np.asarray(right_full, np.int64)
+    c = np.asarray(centers, np.float32)
+    r = np.asarray(radii, np.float32)
+    theta_sq = np.float32(theta) * np.float32(theta)
+    Q = int(max_pair_queue)
+    cur_a = np.array([int(root)], np.int64)
+    cur_b = np.array([int(root)], np.int64)
+    far = [np.full(far_cap, -1, np.int64), np.full(far_cap, -1, np.int64)]
+    near = [np.full(near_cap, -1, np.int64), np.full(near_cap, -1, np.int64)]
+    far_n = near_n = 0
+    fo = no = qo = False
+
+    def append(buf, n, cap, mask, a, b):
+        k = np.nonzero(mask)[0]
+        slots = n + np.arange(k.shape[0])
+        ok = slots < cap
+        buf[0][slots[ok]] = a[k[ok]]
+        buf[1][slots[ok]] = b[k[ok]]
+        return n + k.shape[0], bool((~ok).any())
+
+    while cur_a.shape[0] > 0 and not (fo or no or qo):
+        sa, sb = cur_a, cur_b
+        a_leaf, b_leaf = left[sa] < 0, left[sb] < 0
+        same = sa == sb
+        d = c[sb] - c[sa]
+        d2 = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+        ra, rb = r[sa], r[sb]
+        rs = ra + rb
+        accept = ~same & (theta_sq * d2 > rs * rs)
+        both_leaf = a_leaf & b_leaf
+        is_near = ~accept & both_leaf & ~same
+        refine = ~accept & ~both_leaf
+        far_n, f1 = append(far, far_n, far_cap, accept, sa, sb)
+        near_n, n1 = append(near, near_n, near_cap, is_near, sa, sb)
+        fo, no = fo or f1, no or n1
+        split_a = refine & ~a_leaf & (same | b_leaf | (ra >= rb))
+        split_b = refine & ~b_leaf & (same | a_leaf | (rb > ra))
+        both = split_a & split_b
+        only_a = split_a & ~both
+        only_b = split_b & ~both
+        al, ar, bl, br = left[sa], right[sa], left[sb], right[sb]
+        ca = np.full((sa.shape[0], 4), -1, np.int64)
+        cb = np.full((sa.shape[0], 4), -1, np.int64)
+        m = only_b
+        ca[m, 0], cb[m, 0], ca[m, 1], cb[m, 1] = sa[m], bl[m], sa[m], br[m]
+        m = only_a
+        ca[m, 0], cb[m, 0], ca[m, 1], cb[m, 1] = al[m], sb[m], ar[m], sb[m]
+        m = both & ~same
+        ca[m, 0], cb[m, 0], ca[m, 1], cb[m, 1] = al[m], bl[m], al[m], br[m]
+        ca[m, 2], cb[m, 2], ca[m, 3], cb[m, 3] = ar[m], bl[m], ar[m], br[m]
+        m = both & same
+        ca[m, 0], cb[m, 0], ca[m, 1], cb[m, 1] = al[m], al[m], al[m], ar[m]
+        ca[m, 2], cb[m, 2] = ar[m], ar[m]
+        pa, pb = ca.reshape(-1), cb.reshape(-1)
+        valid = (pa >= 0) & (pb >= 0)
+        pa, pb = pa[valid], pb[valid]
+        if pa.shape[0] > Q:
+            qo = True
+            pa, pb = pa[:Q], pb[:Q]
+        cur_a, cur_b = np.minimum(pa, pb), np.maximum(pa, pb)
+    return dict(far_a=far[0], far_b=far[1], far_count=far_n, near_a=near[0], near_b=near[1],
+                near_count=near_n, far_overflow=fo, near_overflow=no, queue_overflow=qo)

@@ -8,7 +8,7 @@ to this script and are what ``tests/test_golden.py`` checks the oracle
 against.  Within-row order of the interaction / neighbour lists is
 unspecified in the reference (unstable argsort), so rows are stored sorted.
 
-Usage: python tests/golden/make_golden.py [reference_package_dir]
+Usage: python tests/golden/make_golden.py [reference_package_dir] [--mutual-only]
 """
 
 from __future__ import annotations
@@ -56,6 +56,44 @@ def _inputs():
     col = np.array([[float(i), 0.0, 0.0] for i in range(128)], np.float32)
     dup = np.zeros((16, 3), np.float32)
     return dict(uniform300=uni, plummer400=plum, clumps600=clumps, collinear128=col, dup16=dup)
+
+
+def mutual(root: str) -> None:
+    """dual_tree_walk_mutual (the canonical-pair emitter) on the reference's
+    own trees and geometry: left / right children padded to all nodes with -1
+    on leaves, bounding-sphere centres and radii as the MAC inputs, and
+    capacities that fit as well as ones that overflow each buffer."""
+    m = jaxshim.load_reference(root)
+    jnp = sys.modules["jax.numpy"]
+    ti, gi, ii, bd = m["_tree_impl"], m["_geometry_impl"], m["_interactions_impl"], m["bounds"]
+    inputs = _inputs()
+    for name, leaf in (("uniform300", 4), ("plummer400", 8), ("clumps600", 2)):
+        pos = inputs[name]
+        mass = np.linspace(0.5, 1.5, pos.shape[0]).astype(np.float32)
+        p, ms = jnp.asarray(pos), jnp.asarray(mass)
+        b = bd.infer_bounds(p)
+        t, ps, _, _ = ti.build_tree(p, ms, b, leaf_size=leaf, return_reordered=True)
+        g = gi.compute_tree_geometry(t, ps, max_leaf_size=leaf)
+        total = int(np.asarray(t.parent).shape[0])
+        ni = int(t.num_internal_nodes)
+        lf = np.full(total, -1, np.int64)
+        rt = np.full(total, -1, np.int64)
+        lf[:ni] = np.asarray(t.left_child)
+        rt[:ni] = np.asarray(t.right_child)
+        out = dict(left=lf, right=rt, centers=np.asarray(g.center), radii=np.asarray(g.radius))
+        q = 4096
+        runs = [("fit", 0.6, q, 1 << 16, 1 << 16), ("fit_t4", 0.4, q, 1 << 16, 1 << 16),
+                ("far_over", 0.6, q, 50, 1 << 16), ("near_over", 0.6, q, 1 << 16, 40),
+                ("queue_over", 0.6, 24, 1 << 16, 1 << 16)]
+        for tag, theta, q, fc, nc in runs:
+            r = ii.dual_tree_walk_mutual(jnp.asarray(lf), jnp.asarray(rt), jnp.asarray(g.center),
+                                         jnp.asarray(g.radius), theta, jnp.asarray(0),
+                                         max_pair_queue=q, far_cap=fc, near_cap=nc)
+            out[f"{tag}_params"] = np.array([theta, q, fc, nc], np.float64)
+            for f in r._fields:
+                out[f"{tag}_{f}"] = np.asarray(getattr(r, f))
+        np.savez_compressed(os.path.join(HERE, f"mutual_{name}_leaf{leaf}.npz"), **out)
+        print("wrote", f"mutual_{name}_leaf{leaf}")
 
 
 def main(root: str) -> None:
@@ -183,4 +221,10 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/yggdrax")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref = args[0] if args else "/root/reference/yggdrax"
+    if "--mutual-only" in sys.argv:
+        mutual(ref)
+    else:
+        main(ref)
+        mutual(ref)

@@ -352,3 +352,40 @@ def test_traversal_modes_give_identical_lists(cuda_device, oracle, mode):
     og = oracle.compute_tree_geometry(ot, ot.positions_sorted)
     r = oracle.build_interactions_and_neighbors(ot, og, theta=0.5, mac_type="bh")
     _compare_lists(gi, gn, r)
+
+
+def test_compact_far_pairs_and_leaf_neighbors(cuda_device, oracle):
+    """build_compact_far_pairs / build_leaf_neighbor_lists /
+    build_compact_far_pairs_and_leaf_neighbor_lists: the oracle's far rows in
+    node order (targets = the row's node, tags -1) and its near lists; the
+    fixed-capacity form pads with -1 and raises above the capacity."""
+    import yggdrax_b200 as yb
+
+    pos, mass = CASES["uniform65k"]
+    P, M = _to_dev(pos, cuda_device), _to_dev(mass, cuda_device)
+    t, ps = yb.build_tree(P, M, leaf_size=16, return_reordered=True)[:2]
+    g = yb.compute_tree_geometry(t, ps)
+    ot = oracle.build_tree(pos, mass, leaf_size=16)
+    og = oracle.compute_tree_geometry(ot, ot.positions_sorted)
+    r = oracle.build_interactions_and_neighbors(ot, og, theta=0.6, mac_type="dehnen")
+    off, cnt = np.asarray(r["offsets"]), np.asarray(r["far_counts"])
+    src = np.concatenate([np.asarray(r["sources"])[off[k]:off[k] + cnt[k]]
+                          for k in range(cnt.shape[0])])
+    tgt = np.repeat(np.arange(cnt.shape[0]), cnt)
+    cf = yb.build_compact_far_pairs(t, g, theta=0.6, mac_type="dehnen")
+    _assert_eq("compact.sources", _np(cf.sources), src)
+    _assert_eq("compact.targets", _np(cf.targets), tgt)
+    assert int(cf.far_pair_count) == src.shape[0] and bool((_np(cf.tags) == -1).all())
+    nb = yb.build_leaf_neighbor_lists(t, g, theta=0.6, mac_type="dehnen")
+    _assert_eq("leaf_nbrs.neighbors", _np(nb.neighbors), r["neighbors"])
+    _assert_eq("leaf_nbrs.offsets", _np(nb.offsets), r["near_offsets"])
+    cap = src.shape[0] + 100
+    cf2, nb2 = yb.build_compact_far_pairs_and_leaf_neighbor_lists(
+        t, g, theta=0.6, mac_type="dehnen", compact_far_pair_capacity=cap)
+    s2 = _np(cf2.sources)
+    assert s2.shape[0] == cap and (s2[src.shape[0]:] == -1).all()
+    _assert_eq("fused.sources", s2[:src.shape[0]], src)
+    _assert_eq("fused.neighbors", _np(nb2.neighbors), r["neighbors"])
+    with pytest.raises(RuntimeError, match="compact far-pair cap exceeded"):
+        yb.build_compact_far_pairs_and_leaf_neighbor_lists(
+            t, g, theta=0.6, mac_type="dehnen", compact_far_pair_capacity=src.shape[0] - 1)

@@ -17,12 +17,16 @@ from .interactions import (
     MACType,
     NodeInteractionList,
     NodeNeighborList,
+    build_compact_far_pairs,
+    build_compact_far_pairs_and_leaf_neighbor_lists,
     build_interactions_and_neighbors,
+    build_leaf_neighbor_lists,
     set_default_dual_tree_config,
     set_dense_neighbor_budget,
     set_reference_limits,
     set_traversal_mode,
 )
+from .mutual import MutualWalkResult, dual_tree_walk_mutual
 from .morton import (
     encode_and_sort,
     get_common_prefix_length,

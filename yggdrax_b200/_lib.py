@@ -112,6 +112,9 @@ _SIGS = {
     "ygx_batch_build_topology": (I32, [P, P, P, P, P, I64, I64, I32] + [P] * 22 + [SZ, P]),
     "ygx_batch_tree_geometry": (I32, [P, I64, I64, P, P, I64, P, I32, P, P, P, P, P, P, I64, P, P,
                                       P, P, P, SZ, P]),
+    "ygx_mutual_walk_workspace_size": (SZ, [I64, I64]),
+    "ygx_mutual_walk": (I32, [P, P, I32, P, P, I64, F32, I64, I64, I64, I64, P, P, P, P, P, P, P,
+                              P, SZ, P]),
     "ygx_batch_traverse_lists": (I32, [P] * 11 + [I64, P, I64, P, I32, F32, F32, I32, I64, I64,
                                                I64, I64, I32] + [P] * 11 + [SZ, P]),
     "ygx_traverse_stats_read": (I32, [I64, I64, I64, I64, P, SZ, P, P, P]),

@@ -633,12 +633,38 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
                     stats=s, num_levels=num_levels)
 
 
+def _node_order_far_pairs(w, total: int, dev):
+    """The far lists in the count-then-fill layout: rows in node order
+    (``interaction_offsets``), each row's sources ascending; targets are the
+    row's node; tags -1 (no pair policy).  (_raw_to_compact_far_pairs,
+    :5340-5390, reads the same arrays.)"""
+    idt = INDEX_DTYPE
+    counts = w.far_counts.to(torch.int64)
+    no = torch.zeros(total + 1, dtype=torch.int64, device=dev)
+    no[1:] = torch.cumsum(counts, 0)
+    P = int(w.sources.shape[0])
+    node = torch.repeat_interleave(torch.arange(total, device=dev), counts)
+    within = torch.arange(P, device=dev) - no[node]
+    src_pos = w.node_offsets.to(torch.int64)[node] + within
+    raw_src = w.sources[src_pos] if P else w.sources
+    raw_tgt = node.to(idt)
+    tags = torch.full((P,), -1, dtype=idt, device=dev)
+    fpc = torch.tensor(P, dtype=idt, device=dev)
+    return no.to(idt), raw_src, raw_tgt, tags, fpc
+
+
 def _check_capacities(w: _WalkOut, total: int, ni: int, *, max_interactions_per_node,
                       max_neighbors_per_leaf, max_pair_queue, process_block,
-                      traversal_config) -> None:
+                      traversal_config, collect_far: bool = True,
+                      collect_near: bool = True) -> None:
     """Raise where the reference's runner (_run_dual_tree_walk_raw,
-    :3840-4440) would raise on the same pair sets."""
-    s = w.stats
+    :3840-4440) would raise on the same pair sets (a far-only or near-only
+    run checks only the lists it collects)."""
+    s = dict(w.stats)
+    if not collect_far:
+        s["max_far"] = s["far_total"] = 0
+    if not collect_near:
+        s["max_near"] = s["near_total"] = 0
     nl = total - ni
     use_count_pass = (max_interactions_per_node is None and max_pair_queue is None
                       and traversal_config is None)
@@ -754,23 +780,12 @@ def build_interactions_and_neighbors(
         target_block_offsets=tb[3], target_block_size=int(tb[4]))
     out = [interactions, neighbors]
     if return_result or return_compact_far_pairs:
-        # Exact count-then-fill layout: rows in node order.
+        no, raw_src, raw_tgt, tags, fpc = _node_order_far_pairs(w, total, dev)
         idt = INDEX_DTYPE
-        counts = w.far_counts.to(torch.int64)
-        no = torch.zeros(total + 1, dtype=torch.int64, device=dev)
-        no[1:] = torch.cumsum(counts, 0)
-        P = int(w.sources.shape[0])
-        node = torch.repeat_interleave(torch.arange(total, device=dev), counts)
-        within = torch.arange(P, device=dev) - no[node]
-        src_pos = w.node_offsets.to(torch.int64)[node] + within
-        raw_src = w.sources[src_pos] if P else w.sources
-        raw_tgt = node.to(idt)
-        tags = torch.full((P,), -1, dtype=idt, device=dev)
-        fpc = torch.tensor(P, dtype=idt, device=dev)
         if return_result:
             s = w.stats
             out.append(DualTreeWalkResult(
-                interaction_offsets=no.to(idt), interaction_sources=raw_src,
+                interaction_offsets=no, interaction_sources=raw_src,
                 interaction_targets=raw_tgt, interaction_tags=tags,
                 interaction_counts=w.far_counts, neighbor_offsets=w.near_offsets,
                 neighbor_indices=w.neighbors, neighbor_counts=w.near_counts,
@@ -788,9 +803,136 @@ def build_interactions_and_neighbors(
     return tuple(out)
 
 
+def _walk_checked(tree, geometry, theta, mac_type, dehnen_radius_scale, pair_policy,
+                  process_block, checks: dict, collect_far: bool, collect_near: bool):
+    topology = resolve_tree_topology(tree)
+    if mac_type not in _MAC_CODES:
+        raise ValueError(f"Unknown mac_type: {mac_type}")
+    if float(dehnen_radius_scale) <= 0.0:
+        raise ValueError("dehnen_radius_scale must be > 0")
+    if pair_policy is not None:
+        raise NotImplementedError("pair_policy is outside the GPU traversal (default MAC only)")
+    if process_block is not None and process_block < 1:
+        raise ValueError("process_block must be >= 1")
+    total = int(topology.parent.shape[0])
+    ni = int(topology.left_child.shape[0])
+    w = _run_walk(topology, geometry, theta, mac_type, dehnen_radius_scale)
+    if _REFERENCE_LIMITS:
+        _check_capacities(w, total, ni, process_block=process_block, collect_far=collect_far,
+                          collect_near=collect_near, **checks)
+    return topology, w, total, ni
+
+
+def _neighbor_list(w, total: int, ni: int, dev) -> NodeNeighborList:
+    nl = total - ni
+    tb = _target_blocks(w.near_counts, w.near_offsets, w.neighbor_leaf_positions, nl, dev)
+    return NodeNeighborList(
+        offsets=w.near_offsets, neighbors=w.neighbors, leaf_indices=w.leaf_indices,
+        counts=w.near_counts, particle_order_leaf_indices=w.particle_order_leaf_indices,
+        particle_order_to_native_leaf=w.particle_order_to_native_leaf,
+        neighbor_leaf_positions=w.neighbor_leaf_positions, target_block_leaf_ids=tb[0],
+        target_block_source_leaf_ids=tb[1], target_block_valid_mask=tb[2],
+        target_block_offsets=tb[3], target_block_size=int(tb[4]))
+
+
+def build_compact_far_pairs(tree, geometry, theta: float = 0.5,
+                            max_interactions_per_node: Optional[int] = None,
+                            mac_type: MACType = "bh", *, pair_policy=None,
+                            policy_state: object = None, max_pair_queue: Optional[int] = None,
+                            process_block: Optional[int] = None,
+                            traversal_config: Optional[DualTreeTraversalConfig] = None,
+                            retry_logger=None,
+                            dehnen_radius_scale: float = 1.0) -> CompactTaggedFarPairs:
+    """Exact-length far pairs (build_compact_far_pairs,
+    _interactions_impl.py:5765-5816; public wrapper interactions.py:110-175):
+    ``sources`` / ``targets`` / ``tags`` of every directed far entry, rows in
+    node order with ascending sources, tags -1, ``far_pair_count`` their
+    number.  Same walk as build_interactions_and_neighbors."""
+    del retry_logger, policy_state
+    topology, w, total, ni = _walk_checked(
+        tree, geometry, theta, mac_type, dehnen_radius_scale, pair_policy, process_block,
+        dict(max_interactions_per_node=max_interactions_per_node,
+             max_neighbors_per_leaf=_DEFAULT_MAX_NEIGHBORS, max_pair_queue=max_pair_queue,
+             traversal_config=traversal_config), True, False)
+    _, src, tgt, tags, fpc = _node_order_far_pairs(w, total, topology.parent.device)
+    return CompactTaggedFarPairs(sources=src, targets=tgt, tags=tags, far_pair_count=fpc)
+
+
+def build_leaf_neighbor_lists(tree, geometry, theta: float = 0.5,
+                              max_neighbors_per_leaf: int = _DEFAULT_MAX_NEIGHBORS,
+                              max_interactions_per_node: Optional[int] = None,
+                              mac_type: MACType = "bh", *, pair_policy=None,
+                              policy_state: object = None,
+                              max_pair_queue: Optional[int] = None,
+                              process_block: Optional[int] = None,
+                              traversal_config: Optional[DualTreeTraversalConfig] = None,
+                              retry_logger=None,
+                              dehnen_radius_scale: float = 1.0) -> NodeNeighborList:
+    """Near-field neighbour lists of the leaves alone (build_leaf_neighbor_lists,
+    _interactions_impl.py:5917-5990): the NodeNeighborList that
+    build_interactions_and_neighbors returns."""
+    del retry_logger, policy_state
+    topology, w, total, ni = _walk_checked(
+        tree, geometry, theta, mac_type, dehnen_radius_scale, pair_policy, process_block,
+        dict(max_interactions_per_node=max_interactions_per_node,
+             max_neighbors_per_leaf=max_neighbors_per_leaf, max_pair_queue=max_pair_queue,
+             traversal_config=traversal_config), False, True)
+    return _neighbor_list(w, total, ni, topology.parent.device)
+
+
+def build_compact_far_pairs_and_leaf_neighbor_lists(
+        tree, geometry, theta: float = 0.5,
+        max_neighbors_per_leaf: int = _DEFAULT_MAX_NEIGHBORS,
+        max_interactions_per_node: Optional[int] = None, mac_type: MACType = "bh", *,
+        pair_policy=None, policy_state: object = None, max_pair_queue: Optional[int] = None,
+        process_block: Optional[int] = None,
+        traversal_config: Optional[DualTreeTraversalConfig] = None, retry_logger=None,
+        dehnen_radius_scale: float = 1.0, timing_callback=None,
+        compact_far_pair_capacity: Optional[int] = None):
+    """``(CompactTaggedFarPairs, NodeNeighborList)`` from one walk
+    (_interactions_impl.py:5819-5914; public wrapper interactions.py:180-260).
+    With ``compact_far_pair_capacity`` the far arrays are padded with -1 to
+    that length, and a larger pair count raises the reference's RuntimeError
+    (_raw_to_compact_far_pairs, :5340-5360).  ``timing_callback(stage,
+    seconds)`` receives the wall time of the whole call."""
+    import time
+
+    del retry_logger, policy_state
+    t0 = time.perf_counter()
+    topology, w, total, ni = _walk_checked(
+        tree, geometry, theta, mac_type, dehnen_radius_scale, pair_policy, process_block,
+        dict(max_interactions_per_node=max_interactions_per_node,
+             max_neighbors_per_leaf=max_neighbors_per_leaf, max_pair_queue=max_pair_queue,
+             traversal_config=traversal_config), True, True)
+    dev = topology.parent.device
+    _, src, tgt, tags, fpc = _node_order_far_pairs(w, total, dev)
+    if compact_far_pair_capacity is not None:
+        cap = int(compact_far_pair_capacity)
+        P = int(src.shape[0])
+        if P > cap:
+            raise RuntimeError(
+                "strict fused compact far-pair cap exceeded: "
+                f"cap={cap}. Increase JACCPOT_STATIC_STRICT_FUSED_COMPACT_FAR_PAIR_CAP.")
+
+        def pad(x):
+            out = torch.full((cap,), -1, dtype=x.dtype, device=dev)
+            out[:P] = x
+            return out
+
+        src, tgt, tags = pad(src), pad(tgt), pad(tags)
+    far = CompactTaggedFarPairs(sources=src, targets=tgt, tags=tags, far_pair_count=fpc)
+    near = _neighbor_list(w, total, ni, dev)
+    if timing_callback is not None:
+        torch.cuda.synchronize(dev)
+        timing_callback("compact_far_pairs_and_leaf_neighbors", time.perf_counter() - t0)
+    return far, near
+
+
 __all__ = [
     "MACType", "DualTreeTraversalConfig", "DualTreeRetryEvent", "DualTreeWalkResult",
     "NodeInteractionList", "NodeNeighborList", "CompactTaggedFarPairs",
     "build_interactions_and_neighbors", "set_default_dual_tree_config",
+    "build_compact_far_pairs", "build_leaf_neighbor_lists",
+    "build_compact_far_pairs_and_leaf_neighbor_lists",
     "set_dense_neighbor_budget", "set_reference_limits",
 ]
