@@ -457,6 +457,41 @@ int ygx_traverse_stats_read(int64_t total, int64_t num_leaves, int64_t wf_capaci
 
 int ygx_traverse_status(const void* ws, uint32_t* flags_out, cudaStream_t stream);
 
+/* geometry_to_level_major (yggdrax/_geometry_impl.py:342-420): row l of the
+ * (num_levels x max_nodes) outputs holds level l's nodes in nodes_by_level
+ * order (nbl32), zero / -1 past the level's count. */
+int ygx_level_major_geometry(const int32_t* nbl32, const void* level_offsets, int index_bits,
+                             int num_levels, int64_t max_nodes, const float* center,
+                             const float* half_extent, const float* radius,
+                             const float* max_extent, float* o_center, float* o_half,
+                             float* o_radius, float* o_max, void* o_nodes, cudaStream_t stream);
+
+/* _dense_m2l_buffers (yggdrax/dense_interactions.py:34-146): for each of
+ * `slots` level-major slots (node_idx, -1 = empty) and k < max_interactions:
+ * the k-th source of the node's far row (-1 past its count), the mask, the
+ * count per slot and the displacement centre[node] - centre[source]. */
+int ygx_dense_m2l(const void* node_idx, int index_bits, int64_t slots, int64_t max_interactions,
+                  const void* counts, const void* offsets, const void* sources,
+                  const float* center, int64_t total, void* o_src, bool* o_mask, void* o_counts,
+                  float* o_disp, cudaStream_t stream);
+
+/* build_grouped_interactions_from_pairs (yggdrax/grouped_interactions.py:
+ * 75-200) in two calls on one workspace: ygx_grouped_classes computes every
+ * pair's class key (target level, source level, rint in float64 of the
+ * displacement over the target level's cell, root_extent a host double[3]),
+ * sorts the pairs stably by key and returns the number of classes (host);
+ * ygx_grouped_emit then writes the class keys / displacements / offsets, the
+ * pairs in class order and each input pair's class id.  Synchronizes. */
+size_t ygx_grouped_workspace_size(int64_t num_pairs);
+int ygx_grouped_classes(const void* sources, const void* targets, int index_bits,
+                        int64_t num_pairs, const int32_t* level32, const float* center,
+                        const double* root_extent, int64_t* num_classes_out, void* ws,
+                        size_t ws_bytes, cudaStream_t stream);
+int ygx_grouped_emit(const void* sources, const void* targets, int index_bits, int64_t num_pairs,
+                     const double* root_extent, int32_t* class_keys, float* class_disp,
+                     void* class_offsets, void* class_sources, void* class_targets,
+                     void* class_ids, void* ws, size_t ws_bytes, cudaStream_t stream);
+
 /* dual_tree_walk_mutual (yggdrax/_interactions_impl.py:6357-6560): the
  * symmetric walk that emits every unordered node pair once.  left_full /
  * right_full: children of all `total` nodes (-1 on leaves) in the index dtype;

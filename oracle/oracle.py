@@ -623,3 +623,89 @@ def dual_tree_walk_mutual(left_full, right_full, centers, radii, theta, root, *,
         cur_a, cur_b = np.minimum(pa, pb), np.maximum(pa, pb)
     return dict(far_a=far[0], far_b=far[1], far_count=far_n, near_a=near[0], near_b=near[1],
                 near_count=near_n, far_overflow=fo, near_overflow=no, queue_overflow=qo)
+
+
+def level_major_geometry(nodes_by_level, level_offsets, num_levels: int, center, half_extent,
+                         radius, max_extent) -> dict:
+    """geometry_to_level_major (_geometry_impl.py:342-420): (num_levels,
+    max_nodes) buffers, row l = level l's nodes in nodes_by_level order, zero
+    (node index -1) past the level's count; max_nodes = max(counts, 1)."""
+    lo = np.asarray(level_offsets, np.int64)
+    nbl = np.asarray(nodes_by_level, np.int64)
+    counts = (lo[1:] - lo[:-1])[:num_levels]
+    M = int(np.maximum(counts, 1).max())
+    idx = np.full((num_levels, M), -1, np.int64)
+    for lv in range(num_levels):
+        idx[lv, :counts[lv]] = nbl[lo[lv]:lo[lv] + counts[lv]]
+    ok = idx >= 0
+    safe = np.where(ok, idx, 0)
+
+    def take(a, zero_shape):
+        v = np.asarray(a)[safe]
+        return np.where(ok.reshape(ok.shape + (1,) * (v.ndim - 2)), v, 0).astype(np.float32)
+
+    return dict(centers=take(center, 3), half_extents=take(half_extent, 3),
+                radii=take(radius, 0), max_extents=take(max_extent, 0), level_counts=counts,
+                node_indices=idx)
+
+
+def dense_m2l(node_indices, counts, offsets, sources, center) -> dict:
+    """_dense_m2l_buffers (dense_interactions.py:34-146): slot (l, m) of node
+    n gets its far row's sources (-1 past the count), the mask, the count and
+    centre[n] - centre[source] in fp32 (zero where masked)."""
+    idx = np.asarray(node_indices, np.int64)
+    cnt = np.asarray(counts, np.int64)
+    off = np.asarray(offsets, np.int64)
+    srcs = np.asarray(sources, np.int64)
+    if srcs.size == 0:
+        srcs = np.zeros(1, np.int64)
+    c = np.asarray(center, np.float32)
+    K = max(1, int(cnt.max()) if cnt.size else 0)
+    live = idx >= 0
+    n = np.where(live, idx, 0)
+    slot_cnt = np.where(live, cnt[n], 0)
+    k = np.arange(K)[None, None, :]
+    valid = k < slot_cnt[..., None]
+    row = np.where(valid, srcs[np.where(valid, off[n][..., None] + k, 0)], -1)
+    safe = np.clip(row, 0, c.shape[0] - 1)
+    disp = c[n][:, :, None, :] - c[safe]
+    disp = np.where(valid[..., None], disp, np.float32(0)).astype(np.float32)
+    return dict(m2l_sources=row, m2l_mask=valid, m2l_counts=slot_cnt, m2l_displacements=disp)
+
+
+def grouped_from_pairs(sources, targets, node_level, center, bounds_min, bounds_max) -> dict:
+    """build_grouped_interactions_from_pairs (grouped_interactions.py:75-200):
+    float64 displacement indices rint((c_t - c_s) / max(extent / max(2^lt, 1),
+    1e-12)), keys (lt, ls, dx, dy, dz) ordered stably, classes = runs of equal
+    keys, class displacement key * cell in float64 cast to float32; class
+    ids as the reference's searchsorted gives them (see below)."""
+    src = np.asarray(sources, np.int64)
+    tgt = np.asarray(targets, np.int64)
+    c = np.asarray(center, np.float64)
+    lev = np.asarray(node_level, np.int32)
+    ext = np.asarray(bounds_max, np.float64) - np.asarray(bounds_min, np.float64)
+
+    def cell(level):
+        denom = np.power(2.0, level.astype(np.float64))[:, None]
+        return np.maximum(ext[None, :] / np.maximum(denom, 1.0), 1e-12)
+
+    tl, sl = lev[tgt], lev[src]
+    disp = np.rint((c[tgt] - c[src]) / cell(tl)).astype(np.int32)
+    keys = np.stack([tl, sl, disp[:, 0], disp[:, 1], disp[:, 2]], 1).astype(np.int32)
+    order = np.lexsort((keys[:, 4], keys[:, 3], keys[:, 2], keys[:, 1], keys[:, 0]))
+    ks = keys[order]
+    head = np.ones(ks.shape[0], bool)
+    head[1:] = (ks[1:] != ks[:-1]).any(1)
+    starts = np.nonzero(head)[0]
+    # np.searchsorted(class_starts, arange(n)) with side="left" (:163): a pair
+    # that is not the first of its class gets the NEXT class's id -- a quirk
+    # of the reference, reproduced
+    incl = np.cumsum(head)
+    ids_sorted = np.where(head, incl - 1, incl)
+    ids = np.empty_like(ids_sorted)
+    ids[order] = ids_sorted
+    ck = ks[starts]
+    cdisp = (ck[:, 2:5].astype(np.float64) * cell(ck[:, 0])).astype(np.float32)
+    return dict(class_keys=ck, class_displacements=cdisp,
+                class_offsets=np.concatenate([starts, [ks.shape[0]]]).astype(np.int64),
+                class_sources=src[order], class_targets=tgt[order], class_ids=ids.astype(np.int64))

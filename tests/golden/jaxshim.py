@@ -393,6 +393,14 @@ def _mk_lax():
             ys.append(y)
         return carry, ys
 
+    def dynamic_index_in_dim(operand, index, axis=0, keepdims=True):
+        # JAX clamps a dynamic index into range
+        a = np.asarray(operand)
+        i = int(min(max(int(np.asarray(index)), 0), a.shape[axis] - 1))
+        out = np.take(a, [i] if keepdims else i, axis=axis)
+        return _wrap(out)
+
+    lax.dynamic_index_in_dim = dynamic_index_in_dim
     lax.fori_loop = fori_loop
     lax.while_loop = while_loop
     lax.cond = cond

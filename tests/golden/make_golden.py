@@ -8,7 +8,7 @@ to this script and are what ``tests/test_golden.py`` checks the oracle
 against.  Within-row order of the interaction / neighbour lists is
 unspecified in the reference (unstable argsort), so rows are stored sorted.
 
-Usage: python tests/golden/make_golden.py [reference_package_dir] [--mutual-only]
+Usage: python tests/golden/make_golden.py [reference_package_dir] [--mutual-only | --buffers-only]
 """
 
 from __future__ import annotations
@@ -94,6 +94,50 @@ def mutual(root: str) -> None:
                 out[f"{tag}_{f}"] = np.asarray(getattr(r, f))
         np.savez_compressed(os.path.join(HERE, f"mutual_{name}_leaf{leaf}.npz"), **out)
         print("wrote", f"mutual_{name}_leaf{leaf}")
+
+
+def buffers(root: str) -> None:
+    """Dense level-major M2L buffers and class-grouped far pairs, computed by
+    the reference's own densify_interactions / geometry_to_level_major /
+    build_grouped_interactions_from_pairs from its own tree, geometry and
+    far lists (rows sorted, the canonical order both sides use), with the
+    grouped input pairs in node order."""
+    m = jaxshim.load_reference(root)
+    jnp = sys.modules["jax.numpy"]
+    ti, gi, ii, bd = m["_tree_impl"], m["_geometry_impl"], m["_interactions_impl"], m["bounds"]
+    import importlib
+
+    di = importlib.import_module("yggdrax.dense_interactions")
+    gr = m["grouped_interactions"]
+    inputs = _inputs()
+    for name, leaf, theta, mac in (("uniform300", 4, 0.6, "dehnen"), ("plummer400", 8, 0.5, "bh")):
+        pos = inputs[name]
+        mass = np.linspace(0.5, 1.5, pos.shape[0]).astype(np.float32)
+        p, ms = jnp.asarray(pos), jnp.asarray(mass)
+        b = bd.infer_bounds(p)
+        t, ps, _, _ = ti.build_tree(p, ms, b, leaf_size=leaf, return_reordered=True)
+        g = gi.compute_tree_geometry(t, ps, max_leaf_size=leaf)
+        inter, _ = ii.build_interactions_and_neighbors(t, g, theta=theta, mac_type=mac)
+        srt = _rows_sorted(inter.offsets, inter.counts, inter.sources)
+        inter = inter._replace(sources=jnp.asarray(srt))
+        dense = di.densify_interactions(t, g, inter)
+        lg = dense.geometry
+        off, cnt = np.asarray(inter.offsets), np.asarray(inter.counts)
+        src = np.concatenate([srt[off[k]:off[k] + cnt[k]] for k in range(cnt.shape[0])])
+        tgt = np.repeat(np.arange(cnt.shape[0]), cnt)
+        grp = gr.build_grouped_interactions_from_pairs(t, g, jnp.asarray(src), jnp.asarray(tgt),
+                                                       level_offsets=inter.level_offsets)
+        out = dict(theta=np.float64(theta), mac=np.array(mac), leaf=np.int64(leaf),
+                   lm_centers=lg.centers, lm_half_extents=lg.half_extents, lm_radii=lg.radii,
+                   lm_max_extents=lg.max_extents, lm_level_counts=lg.level_counts,
+                   lm_node_indices=lg.node_indices, m2l_sources=dense.m2l_sources,
+                   m2l_displacements=dense.m2l_displacements, m2l_mask=dense.m2l_mask,
+                   m2l_counts=dense.m2l_counts, pair_sources=src, pair_targets=tgt)
+        for f in grp._fields:
+            out[f"grp_{f}"] = np.asarray(getattr(grp, f))
+        np.savez_compressed(os.path.join(HERE, f"buffers_{name}_leaf{leaf}.npz"),
+                            **{k: np.asarray(v) for k, v in out.items()})
+        print("wrote", f"buffers_{name}_leaf{leaf}")
 
 
 def main(root: str) -> None:
@@ -225,6 +269,9 @@ if __name__ == "__main__":
     ref = args[0] if args else "/root/reference/yggdrax"
     if "--mutual-only" in sys.argv:
         mutual(ref)
+    elif "--buffers-only" in sys.argv:
+        buffers(ref)
     else:
         main(ref)
         mutual(ref)
+        buffers(ref)

@@ -8,7 +8,8 @@ Inputs and outputs are torch CUDA tensors in the reference's layouts.
 """
 
 from .dtypes import INDEX_DTYPE, as_index
-from .geometry import TreeGeometry, compute_tree_geometry
+from .geometry import (LevelMajorTreeGeometry, TreeGeometry, compute_tree_geometry,
+                       geometry_to_level_major)
 from .interactions import (
     CompactTaggedFarPairs,
     DualTreeRetryEvent,
@@ -27,6 +28,10 @@ from .interactions import (
     set_traversal_mode,
 )
 from .mutual import MutualWalkResult, dual_tree_walk_mutual
+from .dense_interactions import (DenseInteractionBuffers, build_dense_interactions,
+                                 densify_interactions)
+from .grouped_interactions import (GroupedInteractionBuffers, build_grouped_interactions,
+                                   build_grouped_interactions_from_pairs)
 from .morton import (
     encode_and_sort,
     get_common_prefix_length,

@@ -112,6 +112,11 @@ _SIGS = {
     "ygx_batch_build_topology": (I32, [P, P, P, P, P, I64, I64, I32] + [P] * 22 + [SZ, P]),
     "ygx_batch_tree_geometry": (I32, [P, I64, I64, P, P, I64, P, I32, P, P, P, P, P, P, I64, P, P,
                                       P, P, P, SZ, P]),
+    "ygx_level_major_geometry": (I32, [P, P, I32, I32, I64, P, P, P, P, P, P, P, P, P, P]),
+    "ygx_dense_m2l": (I32, [P, I32, I64, I64, P, P, P, P, I64, P, P, P, P, P]),
+    "ygx_grouped_workspace_size": (SZ, [I64]),
+    "ygx_grouped_classes": (I32, [P, P, I32, I64, P, P, P, P, P, SZ, P]),
+    "ygx_grouped_emit": (I32, [P, P, I32, I64, P, P, P, P, P, P, P, P, SZ, P]),
     "ygx_mutual_walk_workspace_size": (SZ, [I64, I64]),
     "ygx_mutual_walk": (I32, [P, P, I32, P, P, I64, F32, I64, I64, I64, I64, P, P, P, P, P, P, P,
                               P, SZ, P]),

@@ -69,4 +69,49 @@ def compute_tree_geometry(tree, positions_sorted: torch.Tensor, *,
     return TreeGeometry(center, half, radius, max_extent)
 
 
-__all__ = ["TreeGeometry", "compute_tree_geometry"]
+class LevelMajorTreeGeometry(NamedTuple):
+    """Tree geometry in padded level-major buffers (_geometry_impl.py:39-47):
+    ``(num_levels, max_nodes_per_level[, 3])``, zero past each level's nodes,
+    ``node_indices`` -1 there."""
+
+    centers: torch.Tensor
+    half_extents: torch.Tensor
+    radii: torch.Tensor
+    max_extents: torch.Tensor
+    level_counts: torch.Tensor
+    node_indices: torch.Tensor
+
+
+def geometry_to_level_major(tree, geometry: TreeGeometry) -> LevelMajorTreeGeometry:
+    """geometry_to_level_major (geometry.py:79-102, _geometry_impl.py:342-420):
+    row l holds the geometry of the l-th level's nodes in ``nodes_by_level``
+    order; one kernel (``ygx_level_major_geometry``)."""
+    from .dtypes import INDEX_DTYPE
+
+    topology = resolve_tree_topology(tree)
+    d = _dev_of(topology)
+    nlev = _host_of(topology).num_levels
+    if nlev <= 0:
+        raise ValueError("tree must contain at least one populated level")
+    dev = topology.parent.device
+    lo = topology.level_offsets.to(INDEX_DTYPE).contiguous()
+    counts = (lo[1:] - lo[:-1])[:nlev]
+    M = int(torch.clamp(counts, min=1).max())
+    f = lambda *s: torch.empty(s, dtype=torch.float32, device=dev)  # noqa: E731
+    out = LevelMajorTreeGeometry(
+        centers=f(nlev, M, 3), half_extents=f(nlev, M, 3), radii=f(nlev, M),
+        max_extents=f(nlev, M), level_counts=counts,
+        node_indices=torch.empty((nlev, M), dtype=INDEX_DTYPE, device=dev))
+    L.check(L.lib().ygx_level_major_geometry(
+        L.ptr(d.nbl32), L.ptr(lo), INDEX_BITS, nlev, M,
+        L.ptr(geometry.center.contiguous().float()),
+        L.ptr(geometry.half_extent.contiguous().float()),
+        L.ptr(geometry.radius.contiguous().float()),
+        L.ptr(geometry.max_extent.contiguous().float()), L.ptr(out.centers),
+        L.ptr(out.half_extents), L.ptr(out.radii), L.ptr(out.max_extents),
+        L.ptr(out.node_indices), L.stream_handle(dev)), "ygx_level_major_geometry")
+    return out
+
+
+__all__ = ["TreeGeometry", "LevelMajorTreeGeometry", "compute_tree_geometry",
+           "geometry_to_level_major"]

@@ -740,7 +740,7 @@ def build_interactions_and_neighbors(
     Same arguments, defaults and return conventions as the reference
     (``(interactions, neighbors)`` plus, in this order, the raw result, the
     compact far pairs and the grouped buffers when requested).  ``pair_policy``
-    and ``return_grouped`` are outside the GPU pipeline and raise."""
+    is outside the GPU pipeline and raises."""
     topology = resolve_tree_topology(tree)
     if mac_type not in _MAC_CODES:
         raise ValueError(f"Unknown mac_type: {mac_type}")
@@ -750,8 +750,6 @@ def build_interactions_and_neighbors(
         raise NotImplementedError("pair_policy is outside the GPU traversal (default MAC only)")
     if return_grouped and not return_interactions:
         raise ValueError("grouped interaction return requires return_interactions=True")
-    if return_grouped:
-        raise NotImplementedError("grouped interaction buffers are outside the GPU pipeline")
     if process_block is not None and process_block < 1:
         raise ValueError("process_block must be >= 1")
     del retry_logger, policy_state  # no retries happen on this path
@@ -800,6 +798,14 @@ def build_interactions_and_neighbors(
         if return_compact_far_pairs:
             out.append(CompactTaggedFarPairs(sources=raw_src, targets=raw_tgt, tags=tags,
                                              far_pair_count=fpc))
+    if return_grouped:
+        # (:6113-6123) the raw far pairs (node-order rows) grouped by class
+        from .grouped_interactions import build_grouped_interactions_from_pairs
+
+        _, g_src, g_tgt, _, _ = _node_order_far_pairs(w, total, dev)
+        out.append(build_grouped_interactions_from_pairs(
+            topology, geometry, g_src, g_tgt,
+            level_offsets=interactions.level_offsets if interactions is not None else None))
     return tuple(out)
 
 
