@@ -178,9 +178,16 @@ __global__ void __launch_bounds__(kEncodeThreads)
         for (int p = 0; p < hist_passes; ++p) {
           uint32_t d = k < valid ? (uint32_t)(code[k] >> (p * kSortRadixBits)) & (kSortRadix - 1)
                                  : 0xFFFFu;
-          unsigned peers = __match_any_sync(0xffffffffu, d);
-          if (d != 0xFFFFu && lane == __ffs(peers) - 1)
-            atomicAdd(&s_hist[p * kSortRadix + d], (uint32_t)__popc(peers));
+          // One atomic for the warp when all its digits agree (the high
+          // digits of clustered inputs), else one per lane: cheaper than a
+          // match-any, which runs on a slow pipe here.
+          const unsigned vm = __ballot_sync(0xffffffffu, d != 0xFFFFu);
+          const uint32_t dl = __shfl_sync(0xffffffffu, d, vm ? __ffs(vm) - 1 : 0);
+          if (__all_sync(0xffffffffu, d == dl || d == 0xFFFFu)) {
+            if (lane == 0 && vm) atomicAdd(&s_hist[p * kSortRadix + dl], (uint32_t)__popc(vm));
+          } else if (d != 0xFFFFu) {
+            atomicAdd(&s_hist[p * kSortRadix + d], 1u);
+          }
         }
       }
     }
