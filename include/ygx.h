@@ -492,6 +492,22 @@ int ygx_grouped_emit(const void* sources, const void* targets, int index_bits, i
                      void* class_offsets, void* class_sources, void* class_targets,
                      void* class_ids, void* ws, size_t ws_bytes, cudaStream_t stream);
 
+/* compute_tree_mass_moments / compute_tree_multipole_moments
+ * (yggdrax/tree_moments.py:686-877): fp32 prefix sums of mass-weighted
+ * monomials over the sorted particles, differenced at node_ranges (nodes x 2,
+ * inclusive, index dtype), shifted to `centers` (null: the centres of mass).
+ * o_mass / o_com always; with o_packed non-null also the packed coefficients
+ * (nodes x C, C = total_coefficients(max_order)) and the tensors (dipole 3,
+ * second / quadrupole 9, third / octupole 27, fourth / hexadecapole 81 per
+ * node).  Does not synchronize. */
+size_t ygx_moments_workspace_size(int64_t n, int max_order);
+int ygx_tree_moments(const float* positions_sorted, const float* masses_sorted, int64_t n,
+                     const void* node_ranges, int index_bits, int64_t nodes, int max_order,
+                     const float* centers, float* o_mass, float* o_com, float* o_center,
+                     float* o_packed, float* o_dipole, float* o_second, float* o_quad,
+                     float* o_third, float* o_oct, float* o_fourth, float* o_hexa, void* ws,
+                     size_t ws_bytes, cudaStream_t stream);
+
 /* dual_tree_walk_mutual (yggdrax/_interactions_impl.py:6357-6560): the
  * symmetric walk that emits every unordered node pair once.  left_full /
  * right_full: children of all `total` nodes (-1 on leaves) in the index dtype;

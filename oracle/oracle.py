@@ -709,3 +709,154 @@ def grouped_from_pairs(sources, targets, node_level, center, bounds_min, bounds_
     return dict(class_keys=ck, class_displacements=cdisp,
                 class_offsets=np.concatenate([starts, [ks.shape[0]]]).astype(np.int64),
                 class_sources=src[order], class_targets=tgt[order], class_ids=ids.astype(np.int64))
+
+
+def _combos(order: int):
+    """multi_index_tuples(0..order) concatenated (multipole_utils.py)."""
+    out = []
+    for lv in range(order + 1):
+        for i in range(lv + 1):
+            for j in range(lv + 1 - i):
+                out.append((i, j, lv - i - j))
+    return out
+
+
+def tree_mass_moments(node_ranges, positions_sorted, masses_sorted):
+    """compute_tree_mass_moments (tree_moments.py:686-744): fp32 prefix sums
+    of the masses and mass-weighted positions, differenced at each node's
+    range; centre = weighted sum / mass (0 for a massless node)."""
+    r = np.asarray(node_ranges, np.int64)
+    st, en = r[:, 0], r[:, 1] + 1
+    p = np.asarray(positions_sorted, np.float32)
+    m = np.asarray(masses_sorted, np.float32)
+    mp = np.concatenate([np.zeros(1, np.float32), np.cumsum(m)])
+    wp = np.concatenate([np.zeros((1, 3), np.float32), np.cumsum(m[:, None] * p, axis=0)])
+    tot = mp[en] - mp[st]
+    mom = wp[en] - wp[st]
+    safe = np.where(tot == 0, np.ones_like(tot), tot)
+    ctr = np.where(tot[:, None] == 0, np.float32(0), mom / safe[:, None])
+    return tot, ctr
+
+
+def tree_multipole_moments(node_ranges, positions_sorted, masses_sorted, expansion_centers=None,
+                           max_order: int = 2) -> dict:
+    """compute_tree_multipole_moments (tree_moments.py:747-877) and the
+    tensors of _moments_from_raw_packed (:312-395): fp32 cumprod powers,
+    monomials x^a y^b z^c weighted by mass, prefix sums differenced at the
+    node ranges, the binomial shift to the expansion centre (einsum over the
+    stencil), then the symmetric second..fourth moments and their trace-free
+    quadrupole / octupole / hexadecapole, zero for massless nodes."""
+    tot, com = tree_mass_moments(node_ranges, positions_sorted, masses_sorted)
+    center = com if expansion_centers is None else np.asarray(expansion_centers, np.float32)
+    order = int(max_order)
+    p = np.asarray(positions_sorted, np.float32)
+    m = np.asarray(masses_sorted, np.float32)
+    r = np.asarray(node_ranges, np.int64)
+    st, en = r[:, 0], r[:, 1] + 1
+    cb = np.asarray(_combos(order), np.int64)
+    C = cb.shape[0]
+
+    def axis_powers(v):
+        base = np.asarray(v, np.float32)[:, None]
+        ones = np.ones_like(base)
+        if order == 0:
+            return ones
+        return np.cumprod(np.concatenate([ones, np.repeat(base, order, axis=1)], axis=1), axis=1)
+
+    ax, ay, az = axis_powers(p[:, 0]), axis_powers(p[:, 1]), axis_powers(p[:, 2])
+    mono = ax[:, cb[:, 0]] * ay[:, cb[:, 1]] * az[:, cb[:, 2]]
+    w = m[:, None] * mono
+    pre = np.concatenate([np.zeros((1, C), np.float32), np.cumsum(w, axis=0)], axis=0)
+    raw = pre[en] - pre[st]
+    neg = -center
+    cx, cy, cz = axis_powers(neg[:, 0]), axis_powers(neg[:, 1]), axis_powers(neg[:, 2])
+    full = np.asarray(_combos(4), np.int64)
+    T = full.shape[0]
+    gamma = np.zeros((T, T, 3), np.int64)
+    mask = np.zeros((T, T), bool)
+    binom = np.zeros((T, T), np.float64)
+    for i in range(T):
+        for j in range(T):
+            if (full[i] >= full[j]).all():
+                mask[i, j] = True
+                gamma[i, j] = full[i] - full[j]
+                binom[i, j] = (math.comb(*[int(x) for x in (full[i, 0], full[j, 0])])
+                               * math.comb(int(full[i, 1]), int(full[j, 1]))
+                               * math.comb(int(full[i, 2]), int(full[j, 2])))
+    g = np.where(mask[:C, :C, None], gamma[:C, :C], 0)
+    cf = (np.take(cx, g[..., 0], axis=1) * np.take(cy, g[..., 1], axis=1)
+          * np.take(cz, g[..., 2], axis=1))
+    transform = cf * mask[:C, :C].astype(np.float32)[None] * binom[:C, :C].astype(np.float32)[None]
+    packed = np.einsum("nij,nj->ni", transform, raw)
+    return _tensors_from_packed(packed, center, order)
+
+
+def _tensors_from_packed(packed, center, order: int) -> dict:
+    n = packed.shape[0]
+    look = {c: k for k, c in enumerate(_combos(order))}
+    mass = packed[:, 0]
+    dt = packed.dtype
+    dip = np.zeros((n, 3), dt)
+    if order >= 1:
+        dip[:, 0], dip[:, 1], dip[:, 2] = (packed[:, look[(1, 0, 0)]], packed[:, look[(0, 1, 0)]],
+                                           packed[:, look[(0, 0, 1)]])
+    sec = np.zeros((n, 3, 3), dt)
+    thr = np.zeros((n, 3, 3, 3), dt)
+    fou = np.zeros((n, 3, 3, 3, 3), dt)
+
+    def combo_of(*axes):
+        c = [0, 0, 0]
+        for a in axes:
+            c[a] += 1
+        return tuple(c)
+
+    import itertools as it
+    if order >= 2:
+        for i, j in it.product(range(3), repeat=2):
+            sec[:, i, j] = packed[:, look[combo_of(i, j)]]
+    if order >= 3:
+        for i, j, k in it.product(range(3), repeat=3):
+            thr[:, i, j, k] = packed[:, look[combo_of(i, j, k)]]
+    if order >= 4:
+        for i, j, k, l in it.product(range(3), repeat=4):
+            fou[:, i, j, k, l] = packed[:, look[combo_of(i, j, k, l)]]
+    trace = np.trace(sec, axis1=-2, axis2=-1)
+    quad = dt.type(3.0) * sec - trace[:, None, None] * np.eye(3, dtype=dt)
+    octu = np.zeros_like(thr)
+    if order >= 3:
+        r2rk = np.stack([thr[:, 0, 0, k] + thr[:, 1, 1, k] + thr[:, 2, 2, k] for k in range(3)], -1)
+        for i, j, k in it.product(range(3), repeat=3):
+            v = dt.type(5.0) * thr[:, i, j, k]
+            if i == j:
+                v = v - r2rk[:, k]
+            if i == k:
+                v = v - r2rk[:, j]
+            if j == k:
+                v = v - r2rk[:, i]
+            octu[:, i, j, k] = v
+    hexa = np.zeros_like(fou)
+    if order >= 4:
+        r2 = fou[:, 0, 0] + fou[:, 1, 1] + fou[:, 2, 2]
+        r4 = (fou[:, 0, 0, 0, 0] + fou[:, 1, 1, 1, 1] + fou[:, 2, 2, 2, 2]
+              + dt.type(2.0) * (fou[:, 0, 0, 1, 1] + fou[:, 0, 0, 2, 2] + fou[:, 1, 1, 2, 2]))
+        for i, j, k, l in it.product(range(3), repeat=4):
+            v = dt.type(35.0) * fou[:, i, j, k, l]
+            term = np.zeros_like(v)
+            for cond, (a, b) in ((i == j, (k, l)), (i == k, (j, l)), (i == l, (j, k)),
+                                 (j == k, (i, l)), (j == l, (i, k)), (k == l, (i, j))):
+                if cond:
+                    term = term + r2[:, a, b]
+            v = v - dt.type(5.0) * term
+            df = int(i == j and k == l) + int(i == k and j == l) + int(i == l and j == k)
+            if df:
+                v = v + r4 * df
+            hexa[:, i, j, k, l] = v
+    z = mass == 0
+    return dict(mass=mass, center=center, dipole=np.where(z[:, None], 0, dip).astype(dt),
+                second_moment=np.where(z[:, None, None], 0, sec).astype(dt),
+                quadrupole=np.where(z[:, None, None], 0, quad).astype(dt),
+                third_moment=np.where(z[:, None, None, None], 0, thr).astype(dt),
+                octupole=np.where(z[:, None, None, None], 0, octu).astype(dt),
+                fourth_moment=np.where(z[:, None, None, None, None], 0, fou).astype(dt),
+                hexadecapole=np.where(z[:, None, None, None, None], 0, hexa).astype(dt),
+                raw_packed=packed)

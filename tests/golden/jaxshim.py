@@ -128,6 +128,13 @@ class _AtIdx:
 
     def _apply(self, values, op):
         out = np.array(self.arr, copy=True)
+        idx = self.idx if isinstance(self.idx, tuple) else (self.idx,)
+        if any(it is Ellipsis for it in idx) and op == "set" and all(
+                it is Ellipsis or isinstance(it, slice) or np.ndim(it) == 0 for it in idx):
+            # basic (Ellipsis / slice / scalar) indexing, all in range here
+            out[tuple(it if (it is Ellipsis or isinstance(it, slice)) else int(it)
+                      for it in idx)] = np.asarray(values)
+            return _wrap(out)
         arrays, keep = _scatter_index(out, self.idx)
         if all(isinstance(a, slice) for a in arrays):
             tgt = tuple(arrays)
@@ -141,6 +148,13 @@ class _AtIdx:
                 out[tgt] = np.minimum(out[tgt], values)
             return _wrap(out)
         if any(isinstance(a, slice) for a in arrays):
+            if keep is not None and np.ndim(keep) == 0:
+                # scalar indices beside slices (x.at[:, 0].set(v))
+                if not bool(keep):
+                    return _wrap(out)
+                tgt = tuple(a if isinstance(a, slice) else int(a) for a in arrays)
+                out[tgt] = np.asarray(values)
+                return _wrap(out)
             # mixed slice + array: only used with a trailing full slice
             tgt = tuple(a[keep] if (keep is not None and not isinstance(a, slice)) else a
                         for a in arrays)
@@ -203,7 +217,8 @@ def _mk_jnp():
                  "tile", "repeat", "broadcast_to", "ravel", "reshape", "transpose",
                  "take_along_axis", "flip", "diff", "unique", "isnan", "all", "any",
                  "prod", "floor_divide", "expand_dims", "squeeze", "count_nonzero", "ceil",
-                 "argmax", "argmin", "isin", "cumprod", "outer", "meshgrid", "dot"]:
+                 "argmax", "argmin", "isin", "cumprod", "outer", "meshgrid", "dot",
+                 "take", "einsum", "trace"]:
         setattr(jnp, name, w(getattr(np, name)))
     for name in ["int8", "int16", "int32", "int64", "uint8", "uint16", "uint32", "uint64",
                  "float16", "float32", "float64", "bool_", "complex64", "complex128", "iinfo",
@@ -217,6 +232,7 @@ def _mk_jnp():
         a = np.asarray(x, dtype=dtype)
         return _wrap(np.array(a, copy=True) if a.ndim == 0 else a)
     jnp.asarray = asarray
+    jnp.result_type = np.result_type
     jnp.array = lambda x, dtype=None, **k: _wrap(np.array(x, dtype=dtype))
     for name in ["zeros", "ones", "empty", "full", "arange", "zeros_like", "ones_like",
                  "full_like", "empty_like", "linspace", "eye"]:

@@ -8,7 +8,7 @@ to this script and are what ``tests/test_golden.py`` checks the oracle
 against.  Within-row order of the interaction / neighbour lists is
 unspecified in the reference (unstable argsort), so rows are stored sorted.
 
-Usage: python tests/golden/make_golden.py [reference_package_dir] [--mutual-only | --buffers-only]
+Usage: python tests/golden/make_golden.py [reference_package_dir] [--mutual-only | --buffers-only | --moments-only]
 """
 
 from __future__ import annotations
@@ -138,6 +138,41 @@ def buffers(root: str) -> None:
         np.savez_compressed(os.path.join(HERE, f"buffers_{name}_leaf{leaf}.npz"),
                             **{k: np.asarray(v) for k, v in out.items()})
         print("wrote", f"buffers_{name}_leaf{leaf}")
+
+
+def moments(root: str) -> None:
+    """compute_tree_mass_moments / compute_tree_multipole_moments (orders 0-4,
+    about the centres of mass and about the geometric centres) on the
+    reference's own trees."""
+    m = jaxshim.load_reference(root)
+    jnp = sys.modules["jax.numpy"]
+    import importlib
+
+    tm = importlib.import_module("yggdrax.tree_moments")
+    ti, gi, bd = m["_tree_impl"], m["_geometry_impl"], m["bounds"]
+    inputs = _inputs()
+    for name, leaf in (("uniform300", 4), ("plummer400", 8)):
+        pos = inputs[name]
+        mass = np.linspace(0.5, 1.5, pos.shape[0]).astype(np.float32)
+        p, ms = jnp.asarray(pos), jnp.asarray(mass)
+        b = bd.infer_bounds(p)
+        t, ps, msrt, _ = ti.build_tree(p, ms, b, leaf_size=leaf, return_reordered=True)
+        g = gi.compute_tree_geometry(t, ps, max_leaf_size=leaf)
+        mm = tm.compute_tree_mass_moments(t, ps, msrt)
+        out = dict(mass=mm.mass, center_of_mass=mm.center_of_mass)
+        for order in range(5):
+            for tag, ctr in (("com", None), ("geo", jnp.asarray(g.center))):
+                r = tm.compute_tree_multipole_moments(t, ps, msrt, expansion_centers=ctr,
+                                                      max_order=order)
+                for f in ("mass", "center", "dipole", "second_moment", "quadrupole",
+                          "third_moment", "octupole", "fourth_moment", "hexadecapole",
+                          "raw_packed"):
+                    out[f"o{order}_{tag}_{f}"] = getattr(r, f)
+                if order == 4:
+                    out[f"o4_{tag}_packed2"] = tm.pack_multipole_expansions(r, 2)
+        np.savez_compressed(os.path.join(HERE, f"moments_{name}_leaf{leaf}.npz"),
+                            **{k: np.asarray(v) for k, v in out.items()})
+        print("wrote", f"moments_{name}_leaf{leaf}")
 
 
 def main(root: str) -> None:
@@ -271,7 +306,10 @@ if __name__ == "__main__":
         mutual(ref)
     elif "--buffers-only" in sys.argv:
         buffers(ref)
+    elif "--moments-only" in sys.argv:
+        moments(ref)
     else:
         main(ref)
         mutual(ref)
         buffers(ref)
+        moments(ref)

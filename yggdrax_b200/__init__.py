@@ -28,6 +28,8 @@ from .interactions import (
     set_traversal_mode,
 )
 from .mutual import MutualWalkResult, dual_tree_walk_mutual
+from .tree_moments import (TreeMassMoments, TreeMultipoleMoments, compute_tree_mass_moments,
+                           compute_tree_multipole_moments, pack_multipole_expansions)
 from .dense_interactions import (DenseInteractionBuffers, build_dense_interactions,
                                  densify_interactions)
 from .grouped_interactions import (GroupedInteractionBuffers, build_grouped_interactions,

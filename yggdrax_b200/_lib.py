@@ -117,6 +117,8 @@ _SIGS = {
     "ygx_grouped_workspace_size": (SZ, [I64]),
     "ygx_grouped_classes": (I32, [P, P, I32, I64, P, P, P, P, P, SZ, P]),
     "ygx_grouped_emit": (I32, [P, P, I32, I64, P, P, P, P, P, P, P, P, SZ, P]),
+    "ygx_moments_workspace_size": (SZ, [I64, I32]),
+    "ygx_tree_moments": (I32, [P, P, I64, P, I32, I64, I32] + [P] * 13 + [SZ, P]),
     "ygx_mutual_walk_workspace_size": (SZ, [I64, I64]),
     "ygx_mutual_walk": (I32, [P, P, I32, P, P, I64, F32, I64, I64, I64, I64, P, P, P, P, P, P, P,
                               P, SZ, P]),
