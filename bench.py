@@ -479,7 +479,8 @@ def main():
 def mode_timings(step, pos_d, mass_d, n, steps, barrier) -> dict:
     """Device time of the step with the plain two-pass traversal (count walk +
     fill walk, the reference's schedule) and with the learned one-pass
-    traversal (rows sized by the capacity predictor), inputs resident."""
+    traversal (rows sized by the capacity predictor), inputs resident; the
+    median over the steps."""
     import torch
 
     import yggdrax_b200 as yb
@@ -489,16 +490,20 @@ def mode_timings(step, pos_d, mass_d, n, steps, barrier) -> dict:
     for mode in ("two_pass", "learned"):
         yb.set_traversal_mode(mode)
         try:
+            torch.cuda.empty_cache()  # start each schedule from the same allocator state
             for _ in range(2):  # capacity hints of this schedule
                 step(pos_d, mass_d)
             barrier()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
-            for _ in range(steps):
+            per = []
+            for _ in range(steps):  # median step: robust to one slow step
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record()
                 step(pos_d, mass_d)
-            b.record()
-            barrier()
-            ms = a.elapsed_time(b) / steps
+                b.record()
+                barrier()
+                per.append(a.elapsed_time(b))
+            ms = float(np.median(per))
             rec = {"ms_per_step": ms, "value": n / (ms / 1e3)}
             if mode == "learned":
                 rec["predictor"] = {k: LAST_WALK_STATS.get(k) for k in (
