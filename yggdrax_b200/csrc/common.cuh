@@ -4,6 +4,8 @@
 #include <stdint.h>
 #include <stddef.h>
 
+#include <atomic>
+
 #include "../../include/ygx.h"
 
 namespace ygx {
@@ -102,6 +104,21 @@ inline int grid_for(int64_t n, int block, int max_blocks = kNumSMs * 16) {
 }
 
 inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+
+// Raises a kernel's dynamic shared-memory limit on the current device.  The
+// attribute is per device, so `done` keeps one bit per device that has it
+// (set from any host thread).
+template <typename Kernel>
+inline cudaError_t ensure_smem_limit(Kernel kernel, int bytes, std::atomic<uint64_t>& done) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return cudaErrorInvalidDevice;
+  const uint64_t bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+  const cudaError_t e =
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+  return e;
+}
 
 // Bump allocator over a caller-provided workspace.
 struct Arena {

@@ -333,12 +333,10 @@ int onesweep_sort(const uint64_t* keys_in, const uint32_t* vals_in, int64_t n, i
   YGX_CHECK_LAUNCH();
 
   const size_t smem = sizeof(OnesweepSmem);
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaFuncSetAttribute(k_onesweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_onesweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_done = true;
-  }
+  static std::atomic<uint64_t> attr_iota{0}, attr_vals{0};
+  if (ensure_smem_limit(k_onesweep<true>, (int)smem, attr_iota) != cudaSuccess ||
+      ensure_smem_limit(k_onesweep<false>, (int)smem, attr_vals) != cudaSuccess)
+    return YGX_ERR_CUDA;
   const uint64_t* src_k = keys_in;
   const uint32_t* src_v = vals_in;
   for (int p = 0; p < passes; ++p) {

@@ -1872,11 +1872,9 @@ static int finalize_impl(const ygx::TravScratch& s, int64_t total, int64_t L,
                          int64_t max_nbr, cudaStream_t stream) {
   const int grid_small = ygx::kNumSMs * ygx::g_tune.row_grid_per_sm;
   const size_t big_smem = sizeof(int32_t) * ygx::kBlockRowCap;
-  static bool big_attr = false;
-  if (!big_attr) {
-    cudaFuncSetAttribute(ygx::k_rows_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem);
-    big_attr = true;
-  }
+  static std::atomic<uint64_t> big_attr{0};
+  if (ygx::ensure_smem_limit(ygx::k_rows_big, (int)big_smem, big_attr) != cudaSuccess)
+    return YGX_ERR_CUDA;
   const int64_t stride = total > L ? total : L;
   auto rows_pass = [&](int64_t rows, const int64_t* off, const int32_t* cnt, const int32_t* lvl,
                        int32_t* raw, const int64_t* roff, const int32_t* rbase, void* vals,
