@@ -135,6 +135,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def _max_over_ranks(values, device):
+    """Element-wise maximum of ``values`` over all ranks (identity on one)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -424,21 +436,15 @@ def main():
         modes.update(mode_timings(step, pos_d, mass_d, n, args.steps, barrier))
 
     batched = None
-    if not args.no_batched:  # every rank (barriers inside)
-        batched = batched_timing(dev, args.steps, barrier)
+    if not args.no_batched:  # every rank (barriers inside), each on its share of the sets
+        batched = batched_timing(dev, args.steps, barrier, world=world, rank=rank)
 
     breakdown = None
     if args.breakdown:
         breakdown = stage_breakdown(pos_d, mass_d, dev)
 
     # -- aggregate over ranks ---------------------------------------------------
-    t_max, te_max, te_serial_max = t_dev, t_e2e, t_e2e_serial
-    if world > 1:
-        import torch.distributed as dist
-
-        tt = torch.tensor([t_dev, t_e2e, t_e2e_serial], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max, te_max, te_serial_max = float(tt[0]), float(tt[1]), float(tt[2])
+    t_max, te_max, te_serial_max = _max_over_ranks([t_dev, t_e2e, t_e2e_serial], dev)
     if rank == 0:
         cpu = None if args.no_cpu_baseline else cpu_baseline(args.cpu_sample)
         line = {
@@ -515,13 +521,17 @@ def mode_timings(step, pos_d, mass_d, n, steps, barrier) -> dict:
     return out
 
 
-def batched_timing(dev, steps, barrier, sets: int = 4096, loop_sample: int = 64) -> dict:
+def batched_timing(dev, steps, barrier, sets: int = 4096, loop_sample: int = 64,
+                   world: int = 1, rank: int = 0) -> dict:
     """Device time of the batched workload: 4096 independent point sets,
     sizes log-uniform in [256, 65536] (about 48M points), half uniform cube,
     half Plummer, unit masses, seed 3; radix leaf 16, dehnen theta 0.6.  One
     step = the batched build, geometry and exact lists of every set, one
-    launch per stage.  Beside it, the single-set API called set by set on
-    ``loop_sample`` sets, scaled to all sets by point count."""
+    launch per stage.  With several ranks the sets are split into contiguous
+    shares of about equal point counts (the sets are independent: no
+    exchange) and the step time is the slowest rank's.  Beside it, the
+    single-set API called set by set on ``loop_sample`` sets, scaled to all
+    sets by point count."""
     import torch
 
     import yggdrax_b200 as yb
@@ -529,7 +539,11 @@ def batched_timing(dev, steps, barrier, sets: int = 4096, loop_sample: int = 64)
     from yggdrax_b200 import batch as B
     from yggdrax_b200 import inputs
 
-    pos, mass, off = inputs.batched_sets(sets, 3)
+    pos_all, mass_all, off_all = inputs.batched_sets(sets, 3)
+    s0, s1 = B.shard_sets(off_all, rank, world)
+    a, b = int(off_all[s0]), int(off_all[s1])
+    pos, mass, off = pos_all[a:b], mass_all[a:b], off_all[s0:s1 + 1] - a
+    sets = s1 - s0
     P = torch.from_numpy(pos).to(dev)
     M = torch.from_numpy(mass).to(dev)
     lib = L.lib()
@@ -599,9 +613,12 @@ def batched_timing(dev, steps, barrier, sets: int = 4096, loop_sample: int = 64)
     barrier()
     sample_pts = int(sum(off[i + 1] - off[i] for i in pick))
     loop_ms = a.elapsed_time(b) * float(off[-1]) / sample_pts
-    n = int(off[-1])
+    # whole job: all ranks' sets over the slowest rank's step
+    ms, graph_ms, loop_ms = _max_over_ranks([ms, graph_ms, loop_ms], dev)
+    n = int(off_all[-1])
     return {"workload": "4096_sets_loguniform_256_65536_cube_plummer_radix_leaf16_dehnen_theta0.6",
-            "n_sets": sets, "n_particles": n, "total_nodes": nodes, "ms_per_step": ms,
+            "n_sets": int(off_all.shape[0] - 1), "sets_per_rank": sets, "ranks": world,
+            "n_particles": n, "total_nodes_rank0": nodes, "ms_per_step": ms,
             "value": n / (ms / 1e3), "unit": "particles/s", "far_entries": far,
             "near_entries": near, "pairs_per_s": (far + near) / (ms / 1e3),
             "gpu_launches_per_step": launches,

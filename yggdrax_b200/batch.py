@@ -117,6 +117,26 @@ class BatchedTrees:
         return t
 
 
+def shard_sets(offsets, rank: int, world: int):
+    """Sets [s0, s1) of this rank when S independent sets are spread over
+    ``world`` ranks (one GPU each; the sets need no exchange): contiguous
+    ranges cut at the set boundaries nearest to equal point counts, so every
+    rank gets a share of the points within one set's size of N / world."""
+    off = np.asarray(offsets.cpu() if torch.is_tensor(offsets) else offsets, dtype=np.int64)
+    S = off.shape[0] - 1
+    if world < 1 or not (0 <= rank < world):
+        raise ValueError("need 0 <= rank < world")
+    cuts = [0]
+    for k in range(1, world):
+        target = off[-1] * k / world
+        j = int(np.searchsorted(off, target))
+        j = j if j <= S and (j == 0 or abs(off[j] - target) <= abs(off[j - 1] - target)) \
+            else j - 1
+        cuts.append(min(max(j, cuts[-1]), S))
+    cuts.append(S)
+    return cuts[rank], cuts[rank + 1]
+
+
 @dataclass
 class BatchLayout:
     """Set and leaf offsets of a batch: host copies and device copies.  Leaf
