@@ -27,8 +27,8 @@ import torch
 from . import _lib as L
 from .dtypes import INDEX_BITS, INDEX_DTYPE
 from .geometry import TreeGeometry
-from .interactions import (_CAPACITY_HINTS, _MAC_CODES, NodeInteractionList, NodeNeighborList,
-                           _dense_neighbor_budget)
+from .interactions import (_CAPACITY_HINTS, _MAC_CODES, _WF_CAP_MAX, NodeInteractionList,
+                           NodeNeighborList, _dense_neighbor_budget, _grow_wf_cap, _hint_key)
 from .tree import MAX_TREE_LEVELS, RadixTreeTopology
 
 _GENS_HINTS_BATCH: dict = {}
@@ -386,9 +386,9 @@ def build_interactions_and_neighbors_batched(batch: BatchedTrees, geometry: Batc
             node_offsets=z(total + 1), far_counts=z(total), sources=z(0), targets=z(0),
             target_levels=z(0), near_offsets=z(Lt + 1), near_counts=z(Lt), neighbors=z(0),
             stats={})
-    key = ("batch", mac_type, float(theta))
+    key = _hint_key(mac_type, theta, total, "batch")
     hint_wf, hint_log = _CAPACITY_HINTS.get(key, (0.0, 0.0))
-    cap = min((1 << 32) - 4097, max(32 * total + 65536, int(1.25 * hint_wf * total)))
+    cap = min(_WF_CAP_MAX, max(32 * total + 65536, int(1.25 * hint_wf * total)))
     log_cap = max(8 * total + 65536, int(1.1 * hint_log * total))
     while True:
         ws = L.workspace(lib.ygx_traverse_workspace_size(total, Lt, cap, log_cap), dev)
@@ -403,7 +403,7 @@ def build_interactions_and_neighbors_batched(batch: BatchedTrees, geometry: Batc
         f = int(flags[0])
         if f & (L.FLAG_QUEUE_OVERFLOW | L.FLAG_LOG_OVERFLOW) and rc == 0:
             if f & L.FLAG_QUEUE_OVERFLOW:
-                cap = min((1 << 32) - 4097, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
+                cap = _grow_wf_cap(cap, stats)
                 log_cap = max(log_cap, int(stats[L.TSTAT["log_need"]]))
             else:
                 # the reported need fits the re-run; head-room spares another

@@ -213,6 +213,23 @@ _CAPACITY_HINTS: dict = {}
 # Generations of the last walk per (mac, theta): the walk checks its wavefront
 # first after that many (one host sync instead of one per 16 generations).
 _GENS_HINTS: dict = {}
+# Largest wavefront a walk accepts (pair slots are 32-bit, with a block of
+# head-room the kernels append into).
+_WF_CAP_MAX = (1 << 32) - 4097
+
+
+def _hint_key(mac_type: str, theta: float, total: int, kind: str = "tree") -> tuple:
+    """Hints are kept per (mac, theta) and per octave of the tree size: the
+    entries per node that a small tree needs say little about a large one
+    (a few thousand nodes can need a hundred wavefront pairs per node)."""
+    return (kind, mac_type, float(theta), int(total).bit_length())
+
+
+def _grow_wf_cap(cap: int, stats) -> int:
+    """Wavefront capacity for the re-run of a walk that overflowed it."""
+    if cap >= _WF_CAP_MAX:
+        raise L.YgxError("traversal wavefront exceeds 2^32 pairs")
+    return min(_WF_CAP_MAX, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
 _TIMING = os.environ.get("YGGDRAX_B200_TIMING", "0") == "1"  # per-pass CUDA-event times
 TRAVERSAL_MODES = ("log", "two_pass", "learned")
 _TRAVERSAL_MODE = os.environ.get("YGGDRAX_B200_TRAVERSAL_MODE", "log")
@@ -377,10 +394,10 @@ def _learned_walk_fill(topology, d, total, ni, nl, num_levels, center, radius, m
         L.ptr(leafpos32), total, ni, L.ptr(topology.node_ranges.contiguous()), ib, root,
         float(theta), mac, L.ptr(params), float(cal["slack_far"]), float(cal["slack_near"]),
         int(cal["add"]), L.ptr(far_cap), L.ptr(near_cap), st), "ygx_predict_caps")
-    key = (mac_type, float(theta))
+    key = _hint_key(mac_type, theta, total)
     hint_wf, _ = _CAPACITY_HINTS.get(key, (0.0, 0.0))
     cap = int(wf_capacity) if wf_capacity else max(32 * total + 65536, int(1.25 * hint_wf * total))
-    cap = min(cap, (1 << 32) - 1)
+    cap = min(cap, _WF_CAP_MAX)
     h_ovf, h_ext_far, h_ext_near = _LEARNED_HINTS.get(key, (0.0, 0.0, 0.0))
     log_cap = max(65536, int(1.25 * h_ovf * total))
     extra = [int(1.25 * h_ext_far * total), int(1.25 * h_ext_near * total)]
@@ -408,9 +425,7 @@ def _learned_walk_fill(topology, d, total, ni, nl, num_levels, center, radius, m
         f = int(flags[0])
         if f & (L.FLAG_QUEUE_OVERFLOW | L.FLAG_LOG_OVERFLOW) and rc == 0:
             if f & L.FLAG_QUEUE_OVERFLOW:
-                if cap >= (1 << 32) - 1:
-                    raise L.YgxError("traversal wavefront exceeds 2^32 pairs")
-                cap = min((1 << 32) - 1, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
+                cap = _grow_wf_cap(cap, stats)
                 log_cap = max(log_cap, int(stats[L.TSTAT["log_need"]]))
             else:
                 # the reported need fits the re-run; head-room spares another
@@ -511,12 +526,13 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
         P, Q = s["far_total"], s["near_total"]
     else:
         walk_mode = L.WALK_LOG if mode == "log" else L.WALK_COUNT
-        hint_wf, hint_log = _CAPACITY_HINTS.get((mac_type, float(theta)), (0.0, 0.0))
+        key = _hint_key(mac_type, theta, total)
+        hint_wf, hint_log = _CAPACITY_HINTS.get(key, (0.0, 0.0))
         cap = int(wf_capacity) if wf_capacity else max(32 * total + 65536,
                                                        int(1.25 * hint_wf * total))
         log_cap = (max(8 * total + 65536, int(1.1 * hint_log * total))
                    if walk_mode == L.WALK_LOG else 1)
-        cap = min(cap, (1 << 32) - 1)
+        cap = min(cap, _WF_CAP_MAX)
         runs = 0
         while True:
             runs += 1
@@ -527,15 +543,13 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
                 L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32),
                 L.ptr(d.right32), L.ptr(leafpos32), total, ni, mac, float(theta),
                 float(dehnen_radius_scale), root, walk_mode,
-                _GENS_HINTS.get((mac_type, float(theta)), 0), cap, log_cap, stats.ctypes.data,
+                _GENS_HINTS.get(key, 0), cap, log_cap, stats.ctypes.data,
                 flags.ctypes.data, L.ptr(ws), ws.numel(), st)
             f = int(flags[0])
             if f & (L.FLAG_QUEUE_OVERFLOW | L.FLAG_LOG_OVERFLOW) and rc == 0:
                 if f & L.FLAG_QUEUE_OVERFLOW:
-                    if cap >= (1 << 32) - 1:
-                        raise L.YgxError("traversal wavefront exceeds 2^32 pairs")
                     # the needs a truncated walk reports are lower bounds only
-                    cap = min((1 << 32) - 1, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
+                    cap = _grow_wf_cap(cap, stats)
                     log_cap = max(log_cap, int(stats[L.TSTAT["log_need"]]))
                 else:
                     # the reported need fits the re-run; head-room spares another
@@ -552,12 +566,12 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
             break
         if not wf_capacity:
             # hints only grow (inputs that alternate do not re-run the walk)
-            prev = _CAPACITY_HINTS.get((mac_type, float(theta)), (0.0, 0.0))
+            prev = _CAPACITY_HINTS.get(key, (0.0, 0.0))
             log_need = (max(prev[1], int(stats[L.TSTAT["log_need"]]) / total)
                         if walk_mode == L.WALK_LOG else prev[1])
-            _CAPACITY_HINTS[(mac_type, float(theta))] = (
+            _CAPACITY_HINTS[key] = (
                 max(prev[0], int(stats[L.TSTAT["wf_need"]]) / total), log_need)
-        _GENS_HINTS[(mac_type, float(theta))] = int(stats[L.TSTAT["gens"]])
+        _GENS_HINTS[key] = int(stats[L.TSTAT["gens"]])
         if timing:
             evs[1].record()
         s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
