@@ -105,23 +105,32 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
   if (tid == 0) sm.ticket = atomicAdd(ticket_counter, 1u);
   __syncthreads();
   const uint32_t tile = sm.ticket;
-  const int64_t base = (int64_t)tile * kSortTile;
-  const int64_t wbase = base + (int64_t)warp * (kSortItems * 32);
+  // n < 2^30 (checked on the host): 32-bit positions throughout
+  const uint32_t n32 = (uint32_t)n;
+  const uint32_t base = tile * (uint32_t)kSortTile;
+  const uint32_t wbase = base + (uint32_t)warp * (kSortItems * 32);
+  // The digit of a key: one funnel shift of its two 32-bit halves (or the
+  // high half alone for shift >= 32).
+  const bool high = shift >= 32;
+  const uint32_t sh = (uint32_t)shift & 31u;
+  auto digit_of = [&](uint64_t k) -> uint32_t {
+    const uint32_t lo = (uint32_t)k, hi = (uint32_t)(k >> 32);
+    return (high ? hi >> sh : __funnelshift_r(lo, hi, sh)) & (kSortRadix - 1);
+  };
 
   uint64_t keys[kSortItems];
   uint32_t vals[kSortItems];
   uint16_t rank[kSortItems];
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
-    int64_t idx = wbase + i * 32 + lane;
-    keys[i] = idx < n ? keys_in[idx] : ~0ull;
+    const uint32_t idx = wbase + i * 32 + lane;
+    keys[i] = idx < n32 ? keys_in[idx] : ~0ull;
   }
   // Early counts: the tile's digit histogram first, so its aggregate is
   // published and its look-back resolved before the (longer) ranking --
   // successors then find an inclusive prefix sooner.
 #pragma unroll
-  for (int i = 0; i < kSortItems; ++i)
-    atomicAdd(&s_cnt[(uint32_t)(keys[i] >> shift) & (kSortRadix - 1)], 1u);
+  for (int i = 0; i < kSortItems; ++i) atomicAdd(&s_cnt[digit_of(keys[i])], 1u);
   __syncthreads();
   const int d = tid;
   uint32_t total = s_cnt[d];
@@ -167,7 +176,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
     if (timed_out) raise_flag(status, kFlagTimeout);
     st_volatile_u32(&my_lb[d], kFlagInc | ((excl + total) & kCountMask));
   }
-  sm.glob[d] = digit_offsets[d] + excl;
+  const uint32_t glob_d = digit_offsets[d] + excl;
   // Stable warp multisplit, kRankGroup items at a time: the peer mask of
   // every item (lanes holding the same digit) from one ballot per digit bit
   // (match-any measured slower here), then one shared-memory atomic per
@@ -187,7 +196,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i) {
       uint32_t* tb = tb0 + (i & 1) * kSortRadix;
-      const uint32_t dg = (uint32_t)(keys[i] >> shift) & (kSortRadix - 1);
+      const uint32_t dg = digit_of(keys[i]);
       atomicOr(&tb[dg], 1u << lane);
       __syncwarp();
       const unsigned pm = tb[dg];
@@ -206,7 +215,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
     uint32_t dg[kRankGroup], old[kRankGroup];
 #pragma unroll
     for (int u = 0; u < kRankGroup; ++u) {
-      dg[u] = (uint32_t)(keys[g + u] >> shift) & (kSortRadix - 1);
+      dg[u] = digit_of(keys[g + u]);
       unsigned pm = 0xffffffffu;
 #pragma unroll
       for (int b = 0; b < kSortRadixBits; ++b) {
@@ -231,8 +240,8 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
   // values travel with the keys; loading them here overlaps the look-back
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
-    int64_t idx = wbase + i * 32 + lane;
-    vals[i] = kIotaValues ? (uint32_t)idx : (idx < n ? vals_in[idx] : 0u);
+    const uint32_t idx = wbase + i * 32 + lane;
+    vals[i] = kIotaValues ? idx : (idx < n32 ? vals_in[idx] : 0u);
   }
   __syncthreads();
 
@@ -257,25 +266,26 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
   uint32_t wpre = 0;
   for (int w = 0; w < warp; ++w) wpre += sm.warp_tot[w];
   sm.tile_start[d] = wpre + incl - total;
+  // global position of tile slot k holding digit dd = glob[dd] + k
+  sm.glob[d] = glob_d - (wpre + incl - total);
 
   __syncthreads();
 
   // Scatter into shared memory in tile-sorted order.
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
-    uint32_t dd = (uint32_t)(keys[i] >> shift) & (kSortRadix - 1);
+    const uint32_t dd = digit_of(keys[i]);
     uint32_t pos = sm.tile_start[dd] + sm.warp_hist[warp][dd] + rank[i];
     sm.keys[pos] = keys[i];
     sm.vals[pos] = vals[i];
   }
   __syncthreads();
-  const int64_t nvalid = n - base < kSortTile ? n - base : kSortTile;
+  const int nvalid = n32 - base < (uint32_t)kSortTile ? (int)(n32 - base) : kSortTile;
 #pragma unroll 4
   for (int k = tid; k < nvalid; k += kSortThreads) {
-    uint64_t key = sm.keys[k];
-    uint32_t dd = (uint32_t)(key >> shift) & (kSortRadix - 1);
-    uint32_t g = sm.glob[dd] + (uint32_t)k - sm.tile_start[dd];
-    if (g < (uint64_t)n) {
+    const uint64_t key = sm.keys[k];
+    const uint32_t g = sm.glob[digit_of(key)] + (uint32_t)k;
+    if (g < n32) {
       keys_out[g] = key;
       vals_out[g] = sm.vals[k];
     } else {
