@@ -527,6 +527,48 @@ int ygx_mutual_walk(const void* left_full, const void* right_full, int index_bit
                     uint32_t* flags_out, int* gens_out, void* ws, size_t ws_bytes,
                     cudaStream_t stream);
 
+/* compute_explicit_octree_box_geometry (yggdrax/octree.py:422-476): boxes of
+ * M octree cells from their (code, depth); valid (uint8), codes (uint64) and
+ * depths (index dtype) on the device, bounds_min / bounds_max (3 floats each)
+ * on the HOST.  Writes centers / half_extents (M x 3), radii, max_extents
+ * (M) in fp32, zeros on invalid cells. */
+int ygx_octree_box_geometry(const uint8_t* valid, const uint64_t* codes, const void* depths,
+                            int index_bits, int64_t M, const float* bounds_min,
+                            const float* bounds_max, float* centers, float* half_extents,
+                            float* radii, float* max_extents, cudaStream_t stream);
+
+/* _dual_tree_walk_octree_impl (yggdrax/_interactions_impl.py:1908-2597), the
+ * walk behind build_octree_native_far_pairs / build_octree_native_neighbor_lists
+ * (:5556-5717), in octree cell space from (root, root).  children (M x 8
+ * octant slots, -1 empty) and child_counts in the index dtype; centers /
+ * radii / max_extents the cell boxes; leaf_mask (uint8) the leaf test of the
+ * node space in use.  Exactly one of far_row / near_row is given: far_row
+ * (M, int32) = the log row key of every cell (its position in the level
+ * order); near_row (M, int32) = the row of a leaf cell (0..near_rows-1) or
+ * -1.  mac 0 bh (box max extent), 1 dehnen (box radius x scale), 2 engblom
+ * (box radius).  Every accepted (near) pair is logged twice, per generation
+ * first as (row of t, s) then as (row of s, t), into *_key / *_val
+ * (log_capacity entries); *_cnt receive the row lengths.  stats_out (host,
+ * 8 x int64): far log entries, near log entries, accept, near, refine
+ * decisions, generations, the largest wavefront kept.  flags_out (host):
+ * bit 0 a far row above far_row_cap, bit 1 a near row above near_row_cap,
+ * bit 2 more children than max_pair_queue (the walk stops after that
+ * generation, like the reference), bit 4 more children than wf_capacity
+ * (re-run with stats_out[6] or more), bit 5 the log was too short (the walk
+ * ran on; re-run with stats_out[0] or [1] entries).  Synchronizes once per
+ * generation.  A stable sort of the log by key gives the reference's rows. */
+size_t ygx_octree_walk_workspace_size(int64_t M, int64_t wf_capacity);
+int ygx_octree_walk(const void* children, const void* child_counts, int index_bits, int64_t M,
+                    const float* centers, const float* radii, const float* max_extents,
+                    const uint8_t* leaf_mask, const int32_t* far_row, const int32_t* near_row,
+                    int64_t near_rows, int64_t root, int mac, float theta,
+                    float dehnen_radius_scale, int64_t max_pair_queue, int64_t wf_capacity,
+                    int64_t far_row_cap, int64_t near_row_cap, int64_t log_capacity,
+                    uint64_t* far_key, uint32_t* far_val, uint64_t* near_key,
+                    uint32_t* near_val, int32_t* far_cnt, int32_t* near_cnt,
+                    int64_t* stats_out, uint32_t* flags_out, void* ws, size_t ws_bytes,
+                    cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -860,3 +860,250 @@ def _tensors_from_packed(packed, center, order: int) -> dict:
                 fourth_moment=np.where(z[:, None, None, None, None], 0, fou).astype(dt),
                 hexadecapole=np.where(z[:, None, None, None, None], 0, hexa).astype(dt),
                 raw_packed=packed)
+
+
+# ---------------------------------------------------------------------------
+# Native octree walk (octree node space)
+
+
+def _compact3_np(x: np.ndarray) -> np.ndarray:
+    """Every third bit of a uint64 (the inverse of the Morton spread,
+    ``morton.py:32-39``), by the standard mask-and-shift compaction."""
+    x = np.asarray(x, np.uint64) & np.uint64(0x1249249249249249)
+    for sh, m in ((2, 0x10C30C30C30C30C3), (4, 0x100F00F00F00F00F), (8, 0x001F0000FF0000FF),
+                  (16, 0x001F00000000FFFF), (32, 0x00000000001FFFFF)):
+        x = (x ^ (x >> np.uint64(sh))) & np.uint64(m)
+    return x
+
+
+def octree_box_geometry(valid_mask, node_codes, node_depths, bounds_min, bounds_max) -> dict:
+    """``octree.py:422-476`` (compute_explicit_octree_box_geometry) in fp32,
+    each operation rounded: cell = domain / 2^depth, mins = bmin + cell *
+    index, maxs = mins + cell, centres 0.5 (mins + maxs), half extents
+    0.5 (maxs - mins), radius sqrt((h0^2 + h1^2) + h2^2), max extent max(h);
+    zeros on invalid slots."""
+    bmin = np.asarray(bounds_min, np.float32)
+    dom = (np.asarray(bounds_max, np.float32) - bmin).astype(np.float32)
+    d = np.clip(np.asarray(node_depths, np.int64), 0, 21)
+    sh = (21 - d).astype(np.uint64)
+    codes = np.asarray(node_codes, np.uint64)
+    idx = np.stack([_compact3_np(codes) >> sh, _compact3_np(codes >> np.uint64(1)) >> sh,
+                    _compact3_np(codes >> np.uint64(2)) >> sh], axis=1).astype(np.float32)
+    cnt = np.maximum(np.left_shift(np.uint64(1), d.astype(np.uint64)), np.uint64(1))
+    cell = (dom[None, :] / cnt.astype(np.float32)[:, None]).astype(np.float32)
+    mins = (bmin[None, :] + (cell * idx).astype(np.float32)).astype(np.float32)
+    maxs = (mins + cell).astype(np.float32)
+    centers = (np.float32(0.5) * (mins + maxs)).astype(np.float32)
+    half = (np.float32(0.5) * (maxs - mins)).astype(np.float32)
+    s = (half[:, 0] * half[:, 0] + half[:, 1] * half[:, 1]).astype(np.float32)
+    s = (s + half[:, 2] * half[:, 2]).astype(np.float32)
+    radii = np.sqrt(s).astype(np.float32)
+    maxe = np.max(half, axis=1).astype(np.float32)
+    v = np.asarray(valid_mask, bool)
+    centers[~v] = 0.0
+    half[~v] = 0.0
+    radii[~v] = 0.0
+    maxe[~v] = 0.0
+    return dict(centers=centers, half_extents=half, radii=radii, max_extents=maxe)
+
+
+def octree_traversal_view(oct_fields: dict, num_internal: int, bounds_min, bounds_max) -> dict:
+    """``octree.py:577-704`` (build_explicit_octree_traversal_view): the oct
+    tables, the smallest radix node / leaf id carried by each oct cell
+    (-1 where none, or where the cell is invalid / not a leaf), and the box
+    geometry."""
+    o = {k: np.asarray(v) for k, v in oct_fields.items()}
+    valid = o["oct_valid_mask"].astype(bool)
+    leaf = o["oct_leaf_mask"].astype(bool)
+    M = valid.shape[0]
+    r2o = o["radix_node_to_oct"].astype(np.int64)
+    fill = r2o.shape[0]
+    o2r = np.full(M, fill, np.int64)
+    np.minimum.at(o2r, r2o, np.arange(fill, dtype=np.int64))
+    o2r = np.where(valid & (o2r < fill), o2r, -1)
+    l2o = o["radix_leaf_to_oct"].astype(np.int64)
+    lfill = num_internal + l2o.shape[0]
+    o2l = np.full(M, lfill, np.int64)
+    np.minimum.at(o2l, l2o, np.arange(num_internal, lfill, dtype=np.int64))
+    o2l = np.where(leaf & (o2l < lfill), o2l, -1)
+    box = octree_box_geometry(valid, o["oct_node_codes"], o["oct_node_depths"], bounds_min,
+                              bounds_max)
+    return dict(o, oct_to_radix_node=o2r, oct_to_radix_leaf=o2l, box=box)
+
+
+def octree_native_walk(view: dict, theta: float, mac_type: str = "bh", *,
+                       dehnen_radius_scale: float = 1.0, collect_far: bool, collect_near: bool,
+                       max_interactions_per_node: int, max_neighbors_per_leaf: int,
+                       max_pair_queue: int) -> dict:
+    """``_dual_tree_walk_octree_impl`` (_interactions_impl.py:1908-2597) with
+    far rows in octree node space (the far-pairs entry point) and near rows
+    in octree leaf space (the neighbour-list entry point, whose "leaves" are
+    the cells that carry a radix leaf, ``:1958-1981``).
+
+    Per generation: box-centre distance and MAC (:338-395) on the box radius
+    (dehnen / engblom, dehnen scaled) or box max extent (bh); accept / near /
+    refine (:713-728) with the leaf test of the node space in use; split
+    rule (:2247-2257); children from ``_octree_refine_pairs_single`` (:106-
+    165), which takes the first ``child_count`` of the eight octant slots
+    (slots holding -1 are dropped at the push, :2432-2436), canonicalised
+    and compacted in wavefront order.  Accepted pairs go to row t then row s
+    (fwd block then bwd block of the generation, :2243-2300); the reference
+    orders entries of one row within a block by an unstable argsort
+    (:813-873), this restatement keeps wavefront order.  The walk stops after
+    a generation whose pushes exceed the queue or whose row counts exceed a
+    capacity (:2113-2131).  The effective-extent propagation (:876-990)
+    leaves positive extents unchanged; valid cells always have positive
+    boxes."""
+    ch = np.asarray(view["oct_children"], np.int64)
+    cc = np.asarray(view["oct_child_counts"], np.int64)
+    parent = np.asarray(view["oct_parent"], np.int64)
+    M = parent.shape[0]
+    box = view["box"]
+    c = box["centers"]
+    use_sphere = mac_type in ("dehnen", "engblom")
+    ext = (box["radii"] if use_sphere else box["max_extents"]).astype(np.float32)
+    if mac_type == "dehnen":
+        ext = (np.float32(dehnen_radius_scale) * ext).astype(np.float32)
+    if collect_near:
+        carrier = np.zeros(M, bool)
+        carrier[np.asarray(view["radix_leaf_to_oct"], np.int64)] = True
+        leaf_mask = carrier
+        nz = np.nonzero(carrier)[0]
+        L = np.asarray(view["radix_leaf_to_oct"]).shape[0]
+        leaf_indices = np.full(L, -1, np.int64)
+        leaf_indices[:nz.shape[0]] = nz
+        leaf_pos = np.full(M, -1, np.int64)
+        leaf_pos[nz] = np.arange(nz.shape[0])
+    else:
+        leaf_mask = np.asarray(view["oct_leaf_mask"], bool)
+        leaf_indices = None
+        leaf_pos = None
+    theta_sq = np.float32(theta) * np.float32(theta)
+    theta32 = np.sqrt(theta_sq).astype(np.float32)
+    Q = max(int(max_pair_queue), 4)
+    root = int(np.argmin(parent))
+    wt = np.array([root], np.int64)
+    ws = np.array([root], np.int64)
+    far_rows = [[] for _ in range(M)] if collect_far else None
+    n_rows = leaf_indices.shape[0] if collect_near else 0
+    near_rows = [[] for _ in range(n_rows)] if collect_near else None
+    far_cnt = np.zeros(M, np.int64)
+    near_cnt = np.zeros(n_rows, np.int64)
+    wo = fo = no = False
+    acc = nea = ref = 0
+    gens = 0
+    slots = np.arange(8)
+    while wt.shape[0] > 0 and not (wo or fo or no):
+        gens += 1
+        t, s = wt, ws
+        d = (c[t] - c[s]).astype(np.float32)
+        d2 = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]).astype(np.float32)
+        d2 = (d2 + d[:, 2] * d[:, 2]).astype(np.float32)
+        et, es = ext[t], ext[s]
+        diff = t != s
+        if mac_type == "engblom":
+            big, small = np.maximum(et, es), np.minimum(et, es)
+            lhs = (big + theta32 * small).astype(np.float32)
+            ok = (lhs * lhs).astype(np.float32) <= (theta_sq * d2).astype(np.float32)
+        else:
+            sm = (et + es).astype(np.float32)
+            ok = (sm * sm).astype(np.float32) <= (theta_sq * d2).astype(np.float32)
+        mac_ok = diff & (d2 > 0) & ok
+        tl, sl = leaf_mask[t], leaf_mask[s]
+        accept = mac_ok
+        near = ~mac_ok & tl & sl & diff
+        refine = ~accept & ~near
+        acc += int(accept.sum())
+        nea += int(near.sum())
+        ref += int(refine.sum())
+        same = ~diff
+        split_t = refine & ~tl & (same | sl | (et >= es))
+        split_s = refine & ~sl & (same | tl | (es > et))
+        if collect_far:
+            k = np.nonzero(accept)[0]
+            for i in k:  # fwd block
+                far_rows[t[i]].append(s[i])
+            for i in k:  # bwd block
+                far_rows[s[i]].append(t[i])
+            np.add.at(far_cnt, t[k], 1)
+            np.add.at(far_cnt, s[k], 1)
+            if k.shape[0] and far_cnt.max() > max_interactions_per_node:
+                fo = True
+        if collect_near:
+            k = np.nonzero(near)[0]
+            pt, ps = leaf_pos[t[k]], leaf_pos[s[k]]
+            for j, i in enumerate(k):
+                near_rows[pt[j]].append(s[i])
+            for j, i in enumerate(k):
+                near_rows[ps[j]].append(t[i])
+            np.add.at(near_cnt, pt, 1)
+            np.add.at(near_cnt, ps, 1)
+            if k.shape[0] and near_cnt.max() > max_neighbors_per_leaf:
+                no = True
+        pa, pb = [], []
+        for i in np.nonzero(split_t | split_s)[0]:
+            ti, si = t[i], s[i]
+            if split_t[i] and split_s[i]:
+                if same[i]:
+                    for a in range(cc[ti]):
+                        for b in range(a, cc[ti]):
+                            pa.append(ch[ti, a]); pb.append(ch[ti, b])
+                else:
+                    for a in range(cc[ti]):
+                        for b in range(cc[si]):
+                            pa.append(ch[ti, a]); pb.append(ch[si, b])
+            elif split_t[i]:
+                for a in range(cc[ti]):
+                    pa.append(ch[ti, a]); pb.append(si)
+            else:
+                for b in range(cc[si]):
+                    pa.append(ti); pb.append(ch[si, b])
+        pa = np.asarray(pa, np.int64)
+        pb = np.asarray(pb, np.int64)
+        keep = (pa >= 0) & (pb >= 0)
+        pa, pb = pa[keep], pb[keep]
+        if pa.shape[0] > Q:
+            wo = True
+            pa, pb = pa[:Q], pb[:Q]
+        wt, ws = np.minimum(pa, pb), np.maximum(pa, pb)
+    out = dict(queue_overflow=wo, far_overflow=fo, near_overflow=no, accept_decisions=acc,
+               near_decisions=nea, refine_decisions=ref, generations=gens, root=root)
+    if collect_far:
+        nbl = np.asarray(view["oct_nodes_by_level"], np.int64)
+        srcs = [np.asarray(far_rows[v], np.int64) for v in nbl]
+        out["far_counts"] = far_cnt
+        out["sources"] = np.concatenate(srcs) if srcs else np.zeros(0, np.int64)
+        out["targets"] = np.repeat(nbl, far_cnt[nbl])
+    if collect_near:
+        out["near_counts"] = near_cnt
+        out["neighbors"] = (np.concatenate([np.asarray(r, np.int64) for r in near_rows])
+                            if n_rows else np.zeros(0, np.int64))
+        out["leaf_indices"] = leaf_indices
+    return out
+
+
+def octree_native_neighbor_list(walk: dict, oct_node_ranges) -> dict:
+    """``_raw_to_octree_native_neighbors`` (_interactions_impl.py:5411-5553)
+    without target blocks: rows of the valid carrier cells, CSR offsets, the
+    particle order of the carriers (stable by their first particle) and the
+    dense (rows, max row) table of neighbour row positions (-1 padded)."""
+    li = walk["leaf_indices"]
+    keep = li >= 0
+    leaf_indices = li[keep]
+    counts = walk["near_counts"][keep]
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    ranges = np.asarray(oct_node_ranges, np.int64)
+    order = np.argsort(ranges[np.clip(leaf_indices, 0, None), 0], kind="stable")
+    po_to_native = np.zeros(leaf_indices.shape[0], np.int64)
+    po_to_native[order] = np.arange(leaf_indices.shape[0])
+    lookup = np.full(ranges.shape[0], -1, np.int64)
+    lookup[leaf_indices] = np.arange(leaf_indices.shape[0])
+    mx = int(counts.max()) if counts.shape[0] else 0
+    pos = np.full((leaf_indices.shape[0], mx), -1, np.int64)
+    nb = walk["neighbors"][: int(offsets[-1])]
+    for r in range(leaf_indices.shape[0]):
+        row = nb[offsets[r]:offsets[r + 1]]
+        pos[r, :row.shape[0]] = lookup[row]
+    return dict(offsets=offsets, neighbors=nb, leaf_indices=leaf_indices, counts=counts,
+                particle_order_leaf_indices=leaf_indices[order],
+                particle_order_to_native_leaf=po_to_native, neighbor_leaf_positions=pos)

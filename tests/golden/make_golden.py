@@ -8,7 +8,8 @@ to this script and are what ``tests/test_golden.py`` checks the oracle
 against.  Within-row order of the interaction / neighbour lists is
 unspecified in the reference (unstable argsort), so rows are stored sorted.
 
-Usage: python tests/golden/make_golden.py [reference_package_dir] [--mutual-only | --buffers-only | --moments-only]
+Usage: python tests/golden/make_golden.py [reference_package_dir]
+       [--mutual-only | --buffers-only | --moments-only | --octwalk-only]
 """
 
 from __future__ import annotations
@@ -175,6 +176,83 @@ def moments(root: str) -> None:
         print("wrote", f"moments_{name}_leaf{leaf}")
 
 
+def octree_native(root: str) -> None:
+    """build_octree_native_far_pairs / build_octree_native_neighbor_lists on
+    the reference's own octree topologies (adaptive and fixed depth), with
+    capacities that fit and ones that overflow a far row or the queue (the
+    error text is stored)."""
+    m = jaxshim.load_reference(root)
+    jnp = sys.modules["jax.numpy"]
+    ti, oc, gi, ii, bd = (m["_tree_impl"], m["octree"], m["_geometry_impl"],
+                          m["_interactions_impl"], m["bounds"])
+    inputs = _inputs()
+    # a jittered 8x8x8 lattice: every cell of a depth-2 (3) octree occupied,
+    # so the octant-slot refinement keeps every child and both lists are full
+    rng = np.random.default_rng(77)
+    g = (np.stack(np.meshgrid(*[np.arange(8)] * 3, indexing="ij"), -1).reshape(-1, 3) + 0.5) / 4
+    inputs["lattice512"] = (g - 1.0 + rng.uniform(-0.05, 0.05, g.shape)).astype(np.float32)
+    inputs["uniform512"] = rng.uniform(-1, 1, (512, 3)).astype(np.float32)
+    cases = (("uniform300", "adaptive", 4), ("plummer400", "adaptive", 8),
+             ("clumps600", "fixed", 8), ("plummer400", "fixed", 4), ("lattice512", "fixed", 8),
+             ("lattice512", "fixed", 1), ("uniform512", "fixed", 4))
+    only = os.environ.get("OCTWALK_CASES")
+    if only:
+        cases = tuple(c for c in cases if f"{c[0]}_{c[1]}{c[2]}" in only.split(","))
+    for name, kind, leaf in cases:
+        pos = inputs[name]
+        mass = np.linspace(0.5, 1.5, pos.shape[0]).astype(np.float32)
+        p, ms = jnp.asarray(pos), jnp.asarray(mass)
+        b = bd.infer_bounds(p)
+        if kind == "fixed":
+            t, ps, _, _ = ti.build_fixed_depth_tree(p, ms, b, target_leaf_particles=leaf,
+                                                    refine_local=True, return_reordered=True)
+            g = gi.compute_tree_geometry(t, ps)
+        else:
+            t, ps, _, _ = ti.build_tree(p, ms, b, leaf_size=leaf, return_reordered=True)
+            g = gi.compute_tree_geometry(t, ps, max_leaf_size=leaf)
+        aug = oc.augment_radix_topology_with_octree(t)
+        view = oc.build_explicit_octree_traversal_view(aug)
+        out = {f: np.asarray(getattr(aug, f)) for f in OCT_FIELDS}
+        out.update(num_internal=np.int64(int(t.num_internal_nodes)),
+                   radix_total=np.int64(int(np.asarray(t.parent).shape[0])),
+                   bounds_min=np.asarray(t.bounds_min), bounds_max=np.asarray(t.bounds_max),
+                   oct_to_radix_node=np.asarray(view.oct_to_radix_node),
+                   oct_to_radix_leaf=np.asarray(view.oct_to_radix_leaf),
+                   box_centers=np.asarray(view.box_centers),
+                   box_half_extents=np.asarray(view.box_half_extents),
+                   box_radii=np.asarray(view.box_radii),
+                   box_max_extents=np.asarray(view.box_max_extents))
+        q = 8192
+        runs = [("dehnen06", 0.6, "dehnen", 512, 2048, q), ("bh05", 0.5, "bh", 512, 2048, q),
+                ("far_over", 0.6, "dehnen", 3, 2048, q), ("near_over", 0.6, "dehnen", 512, 2, q),
+                ("queue_over", 0.6, "dehnen", 512, 2048, 16)]
+        for tag, theta, mac, fcap, ncap, qcap in runs:
+            cfg = ii.DualTreeTraversalConfig(max_pair_queue=qcap, process_block=64,
+                                             max_interactions_per_node=fcap,
+                                             max_neighbors_per_leaf=ncap)
+            out[f"{tag}_params"] = np.array([theta, fcap, ncap, qcap], np.float64)
+            out[f"{tag}_mac"] = np.array(mac)
+            try:
+                fp = ii.build_octree_native_far_pairs(aug, g, theta=theta, mac_type=mac,
+                                                      traversal_config=cfg)
+                for f in fp._fields:
+                    out[f"{tag}_far_{f}"] = np.asarray(getattr(fp, f))
+            except RuntimeError as e:
+                out[f"{tag}_far_error"] = np.array(str(e))
+            try:
+                nb = ii.build_octree_native_neighbor_lists(aug, g, theta=theta, mac_type=mac,
+                                                           traversal_config=cfg)
+                for f in ("offsets", "neighbors", "leaf_indices", "counts",
+                          "particle_order_leaf_indices", "particle_order_to_native_leaf",
+                          "neighbor_leaf_positions"):
+                    out[f"{tag}_near_{f}"] = np.asarray(getattr(nb, f))
+            except RuntimeError as e:
+                out[f"{tag}_near_error"] = np.array(str(e))
+        fname = f"octwalk_{name}_{kind}{leaf}"
+        np.savez_compressed(os.path.join(HERE, f"{fname}.npz"), **out)
+        print("wrote", fname, flush=True)
+
+
 def main(root: str) -> None:
     m = jaxshim.load_reference(root)
     jnp = sys.modules["jax.numpy"]
@@ -308,8 +386,11 @@ if __name__ == "__main__":
         buffers(ref)
     elif "--moments-only" in sys.argv:
         moments(ref)
+    elif "--octwalk-only" in sys.argv:
+        octree_native(ref)
     else:
         main(ref)
         mutual(ref)
         buffers(ref)
         moments(ref)
+        octree_native(ref)

@@ -28,6 +28,11 @@ from .interactions import (
     set_traversal_mode,
 )
 from .mutual import MutualWalkResult, dual_tree_walk_mutual
+from .octree_walk import (CompactTaggedOctreeFarPairs, ExplicitOctreeBoxGeometry,
+                          ExplicitOctreeTraversalView, OctreeNativeNeighborList,
+                          build_explicit_octree_traversal_view, build_octree_native_far_pairs,
+                          build_octree_native_neighbor_lists,
+                          compute_explicit_octree_box_geometry)
 from .tree_moments import (TreeMassMoments, TreeMultipoleMoments, compute_tree_mass_moments,
                            compute_tree_multipole_moments, pack_multipole_expansions)
 from .dense_interactions import (DenseInteractionBuffers, build_dense_interactions,

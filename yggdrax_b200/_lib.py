@@ -63,6 +63,10 @@ _SIGS = {
     "ygx_morton_encode": (I32, [P, I64, P, P, P]),
     "ygx_encode_sort_workspace_size": (SZ, [I64]),
     "ygx_encode_sort": (I32, [P, I64, P, P, P, P, P, SZ, P]),
+    "ygx_octree_box_geometry": (I32, [P, P, P, I32, I64, P, P, P, P, P, P, P]),
+    "ygx_octree_walk_workspace_size": (SZ, [I64, I64]),
+    "ygx_octree_walk": (I32, [P, P, I32, I64, P, P, P, P, P, P, I64, I64, I32, F32, F32, I64,
+                              I64, I64, I64, I64, P, P, P, P, P, P, P, P, P, SZ, P]),
     "ygx_sort_pairs_workspace_size": (SZ, [I64]),
     "ygx_sort_pairs": (I32, [P, P, I64, I32, I32, P, P, P, SZ, P]),
     "ygx_sort_pairs_noalloc": (I32, [P, P, I64, I32, I32, P, P, P]),
