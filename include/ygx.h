@@ -55,6 +55,8 @@ enum {
 #define YGX_TUNE_WALK_BLOCKS 2 /* walk CTAs per SM (2..6)                              */
 #define YGX_TUNE_REFIT_WARPS 3 /* warps per CTA of the leaf refit (2, 4, 8)            */
 #define YGX_TUNE_ROW_GRID 4    /* CTAs per SM of the short-row finalize (4..32, pow2)  */
+#define YGX_TUNE_SORT_TILE 5   /* onesweep tile: 0 16x256 keys 3/SM, 1 12x256 4/SM,     */
+                               /* 2 20x256 2/SM, 3 24x256 2/SM                          */
 
 /* traversal statistics words (host array of YGX_TSTAT_WORDS uint64) */
 #define YGX_TSTAT_WORDS 16

@@ -23,12 +23,14 @@ def tune_mod(monkeypatch, tmp_path):
 def test_knob_table_roundtrip(tune_mod):
     from yggdrax_b200 import _lib as L
 
-    tune_mod.apply({"walk_blocks": 4, "row_grid": 8, "sort_rank": 2, "sort_skew": 100})
+    tune_mod.apply({"walk_blocks": 4, "row_grid": 8, "sort_rank": 2, "sort_skew": 100,
+                    "sort_tile": 3})
     cur = tune_mod.current()
-    assert cur["walk_blocks"] == 4 and cur["row_grid"] == 8
+    assert cur["walk_blocks"] == 4 and cur["row_grid"] == 8 and cur["sort_tile"] == 3
     assert cur["sort_rank"] == 2 and cur["sort_skew"] == 100
     for knob, bad in (("walk_blocks", 1), ("walk_blocks", 7), ("refit_warps", 3),
-                      ("row_grid", 12), ("sort_rank", 3), ("sort_skew", 0), ("sort_skew", 257)):
+                      ("row_grid", 12), ("sort_rank", 3), ("sort_skew", 0), ("sort_skew", 257),
+                      ("sort_tile", -1), ("sort_tile", 4)):
         with pytest.raises(ValueError):
             tune_mod.apply({knob: bad})
         assert tune_mod.current()[knob] == cur[knob]

@@ -238,26 +238,37 @@ def test_single_leaf_tree(cuda_device, oracle):
     assert int(gn.counts.sum()) == 0
 
 
-def test_sort_pairs_is_stable(cuda_device):
+@pytest.mark.parametrize("tile", [0, 1, 2, 3])
+def test_sort_pairs_is_stable(cuda_device, tile):
+    """Stable sort under every onesweep tile shape (3072-6144 keys per tile);
+    sizes straddle tile boundaries of each shape."""
     import torch
 
     from yggdrax_b200 import _lib as L
+    from yggdrax_b200 import autotune
 
-    rng = np.random.default_rng(3)
-    for n, bits in [(1, 8), (4095, 8), (4097, 16), (100003, 63), (300000, 20)]:
-        keys = rng.integers(0, 1 << min(bits, 62), size=n, dtype=np.uint64)
-        keys[: n // 3] = keys[0]  # many ties
-        k = torch.from_numpy(keys).to(cuda_device)
-        ko = torch.empty_like(k)
-        vo = torch.empty(n, dtype=torch.int32, device=cuda_device)
-        lib = L.lib()
-        ws = L.workspace(lib.ygx_sort_pairs_workspace_size(n), cuda_device)
-        L.check(lib.ygx_sort_pairs(L.ptr(k), None, n, 0, bits, L.ptr(ko), L.ptr(vo), L.ptr(ws),
-                                   ws.numel(), L.stream_handle(cuda_device)), "sort")
-        want = np.argsort(keys, kind="stable")
-        np.testing.assert_array_equal(vo.cpu().numpy(), want)
-        np.testing.assert_array_equal(ko.cpu().numpy(), keys[want])
-        assert L.read_status(ws) == 0
+    rng = np.random.default_rng(3 + tile)
+    saved = autotune.current()
+    autotune.apply({"sort_tile": tile})
+    try:
+        for n, bits in [(1, 8), (3071, 8), (4095, 8), (4097, 16), (5121, 12), (6145, 24),
+                        (100003, 63), (300000, 20)]:
+            keys = rng.integers(0, 1 << min(bits, 62), size=n, dtype=np.uint64)
+            keys[: n // 3] = keys[0]  # many ties
+            k = torch.from_numpy(keys).to(cuda_device)
+            ko = torch.empty_like(k)
+            vo = torch.empty(n, dtype=torch.int32, device=cuda_device)
+            lib = L.lib()
+            ws = L.workspace(lib.ygx_sort_pairs_workspace_size(n), cuda_device)
+            L.check(lib.ygx_sort_pairs(L.ptr(k), None, n, 0, bits, L.ptr(ko), L.ptr(vo),
+                                       L.ptr(ws), ws.numel(), L.stream_handle(cuda_device)),
+                    "sort")
+            want = np.argsort(keys, kind="stable")
+            np.testing.assert_array_equal(vo.cpu().numpy(), want)
+            np.testing.assert_array_equal(ko.cpu().numpy(), keys[want])
+            assert L.read_status(ws) == 0
+    finally:
+        autotune.apply(saved)
 
 
 def test_long_rows_match_oracle(cuda_device, oracle):

@@ -37,7 +37,7 @@ FLAG_MALFORMED = 1 << 4
 FLAG_BAD_INPUT = 1 << 5
 FLAG_LOG_OVERFLOW = 1 << 6
 WALK_LOG = 0
-TUNE = dict(sort_rank=0, sort_skew=1, walk_blocks=2, refit_warps=3, row_grid=4)
+TUNE = dict(sort_rank=0, sort_skew=1, walk_blocks=2, refit_warps=3, row_grid=4, sort_tile=5)
 WALK_COUNT = 1
 
 TSTAT_WORDS = 16

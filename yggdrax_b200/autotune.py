@@ -3,7 +3,7 @@
 The library exposes a few process-wide knobs (``ygx_tune_set``): how the
 onesweep sort ranks a tile's keys (warp ballots, per-warp peer tables, or a
 per-pass choice by how concentrated the pass's digits are, with its
-threshold), how many CTAs per SM the traversal walk runs, the warps per CTA
+threshold) and its tile shape (keys per thread, CTAs per SM), how many CTAs per SM the traversal walk runs, the warps per CTA
 of the leaf refit, and the CTAs per SM of the short-row finalize.  None of
 them changes a result.  This module measures candidate settings on the
 caller's own workload with CUDA events and keeps the fastest:
@@ -28,9 +28,10 @@ import torch
 
 from . import _lib as L
 
-KNOBS = ("sort_rank", "sort_skew", "walk_blocks", "refit_warps", "row_grid")
+KNOBS = ("sort_rank", "sort_skew", "sort_tile", "walk_blocks", "refit_warps", "row_grid")
 SPACE: Dict[str, tuple] = {
     "sort_rank": (0, 1, 2),
+    "sort_tile": (0, 1, 2, 3),
     "sort_skew": (8, 16, 32, 64, 128),
     "walk_blocks": (3, 4, 5, 6),
     "refit_warps": (2, 4, 8),
@@ -147,6 +148,17 @@ def tune(step: Callable[[], object], dev: torch.device, *, codes: Optional[torch
                 if log is not None:
                     log.append({"stage": "sort", "config": cfg, "ms": ms})
         best = min(results, key=lambda r: r[0])[1]
+        base_sort = min(r[0] for r in results)
+        for tile in SPACE["sort_tile"]:
+            if tile == best["sort_tile"]:
+                continue
+            cfg = dict(best, sort_tile=tile)
+            apply(cfg)
+            ms = time_ms(run, dev, reps=max(reps, 5))
+            if log is not None:
+                log.append({"stage": "sort", "config": cfg, "ms": ms})
+            if ms < base_sort * 0.99:
+                best, base_sort = cfg, ms
         apply(best)
     base = time_ms(step, dev, reps=reps)
     if log is not None:

@@ -20,6 +20,7 @@ struct Tune {
   int walk_blocks_per_sm = 6;  // walk CTAs per SM (<= kWalkBlocksPerSM)
   int refit_warps = 8;         // warps per CTA of the leaf refit
   int row_grid_per_sm = 16;    // CTAs per SM of the short-row finalize kernels
+  int sort_tile = 0;           // onesweep tile shape (index into kSortShape, sort.cuh)
 };
 extern Tune g_tune;
 

@@ -69,28 +69,33 @@ __global__ void k_hist_scan(const uint32_t* __restrict__ hist, uint32_t* __restr
 
 constexpr int kPeerWords = (kSortThreads / 32) * 2 * kSortRadix;  // peer tables, in keys[]
 
+template <int kItems>
 struct __align__(16) OnesweepSmem {
+  static constexpr int kTile = kSortThreads * kItems;
   uint32_t warp_hist[kSortThreads / 32][kSortRadix];
   uint32_t tile_start[kSortRadix];
   uint32_t glob[kSortRadix];
   uint32_t warp_tot[kSortThreads / 32];
   uint32_t ticket;
-  alignas(16) uint64_t keys[kSortTile];  // 16-byte aligned: zeroed with uint4 stores
-  uint32_t vals[kSortTile];
+  alignas(16) uint64_t keys[kTile];  // 16-byte aligned: zeroed with uint4 stores
+  uint32_t vals[kTile];
 };
-static_assert(offsetof(OnesweepSmem, keys) % 16 == 0, "key staging area is 16-byte aligned");
-static_assert(kPeerWords * sizeof(uint32_t) <= kSortTile * sizeof(uint64_t),
-              "peer tables fit in the key staging area");
+static_assert(kPeerWords * sizeof(uint32_t) <= kSortTileMin * sizeof(uint64_t),
+              "peer tables fit in the key staging area of the smallest tile");
 
-template <bool kIotaValues>
-__global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
+template <bool kIotaValues, int kItems, int kBlocksPerSM>
+__global__ void __launch_bounds__(kSortThreads, kBlocksPerSM)
     k_onesweep(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                int64_t n, int shift, const uint32_t* __restrict__ digit_offsets,
                uint32_t* __restrict__ lookback, uint32_t* __restrict__ ticket_counter,
                uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                const uint32_t* __restrict__ rank_mode, uint32_t* __restrict__ status) {
+  using Smem = OnesweepSmem<kItems>;
+  static_assert(offsetof(Smem, keys) % 16 == 0, "key staging area is 16-byte aligned");
+  constexpr int kSortItems = kItems;
+  constexpr int kSortTile = Smem::kTile;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  OnesweepSmem& sm = *reinterpret_cast<OnesweepSmem*>(smem_raw);
+  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool peer_tables = *rank_mode != 0;  // uniform over the grid
 
@@ -294,6 +299,42 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM)
   }
 }
 
+// Arguments of one onesweep pass.
+struct OnesweepPass {
+  const uint64_t* keys_in;
+  const uint32_t* vals_in;  // nullptr: values are the input positions
+  int64_t n;
+  int shift;
+  const uint32_t* offsets;
+  uint32_t* lookback;
+  uint32_t* counter;
+  uint64_t* keys_out;
+  uint32_t* vals_out;
+  const uint32_t* rank_mode;
+  uint32_t* status;
+};
+
+template <int kItems, int kBlocksPerSM>
+cudaError_t launch_onesweep(const OnesweepPass& a, unsigned tiles, cudaStream_t st) {
+  const size_t smem = sizeof(OnesweepSmem<kItems>);
+  static std::atomic<uint64_t> attr_iota{0}, attr_vals{0};
+  if (ensure_smem_limit(k_onesweep<true, kItems, kBlocksPerSM>, (int)smem, attr_iota) !=
+          cudaSuccess ||
+      ensure_smem_limit(k_onesweep<false, kItems, kBlocksPerSM>, (int)smem, attr_vals) !=
+          cudaSuccess)
+    return cudaErrorInvalidValue;
+  if (a.vals_in == nullptr)
+    k_onesweep<true, kItems, kBlocksPerSM><<<tiles, kSortThreads, smem, st>>>(
+        a.keys_in, nullptr, a.n, a.shift, a.offsets, a.lookback, a.counter, a.keys_out,
+        a.vals_out, a.rank_mode, a.status);
+  else
+    k_onesweep<false, kItems, kBlocksPerSM><<<tiles, kSortThreads, smem, st>>>(
+        a.keys_in, a.vals_in, a.n, a.shift, a.offsets, a.lookback, a.counter, a.keys_out,
+        a.vals_out, a.rank_mode, a.status);
+  note_launch();
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 size_t onesweep_scratch_bytes(int64_t n, int max_passes) {
@@ -304,7 +345,7 @@ size_t onesweep_scratch_bytes(int64_t n, int max_passes) {
 
 SortScratch carve_sort_scratch(Arena& a, int64_t n, int max_passes) {
   SortScratch s;
-  const int64_t tiles = sort_tiles(n) > 0 ? sort_tiles(n) : 1;
+  const int64_t tiles = sort_tiles(n, kSortTileMin) > 0 ? sort_tiles(n, kSortTileMin) : 1;
   // hist, lookback and counters are contiguous so one memset clears them.
   s.hist = a.take<uint32_t>((size_t)max_passes * kSortRadix);
   s.lookback = a.take<uint32_t>((size_t)max_passes * tiles * kSortRadix);
@@ -331,7 +372,6 @@ int onesweep_sort(const uint64_t* keys_in, const uint32_t* vals_in, int64_t n, i
   if (vals_in != nullptr && (const void*)vals_in == (const void*)vals_out) return YGX_ERR_ARG;
   const int passes = sort_passes(begin_bit, end_bit);
   if (passes > 8) return YGX_ERR_ARG;
-  const int64_t tiles = sort_tiles(n);
   if (!hist_ready) {
     if (sort_scratch_reset(s, n, passes, st) != cudaSuccess) return YGX_ERR_CUDA;
     k_histogram<<<grid_for(n, 256, kNumSMs * 4), 256, 0, st>>>(keys_in, n, begin_bit, passes,
@@ -342,13 +382,10 @@ int onesweep_sort(const uint64_t* keys_in, const uint32_t* vals_in, int64_t n, i
                                              g_tune.sort_rank_policy, g_tune.sort_skew_q8);
   YGX_CHECK_LAUNCH();
 
-  const size_t smem = sizeof(OnesweepSmem);
-  static std::atomic<uint64_t> attr_iota{0}, attr_vals{0};
-  if (ensure_smem_limit(k_onesweep<true>, (int)smem, attr_iota) != cudaSuccess ||
-      ensure_smem_limit(k_onesweep<false>, (int)smem, attr_vals) != cudaSuccess)
-    return YGX_ERR_CUDA;
   const uint64_t* src_k = keys_in;
   const uint32_t* src_v = vals_in;
+  const int shape = g_tune.sort_tile;
+  const int64_t tiles = sort_tiles(n, kSortThreads * kSortShape[shape].items);
   for (int p = 0; p < passes; ++p) {
     bool to_out = ((passes - 1 - p) % 2) == 0;
     uint64_t* dk = to_out ? keys_out : s.keys_tmp;
@@ -361,16 +398,26 @@ int onesweep_sort(const uint64_t* keys_in, const uint32_t* vals_in, int64_t n, i
         return YGX_ERR_CUDA;
       src_k = stage;
     }
-    uint32_t* lb = s.lookback + (size_t)p * tiles * kSortRadix;
-    const uint32_t* offs = s.offsets + p * kSortRadix;
-    int shift = begin_bit + p * kSortRadixBits;
-    if (p == 0 && src_v == nullptr)
-      k_onesweep<true><<<(unsigned)tiles, kSortThreads, smem, st>>>(
-          src_k, nullptr, n, shift, offs, lb, s.counters + p, dk, dv, s.rank_mode + p, status);
-    else
-      k_onesweep<false><<<(unsigned)tiles, kSortThreads, smem, st>>>(
-          src_k, src_v, n, shift, offs, lb, s.counters + p, dk, dv, s.rank_mode + p, status);
-    YGX_CHECK_LAUNCH();
+    OnesweepPass a;
+    a.keys_in = src_k;
+    a.vals_in = (p == 0 && src_v == nullptr) ? nullptr : src_v;
+    a.n = n;
+    a.shift = begin_bit + p * kSortRadixBits;
+    a.offsets = s.offsets + p * kSortRadix;
+    a.lookback = s.lookback + (size_t)p * tiles * kSortRadix;
+    a.counter = s.counters + p;
+    a.keys_out = dk;
+    a.vals_out = dv;
+    a.rank_mode = s.rank_mode + p;
+    a.status = status;
+    cudaError_t e;
+    switch (shape) {
+      case 1: e = launch_onesweep<12, 4>(a, (unsigned)tiles, st); break;
+      case 2: e = launch_onesweep<20, 2>(a, (unsigned)tiles, st); break;
+      case 3: e = launch_onesweep<24, 2>(a, (unsigned)tiles, st); break;
+      default: e = launch_onesweep<16, 3>(a, (unsigned)tiles, st); break;
+    }
+    if (e != cudaSuccess) return YGX_ERR_CUDA;
     src_k = dk;
     src_v = dv;
   }

@@ -8,15 +8,24 @@ namespace ygx {
 constexpr int kSortRadixBits = 8;
 constexpr int kSortRadix = 1 << kSortRadixBits;
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
-constexpr int kSortBlocksPerSM = 3;                   // onesweep CTAs resident per SM
 static_assert(kSortThreads == kSortRadix, "onesweep: thread t owns digit t");
+
+// Tile shapes of the onesweep kernel (knob YGX_TUNE_SORT_TILE): keys per
+// thread and CTAs resident per SM.  Shape 0 is the default.  The look-back
+// scratch is sized for the smallest tile, so every shape fits the same
+// workspace.
+struct SortTileShape {
+  int items;          // keys per thread; tile = 256 * items keys
+  int blocks_per_sm;  // launch bound: CTAs resident per SM
+};
+constexpr int kSortTileShapes = 4;
+constexpr SortTileShape kSortShape[kSortTileShapes] = {{16, 3}, {12, 4}, {20, 2}, {24, 2}};
+constexpr int kSortTileMin = kSortThreads * 12;  // 3072 keys: the smallest tile
 
 inline int sort_passes(int begin_bit, int end_bit) {
   return (end_bit - begin_bit + kSortRadixBits - 1) / kSortRadixBits;
 }
-inline int64_t sort_tiles(int64_t n) { return (n + kSortTile - 1) / kSortTile; }
+inline int64_t sort_tiles(int64_t n, int tile) { return (n + tile - 1) / tile; }
 
 // Scratch needed by onesweep_sort for n keys (per-pass histograms, digit
 // offsets, look-back words, tile counters, ping-pong key/value buffers).

@@ -1,7 +1,7 @@
 // Launch-shape knobs chosen by the autotuner (yggdrax_b200/autotune.py).
 // One process-wide table; each knob has a fixed set of legal values, so a
 // bad value is rejected here and never reaches a kernel launch.
-#include "common.cuh"
+#include "sort.cuh"
 
 namespace ygx {
 
@@ -15,6 +15,7 @@ bool legal(int knob, int v) {
     case YGX_TUNE_WALK_BLOCKS: return v >= 2 && v <= 6;
     case YGX_TUNE_REFIT_WARPS: return v == 2 || v == 4 || v == 8;
     case YGX_TUNE_ROW_GRID: return v == 4 || v == 8 || v == 16 || v == 32;
+    case YGX_TUNE_SORT_TILE: return v >= 0 && v < kSortTileShapes;
     default: return false;
   }
 }
@@ -25,6 +26,7 @@ int* slot(int knob) {
     case YGX_TUNE_WALK_BLOCKS: return &g_tune.walk_blocks_per_sm;
     case YGX_TUNE_REFIT_WARPS: return &g_tune.refit_warps;
     case YGX_TUNE_ROW_GRID: return &g_tune.row_grid_per_sm;
+    case YGX_TUNE_SORT_TILE: return &g_tune.sort_tile;
     default: return nullptr;
   }
 }
