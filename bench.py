@@ -54,6 +54,11 @@ LEAF = 32
 THETA = 0.6
 MAC = "dehnen"
 WORKLOAD = "plummer_16M_radix_leaf32_dehnen_theta0.6_exact_lists"
+
+
+def workload_name(n: int) -> str:
+    """The workload label for an n-particle run (the 16M name at the default size)."""
+    return WORKLOAD if n == N_DEFAULT else WORKLOAD.replace("16M", str(n))
 METRIC = "particles/s full build+traversal (Morton, sort, radix build, geometry, exact lists)"
 
 
@@ -251,6 +256,19 @@ def sort_roofline(codes, dev, reps: int) -> dict:
         b.record(stream)
         torch.cuda.synchronize(dev)
         sort_ms.append(a.elapsed_time(b))
+    # Library reference point: CUB's radix sort through torch.sort (stable,
+    # int64 keys, int64 indices: 32 B per key per pass) on the same codes.
+    lib_ms = []
+    c64 = codes.view(torch.int64)
+    for i in range(reps + 2):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        torch.sort(c64, stable=True)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        if i >= 2:
+            lib_ms.append(a.elapsed_time(b))
     passes = 8
     sort_s = float(np.median(sort_ms)) / 1e3
     bytes_per_pass = 24.0 * n
@@ -260,7 +278,8 @@ def sort_roofline(codes, dev, reps: int) -> dict:
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_kind": peak_kind,
             "traffic": SORT_PASS_DRAM_BYTES.get(n), "algorithmic_bytes_per_launch": bytes_per_pass,
-            "launch_ms_avg": sort_s / passes * 1e3, "n_keys": n}
+            "launch_ms_avg": sort_s / passes * 1e3, "n_keys": n,
+            "sort_ms": sort_s * 1e3, "torch_sort_stable_ms": float(np.median(lib_ms))}
 
 
 def main():
@@ -452,7 +471,7 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+int64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_particles": n, "leaf_size": LEAF,
+            "config": {"workload": workload_name(n), "n_particles": n, "leaf_size": LEAF,
                        "mac": MAC, "theta": THETA, "total_nodes": total_nodes,
                        "far_entries": far_entries, "near_entries": near_entries,
                        "pairs_per_s": world * (far_entries + near_entries) / t_max,

@@ -10,21 +10,51 @@ namespace {
 // ---------------------------------------------------------------------------
 // _tree_impl.py:900-926 and :1047-1050: positions/masses gathered into Morton
 // order, particle_indices in the index dtype, inverse permutation scatter.
-__global__ void k_reorder(const float* __restrict__ pos, const float* __restrict__ mass,
-                          const uint32_t* __restrict__ order, int64_t n, int index_bits,
-                          float* __restrict__ pos_sorted, float* __restrict__ mass_sorted,
-                          void* __restrict__ particle_indices, void* __restrict__ inverse) {
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t v = order[k];
-    if (pos_sorted) {
-      pos_sorted[3 * k] = __ldg(pos + 3 * (int64_t)v);
-      pos_sorted[3 * k + 1] = __ldg(pos + 3 * (int64_t)v + 1);
-      pos_sorted[3 * k + 2] = __ldg(pos + 3 * (int64_t)v + 2);
+// Each thread takes kReorderItems particles of a 256 x kReorderItems chunk
+// (coalesced index loads and sorted-order stores) and issues all of their
+// random gathers before any store, so several gathers are in flight per
+// thread instead of one dependent chain per particle.
+constexpr int kReorderItems = 4;
+constexpr int kReorderThreads = 256;
+
+__global__ void __launch_bounds__(kReorderThreads)
+    k_reorder(const float* __restrict__ pos, const float* __restrict__ mass,
+              const uint32_t* __restrict__ order, int64_t n, int index_bits,
+              float* __restrict__ pos_sorted, float* __restrict__ mass_sorted,
+              void* __restrict__ particle_indices, void* __restrict__ inverse) {
+  constexpr int64_t kChunk = (int64_t)kReorderThreads * kReorderItems;
+  for (int64_t k0 = (int64_t)blockIdx.x * kChunk + threadIdx.x; k0 < n;
+       k0 += (int64_t)gridDim.x * kChunk) {
+    uint32_t v[kReorderItems];
+    float x[kReorderItems], y[kReorderItems], z[kReorderItems], m[kReorderItems];
+#pragma unroll
+    for (int u = 0; u < kReorderItems; ++u) {
+      const int64_t k = k0 + (int64_t)u * kReorderThreads;
+      v[u] = k < n ? order[k] : 0u;
     }
-    if (mass_sorted) mass_sorted[k] = __ldg(mass + v);
-    if (particle_indices) store_idx(particle_indices, index_bits, k, v);
-    if (inverse) store_idx(inverse, index_bits, v, k);
+#pragma unroll
+    for (int u = 0; u < kReorderItems; ++u) {
+      const int64_t k = k0 + (int64_t)u * kReorderThreads;
+      if (k < n && pos_sorted) {
+        x[u] = __ldg(pos + 3 * (int64_t)v[u]);
+        y[u] = __ldg(pos + 3 * (int64_t)v[u] + 1);
+        z[u] = __ldg(pos + 3 * (int64_t)v[u] + 2);
+      }
+      if (k < n && mass_sorted) m[u] = __ldg(mass + v[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < kReorderItems; ++u) {
+      const int64_t k = k0 + (int64_t)u * kReorderThreads;
+      if (k >= n) continue;
+      if (pos_sorted) {
+        pos_sorted[3 * k] = x[u];
+        pos_sorted[3 * k + 1] = y[u];
+        pos_sorted[3 * k + 2] = z[u];
+      }
+      if (mass_sorted) mass_sorted[k] = m[u];
+      if (particle_indices) store_idx(particle_indices, index_bits, k, v[u]);
+      if (inverse) store_idx(inverse, index_bits, v[u], k);
+    }
   }
 }
 
@@ -611,7 +641,9 @@ int ygx_reorder(const float* positions, const float* masses, const uint32_t* ord
                 int index_bits, float* positions_sorted, float* masses_sorted,
                 void* particle_indices, void* inverse, cudaStream_t stream) {
   if (n < 1 || !order || (index_bits != 32 && index_bits != 64)) return YGX_ERR_ARG;
-  ygx::k_reorder<<<ygx::grid_for(n, 256), 256, 0, stream>>>(
+  ygx::k_reorder<<<ygx::grid_for((n + ygx::kReorderItems - 1) / ygx::kReorderItems,
+                                  ygx::kReorderThreads),
+                   ygx::kReorderThreads, 0, stream>>>(
       positions, masses, order, n, index_bits, positions_sorted, masses_sorted, particle_indices,
       inverse);
   YGX_CHECK_LAUNCH();
