@@ -74,7 +74,7 @@ def _peaks():
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -82,6 +82,11 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.window = None  # (start, end) host wall-clock seconds of the timed region
+
+    def mark(self, start: float, end: float) -> None:
+        """Record the timed region; summary() then keeps only samples inside it."""
+        self.window = (start, end)
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -89,7 +94,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -112,21 +117,24 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], [], set()
+        import datetime
+
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []  # (time or None, sm MHz, max MHz, active reasons)
         try:
             for line in open(self.path):
                 f = [x.strip() for x in line.split(",")]
-                if len(f) < 9:
+                if len(f) < 10:
                     continue
                 try:
-                    sm.append(float(f[1]))
-                    mx.append(float(f[2]))
+                    t = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                except ValueError:
+                    t = None
+                try:
+                    rows.append((t, float(f[2]), float(f[3]),
+                                 {n for n, v in zip(names, f[6:10]) if v.lower() == "active"}))
                 except ValueError:
                     continue
-                for name, v in zip(names, f[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(name)
         except Exception:
             pass
         finally:
@@ -134,10 +142,20 @@ class ClockSampler:
                 os.unlink(self.path)
             except Exception:
                 pass
-        if not sm:
+        inside = rows
+        if self.window is not None:
+            lo, hi = self.window
+            inside = [r for r in rows if r[0] is not None and lo <= r[0] <= hi]
+        where = "timed region"
+        if not inside:  # region shorter than one sample interval: keep every sample
+            inside, where = rows, "whole sampler run (no sample fell inside the timed region)"
+        if not inside:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
-                "reasons": sorted(reasons), "samples": len(sm)}
+        reasons = set().union(*(r[3] for r in inside))
+        return {"sm_mhz": float(np.median([r[1] for r in inside])),
+                "sm_max_mhz": float(max(r[2] for r in inside)),
+                "reasons": sorted(reasons), "samples": len(inside), "samples_from": where,
+                "interval_ms": 20}
 
 
 def _max_over_ranks(values, device):
@@ -380,11 +398,13 @@ def main():
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     with ClockSampler(torch.cuda.current_device()) as clk:
         barrier()
+        w0 = time.time()
         ev[0].record()
         for _ in range(args.steps):
             tree, geom, inter, nbrs = step(pos_d, mass_d)
         ev[1].record()
         barrier()
+        clk.mark(w0, time.time())
     launches = lib.ygx_launch_counter() - launches0
     t_dev = ev[0].elapsed_time(ev[1]) / 1e3 / args.steps
     far_entries = int(inter.sources.numel())
