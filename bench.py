@@ -310,6 +310,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--breakdown", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the compact / mutual / moments / grouped / octree-walk timings")
     ap.add_argument("--no-modes", action="store_true",
                     help="skip timing the two-pass and learned traversal schedules")
     ap.add_argument("--no-tune", action="store_true",
@@ -478,6 +480,14 @@ def main():
     if not args.no_batched:  # every rank (barriers inside), each on its share of the sets
         batched = batched_timing(dev, args.steps, barrier, world=world, rank=rank)
 
+    extras = None
+    if not args.no_extras and world == 1:
+        try:
+            extras = extras_timing(dev)
+        except Exception as e:  # the main line stands without them
+            extras = {"error": f"{type(e).__name__}: {e}"[:300]}
+        torch.cuda.empty_cache()
+
     breakdown = None
     if args.breakdown:
         breakdown = stage_breakdown(pos_d, mass_d, dev)
@@ -509,6 +519,7 @@ def main():
             "gpu_launches": int(launches),
             "modes": modes,
             "batched": batched,
+            "extras": extras,
         }
         if breakdown is not None:
             line["breakdown_ms"] = breakdown
@@ -667,6 +678,87 @@ def batched_timing(dev, steps, barrier, sets: int = 4096, loop_sample: int = 64,
             "single_set_loop": {"ms_estimate": loop_ms, "sample_sets": len(pick),
                                 "sample_particles": sample_pts,
                                 "speedup_of_batched": loop_ms / ms}}
+
+
+def extras_timing(dev, n: int = 1 << 22, reps: int = 3) -> dict:
+    """Device time (CUDA events, median of ``reps`` after one warm-up call) of
+    the outputs beside the main lists, each on a 4,194,304-particle input:
+    compact far pairs + leaf neighbour lists, the mutual canonical-pair walk,
+    order-4 multipole moments and class-grouped far pairs on the Plummer
+    radix tree (leaf 32, theta 0.6), and the native octree walk (far pairs,
+    neighbour lists) on a fixed-depth octree of Plummer clumps.  A failing leg
+    reports its error instead of a time."""
+    import torch
+
+    import yggdrax_b200 as yb
+    from yggdrax_b200 import inputs
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        ts = []
+        out = None
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            out = fn()
+            b.record()
+            torch.cuda.synchronize(dev)
+            ts.append(a.elapsed_time(b))
+        return float(np.median(ts)), out
+
+    res = {"n_particles": n}
+    pos, mass = inputs.plummer(n, 1)
+    P, M = torch.from_numpy(pos).to(dev), torch.from_numpy(mass).to(dev)
+    tree, ps, ms = yb.build_tree(P, M, leaf_size=LEAF, return_reordered=True)[:3]
+    geom = yb.compute_tree_geometry(tree, ps)
+    total, ni = int(tree.parent.shape[0]), int(tree.left_child.shape[0])
+
+    def leg(name, fn, count):
+        try:
+            ms_, out = timed(fn)
+            c = count(out)
+            res[name] = {"ms": ms_, "entries": c, "entries_per_s": c / (ms_ / 1e3)}
+        except Exception as e:  # report, keep the bench line
+            res[name] = {"error": f"{type(e).__name__}: {e}"[:300]}
+
+    leg("compact_far_pairs_and_leaf_neighbors",
+        lambda: yb.build_compact_far_pairs_and_leaf_neighbor_lists(
+            tree, geom, theta=THETA, mac_type=MAC),
+        lambda o: int(o[0].sources.numel()) + int(o[1].neighbors.numel()))
+    lf = torch.full((total,), -1, dtype=torch.int64, device=dev)
+    rt = lf.clone()
+    lf[:ni] = tree.left_child.to(torch.int64)
+    rt[:ni] = tree.right_child.to(torch.int64)
+    leg("mutual_walk",
+        lambda: yb.dual_tree_walk_mutual(lf, rt, geom.center, geom.radius, THETA, 0,
+                                         max_pair_queue=1 << 26, far_cap=1 << 26,
+                                         near_cap=1 << 26),
+        lambda o: int(o.far_count) + int(o.near_count))
+    leg("multipole_moments_order4",
+        lambda: yb.compute_tree_multipole_moments(tree, ps, ms, max_order=4),
+        lambda o: n)
+    inter = yb.build_interactions_and_neighbors(tree, geom, theta=THETA, mac_type=MAC)[0]
+    leg("grouped_far_pairs",
+        lambda: yb.build_grouped_interactions(tree, geom, inter),
+        lambda o: int(inter.sources.numel()))
+    del tree, ps, ms, geom, inter, lf, rt, P, M
+    pos, mass = inputs.plummer_clumps(n, 2)
+    P, M = torch.from_numpy(pos).to(dev), torch.from_numpy(mass).to(dev)
+    otree = yb.build_fixed_depth_octree(P, M, max_depth=6, return_reordered=True)[0]
+    topo = otree.topology if hasattr(otree, "topology") else otree
+    cfg = yb.DualTreeTraversalConfig(max_pair_queue=1 << 26, process_block=256,
+                                     max_interactions_per_node=1 << 20,
+                                     max_neighbors_per_leaf=1 << 20)
+    leg("octree_native_far_pairs",
+        lambda: yb.build_octree_native_far_pairs(topo, None, theta=THETA, mac_type=MAC,
+                                                 traversal_config=cfg),
+        lambda o: int(o.sources.numel()))
+    leg("octree_native_neighbor_lists",
+        lambda: yb.build_octree_native_neighbor_lists(topo, None, theta=THETA, mac_type=MAC,
+                                                      traversal_config=cfg),
+        lambda o: int(o.neighbors.numel()))
+    return res
 
 
 def stage_breakdown(pos_d, mass_d, dev):
