@@ -1,5 +1,6 @@
-"""The reference's hot-path test properties, re-expressed
-against the CPU oracle: sorted codes, stable ties, parent/child consistency,
+"""The reference's hot-path test properties (tests/test_tree.py,
+test_tree_geometry.py, test_tree_interactions.py, test_octree_topology.py,
+test_morton.py of yggdrax), re-expressed against the CPU oracle: sorted codes, stable ties, parent/child consistency,
 DFS leaf order, node counts, fixed-depth shape, geometry clamps, MAC
 consistency and symmetry of the lists."""
 
