@@ -340,7 +340,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    build_ext.build()
+    if local == 0:  # one builder per node (normally a no-op: the library is prebuilt)
+        build_ext.build()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
     lib = L.lib()
     # The reference's count-pass sizing check rejects Plummer spheres of this
     # size (its outermost halo leaf is near to every leaf); the lists are
