@@ -21,9 +21,10 @@ the whole step.
   walk into rows sized by the learned capacity predictor, with its overflow
   and over-allocation figures).
 * ``cpu_baseline``: the CPU restatement of the pipeline (OpenMP, all host
-  cores) on a bounded sample.
+  cores) on the full workload, timed once.
 * ``--impl reference``: that CPU implementation on the host cores as the
-  reference arm (the reference itself is JAX, which this image lacks).
+  reference arm (the reference itself is JAX, which this image lacks), every
+  step the full workload, with the same ``config``.
 
 With ``--gpus N`` (torchrun, one rank per GPU) every rank runs its own
 replica: the path does not shard, so there is no collective; the value is
@@ -187,52 +188,70 @@ def cpu_pipeline(pos, mass):
     return t, r
 
 
-def cpu_baseline(sample_n: int, reps: int = 1):
+def workload_config(n: int, world: int, total_nodes: int, far_entries: int,
+                    near_entries: int) -> dict:
+    """The workload definition both arms report (identical dicts when the
+    arms ran the same workload)."""
+    return {"workload": workload_name(n), "n_particles": n, "leaf_size": LEAF, "mac": MAC,
+            "theta": THETA, "total_nodes": total_nodes, "far_entries": far_entries,
+            "near_entries": near_entries,
+            "l2": (f"inputs ({16 * n / 1e6:.0f} MB) "
+                   f"{'larger' if 16 * n > 126e6 else 'smaller'} than L2 (126 MB); "
+                   "no flush between steps"),
+            "parallelism": f"replicas{world}"}
+
+
+def cpu_baseline(n: int):
+    """The CPU restatement on the full workload, timed once (wall clock,
+    all host threads) after one untimed warm call on a small sample."""
     from oracle import oracle as O
     from yggdrax_b200 import inputs
 
     O.build()
-    pos, mass = inputs.plummer(sample_n, 4)
-    cpu_pipeline(pos[:4096], mass[:4096])  # load + warm
-    best = None
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        cpu_pipeline(pos, mass)
-        dt = time.perf_counter() - t0
-        best = dt if best is None else min(best, dt)
-    return {"value": sample_n / best, "unit": "particles/s", "cores": O.num_threads(),
-            "kind": "port",
-            "sample": f"{sample_n} Plummer particles (seed 4), same step, wall clock, "
-                      f"best of {reps}"}
+    pos, mass = inputs.plummer(n, 4)
+    cpu_pipeline(pos[:65536], mass[:65536])  # load the library, start the thread pool
+    t0 = time.perf_counter()
+    cpu_pipeline(pos, mass)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "particles/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"the full workload ({n} Plummer particles, seed 4, radix leaf "
+                      f"{LEAF}, {MAC} theta {THETA}, exact lists), one timed run, wall "
+                      "clock, after one untimed warm call on 65,536 of the particles"}
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the path (the reference
+    itself is JAX, absent from this image) on the host cores, every step the
+    full workload of this arm."""
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
-    sample_n = args.cpu_sample
+    n = args.n
     from oracle import oracle as O
     from yggdrax_b200 import inputs
 
     O.build()
-    pos, mass = inputs.plummer(sample_n, 4)
+    pos, mass = inputs.plummer(n, 4)
     for _ in range(args.warmup):
-        cpu_pipeline(pos, mass)
+        t, r = cpu_pipeline(pos, mass)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        cpu_pipeline(pos, mass)
+        t, r = cpu_pipeline(pos, mass)
     dt = (time.perf_counter() - t0) / max(1, args.steps)
-    v = sample_n / dt
+    v = n / dt
+    cfg = workload_config(n, args.gpus, int(t.node_ranges.shape[0]), int(r["sources"].shape[0]),
+                          int(r["neighbors"].shape[0]))
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "particles/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+int64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_particles": sample_n, "parallelism": "cpu"},
+        "config": cfg,
         "cpu_baseline": {"value": v, "unit": "particles/s", "cores": O.num_threads(),
                          "kind": "port",
-                         "sample": f"{sample_n} Plummer particles (seed 4) per step; the "
-                                   "reference is JAX-only and JAX is not installed"},
+                         "sample": f"the full workload ({n} Plummer particles) every step, "
+                                   "wall clock, all host threads; the reference is JAX-only "
+                                   "and JAX is not installed"},
         "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -308,7 +327,6 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
-    ap.add_argument("--cpu-sample", type=int, default=1 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--breakdown", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
@@ -501,19 +519,15 @@ def main():
     # -- aggregate over ranks ---------------------------------------------------
     t_max, te_max, te_serial_max = _max_over_ranks([t_dev, t_e2e, t_e2e_serial], dev)
     if rank == 0:
-        cpu = None if args.no_cpu_baseline else cpu_baseline(args.cpu_sample)
+        cpu = None if args.no_cpu_baseline else cpu_baseline(n)
         line = {
             "metric": METRIC, "value": world * n / t_max, "unit": "particles/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+int64", "data": "synthetic",
-            "config": {"workload": workload_name(n), "n_particles": n, "leaf_size": LEAF,
-                       "mac": MAC, "theta": THETA, "total_nodes": total_nodes,
-                       "far_entries": far_entries, "near_entries": near_entries,
-                       "pairs_per_s": world * (far_entries + near_entries) / t_max,
-                       "l2": "inputs (268 MB) larger than L2; no flush between steps",
-                       "traversal_mode": "log", "parallelism": f"replicas{world}",
-                       "autotune": tuning},
+            "config": workload_config(n, world, total_nodes, far_entries, near_entries),
+            "pairs_per_s": world * (far_entries + near_entries) / t_max,
+            "traversal_mode": "log", "autotune": tuning,
             "e2e": {"value": world * n / te_max, "unit": "particles/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "schedule": "next step's upload overlapped with this step's compute "

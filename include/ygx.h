@@ -57,6 +57,9 @@ enum {
 #define YGX_TUNE_ROW_GRID 4    /* CTAs per SM of the short-row finalize (4..32, pow2)  */
 #define YGX_TUNE_SORT_TILE 5   /* onesweep tile: 0 16x256 keys 3/SM, 1 12x256 4/SM,     */
                                /* 2 20x256 2/SM, 3 24x256 2/SM                          */
+#define YGX_TUNE_SPIN_LIMIT 6  /* iterations a device-side wait (sort look-back) spins   */
+                               /* before it gives up and flags YGX_FLAG_TIMEOUT          */
+                               /* (0..2^24; default 2^22); not a performance knob        */
 
 /* traversal statistics words (host array of YGX_TSTAT_WORDS uint64) */
 #define YGX_TSTAT_WORDS 16
@@ -135,6 +138,12 @@ int ygx_sort_pairs(const uint64_t* keys_in, const uint32_t* values_in, int64_t n
 int ygx_sort_pairs_noalloc(const uint64_t* keys_in, const uint32_t* values_in, int64_t n,
                            int begin_bit, int end_bit, uint64_t* keys_out, uint32_t* values_out,
                            cudaStream_t stream);
+/* Status word of the last ygx_sort_pairs_noalloc call on the stream's
+ * device (YGX_FLAG_TIMEOUT: a look-back wait gave up; YGX_FLAG_BAD_INPUT: an
+ * inconsistent digit histogram), copied to host *host_flags in stream order;
+ * synchronizes the stream.  0 means the sort completed.  Allocates nothing.
+ * No counterpart in the reference. */
+int ygx_sort_pairs_noalloc_status(uint32_t* host_flags, cudaStream_t stream);
 
 /* reorder_particles_by_indices / inverse_permutation
  * (yggdrax/_tree_impl.py:900-926): any output may be NULL. */

@@ -36,6 +36,36 @@ inline float fmax_nan(float a, float b) {
 }
 inline int clz64(u64 x) { return x ? __builtin_clzll(x) : 64; }
 
+// Vector storage whose resize leaves new elements uninitialised (every
+// element is written before it is read), so growing a buffer costs no
+// serial zero fill.
+template <class T>
+struct UninitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind { using other = UninitAlloc<U>; };
+  UninitAlloc() = default;
+  template <class U>
+  UninitAlloc(const UninitAlloc<U>&) {}
+  template <class U>
+  void construct(U* p) noexcept { ::new ((void*)p) U; }
+  template <class U, class... A>
+  void construct(U* p, A&&... a) { ::new ((void*)p) U(std::forward<A>(a)...); }
+};
+typedef std::vector<i64, UninitAlloc<i64>> ivec;
+
+// Appends the per-thread buffers bufs[0..nt) to out in thread order (the
+// order of the serial loop under a static schedule), copying in parallel.
+void concat_parallel(ivec& out, std::vector<ivec>& bufs) {
+  const int nt = (int)bufs.size();
+  std::vector<size_t> off(nt + 1, out.size());
+  for (int q = 0; q < nt; ++q) off[q + 1] = off[q] + bufs[q].size();
+  out.resize(off[nt]);
+#pragma omp parallel for schedule(static, 1)
+  for (int q = 0; q < nt; ++q)
+    if (!bufs[q].empty()) std::memcpy(out.data() + off[q], bufs[q].data(), bufs[q].size() * 8);
+}
+
+
 // morton.py:22-30 (_spread3_u64)
 inline u64 spread3(u64 x) {
   x &= 0x1FFFFFull;
@@ -719,30 +749,43 @@ int ygo_geometry(const i64* node_ranges, i64 total, const i64* left, const i64* 
 // same BFS generations, records every accepted and near canonical pair
 // once, and counts decisions.  mac: 0 = bh, 1 = dehnen, 2 = engblom;
 // `ext` are the per-node MAC extents already selected and scaled.
+// Pairs are packed as (first << 32) | second (node ids stay below 2^31); a
+// pair with a missing (-1) node packs to -1 and is skipped when evaluated.
+inline i64 pack2(i64 a, i64 b) {
+  return (a < 0 || b < 0) ? -1 : (i64)(((u64)a << 32) | (u64)(uint32_t)b);
+}
+inline i64 first2(i64 p) { return (i64)((u64)p >> 32); }
+inline i64 second2(i64 p) { return (i64)(uint32_t)(u64)p; }
+
 struct WalkResult {
-  std::vector<i64> far_lo, far_hi, near_lo, near_hi;
+  ivec far, nearp;  // accepted / near canonical pairs (lo, hi), packed
   i64 accept = 0, nearc = 0, refine = 0, max_wf = 1, generations = 0;
 };
 
 void* ygo_walk(const float* center, const float* ext, const i64* left, const i64* right,
                i64 total, i64 ni, float theta_sq, int mac, i64 root) {
   WalkResult* R = new WalkResult();
-  std::vector<i64> wt{root}, ws{root};
+  ivec wf{pack2(root, root)}, nwf;
   const float theta = std::sqrt(theta_sq);
-  int nt = omp_get_max_threads();
-  while (!wt.empty()) {
+  const int nt = omp_get_max_threads();
+  // per-thread buffers, kept (with their capacity) across generations; each
+  // thread fills private copies and swaps them in (no shared cache lines)
+  std::vector<ivec> nt_w(nt), fl(nt), nl(nt);
+  while (!wf.empty()) {
     R->generations++;
-    i64 W = (i64)wt.size();
-    std::vector<std::vector<i64>> nt_t(nt), nt_s(nt), fl(nt), fh(nt), nl(nt), nh(nt);
+    const i64 W = (i64)wf.size();
     std::vector<i64> acc(nt, 0), nrc(nt, 0), ref(nt, 0);
-#pragma omp parallel
+#pragma omp parallel num_threads(nt)
     {
-      int tid = omp_get_thread_num();
-      auto& Pt = nt_t[tid]; auto& Ps = nt_s[tid];
+      const int tid = omp_get_thread_num();
+      ivec Pw, Fl, Nl;
+      Pw.swap(nt_w[tid]); Fl.swap(fl[tid]); Nl.swap(nl[tid]);
+      Pw.clear(); Fl.clear(); Nl.clear();
+      i64 a_ = 0, n_ = 0, r_ = 0;
 #pragma omp for schedule(static)
       for (i64 k = 0; k < W; ++k) {
-        i64 t = wt[k], s = ws[k];
-        if (t < 0 || s < 0) continue;
+        if (wf[k] < 0) continue;
+        const i64 t = first2(wf[k]), s = second2(wf[k]);
         float dx = center[3 * t] - center[3 * s];
         float dy = center[3 * t + 1] - center[3 * s + 1];
         float dz = center[3 * t + 2] - center[3 * s + 2];
@@ -763,20 +806,20 @@ void* ygo_walk(const float* center, const float* ext, const i64* left, const i64
         bool mac_ok = diff && (d2 > 0.0f) && ok;
         bool t_int = t < ni, s_int = s < ni;
         if (mac_ok) {
-          acc[tid]++;
-          fl[tid].push_back(t); fh[tid].push_back(s);
+          a_++;
+          Fl.push_back(pack2(t, s));
           continue;
         }
         if (!t_int && !s_int && diff) {
-          nrc[tid]++;
-          nl[tid].push_back(t); nh[tid].push_back(s);
+          n_++;
+          Nl.push_back(pack2(t, s));
           continue;
         }
-        ref[tid]++;
+        r_++;
         bool same = t == s;
         bool st = t_int && (same || !s_int || et >= es);
         bool ss = s_int && (same || !t_int || es > et);
-        auto push = [&](i64 a, i64 b) { Pt.push_back(std::min(a, b)); Ps.push_back(std::max(a, b)); };
+        auto push = [&](i64 a, i64 b) { Pw.push_back(pack2(std::min(a, b), std::max(a, b))); };
         if (st && ss) {
           if (same) {
             push(left[t], left[t]); push(left[t], right[t]); push(right[t], right[t]);
@@ -790,18 +833,16 @@ void* ygo_walk(const float* center, const float* ext, const i64* left, const i64
           push(t, left[s]); push(t, right[s]);
         }
       }
+      acc[tid] = a_; nrc[tid] = n_; ref[tid] = r_;
+      nt_w[tid].swap(Pw); fl[tid].swap(Fl); nl[tid].swap(Nl);
     }
-    wt.clear(); ws.clear();
-    for (int q = 0; q < nt; ++q) {
-      wt.insert(wt.end(), nt_t[q].begin(), nt_t[q].end());
-      ws.insert(ws.end(), nt_s[q].begin(), nt_s[q].end());
-      R->far_lo.insert(R->far_lo.end(), fl[q].begin(), fl[q].end());
-      R->far_hi.insert(R->far_hi.end(), fh[q].begin(), fh[q].end());
-      R->near_lo.insert(R->near_lo.end(), nl[q].begin(), nl[q].end());
-      R->near_hi.insert(R->near_hi.end(), nh[q].begin(), nh[q].end());
-      R->accept += acc[q]; R->nearc += nrc[q]; R->refine += ref[q];
-    }
-    R->max_wf = std::max<i64>(R->max_wf, (i64)wt.size());
+    nwf.clear();
+    concat_parallel(nwf, nt_w);
+    concat_parallel(R->far, fl);
+    concat_parallel(R->nearp, nl);
+    for (int q = 0; q < nt; ++q) { R->accept += acc[q]; R->nearc += nrc[q]; R->refine += ref[q]; }
+    wf.swap(nwf);
+    R->max_wf = std::max<i64>(R->max_wf, (i64)wf.size());
     if (R->generations > 100000) break;
   }
   return R;
@@ -810,7 +851,7 @@ void* ygo_walk(const float* center, const float* ext, const i64* left, const i64
 // sizes: [num_far_pairs, num_near_pairs, accept, near, refine, max_wf, generations]
 void ygo_walk_sizes(void* h, i64* out) {
   WalkResult* R = (WalkResult*)h;
-  out[0] = (i64)R->far_lo.size(); out[1] = (i64)R->near_lo.size();
+  out[0] = (i64)R->far.size(); out[1] = (i64)R->nearp.size();
   out[2] = R->accept; out[3] = R->nearc; out[4] = R->refine; out[5] = R->max_wf;
   out[6] = R->generations;
 }
@@ -826,36 +867,54 @@ void ygo_walk_lists(void* h, i64 total, const i64* nodes_by_level, const i64* le
                     i64 L, i64* far_counts, i64* node_offsets, i64* far_sources,
                     i64* far_targets, i64* near_counts, i64* near_offsets,
                     i64* near_neighbors) {
+  // Rows are sorted at the end, so entries may be placed in any order: the
+  // scatters run in parallel with atomic row cursors.
   WalkResult* R = (WalkResult*)h;
-  const i64 P = (i64)R->far_lo.size();
-  std::vector<i64> rank(total);
-  for (i64 r = 0; r < total; ++r) rank[nodes_by_level[r]] = r;
+  const i64 P = (i64)R->far.size();
+  const i64* fp = R->far.data();
   std::vector<i64> cnt(total, 0);
-  for (i64 k = 0; k < P; ++k) { cnt[R->far_lo[k]]++; cnt[R->far_hi[k]]++; }
+#pragma omp parallel for schedule(static)
+  for (i64 k = 0; k < P; ++k) {
+    __atomic_fetch_add(&cnt[first2(fp[k])], 1, __ATOMIC_RELAXED);
+    __atomic_fetch_add(&cnt[second2(fp[k])], 1, __ATOMIC_RELAXED);
+  }
   std::vector<i64> start(total + 1, 0);  // by rank
   for (i64 r = 0; r < total; ++r) start[r + 1] = start[r] + cnt[nodes_by_level[r]];
-  for (i64 v = 0; v < total; ++v) { far_counts[v] = cnt[v]; node_offsets[v] = start[rank[v]]; }
+#pragma omp parallel for schedule(static)
+  for (i64 r = 0; r < total; ++r) {
+    const i64 v = nodes_by_level[r];
+    far_counts[v] = cnt[v];
+    node_offsets[v] = start[r];
+  }
   node_offsets[total] = 2 * P;
-  std::vector<i64> cur(total);
-  for (i64 v = 0; v < total; ++v) cur[v] = node_offsets[v];
+  std::vector<i64> cur(node_offsets, node_offsets + total);
+#pragma omp parallel for schedule(static)
   for (i64 k = 0; k < P; ++k) {
-    i64 a = R->far_lo[k], b = R->far_hi[k];
-    far_sources[cur[a]] = b; far_targets[cur[a]++] = a;
-    far_sources[cur[b]] = a; far_targets[cur[b]++] = b;
+    const i64 a = first2(fp[k]), b = second2(fp[k]);
+    const i64 pa = __atomic_fetch_add(&cur[a], 1, __ATOMIC_RELAXED);
+    far_sources[pa] = b; far_targets[pa] = a;
+    const i64 pb = __atomic_fetch_add(&cur[b], 1, __ATOMIC_RELAXED);
+    far_sources[pb] = a; far_targets[pb] = b;
   }
 #pragma omp parallel for schedule(dynamic, 256)
   for (i64 v = 0; v < total; ++v)
     std::sort(far_sources + node_offsets[v], far_sources + node_offsets[v] + cnt[v]);
-  const i64 Q = (i64)R->near_lo.size();
+  const i64 Q = (i64)R->nearp.size();
+  const i64* np_ = R->nearp.data();
   std::vector<i64> ncnt(L, 0);
-  for (i64 k = 0; k < Q; ++k) { ncnt[leaf_position[R->near_lo[k]]]++; ncnt[leaf_position[R->near_hi[k]]]++; }
+#pragma omp parallel for schedule(static)
+  for (i64 k = 0; k < Q; ++k) {
+    __atomic_fetch_add(&ncnt[leaf_position[first2(np_[k])]], 1, __ATOMIC_RELAXED);
+    __atomic_fetch_add(&ncnt[leaf_position[second2(np_[k])]], 1, __ATOMIC_RELAXED);
+  }
   near_offsets[0] = 0;
   for (i64 j = 0; j < L; ++j) { near_counts[j] = ncnt[j]; near_offsets[j + 1] = near_offsets[j] + ncnt[j]; }
   std::vector<i64> ncur(near_offsets, near_offsets + L);
+#pragma omp parallel for schedule(static)
   for (i64 k = 0; k < Q; ++k) {
-    i64 a = R->near_lo[k], b = R->near_hi[k];
-    near_neighbors[ncur[leaf_position[a]]++] = b;
-    near_neighbors[ncur[leaf_position[b]]++] = a;
+    const i64 a = first2(np_[k]), b = second2(np_[k]);
+    near_neighbors[__atomic_fetch_add(&ncur[leaf_position[a]], 1, __ATOMIC_RELAXED)] = b;
+    near_neighbors[__atomic_fetch_add(&ncur[leaf_position[b]], 1, __ATOMIC_RELAXED)] = a;
   }
 #pragma omp parallel for schedule(dynamic, 256)
   for (i64 j = 0; j < L; ++j)

@@ -1,14 +1,15 @@
 """Generate golden fixtures by running the reference yggdrax source.
 
-Run in a container that has the reference checkout (default
-/root/reference/yggdrax) but no JAX: the reference modules are imported over
+Run in a container that has the reference checkout (its package directory,
+the one holding ``tree.py``, is a required argument) but no JAX: the
+reference modules are imported over
 ``jaxshim`` (NumPy with JAX's indexing / scatter / search semantics) and
 executed on small seeded inputs.  The outputs are written as ``*.npz`` next
 to this script and are what ``tests/test_golden.py`` checks the oracle
 against.  Within-row order of the interaction / neighbour lists is
 unspecified in the reference (unstable argsort), so rows are stored sorted.
 
-Usage: python tests/golden/make_golden.py [reference_package_dir]
+Usage: python tests/golden/make_golden.py REFERENCE_PACKAGE_DIR
        [--mutual-only | --buffers-only | --moments-only | --octwalk-only]
 """
 
@@ -379,7 +380,11 @@ def main(root: str) -> None:
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    ref = args[0] if args else "/root/reference/yggdrax"
+    if len(args) != 1 or not os.path.isfile(os.path.join(args[0], "tree.py")):
+        sys.exit("usage: make_golden.py REFERENCE_PACKAGE_DIR [--mutual-only | --buffers-only"
+                 " | --moments-only | --octwalk-only]\n(the directory of the reference's"
+                 " yggdrax package, which holds tree.py)")
+    ref = args[0]
     if "--mutual-only" in sys.argv:
         mutual(ref)
     elif "--buffers-only" in sys.argv:

@@ -142,3 +142,54 @@ def test_graph_pipeline_replays_equal_the_ordinary_path(cuda_device):
         assert not small.last_replayed and small.captures == 2 + k
         for a, b in zip(got, ref):
             assert np.array_equal(a, b)
+
+
+def test_batched_c4_workload_sampled_sets_match_oracle(cuda_device, oracle):
+    """The full batched workload (4096 sets, sizes floor(exp(U[ln 256,
+    ln 65536])), half uniform cubes, half Plummer spheres, seed 3; about 48M
+    points) built, measured and walked in one pass per stage; 48 sampled sets
+    plus the smallest and the largest compared with the oracle run on that
+    set alone (radix leaf 16, dehnen 0.6): topology, geometry and lists, bit
+    for bit."""
+    import torch
+
+    from yggdrax_b200 import batch as B
+    from yggdrax_b200 import inputs
+
+    pos, mass, off = inputs.batched_sets(4096, 3)
+    P = torch.from_numpy(pos).to(cuda_device)
+    M = torch.from_numpy(mass).to(cuda_device)
+    bt = B.build_trees_batched(P, M, off, leaf_size=16)
+    bg = B.compute_tree_geometry_batched(bt)
+    bi = B.build_interactions_and_neighbors_batched(bt, bg, theta=0.6, mac_type="dehnen")
+    sizes = np.diff(off)
+    rng = np.random.default_rng(17)
+    pick = set(rng.choice(4096, size=48, replace=False).tolist())
+    pick |= {int(np.argmin(sizes)), int(np.argmax(sizes))}
+    for i in sorted(pick):
+        a, b = int(off[i]), int(off[i + 1])
+        ot = oracle.build_tree(pos[a:b], mass[a:b], leaf_size=16)
+        tb = bt.tree(i)
+        for f in ("parent", "left_child", "right_child", "particle_indices", "morton_codes",
+                  "node_ranges", "node_level", "level_offsets", "nodes_by_level",
+                  "bounds_min", "bounds_max", "leaf_codes"):
+            _eq(f"set {i} {f}", getattr(tb, f), getattr(ot, f))
+        _eq(f"set {i} positions_sorted", bt.positions_sorted[a:b], ot.positions_sorted)
+        og = oracle.compute_tree_geometry(ot, ot.positions_sorted)
+        gb = bg.geometry(bt, i)
+        for f in ("center", "half_extent", "radius", "max_extent"):
+            _eq(f"set {i} {f}", getattr(gb, f), getattr(og, f))
+        if ot.num_internal_nodes == 0:
+            continue
+        r = oracle.build_interactions_and_neighbors(ot, og, theta=0.6, mac_type="dehnen")
+        fb, nb = bi.lists(bt, i)
+        _eq(f"set {i} far.counts", fb.counts, r["far_counts"])
+        _eq(f"set {i} far.offsets", fb.offsets, r["offsets"])
+        _eq(f"set {i} far.sources", fb.sources, r["sources"])
+        _eq(f"set {i} far.targets", fb.targets, r["targets"])
+        _eq(f"set {i} far.level_offsets", fb.level_offsets, r["level_offsets"])
+        _eq(f"set {i} far.target_levels", fb.target_levels, r["target_levels"])
+        _eq(f"set {i} near.counts", nb.counts, r["near_counts"])
+        _eq(f"set {i} near.offsets", nb.offsets, r["near_offsets"])
+        _eq(f"set {i} near.neighbors", nb.neighbors, r["neighbors"])
+        _eq(f"set {i} near.leaf_indices", nb.leaf_indices, r["leaf_indices"])

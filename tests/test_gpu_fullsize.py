@@ -2,9 +2,13 @@
 
 * 4,194,304-particle Plummer sphere, octree build, leaf 32, dehnen 0.6 and
   bh 0.5: tree, geometry and lists equal to the oracle's, bit for bit.
-* 16,777,216-particle Plummer sphere (radix, leaf 32, dehnen 0.6) and the
-  16,777,216-point clump mixture (fixed-depth octree with local refinement,
-  dehnen 0.6): size-independent properties -- the sort is a permutation in
+* The benchmarked workload -- 16,777,216 Plummer particles (seed 4), radix
+  leaf 32, dehnen 0.6, exact lists -- and the 16,777,216-point clump mixture
+  (seed 2, fixed-depth octree, max_depth 10, local refinement, dehnen 0.6):
+  tree, octree tables, geometry, far / near lists and decision counts equal
+  to the oracle's, bit for bit.
+* The same two workloads through size-independent properties as well
+  (cheap, and independent of the oracle): the sort is a permutation in
   code order, the far and near lists are symmetric, every sampled far entry
   passes the MAC and every sampled near entry fails it (recomputed in the
   reference's fp32 order), and for sampled leaves every other particle is
@@ -195,5 +199,77 @@ def test_c3_clumps_16m_fixed_depth_properties(cuda_device):
         # the dense buffers at this size exceed the device, as in the reference
         with pytest.raises(MemoryError):
             yb.densify_interactions(t, g, inter)
+    finally:
+        yb.set_reference_limits(True)
+
+
+def _compare_full(gt, ps, gg, ot, og, gi, gn, res, r, octree: bool):
+    """Every output of the GPU pipeline against the oracle's (bit for bit),
+    freeing host copies as it goes."""
+    from test_gpu_parity import RADIX_FIELDS, _assert_eq, _compare_lists
+
+    topo = gt.topology
+    for f in RADIX_FIELDS:
+        _assert_eq(f, _np(getattr(topo, f)), getattr(ot, f))
+    assert int(topo.num_levels) == ot.num_levels
+    _assert_eq("positions_sorted", _np(ps), ot.positions_sorted)
+    if octree:
+        for f in ("oct_parent", "oct_children", "oct_node_codes", "oct_node_depths",
+                  "oct_node_ranges", "oct_level_offsets", "oct_leaf_nodes",
+                  "radix_node_to_oct", "radix_leaf_to_oct"):
+            _assert_eq(f, _np(getattr(gt, f)), ot.octree[f])
+    for f in ("center", "half_extent", "radius", "max_extent"):
+        _assert_eq(f, _np(getattr(gg, f)), getattr(og, f))
+    _compare_lists(gi, gn, r)
+    assert int(res.accept_decisions) == r["accept_decisions"]
+    assert int(res.near_decisions) == r["near_decisions"]
+    assert int(res.refine_decisions) == r["refine_decisions"]
+
+
+def test_c5_plummer_16m_matches_oracle(cuda_device, oracle):
+    """The benchmarked workload, bit for bit against the oracle."""
+    import torch
+
+    import yggdrax_b200 as yb
+    from yggdrax_b200 import inputs
+
+    pos, mass = inputs.plummer(16_777_216, 4)
+    P, M = torch.from_numpy(pos).to(cuda_device), torch.from_numpy(mass).to(cuda_device)
+    yb.set_reference_limits(False)
+    try:
+        gt, ps = yb.build_tree(P, M, leaf_size=32, return_reordered=True)[:2]
+        gg = yb.compute_tree_geometry(gt, ps)
+        gi, gn, res = yb.build_interactions_and_neighbors(gt, gg, theta=0.6, mac_type="dehnen",
+                                                          return_result=True)
+        del P, M
+        ot = oracle.build_tree(pos, mass, leaf_size=32)
+        og = oracle.compute_tree_geometry(ot, ot.positions_sorted)
+        r = oracle.build_interactions_and_neighbors(ot, og, theta=0.6, mac_type="dehnen")
+        _compare_full(gt, ps, gg, ot, og, gi, gn, res, r, octree=False)
+    finally:
+        yb.set_reference_limits(True)
+
+
+def test_c3_clumps_16m_matches_oracle(cuda_device, oracle):
+    """The clump mixture on the fixed-depth octree, bit for bit against the
+    oracle (octree tables included)."""
+    import torch
+
+    import yggdrax_b200 as yb
+    from yggdrax_b200 import inputs
+
+    pos, mass = inputs.plummer_clumps(16_777_216, 2)
+    P, M = torch.from_numpy(pos).to(cuda_device), torch.from_numpy(mass).to(cuda_device)
+    yb.set_reference_limits(False)
+    try:
+        gt, ps = yb.build_fixed_depth_octree(P, M, max_depth=10, return_reordered=True)[:2]
+        gg = yb.compute_tree_geometry(gt, ps)
+        gi, gn, res = yb.build_interactions_and_neighbors(gt, gg, theta=0.6, mac_type="dehnen",
+                                                          return_result=True)
+        del P, M
+        ot = oracle.build_fixed_depth_octree(pos, mass, max_depth=10)
+        og = oracle.compute_tree_geometry(ot, ot.positions_sorted)
+        r = oracle.build_interactions_and_neighbors(ot, og, theta=0.6, mac_type="dehnen")
+        _compare_full(gt, ps, gg, ot, og, gi, gn, res, r, octree=True)
     finally:
         yb.set_reference_limits(True)

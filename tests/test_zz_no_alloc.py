@@ -5,8 +5,11 @@ example an XLA custom-call handler registered without a scratch request,
 whose framework already holds the GPU's memory pool.  Its scratch is a fixed
 array inside libygx.so, so these tests check, through the C ABI, that two
 calls in a row (sharing that array) each match the workspace-based
-ygx_sort_pairs exactly, and that sizes above the array's limit are refused.
-This file sorts last so a failure here never hides another test's result.
+ygx_sort_pairs exactly, that the array's status word reads 0 after each
+call (ygx_sort_pairs_noalloc_status), that the value-less and in-place forms
+sort stably under the default and a non-default tile shape, and that sizes
+above the array's limit are refused.  This file sorts last so a failure here
+never hides another test's result.
 """
 
 import numpy as np
@@ -42,6 +45,13 @@ def _sort_noalloc(lib, L, keys, vals, bits, dev):
     return ko, vo
 
 
+def _noalloc_flags(lib, L, dev):
+    flags = np.zeros(1, np.uint32)
+    L.check(lib.ygx_sort_pairs_noalloc_status(flags.ctypes.data, L.stream_handle(dev)),
+            "ygx_sort_pairs_noalloc_status")
+    return int(flags[0])
+
+
 def test_noalloc_sort_matches_workspace_sort_twice(cuda_device):
     import torch
 
@@ -59,6 +69,7 @@ def test_noalloc_sort_matches_workspace_sort_twice(cuda_device):
         vals = torch.from_numpy(vals_np).to(cuda_device)
         k_ref, v_ref = _sort_with_workspace(lib, L, keys, vals, bits, cuda_device)
         k_na, v_na = _sort_noalloc(lib, L, keys, vals, bits, cuda_device)
+        assert _noalloc_flags(lib, L, cuda_device) == 0
         torch.cuda.synchronize(cuda_device)
         assert torch.equal(k_na, k_ref)
         assert torch.equal(v_na, v_ref)
@@ -79,3 +90,45 @@ def test_noalloc_sort_rejects_sizes_above_its_limit(cuda_device):
     rc = lib.ygx_sort_pairs_noalloc(L.ptr(keys), None, n, 0, 8, L.ptr(ko), L.ptr(vo),
                                     L.stream_handle(cuda_device))
     assert rc == YGX_ERR_TOO_LARGE
+
+
+@pytest.mark.parametrize("tile", [0, 2])
+def test_noalloc_sort_without_values_and_in_place(cuda_device, tile):
+    """values_in == NULL (each value is the input position) and keys_in ==
+    keys_out (the input is staged inside the shared array first), at the
+    array's key limit, under the default and one other tile shape."""
+    import torch
+
+    from yggdrax_b200 import _lib as L
+
+    lib = L.lib()
+    old = np.zeros(1, np.int32)
+    L.check(lib.ygx_tune_get(L.TUNE["sort_tile"], old.ctypes.data), "ygx_tune_get")
+    L.check(lib.ygx_tune_set(L.TUNE["sort_tile"], tile), "ygx_tune_set")
+    try:
+        rng = np.random.default_rng(12 + tile)
+        n = MAX_KEYS
+        keys_np = rng.integers(0, 1 << 20, size=n, dtype=np.uint64)  # many ties
+        order = np.argsort(keys_np, kind="stable")
+        st = L.stream_handle(cuda_device)
+        # no values: positions travel with the keys
+        keys = torch.from_numpy(keys_np).to(cuda_device)
+        ko = torch.empty_like(keys)
+        vo = torch.empty(n, dtype=torch.int32, device=cuda_device)
+        L.check(lib.ygx_sort_pairs_noalloc(L.ptr(keys), None, n, 0, 20, L.ptr(ko), L.ptr(vo),
+                                           st), "ygx_sort_pairs_noalloc")
+        assert _noalloc_flags(lib, L, cuda_device) == 0
+        np.testing.assert_array_equal(vo.cpu().numpy(), order.astype(np.int32))
+        np.testing.assert_array_equal(ko.cpu().numpy(), keys_np[order])
+        # in place: keys_in is keys_out
+        vals_np = rng.permutation(n).astype(np.int32)
+        kio = torch.from_numpy(keys_np.copy()).to(cuda_device)
+        vals = torch.from_numpy(vals_np).to(cuda_device)
+        vo2 = torch.empty(n, dtype=torch.int32, device=cuda_device)
+        L.check(lib.ygx_sort_pairs_noalloc(L.ptr(kio), L.ptr(vals), n, 0, 20, L.ptr(kio),
+                                           L.ptr(vo2), st), "ygx_sort_pairs_noalloc")
+        assert _noalloc_flags(lib, L, cuda_device) == 0
+        np.testing.assert_array_equal(kio.cpu().numpy(), keys_np[order])
+        np.testing.assert_array_equal(vo2.cpu().numpy(), vals_np[order])
+    finally:
+        L.check(lib.ygx_tune_set(L.TUNE["sort_tile"], int(old[0])), "ygx_tune_set")

@@ -37,7 +37,8 @@ FLAG_MALFORMED = 1 << 4
 FLAG_BAD_INPUT = 1 << 5
 FLAG_LOG_OVERFLOW = 1 << 6
 WALK_LOG = 0
-TUNE = dict(sort_rank=0, sort_skew=1, walk_blocks=2, refit_warps=3, row_grid=4, sort_tile=5)
+TUNE = dict(sort_rank=0, sort_skew=1, walk_blocks=2, refit_warps=3, row_grid=4, sort_tile=5,
+            spin_limit=6)
 WALK_COUNT = 1
 
 TSTAT_WORDS = 16
@@ -70,6 +71,7 @@ _SIGS = {
     "ygx_sort_pairs_workspace_size": (SZ, [I64]),
     "ygx_sort_pairs": (I32, [P, P, I64, I32, I32, P, P, P, SZ, P]),
     "ygx_sort_pairs_noalloc": (I32, [P, P, I64, I32, I32, P, P, P]),
+    "ygx_sort_pairs_noalloc_status": (I32, [P, P]),
     "ygx_reorder": (I32, [P, P, P, I64, I32, P, P, P, P, P]),
     "ygx_leaves_adaptive": (I32, [P, I64, I64, I32, P, P, P, P, P]),
     "ygx_leaves_fixed": (I32, [P, I64, I32, I32, P, P, P, P, P]),

@@ -21,6 +21,7 @@ struct Tune {
   int refit_warps = 8;         // warps per CTA of the leaf refit
   int row_grid_per_sm = 16;    // CTAs per SM of the short-row finalize kernels
   int sort_tile = 0;           // onesweep tile shape (index into kSortShape, sort.cuh)
+  int spin_limit = 1 << 22;    // iterations of a device-side wait before it gives up
 };
 extern Tune g_tune;
 
@@ -37,12 +38,11 @@ enum StatusFlag : uint32_t {
   kFlagLogOverflow = 1u << 6,
 };
 
-// Iteration limit of every device-side spin (decoupled look-back).  A wait
-// this long means a producer did not make progress; the waiter records
+// Iteration limit of every device-side spin (decoupled look-back), passed to
+// the kernels from g_tune.spin_limit (knob YGX_TUNE_SPIN_LIMIT).  A wait this
+// long means a producer did not make progress; the waiter records
 // kFlagTimeout and continues with what it has, so the launch always ends.
-#ifndef YGX_SPIN_LIMIT
-#define YGX_SPIN_LIMIT (1u << 22)
-#endif
+constexpr int kSpinLimitMax = 1 << 24;
 
 __device__ __forceinline__ void raise_flag(uint32_t* status, uint32_t f) {
   if (status) atomicOr(status, f);

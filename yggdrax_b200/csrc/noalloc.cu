@@ -17,6 +17,12 @@
 // zero.  Two calls whose work overlaps on the GPU (different streams, or
 // different host threads without ordering) race on the array and corrupt
 // each other's results -- order such calls on one stream.
+//
+// The first 4 bytes of the array are the sort's status word (YGX_FLAG_*
+// bits: a look-back wait that gave up, an inconsistent histogram).  Each
+// call zeroes it before sorting; ygx_sort_pairs_noalloc_status reads it back
+// after a call, so a caller can tell a complete sort from one that was cut
+// short.
 #include <mutex>
 
 #include "sort.cuh"
@@ -29,25 +35,58 @@ constexpr size_t kNoAllocBytes = size_t(4) << 20;      // 4 MiB per GPU
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
+// cuCtxGetCurrent, reached through the runtime's driver entry point so the
+// library needs no link against libcuda.
+typedef int (*CtxGetCurrentFn)(void** ctx);
+
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
-void* g_scratch_ptr[kMaxDevices] = {};
+struct ScratchSlot {
+  void* ptr = nullptr;
+  void* ctx = nullptr;  // context the address belongs to
+};
+ScratchSlot g_scratch[kMaxDevices];
 
-// Device address of g_noalloc_scratch on the current device.  The host-side
-// name of a __device__ array is only a stand-in, so the address is looked up
-// once per device (with that device current) and cached.
-int scratch_address(void** out) {
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (CtxGetCurrentFn) nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
+
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the array's name is only a stand-in, so the address is looked up with
+// cudaGetSymbolAddress, with the device current, and cached per device
+// together with the context it was taken in: after cudaDeviceReset the
+// module is loaded again into a new context and the array may sit
+// elsewhere, so a changed context triggers a fresh look-up.  (Where the
+// driver entry point is unavailable the address is looked up on every call.)
+// The stream must belong to the current device.
+int scratch_address(cudaStream_t stream, void** out) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess) return YGX_ERR_CUDA;
   if (dev < 0 || dev >= kMaxDevices) return YGX_ERR_ARG;
+  int sdev = -1;
+  if (cudaStreamGetDevice(stream, &sdev) != cudaSuccess) return YGX_ERR_ARG;
+  if (sdev != dev) return YGX_ERR_ARG;
+  void* ctx = nullptr;
+  CtxGetCurrentFn get = ctx_get_current();
+  const bool have_ctx = get != nullptr && get(&ctx) == 0 && ctx != nullptr;
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (g_scratch_ptr[dev] == nullptr) {
+  ScratchSlot& s = g_scratch[dev];
+  if (s.ptr == nullptr || !have_ctx || s.ctx != ctx) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr) return YGX_ERR_CUDA;
-    g_scratch_ptr[dev] = p;
+    s.ptr = p;
+    s.ctx = have_ctx ? ctx : nullptr;
   }
-  *out = g_scratch_ptr[dev];
+  *out = s.ptr;
   return YGX_OK;
 }
 
@@ -64,7 +103,7 @@ int ygx_sort_pairs_noalloc(const uint64_t* keys_in, const uint32_t* values_in, i
   if (ygx::onesweep_scratch_bytes(ygx::kNoAllocMaxKeys) + 256 > ygx::kNoAllocBytes)
     return YGX_ERR_ARG;  // layout does not fit (build-time sizing error)
   void* base = nullptr;
-  int rc = ygx::scratch_address(&base);
+  int rc = ygx::scratch_address(stream, &base);
   if (rc != YGX_OK) return rc;
   ygx::Arena a{(char*)base, 0, ygx::kNoAllocBytes};
   uint32_t* status = a.take<uint32_t>(64);
@@ -73,6 +112,20 @@ int ygx_sort_pairs_noalloc(const uint64_t* keys_in, const uint32_t* values_in, i
   if (cudaMemsetAsync(status, 0, sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
   return ygx::onesweep_sort(keys_in, values_in, n, begin_bit, end_bit, keys_out, values_out, s,
                             false, status, stream);
+}
+
+int ygx_sort_pairs_noalloc_status(uint32_t* host_flags, cudaStream_t stream) {
+  if (!host_flags) return YGX_ERR_ARG;
+  void* base = nullptr;
+  int rc = ygx::scratch_address(stream, &base);
+  if (rc != YGX_OK) return rc;
+  uint32_t v = 0;
+  if (cudaMemcpyAsync(&v, base, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
+      cudaSuccess)
+    return YGX_ERR_CUDA;
+  if (cudaStreamSynchronize(stream) != cudaSuccess) return YGX_ERR_CUDA;
+  *host_flags = v;
+  return YGX_OK;
 }
 
 }  // extern "C"

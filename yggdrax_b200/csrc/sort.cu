@@ -89,7 +89,8 @@ __global__ void __launch_bounds__(kSortThreads, kBlocksPerSM)
                int64_t n, int shift, const uint32_t* __restrict__ digit_offsets,
                uint32_t* __restrict__ lookback, uint32_t* __restrict__ ticket_counter,
                uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
-               const uint32_t* __restrict__ rank_mode, uint32_t* __restrict__ status) {
+               const uint32_t* __restrict__ rank_mode, uint32_t* __restrict__ status,
+               uint32_t spin_limit) {
   using Smem = OnesweepSmem<kItems>;
   static_assert(offsetof(Smem, keys) % 16 == 0, "key staging area is 16-byte aligned");
   constexpr int kSortItems = kItems;
@@ -163,7 +164,7 @@ __global__ void __launch_bounds__(kSortThreads, kBlocksPerSM)
         if ((w & ~kCountMask) == 0) {
           const uint32_t* p = lookback + (size_t)(j - k) * kSortRadix + d;
           uint32_t spins = 0;
-          while ((w & ~kCountMask) == 0 && spins < YGX_SPIN_LIMIT) {
+          while ((w & ~kCountMask) == 0 && spins < spin_limit) {
             __nanosleep(32);
             w = ld_volatile_u32(p);
             ++spins;
@@ -312,6 +313,7 @@ struct OnesweepPass {
   uint32_t* vals_out;
   const uint32_t* rank_mode;
   uint32_t* status;
+  uint32_t spin_limit;
 };
 
 template <int kItems, int kBlocksPerSM>
@@ -326,11 +328,11 @@ cudaError_t launch_onesweep(const OnesweepPass& a, unsigned tiles, cudaStream_t 
   if (a.vals_in == nullptr)
     k_onesweep<true, kItems, kBlocksPerSM><<<tiles, kSortThreads, smem, st>>>(
         a.keys_in, nullptr, a.n, a.shift, a.offsets, a.lookback, a.counter, a.keys_out,
-        a.vals_out, a.rank_mode, a.status);
+        a.vals_out, a.rank_mode, a.status, a.spin_limit);
   else
     k_onesweep<false, kItems, kBlocksPerSM><<<tiles, kSortThreads, smem, st>>>(
         a.keys_in, a.vals_in, a.n, a.shift, a.offsets, a.lookback, a.counter, a.keys_out,
-        a.vals_out, a.rank_mode, a.status);
+        a.vals_out, a.rank_mode, a.status, a.spin_limit);
   note_launch();
   return cudaGetLastError();
 }
@@ -410,6 +412,7 @@ int onesweep_sort(const uint64_t* keys_in, const uint32_t* vals_in, int64_t n, i
     a.vals_out = dv;
     a.rank_mode = s.rank_mode + p;
     a.status = status;
+    a.spin_limit = (uint32_t)g_tune.spin_limit;
     cudaError_t e;
     switch (shape) {
       case 1: e = launch_onesweep<12, 4>(a, (unsigned)tiles, st); break;

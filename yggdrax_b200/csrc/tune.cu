@@ -16,6 +16,7 @@ bool legal(int knob, int v) {
     case YGX_TUNE_REFIT_WARPS: return v == 2 || v == 4 || v == 8;
     case YGX_TUNE_ROW_GRID: return v == 4 || v == 8 || v == 16 || v == 32;
     case YGX_TUNE_SORT_TILE: return v >= 0 && v < kSortTileShapes;
+    case YGX_TUNE_SPIN_LIMIT: return v >= 0 && v <= kSpinLimitMax;
     default: return false;
   }
 }
@@ -27,6 +28,7 @@ int* slot(int knob) {
     case YGX_TUNE_REFIT_WARPS: return &g_tune.refit_warps;
     case YGX_TUNE_ROW_GRID: return &g_tune.row_grid_per_sm;
     case YGX_TUNE_SORT_TILE: return &g_tune.sort_tile;
+    case YGX_TUNE_SPIN_LIMIT: return &g_tune.spin_limit;
     default: return nullptr;
   }
 }

@@ -667,13 +667,35 @@ def _node_order_far_pairs(w, total: int, dev):
     return no.to(idt), raw_src, raw_tgt, tags, fpc
 
 
-def _check_capacities(w: _WalkOut, total: int, ni: int, *, max_interactions_per_node,
-                      max_neighbors_per_leaf, max_pair_queue, process_block,
-                      traversal_config, collect_far: bool = True,
-                      collect_near: bool = True) -> None:
+def _check_capacities(w: _WalkOut, total: int, ni: int, **kw) -> None:
     """Raise where the reference's runner (_run_dual_tree_walk_raw,
     :3840-4440) would raise on the same pair sets (a far-only or near-only
     run checks only the lists it collects)."""
+    v = _capacity_violations(w, total, ni, **kw)
+    if v:
+        raise RuntimeError(v[0][1])
+
+
+def _overflow_flags(w: _WalkOut, total: int, ni: int, **kw) -> tuple:
+    """``(queue_overflow, far_overflow, near_overflow)`` of the reference's
+    padded walk (_dual_tree_walk_impl, :1119-1905) with the capacities the
+    caller gave, evaluated on the exact walk's maxima: the flags its
+    ``DualTreeWalkResult`` would carry where it returns them instead of
+    raising (:4417-4421).  The count-then-fill schedule (no capacities)
+    never overflows its exact-size buffers: all False there."""
+    kinds = {k for k, _ in _capacity_violations(w, total, ni, **kw)}
+    return ("queue" in kinds, "far" in kinds, "near" in kinds)
+
+
+def _capacity_violations(w: _WalkOut, total: int, ni: int, *, max_interactions_per_node,
+                         max_neighbors_per_leaf, max_pair_queue, process_block,
+                         traversal_config, collect_far: bool = True,
+                         collect_near: bool = True) -> list:
+    """Every check of the reference's runner that the walk's maxima fail, as
+    ``(kind, message)`` in the order the runner tests them; kind is
+    ``queue`` / ``far`` / ``near`` for the padded walk's overflow flags and
+    ``count`` for the count-then-fill schedule's own errors."""
+    out = []
     s = dict(w.stats)
     if not collect_far:
         s["max_far"] = s["far_total"] = 0
@@ -686,18 +708,18 @@ def _check_capacities(w: _WalkOut, total: int, ni: int, *, max_interactions_per_
         conservative = max(total * DEFAULT_PAIR_QUEUE_MULTIPLIER,
                            _auto_pair_queue_candidates(total, ni)[-1])
         if s["max_wf"] > conservative:
-            raise RuntimeError(
-                "Count-pass traversal wavefront overflowed its conservative buffer.")
+            out.append(("count",
+                        "Count-pass traversal wavefront overflowed its conservative buffer."))
         if max(1, s["max_near"]) > max(1, _INT32_MAX // max(1, nl)):
-            raise RuntimeError(
+            out.append(("count",
                 "Suggested per-leaf neighbor capacity is too large to safely allocate on the "
                 "host (would overflow int32). Enable local refinement or pass explicit "
-                "capacities (max_neighbors_per_leaf / max_interactions_per_node).")
+                "capacities (max_neighbors_per_leaf / max_interactions_per_node)."))
         if s["far_total"] > _INT32_MAX or s["near_total"] > _INT32_MAX:
-            raise RuntimeError(
+            out.append(("count",
                 "Dual-tree traversal pair totals exceed signed int32 capacity; refine the tree "
-                "or use a lower-memory traversal strategy.")
-        return
+                "or use a lower-memory traversal strategy."))
+        return out
     config = traversal_config if traversal_config is not None else _GLOBAL_DUAL_TREE_CONFIG
     auto = _auto_pair_queue_candidates(total, ni)
     if config is not None:
@@ -721,12 +743,13 @@ def _check_capacities(w: _WalkOut, total: int, ni: int, *, max_interactions_per_
             qmsg = ("Pair queue capacity exceeded; pass a larger max_pair_queue value to "
                     "override auto-scaling.")
     if s["max_wf"] > queue[-1]:
-        raise RuntimeError(qmsg)
+        out.append(("queue", qmsg))
     if s["max_far"] > K:
-        raise RuntimeError(_FAR_MSG)
+        out.append(("far", _FAR_MSG))
     hard_cap = max(1, _INT32_MAX // max(1, nl))
     if s["max_near"] > max(min(max(1, nbr_limit), hard_cap), hard_cap):
-        raise RuntimeError(_NEAR_MSG)
+        out.append(("near", _NEAR_MSG))
+    return out
 
 
 def build_interactions_and_neighbors(
@@ -770,11 +793,11 @@ def build_interactions_and_neighbors(
     total = int(topology.parent.shape[0])
     ni = int(topology.left_child.shape[0])
     w = _run_walk(topology, geometry, theta, mac_type, dehnen_radius_scale)
+    caps = dict(max_interactions_per_node=max_interactions_per_node,
+                max_neighbors_per_leaf=max_neighbors_per_leaf, max_pair_queue=max_pair_queue,
+                process_block=process_block, traversal_config=traversal_config)
     if _REFERENCE_LIMITS:
-        _check_capacities(w, total, ni, max_interactions_per_node=max_interactions_per_node,
-                          max_neighbors_per_leaf=max_neighbors_per_leaf,
-                          max_pair_queue=max_pair_queue, process_block=process_block,
-                          traversal_config=traversal_config)
+        _check_capacities(w, total, ni, **caps)
     dev = topology.parent.device
     interactions = None
     if return_interactions:
@@ -796,6 +819,10 @@ def build_interactions_and_neighbors(
         idt = INDEX_DTYPE
         if return_result:
             s = w.stats
+            # with the reference limits on, a failing check raised above, so
+            # these are all False; with them off they say what the padded
+            # walk would have flagged (the lists themselves stay exact)
+            q_ovf, f_ovf, n_ovf = _overflow_flags(w, total, ni, **caps)
             out.append(DualTreeWalkResult(
                 interaction_offsets=no, interaction_sources=raw_src,
                 interaction_targets=raw_tgt, interaction_tags=tags,
@@ -803,9 +830,9 @@ def build_interactions_and_neighbors(
                 neighbor_indices=w.neighbors, neighbor_counts=w.near_counts,
                 leaf_indices=w.leaf_indices, far_pair_count=fpc,
                 near_pair_count=torch.tensor(int(w.neighbors.shape[0]), dtype=idt, device=dev),
-                queue_overflow=torch.tensor(False, device=dev),
-                far_overflow=torch.tensor(False, device=dev),
-                near_overflow=torch.tensor(False, device=dev),
+                queue_overflow=torch.tensor(q_ovf, device=dev),
+                far_overflow=torch.tensor(f_ovf, device=dev),
+                near_overflow=torch.tensor(n_ovf, device=dev),
                 accept_decisions=torch.tensor(s["accept"], dtype=idt, device=dev),
                 near_decisions=torch.tensor(s["near"], dtype=idt, device=dev),
                 refine_decisions=torch.tensor(s["refine"], dtype=idt, device=dev)))
