@@ -60,6 +60,8 @@ enum {
 #define YGX_TUNE_SPIN_LIMIT 6  /* iterations a device-side wait (sort look-back) spins   */
                                /* before it gives up and flags YGX_FLAG_TIMEOUT          */
                                /* (0..2^24; default 2^22); not a performance knob        */
+#define YGX_TUNE_TARGET_BUDGET 7 /* steps one warp spends on a piece of a target before */
+                                 /* handing the rest to other warps (1..4096; 64)      */
 
 /* traversal statistics words (host array of YGX_TSTAT_WORDS uint64) */
 #define YGX_TSTAT_WORDS 16
@@ -331,6 +333,50 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
                           void* far_targets, void* target_levels, void* neighbors,
                           void* neighbor_leaf_positions, int64_t max_nbr, void* ws,
                           size_t ws_bytes, cudaStream_t stream);
+/* ---- per-target walk: the same exact lists, row by row -------------------
+ * Replaces the count walk + compact fill walk of
+ * build_interactions_and_neighbors (_interactions_impl.py:2600-3558; the
+ * pair set of _dual_tree_walk_impl, :1119-1905) and the layouts of
+ * _result_to_interactions / _result_to_neighbors (:3561-3837).  One warp
+ * per target node walks the pairs {t, s} of the reference's symmetric walk
+ * that involve t, from the parent's "split on my side" list, in Morton
+ * order, so every row comes out in ascending order with no sort; long
+ * expansions are split into pieces run by other warps.  Well-formed single
+ * trees only (nodes 0..num_internal-1 internal, root `root`).
+ * caps (host, 8 int64): entry capacities of the far pool, near pool, split
+ * lists, spill area; record capacities of far chunks, near chunks,
+ * split-list chunks; continuation queue.  needs_out (host, 9 uint64): what
+ * each of them needed (re-run with at least these when
+ * YGX_FLAG_LOG_OVERFLOW is set), then the most chunks one split list had.
+ * flags_out also reports YGX_FLAG_TIMEOUT (a bounded wait gave up) and
+ * YGX_FLAG_MALFORMED (a split list had more chunks than can be ordered);
+ * with either flag the lists are not produced: use ygx_traverse_walk.
+ * stats_out as for ygx_traverse_walk (wf_need / log_need are 0).
+ * Synchronizes the stream. */
+size_t ygx_target_walk_workspace_size(int64_t total, int64_t num_leaves, const int64_t* caps);
+int ygx_target_walk(const float* center, const float* radius, const float* max_extent,
+                    const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
+                    const int32_t* parent32, const int32_t* level32, const int32_t* nbl32,
+                    int64_t total, int64_t num_internal, int root, int mac, float theta,
+                    float dehnen_radius_scale, const int64_t* caps,
+                    const void* tree_level_offsets, int num_levels, int index_bits,
+                    uint64_t* stats_out, uint64_t* needs_out, uint32_t* flags_out, void* ws,
+                    size_t ws_bytes, cudaStream_t stream);
+/* After ygx_target_walk on the same workspace and capacities: the offset /
+ * count tables and the rows (level-major far sources / targets /
+ * target_levels, leaf-ordered near neighbours) in the index dtype, and
+ * with max_nbr > 0 the dense neighbour_leaf_positions table (L x max_nbr).
+ * far_records / near_records: needs_out[4] / needs_out[5] of the walk. */
+int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* caps,
+                          const int32_t* nbl32, const int32_t* level32,
+                          const void* tree_level_offsets, int num_levels, int index_bits,
+                          int64_t far_total, int64_t near_total, uint64_t far_records,
+                          uint64_t near_records, void* node_offsets, void* far_counts,
+                          void* level_offsets, void* sources, void* targets, void* target_levels,
+                          void* near_offsets, void* near_counts, void* neighbors,
+                          const int32_t* leafpos32, int64_t max_nbr,
+                          void* neighbor_leaf_positions, void* ws, size_t ws_bytes,
+                          cudaStream_t stream);
 /* ---- learned row-capacity predictor (no counterpart in the reference) -----
  * A per-node MLP (YGX_MLP_INPUTS -> 64 -> 64 -> 2, ReLU, fp32) that predicts
  * log2(1 + far row length) and log2(1 + near row length) from the node's

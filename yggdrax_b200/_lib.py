@@ -38,7 +38,7 @@ FLAG_BAD_INPUT = 1 << 5
 FLAG_LOG_OVERFLOW = 1 << 6
 WALK_LOG = 0
 TUNE = dict(sort_rank=0, sort_skew=1, walk_blocks=2, refit_warps=3, row_grid=4, sort_tile=5,
-            spin_limit=6)
+            spin_limit=6, target_budget=7)
 WALK_COUNT = 1
 
 TSTAT_WORDS = 16
@@ -106,6 +106,12 @@ _SIGS = {
     "ygx_mlp_train_step": (I32, [P, P, P, I32, F32, P, P, P, I64, P, P, SZ, P]),
     "ygx_predict_caps": (I32, [P, P, P, P, P, P, I64, I64, P, I32, I32, F32, I32, P, F32, F32,
                                I32, P, P, P]),
+    "ygx_target_walk_workspace_size": (SZ, [I64, I64, P]),
+    "ygx_target_walk": (I32, [P, P, P, P, P, P, P, P, P, I64, I64, I32, I32, F32, F32, P, P, I32,
+                              I32, P, P, P, P, SZ, P]),
+    "ygx_target_walk_lists": (I32, [I64, I64, P, P, P, P, I32, I32, I64, I64, ctypes.c_uint64,
+                                    ctypes.c_uint64, P, P, P, P, P, P, P, P, P, P, I64, P, P,
+                                    SZ, P]),
     "ygx_traverse_finalize": (I32, [I64, I64, I64, I64, P, P, I32, P, P, P, P, P, P, P, P, P, P,
                                     P, I64, P, SZ, P]),
     "ygx_batch_encode_sort_workspace_size": (SZ, [I64]),

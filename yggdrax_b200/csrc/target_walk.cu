@@ -1,0 +1,1261 @@
+// Per-target dual-tree traversal: the exact far / near lists of the
+// symmetric walk (_interactions_impl.py:1119-1905, 2600-3558; result
+// layouts :3561-3837) produced row by row, without a pair log, an atomic
+// scatter or a per-row sort.
+//
+// The reference's walk refines canonical node pairs breadth first from
+// (root, root).  Seen from one node t, the visited pairs {t, s} are:
+//  * the pairs inherited from the parent p: every {p, s} that the walk
+//    refined by splitting p (the split rule on the canonical orientation,
+//    :1444-1454), plus the sibling pair {L, R} that the self pair {p, p}
+//    produces;
+//  * and, recursively, the children {t, s.left}, {t, s.right} of every
+//    visited {t, s} refined by splitting s.
+// So t's pairs follow from its parent's "split on my side" list S_p alone,
+// and the nodes can be processed top down, one warp per target, each warp
+// evaluating the MAC (:338-395) in the reference's fp32 order on exactly the
+// pairs the reference evaluates (every unordered pair twice, once from each
+// side).
+//
+// Row order without sorting: the candidates of one target are disjoint
+// subtrees, and a warp walks them in Morton order (an ordered depth-first
+// expansion: it pops the 32 leftmost pending candidates, emits the leading
+// ones that are resolved, and pushes the rest back in order).  For disjoint
+// Karras ranges, Morton order is id order within internal nodes (an internal
+// node's id is the first or last leaf of its range) and within leaves (id =
+// num_internal + leaf index), and every internal id is below every leaf id.
+// So a far row in ascending id order is its internal entries in Morton order
+// followed by its leaf entries in Morton order, and a near row (leaves only)
+// is the Morton order itself.  The warp stages the two far classes and the
+// near entries separately; every flushed chunk is keyed by (row, class,
+// first id), and one sort of the chunk records (not of the entries) puts all
+// rows in their final, ascending order.
+//
+// Work balance: a target whose expansion runs longer than a step budget, or
+// whose ordered stack fills, spills its pending candidates (in order) and
+// hands them to other warps as continuation pieces.  Pieces of one target
+// cover disjoint Morton intervals, so their chunks still sort into place.
+// A node's own "split on my side" list is compacted into one Morton-ordered
+// array when its last piece ends, and only then may its children start.
+// One persistent launch processes every level: warps take pieces first,
+// then targets in level order, and wait (bounded) only on a parent that is
+// still in progress.
+#include "scan.cuh"
+#include "sort.cuh"
+
+namespace ygx {
+namespace {
+
+struct __align__(16) TwRec {
+  float4 c;  // center x, y, z; MAC extent
+  int4 k;    // left, right (-1 for leaves), leaf position (-1 internal), first leaf index
+};
+
+enum TwMac { kTwBH = 0, kTwDehnen = 1, kTwEngblom = 2 };
+
+// Candidate entry (64 bits): node id (31 bits) | generation << 32 (12 bits)
+// | state << 44 (2 bits) | before << 46.  States: 0 pending, 1 far, 2 near,
+// 3 split on the target's side.  "before": the node's range starts before
+// the target's (counted for the children's sibling insertion point).
+__device__ __forceinline__ unsigned long long tw_ent(int s, int gen, int state, int before) {
+  return (unsigned long long)(uint32_t)s | ((unsigned long long)(uint32_t)gen << 32) |
+         ((unsigned long long)(uint32_t)state << 44) | ((unsigned long long)(uint32_t)before << 46);
+}
+__device__ __forceinline__ int tw_s(unsigned long long e) { return (int)(e & 0x7fffffffull); }
+__device__ __forceinline__ int tw_gen(unsigned long long e) { return (int)((e >> 32) & 0xfffull); }
+__device__ __forceinline__ int tw_state(unsigned long long e) { return (int)((e >> 44) & 3ull); }
+__device__ __forceinline__ int tw_before(unsigned long long e) { return (int)((e >> 46) & 1ull); }
+constexpr unsigned long long kTwPendingMask = 0xfffffffffffull;  // id + generation
+
+constexpr int kTwWarps = 8;
+constexpr int kTwThreads = kTwWarps * 32;
+constexpr int kTwBlocksPerSM = 4;
+constexpr int kTwStk = 256;    // ordered stack entries per warp
+constexpr int kTwStgF = 128;   // staging of far-internal / far-leaf / near entries
+constexpr int kTwStgS = 256;   // staging of split-list entries
+constexpr int kTwHist = 256;   // generations counted per CTA (pair generations < 2 x depth)
+constexpr int kTwCmpMax = 256; // chunks a split list may have before compaction
+constexpr int kTwSpillGroup = 8;
+constexpr int kTwInhGroup = 64;
+
+struct TwWarpSmem {
+  unsigned long long stk[kTwStk];
+  unsigned long long stg_s[kTwStgS];
+  int32_t stg_fi[kTwStgF];
+  int32_t stg_fl[kTwStgF];
+  int32_t stg_n[kTwStgF];
+};
+struct TwSmem {
+  TwWarpSmem w[kTwWarps];
+  unsigned int hist[kTwHist];
+};
+
+// Control block (zeroed before the walk).
+struct TwCtl {
+  unsigned long long far_cur, near_cur, s_cur, spill_cur;  // pool cursors (entries)
+  unsigned long long acc_sides, near_sides, ref_sides;     // decision counts (per side)
+  unsigned int far_rec_cur, near_rec_cur, s_rec_cur;       // chunk record cursors
+  unsigned int q_head, q_tail;                             // continuation queue
+  unsigned int tick;                                       // next target
+  int work;                                                // targets + pieces outstanding
+  unsigned int max_cmp;                                    // most chunks of one split list
+  unsigned int pad[4];
+};
+
+struct TwPiece {
+  long long spill_off;
+  int t;
+  int spill_cnt;
+  int inh_b, inh_e;
+};
+
+struct TwChunk {  // a flushed far / near chunk
+  long long off;
+  int cnt;
+  int t;
+};
+struct TwSChunk {  // a flushed split-list chunk (linked per node)
+  long long off;
+  int cnt;
+  unsigned int key;  // first leaf of the chunk's first entry
+  int next;
+  int pad;
+};
+
+struct TwArgs {
+  const TwRec* recs;
+  const int32_t* nbl;        // nodes in level order
+  const int32_t* parent;
+  const int32_t* level;      // node depth
+  const int32_t* rank;       // position in nbl
+  int32_t ni, total, lo, n_targets;
+  float theta_sq, theta;
+  // per node
+  long long* s_off;
+  int32_t* s_cnt;
+  int32_t* s_ins;
+  int32_t* s_head;
+  int32_t* s_nch;
+  int32_t* pieces_left;
+  int32_t* done;
+  int32_t* far_cnt;   // per node
+  int32_t* near_cnt;  // per leaf position
+  // pools
+  int32_t* far_pool;
+  int32_t* near_pool;
+  unsigned long long* s_pool;
+  unsigned long long* spill;
+  unsigned long long far_cap, near_cap, s_cap, spill_cap;
+  unsigned long long* far_keys;
+  TwChunk* far_recs;
+  unsigned long long* near_keys;
+  TwChunk* near_recs;
+  TwSChunk* s_recs;
+  unsigned int far_rec_cap, near_rec_cap, s_rec_cap, q_cap;
+  TwPiece* queue;
+  unsigned int* q_ready;
+  unsigned int* gen_hist;  // global, kTwHist words
+  TwCtl* ctl;
+  uint32_t* status;
+  uint32_t spin_limit;
+  int budget;
+};
+
+__device__ __forceinline__ unsigned lanemask_lt_() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+__device__ __forceinline__ int ld_acquire_i32(const int32_t* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned ld_volatile_u32_(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_volatile_i32_(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_i32(int32_t* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// setup
+
+// first[v]: index of the first (leftmost) leaf under node v.  Each leaf
+// climbs while it is its parent's left child.
+__global__ void k_tw_first_leaf(const int32_t* __restrict__ parent, const int32_t* __restrict__ left,
+                                int32_t ni, int32_t total, int32_t* __restrict__ first) {
+  for (int32_t v = ni + blockIdx.x * blockDim.x + threadIdx.x; v < total;
+       v += gridDim.x * blockDim.x) {
+    const int32_t j = v - ni;
+    first[v] = j;
+    int32_t c = v;
+    for (int guard = 0; guard < 128; ++guard) {
+      const int32_t p = parent[c];
+      if (p < 0 || p >= ni || left[p] != c) break;
+      first[p] = j;
+      c = p;
+    }
+  }
+}
+
+__global__ void k_tw_recs(const float* __restrict__ center, const float* __restrict__ radius,
+                          const float* __restrict__ max_extent, const int32_t* __restrict__ left32,
+                          const int32_t* __restrict__ right32, const int32_t* __restrict__ leafpos,
+                          const int32_t* __restrict__ first, int32_t total, int mac,
+                          float dehnen_scale, const int32_t* __restrict__ nbl,
+                          int32_t* __restrict__ rank, TwRec* __restrict__ recs,
+                          uint32_t* __restrict__ status) {
+  for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    // _build_mac_extents (_interactions_impl.py:993-1061)
+    float e = mac == kTwBH ? max_extent[k] : radius[k];
+    if (mac == kTwDehnen) e = __fmul_rn(dehnen_scale, e);
+    if (!(e > 0.0f)) raise_flag(status, kFlagBadInput);
+    TwRec r;
+    r.c = make_float4(center[3 * k], center[3 * k + 1], center[3 * k + 2], e);
+    r.k = make_int4(left32[k], right32[k], leafpos[k], first[k]);
+    recs[k] = r;
+    rank[nbl[k]] = k;
+  }
+}
+
+// Root: done, empty split list.  Every other node: no chunks yet.
+__global__ void k_tw_init_nodes(int32_t total, int32_t root, int32_t* __restrict__ s_head,
+                                long long* __restrict__ s_off, int32_t* __restrict__ done) {
+  for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    s_head[k] = -1;
+    s_off[k] = 0;
+    done[k] = k == root ? 1 : 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the walk
+
+// Warp-collective: writes the n staged int32 entries to `pool` at a fresh
+// offset and records the chunk.  Returns nothing; counts rows.
+__device__ __forceinline__ void tw_flush_rows(const int32_t* stg, int n, int lane, int t,
+                                              unsigned long long key_hi, unsigned cls_bit,
+                                              int32_t* pool, unsigned long long cap,
+                                              unsigned long long* pool_cur, unsigned long long* keys,
+                                              TwChunk* recs, unsigned rec_cap, unsigned* rec_cur,
+                                              int32_t* cnt_row, uint32_t* status) {
+  if (n == 0) return;
+  unsigned long long off = 0;
+  unsigned ri = 0;
+  if (lane == 0) {
+    off = atomicAdd(pool_cur, (unsigned long long)n);
+    ri = atomicAdd(rec_cur, 1u);
+  }
+  off = __shfl_sync(0xffffffffu, off, 0);
+  ri = __shfl_sync(0xffffffffu, ri, 0);
+  const bool fits = off + (unsigned long long)n <= cap && ri < rec_cap;
+  if (fits) {
+    for (int k = lane; k < n; k += 32) pool[off + k] = stg[k];
+    if (lane == 0) {
+      keys[ri] = key_hi | cls_bit | (unsigned long long)(uint32_t)stg[0];
+      TwChunk c;
+      c.off = (long long)off;
+      c.cnt = n;
+      c.t = t;
+      recs[ri] = c;
+      atomicAdd(cnt_row, n);
+    }
+  } else if (lane == 0) {
+    raise_flag(status, kFlagLogOverflow);
+  }
+}
+
+__device__ __forceinline__ void tw_flush_split(const unsigned long long* stg, int n, int lane, int t,
+                                               const TwArgs& a) {
+  if (n == 0) return;
+  unsigned long long off = 0;
+  unsigned ri = 0;
+  if (lane == 0) {
+    off = atomicAdd(&a.ctl->s_cur, (unsigned long long)n);
+    ri = atomicAdd(&a.ctl->s_rec_cur, 1u);
+  }
+  off = __shfl_sync(0xffffffffu, off, 0);
+  ri = __shfl_sync(0xffffffffu, ri, 0);
+  const bool fits = off + (unsigned long long)n <= a.s_cap && ri < a.s_rec_cap;
+  int before = 0;
+  for (int k = lane; k < n; k += 32) {
+    const unsigned long long e = stg[k];
+    before += tw_before(e);
+    if (fits) a.s_pool[off + k] = e & kTwPendingMask;  // stored as pending entries
+  }
+  for (int o = 16; o > 0; o >>= 1) before += __shfl_xor_sync(0xffffffffu, before, o);
+  if (lane == 0) {
+    if (fits) {
+      TwSChunk c;
+      c.off = (long long)off;
+      c.cnt = n;
+      c.key = (unsigned)a.recs[tw_s(stg[0])].k.w;
+      c.pad = 0;
+      c.next = atomicExch(&a.s_head[t], (int)ri);
+      a.s_recs[ri] = c;
+      atomicAdd(&a.s_cnt[t], n);
+      atomicAdd(&a.s_ins[t], before);
+      atomicAdd(&a.s_nch[t], 1);
+    } else {
+      raise_flag(a.status, kFlagLogOverflow);
+    }
+  }
+}
+
+// Warp-collective: compacts node t's split-list chunks (Morton order by their
+// first leaf) into one array.  Called by the warp that ends t's last piece.
+__device__ void tw_compact_split(int t, int lane, const TwArgs& a, unsigned long long* scratch) {
+  const int nch = ld_volatile_i32_(&a.s_nch[t]);
+  if (nch == 0) {
+    if (lane == 0) a.s_off[t] = 0;
+    return;
+  }
+  const int head = ld_volatile_i32_(&a.s_head[t]);
+  if (nch == 1) {
+    if (lane == 0) a.s_off[t] = a.s_recs[head].off;
+    return;
+  }
+  if (lane == 0) atomicMax(&a.ctl->max_cmp, (unsigned)nch);
+  if (nch > kTwCmpMax) {  // cannot order it here: report (the host falls back)
+    if (lane == 0) {
+      raise_flag(a.status, kFlagMalformed);
+      a.s_cnt[t] = 0;  // children see an empty list (the result is discarded)
+      a.s_ins[t] = 0;
+    }
+    return;
+  }
+  // collect (key << 32 | record) pairs; lane 0 walks the list
+  if (lane == 0) {
+    int r = head, k = 0;
+    while (r >= 0 && k < nch) {
+      const TwSChunk c = a.s_recs[r];
+      scratch[k++] = ((unsigned long long)c.key << 32) | (unsigned)r;
+      r = c.next;
+    }
+  }
+  __syncwarp();
+  // odd-even transposition sort of nch <= 256 keys (small; rare)
+  for (int pass = 0; pass < nch; ++pass) {
+    for (int i = 2 * lane + (pass & 1); i + 1 < nch; i += 64) {
+      const unsigned long long x = scratch[i], y = scratch[i + 1];
+      if (x > y) {
+        scratch[i] = y;
+        scratch[i + 1] = x;
+      }
+    }
+    __syncwarp();
+  }
+  const int total = ld_volatile_i32_(&a.s_cnt[t]);
+  unsigned long long off = 0;
+  if (lane == 0) off = atomicAdd(&a.ctl->s_cur, (unsigned long long)total);
+  off = __shfl_sync(0xffffffffu, off, 0);
+  if (off + (unsigned long long)total > a.s_cap) {
+    if (lane == 0) {
+      raise_flag(a.status, kFlagLogOverflow);
+      a.s_cnt[t] = 0;
+      a.s_ins[t] = 0;
+    }
+    return;
+  }
+  unsigned long long pos = off;
+  for (int k = 0; k < nch; ++k) {
+    const TwSChunk c = a.s_recs[(unsigned)(scratch[k] & 0xffffffffu)];
+    for (int e = lane; e < c.cnt; e += 32) a.s_pool[pos + e] = a.s_pool[c.off + e];
+    pos += (unsigned long long)c.cnt;
+  }
+  if (lane == 0) a.s_off[t] = (long long)off;
+}
+
+// Warp-collective: the rest of this piece -- P pending outputs (lane l holds
+// nout of them from index k0), then the ordered stack (top first), then the
+// source remainder from `cur` -- is handed to other warps as continuation
+// pieces, in groups.  Pieces of one target cover disjoint Morton intervals,
+// so their output chunks sort into place whatever warp runs them.
+__device__ void tw_hand_off(const TwArgs& a, int lane, int t, const TwPiece& pc, int cur,
+                            int nout, int k0, unsigned long long o0, unsigned long long o1, int P,
+                            const unsigned long long* stk, int stk_n) {
+  const int E = P + stk_n;
+  unsigned long long off = 0;
+  if (lane == 0 && E > 0) off = atomicAdd(&a.ctl->spill_cur, (unsigned long long)E);
+  off = __shfl_sync(0xffffffffu, off, 0);
+  if (off + (unsigned long long)E > a.spill_cap) {
+    if (lane == 0) raise_flag(a.status, kFlagLogOverflow);
+    return;
+  }
+  if (nout >= 1) a.spill[off + k0] = o0;
+  if (nout == 2) a.spill[off + k0 + 1] = o1;
+  for (int j = lane; j < stk_n; j += 32) a.spill[off + P + j] = stk[stk_n - 1 - j];
+  const int np_sp = (E + kTwSpillGroup - 1) / kTwSpillGroup;
+  const int rem_sp = cur < pc.spill_cnt ? pc.spill_cnt - cur : 0;
+  const int np_rs = (rem_sp + kTwSpillGroup - 1) / kTwSpillGroup;
+  const int inh_from = pc.inh_b + (cur > pc.spill_cnt ? cur - pc.spill_cnt : 0);
+  const int rem_in = pc.inh_e - inh_from;
+  const int np_in = rem_in > 0 ? (rem_in + kTwInhGroup - 1) / kTwInhGroup : 0;
+  const int np = np_sp + np_rs + np_in;
+  if (np == 0) return;
+  unsigned slot = 0;
+  int n_ok = 0;
+  if (lane == 0) {
+    slot = atomicAdd(&a.ctl->q_tail, (unsigned)np);
+    n_ok = slot >= a.q_cap ? 0 : (int)min((unsigned)np, a.q_cap - slot);
+    if (n_ok < np) raise_flag(a.status, kFlagLogOverflow);
+    // counted before any of them can be taken (and finished) by another warp
+    if (n_ok > 0) {
+      atomicAdd(&a.pieces_left[t], n_ok);
+      atomicAdd(&a.ctl->work, n_ok);
+    }
+    __threadfence();
+  }
+  slot = __shfl_sync(0xffffffffu, slot, 0);
+  n_ok = __shfl_sync(0xffffffffu, n_ok, 0);
+  __syncwarp();
+  for (int k = lane; k < n_ok; k += 32) {
+    TwPiece q;
+    q.t = t;
+    if (k < np_sp) {
+      q.spill_off = (long long)(off + (unsigned long long)k * kTwSpillGroup);
+      q.spill_cnt = min(kTwSpillGroup, E - k * kTwSpillGroup);
+      q.inh_b = q.inh_e = 0;
+    } else if (k < np_sp + np_rs) {
+      const int j = k - np_sp;
+      q.spill_off = pc.spill_off + cur + (long long)j * kTwSpillGroup;
+      q.spill_cnt = min(kTwSpillGroup, rem_sp - j * kTwSpillGroup);
+      q.inh_b = q.inh_e = 0;
+    } else {
+      const int j = k - np_sp - np_rs;
+      q.spill_off = 0;
+      q.spill_cnt = 0;
+      q.inh_b = inh_from + j * kTwInhGroup;
+      q.inh_e = min(pc.inh_e, q.inh_b + kTwInhGroup);
+    }
+    a.queue[slot + k] = q;
+    __threadfence();
+    atomicExch(&a.q_ready[slot + k], 1u);
+  }
+}
+
+template <int kMac>
+__global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a) {
+  extern __shared__ __align__(16) unsigned char tw_smem_raw[];
+  TwSmem& sm = *reinterpret_cast<TwSmem*>(tw_smem_raw);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  TwWarpSmem& W = sm.w[warp];
+  for (int i = threadIdx.x; i < kTwHist; i += kTwThreads) sm.hist[i] = 0;
+  __syncthreads();
+  const unsigned lt = lanemask_lt_();
+  unsigned long long acc_sides = 0, near_sides = 0, ref_sides = 0;
+  int held = -1;  // a claimed target waiting for its parent
+  uint32_t idle = 0;
+  bool give_up = false;
+
+  while (!give_up) {
+    // ---- fetch: continuation pieces first, then the held target, then a new target
+    int kind = 0;  // 0 none, 1 piece, 2 target
+    TwPiece pc;
+    pc.t = -1;
+    pc.spill_off = 0;
+    pc.spill_cnt = 0;
+    pc.inh_b = pc.inh_e = 0;
+    {
+      int slot = -1;
+      if (lane == 0) {
+        unsigned h = ld_volatile_u32_(&a.ctl->q_head);
+        const unsigned tl = ld_volatile_u32_(&a.ctl->q_tail);
+        while (h < tl && h < a.q_cap) {
+          const unsigned got = atomicCAS(&a.ctl->q_head, h, h + 1);
+          if (got == h) {
+            slot = (int)h;
+            break;
+          }
+          h = got;
+        }
+      }
+      slot = __shfl_sync(0xffffffffu, slot, 0);
+      if (slot >= 0) {
+        if (lane == 0) {
+          uint32_t spins = 0;
+          while (ld_volatile_u32_(&a.q_ready[slot]) == 0u && spins < a.spin_limit) {
+            __nanosleep(64);
+            ++spins;
+          }
+          if (ld_volatile_u32_(&a.q_ready[slot]) == 0u) {
+            raise_flag(a.status, kFlagTimeout);
+            slot = -2;
+          } else {
+            __threadfence();
+          }
+        }
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        if (slot == -2) break;
+        __syncwarp();
+        pc = a.queue[slot];
+        kind = 1;
+      }
+    }
+    if (kind == 0 && held >= 0) {
+      const int p = a.parent[held];
+      int ready = 0;
+      if (lane == 0) ready = ld_acquire_i32(&a.done[p]);
+      ready = __shfl_sync(0xffffffffu, ready, 0);
+      __syncwarp();
+      if (ready) {
+        pc.t = held;
+        held = -1;
+        kind = 2;
+      }
+    }
+    if (kind == 0 && held < 0) {
+      int idx = -1;
+      if (lane == 0) {
+        if (ld_volatile_u32_(&a.ctl->tick) < (unsigned)a.n_targets) {
+          atomicAdd(&a.ctl->work, 1);
+          const unsigned i = atomicAdd(&a.ctl->tick, 1u);
+          if (i < (unsigned)a.n_targets) idx = (int)i;
+          else atomicSub(&a.ctl->work, 1);
+        }
+      }
+      idx = __shfl_sync(0xffffffffu, idx, 0);
+      if (idx >= 0) {
+        held = a.nbl[a.lo + idx];
+        idle = 0;
+        continue;  // check its parent next round (queue first)
+      }
+    }
+    if (kind == 0) {
+      int fin = 0;
+      if (lane == 0)
+        fin = held < 0 && ld_volatile_u32_(&a.ctl->tick) >= (unsigned)a.n_targets &&
+              ld_volatile_i32_(&a.ctl->work) <= 0;
+      fin = __shfl_sync(0xffffffffu, fin, 0);
+      if (fin) break;
+      __nanosleep(128);
+      if (++idle >= a.spin_limit) {
+        if (lane == 0) raise_flag(a.status, kFlagTimeout);
+        give_up = true;
+      }
+      continue;
+    }
+    idle = 0;
+
+    // ---- one piece of target t
+    const int t = pc.t;
+    const TwRec T = a.recs[t];
+    const int p = a.parent[t];
+    const int32_t* pk = &a.recs[p].k.x;  // children of p
+    const int sib = pk[0] == t ? pk[1] : pk[0];
+    const int sib_gen = a.level[p] + 1;
+    if (kind == 2) {
+      pc.spill_cnt = 0;
+      pc.inh_b = 0;
+      pc.inh_e = a.s_cnt[p] + 1;  // parent's split list plus the sibling
+      if (lane == 0) a.pieces_left[t] = 1;
+    }
+    const long long s_base = a.s_off[p];
+    const int s_ins = a.s_ins[p];
+    const int src_len = pc.spill_cnt + (pc.inh_e - pc.inh_b);
+    const bool t_leaf = T.k.x < 0;
+    const unsigned long long far_hi = (unsigned long long)(uint32_t)a.rank[t] << 32;
+    const unsigned long long near_hi = (unsigned long long)(uint32_t)T.k.z << 32;
+    int cur = 0, stk_n = 0, steps = 0;
+    int n_fi = 0, n_fl = 0, n_n = 0, n_s = 0;
+
+    while (stk_n > 0 || cur < src_len) {
+      // window: the leftmost (up to) 32 candidates -- stack top first, then source
+      const int take_stk = stk_n < 32 ? stk_n : 32;
+      const int rest = src_len - cur;
+      const int take_src = (32 - take_stk) < rest ? (32 - take_stk) : rest;
+      const int n = take_stk + take_src;
+      unsigned long long e = 0;
+      bool valid = lane < n;
+      if (lane < take_stk) {
+        e = W.stk[stk_n - 1 - lane];
+      } else if (valid) {
+        const int c = cur + (lane - take_stk);
+        if (c < pc.spill_cnt) {
+          e = a.spill[pc.spill_off + c];
+        } else {
+          const int q = pc.inh_b + (c - pc.spill_cnt);
+          if (q < s_ins) e = a.s_pool[s_base + q];
+          else if (q == s_ins) e = tw_ent(sib, sib_gen, 0, 0);
+          else e = a.s_pool[s_base + q - 1];
+        }
+      }
+      stk_n -= take_stk;
+      cur += take_src;
+      __syncwarp();  // the popped slots are rewritten below
+      // evaluate pending candidates (an id outside the tree is dropped and
+      // reported, never dereferenced)
+      if (valid && (unsigned)tw_s(e) >= (unsigned)a.total) {
+        raise_flag(a.status, kFlagBadInput);
+        valid = false;
+      }
+      int state = valid ? tw_state(e) : 0;
+      bool refine_s = false;
+      unsigned long long c0 = 0, c1 = 0;
+      if (valid && state == 0) {
+        const int s = tw_s(e);
+        const int g = tw_gen(e);
+        const TwRec B = a.recs[s];
+        const float dx = __fsub_rn(T.c.x, B.c.x);
+        const float dy = __fsub_rn(T.c.y, B.c.y);
+        const float dz = __fsub_rn(T.c.z, B.c.z);
+        float d2 = __fmul_rn(dx, dx);
+        d2 = __fadd_rn(d2, __fmul_rn(dy, dy));
+        d2 = __fadd_rn(d2, __fmul_rn(dz, dz));
+        const float et = T.c.w, es = B.c.w;
+        bool ok;
+        if (kMac == kTwEngblom) {
+          const float big = fmax_nan(et, es), small = fmin_nan(et, es);
+          const float lhs = __fadd_rn(big, __fmul_rn(a.theta, small));
+          ok = __fmul_rn(lhs, lhs) <= __fmul_rn(a.theta_sq, d2);
+        } else {
+          const float sum = __fadd_rn(et, es);
+          ok = __fmul_rn(sum, sum) <= __fmul_rn(a.theta_sq, d2);
+        }
+        const bool s_leaf = B.k.x < 0;
+        atomicAdd(&sm.hist[g < kTwHist ? g : kTwHist - 1], 1u);
+        if (d2 > 0.0f && ok) {
+          state = 1;
+          ++acc_sides;
+        } else if (t_leaf && s_leaf) {
+          state = 2;
+          ++near_sides;
+        } else {
+          ++ref_sides;
+          // split rule on the canonical (lo, hi) orientation
+          const bool t_lo = t < s;
+          const float e_lo = t_lo ? et : es, e_hi = t_lo ? es : et;
+          const bool lo_int = t_lo ? !t_leaf : !s_leaf, hi_leaf = t_lo ? s_leaf : t_leaf;
+          const bool split_lo = lo_int && (hi_leaf || e_lo >= e_hi);
+          const bool split_t = t_lo ? split_lo : !split_lo;
+          if (split_t) {
+            state = 3;
+            e = tw_ent(s, g + 1, 3, B.k.w < T.k.w ? 1 : 0);
+          } else {
+            refine_s = true;
+            c0 = tw_ent(B.k.x, g + 1, 0, 0);
+            c1 = tw_ent(B.k.y, g + 1, 0, 0);
+          }
+        }
+        if (state == 1 || state == 2) e = tw_ent(s, g, state, 0);
+      }
+      const unsigned refm = __ballot_sync(0xffffffffu, refine_s);
+      const int f = refm ? __ffs(refm) - 1 : n;  // lanes [0, f) are resolved: emit them
+      const bool emit = valid && lane < f;
+      // ---- emit in lane order to the staging buffers (flush when full)
+      {
+        const int s = tw_s(e);
+        const bool is_fi = emit && state == 1 && s < a.ni;
+        const bool is_fl = emit && state == 1 && s >= a.ni;
+        const bool is_n = emit && state == 2;
+        const bool is_s = emit && state == 3;
+        const unsigned mfi = __ballot_sync(0xffffffffu, is_fi);
+        const unsigned mfl = __ballot_sync(0xffffffffu, is_fl);
+        const unsigned mn = __ballot_sync(0xffffffffu, is_n);
+        const unsigned ms = __ballot_sync(0xffffffffu, is_s);
+        if (mfi) {
+          if (n_fi + __popc(mfi) > kTwStgF) {
+            __syncwarp();
+            tw_flush_rows(W.stg_fi, n_fi, lane, t, far_hi, 0u, a.far_pool, a.far_cap,
+                          &a.ctl->far_cur, a.far_keys, a.far_recs, a.far_rec_cap,
+                          &a.ctl->far_rec_cur, &a.far_cnt[t], a.status);
+            n_fi = 0;
+            __syncwarp();
+          }
+          if (is_fi) W.stg_fi[n_fi + __popc(mfi & lt)] = s;
+          n_fi += __popc(mfi);
+        }
+        if (mfl) {
+          if (n_fl + __popc(mfl) > kTwStgF) {
+            __syncwarp();
+            tw_flush_rows(W.stg_fl, n_fl, lane, t, far_hi, 0x80000000u, a.far_pool, a.far_cap,
+                          &a.ctl->far_cur, a.far_keys, a.far_recs, a.far_rec_cap,
+                          &a.ctl->far_rec_cur, &a.far_cnt[t], a.status);
+            n_fl = 0;
+            __syncwarp();
+          }
+          if (is_fl) W.stg_fl[n_fl + __popc(mfl & lt)] = s;
+          n_fl += __popc(mfl);
+        }
+        if (mn) {
+          if (n_n + __popc(mn) > kTwStgF) {
+            __syncwarp();
+            tw_flush_rows(W.stg_n, n_n, lane, t, near_hi, 0u, a.near_pool, a.near_cap,
+                          &a.ctl->near_cur, a.near_keys, a.near_recs, a.near_rec_cap,
+                          &a.ctl->near_rec_cur, &a.near_cnt[T.k.z], a.status);
+            n_n = 0;
+            __syncwarp();
+          }
+          if (is_n) W.stg_n[n_n + __popc(mn & lt)] = s;
+          n_n += __popc(mn);
+        }
+        if (ms) {
+          if (n_s + __popc(ms) > kTwStgS) {
+            __syncwarp();
+            tw_flush_split(W.stg_s, n_s, lane, t, a);
+            n_s = 0;
+            __syncwarp();
+          }
+          if (is_s) W.stg_s[n_s + __popc(ms & lt)] = e;
+          n_s += __popc(ms);
+        }
+      }
+      // ---- push lanes [f, n) back in order (children replace their parent)
+      const int nout = (valid && lane >= f) ? (refine_s ? 2 : 1) : 0;
+      int incl = nout;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int P = __shfl_sync(0xffffffffu, incl, 31);
+      const int k0 = incl - nout;  // this lane's first output index
+      ++steps;
+      if (stk_n + P > kTwStk) {
+        // no room on the stack: hand these outputs, the stack and the rest
+        // of the source to other warps
+        tw_hand_off(a, lane, t, pc, cur, nout, k0, refine_s ? c0 : e, c1, P, W.stk, stk_n);
+        stk_n = 0;
+        cur = src_len;
+        break;
+      }
+      if (nout >= 1) W.stk[stk_n + P - 1 - k0] = refine_s ? c0 : e;
+      if (nout == 2) W.stk[stk_n + P - 2 - k0] = c1;
+      stk_n += P;
+      __syncwarp();
+      if (steps >= a.budget && (stk_n > 0 || cur < src_len)) {
+        // out of budget: hand the stack and the rest of the source off
+        tw_hand_off(a, lane, t, pc, cur, 0, 0, 0ull, 0ull, 0, W.stk, stk_n);
+        stk_n = 0;
+        cur = src_len;
+        break;
+      }
+    }
+    // ---- end of the piece: flush, then account
+    __syncwarp();
+    tw_flush_rows(W.stg_fi, n_fi, lane, t, far_hi, 0u, a.far_pool, a.far_cap, &a.ctl->far_cur,
+                  a.far_keys, a.far_recs, a.far_rec_cap, &a.ctl->far_rec_cur, &a.far_cnt[t],
+                  a.status);
+    tw_flush_rows(W.stg_fl, n_fl, lane, t, far_hi, 0x80000000u, a.far_pool, a.far_cap,
+                  &a.ctl->far_cur, a.far_keys, a.far_recs, a.far_rec_cap, &a.ctl->far_rec_cur,
+                  &a.far_cnt[t], a.status);
+    if (t_leaf)
+      tw_flush_rows(W.stg_n, n_n, lane, t, near_hi, 0u, a.near_pool, a.near_cap,
+                    &a.ctl->near_cur, a.near_keys, a.near_recs, a.near_rec_cap,
+                    &a.ctl->near_rec_cur, &a.near_cnt[T.k.z], a.status);
+    tw_flush_split(W.stg_s, n_s, lane, t, a);
+    __syncwarp();
+    int last = 0;
+    if (lane == 0) {
+      __threadfence();
+      last = atomicSub(&a.pieces_left[t], 1) == 1;
+      if (last) __threadfence();
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (last) {
+      if (!t_leaf) tw_compact_split(t, lane, a, W.stk);
+      __syncwarp();
+      if (lane == 0) {
+        __threadfence();
+        st_release_i32(&a.done[t], 1);
+      }
+    }
+    if (lane == 0) atomicSub(&a.ctl->work, 1);
+    __syncwarp();
+  }
+  // ---- statistics
+  for (int o = 16; o > 0; o >>= 1) {
+    acc_sides += __shfl_xor_sync(0xffffffffu, acc_sides, o);
+    near_sides += __shfl_xor_sync(0xffffffffu, near_sides, o);
+    ref_sides += __shfl_xor_sync(0xffffffffu, ref_sides, o);
+  }
+  if (lane == 0) {
+    if (acc_sides) atomicAdd(&a.ctl->acc_sides, acc_sides);
+    if (near_sides) atomicAdd(&a.ctl->near_sides, near_sides);
+    if (ref_sides) atomicAdd(&a.ctl->ref_sides, ref_sides);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kTwHist; i += kTwThreads)
+    if (sm.hist[i]) atomicAdd(&a.gen_hist[i], sm.hist[i]);
+}
+
+// ---------------------------------------------------------------------------
+// statistics and assembly
+
+// Row totals and maxima (far per node, near per leaf position).
+__global__ void k_tw_row_stats(const int32_t* __restrict__ far_cnt, int32_t total,
+                               const int32_t* __restrict__ near_cnt, int32_t L,
+                               unsigned long long* __restrict__ out) {
+  unsigned long long fs = 0, ns = 0, fm = 0, nm = 0;
+  for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    const unsigned long long v = (unsigned long long)far_cnt[k];
+    fs += v;
+    fm = v > fm ? v : fm;
+    if (k < L) {
+      const unsigned long long w = (unsigned long long)near_cnt[k];
+      ns += w;
+      nm = w > nm ? w : nm;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    fs += __shfl_xor_sync(0xffffffffu, fs, o);
+    ns += __shfl_xor_sync(0xffffffffu, ns, o);
+    const unsigned long long x = __shfl_xor_sync(0xffffffffu, fm, o);
+    const unsigned long long y = __shfl_xor_sync(0xffffffffu, nm, o);
+    fm = x > fm ? x : fm;
+    nm = y > nm ? y : nm;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (fs) atomicAdd(&out[0], fs);
+    if (ns) atomicAdd(&out[1], ns);
+    atomicMax(&out[2], fm);
+    atomicMax(&out[3], nm);
+  }
+}
+
+// Chunk counts in sorted key order.
+__global__ void k_tw_sorted_counts(const uint32_t* __restrict__ order, const TwChunk* __restrict__ recs,
+                                   int64_t m, int32_t* __restrict__ cnt) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x)
+    cnt[i] = recs[order[i]].cnt;
+}
+
+// One warp per chunk (in sorted order): copies its entries to their final
+// place, widened to the index dtype; far chunks also write the target and
+// its level for every entry.
+__global__ void __launch_bounds__(256)
+    k_tw_copy(const uint32_t* __restrict__ order, const TwChunk* __restrict__ recs, int64_t m,
+              const int64_t* __restrict__ dest, const int32_t* __restrict__ pool, int index_bits,
+              void* vals_out, void* tgt_out, void* lvl_out, const int32_t* __restrict__ level) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = w0; i < m; i += nw) {
+    const TwChunk c = recs[order[i]];
+    const int64_t d = dest[i];
+    const int lv = tgt_out ? level[c.t] : 0;
+    for (int k = lane; k < c.cnt; k += 32) {
+      store_idx(vals_out, index_bits, d + k, pool[c.off + k]);
+      if (tgt_out) {
+        store_idx(tgt_out, index_bits, d + k, c.t);
+        store_idx(lvl_out, index_bits, d + k, lv);
+      }
+    }
+  }
+}
+
+// counts in nodes_by_level order; far offsets; index-dtype tables
+__global__ void k_tw_gather(const int32_t* __restrict__ cnt, const int32_t* __restrict__ nbl,
+                            int32_t m, int32_t* __restrict__ out) {
+  for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x)
+    out[r] = cnt[nbl[r]];
+}
+__global__ void k_tw_far_tables(const int64_t* __restrict__ obl, const int32_t* __restrict__ nbl,
+                                const int32_t* __restrict__ cnt, int32_t total, int index_bits,
+                                void* node_offsets, void* counts_out, const void* tree_level_offsets,
+                                int num_levels, void* level_offsets_out) {
+  for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r <= total; r += gridDim.x * blockDim.x) {
+    if (r == total) {
+      store_idx(node_offsets, index_bits, total, obl[total]);
+    } else {
+      const int32_t v = nbl[r];
+      store_idx(node_offsets, index_bits, v, obl[r]);
+      store_idx(counts_out, index_bits, v, cnt[v]);
+    }
+    if (r <= num_levels) {
+      const int64_t li = load_idx(tree_level_offsets, index_bits, r);
+      store_idx(level_offsets_out, index_bits, r, obl[li]);
+    }
+  }
+}
+__global__ void k_tw_near_tables(const int64_t* __restrict__ off, const int32_t* __restrict__ cnt,
+                                 int32_t L, int index_bits, void* offsets_out, void* counts_out) {
+  for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j <= L; j += gridDim.x * blockDim.x) {
+    store_idx(offsets_out, index_bits, j, off[j]);
+    if (j < L) store_idx(counts_out, index_bits, j, cnt[j]);
+  }
+}
+
+// Dense neighbour leaf positions (L x max_nbr, -1 padded) of
+// _result_to_neighbors (:3658-3688).
+__global__ void k_tw_nbr_leaf_pos(const int64_t* __restrict__ near_off,
+                                  const int32_t* __restrict__ near_cnt, int64_t L,
+                                  const void* neighbors, int index_bits,
+                                  const int32_t* __restrict__ leafpos, int64_t max_nbr, void* out) {
+  const int64_t n = L * max_nbr;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = e / max_nbr, k = e - j * max_nbr;
+    int64_t v = -1;
+    if (k < near_cnt[j]) v = leafpos[load_idx(neighbors, index_bits, near_off[j] + k)];
+    store_idx(out, index_bits, e, v);
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// workspace
+
+struct TwCaps {
+  int64_t far, near_, split, spill, far_rec, near_rec, s_rec, queue;
+};
+
+struct TwScratch {
+  uint32_t* status;
+  TwCtl* ctl;
+  unsigned int* gen_hist;
+  unsigned long long* rowstat;  // 4 words
+  TwRec* recs;
+  int32_t* first;
+  int32_t* rank;
+  long long* s_off;
+  int32_t* s_cnt;
+  int32_t* s_ins;
+  int32_t* s_head;
+  int32_t* s_nch;
+  int32_t* pieces_left;
+  int32_t* done;
+  int32_t* far_cnt;
+  int32_t* near_cnt;
+  int32_t* far_pool;
+  int32_t* near_pool;
+  unsigned long long* s_pool;
+  unsigned long long* spill;
+  unsigned long long* far_keys;
+  TwChunk* far_recs;
+  unsigned long long* near_keys;
+  TwChunk* near_recs;
+  TwSChunk* s_recs;
+  TwPiece* queue;
+  unsigned int* q_ready;
+  // assembly
+  uint32_t* order;            // sorted record indices (max of far / near records)
+  unsigned long long* keys_sorted;
+  int32_t* sorted_cnt;
+  int64_t* dest;
+  int64_t* scan_tmp;
+  int32_t* cnt_by_level;
+  int64_t* obl;
+  int64_t* near_off;
+  void* sort_ws;
+  size_t sort_ws_bytes;
+};
+
+static TwScratch carve_tw(Arena& a, int64_t total, int64_t L, const TwCaps& c) {
+  TwScratch s;
+  // status word, control block, histogram and row stats first: one memset
+  s.status = a.take<uint32_t>(64);
+  s.ctl = a.take<TwCtl>(1);
+  s.gen_hist = a.take<unsigned int>(kTwHist);
+  s.rowstat = a.take<unsigned long long>(8);
+  // per node, zeroed: split counts, insertion points, chunk counts, pieces
+  s.s_cnt = a.take<int32_t>(total);
+  s.s_ins = a.take<int32_t>(total);
+  s.s_nch = a.take<int32_t>(total);
+  s.pieces_left = a.take<int32_t>(total);
+  s.far_cnt = a.take<int32_t>(total);
+  s.near_cnt = a.take<int32_t>(L > 0 ? L : 1);
+  // per node, written before use
+  s.recs = a.take<TwRec>(total);
+  s.first = a.take<int32_t>(total);
+  s.rank = a.take<int32_t>(total);
+  s.s_off = a.take<long long>(total);
+  s.s_head = a.take<int32_t>(total);
+  s.done = a.take<int32_t>(total);
+  s.q_ready = a.take<unsigned int>(c.queue);
+  s.far_pool = a.take<int32_t>(c.far);
+  s.near_pool = a.take<int32_t>(c.near_);
+  s.s_pool = a.take<unsigned long long>(c.split);
+  s.spill = a.take<unsigned long long>(c.spill);
+  s.far_keys = a.take<unsigned long long>(c.far_rec);
+  s.far_recs = a.take<TwChunk>(c.far_rec);
+  s.near_keys = a.take<unsigned long long>(c.near_rec);
+  s.near_recs = a.take<TwChunk>(c.near_rec);
+  s.s_recs = a.take<TwSChunk>(c.s_rec);
+  s.queue = a.take<TwPiece>(c.queue);
+  const int64_t mrec = c.far_rec > c.near_rec ? c.far_rec : c.near_rec;
+  s.order = a.take<uint32_t>(mrec);
+  s.keys_sorted = a.take<unsigned long long>(mrec);
+  s.sorted_cnt = a.take<int32_t>(mrec);
+  s.dest = a.take<int64_t>(mrec + 1);
+  const int64_t scan_n = mrec > total ? mrec : total;
+  s.scan_tmp = a.take<int64_t>(scan_scratch_elems(scan_n));
+  s.cnt_by_level = a.take<int32_t>(total);
+  s.obl = a.take<int64_t>(total + 1);
+  s.near_off = a.take<int64_t>((L > 0 ? L : 1) + 1);
+  s.sort_ws_bytes = onesweep_scratch_bytes(mrec) + 256;
+  s.sort_ws = a.take<unsigned char>(s.sort_ws_bytes);
+  return s;
+}
+
+static bool caps_ok(const TwCaps& c) {
+  return c.far >= 1 && c.near_ >= 1 && c.split >= 1 && c.spill >= 1 && c.far_rec >= 1 &&
+         c.near_rec >= 1 && c.s_rec >= 1 && c.queue >= 1 && c.far_rec < (int64_t)UINT32_MAX &&
+         c.near_rec < (int64_t)UINT32_MAX && c.s_rec < (int64_t)INT32_MAX &&
+         c.queue < (int64_t)UINT32_MAX && c.far_rec < (1ll << 30) && c.near_rec < (1ll << 30);
+}
+
+}  // namespace ygx
+
+extern "C" {
+
+size_t ygx_target_walk_workspace_size(int64_t total, int64_t num_leaves, const int64_t* caps) {
+  if (!caps) return 0;
+  ygx::TwCaps c{caps[0], caps[1], caps[2], caps[3], caps[4], caps[5], caps[6], caps[7]};
+  ygx::Arena a{nullptr, 0, 0};
+  ygx::carve_tw(a, total, num_leaves, c);
+  return a.used + 256;
+}
+
+int ygx_target_walk(const float* center, const float* radius, const float* max_extent,
+                    const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
+                    const int32_t* parent32, const int32_t* level32, const int32_t* nbl32,
+                    int64_t total, int64_t num_internal, int root, int mac, float theta,
+                    float dehnen_radius_scale, const int64_t* caps,
+                    const void* tree_level_offsets, int num_levels, int index_bits,
+                    uint64_t* stats_out, uint64_t* needs_out,
+                    uint32_t* flags_out, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  using namespace ygx;
+  if (total < 3 || total > INT32_MAX || num_internal < 1 || mac < 0 || mac > 2 || !caps ||
+      !stats_out || !needs_out || !flags_out || !tree_level_offsets || num_levels < 2 ||
+      num_levels > kTwHist / 2 || root < 0 || root >= total ||
+      (index_bits != 32 && index_bits != 64))
+    return YGX_ERR_ARG;
+  if (!center || !radius || !max_extent || !left32 || !right32 || !leafpos32 || !parent32 ||
+      !level32 || !nbl32 || !ws)
+    return YGX_ERR_ARG;
+  TwCaps c{caps[0], caps[1], caps[2], caps[3], caps[4], caps[5], caps[6], caps[7]};
+  if (!caps_ok(c)) return YGX_ERR_ARG;
+  if (ws_bytes < ygx_target_walk_workspace_size(total, total - num_internal, caps))
+    return YGX_ERR_ARG;
+  const int64_t L = total - num_internal;
+  Arena ar{(char*)ws, 0, ws_bytes};
+  TwScratch s = carve_tw(ar, total, L, c);
+  const size_t zero_bytes = (size_t)((char*)(s.near_cnt + (L > 0 ? L : 1)) - (char*)s.status);
+  if (cudaMemsetAsync(s.status, 0, zero_bytes, stream) != cudaSuccess ||
+      cudaMemsetAsync(s.q_ready, 0, sizeof(unsigned int) * c.queue, stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  const int32_t T = (int32_t)total, NI = (int32_t)num_internal;
+  k_tw_first_leaf<<<grid_for(L, 256), 256, 0, stream>>>(parent32, left32, NI, T, s.first);
+  YGX_CHECK_LAUNCH();
+  k_tw_recs<<<grid_for(total, 256), 256, 0, stream>>>(center, radius, max_extent, left32,
+                                                      right32, leafpos32, s.first, T, mac,
+                                                      dehnen_radius_scale, nbl32, s.rank, s.recs,
+                                                      s.status);
+  YGX_CHECK_LAUNCH();
+  k_tw_init_nodes<<<grid_for(total, 256), 256, 0, stream>>>(T, root, s.s_head, s.s_off, s.done);
+  YGX_CHECK_LAUNCH();
+  const float th = theta;
+  TwArgs a;
+  a.recs = s.recs;
+  a.nbl = nbl32;
+  a.parent = parent32;
+  a.level = level32;
+  a.rank = s.rank;
+  a.ni = NI;
+  a.total = T;
+  a.lo = 1;  // level 0 holds the root alone
+  a.n_targets = T - 1;
+  a.theta_sq = th * th;
+  a.theta = sqrtf(a.theta_sq);
+  a.s_off = s.s_off;
+  a.s_cnt = s.s_cnt;
+  a.s_ins = s.s_ins;
+  a.s_head = s.s_head;
+  a.s_nch = s.s_nch;
+  a.pieces_left = s.pieces_left;
+  a.done = s.done;
+  a.far_cnt = s.far_cnt;
+  a.near_cnt = s.near_cnt;
+  a.far_pool = s.far_pool;
+  a.near_pool = s.near_pool;
+  a.s_pool = s.s_pool;
+  a.spill = s.spill;
+  a.far_cap = (unsigned long long)c.far;
+  a.near_cap = (unsigned long long)c.near_;
+  a.s_cap = (unsigned long long)c.split;
+  a.spill_cap = (unsigned long long)c.spill;
+  a.far_keys = s.far_keys;
+  a.far_recs = s.far_recs;
+  a.near_keys = s.near_keys;
+  a.near_recs = s.near_recs;
+  a.s_recs = s.s_recs;
+  a.far_rec_cap = (unsigned)c.far_rec;
+  a.near_rec_cap = (unsigned)c.near_rec;
+  a.s_rec_cap = (unsigned)c.s_rec;
+  a.q_cap = (unsigned)c.queue;
+  a.queue = s.queue;
+  a.q_ready = s.q_ready;
+  a.gen_hist = s.gen_hist;
+  a.ctl = s.ctl;
+  a.status = s.status;
+  a.spin_limit = (uint32_t)g_tune.spin_limit;
+  a.budget = g_tune.target_budget;
+  const size_t smem = sizeof(TwSmem);
+  static std::atomic<uint64_t> attr0{0}, attr1{0}, attr2{0};
+  const int grid = kNumSMs * kTwBlocksPerSM;
+  cudaError_t e = cudaSuccess;
+  switch (mac) {
+    case kTwBH:
+      e = ensure_smem_limit(k_tw_walk<kTwBH>, (int)smem, attr0);
+      if (e == cudaSuccess) k_tw_walk<kTwBH><<<grid, kTwThreads, smem, stream>>>(a);
+      break;
+    case kTwDehnen:
+      e = ensure_smem_limit(k_tw_walk<kTwDehnen>, (int)smem, attr1);
+      if (e == cudaSuccess) k_tw_walk<kTwDehnen><<<grid, kTwThreads, smem, stream>>>(a);
+      break;
+    default:
+      e = ensure_smem_limit(k_tw_walk<kTwEngblom>, (int)smem, attr2);
+      if (e == cudaSuccess) k_tw_walk<kTwEngblom><<<grid, kTwThreads, smem, stream>>>(a);
+      break;
+  }
+  if (e != cudaSuccess) return YGX_ERR_CUDA;
+  YGX_CHECK_LAUNCH();
+  k_tw_row_stats<<<grid_for(total, 256, kNumSMs * 4), 256, 0, stream>>>(s.far_cnt, T, s.near_cnt,
+                                                                       (int32_t)L, s.rowstat);
+  YGX_CHECK_LAUNCH();
+  TwCtl ctl;
+  unsigned int hist[kTwHist];
+  unsigned long long rs[4];
+  int64_t lvl_off[kTwHist / 2 + 1];
+  int32_t lvl_off32[kTwHist / 2 + 1];
+  const bool i64 = index_bits == 64;
+  if (cudaMemcpyAsync(i64 ? (void*)lvl_off : (void*)lvl_off32, tree_level_offsets,
+                      (size_t)(num_levels + 1) * (i64 ? 8 : 4), cudaMemcpyDeviceToHost,
+                      stream) != cudaSuccess ||
+      cudaMemcpyAsync(&ctl, s.ctl, sizeof(TwCtl), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaMemcpyAsync(hist, s.gen_hist, sizeof(hist), cudaMemcpyDeviceToHost, stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(rs, s.rowstat, sizeof(rs), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaMemcpyAsync(flags_out, s.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  // generations: every node's self pair {v, v} sits at generation depth(v);
+  // every other pair was evaluated once from each side
+  unsigned long long wf2[kTwHist];
+  for (int g = 0; g < kTwHist; ++g) wf2[g] = hist[g];
+  if (!i64)
+    for (int l = 0; l <= num_levels; ++l) lvl_off[l] = lvl_off32[l];
+  for (int l = 0; l < num_levels && l < kTwHist; ++l)
+    wf2[l] += 2ull * (unsigned long long)(lvl_off[l + 1] - lvl_off[l]);
+  unsigned long long mw = 1, gens = 0;
+  for (int g = 0; g < kTwHist; ++g) {
+    if (wf2[g] == 0) continue;
+    gens = (unsigned long long)g + 1;
+    if (g > 0 && wf2[g] / 2 > mw) mw = wf2[g] / 2;
+  }
+  for (int k = 0; k < YGX_TSTAT_WORDS; ++k) stats_out[k] = 0;
+  stats_out[YGX_TSTAT_FAR_TOTAL] = rs[0];
+  stats_out[YGX_TSTAT_NEAR_TOTAL] = rs[1];
+  stats_out[YGX_TSTAT_MAX_FAR] = rs[2];
+  stats_out[YGX_TSTAT_MAX_NEAR] = rs[3];
+  stats_out[YGX_TSTAT_ACCEPT] = ctl.acc_sides / 2;
+  stats_out[YGX_TSTAT_NEAR] = ctl.near_sides / 2;
+  stats_out[YGX_TSTAT_REFINE] = ctl.ref_sides / 2 + (unsigned long long)total;
+  stats_out[YGX_TSTAT_MAX_WF] = mw;
+  stats_out[YGX_TSTAT_GENS] = gens;
+  // what each capacity needed (a re-run with these fits)
+  needs_out[0] = ctl.far_cur;
+  needs_out[1] = ctl.near_cur;
+  needs_out[2] = ctl.s_cur;
+  needs_out[3] = ctl.spill_cur;
+  needs_out[4] = ctl.far_rec_cur;
+  needs_out[5] = ctl.near_rec_cur;
+  needs_out[6] = ctl.s_rec_cur;
+  needs_out[7] = ctl.q_tail;
+  needs_out[8] = ctl.max_cmp;
+  return YGX_OK;
+}
+
+// After ygx_target_walk on the same workspace (and with its capacities):
+// the level-major far lists and the leaf-order near lists in the index dtype,
+// with the reference's offset / count tables.
+int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* caps,
+                          const int32_t* nbl32, const int32_t* level32,
+                          const void* tree_level_offsets, int num_levels, int index_bits,
+                          int64_t far_total, int64_t near_total, uint64_t far_records,
+                          uint64_t near_records, void* node_offsets, void* far_counts,
+                          void* level_offsets, void* sources, void* targets, void* target_levels,
+                          void* near_offsets, void* near_counts, void* neighbors,
+                          const int32_t* leafpos32, int64_t max_nbr,
+                          void* neighbor_leaf_positions, void* ws, size_t ws_bytes,
+                          cudaStream_t stream) {
+  using namespace ygx;
+  if (total < 3 || num_internal < 1 || !caps || !ws || (index_bits != 32 && index_bits != 64))
+    return YGX_ERR_ARG;
+  TwCaps c{caps[0], caps[1], caps[2], caps[3], caps[4], caps[5], caps[6], caps[7]};
+  if (!caps_ok(c)) return YGX_ERR_ARG;
+  if (ws_bytes < ygx_target_walk_workspace_size(total, total - num_internal, caps))
+    return YGX_ERR_ARG;
+  if ((int64_t)far_records > c.far_rec || (int64_t)near_records > c.near_rec) return YGX_ERR_ARG;
+  const int64_t L = total - num_internal;
+  Arena ar{(char*)ws, 0, ws_bytes};
+  TwScratch s = carve_tw(ar, total, L, c);
+  const int32_t T = (int32_t)total;
+  // offset / count tables
+  k_tw_gather<<<grid_for(total, 256), 256, 0, stream>>>(s.far_cnt, nbl32, T, s.cnt_by_level);
+  YGX_CHECK_LAUNCH();
+  int rc = exclusive_scan<int32_t>(s.cnt_by_level, total, s.obl, s.scan_tmp, stream);
+  if (rc) return rc;
+  k_tw_far_tables<<<grid_for(total + 1, 256), 256, 0, stream>>>(
+      s.obl, nbl32, s.far_cnt, T, index_bits, node_offsets, far_counts, tree_level_offsets,
+      num_levels, level_offsets);
+  YGX_CHECK_LAUNCH();
+  rc = exclusive_scan<int32_t>(s.near_cnt, L, s.near_off, s.scan_tmp, stream);
+  if (rc) return rc;
+  k_tw_near_tables<<<grid_for(L + 1, 256), 256, 0, stream>>>(s.near_off, s.near_cnt, (int32_t)L,
+                                                            index_bits, near_offsets, near_counts);
+  YGX_CHECK_LAUNCH();
+  // rows: sort the chunk records by (row, class, first id), place them by a
+  // scan of their counts, copy
+  SortScratch sw;
+  {
+    Arena sa{(char*)s.sort_ws, 0, s.sort_ws_bytes};
+    sw = carve_sort_scratch(sa, c.far_rec > c.near_rec ? c.far_rec : c.near_rec);
+  }
+  for (int pass = 0; pass < 2; ++pass) {
+    const bool far = pass == 0;
+    const int64_t m = (int64_t)(far ? far_records : near_records);
+    if (m == 0) continue;
+    // key bits: row (rank or leaf position) << 32 | class | id
+    int64_t rows = far ? total : L;
+    int hi_bits = 1;
+    while ((1ll << hi_bits) < rows) ++hi_bits;
+    rc = onesweep_sort(reinterpret_cast<const uint64_t*>(far ? s.far_keys : s.near_keys),
+                       nullptr, m, 0, 32 + hi_bits, reinterpret_cast<uint64_t*>(s.keys_sorted),
+                       s.order, sw, false, s.status, stream);
+    if (rc) return rc;
+    k_tw_sorted_counts<<<grid_for(m, 256), 256, 0, stream>>>(s.order, far ? s.far_recs : s.near_recs,
+                                                            m, s.sorted_cnt);
+    YGX_CHECK_LAUNCH();
+    rc = exclusive_scan<int32_t>(s.sorted_cnt, m, s.dest, s.scan_tmp, stream);
+    if (rc) return rc;
+    k_tw_copy<<<grid_for(m * 32, 256, kNumSMs * 16), 256, 0, stream>>>(
+        s.order, far ? s.far_recs : s.near_recs, m, s.dest, far ? s.far_pool : s.near_pool,
+        index_bits, far ? sources : neighbors, far ? targets : nullptr,
+        far ? target_levels : nullptr, level32);
+    YGX_CHECK_LAUNCH();
+  }
+  if (max_nbr > 0 && neighbor_leaf_positions && leafpos32 && L > 0) {
+    k_tw_nbr_leaf_pos<<<grid_for(L * max_nbr, 256), 256, 0, stream>>>(
+        s.near_off, s.near_cnt, L, neighbors, index_bits, leafpos32, max_nbr,
+        neighbor_leaf_positions);
+    YGX_CHECK_LAUNCH();
+  }
+  (void)far_total;
+  (void)near_total;
+  return YGX_OK;
+}
+
+}  // extern "C"

@@ -17,6 +17,7 @@ bool legal(int knob, int v) {
     case YGX_TUNE_ROW_GRID: return v == 4 || v == 8 || v == 16 || v == 32;
     case YGX_TUNE_SORT_TILE: return v >= 0 && v < kSortTileShapes;
     case YGX_TUNE_SPIN_LIMIT: return v >= 0 && v <= kSpinLimitMax;
+    case YGX_TUNE_TARGET_BUDGET: return v >= 1 && v <= 4096;
     default: return false;
   }
 }
@@ -29,6 +30,7 @@ int* slot(int knob) {
     case YGX_TUNE_ROW_GRID: return &g_tune.row_grid_per_sm;
     case YGX_TUNE_SORT_TILE: return &g_tune.sort_tile;
     case YGX_TUNE_SPIN_LIMIT: return &g_tune.spin_limit;
+    case YGX_TUNE_TARGET_BUDGET: return &g_tune.target_budget;
     default: return nullptr;
   }
 }

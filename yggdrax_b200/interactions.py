@@ -231,7 +231,7 @@ def _grow_wf_cap(cap: int, stats) -> int:
         raise L.YgxError("traversal wavefront exceeds 2^32 pairs")
     return min(_WF_CAP_MAX, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
 _TIMING = os.environ.get("YGGDRAX_B200_TIMING", "0") == "1"  # per-pass CUDA-event times
-TRAVERSAL_MODES = ("log", "two_pass", "learned")
+TRAVERSAL_MODES = ("log", "two_pass", "learned", "target")
 _TRAVERSAL_MODE = os.environ.get("YGGDRAX_B200_TRAVERSAL_MODE", "log")
 
 
@@ -244,7 +244,11 @@ def set_traversal_mode(mode: str) -> None:
       walks (counts, then entries written at row cursors);
     * ``"learned"``: one walk writing straight into rows sized by the learned
       capacity predictor (``yggdrax_b200.predictor``); rows that outgrow
-      their prediction are completed from a log.
+      their prediction are completed from a log;
+    * ``"target"``: one warp per target node walks that node's pairs in
+      Morton order, so the rows come out in ascending order with no scatter
+      and no row sort (``ygx_target_walk``); trees with tied leaf codes use
+      ``"log"``.
 
     Environment: ``YGGDRAX_B200_TRAVERSAL_MODE``."""
     global _TRAVERSAL_MODE
@@ -482,6 +486,125 @@ def _learned_walk_fill(topology, d, total, ni, nl, num_levels, center, radius, m
             far_counts, level_offsets, near_offsets, near_counts)
 
 
+# Target mode, per (mac, theta, size octave): what each capacity needed per
+# tree node in the last walk (far / near pools, split lists, spill area,
+# far / near / split chunk records, continuation queue).
+_TARGET_HINTS: dict = {}
+_TARGET_FALLBACK_WARNED: set = set()
+
+
+def _target_caps(total: int, nl: int, hint) -> list:
+    if hint is not None:
+        return [max(1 << 16, int(1.15 * h * total) + 4096) for h in hint]
+    far = max(1 << 20, 256 * total)
+    near = max(1 << 20, 1024 * nl)
+    split = max(1 << 20, 512 * total)
+    return [far, near, split, max(1 << 20, 64 * total), 4 * total + far // 32 + 4096,
+            4 * nl + near // 32 + 4096, 4 * total + split // 64 + 4096, 4 * total + 65536]
+
+
+def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_extent, leafpos32,
+                 theta, mac_type, mac, dehnen_radius_scale, root, timing, evs):
+    """ygx_target_walk + ygx_target_walk_lists: returns the output arrays and
+    stats, or None when the walk cannot serve this tree (then the caller
+    runs the log schedule)."""
+    lib = L.lib()
+    dev = topology.parent.device
+    st = L.stream_handle(dev)
+    ib, idt = INDEX_BITS, INDEX_DTYPE
+    key = _hint_key(mac_type, theta, total, "target")
+    caps = _target_caps(total, nl, _TARGET_HINTS.get(key))
+    runs = 0
+    while True:
+        runs += 1
+        caps_np = np.asarray(caps, np.int64)
+        ws = L.workspace(lib.ygx_target_walk_workspace_size(total, nl, caps_np.ctypes.data), dev)
+        stats = np.zeros(L.TSTAT_WORDS, np.uint64)
+        needs = np.zeros(9, np.uint64)
+        flags = np.zeros(1, np.uint32)
+        L.check(lib.ygx_target_walk(
+            L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32), L.ptr(d.right32),
+            L.ptr(leafpos32), L.ptr(d.parent32), L.ptr(d.level32), L.ptr(d.nbl32), total, ni,
+            root, mac, float(theta), float(dehnen_radius_scale), caps_np.ctypes.data,
+            L.ptr(topology.level_offsets), num_levels, ib, stats.ctypes.data,
+            needs.ctypes.data, flags.ctypes.data, L.ptr(ws), ws.numel(), st), "ygx_target_walk")
+        f = int(flags[0])
+        if f & L.FLAG_BAD_INPUT:
+            raise ValueError("MAC extents must be positive (geometry has zero or NaN extents)")
+        if f & (L.FLAG_TIMEOUT | L.FLAG_MALFORMED):
+            if key not in _TARGET_FALLBACK_WARNED:
+                _TARGET_FALLBACK_WARNED.add(key)
+                logger.warning("target walk could not serve this tree (flags %#x); using the "
+                               "log schedule", f)
+            return None
+        if f & L.FLAG_LOG_OVERFLOW:
+            # A walk cut short by one capacity reports only the needs of the
+            # work it did: grow what overflowed by 2x its need and re-run.
+            grown = [c if int(n) <= c else 2 * int(n) + 4096 for c, n in zip(caps, needs[:8])]
+            if grown == caps or runs > 12:
+                raise L.YgxError(f"target walk capacities did not converge (flags {f:#x})")
+            caps = grown
+            del ws
+            continue
+        if f:
+            raise L.YgxError(f"target walk reported flags {f:#x}")
+        break
+    prev = _TARGET_HINTS.get(key)
+    cur = [int(n) / total for n in needs[:8]]
+    _TARGET_HINTS[key] = cur if prev is None else [max(a, b) for a, b in zip(prev, cur)]
+    if timing:
+        evs[1].record()
+    s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
+    P, Q = s["far_total"], s["near_total"]
+    node_offsets = torch.empty(total + 1, dtype=idt, device=dev)
+    far_counts = torch.empty(total, dtype=idt, device=dev)
+    level_offsets = torch.empty(num_levels + 1, dtype=idt, device=dev)
+    near_offsets = torch.empty(nl + 1, dtype=idt, device=dev)
+    near_counts = torch.empty(nl, dtype=idt, device=dev)
+    sources = torch.empty(P, dtype=idt, device=dev)
+    targets = torch.empty(P, dtype=idt, device=dev)
+    target_levels = torch.empty(P, dtype=idt, device=dev)
+    neighbors = torch.empty(Q, dtype=idt, device=dev)
+    max_nbr = _dense_table_width(s["max_near"], nl, ib, dev)
+    nlp = torch.empty((nl, max_nbr), dtype=idt, device=dev)
+    if timing:
+        evs[2].record()
+    L.check(lib.ygx_target_walk_lists(
+        total, ni, caps_np.ctypes.data, L.ptr(d.nbl32), L.ptr(d.level32),
+        L.ptr(topology.level_offsets), num_levels, ib, P, Q, int(needs[4]), int(needs[5]),
+        L.ptr(node_offsets), L.ptr(far_counts), L.ptr(level_offsets), L.ptr(sources),
+        L.ptr(targets), L.ptr(target_levels), L.ptr(near_offsets), L.ptr(near_counts),
+        L.ptr(neighbors), L.ptr(leafpos32), max_nbr, L.ptr(nlp) if max_nbr > 0 else None,
+        L.ptr(ws), ws.numel(), st), "ygx_target_walk_lists")
+    f = L.read_status(ws)
+    if f:
+        raise L.YgxError(f"target walk lists reported flags {f:#x}")
+    LAST_WALK_STATS.clear()
+    LAST_WALK_STATS.update(s, mode="target", walk_runs=runs,
+                           split_list_max_chunks=int(needs[8]),
+                           continuation_pieces=int(needs[7]))
+    if P == 0:
+        node_offsets.zero_()
+        level_offsets.zero_()
+    return s, node_offsets, far_counts, level_offsets, sources, targets, target_levels, \
+        near_offsets, near_counts, neighbors, nlp
+
+
+def _dense_table_width(max_near: int, nl: int, ib: int, dev) -> int:
+    """Width of the dense neighbour_leaf_positions table, or 0 when it would
+    not fit the budget (warned once per table shape)."""
+    dense_bytes = nl * max_near * (4 if ib == 32 else 8)
+    if dense_bytes > _dense_neighbor_budget(dev):
+        if (nl, max_near) not in _DENSE_WARNED:  # once per table shape
+            _DENSE_WARNED.add((nl, max_near))
+            logger.warning(
+                "neighbor_leaf_positions would need %.1f GiB (%d leaves x %d neighbours); "
+                "returning an empty (L, 0) table -- raise the budget with "
+                "set_dense_neighbor_budget() to build it", dense_bytes / 2**30, nl, max_near)
+        return 0
+    return max_near
+
+
 def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_scale: float,
               wf_capacity: Optional[int] = None) -> _WalkOut:
     """Walk (counts + pair log) -> scan -> fill (scatter) -> finalize on the GPU."""
@@ -518,6 +641,28 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     mac = _MAC_CODES[mac_type]
     root = _root_of(topology, d)
     far_raw_off = near_raw_off = None
+    if mode == "target" and not _host_of(topology).malformed and num_levels >= 2:
+        out = _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_extent,
+                           leafpos32, theta, mac_type, mac, dehnen_radius_scale, root, timing,
+                           evs)
+        if out is not None:
+            (s, node_offsets, far_counts, level_offsets, sources, targets, target_levels,
+             near_offsets, near_counts, neighbors, nlp) = out
+            if timing:
+                evs[3].record()
+                torch.cuda.synchronize(dev)
+                LAST_WALK_STATS.update(walk_ms=evs[0].elapsed_time(evs[1]),
+                                       fill_ms=evs[1].elapsed_time(evs[2]),
+                                       finalize_ms=evs[2].elapsed_time(evs[3]))
+            return _WalkOut(far_counts=far_counts, node_offsets=node_offsets,
+                            level_offsets=level_offsets, sources=sources, targets=targets,
+                            target_levels=target_levels, near_counts=near_counts,
+                            near_offsets=near_offsets, neighbors=neighbors,
+                            neighbor_leaf_positions=nlp, leaf_indices=leaf_indices,
+                            particle_order_leaf_indices=po,
+                            particle_order_to_native_leaf=po_to_native, stats=s,
+                            num_levels=num_levels)
+        mode = "log"
     if mode == "learned":
         (ws, cap, log_cap, s, far_src32, near_nbr32, far_raw_off, near_raw_off, node_offsets,
          far_counts, level_offsets, near_offsets, near_counts) = _learned_walk_fill(
@@ -607,16 +752,7 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     targets = torch.empty(P, dtype=idt, device=dev)
     target_levels = torch.empty(P, dtype=idt, device=dev)
     neighbors = torch.empty(Q, dtype=idt, device=dev)
-    max_nbr = s["max_near"]
-    dense_bytes = nl * max_nbr * (4 if ib == 32 else 8)
-    if dense_bytes > _dense_neighbor_budget(dev):
-        if (nl, max_nbr) not in _DENSE_WARNED:  # once per table shape
-            _DENSE_WARNED.add((nl, max_nbr))
-            logger.warning(
-                "neighbor_leaf_positions would need %.1f GiB (%d leaves x %d neighbours); "
-                "returning an empty (L, 0) table -- raise the budget with "
-                "set_dense_neighbor_budget() to build it", dense_bytes / 2**30, nl, max_nbr)
-        max_nbr = 0
+    max_nbr = _dense_table_width(s["max_near"], nl, ib, dev)
     nlp = torch.empty((nl, max_nbr), dtype=idt, device=dev)
     L.check(lib.ygx_traverse_finalize(
         total, ni, cap, log_cap, L.ptr(d.level32), L.ptr(leafpos32), ib, L.ptr(far_src32),
