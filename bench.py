@@ -554,16 +554,17 @@ def main():
 
 def mode_timings(step, pos_d, mass_d, n, steps, barrier) -> dict:
     """Device time of the step with the plain two-pass traversal (count walk +
-    fill walk, the reference's schedule) and with the learned one-pass
-    traversal (rows sized by the capacity predictor), inputs resident; the
-    median over the steps."""
+    fill walk, the reference's schedule), with the learned one-pass traversal
+    (rows sized by the capacity predictor) and with the per-target walk
+    (rows in Morton order, no scatter or sort), inputs resident; the median
+    over the steps."""
     import torch
 
     import yggdrax_b200 as yb
     from yggdrax_b200.interactions import LAST_WALK_STATS
 
     out = {}
-    for mode in ("two_pass", "learned"):
+    for mode in ("two_pass", "learned", "target"):
         yb.set_traversal_mode(mode)
         try:
             torch.cuda.empty_cache()  # start each schedule from the same allocator state
@@ -585,6 +586,9 @@ def mode_timings(step, pos_d, mass_d, n, steps, barrier) -> dict:
                 rec["predictor"] = {k: LAST_WALK_STATS.get(k) for k in (
                     "over_allocation", "overflow_row_fraction", "overflow_entry_fraction",
                     "ovf_rows", "padded_far", "padded_near", "walk_runs")}
+            if mode == "target":
+                rec["walk"] = {k: LAST_WALK_STATS.get(k) for k in (
+                    "continuation_pieces", "pieces_run", "busy_fraction", "walk_runs")}
             out[mode] = rec
         finally:
             yb.set_traversal_mode("log")

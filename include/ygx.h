@@ -345,9 +345,10 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
  * trees only (nodes 0..num_internal-1 internal, root `root`).
  * caps (host, 8 int64): entry capacities of the far pool, near pool, split
  * lists, spill area; record capacities of far chunks, near chunks,
- * split-list chunks; continuation queue.  needs_out (host, 9 uint64): what
+ * split-list chunks; continuation queue.  needs_out (host, 12 uint64): what
  * each of them needed (re-run with at least these when
- * YGX_FLAG_LOG_OVERFLOW is set), then the most chunks one split list had.
+ * YGX_FLAG_LOG_OVERFLOW is set), then the most chunks one split list had,
+ * the warp cycles spent on pieces and waiting, and the pieces run.
  * flags_out also reports YGX_FLAG_TIMEOUT (a bounded wait gave up) and
  * YGX_FLAG_MALFORMED (a split list had more chunks than can be ordered);
  * with either flag the lists are not produced: use ygx_traverse_walk.

@@ -78,7 +78,17 @@ constexpr int kTwCmpMax = 256; // chunks a split list may have before compaction
 constexpr int kTwSpillGroup = 8;
 constexpr int kTwInhGroup = 64;
 
+// A warp's current allocation block in one pool (kept in shared memory):
+// pool space is claimed from the global cursor in blocks, so most flushes
+// need no global atomic.
+struct TwBlk {
+  unsigned long long cur, end;
+};
+struct TwBlkSet {
+  TwBlk far, near_, s, far_r, near_r, s_r;
+};
 struct TwWarpSmem {
+  TwBlkSet al;  // the warp's allocation blocks
   unsigned long long stk[kTwStk];
   unsigned long long stg_s[kTwStgS];
   int32_t stg_fi[kTwStgF];
@@ -90,17 +100,31 @@ struct TwSmem {
   unsigned int hist[kTwHist];
 };
 
-// Control block (zeroed before the walk).
-struct TwCtl {
-  unsigned long long far_cur, near_cur, s_cur, spill_cur;  // pool cursors (entries)
-  unsigned long long acc_sides, near_sides, ref_sides;     // decision counts (per side)
-  unsigned int far_rec_cur, near_rec_cur, s_rec_cur;       // chunk record cursors
-  unsigned int q_head, q_tail;                             // continuation queue
-  unsigned int tick;                                       // next target
-  int work;                                                // targets + pieces outstanding
-  unsigned int max_cmp;                                    // most chunks of one split list
-  unsigned int pad[4];
+// Control block (zeroed before the walk).  Every counter that many warps
+// update or poll sits on its own 128-byte line, so the atomics of one do not
+// queue behind traffic on another.
+#define TW_LINE(type, name) \
+  type name;                \
+  char name##_pad[128 - sizeof(type)]
+struct __align__(128) TwCtl {
+  TW_LINE(unsigned long long, far_cur);  // pool cursors (entries)
+  TW_LINE(unsigned long long, near_cur);
+  TW_LINE(unsigned long long, s_cur);
+  TW_LINE(unsigned long long, spill_cur);
+  TW_LINE(unsigned int, far_rec_cur);    // chunk record cursors
+  TW_LINE(unsigned int, near_rec_cur);
+  TW_LINE(unsigned int, s_rec_cur);
+  TW_LINE(unsigned int, q_head);         // continuation queue: tickets taken
+  TW_LINE(unsigned int, q_tail);         // slots filled
+  TW_LINE(unsigned int, tick);           // next target
+  TW_LINE(int, work);                    // targets + pieces outstanding
+  // written once per warp at exit
+  unsigned long long acc_sides, near_sides, ref_sides;  // decision counts (per side)
+  unsigned long long busy_cycles, idle_cycles, pieces;  // where the warps' time went
+  unsigned int max_cmp;                                 // most chunks of one split list
+  unsigned int pad[3];
 };
+#undef TW_LINE
 
 struct TwPiece {
   long long spill_off;
@@ -159,7 +183,40 @@ struct TwArgs {
   uint32_t* status;
   uint32_t spin_limit;
   int budget;
+  unsigned long long blk_entries;  // pool block (entries) per claim
+  unsigned int blk_records;        // record block per claim
 };
+
+// Takes n slots from the warp's block *b (in shared memory, touched by lane
+// 0 only), claiming a new block of at least `blk` slots from the global
+// cursor when *b is short.  Warp-collective; false (and the block dropped)
+// when the pool is out of room.
+template <typename U>
+__device__ __forceinline__ bool tw_take(TwBlk* b, unsigned long long n, unsigned long long blk,
+                                        U* cursor, unsigned long long cap, int lane,
+                                        unsigned long long* off) {
+  unsigned long long o = 0;
+  int ok = 1;
+  if (lane == 0) {
+    if (b->cur + n > b->end) {
+      const unsigned long long sz = n > blk ? n : blk;
+      const unsigned long long g = (unsigned long long)atomicAdd(cursor, (U)sz);
+      if (g + sz > cap) {
+        b->cur = b->end = 0;
+        ok = 0;
+      } else {
+        b->cur = g;
+        b->end = g + sz;
+      }
+    }
+    if (ok) {
+      o = b->cur;
+      b->cur += n;
+    }
+  }
+  *off = __shfl_sync(0xffffffffu, o, 0);
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
 
 __device__ __forceinline__ unsigned lanemask_lt_() {
   unsigned m;
@@ -239,25 +296,20 @@ __global__ void k_tw_init_nodes(int32_t total, int32_t root, int32_t* __restrict
 // ---------------------------------------------------------------------------
 // the walk
 
-// Warp-collective: writes the n staged int32 entries to `pool` at a fresh
-// offset and records the chunk.  Returns nothing; counts rows.
+// Warp-collective: writes the n staged int32 entries to `pool` and records
+// the chunk (key: row | class | first id); counts the row.
 __device__ __forceinline__ void tw_flush_rows(const int32_t* stg, int n, int lane, int t,
                                               unsigned long long key_hi, unsigned cls_bit,
                                               int32_t* pool, unsigned long long cap,
-                                              unsigned long long* pool_cur, unsigned long long* keys,
-                                              TwChunk* recs, unsigned rec_cap, unsigned* rec_cur,
-                                              int32_t* cnt_row, uint32_t* status) {
+                                              unsigned long long* pool_cur, TwBlk* pb,
+                                              unsigned long long* keys, TwChunk* recs,
+                                              unsigned rec_cap, unsigned* rec_cur, TwBlk* rb,
+                                              int32_t* cnt_row, const TwArgs& a) {
   if (n == 0) return;
-  unsigned long long off = 0;
-  unsigned ri = 0;
-  if (lane == 0) {
-    off = atomicAdd(pool_cur, (unsigned long long)n);
-    ri = atomicAdd(rec_cur, 1u);
-  }
-  off = __shfl_sync(0xffffffffu, off, 0);
-  ri = __shfl_sync(0xffffffffu, ri, 0);
-  const bool fits = off + (unsigned long long)n <= cap && ri < rec_cap;
-  if (fits) {
+  unsigned long long off = 0, ri = 0;
+  const bool ok = tw_take(pb, (unsigned long long)n, a.blk_entries, pool_cur, cap, lane, &off) &&
+                  tw_take(rb, 1ull, a.blk_records, rec_cur, rec_cap, lane, &ri);
+  if (ok) {
     for (int k = lane; k < n; k += 32) pool[off + k] = stg[k];
     if (lane == 0) {
       keys[ri] = key_hi | cls_bit | (unsigned long long)(uint32_t)stg[0];
@@ -269,22 +321,17 @@ __device__ __forceinline__ void tw_flush_rows(const int32_t* stg, int n, int lan
       atomicAdd(cnt_row, n);
     }
   } else if (lane == 0) {
-    raise_flag(status, kFlagLogOverflow);
+    raise_flag(a.status, kFlagLogOverflow);
   }
 }
 
 __device__ __forceinline__ void tw_flush_split(const unsigned long long* stg, int n, int lane, int t,
-                                               const TwArgs& a) {
+                                               const TwArgs& a, TwBlkSet& al) {
   if (n == 0) return;
-  unsigned long long off = 0;
-  unsigned ri = 0;
-  if (lane == 0) {
-    off = atomicAdd(&a.ctl->s_cur, (unsigned long long)n);
-    ri = atomicAdd(&a.ctl->s_rec_cur, 1u);
-  }
-  off = __shfl_sync(0xffffffffu, off, 0);
-  ri = __shfl_sync(0xffffffffu, ri, 0);
-  const bool fits = off + (unsigned long long)n <= a.s_cap && ri < a.s_rec_cap;
+  unsigned long long off = 0, ri = 0;
+  const bool fits =
+      tw_take(&al.s, (unsigned long long)n, a.blk_entries, &a.ctl->s_cur, a.s_cap, lane, &off) &&
+      tw_take(&al.s_r, 1ull, a.blk_records, &a.ctl->s_rec_cur, a.s_rec_cap, lane, &ri);
   int before = 0;
   for (int k = lane; k < n; k += 32) {
     const unsigned long long e = stg[k];
@@ -449,61 +496,49 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   TwWarpSmem& W = sm.w[warp];
   for (int i = threadIdx.x; i < kTwHist; i += kTwThreads) sm.hist[i] = 0;
+  TwBlkSet& al = W.al;
+  if (lane == 0) al.far = al.near_ = al.s = al.far_r = al.near_r = al.s_r = TwBlk{0ull, 0ull};
   __syncthreads();
   const unsigned lt = lanemask_lt_();
   unsigned long long acc_sides = 0, near_sides = 0, ref_sides = 0;
-  int held = -1;  // a claimed target waiting for its parent
+  unsigned long long busy = 0, idle_cyc = 0, npieces = 0;
+  int held = -1;          // a claimed target waiting for its parent
+  long long ticket = -1;  // this warp's slot in the continuation queue
   uint32_t idle = 0;
-  bool give_up = false;
+  unsigned backoff = 256;  // ns, doubled while there is nothing to do
+  long long t_idle0 = clock64();
 
-  while (!give_up) {
-    // ---- fetch: continuation pieces first, then the held target, then a new target
+  while (true) {
+    // ---- fetch.  Each warp holds one queue ticket (taken with a plain
+    // atomicAdd, so claims never retry) and runs the piece that lands in its
+    // slot; otherwise the held target once its parent is done; otherwise it
+    // claims the next target in level order.
     int kind = 0;  // 0 none, 1 piece, 2 target
     TwPiece pc;
     pc.t = -1;
     pc.spill_off = 0;
     pc.spill_cnt = 0;
     pc.inh_b = pc.inh_e = 0;
-    {
-      int slot = -1;
-      if (lane == 0) {
-        unsigned h = ld_volatile_u32_(&a.ctl->q_head);
-        const unsigned tl = ld_volatile_u32_(&a.ctl->q_tail);
-        while (h < tl && h < a.q_cap) {
-          const unsigned got = atomicCAS(&a.ctl->q_head, h, h + 1);
-          if (got == h) {
-            slot = (int)h;
-            break;
-          }
-          h = got;
-        }
-      }
-      slot = __shfl_sync(0xffffffffu, slot, 0);
-      if (slot >= 0) {
-        if (lane == 0) {
-          uint32_t spins = 0;
-          while (ld_volatile_u32_(&a.q_ready[slot]) == 0u && spins < a.spin_limit) {
-            __nanosleep(64);
-            ++spins;
-          }
-          if (ld_volatile_u32_(&a.q_ready[slot]) == 0u) {
-            raise_flag(a.status, kFlagTimeout);
-            slot = -2;
-          } else {
-            __threadfence();
-          }
-        }
-        slot = __shfl_sync(0xffffffffu, slot, 0);
-        if (slot == -2) break;
+    if (ticket < 0) {
+      unsigned h = 0;
+      if (lane == 0) h = atomicAdd(&a.ctl->q_head, 1u);
+      ticket = (long long)__shfl_sync(0xffffffffu, h, 0);
+    }
+    if (ticket < (long long)a.q_cap) {
+      unsigned r = 0;
+      if (lane == 0) r = ld_volatile_u32_(&a.q_ready[ticket]);
+      r = __shfl_sync(0xffffffffu, r, 0);
+      if (r) {
+        __threadfence();
         __syncwarp();
-        pc = a.queue[slot];
+        pc = a.queue[ticket];
+        ticket = -1;
         kind = 1;
       }
     }
     if (kind == 0 && held >= 0) {
-      const int p = a.parent[held];
       int ready = 0;
-      if (lane == 0) ready = ld_acquire_i32(&a.done[p]);
+      if (lane == 0) ready = ld_acquire_i32(&a.done[a.parent[held]]);
       ready = __shfl_sync(0xffffffffu, ready, 0);
       __syncwarp();
       if (ready) {
@@ -526,31 +561,39 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
       if (idx >= 0) {
         held = a.nbl[a.lo + idx];
         idle = 0;
-        continue;  // check its parent next round (queue first)
+        backoff = 256;
+        continue;  // check its parent next round (queue slot first)
       }
     }
     if (kind == 0) {
+      // done when every target is claimed and nothing is outstanding: no
+      // piece can be pushed any more (an unfilled ticket is abandoned)
       int fin = 0;
       if (lane == 0)
         fin = held < 0 && ld_volatile_u32_(&a.ctl->tick) >= (unsigned)a.n_targets &&
               ld_volatile_i32_(&a.ctl->work) <= 0;
       fin = __shfl_sync(0xffffffffu, fin, 0);
       if (fin) break;
-      __nanosleep(128);
+      __nanosleep(backoff);
+      backoff = backoff < 4096 ? backoff * 2 : 4096;
       if (++idle >= a.spin_limit) {
         if (lane == 0) raise_flag(a.status, kFlagTimeout);
-        give_up = true;
+        break;
       }
       continue;
     }
     idle = 0;
+    backoff = 256;
+    const long long t_busy0 = clock64();
+    idle_cyc += (unsigned long long)(t_busy0 - t_idle0);
+    ++npieces;
 
     // ---- one piece of target t
     const int t = pc.t;
     const TwRec T = a.recs[t];
     const int p = a.parent[t];
-    const int32_t* pk = &a.recs[p].k.x;  // children of p
-    const int sib = pk[0] == t ? pk[1] : pk[0];
+    const int4 pk = a.recs[p].k;  // children of p
+    const int sib = pk.x == t ? pk.y : pk.x;
     const int sib_gen = a.level[p] + 1;
     if (kind == 2) {
       pc.spill_cnt = 0;
@@ -566,6 +609,28 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
     const unsigned long long near_hi = (unsigned long long)(uint32_t)T.k.z << 32;
     int cur = 0, stk_n = 0, steps = 0;
     int n_fi = 0, n_fl = 0, n_n = 0, n_s = 0;
+    auto flush_fi = [&]() {
+      tw_flush_rows(W.stg_fi, n_fi, lane, t, far_hi, 0u, a.far_pool, a.far_cap, &a.ctl->far_cur,
+                    &al.far, a.far_keys, a.far_recs, a.far_rec_cap, &a.ctl->far_rec_cur,
+                    &al.far_r, &a.far_cnt[t], a);
+      n_fi = 0;
+    };
+    auto flush_fl = [&]() {
+      tw_flush_rows(W.stg_fl, n_fl, lane, t, far_hi, 0x80000000u, a.far_pool, a.far_cap,
+                    &a.ctl->far_cur, &al.far, a.far_keys, a.far_recs, a.far_rec_cap,
+                    &a.ctl->far_rec_cur, &al.far_r, &a.far_cnt[t], a);
+      n_fl = 0;
+    };
+    auto flush_n = [&]() {
+      tw_flush_rows(W.stg_n, n_n, lane, t, near_hi, 0u, a.near_pool, a.near_cap,
+                    &a.ctl->near_cur, &al.near_, a.near_keys, a.near_recs, a.near_rec_cap,
+                    &a.ctl->near_rec_cur, &al.near_r, &a.near_cnt[t_leaf ? T.k.z : 0], a);
+      n_n = 0;
+    };
+    auto flush_s = [&]() {
+      tw_flush_split(W.stg_s, n_s, lane, t, a, al);
+      n_s = 0;
+    };
 
     while (stk_n > 0 || cur < src_len) {
       // window: the leftmost (up to) 32 candidates -- stack top first, then source
@@ -664,10 +729,7 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
         if (mfi) {
           if (n_fi + __popc(mfi) > kTwStgF) {
             __syncwarp();
-            tw_flush_rows(W.stg_fi, n_fi, lane, t, far_hi, 0u, a.far_pool, a.far_cap,
-                          &a.ctl->far_cur, a.far_keys, a.far_recs, a.far_rec_cap,
-                          &a.ctl->far_rec_cur, &a.far_cnt[t], a.status);
-            n_fi = 0;
+            flush_fi();
             __syncwarp();
           }
           if (is_fi) W.stg_fi[n_fi + __popc(mfi & lt)] = s;
@@ -676,10 +738,7 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
         if (mfl) {
           if (n_fl + __popc(mfl) > kTwStgF) {
             __syncwarp();
-            tw_flush_rows(W.stg_fl, n_fl, lane, t, far_hi, 0x80000000u, a.far_pool, a.far_cap,
-                          &a.ctl->far_cur, a.far_keys, a.far_recs, a.far_rec_cap,
-                          &a.ctl->far_rec_cur, &a.far_cnt[t], a.status);
-            n_fl = 0;
+            flush_fl();
             __syncwarp();
           }
           if (is_fl) W.stg_fl[n_fl + __popc(mfl & lt)] = s;
@@ -688,10 +747,7 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
         if (mn) {
           if (n_n + __popc(mn) > kTwStgF) {
             __syncwarp();
-            tw_flush_rows(W.stg_n, n_n, lane, t, near_hi, 0u, a.near_pool, a.near_cap,
-                          &a.ctl->near_cur, a.near_keys, a.near_recs, a.near_rec_cap,
-                          &a.ctl->near_rec_cur, &a.near_cnt[T.k.z], a.status);
-            n_n = 0;
+            flush_n();
             __syncwarp();
           }
           if (is_n) W.stg_n[n_n + __popc(mn & lt)] = s;
@@ -700,8 +756,7 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
         if (ms) {
           if (n_s + __popc(ms) > kTwStgS) {
             __syncwarp();
-            tw_flush_split(W.stg_s, n_s, lane, t, a);
-            n_s = 0;
+            flush_s();
             __syncwarp();
           }
           if (is_s) W.stg_s[n_s + __popc(ms & lt)] = e;
@@ -741,17 +796,10 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
     }
     // ---- end of the piece: flush, then account
     __syncwarp();
-    tw_flush_rows(W.stg_fi, n_fi, lane, t, far_hi, 0u, a.far_pool, a.far_cap, &a.ctl->far_cur,
-                  a.far_keys, a.far_recs, a.far_rec_cap, &a.ctl->far_rec_cur, &a.far_cnt[t],
-                  a.status);
-    tw_flush_rows(W.stg_fl, n_fl, lane, t, far_hi, 0x80000000u, a.far_pool, a.far_cap,
-                  &a.ctl->far_cur, a.far_keys, a.far_recs, a.far_rec_cap, &a.ctl->far_rec_cur,
-                  &a.far_cnt[t], a.status);
-    if (t_leaf)
-      tw_flush_rows(W.stg_n, n_n, lane, t, near_hi, 0u, a.near_pool, a.near_cap,
-                    &a.ctl->near_cur, a.near_keys, a.near_recs, a.near_rec_cap,
-                    &a.ctl->near_rec_cur, &a.near_cnt[T.k.z], a.status);
-    tw_flush_split(W.stg_s, n_s, lane, t, a);
+    flush_fi();
+    flush_fl();
+    if (t_leaf) flush_n();
+    flush_s();
     __syncwarp();
     int last = 0;
     if (lane == 0) {
@@ -770,8 +818,29 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
     }
     if (lane == 0) atomicSub(&a.ctl->work, 1);
     __syncwarp();
+    t_idle0 = clock64();
+    busy += (unsigned long long)(t_idle0 - t_busy0);
+  }
+  // ---- unused record slots of this warp's last blocks: empty chunks
+  __syncwarp();
+  for (unsigned long long k = al.far_r.cur + lane; k < al.far_r.end; k += 32) {
+    a.far_keys[k] = 0ull;
+    TwChunk c;
+    c.off = 0;
+    c.cnt = 0;
+    c.t = 0;
+    a.far_recs[k] = c;
+  }
+  for (unsigned long long k = al.near_r.cur + lane; k < al.near_r.end; k += 32) {
+    a.near_keys[k] = 0ull;
+    TwChunk c;
+    c.off = 0;
+    c.cnt = 0;
+    c.t = 0;
+    a.near_recs[k] = c;
   }
   // ---- statistics
+  idle_cyc += (unsigned long long)(clock64() - t_idle0);
   for (int o = 16; o > 0; o >>= 1) {
     acc_sides += __shfl_xor_sync(0xffffffffu, acc_sides, o);
     near_sides += __shfl_xor_sync(0xffffffffu, near_sides, o);
@@ -781,6 +850,9 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
     if (acc_sides) atomicAdd(&a.ctl->acc_sides, acc_sides);
     if (near_sides) atomicAdd(&a.ctl->near_sides, near_sides);
     if (ref_sides) atomicAdd(&a.ctl->ref_sides, ref_sides);
+    atomicAdd(&a.ctl->busy_cycles, busy);
+    atomicAdd(&a.ctl->idle_cycles, idle_cyc);
+    atomicAdd(&a.ctl->pieces, npieces);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < kTwHist; i += kTwThreads)
@@ -1101,6 +1173,19 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
   a.status = s.status;
   a.spin_limit = (uint32_t)g_tune.spin_limit;
   a.budget = g_tune.target_budget;
+  {
+    // allocation blocks: small enough that every warp's open blocks fit the
+    // pools many times over, large enough to keep the global cursors quiet
+    const long long nwarps = (long long)kNumSMs * kTwBlocksPerSM * kTwWarps;
+    long long me = c.far < c.near_ ? c.far : c.near_;
+    me = me < c.split ? me : c.split;
+    long long be = me / (nwarps * 16);
+    a.blk_entries = (unsigned long long)(be < 32 ? 32 : (be > 2048 ? 2048 : be));
+    long long mr = c.far_rec < c.near_rec ? c.far_rec : c.near_rec;
+    mr = mr < c.s_rec ? mr : c.s_rec;
+    long long br = mr / (nwarps * 8);
+    a.blk_records = (unsigned)(br < 4 ? 4 : (br > 64 ? 64 : br));
+  }
   const size_t smem = sizeof(TwSmem);
   static std::atomic<uint64_t> attr0{0}, attr1{0}, attr2{0};
   const int grid = kNumSMs * kTwBlocksPerSM;
@@ -1175,6 +1260,9 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
   needs_out[6] = ctl.s_rec_cur;
   needs_out[7] = ctl.q_tail;
   needs_out[8] = ctl.max_cmp;
+  needs_out[9] = ctl.busy_cycles;  // warp cycles on pieces / waiting, pieces run
+  needs_out[10] = ctl.idle_cycles;
+  needs_out[11] = ctl.pieces;
   return YGX_OK;
 }
 

@@ -520,7 +520,7 @@ def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_ext
         caps_np = np.asarray(caps, np.int64)
         ws = L.workspace(lib.ygx_target_walk_workspace_size(total, nl, caps_np.ctypes.data), dev)
         stats = np.zeros(L.TSTAT_WORDS, np.uint64)
-        needs = np.zeros(9, np.uint64)
+        needs = np.zeros(12, np.uint64)
         flags = np.zeros(1, np.uint32)
         L.check(lib.ygx_target_walk(
             L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32), L.ptr(d.right32),
@@ -582,7 +582,8 @@ def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_ext
     LAST_WALK_STATS.clear()
     LAST_WALK_STATS.update(s, mode="target", walk_runs=runs,
                            split_list_max_chunks=int(needs[8]),
-                           continuation_pieces=int(needs[7]))
+                           continuation_pieces=int(needs[7]), pieces_run=int(needs[11]),
+                           busy_fraction=int(needs[9]) / max(1, int(needs[9]) + int(needs[10])))
     if P == 0:
         node_offsets.zero_()
         level_offsets.zero_()
