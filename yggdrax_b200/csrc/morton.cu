@@ -4,12 +4,13 @@
 // (morton.py:43-77) and the stable argsort of the codes
 // (_tree_impl.py:401, tree.py:403).
 //
-// k_bbox reads the positions once with 16-byte loads and reduces min/max per
-// axis; its last CTA (arrival counter, no waiting) applies the reference's
-// padding.  k_encode reads the positions again (the second read is served
-// largely from L2 for inputs up to ~100 MB), writes the codes, and builds the
-// per-pass digit histograms of the following radix sort so the sort never
-// re-reads the keys for them.
+// k_bbox_encode (one cooperative launch) reduces the per-axis min / max, pads
+// the bounds in its last-arriving CTA, and encodes every point with them,
+// building the per-pass digit histograms of the following radix sort so the
+// sort never re-reads the keys for them; each thread keeps its first chunks
+// in registers across the wait and re-reads the rest in L2-friendly order.
+// k_bbox + k_encode are the two-launch form (used for caller-supplied bounds
+// and where a cooperative launch is unavailable).
 #include "morton.cuh"
 #include "sort.cuh"
 
@@ -18,6 +19,7 @@ namespace {
 
 constexpr int kBBoxThreads = 256;
 constexpr int kBBoxBlocks = kNumSMs * 4;
+constexpr int kFusedMaxBlocks = kNumSMs * 8;  // the fused kernel's grid at most
 
 struct Box {
   float mn[3], mx[3];
@@ -197,6 +199,195 @@ __global__ void __launch_bounds__(kEncodeThreads)
     if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
 }
 
+// Digit histograms of the following sort for the (up to) four codes of one
+// lane; every lane of the warp calls it together.
+__device__ __forceinline__ void hist_codes(uint32_t* s_hist, const uint64_t* code, int valid,
+                                           int passes, int lane) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    for (int p = 0; p < passes; ++p) {
+      const uint32_t d = k < valid ? (uint32_t)(code[k] >> (p * kSortRadixBits)) & (kSortRadix - 1)
+                                   : 0xFFFFu;
+      const unsigned vm = __ballot_sync(0xffffffffu, d != 0xFFFFu);
+      const uint32_t dl = __shfl_sync(0xffffffffu, d, vm ? __ffs(vm) - 1 : 0);
+      if (__all_sync(0xffffffffu, d == dl || d == 0xFFFFu)) {
+        if (lane == 0 && vm) atomicAdd(&s_hist[p * kSortRadix + dl], (uint32_t)__popc(vm));
+      } else if (d != 0xFFFFu) {
+        atomicAdd(&s_hist[p * kSortRadix + d], 1u);
+      }
+    }
+  }
+}
+
+// Loads chunk c (four particles) into f; returns the number of particles in it.
+__device__ __forceinline__ int load_any_chunk(const float* __restrict__ pos, int64_t n, int64_t c,
+                                              bool vec, float f[12]) {
+  if (4 * c + 4 <= n) {
+    load_chunk(pos, c, vec, f);
+    return 4;
+  }
+  int v = 0;
+  for (int k = 0; k < 4; ++k) {
+    const int64_t i = 4 * c + k;
+    if (i < n) {
+      f[3 * k] = pos[3 * i];
+      f[3 * k + 1] = pos[3 * i + 1];
+      f[3 * k + 2] = pos[3 * i + 2];
+      ++v;
+    } else {
+      f[3 * k] = f[3 * k + 1] = f[3 * k + 2] = 0.0f;
+    }
+  }
+  return v;
+}
+
+// Fused infer_bounds + morton_encode_impl + sort histograms, one cooperative
+// launch (every CTA resident).  Phase 1 reduces the per-axis min / max; each
+// thread walks its chunks from the last to the first and keeps its first two
+// in registers.  The last CTA to arrive pads the bounds (bounds.py:29-33) and
+// publishes them; the others wait for that flag (bounded spin; on give-up the
+// status word gets YGX_FLAG_TIMEOUT and the CTA stops).  Phase 2 encodes the
+// two kept chunks without reading them again, then the rest first to last --
+// the order in which phase 1 read them last, so the re-reads are mostly
+// served from L2.
+__global__ void __launch_bounds__(kEncodeThreads, 3)
+    k_bbox_encode(const float* __restrict__ pos, int64_t n, float* __restrict__ partials,
+                  unsigned* __restrict__ arrivals, float* __restrict__ bounds_out,
+                  uint64_t* __restrict__ codes, uint32_t* __restrict__ hist, int passes,
+                  uint32_t spin_limit, uint32_t* __restrict__ status) {
+  __shared__ uint32_t s_hist[8 * kSortRadix];
+  __shared__ Box s_box[kEncodeThreads / 32];
+  __shared__ int s_last, s_ok;
+  for (int i = threadIdx.x; i < passes * kSortRadix; i += blockDim.x) s_hist[i] = 0;
+  const bool vec = (reinterpret_cast<uintptr_t>(pos) & 15) == 0 &&
+                   (reinterpret_cast<uintptr_t>(codes) & 15) == 0;
+  const int64_t chunks = (n + 3) / 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // the same iteration count for every lane of a warp (histogram ballots)
+  const int64_t gw = g - lane;
+  const int64_t K = gw < chunks ? (chunks - gw + stride - 1) / stride : 0;
+  Box b;
+  b.init();
+  float keep0[12], keep1[12];
+  int v0 = 0, v1 = 0;
+  for (int64_t k = K - 1; k >= 0; --k) {
+    const int64_t c = g + k * stride;
+    float f[12];
+    int v = 0;
+    if (c < chunks) {
+      v = load_any_chunk(pos, n, c, vec, f);
+#pragma unroll
+      for (int j = 0; j < 12; ++j)
+        if (j / 3 < v) b.add(j % 3, f[j]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 12; ++j) f[j] = 0.0f;
+    }
+    if (k == 0) {
+#pragma unroll
+      for (int j = 0; j < 12; ++j) keep0[j] = f[j];
+      v0 = v;
+    } else if (k == 1) {
+#pragma unroll
+      for (int j = 0; j < 12; ++j) keep1[j] = f[j];
+      v1 = v;
+    }
+  }
+  b.warp_reduce();
+  if (lane == 0) s_box[warp] = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Box t = s_box[0];
+    for (int w = 1; w < kEncodeThreads / 32; ++w) t.merge(s_box[w]);
+    float* out = partials + 8 * blockIdx.x;
+    for (int a = 0; a < 3; ++a) { out[a] = t.mn[a]; out[3 + a] = t.mx[a]; }
+    out[6] = __uint_as_float(t.nan);
+    __threadfence();
+    s_last = atomicAdd(&arrivals[0], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    Box t;
+    t.init();
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+      const volatile float* q = partials + 8 * k;
+      Box o;
+      for (int a = 0; a < 3; ++a) { o.mn[a] = q[a]; o.mx[a] = q[3 + a]; }
+      o.nan = __float_as_uint(q[6]);
+      t.merge(o);
+    }
+    t.warp_reduce();
+    if (lane == 0) s_box[warp] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      Box r = s_box[0];
+      for (int w = 1; w < kEncodeThreads / 32; ++w) r.merge(s_box[w]);
+      const float qnan = __int_as_float(0x7fc00000);
+      for (int a = 0; a < 3; ++a) {
+        const float lo = (r.nan >> a) & 1 ? qnan : r.mn[a];
+        const float hi = (r.nan >> a) & 1 ? qnan : r.mx[a];
+        const float span = __fsub_rn(hi, lo);
+        const float pad = fmax_nan(__fmul_rn(span, 0.05f), 1e-6f);
+        bounds_out[a] = __fsub_rn(lo, pad);
+        bounds_out[3 + a] = __fadd_rn(hi, pad);
+      }
+      __threadfence();
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(arrivals + 1), "r"(1u) : "memory");
+    }
+  }
+  if (threadIdx.x == 0) {
+    unsigned ready = 0, spins = 0;
+    while (true) {
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(ready) : "l"(arrivals + 1) : "memory");
+      if (ready || spins >= spin_limit) break;
+      __nanosleep(64);
+      ++spins;
+    }
+    s_ok = ready != 0;
+    if (!ready) raise_flag(status, kFlagTimeout);
+  }
+  __syncthreads();
+  if (!s_ok) return;
+  float mn[3], span[3];
+  for (int a = 0; a < 3; ++a) {
+    mn[a] = bounds_out[a];
+    span[a] = __fsub_rn(bounds_out[3 + a], bounds_out[a]);
+  }
+  for (int64_t k = 0; k < K; ++k) {
+    const int64_t c = g + k * stride;
+    float f[12];
+    int v;
+    if (k == 0) {
+#pragma unroll
+      for (int j = 0; j < 12; ++j) f[j] = keep0[j];
+      v = v0;
+    } else if (k == 1) {
+#pragma unroll
+      for (int j = 0; j < 12; ++j) f[j] = keep1[j];
+      v = v1;
+    } else {
+      v = c < chunks ? load_any_chunk(pos, n, c, vec, f) : 0;
+    }
+    uint64_t code[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) code[q] = encode_one(f[3 * q], f[3 * q + 1], f[3 * q + 2], mn, span);
+    if (v == 4 && vec) {
+      ulonglong2* o = reinterpret_cast<ulonglong2*>(codes + 4 * c);
+      o[0] = make_ulonglong2(code[0], code[1]);
+      o[1] = make_ulonglong2(code[2], code[3]);
+    } else {
+      for (int q = 0; q < v; ++q) codes[4 * c + q] = code[q];
+    }
+    if (passes > 0) hist_codes(s_hist, code, v, passes, lane);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * kSortRadix; i += blockDim.x)
+    if (s_hist[i]) atomicAdd(&hist[i], s_hist[i]);
+}
+
 // ---- batched sets (segments [off[s], off[s+1]) of one position array) ---------
 
 // Bounds of every set: one CTA per set, the same reduction and padding as
@@ -286,6 +477,30 @@ __global__ void k_gather_codes(const uint64_t* __restrict__ codes, const uint32_
 
 }  // namespace
 
+// Grid of the fused kernel: every CTA must be resident at once (cooperative
+// launch), at most kFusedMaxBlocks; 0 when the device cannot say.
+static int fused_grid() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  static std::atomic<int> cache[64];
+  int g = cache[dev].load(std::memory_order_relaxed);
+  if (g != 0) return g > 0 ? g : 0;
+  int per_sm = 0, sms = 0, coop = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bbox_encode, kEncodeThreads, 0) !=
+          cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    g = -1;
+  } else {
+    g = coop ? per_sm * sms : -1;
+    if (g > kFusedMaxBlocks) g = kFusedMaxBlocks;
+    if (g <= 0) g = -1;
+  }
+  cache[dev].store(g, std::memory_order_relaxed);
+  return g > 0 ? g : 0;
+}
+
 struct EncodeSortLayout {
   uint32_t* status;
   float* partials;
@@ -296,7 +511,7 @@ struct EncodeSortLayout {
 static EncodeSortLayout carve_encode_sort(Arena& a, int64_t n) {
   EncodeSortLayout l;
   l.status = a.take<uint32_t>(64);
-  l.partials = a.take<float>(8 * kBBoxBlocks);
+  l.partials = a.take<float>(8 * kFusedMaxBlocks);
   l.arrivals = a.take<unsigned>(64);
   l.sort = carve_sort_scratch(a, n);
   return l;
@@ -436,19 +651,51 @@ int ygx_encode_sort(const float* positions, int64_t n, const float* bounds_in, f
     if (cudaMemcpyAsync(bounds_out, bounds_in, 6 * sizeof(float), cudaMemcpyDeviceToDevice,
                         stream) != cudaSuccess)
       return YGX_ERR_CUDA;
-  } else {
-    if (cudaMemsetAsync(l.arrivals, 0, sizeof(unsigned), stream) != cudaSuccess) return YGX_ERR_CUDA;
-    int grid = ygx::grid_for((n + 3) / 4, ygx::kBBoxThreads, ygx::kBBoxBlocks);
-    ygx::k_bbox<<<grid, ygx::kBBoxThreads, 0, stream>>>(positions, n, l.partials, l.arrivals,
-                                                        bounds_out);
-    YGX_CHECK_LAUNCH();
   }
   const int passes = ygx::sort_passes(0, 63);
   if (ygx::sort_scratch_reset(l.sort, n, passes, stream) != cudaSuccess) return YGX_ERR_CUDA;
-  int grid = ygx::grid_for((n + 3) / 4, ygx::kEncodeThreads, ygx::kNumSMs * 8);
-  ygx::k_encode<<<grid, ygx::kEncodeThreads, 0, stream>>>(positions, n, bounds_out, codes_sorted,
-                                                          l.sort.hist, passes);
-  YGX_CHECK_LAUNCH();
+  bool fused = false;
+  if (!bounds_in) {
+    // one cooperative launch: bounds, codes and histograms (see k_bbox_encode)
+    int grid = ygx::fused_grid();
+    if (grid > 0) {
+      const int64_t want = ((n + 3) / 4 + ygx::kEncodeThreads - 1) / ygx::kEncodeThreads;
+      if (want < grid) grid = want > 0 ? (int)want : 1;
+      if (cudaMemsetAsync(l.arrivals, 0, 2 * sizeof(unsigned), stream) != cudaSuccess)
+        return YGX_ERR_CUDA;
+      const float* p_ = positions;
+      int64_t n_ = n;
+      float* part_ = l.partials;
+      unsigned* arr_ = l.arrivals;
+      float* bo_ = bounds_out;
+      uint64_t* co_ = codes_sorted;
+      uint32_t* hi_ = l.sort.hist;
+      int pa_ = passes;
+      uint32_t sl_ = (uint32_t)ygx::g_tune.spin_limit;
+      uint32_t* st_ = l.status;
+      void* args[] = {&p_, &n_, &part_, &arr_, &bo_, &co_, &hi_, &pa_, &sl_, &st_};
+      const cudaError_t e = cudaLaunchCooperativeKernel((const void*)ygx::k_bbox_encode,
+                                                        dim3((unsigned)grid),
+                                                        dim3(ygx::kEncodeThreads), args, 0, stream);
+      ygx::note_launch();
+      if (e == cudaSuccess) fused = true;
+      else (void)cudaGetLastError();  // not launchable here: the two-kernel path below
+    }
+    if (!fused) {
+      if (cudaMemsetAsync(l.arrivals, 0, sizeof(unsigned), stream) != cudaSuccess)
+        return YGX_ERR_CUDA;
+      int g2 = ygx::grid_for((n + 3) / 4, ygx::kBBoxThreads, ygx::kBBoxBlocks);
+      ygx::k_bbox<<<g2, ygx::kBBoxThreads, 0, stream>>>(positions, n, l.partials, l.arrivals,
+                                                        bounds_out);
+      YGX_CHECK_LAUNCH();
+    }
+  }
+  if (!fused) {
+    int grid = ygx::grid_for((n + 3) / 4, ygx::kEncodeThreads, ygx::kNumSMs * 8);
+    ygx::k_encode<<<grid, ygx::kEncodeThreads, 0, stream>>>(positions, n, bounds_out,
+                                                            codes_sorted, l.sort.hist, passes);
+    YGX_CHECK_LAUNCH();
+  }
   return ygx::onesweep_sort(codes_sorted, nullptr, n, 0, 63, codes_sorted, order, l.sort, true,
                             l.status, stream);
 }
