@@ -378,6 +378,48 @@ int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* ca
                           const int32_t* leafpos32, int64_t max_nbr,
                           void* neighbor_leaf_positions, void* ws, size_t ws_bytes,
                           cudaStream_t stream);
+/* ---- row re-layouts ---------------------------------------------------------
+ * Device forms of the jnp gathers / cumsum / nonzero the reference uses to
+ * re-lay its lists.  Index arrays are in the index dtype (index_bits). */
+size_t ygx_layout_workspace_size(int64_t n);
+/* offsets_out[0..n] = exclusive cumulative sum of counts[0..n) (the jnp.cumsum
+ * row offsets of _result_to_neighbors, _interactions_impl.py:3640-3837). */
+int ygx_counts_to_offsets(const void* counts, int64_t n, int index_bits, void* offsets_out,
+                          void* ws, size_t ws_bytes, cudaStream_t stream);
+/* Level-major far rows (node_offsets[v] = start of node v's row in sources)
+ * -> the count-then-fill node-order layout: out_offsets[0..total] = node-order
+ * row starts, out_sources / out_targets (may be NULL) the rows in node order
+ * with every entry's target node (DualTreeWalkResult interaction_*,
+ * CompactTaggedFarPairs; _interactions_impl.py:3561-3637, 5340-5390). */
+int ygx_node_order_far_rows(int64_t total, const void* far_counts, const void* node_offsets,
+                            const void* sources, int index_bits, void* out_offsets,
+                            void* out_sources, void* out_targets, void* ws, size_t ws_bytes,
+                            cudaStream_t stream);
+/* The distinct cells named by idx[0..n_idx) in ascending order (cells_out,
+ * capacity M) with rank_out[c] = position of cell c in that list or -1, and
+ * their number in host *count_out -- jnp.nonzero of the carrier mask of the
+ * native octree walk (_interactions_impl.py:5411-5553).  Synchronizes the
+ * stream; an index outside [0, M) returns YGX_ERR_ARG. */
+int ygx_flag_compact(const void* idx, int64_t n_idx, int64_t M, int index_bits,
+                     int32_t* rank_out, void* cells_out, int64_t* count_out, void* ws,
+                     size_t ws_bytes, cudaStream_t stream);
+/* out[j * width + k] = lookup[values[offsets[j] + k]] for k < counts[j], else
+ * -1 (rows x width): the dense neighbor_leaf_positions table
+ * (_interactions_impl.py:3658-3688).  lookup is int32 over lookup_n values. */
+int ygx_dense_row_table(const void* offsets, const void* counts, int64_t rows, const void* values,
+                        const int32_t* lookup, int64_t lookup_n, int index_bits, int64_t width,
+                        void* out, cudaStream_t stream);
+/* out[i] = table[idx[i]] (idx int64; an index outside the table writes -1
+ * and sets YGX_FLAG_BAD_INPUT in the status word at ws). */
+int ygx_gather_index(const void* table, int64_t table_n, const int64_t* idx, int64_t n,
+                     int index_bits, void* out, void* ws, size_t ws_bytes, cudaStream_t stream);
+/* out[idx[i]] = i for i < n (a permutation's inverse, the jnp scatter of
+ * inverse_permutation, _tree_impl.py:900-910); idx and out are int32 or int64
+ * (idx_bits, out_bits); an index outside [0, out_n) sets YGX_FLAG_BAD_INPUT in
+ * the status word at ws. */
+int ygx_scatter_positions(const void* idx, int idx_bits, int64_t n, int64_t out_n, void* out,
+                          int out_bits, void* ws, size_t ws_bytes, cudaStream_t stream);
+
 /* ---- learned row-capacity predictor (no counterpart in the reference) -----
  * A per-node MLP (YGX_MLP_INPUTS -> 64 -> 64 -> 2, ReLU, fp32) that predicts
  * log2(1 + far row length) and log2(1 + near row length) from the node's

@@ -106,6 +106,13 @@ _SIGS = {
     "ygx_mlp_train_step": (I32, [P, P, P, I32, F32, P, P, P, I64, P, P, SZ, P]),
     "ygx_predict_caps": (I32, [P, P, P, P, P, P, I64, I64, P, I32, I32, F32, I32, P, F32, F32,
                                I32, P, P, P]),
+    "ygx_layout_workspace_size": (SZ, [I64]),
+    "ygx_counts_to_offsets": (I32, [P, I64, I32, P, P, SZ, P]),
+    "ygx_node_order_far_rows": (I32, [I64, P, P, P, I32, P, P, P, P, SZ, P]),
+    "ygx_flag_compact": (I32, [P, I64, I64, I32, P, P, P, P, SZ, P]),
+    "ygx_dense_row_table": (I32, [P, P, I64, P, P, I64, I32, I64, P, P]),
+    "ygx_gather_index": (I32, [P, I64, P, I64, I32, P, P, SZ, P]),
+    "ygx_scatter_positions": (I32, [P, I32, I64, I64, P, I32, P, SZ, P]),
     "ygx_target_walk_workspace_size": (SZ, [I64, I64, P]),
     "ygx_target_walk": (I32, [P, P, P, P, P, P, P, P, P, I64, I64, I32, I32, F32, F32, P, P, I32,
                               I32, P, P, P, P, SZ, P]),

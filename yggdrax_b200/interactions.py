@@ -788,20 +788,22 @@ def _node_order_far_pairs(w, total: int, dev):
     """The far lists in the count-then-fill layout: rows in node order
     (``interaction_offsets``), each row's sources ascending; targets are the
     row's node; tags -1 (no pair policy).  (_raw_to_compact_far_pairs,
-    :5340-5390, reads the same arrays.)"""
+    :5340-5390, reads the same arrays.)  One CUDA re-layout of the level-major
+    rows (ygx_node_order_far_rows)."""
     idt = INDEX_DTYPE
-    counts = w.far_counts.to(torch.int64)
-    no = torch.zeros(total + 1, dtype=torch.int64, device=dev)
-    no[1:] = torch.cumsum(counts, 0)
+    lib = L.lib()
     P = int(w.sources.shape[0])
-    node = torch.repeat_interleave(torch.arange(total, device=dev), counts)
-    within = torch.arange(P, device=dev) - no[node]
-    src_pos = w.node_offsets.to(torch.int64)[node] + within
-    raw_src = w.sources[src_pos] if P else w.sources
-    raw_tgt = node.to(idt)
+    no = torch.empty(total + 1, dtype=idt, device=dev)
+    raw_src = torch.empty(P, dtype=idt, device=dev)
+    raw_tgt = torch.empty(P, dtype=idt, device=dev)
+    ws = L.workspace(lib.ygx_layout_workspace_size(total), dev)
+    L.check(lib.ygx_node_order_far_rows(
+        total, L.ptr(w.far_counts), L.ptr(w.node_offsets), L.ptr(w.sources) if P else None,
+        INDEX_BITS, L.ptr(no), L.ptr(raw_src) if P else None, L.ptr(raw_tgt) if P else None,
+        L.ptr(ws), ws.numel(), L.stream_handle(dev)), "ygx_node_order_far_rows")
     tags = torch.full((P,), -1, dtype=idt, device=dev)
     fpc = torch.tensor(P, dtype=idt, device=dev)
-    return no.to(idt), raw_src, raw_tgt, tags, fpc
+    return no, raw_src, raw_tgt, tags, fpc
 
 
 def _check_capacities(w: _WalkOut, total: int, ni: int, **kw) -> None:

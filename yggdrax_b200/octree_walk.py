@@ -203,7 +203,8 @@ def _walk(view: ExplicitOctreeTraversalView, theta: float, mac_type: str,
     """One walk collecting far rows (far=True) or near rows, re-run with
     larger buffers when the wavefront or the pair log did not fit.  Returns
     (sorted keys, sorted values, row counts, leaf cells or None, flags,
-    stats)."""
+    stats, row of every cell (int32; level rank for far walks, carrier row or
+    -1 for near walks))."""
     if mac_type not in _MAC_CODES:
         raise ValueError(f"Unknown mac_type: {mac_type}")
     if dehnen_radius_scale <= 0:
@@ -214,18 +215,26 @@ def _walk(view: ExplicitOctreeTraversalView, theta: float, mac_type: str,
     M = int(view.parent.shape[0])
     root = int(torch.argmin(view.parent).item())  # first cell without a parent
     rank = torch.empty(M, dtype=torch.int32, device=dev)
+    lws = L.workspace(lib.ygx_layout_workspace_size(M), dev)
     if far:
-        rank[view.nodes_by_level.long()] = torch.arange(M, dtype=torch.int32, device=dev)
+        # rank of every cell in level order (the far rows' sort key)
+        nbl = view.nodes_by_level.to(INDEX_DTYPE).contiguous()
+        L.check(lib.ygx_scatter_positions(L.ptr(nbl), INDEX_BITS, M, M, L.ptr(rank), 32,
+                                          L.ptr(lws), lws.numel(), st), "ygx_scatter_positions")
         leaf8 = view.leaf_mask.to(torch.uint8).contiguous()
         near_row, cells, rows = None, None, M
     else:
-        carrier = torch.zeros(M, dtype=torch.bool, device=dev)
-        carrier[view.radix_leaf_to_oct.long()] = True
-        leaf8 = carrier.to(torch.uint8).contiguous()
-        cells = torch.nonzero(carrier).flatten()
-        rows = int(cells.shape[0])
-        rank.fill_(-1)
-        rank[cells] = torch.arange(rows, dtype=torch.int32, device=dev)
+        # the carrier cells (those holding a radix leaf) in cell order, and the
+        # row of each (-1 for the others)
+        r2o = view.radix_leaf_to_oct.to(INDEX_DTYPE).contiguous()
+        cells = torch.empty(M, dtype=INDEX_DTYPE, device=dev)
+        nrows = np.zeros(1, np.int64)
+        L.check(lib.ygx_flag_compact(L.ptr(r2o), int(r2o.shape[0]), M, INDEX_BITS, L.ptr(rank),
+                                     L.ptr(cells), nrows.ctypes.data, L.ptr(lws), lws.numel(),
+                                     st), "ygx_flag_compact")
+        rows = int(nrows[0])
+        cells = cells[:rows]
+        leaf8 = (rank >= 0).to(torch.uint8).contiguous()
         near_row = rank
     children = view.children.to(INDEX_DTYPE).contiguous()
     counts = view.child_counts.to(INDEX_DTYPE).contiguous()
@@ -263,7 +272,7 @@ def _walk(view: ExplicitOctreeTraversalView, theta: float, mac_type: str,
         break
     _OCT_HINTS[hkey] = (max(h_wf, int(stats[6]) / M), max(h_log, n / M))
     if stop:
-        return None, None, cnt[:rows], cells, f, stats
+        return None, None, cnt[:rows], cells, f, stats, rank
     ko = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
     vo = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
     if n:
@@ -271,7 +280,7 @@ def _walk(view: ExplicitOctreeTraversalView, theta: float, mac_type: str,
         bits = max(1, (max(rows, 2) - 1).bit_length())
         L.check(lib.ygx_sort_pairs(L.ptr(key), L.ptr(val), n, 0, bits, L.ptr(ko), L.ptr(vo),
                                    L.ptr(ws), ws.numel(), st), "ygx_sort_pairs")
-    return ko[:n], vo[:n], cnt[:rows], cells, f, stats
+    return ko[:n], vo[:n], cnt[:rows], cells, f, stats, rank
 
 
 def _octree_topology(tree, what: str):
@@ -308,14 +317,21 @@ def build_octree_native_far_pairs(
     q, fcap, ncap = _capacities(topo, max_interactions_per_node, _DEFAULT_MAX_NEIGHBORS,
                                 max_pair_queue, process_block, traversal_config)
     view = build_explicit_octree_traversal_view(topo)
-    ko, vo, cnt, _, f, _ = _walk(view, theta, mac_type, dehnen_radius_scale, far=True, queue=q,
-                                 far_cap=fcap, near_cap=ncap)
+    ko, vo, cnt, _, f, _, _ = _walk(view, theta, mac_type, dehnen_radius_scale, far=True,
+                                    queue=q, far_cap=fcap, near_cap=ncap)
     if f & _FLAG_FAR:
         raise RuntimeError(_FAR_MSG)
     if f & _FLAG_QUEUE:
         raise RuntimeError(_QUEUE_MSG)
     sources = vo.to(INDEX_DTYPE)
-    targets = view.nodes_by_level[ko]
+    lib = L.lib()
+    dev = sources.device
+    nbl = view.nodes_by_level.to(INDEX_DTYPE).contiguous()
+    targets = torch.empty_like(sources)
+    gws = L.workspace(256, dev)
+    L.check(lib.ygx_gather_index(L.ptr(nbl), int(nbl.shape[0]), L.ptr(ko.contiguous()),
+                                 int(ko.shape[0]), INDEX_BITS, L.ptr(targets), L.ptr(gws),
+                                 gws.numel(), L.stream_handle(dev)), "ygx_gather_index")
     tags = torch.full_like(sources, -1)
     return CompactTaggedOctreeFarPairs(sources=sources, targets=targets, tags=tags)
 
@@ -347,8 +363,9 @@ def build_octree_native_neighbor_lists(
     q, fcap, ncap = _capacities(topo, max_interactions_per_node, max_neighbors_per_leaf,
                                 max_pair_queue, process_block, traversal_config)
     view = build_explicit_octree_traversal_view(topo)
-    ko, vo, counts32, cells, f, _ = _walk(view, theta, mac_type, dehnen_radius_scale,
-                                          far=False, queue=q, far_cap=fcap, near_cap=ncap)
+    ko, vo, counts32, cells, f, _, row_of_cell = _walk(
+        view, theta, mac_type, dehnen_radius_scale, far=False, queue=q, far_cap=fcap,
+        near_cap=ncap)
     if f & _FLAG_NEAR:
         raise RuntimeError(_NEAR_MSG)
     if f & _FLAG_QUEUE:
@@ -356,24 +373,29 @@ def build_octree_native_neighbor_lists(
     dev = cells.device
     idt = INDEX_DTYPE
     rows = int(cells.shape[0])
+    lib = L.lib()
+    st = L.stream_handle(dev)
     leaf_indices = cells.to(idt)
     counts = counts32.to(idt)
-    offsets = torch.zeros(rows + 1, dtype=idt, device=dev)
-    offsets[1:] = torch.cumsum(counts, 0)
+    offsets = torch.empty(rows + 1, dtype=idt, device=dev)
+    lws = L.workspace(lib.ygx_layout_workspace_size(rows), dev)
+    L.check(lib.ygx_counts_to_offsets(L.ptr(counts) if rows else None, rows, INDEX_BITS,
+                                      L.ptr(offsets), L.ptr(lws), lws.numel(), st),
+            "ygx_counts_to_offsets")
     neighbors = vo.to(idt)
     # particle order of the carrier cells: stable by their first particle
-    lib = L.lib()
     starts = view.node_ranges[leaf_indices.long(), 0].to(torch.int64).contiguous()
     order32 = torch.empty(max(rows, 1), dtype=torch.int32, device=dev)
     if rows:
         kk = torch.empty_like(starts)
         ws = L.workspace(lib.ygx_sort_pairs_workspace_size(rows), dev)
         L.check(lib.ygx_sort_pairs(L.ptr(starts), None, rows, 0, 64, L.ptr(kk), L.ptr(order32),
-                                   L.ptr(ws), ws.numel(), L.stream_handle(dev)),
-                "ygx_sort_pairs")
+                                   L.ptr(ws), ws.numel(), st), "ygx_sort_pairs")
     order = order32[:rows].to(torch.int64)
     po_to_native = torch.empty(rows, dtype=idt, device=dev)
-    po_to_native[order] = torch.arange(rows, dtype=idt, device=dev)
+    L.check(lib.ygx_scatter_positions(L.ptr(order32), 32, rows, rows, L.ptr(po_to_native),
+                                      INDEX_BITS, L.ptr(lws), lws.numel(), st),
+            "ygx_scatter_positions")
     # dense (rows, longest row) table of neighbour row positions, -1 padded
     max_nbr = int(counts.max().item()) if rows else 0
     dense_bytes = rows * max_nbr * (4 if INDEX_BITS == 32 else 8)
@@ -387,11 +409,11 @@ def build_octree_native_neighbor_lists(
         max_nbr = 0
     pos = torch.full((rows, max_nbr), -1, dtype=idt, device=dev)
     if max_nbr and neighbors.numel():
-        lookup = torch.full((int(view.parent.shape[0]),), -1, dtype=idt, device=dev)
-        lookup[leaf_indices.long()] = torch.arange(rows, dtype=idt, device=dev)
-        row_of = torch.repeat_interleave(torch.arange(rows, device=dev), counts)
-        col = torch.arange(neighbors.numel(), device=dev) - offsets[row_of]
-        pos[row_of, col] = lookup[neighbors.long()]
+        # row of every neighbour cell (rank_of_cell from the carrier compaction)
+        L.check(lib.ygx_dense_row_table(L.ptr(offsets), L.ptr(counts), rows, L.ptr(neighbors),
+                                        L.ptr(row_of_cell), int(row_of_cell.shape[0]),
+                                        INDEX_BITS, max_nbr, L.ptr(pos), st),
+                "ygx_dense_row_table")
     tb = _target_blocks(counts, offsets, pos, rows, dev)
     return OctreeNativeNeighborList(
         offsets=offsets, neighbors=neighbors, leaf_indices=leaf_indices, counts=counts,
