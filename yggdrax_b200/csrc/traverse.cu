@@ -422,15 +422,16 @@ __global__ void k_init_cursors(const int64_t* __restrict__ far_off, int64_t tota
 }
 
 // Scatter pass: CTA b reads its log region back in order and writes each
-// pair into both endpoints' rows.  Cursors start at each row's offset, so
-// the aggregated atomic yields the write position; k_check_cursors then
+// pair into both endpoints' rows.  Far rows (keys 0..total-1) and near rows
+// (keys total + leaf position) share one cursor array, so every entry makes
+// two warp-aggregated cursor claims whatever its kind.  Cursors start at each
+// row's offset, so the claim yields the write position; k_check_cursors then
 // verifies every row ended exactly at its end.  Nothing past the totals is
 // written.
 __global__ void __launch_bounds__(256)
     k_log_scatter(const int2* __restrict__ log, const unsigned long long* __restrict__ log_cnt,
-                  unsigned long long LR, const int32_t* __restrict__ leafpos,
-                  unsigned long long* __restrict__ far_pos,
-                  unsigned long long* __restrict__ near_pos, unsigned long long far_total,
+                  unsigned long long LR, const int32_t* __restrict__ leafpos, int32_t total,
+                  unsigned long long* __restrict__ pos, unsigned long long far_total,
                   unsigned long long near_total, int32_t* __restrict__ far_src,
                   int32_t* __restrict__ near_nbr, uint32_t* __restrict__ status,
                   uint32_t skip_mask) {
@@ -442,26 +443,24 @@ __global__ void __launch_bounds__(256)
     for (unsigned long long base = threadIdx.x & ~31u; base < n; base += blockDim.x) {
       const unsigned long long i = base + lane;
       int t = 0, sv = 0;
-      bool far = false, nearp = false;
+      bool act = false, nearp = false;
       if (i < n) {
         const int2 e = src[i];
         t = e.x;
         sv = e.y & 0x7fffffff;
         nearp = e.y < 0;
-        far = !nearp;
+        act = true;
       }
-      const unsigned long long pt = agg_pos(far_pos, t, far);
-      const unsigned long long ps = agg_pos(far_pos, sv, far);
-      if (far) {
-        if (pt < far_total) far_src[pt] = sv; else raise_flag(status, kFlagFarOverflow);
-        if (ps < far_total) far_src[ps] = t; else raise_flag(status, kFlagFarOverflow);
-      }
-      const int lt = nearp ? leafpos[t] : 0, ls = nearp ? leafpos[sv] : 0;
-      const unsigned long long qt = agg_pos(near_pos, lt, nearp);
-      const unsigned long long qs = agg_pos(near_pos, ls, nearp);
-      if (nearp) {
-        if (qt < near_total) near_nbr[qt] = sv; else raise_flag(status, kFlagNearOverflow);
-        if (qs < near_total) near_nbr[qs] = t; else raise_flag(status, kFlagNearOverflow);
+      const int kt = act ? (nearp ? total + leafpos[t] : t) : 0;
+      const int ks = act ? (nearp ? total + leafpos[sv] : sv) : 0;
+      const unsigned long long pt = agg_pos(pos, kt, act);
+      const unsigned long long ps = agg_pos(pos, ks, act);
+      if (act) {
+        int32_t* dst = nearp ? near_nbr : far_src;
+        const unsigned long long lim = nearp ? near_total : far_total;
+        const uint32_t fl = nearp ? kFlagNearOverflow : kFlagFarOverflow;
+        if (pt < lim) dst[pt] = sv; else raise_flag(status, fl);
+        if (ps < lim) dst[ps] = t; else raise_flag(status, fl);
       }
     }
   }
@@ -1288,8 +1287,9 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap, i
   s.obl = a.take<int64_t>(total + 1);
   s.far_off = a.take<int64_t>(total + 1);
   s.near_off = a.take<int64_t>(L + 1);
-  s.far_pos = a.take<unsigned long long>(total);
-  s.near_pos = a.take<unsigned long long>(L);
+  // one cursor array: far rows 0..total-1, then the near rows
+  s.far_pos = a.take<unsigned long long>(total + L);
+  s.near_pos = s.far_pos ? s.far_pos + total : nullptr;
   s.scan_tmp = a.take<int64_t>(scan_scratch_elems(total > L ? total : L));
   s.big_rows = a.take<int32_t>(total > L ? total : L);
   s.class_rows = a.take<int32_t>((size_t)kRowClasses * (total > L ? total : L));
@@ -1587,7 +1587,7 @@ int ygx_traverse_fill(int64_t total, int64_t num_internal, int64_t wf_capacity,
                                                                      s.near_off, L, s.near_pos);
   YGX_CHECK_LAUNCH();
   ygx::k_log_scatter<<<ygx::kWalkGrid, 256, 0, stream>>>(
-      s.log, s.log_cnt, s.log_region, leafpos32, s.far_pos, s.near_pos,
+      s.log, s.log_cnt, s.log_region, leafpos32, (int32_t)total, s.far_pos,
       (unsigned long long)far_total, (unsigned long long)near_total, far_src32, near_nbr32,
       s.status, 0u);
   YGX_CHECK_LAUNCH();
@@ -1989,7 +1989,7 @@ int ygx_batch_traverse_lists(
                                                                      s.near_off, Lt, s.near_pos);
   YGX_CHECK_LAUNCH();
   ygx::k_log_scatter<<<ygx::kWalkGrid, 256, 0, stream>>>(
-      s.log, s.log_cnt, s.log_region, leafpos32, s.far_pos, s.near_pos,
+      s.log, s.log_cnt, s.log_region, leafpos32, (int32_t)total, s.far_pos,
       (unsigned long long)far_capacity, (unsigned long long)near_capacity, far_src32, near_nbr32,
       s.status, stop);
   YGX_CHECK_LAUNCH();
