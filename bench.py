@@ -426,17 +426,20 @@ def main():
         barrier()
         w0 = time.time()
         ev[0].record()
+        out = None
         for _ in range(args.steps):
-            tree, geom, inter, nbrs = step(pos_d, mass_d)
+            out = None  # a step's outputs are released before the next allocates
+            out = step(pos_d, mass_d)
         ev[1].record()
         barrier()
         clk.mark(w0, time.time())
     launches = lib.ygx_launch_counter() - launches0
     t_dev = ev[0].elapsed_time(ev[1]) / 1e3 / args.steps
+    tree, geom, inter, nbrs = out
     far_entries = int(inter.sources.numel())
     near_entries = int(nbrs.neighbors.numel())
     total_nodes = int(tree.parent.shape[0])
-    del tree, geom, inter, nbrs
+    del tree, geom, inter, nbrs, out
 
     # -- end to end through the public API from host buffers --------------------
     # Every step copies its inputs from pinned host memory and reads its
@@ -448,7 +451,9 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     d2h = 0
     e0.record()
+    inter = nbrs = None
     for _ in range(args.steps):
+        inter = nbrs = None
         P = pos_h.to(dev, non_blocking=True)
         M = mass_h.to(dev, non_blocking=True)
         _, _, inter, nbrs = step(P, M)
@@ -479,7 +484,9 @@ def main():
     for k in range(2):
         free[k].record(comp)  # after e0: every copy is inside the timed region
     upload(0)
+    inter = nbrs = None
     for k in range(args.steps):
+        inter = nbrs = None
         comp.wait_event(ready[k % 2])
         if k + 1 < args.steps:
             upload(k + 1)
