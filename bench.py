@@ -339,6 +339,8 @@ def main():
                     help="skip timing the batched workload (4096 uneven point sets)")
     ap.add_argument("--roofline-only", action="store_true",
                     help="time only the sort roofline leg (for profiling it)")
+    ap.add_argument("--mode", default="log", choices=["log", "two_pass", "learned", "target"],
+                    help="traversal schedule of the main timing (all give the same lists)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -370,6 +372,7 @@ def main():
     # size (its outermost halo leaf is near to every leaf); the lists are
     # exact without its dense buffers, so run past that check.
     yb.set_reference_limits(False)
+    yb.set_traversal_mode(args.mode)
 
     n = args.n
     pos_np, mass_np = inputs.plummer(n, 4)
@@ -503,9 +506,9 @@ def main():
                              max(3, args.steps))
 
     # -- the same step with the other traversal schedules (same exact lists) ----
-    modes = {"log": {"ms_per_step": t_dev * 1e3, "value": n / t_dev}}
+    modes = {args.mode: {"ms_per_step": t_dev * 1e3, "value": n / t_dev}}
     if not args.no_modes:
-        modes.update(mode_timings(step, pos_d, mass_d, n, args.steps, barrier))
+        modes.update(mode_timings(step, pos_d, mass_d, n, args.steps, barrier, args.mode))
 
     batched = None
     if not args.no_batched:  # every rank (barriers inside), each on its share of the sets
@@ -534,7 +537,7 @@ def main():
             "vs_baseline": None, "dtype": "f32+int64", "data": "synthetic",
             "config": workload_config(n, world, total_nodes, far_entries, near_entries),
             "pairs_per_s": world * (far_entries + near_entries) / t_max,
-            "traversal_mode": "log", "autotune": tuning,
+            "traversal_mode": args.mode, "autotune": tuning,
             "e2e": {"value": world * n / te_max, "unit": "particles/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "schedule": "next step's upload overlapped with this step's compute "
@@ -559,7 +562,7 @@ def main():
     return 0
 
 
-def mode_timings(step, pos_d, mass_d, n, steps, barrier) -> dict:
+def mode_timings(step, pos_d, mass_d, n, steps, barrier, main_mode: str = "log") -> dict:
     """Device time of the step with the plain two-pass traversal (count walk +
     fill walk, the reference's schedule), with the learned one-pass traversal
     (rows sized by the capacity predictor) and with the per-target walk
@@ -571,7 +574,7 @@ def mode_timings(step, pos_d, mass_d, n, steps, barrier) -> dict:
     from yggdrax_b200.interactions import LAST_WALK_STATS
 
     out = {}
-    for mode in ("two_pass", "learned", "target"):
+    for mode in [m for m in ("log", "two_pass", "learned", "target") if m != main_mode]:
         yb.set_traversal_mode(mode)
         try:
             torch.cuda.empty_cache()  # start each schedule from the same allocator state
@@ -598,7 +601,7 @@ def mode_timings(step, pos_d, mass_d, n, steps, barrier) -> dict:
                     "continuation_pieces", "pieces_run", "busy_fraction", "walk_runs")}
             out[mode] = rec
         finally:
-            yb.set_traversal_mode("log")
+            yb.set_traversal_mode(main_mode)
     return out
 
 
