@@ -339,7 +339,8 @@ def main():
                     help="skip timing the batched workload (4096 uneven point sets)")
     ap.add_argument("--roofline-only", action="store_true",
                     help="time only the sort roofline leg (for profiling it)")
-    ap.add_argument("--mode", default="log", choices=["log", "two_pass", "learned", "target"],
+    ap.add_argument("--mode", default="log",
+                    choices=["log", "two_pass", "learned", "target", "target_ordered"],
                     help="traversal schedule of the main timing (all give the same lists)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -566,15 +567,16 @@ def mode_timings(step, pos_d, mass_d, n, steps, barrier, main_mode: str = "log")
     """Device time of the step with the plain two-pass traversal (count walk +
     fill walk, the reference's schedule), with the learned one-pass traversal
     (rows sized by the capacity predictor) and with the per-target walk
-    (rows in Morton order, no scatter or sort), inputs resident; the median
-    over the steps."""
+    (rows without a scatter, then sorted; or in Morton order straight from
+    the walk), inputs resident; the median over the steps."""
     import torch
 
     import yggdrax_b200 as yb
     from yggdrax_b200.interactions import LAST_WALK_STATS
 
     out = {}
-    for mode in [m for m in ("log", "two_pass", "learned", "target") if m != main_mode]:
+    for mode in [m for m in ("log", "two_pass", "learned", "target", "target_ordered")
+                 if m != main_mode]:
         yb.set_traversal_mode(mode)
         try:
             torch.cuda.empty_cache()  # start each schedule from the same allocator state
@@ -596,9 +598,10 @@ def mode_timings(step, pos_d, mass_d, n, steps, barrier, main_mode: str = "log")
                 rec["predictor"] = {k: LAST_WALK_STATS.get(k) for k in (
                     "over_allocation", "overflow_row_fraction", "overflow_entry_fraction",
                     "ovf_rows", "padded_far", "padded_near", "walk_runs")}
-            if mode == "target":
+            if mode in ("target", "target_ordered"):
                 rec["walk"] = {k: LAST_WALK_STATS.get(k) for k in (
-                    "continuation_pieces", "pieces_run", "busy_fraction", "walk_runs")}
+                    "continuation_pieces", "pieces_run", "busy_fraction", "walk_runs", "steps",
+                    "lane_fill")}
             out[mode] = rec
         finally:
             yb.set_traversal_mode(main_mode)

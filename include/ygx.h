@@ -339,27 +339,33 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
  * pair set of _dual_tree_walk_impl, :1119-1905) and the layouts of
  * _result_to_interactions / _result_to_neighbors (:3561-3837).  One warp
  * per target node walks the pairs {t, s} of the reference's symmetric walk
- * that involve t, from the parent's "split on my side" list, in Morton
- * order, so every row comes out in ascending order with no sort; long
- * expansions are split into pieces run by other warps.  Well-formed single
+ * that involve t, from the parent's "split on my side" list; long
+ * expansions are split into pieces run by other warps.  ordered != 0: the
+ * warp walks its candidates in Morton order, so every row comes out in
+ * ascending order with no sort; ordered == 0: every resolved candidate is
+ * emitted at once and only refined ones are expanded (no re-popped lanes),
+ * and ygx_target_walk_lists sorts the rows.  The same `ordered` must be
+ * passed to all three calls of one walk.  Well-formed single
  * trees only (nodes 0..num_internal-1 internal, root `root`).
  * caps (host, 8 int64): entry capacities of the far pool, near pool, split
  * lists, spill area; record capacities of far chunks, near chunks,
- * split-list chunks; continuation queue.  needs_out (host, 12 uint64): what
+ * split-list chunks; continuation queue.  needs_out (host, 14 uint64): what
  * each of them needed (re-run with at least these when
  * YGX_FLAG_LOG_OVERFLOW is set), then the most chunks one split list had,
- * the warp cycles spent on pieces and waiting, and the pieces run.
+ * the warp cycles spent on pieces and waiting, the pieces run, the 32-wide
+ * steps run and the candidates those steps held.
  * flags_out also reports YGX_FLAG_TIMEOUT (a bounded wait gave up) and
  * YGX_FLAG_MALFORMED (a split list had more chunks than can be ordered);
  * with either flag the lists are not produced: use ygx_traverse_walk.
  * stats_out as for ygx_traverse_walk (wf_need / log_need are 0).
  * Synchronizes the stream. */
-size_t ygx_target_walk_workspace_size(int64_t total, int64_t num_leaves, const int64_t* caps);
+size_t ygx_target_walk_workspace_size(int64_t total, int64_t num_leaves, const int64_t* caps,
+                                      int ordered);
 int ygx_target_walk(const float* center, const float* radius, const float* max_extent,
                     const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
                     const int32_t* parent32, const int32_t* level32, const int32_t* nbl32,
                     int64_t total, int64_t num_internal, int root, int mac, float theta,
-                    float dehnen_radius_scale, const int64_t* caps,
+                    float dehnen_radius_scale, const int64_t* caps, int ordered,
                     const void* tree_level_offsets, int num_levels, int index_bits,
                     uint64_t* stats_out, uint64_t* needs_out, uint32_t* flags_out, void* ws,
                     size_t ws_bytes, cudaStream_t stream);
@@ -368,7 +374,7 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
  * target_levels, leaf-ordered near neighbours) in the index dtype, and
  * with max_nbr > 0 the dense neighbour_leaf_positions table (L x max_nbr).
  * far_records / near_records: needs_out[4] / needs_out[5] of the walk. */
-int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* caps,
+int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* caps, int ordered,
                           const int32_t* nbl32, const int32_t* level32,
                           const void* tree_level_offsets, int num_levels, int index_bits,
                           int64_t far_total, int64_t near_total, uint64_t far_records,

@@ -1,12 +1,15 @@
-"""The per-target walk (traversal mode "target") against the oracle.
+"""The per-target walk (traversal modes "target" and "target_ordered")
+against the oracle.
 
 One warp per target node walks that node's pairs of the reference's
-symmetric walk in Morton order (ygx_target_walk); its rows must equal the
-oracle's bit for bit -- offsets, counts, level-major far rows, leaf-order near
-rows -- and its decision counts, largest wavefront and generation count must
-equal what the generation-by-generation walk reports.  The hand-off of long
-expansions to other warps is exercised by a budget of one step per piece,
-and the capacity re-run by starting from capacities far too small.
+symmetric walk (ygx_target_walk): in Morton order ("target_ordered", rows
+ascending straight from the walk) or emitting every resolved pair at once
+("target", rows sorted afterwards).  Its rows must equal the oracle's bit for
+bit -- offsets, counts, level-major far rows, leaf-order near rows -- and its
+decision counts, largest wavefront and generation count must equal what the
+generation-by-generation walk reports.  The hand-off of long expansions to
+other warps is exercised by a budget of one step per piece, and the capacity
+re-run by starting from capacities far too small.
 """
 
 import numpy as np
@@ -35,7 +38,10 @@ def _obuild(oracle, kind, pos, mass, leaf):
     return oracle.build_fixed_depth_octree(pos, mass, target_leaf_particles=leaf)
 
 
-def _run(yb, gt, gg, theta, mac, budget=None):
+MODES = ("target", "target_ordered")
+
+
+def _run(yb, gt, gg, theta, mac, budget=None, mode="target"):
     from yggdrax_b200 import _lib as L
     from yggdrax_b200.interactions import LAST_WALK_STATS
 
@@ -44,7 +50,7 @@ def _run(yb, gt, gg, theta, mac, budget=None):
     L.check(lib.ygx_tune_get(L.TUNE["target_budget"], old.ctypes.data), "ygx_tune_get")
     if budget is not None:
         L.check(lib.ygx_tune_set(L.TUNE["target_budget"], budget), "ygx_tune_set")
-    yb.set_traversal_mode("target")
+    yb.set_traversal_mode(mode)
     try:
         gi, gn, res = yb.build_interactions_and_neighbors(gt, gg, theta=theta, mac_type=mac,
                                                           return_result=True)
@@ -55,6 +61,7 @@ def _run(yb, gt, gg, theta, mac, budget=None):
     return gi, gn, res, stats
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("case,kind,leaf,mac,theta,budget", [
     ("uniform65k", "radix", 16, "dehnen", 0.6, None),
     ("uniform65k", "radix", 16, "bh", 0.5, None),
@@ -66,7 +73,8 @@ def _run(yb, gt, gg, theta, mac, budget=None):
     ("collinear128", "radix", 4, "dehnen", 0.6, None),
     ("dup64", "radix", 4, "dehnen", 0.6, None),  # tied codes: served by the log walk
 ])
-def test_target_walk_matches_oracle(cuda_device, oracle, case, kind, leaf, mac, theta, budget):
+def test_target_walk_matches_oracle(cuda_device, oracle, case, kind, leaf, mac, theta, budget,
+                                    mode):
     import yggdrax_b200 as yb
     from test_gpu_parity import BOUNDS, CASES, _assert_eq, _compare_lists, _to_dev
 
@@ -75,7 +83,7 @@ def test_target_walk_matches_oracle(cuda_device, oracle, case, kind, leaf, mac, 
     del BOUNDS
     gt, ps = _build(yb, kind, P, M, leaf)
     gg = yb.compute_tree_geometry(gt, ps)
-    gi, gn, res, st = _run(yb, gt, gg, theta, mac, budget)
+    gi, gn, res, st = _run(yb, gt, gg, theta, mac, budget, mode)
     ot = _obuild(oracle, kind, pos, mass, leaf)
     og = oracle.compute_tree_geometry(ot, ot.positions_sorted)
     r = oracle.build_interactions_and_neighbors(ot, og, theta=theta, mac_type=mac)
@@ -92,7 +100,8 @@ def test_target_walk_matches_oracle(cuda_device, oracle, case, kind, leaf, mac, 
         assert st["continuation_pieces"] > 0
 
 
-def test_target_walk_capacities_grow_on_overflow(cuda_device):
+@pytest.mark.parametrize("mode", MODES)
+def test_target_walk_capacities_grow_on_overflow(cuda_device, mode):
     """Capacities far too small: the walk reports what it needed and the
     re-run returns the same lists as a walk sized right."""
     import yggdrax_b200 as yb
@@ -105,11 +114,11 @@ def test_target_walk_capacities_grow_on_overflow(cuda_device):
     gt, ps = yb.build_tree(P, M, leaf_size=16, return_reordered=True)[:2]
     gg = yb.compute_tree_geometry(gt, ps)
     total = int(gt.parent.shape[0])
-    key = I._hint_key("dehnen", 0.6, total, "target")
+    key = I._hint_key("dehnen", 0.6, total, mode)
     I._TARGET_HINTS[key] = [1e-6] * 8  # next walk starts from tiny capacities
-    a, an, _, st = _run(yb, gt, gg, 0.6, "dehnen")
+    a, an, _, st = _run(yb, gt, gg, 0.6, "dehnen", mode=mode)
     assert st["walk_runs"] > 1
-    b, bn, _, st2 = _run(yb, gt, gg, 0.6, "dehnen")
+    b, bn, _, st2 = _run(yb, gt, gg, 0.6, "dehnen", mode=mode)
     assert st2["walk_runs"] == 1
     for f in ("offsets", "counts", "sources", "targets", "level_offsets", "target_levels"):
         np.testing.assert_array_equal(_np(getattr(a, f)), _np(getattr(b, f)), err_msg=f)
@@ -117,7 +126,8 @@ def test_target_walk_capacities_grow_on_overflow(cuda_device):
         np.testing.assert_array_equal(_np(getattr(an, f)), _np(getattr(bn, f)), err_msg=f)
 
 
-def test_target_walk_4m_plummer_matches_log_walk(cuda_device):
+@pytest.mark.parametrize("mode", MODES)
+def test_target_walk_4m_plummer_matches_log_walk(cuda_device, mode):
     """4M Plummer sphere (the heavy halo leaves are split over many warps):
     the target walk and the log walk return identical lists."""
     import yggdrax_b200 as yb
@@ -130,7 +140,7 @@ def test_target_walk_4m_plummer_matches_log_walk(cuda_device):
     gg = yb.compute_tree_geometry(gt, ps)
     yb.set_reference_limits(False)
     try:
-        a, an, ares, _ = _run(yb, gt, gg, 0.6, "dehnen")
+        a, an, ares, _ = _run(yb, gt, gg, 0.6, "dehnen", mode=mode)
         b, bn, bres = yb.build_interactions_and_neighbors(gt, gg, theta=0.6, mac_type="dehnen",
                                                           return_result=True)
     finally:

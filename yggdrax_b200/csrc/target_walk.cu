@@ -40,6 +40,7 @@
 // One persistent launch processes every level: warps take pieces first,
 // then targets in level order, and wait (bounded) only on a parent that is
 // still in progress.
+#include "rows.cuh"
 #include "scan.cuh"
 #include "sort.cuh"
 
@@ -87,8 +88,16 @@ struct TwBlk {
 struct TwBlkSet {
   TwBlk far, near_, s, far_r, near_r, s_r;
 };
+// A warp's counters (lane 0 only): decisions per side, cycles on pieces and
+// waiting, pieces, 32-wide steps and the candidates they held.
+struct TwWarpStats {
+  unsigned long long acc, near_, ref, busy, idle, pieces, steps, lanes;
+};
+constexpr unsigned kTwNoTicket = 0xffffffffu;
 struct TwWarpSmem {
   TwBlkSet al;  // the warp's allocation blocks
+  TwWarpStats st;
+  long long t_mark;  // clock at the last piece boundary
   unsigned long long stk[kTwStk];
   unsigned long long stg_s[kTwStgS];
   int32_t stg_fi[kTwStgF];
@@ -121,6 +130,7 @@ struct __align__(128) TwCtl {
   // written once per warp at exit
   unsigned long long acc_sides, near_sides, ref_sides;  // decision counts (per side)
   unsigned long long busy_cycles, idle_cycles, pieces;  // where the warps' time went
+  unsigned long long steps, lanes;  // 32-wide steps run, candidates they held
   unsigned int max_cmp;                                 // most chunks of one split list
   unsigned int pad[3];
 };
@@ -357,8 +367,11 @@ __device__ __forceinline__ void tw_flush_split(const unsigned long long* stg, in
   }
 }
 
-// Warp-collective: compacts node t's split-list chunks (Morton order by their
-// first leaf) into one array.  Called by the warp that ends t's last piece.
+// Warp-collective: compacts node t's split-list chunks into one array --
+// in Morton order by their first leaf when kSortChunks (ordered walks; at
+// most kTwCmpMax chunks), else in list order.  Called by the warp that ends
+// t's last piece.
+template <bool kSortChunks>
 __device__ void tw_compact_split(int t, int lane, const TwArgs& a, unsigned long long* scratch) {
   const int nch = ld_volatile_i32_(&a.s_nch[t]);
   if (nch == 0) {
@@ -371,34 +384,36 @@ __device__ void tw_compact_split(int t, int lane, const TwArgs& a, unsigned long
     return;
   }
   if (lane == 0) atomicMax(&a.ctl->max_cmp, (unsigned)nch);
-  if (nch > kTwCmpMax) {  // cannot order it here: report (the host falls back)
+  if (kSortChunks) {
+    if (nch > kTwCmpMax) {  // cannot order it here: report (the host falls back)
+      if (lane == 0) {
+        raise_flag(a.status, kFlagMalformed);
+        a.s_cnt[t] = 0;  // children see an empty list (the result is discarded)
+        a.s_ins[t] = 0;
+      }
+      return;
+    }
+    // collect (key << 32 | record) pairs; lane 0 walks the list
     if (lane == 0) {
-      raise_flag(a.status, kFlagMalformed);
-      a.s_cnt[t] = 0;  // children see an empty list (the result is discarded)
-      a.s_ins[t] = 0;
-    }
-    return;
-  }
-  // collect (key << 32 | record) pairs; lane 0 walks the list
-  if (lane == 0) {
-    int r = head, k = 0;
-    while (r >= 0 && k < nch) {
-      const TwSChunk c = a.s_recs[r];
-      scratch[k++] = ((unsigned long long)c.key << 32) | (unsigned)r;
-      r = c.next;
-    }
-  }
-  __syncwarp();
-  // odd-even transposition sort of nch <= 256 keys (small; rare)
-  for (int pass = 0; pass < nch; ++pass) {
-    for (int i = 2 * lane + (pass & 1); i + 1 < nch; i += 64) {
-      const unsigned long long x = scratch[i], y = scratch[i + 1];
-      if (x > y) {
-        scratch[i] = y;
-        scratch[i + 1] = x;
+      int r = head, k = 0;
+      while (r >= 0 && k < nch) {
+        const TwSChunk c = a.s_recs[r];
+        scratch[k++] = ((unsigned long long)c.key << 32) | (unsigned)r;
+        r = c.next;
       }
     }
     __syncwarp();
+    // odd-even transposition sort of nch <= 256 keys (small; rare)
+    for (int pass = 0; pass < nch; ++pass) {
+      for (int i = 2 * lane + (pass & 1); i + 1 < nch; i += 64) {
+        const unsigned long long x = scratch[i], y = scratch[i + 1];
+        if (x > y) {
+          scratch[i] = y;
+          scratch[i + 1] = x;
+        }
+      }
+      __syncwarp();
+    }
   }
   const int total = ld_volatile_i32_(&a.s_cnt[t]);
   unsigned long long off = 0;
@@ -413,10 +428,14 @@ __device__ void tw_compact_split(int t, int lane, const TwArgs& a, unsigned long
     return;
   }
   unsigned long long pos = off;
+  int r = head;
   for (int k = 0; k < nch; ++k) {
-    const TwSChunk c = a.s_recs[(unsigned)(scratch[k] & 0xffffffffu)];
+    if (!kSortChunks && r < 0) break;
+    const int ri = kSortChunks ? (int)(unsigned)(scratch[k] & 0xffffffffu) : r;
+    const TwSChunk c = a.s_recs[ri];
     for (int e = lane; e < c.cnt; e += 32) a.s_pool[pos + e] = a.s_pool[c.off + e];
     pos += (unsigned long long)c.cnt;
+    r = c.next;
   }
   if (lane == 0) a.s_off[t] = (long long)off;
 }
@@ -489,7 +508,16 @@ __device__ void tw_hand_off(const TwArgs& a, int lane, int t, const TwPiece& pc,
   }
 }
 
-template <int kMac>
+// kOrd: rows in ascending order straight from the walk (the ordered
+// expansion above).  Otherwise every resolved candidate is emitted at once
+// and only the children of refined ones go back on the stack (no re-popped
+// lanes, no ordered push); the rows are sorted after the walk.
+//
+// Each step is software-pipelined: once this window's outputs are on the
+// stack, the next window is popped and its node records are requested, and
+// only then are this window's resolved entries staged (and flushed), so the
+// record gathers of step k + 1 overlap the emission work of step k.
+template <int kMac, bool kOrd>
 __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a) {
   extern __shared__ __align__(16) unsigned char tw_smem_raw[];
   TwSmem& sm = *reinterpret_cast<TwSmem*>(tw_smem_raw);
@@ -497,16 +525,17 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
   TwWarpSmem& W = sm.w[warp];
   for (int i = threadIdx.x; i < kTwHist; i += kTwThreads) sm.hist[i] = 0;
   TwBlkSet& al = W.al;
-  if (lane == 0) al.far = al.near_ = al.s = al.far_r = al.near_r = al.s_r = TwBlk{0ull, 0ull};
+  if (lane == 0) {
+    al.far = al.near_ = al.s = al.far_r = al.near_r = al.s_r = TwBlk{0ull, 0ull};
+    W.st = TwWarpStats{0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+    W.t_mark = clock64();
+  }
   __syncthreads();
   const unsigned lt = lanemask_lt_();
-  unsigned long long acc_sides = 0, near_sides = 0, ref_sides = 0;
-  unsigned long long busy = 0, idle_cyc = 0, npieces = 0;
-  int held = -1;          // a claimed target waiting for its parent
-  long long ticket = -1;  // this warp's slot in the continuation queue
+  int held = -1;                 // a claimed target waiting for its parent
+  unsigned ticket = kTwNoTicket; // this warp's slot in the continuation queue
   uint32_t idle = 0;
   unsigned backoff = 256;  // ns, doubled while there is nothing to do
-  long long t_idle0 = clock64();
 
   while (true) {
     // ---- fetch.  Each warp holds one queue ticket (taken with a plain
@@ -519,12 +548,12 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
     pc.spill_off = 0;
     pc.spill_cnt = 0;
     pc.inh_b = pc.inh_e = 0;
-    if (ticket < 0) {
+    if (ticket == kTwNoTicket) {
       unsigned h = 0;
       if (lane == 0) h = atomicAdd(&a.ctl->q_head, 1u);
-      ticket = (long long)__shfl_sync(0xffffffffu, h, 0);
+      ticket = __shfl_sync(0xffffffffu, h, 0);
     }
-    if (ticket < (long long)a.q_cap) {
+    if (ticket < a.q_cap) {
       unsigned r = 0;
       if (lane == 0) r = ld_volatile_u32_(&a.q_ready[ticket]);
       r = __shfl_sync(0xffffffffu, r, 0);
@@ -532,7 +561,7 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
         __threadfence();
         __syncwarp();
         pc = a.queue[ticket];
-        ticket = -1;
+        ticket = kTwNoTicket;
         kind = 1;
       }
     }
@@ -584,13 +613,18 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
     }
     idle = 0;
     backoff = 256;
-    const long long t_busy0 = clock64();
-    idle_cyc += (unsigned long long)(t_busy0 - t_idle0);
-    ++npieces;
+    if (lane == 0) {
+      const long long now = clock64();
+      W.st.idle += (unsigned long long)(now - W.t_mark);
+      W.t_mark = now;
+      W.st.pieces += 1ull;
+    }
 
     // ---- one piece of target t
     const int t = pc.t;
-    const TwRec T = a.recs[t];
+    const float4 Tc = a.recs[t].c;
+    const int t_left = a.recs[t].k.x, t_first = a.recs[t].k.w;
+    const bool t_leaf = t_left < 0;
     const int p = a.parent[t];
     const int4 pk = a.recs[p].k;  // children of p
     const int sib = pk.x == t ? pk.y : pk.x;
@@ -602,47 +636,50 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
       if (lane == 0) a.pieces_left[t] = 1;
     }
     const long long s_base = a.s_off[p];
-    const int s_ins = a.s_ins[p];
+    const int s_ins = kOrd ? a.s_ins[p] : 0;
     const int src_len = pc.spill_cnt + (pc.inh_e - pc.inh_b);
-    const bool t_leaf = T.k.x < 0;
-    const unsigned long long far_hi = (unsigned long long)(uint32_t)a.rank[t] << 32;
-    const unsigned long long near_hi = (unsigned long long)(uint32_t)T.k.z << 32;
-    int cur = 0, stk_n = 0, steps = 0;
+    int cur = 0, stk_n = 0, steps = 0, lanes = 0;
     int n_fi = 0, n_fl = 0, n_n = 0, n_s = 0;
+    unsigned c_acc = 0, c_near = 0, c_ref = 0;  // this lane's decisions in this piece
     auto flush_fi = [&]() {
-      tw_flush_rows(W.stg_fi, n_fi, lane, t, far_hi, 0u, a.far_pool, a.far_cap, &a.ctl->far_cur,
+      const unsigned long long hi = (unsigned long long)(uint32_t)a.rank[t] << 32;
+      tw_flush_rows(W.stg_fi, n_fi, lane, t, hi, 0u, a.far_pool, a.far_cap, &a.ctl->far_cur,
                     &al.far, a.far_keys, a.far_recs, a.far_rec_cap, &a.ctl->far_rec_cur,
                     &al.far_r, &a.far_cnt[t], a);
       n_fi = 0;
     };
     auto flush_fl = [&]() {
-      tw_flush_rows(W.stg_fl, n_fl, lane, t, far_hi, 0x80000000u, a.far_pool, a.far_cap,
+      const unsigned long long hi = (unsigned long long)(uint32_t)a.rank[t] << 32;
+      tw_flush_rows(W.stg_fl, n_fl, lane, t, hi, 0x80000000u, a.far_pool, a.far_cap,
                     &a.ctl->far_cur, &al.far, a.far_keys, a.far_recs, a.far_rec_cap,
                     &a.ctl->far_rec_cur, &al.far_r, &a.far_cnt[t], a);
       n_fl = 0;
     };
     auto flush_n = [&]() {
-      tw_flush_rows(W.stg_n, n_n, lane, t, near_hi, 0u, a.near_pool, a.near_cap,
-                    &a.ctl->near_cur, &al.near_, a.near_keys, a.near_recs, a.near_rec_cap,
-                    &a.ctl->near_rec_cur, &al.near_r, &a.near_cnt[t_leaf ? T.k.z : 0], a);
+      const int lp = a.recs[t].k.z;  // leaf position (leaf targets only)
+      const unsigned long long hi = (unsigned long long)(uint32_t)lp << 32;
+      tw_flush_rows(W.stg_n, n_n, lane, t, hi, 0u, a.near_pool, a.near_cap, &a.ctl->near_cur,
+                    &al.near_, a.near_keys, a.near_recs, a.near_rec_cap, &a.ctl->near_rec_cur,
+                    &al.near_r, &a.near_cnt[lp], a);
       n_n = 0;
     };
     auto flush_s = [&]() {
       tw_flush_split(W.stg_s, n_s, lane, t, a, al);
       n_s = 0;
     };
-
-    while (stk_n > 0 || cur < src_len) {
-      // window: the leftmost (up to) 32 candidates -- stack top first, then source
+    // Pops the next window -- the leftmost (up to) 32 candidates: stack top
+    // first, then source -- and requests the node records of its pending
+    // candidates (an id outside the tree is not read; it is reported when
+    // the window is evaluated).
+    auto load_window = [&](unsigned long long& e, int& n, float4& Bc, int4& Bk) {
       const int take_stk = stk_n < 32 ? stk_n : 32;
       const int rest = src_len - cur;
       const int take_src = (32 - take_stk) < rest ? (32 - take_stk) : rest;
-      const int n = take_stk + take_src;
-      unsigned long long e = 0;
-      bool valid = lane < n;
+      n = take_stk + take_src;
+      e = 0ull;
       if (lane < take_stk) {
         e = W.stk[stk_n - 1 - lane];
-      } else if (valid) {
+      } else if (lane < n) {
         const int c = cur + (lane - take_stk);
         if (c < pc.spill_cnt) {
           e = a.spill[pc.spill_off + c];
@@ -655,9 +692,25 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
       }
       stk_n -= take_stk;
       cur += take_src;
-      __syncwarp();  // the popped slots are rewritten below
-      // evaluate pending candidates (an id outside the tree is dropped and
-      // reported, never dereferenced)
+      Bc = make_float4(0.f, 0.f, 0.f, 0.f);
+      Bk = make_int4(-1, -1, -1, -1);
+      if (lane < n && tw_state(e) == 0 && (unsigned)tw_s(e) < (unsigned)a.total) {
+        const TwRec* r = a.recs + tw_s(e);
+        Bc = r->c;
+        Bk = r->k;
+      }
+      __syncwarp();  // the popped slots are rewritten by later pushes
+    };
+
+    unsigned long long e;
+    int n;
+    float4 Bc;
+    int4 Bk;
+    load_window(e, n, Bc, Bk);
+    while (n > 0) {
+      // ---- evaluate pending candidates (an id outside the tree is dropped
+      // and reported, never dereferenced)
+      bool valid = lane < n;
       if (valid && (unsigned)tw_s(e) >= (unsigned)a.total) {
         raise_flag(a.status, kFlagBadInput);
         valid = false;
@@ -668,14 +721,13 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
       if (valid && state == 0) {
         const int s = tw_s(e);
         const int g = tw_gen(e);
-        const TwRec B = a.recs[s];
-        const float dx = __fsub_rn(T.c.x, B.c.x);
-        const float dy = __fsub_rn(T.c.y, B.c.y);
-        const float dz = __fsub_rn(T.c.z, B.c.z);
+        const float dx = __fsub_rn(Tc.x, Bc.x);
+        const float dy = __fsub_rn(Tc.y, Bc.y);
+        const float dz = __fsub_rn(Tc.z, Bc.z);
         float d2 = __fmul_rn(dx, dx);
         d2 = __fadd_rn(d2, __fmul_rn(dy, dy));
         d2 = __fadd_rn(d2, __fmul_rn(dz, dz));
-        const float et = T.c.w, es = B.c.w;
+        const float et = Tc.w, es = Bc.w;
         bool ok;
         if (kMac == kTwEngblom) {
           const float big = fmax_nan(et, es), small = fmin_nan(et, es);
@@ -685,16 +737,16 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
           const float sum = __fadd_rn(et, es);
           ok = __fmul_rn(sum, sum) <= __fmul_rn(a.theta_sq, d2);
         }
-        const bool s_leaf = B.k.x < 0;
+        const bool s_leaf = Bk.x < 0;
         atomicAdd(&sm.hist[g < kTwHist ? g : kTwHist - 1], 1u);
         if (d2 > 0.0f && ok) {
           state = 1;
-          ++acc_sides;
+          ++c_acc;
         } else if (t_leaf && s_leaf) {
           state = 2;
-          ++near_sides;
+          ++c_near;
         } else {
-          ++ref_sides;
+          ++c_ref;
           // split rule on the canonical (lo, hi) orientation
           const bool t_lo = t < s;
           const float e_lo = t_lo ? et : es, e_hi = t_lo ? es : et;
@@ -703,27 +755,29 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
           const bool split_t = t_lo ? split_lo : !split_lo;
           if (split_t) {
             state = 3;
-            e = tw_ent(s, g + 1, 3, B.k.w < T.k.w ? 1 : 0);
+            e = tw_ent(s, g + 1, 3, (kOrd && Bk.w < t_first) ? 1 : 0);
           } else {
             refine_s = true;
-            c0 = tw_ent(B.k.x, g + 1, 0, 0);
-            c1 = tw_ent(B.k.y, g + 1, 0, 0);
+            c0 = tw_ent(Bk.x, g + 1, 0, 0);
+            c1 = tw_ent(Bk.y, g + 1, 0, 0);
           }
         }
         if (state == 1 || state == 2) e = tw_ent(s, g, state, 0);
       }
       const unsigned refm = __ballot_sync(0xffffffffu, refine_s);
-      const int f = refm ? __ffs(refm) - 1 : n;  // lanes [0, f) are resolved: emit them
-      const bool emit = valid && lane < f;
-      // ---- emit in lane order to the staging buffers (flush when full)
-      {
+      // ordered: lanes [0, f) are resolved -- emit them; unordered: every
+      // resolved lane
+      const int f = kOrd ? (refm ? __ffs(refm) - 1 : n) : n;
+      const bool emit = valid && lane < f && (kOrd || !refine_s);
+      // ---- stage this window's emitted entries (flushing when full)
+      auto emit_window = [&]() {
         const int s = tw_s(e);
-        const bool is_fi = emit && state == 1 && s < a.ni;
-        const bool is_fl = emit && state == 1 && s >= a.ni;
+        const bool is_fi = emit && state == 1 && (!kOrd || s < a.ni);
+        const bool is_fl = kOrd && emit && state == 1 && s >= a.ni;
         const bool is_n = emit && state == 2;
         const bool is_s = emit && state == 3;
         const unsigned mfi = __ballot_sync(0xffffffffu, is_fi);
-        const unsigned mfl = __ballot_sync(0xffffffffu, is_fl);
+        const unsigned mfl = kOrd ? __ballot_sync(0xffffffffu, is_fl) : 0u;
         const unsigned mn = __ballot_sync(0xffffffffu, is_n);
         const unsigned ms = __ballot_sync(0xffffffffu, is_s);
         if (mfi) {
@@ -735,7 +789,7 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
           if (is_fi) W.stg_fi[n_fi + __popc(mfi & lt)] = s;
           n_fi += __popc(mfi);
         }
-        if (mfl) {
+        if (kOrd && mfl) {
           if (n_fl + __popc(mfl) > kTwStgF) {
             __syncwarp();
             flush_fl();
@@ -762,21 +816,31 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
           if (is_s) W.stg_s[n_s + __popc(ms & lt)] = e;
           n_s += __popc(ms);
         }
-      }
-      // ---- push lanes [f, n) back in order (children replace their parent)
-      const int nout = (valid && lane >= f) ? (refine_s ? 2 : 1) : 0;
-      int incl = nout;
+      };
+      // ---- outputs that go back on the stack: ordered, lanes [f, n) in
+      // order (children replace their parent); unordered, the children
+      int nout, P, k0;  // this lane's outputs, the warp's, this lane's first index
+      if (kOrd) {
+        nout = (valid && lane >= f) ? (refine_s ? 2 : 1) : 0;
+        int incl = nout;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        P = __shfl_sync(0xffffffffu, incl, 31);
+        k0 = incl - nout;
+      } else {
+        nout = refine_s ? 2 : 0;
+        P = 2 * __popc(refm);
+        k0 = 2 * __popc(refm & lt);
       }
-      const int P = __shfl_sync(0xffffffffu, incl, 31);
-      const int k0 = incl - nout;  // this lane's first output index
       ++steps;
+      lanes += n;
       if (stk_n + P > kTwStk) {
         // no room on the stack: hand these outputs, the stack and the rest
         // of the source to other warps
+        emit_window();
         tw_hand_off(a, lane, t, pc, cur, nout, k0, refine_s ? c0 : e, c1, P, W.stk, stk_n);
         stk_n = 0;
         cur = src_len;
@@ -788,18 +852,43 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
       __syncwarp();
       if (steps >= a.budget && (stk_n > 0 || cur < src_len)) {
         // out of budget: hand the stack and the rest of the source off
+        emit_window();
         tw_hand_off(a, lane, t, pc, cur, 0, 0, 0ull, 0ull, 0, W.stk, stk_n);
         stk_n = 0;
         cur = src_len;
         break;
       }
+      // ---- next window first (its record gathers are in flight while this
+      // window's entries are staged), then this window's emission
+      unsigned long long e2;
+      int n2;
+      float4 Bc2;
+      int4 Bk2;
+      load_window(e2, n2, Bc2, Bk2);
+      emit_window();
+      e = e2;
+      n = n2;
+      Bc = Bc2;
+      Bk = Bk2;
     }
     // ---- end of the piece: flush, then account
     __syncwarp();
     flush_fi();
-    flush_fl();
+    if (kOrd) flush_fl();
     if (t_leaf) flush_n();
     flush_s();
+    for (int o = 16; o > 0; o >>= 1) {
+      c_acc += __shfl_xor_sync(0xffffffffu, c_acc, o);
+      c_near += __shfl_xor_sync(0xffffffffu, c_near, o);
+      c_ref += __shfl_xor_sync(0xffffffffu, c_ref, o);
+    }
+    if (lane == 0) {
+      W.st.acc += c_acc;
+      W.st.near_ += c_near;
+      W.st.ref += c_ref;
+      W.st.steps += (unsigned long long)steps;
+      W.st.lanes += (unsigned long long)lanes;
+    }
     __syncwarp();
     int last = 0;
     if (lane == 0) {
@@ -809,17 +898,20 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
     }
     last = __shfl_sync(0xffffffffu, last, 0);
     if (last) {
-      if (!t_leaf) tw_compact_split(t, lane, a, W.stk);
+      if (!t_leaf) tw_compact_split<kOrd>(t, lane, a, W.stk);
       __syncwarp();
       if (lane == 0) {
         __threadfence();
         st_release_i32(&a.done[t], 1);
       }
     }
-    if (lane == 0) atomicSub(&a.ctl->work, 1);
+    if (lane == 0) {
+      atomicSub(&a.ctl->work, 1);
+      const long long now = clock64();
+      W.st.busy += (unsigned long long)(now - W.t_mark);
+      W.t_mark = now;
+    }
     __syncwarp();
-    t_idle0 = clock64();
-    busy += (unsigned long long)(t_idle0 - t_busy0);
   }
   // ---- unused record slots of this warp's last blocks: empty chunks
   __syncwarp();
@@ -840,19 +932,17 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
     a.near_recs[k] = c;
   }
   // ---- statistics
-  idle_cyc += (unsigned long long)(clock64() - t_idle0);
-  for (int o = 16; o > 0; o >>= 1) {
-    acc_sides += __shfl_xor_sync(0xffffffffu, acc_sides, o);
-    near_sides += __shfl_xor_sync(0xffffffffu, near_sides, o);
-    ref_sides += __shfl_xor_sync(0xffffffffu, ref_sides, o);
-  }
   if (lane == 0) {
-    if (acc_sides) atomicAdd(&a.ctl->acc_sides, acc_sides);
-    if (near_sides) atomicAdd(&a.ctl->near_sides, near_sides);
-    if (ref_sides) atomicAdd(&a.ctl->ref_sides, ref_sides);
-    atomicAdd(&a.ctl->busy_cycles, busy);
-    atomicAdd(&a.ctl->idle_cycles, idle_cyc);
-    atomicAdd(&a.ctl->pieces, npieces);
+    W.st.idle += (unsigned long long)(clock64() - W.t_mark);
+    const TwWarpStats& q = W.st;
+    if (q.acc) atomicAdd(&a.ctl->acc_sides, q.acc);
+    if (q.near_) atomicAdd(&a.ctl->near_sides, q.near_);
+    if (q.ref) atomicAdd(&a.ctl->ref_sides, q.ref);
+    atomicAdd(&a.ctl->busy_cycles, q.busy);
+    atomicAdd(&a.ctl->idle_cycles, q.idle);
+    atomicAdd(&a.ctl->pieces, q.pieces);
+    atomicAdd(&a.ctl->steps, q.steps);
+    atomicAdd(&a.ctl->lanes, q.lanes);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < kTwHist; i += kTwThreads)
@@ -925,6 +1015,22 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Unordered rows: one warp per chunk copies its int32 entries to the row's
+// raw area (the rows are sorted afterwards).
+__global__ void __launch_bounds__(256)
+    k_tw_copy_raw(const uint32_t* __restrict__ order, const TwChunk* __restrict__ recs, int64_t m,
+                  const int64_t* __restrict__ dest, const int32_t* __restrict__ pool,
+                  int32_t* __restrict__ raw) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = w0; i < m; i += nw) {
+    const TwChunk c = recs[order[i]];
+    const int64_t d = dest[i];
+    for (int k = lane; k < c.cnt; k += 32) raw[d + k] = pool[c.off + k];
+  }
+}
+
 // counts in nodes_by_level order; far offsets; index-dtype tables
 __global__ void k_tw_gather(const int32_t* __restrict__ cnt, const int32_t* __restrict__ nbl,
                             int32_t m, int32_t* __restrict__ out) {
@@ -934,13 +1040,16 @@ __global__ void k_tw_gather(const int32_t* __restrict__ cnt, const int32_t* __re
 __global__ void k_tw_far_tables(const int64_t* __restrict__ obl, const int32_t* __restrict__ nbl,
                                 const int32_t* __restrict__ cnt, int32_t total, int index_bits,
                                 void* node_offsets, void* counts_out, const void* tree_level_offsets,
-                                int num_levels, void* level_offsets_out) {
+                                int num_levels, void* level_offsets_out,
+                                int64_t* __restrict__ off_node) {
   for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r <= total; r += gridDim.x * blockDim.x) {
     if (r == total) {
       store_idx(node_offsets, index_bits, total, obl[total]);
+      if (off_node) off_node[total] = obl[total];
     } else {
       const int32_t v = nbl[r];
       store_idx(node_offsets, index_bits, v, obl[r]);
+      if (off_node) off_node[v] = obl[r];
       store_idx(counts_out, index_bits, v, cnt[v]);
     }
     if (r <= num_levels) {
@@ -1021,9 +1130,14 @@ struct TwScratch {
   int64_t* near_off;
   void* sort_ws;
   size_t sort_ws_bytes;
+  // unordered walks: rows assembled raw, then sorted
+  int32_t* far_raw;
+  int32_t* near_raw;
+  int64_t* far_off_node;
+  RowSortScratch rs;
 };
 
-static TwScratch carve_tw(Arena& a, int64_t total, int64_t L, const TwCaps& c) {
+static TwScratch carve_tw(Arena& a, int64_t total, int64_t L, const TwCaps& c, bool ordered) {
   TwScratch s;
   // status word, control block, histogram and row stats first: one memset
   s.status = a.take<uint32_t>(64);
@@ -1067,6 +1181,15 @@ static TwScratch carve_tw(Arena& a, int64_t total, int64_t L, const TwCaps& c) {
   s.near_off = a.take<int64_t>((L > 0 ? L : 1) + 1);
   s.sort_ws_bytes = onesweep_scratch_bytes(mrec) + 256;
   s.sort_ws = a.take<unsigned char>(s.sort_ws_bytes);
+  s.far_raw = s.near_raw = nullptr;
+  s.far_off_node = nullptr;
+  s.rs = RowSortScratch{nullptr, nullptr, nullptr, nullptr, 0};
+  if (!ordered) {
+    s.far_raw = a.take<int32_t>(c.far);
+    s.near_raw = a.take<int32_t>(c.near_);
+    s.far_off_node = a.take<int64_t>(total + 1);
+    s.rs = carve_row_sort(a, total, L);
+  }
   return s;
 }
 
@@ -1081,11 +1204,12 @@ static bool caps_ok(const TwCaps& c) {
 
 extern "C" {
 
-size_t ygx_target_walk_workspace_size(int64_t total, int64_t num_leaves, const int64_t* caps) {
+size_t ygx_target_walk_workspace_size(int64_t total, int64_t num_leaves, const int64_t* caps,
+                                      int ordered) {
   if (!caps) return 0;
   ygx::TwCaps c{caps[0], caps[1], caps[2], caps[3], caps[4], caps[5], caps[6], caps[7]};
   ygx::Arena a{nullptr, 0, 0};
-  ygx::carve_tw(a, total, num_leaves, c);
+  ygx::carve_tw(a, total, num_leaves, c, ordered != 0);
   return a.used + 256;
 }
 
@@ -1093,7 +1217,7 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
                     const int32_t* left32, const int32_t* right32, const int32_t* leafpos32,
                     const int32_t* parent32, const int32_t* level32, const int32_t* nbl32,
                     int64_t total, int64_t num_internal, int root, int mac, float theta,
-                    float dehnen_radius_scale, const int64_t* caps,
+                    float dehnen_radius_scale, const int64_t* caps, int ordered,
                     const void* tree_level_offsets, int num_levels, int index_bits,
                     uint64_t* stats_out, uint64_t* needs_out,
                     uint32_t* flags_out, void* ws, size_t ws_bytes, cudaStream_t stream) {
@@ -1108,11 +1232,11 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
     return YGX_ERR_ARG;
   TwCaps c{caps[0], caps[1], caps[2], caps[3], caps[4], caps[5], caps[6], caps[7]};
   if (!caps_ok(c)) return YGX_ERR_ARG;
-  if (ws_bytes < ygx_target_walk_workspace_size(total, total - num_internal, caps))
+  if (ws_bytes < ygx_target_walk_workspace_size(total, total - num_internal, caps, ordered))
     return YGX_ERR_ARG;
   const int64_t L = total - num_internal;
   Arena ar{(char*)ws, 0, ws_bytes};
-  TwScratch s = carve_tw(ar, total, L, c);
+  TwScratch s = carve_tw(ar, total, L, c, ordered != 0);
   const size_t zero_bytes = (size_t)((char*)(s.near_cnt + (L > 0 ? L : 1)) - (char*)s.status);
   if (cudaMemsetAsync(s.status, 0, zero_bytes, stream) != cudaSuccess ||
       cudaMemsetAsync(s.q_ready, 0, sizeof(unsigned int) * c.queue, stream) != cudaSuccess)
@@ -1187,23 +1311,26 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
     a.blk_records = (unsigned)(br < 4 ? 4 : (br > 64 ? 64 : br));
   }
   const size_t smem = sizeof(TwSmem);
-  static std::atomic<uint64_t> attr0{0}, attr1{0}, attr2{0};
+  static std::atomic<uint64_t> attr[6];
   const int grid = kNumSMs * kTwBlocksPerSM;
   cudaError_t e = cudaSuccess;
-  switch (mac) {
-    case kTwBH:
-      e = ensure_smem_limit(k_tw_walk<kTwBH>, (int)smem, attr0);
-      if (e == cudaSuccess) k_tw_walk<kTwBH><<<grid, kTwThreads, smem, stream>>>(a);
-      break;
-    case kTwDehnen:
-      e = ensure_smem_limit(k_tw_walk<kTwDehnen>, (int)smem, attr1);
-      if (e == cudaSuccess) k_tw_walk<kTwDehnen><<<grid, kTwThreads, smem, stream>>>(a);
-      break;
-    default:
-      e = ensure_smem_limit(k_tw_walk<kTwEngblom>, (int)smem, attr2);
-      if (e == cudaSuccess) k_tw_walk<kTwEngblom><<<grid, kTwThreads, smem, stream>>>(a);
-      break;
+#define YGX_TW(M, O, I)                                                         \
+  e = ensure_smem_limit(k_tw_walk<M, O>, (int)smem, attr[I]);                   \
+  if (e == cudaSuccess) k_tw_walk<M, O><<<grid, kTwThreads, smem, stream>>>(a);
+  if (ordered) {
+    switch (mac) {
+      case kTwBH: YGX_TW(kTwBH, true, 0) break;
+      case kTwDehnen: YGX_TW(kTwDehnen, true, 1) break;
+      default: YGX_TW(kTwEngblom, true, 2) break;
+    }
+  } else {
+    switch (mac) {
+      case kTwBH: YGX_TW(kTwBH, false, 3) break;
+      case kTwDehnen: YGX_TW(kTwDehnen, false, 4) break;
+      default: YGX_TW(kTwEngblom, false, 5) break;
+    }
   }
+#undef YGX_TW
   if (e != cudaSuccess) return YGX_ERR_CUDA;
   YGX_CHECK_LAUNCH();
   k_tw_row_stats<<<grid_for(total, 256, kNumSMs * 4), 256, 0, stream>>>(s.far_cnt, T, s.near_cnt,
@@ -1263,13 +1390,15 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
   needs_out[9] = ctl.busy_cycles;  // warp cycles on pieces / waiting, pieces run
   needs_out[10] = ctl.idle_cycles;
   needs_out[11] = ctl.pieces;
+  needs_out[12] = ctl.steps;  // 32-wide steps and the candidates they held
+  needs_out[13] = ctl.lanes;
   return YGX_OK;
 }
 
 // After ygx_target_walk on the same workspace (and with its capacities):
 // the level-major far lists and the leaf-order near lists in the index dtype,
 // with the reference's offset / count tables.
-int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* caps,
+int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* caps, int ordered,
                           const int32_t* nbl32, const int32_t* level32,
                           const void* tree_level_offsets, int num_levels, int index_bits,
                           int64_t far_total, int64_t near_total, uint64_t far_records,
@@ -1284,12 +1413,13 @@ int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* ca
     return YGX_ERR_ARG;
   TwCaps c{caps[0], caps[1], caps[2], caps[3], caps[4], caps[5], caps[6], caps[7]};
   if (!caps_ok(c)) return YGX_ERR_ARG;
-  if (ws_bytes < ygx_target_walk_workspace_size(total, total - num_internal, caps))
+  if (ws_bytes < ygx_target_walk_workspace_size(total, total - num_internal, caps, ordered))
     return YGX_ERR_ARG;
   if ((int64_t)far_records > c.far_rec || (int64_t)near_records > c.near_rec) return YGX_ERR_ARG;
+  if (!ordered && (far_total > c.far || near_total > c.near_)) return YGX_ERR_ARG;
   const int64_t L = total - num_internal;
   Arena ar{(char*)ws, 0, ws_bytes};
-  TwScratch s = carve_tw(ar, total, L, c);
+  TwScratch s = carve_tw(ar, total, L, c, ordered != 0);
   const int32_t T = (int32_t)total;
   // offset / count tables
   k_tw_gather<<<grid_for(total, 256), 256, 0, stream>>>(s.far_cnt, nbl32, T, s.cnt_by_level);
@@ -1298,7 +1428,7 @@ int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* ca
   if (rc) return rc;
   k_tw_far_tables<<<grid_for(total + 1, 256), 256, 0, stream>>>(
       s.obl, nbl32, s.far_cnt, T, index_bits, node_offsets, far_counts, tree_level_offsets,
-      num_levels, level_offsets);
+      num_levels, level_offsets, s.far_off_node);
   YGX_CHECK_LAUNCH();
   rc = exclusive_scan<int32_t>(s.near_cnt, L, s.near_off, s.scan_tmp, stream);
   if (rc) return rc;
@@ -1329,11 +1459,26 @@ int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* ca
     YGX_CHECK_LAUNCH();
     rc = exclusive_scan<int32_t>(s.sorted_cnt, m, s.dest, s.scan_tmp, stream);
     if (rc) return rc;
-    k_tw_copy<<<grid_for(m * 32, 256, kNumSMs * 16), 256, 0, stream>>>(
-        s.order, far ? s.far_recs : s.near_recs, m, s.dest, far ? s.far_pool : s.near_pool,
-        index_bits, far ? sources : neighbors, far ? targets : nullptr,
-        far ? target_levels : nullptr, level32);
+    if (ordered) {
+      k_tw_copy<<<grid_for(m * 32, 256, kNumSMs * 16), 256, 0, stream>>>(
+          s.order, far ? s.far_recs : s.near_recs, m, s.dest, far ? s.far_pool : s.near_pool,
+          index_bits, far ? sources : neighbors, far ? targets : nullptr,
+          far ? target_levels : nullptr, level32);
+    } else {
+      k_tw_copy_raw<<<grid_for(m * 32, 256, kNumSMs * 16), 256, 0, stream>>>(
+          s.order, far ? s.far_recs : s.near_recs, m, s.dest, far ? s.far_pool : s.near_pool,
+          far ? s.far_raw : s.near_raw);
+    }
     YGX_CHECK_LAUNCH();
+  }
+  if (!ordered) {
+    // every raw row sits at its final offset: sort and widen
+    rc = row_sort_pass(s.rs, total, s.far_off_node, s.far_cnt, level32, s.far_raw, nullptr,
+                       nullptr, index_bits, sources, targets, target_levels, total, stream);
+    if (rc) return rc;
+    rc = row_sort_pass(s.rs, L, s.near_off, s.near_cnt, nullptr, s.near_raw, nullptr, nullptr,
+                       index_bits, neighbors, nullptr, nullptr, total, stream);
+    if (rc) return rc;
   }
   if (max_nbr > 0 && neighbor_leaf_positions && leafpos32 && L > 0) {
     k_tw_nbr_leaf_pos<<<grid_for(L * max_nbr, 256), 256, 0, stream>>>(
@@ -1341,8 +1486,6 @@ int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* ca
         neighbor_leaf_positions);
     YGX_CHECK_LAUNCH();
   }
-  (void)far_total;
-  (void)near_total;
   return YGX_OK;
 }
 

@@ -18,6 +18,7 @@
 // scatter pass reads the log back coalesced and writes each pair into both
 // endpoints' rows at atomic cursors; the finalize pass sorts every row
 // (canonical order) and widens it into the level-major int64/int32 outputs.
+#include "rows.cuh"
 #include "scan.cuh"
 
 namespace ygx {
@@ -1267,6 +1268,44 @@ static int64_t region_capacity(int64_t cap) {
 }
 constexpr int kBigGrid = kNumSMs * 3;
 
+RowSortScratch carve_row_sort(Arena& a, int64_t total, int64_t L) {
+  RowSortScratch s;
+  s.stride = total > L ? total : L;
+  s.n_big = a.take<uint32_t>(64);
+  s.big_rows = a.take<int32_t>(s.stride);
+  s.class_rows = a.take<int32_t>((size_t)kRowClasses * s.stride);
+  s.bitmaps = a.take<uint32_t>((size_t)kBigGrid * ((total + 31) / 32));
+  return s;
+}
+
+int row_sort_pass(const RowSortScratch& s, int64_t rows, const int64_t* off, const int32_t* cnt,
+                  const int32_t* lvl, int32_t* raw, const int64_t* roff, const int32_t* rbase,
+                  int index_bits, void* vals, void* tgts, void* lvls, int64_t universe,
+                  cudaStream_t stream) {
+  const int grid_small = kNumSMs * g_tune.row_grid_per_sm;
+  const size_t big_smem = sizeof(int32_t) * kBlockRowCap;
+  static std::atomic<uint64_t> big_attr{0};
+  if (ensure_smem_limit(k_rows_big, (int)big_smem, big_attr) != cudaSuccess) return YGX_ERR_CUDA;
+  if (rows > s.stride) return YGX_ERR_ARG;
+  if (cudaMemsetAsync(s.n_big, 0, 16 * sizeof(uint32_t), stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  k_rows_classify<<<grid_for(rows, 256), 256, 0, stream>>>(rows, cnt, s.class_rows, s.stride,
+                                                           s.n_big + 1, s.big_rows, s.n_big);
+  YGX_CHECK_LAUNCH();
+#define YGX_ROWS(C, R)                                                                        \
+  k_rows_class<R><<<grid_small, 256, 0, stream>>>(s.class_rows + (C) * s.stride, s.n_big + 1 + (C), \
+                                                  off, cnt, lvl, raw, roff, rbase, index_bits,  \
+                                                  vals, tgts, lvls);                            \
+  YGX_CHECK_LAUNCH();
+  YGX_ROWS(0, 1) YGX_ROWS(1, 2) YGX_ROWS(2, 4) YGX_ROWS(3, 8) YGX_ROWS(4, 16) YGX_ROWS(5, 32)
+#undef YGX_ROWS
+  k_rows_big<<<kBigGrid, kBigThreads, big_smem, stream>>>(s.big_rows, s.n_big, s.stride, off, cnt,
+                                                          lvl, raw, roff, rbase, index_bits, vals,
+                                                          tgts, lvls, s.bitmaps, universe);
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
 // Entries per CTA log region for a total log capacity.
 static int64_t log_region_capacity(int64_t log_cap) {
   const int64_t r = (log_cap + kWalkGrid - 1) / kWalkGrid;
@@ -1870,38 +1909,14 @@ static int finalize_impl(const ygx::TravScratch& s, int64_t total, int64_t L,
                          const int32_t* near_row_base, void* far_sources, void* far_targets,
                          void* target_levels, void* neighbors, void* neighbor_leaf_positions,
                          int64_t max_nbr, cudaStream_t stream) {
-  const int grid_small = ygx::kNumSMs * ygx::g_tune.row_grid_per_sm;
-  const size_t big_smem = sizeof(int32_t) * ygx::kBlockRowCap;
-  static std::atomic<uint64_t> big_attr{0};
-  if (ygx::ensure_smem_limit(ygx::k_rows_big, (int)big_smem, big_attr) != cudaSuccess)
-    return YGX_ERR_CUDA;
-  const int64_t stride = total > L ? total : L;
-  auto rows_pass = [&](int64_t rows, const int64_t* off, const int32_t* cnt, const int32_t* lvl,
-                       int32_t* raw, const int64_t* roff, const int32_t* rbase, void* vals,
-                       void* tgts, void* lvls) -> int {
-    if (cudaMemsetAsync(s.n_big, 0, 16 * sizeof(uint32_t), stream) != cudaSuccess) return YGX_ERR_CUDA;
-    ygx::k_rows_classify<<<ygx::grid_for(rows, 256), 256, 0, stream>>>(
-        rows, cnt, s.class_rows, stride, s.n_big + 1, s.big_rows, s.n_big);
-    YGX_CHECK_LAUNCH();
-#define YGX_ROWS(C, R)                                                                       \
-  ygx::k_rows_class<R><<<grid_small, 256, 0, stream>>>(s.class_rows + (C) * stride,            \
-                                                       s.n_big + 1 + (C), off, cnt, lvl, raw, \
-                                                       roff, rbase, index_bits, vals, tgts,   \
-                                                       lvls);                                 \
-  YGX_CHECK_LAUNCH();
-    YGX_ROWS(0, 1) YGX_ROWS(1, 2) YGX_ROWS(2, 4) YGX_ROWS(3, 8) YGX_ROWS(4, 16) YGX_ROWS(5, 32)
-#undef YGX_ROWS
-    ygx::k_rows_big<<<ygx::kBigGrid, ygx::kBigThreads, big_smem, stream>>>(
-        s.big_rows, s.n_big, stride, off, cnt, lvl, raw, roff, rbase, index_bits, vals, tgts, lvls,
-        s.bitmaps, total);
-    YGX_CHECK_LAUNCH();
-    return YGX_OK;
-  };
-  int rc2 = rows_pass(total, s.far_off, s.far_cnt, level32, far_src32, far_raw_off,
-                      far_row_base, far_sources, far_targets, target_levels);
+  const ygx::RowSortScratch rs{s.n_big, s.big_rows, s.class_rows, s.bitmaps,
+                               total > L ? total : L};
+  int rc2 = ygx::row_sort_pass(rs, total, s.far_off, s.far_cnt, level32, far_src32, far_raw_off,
+                               far_row_base, index_bits, far_sources, far_targets, target_levels,
+                               total, stream);
   if (rc2) return rc2;
-  rc2 = rows_pass(L, s.near_off, s.near_cnt, nullptr, near_nbr32, near_raw_off, near_row_base,
-                  neighbors, nullptr, nullptr);
+  rc2 = ygx::row_sort_pass(rs, L, s.near_off, s.near_cnt, nullptr, near_nbr32, near_raw_off,
+                           near_row_base, index_bits, neighbors, nullptr, nullptr, total, stream);
   if (rc2) return rc2;
   if (neighbor_leaf_positions && max_nbr > 0) {
     ygx::k_neighbor_leaf_positions<<<ygx::grid_for(L * max_nbr, 256), 256, 0, stream>>>(

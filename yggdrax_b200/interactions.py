@@ -231,7 +231,7 @@ def _grow_wf_cap(cap: int, stats) -> int:
         raise L.YgxError("traversal wavefront exceeds 2^32 pairs")
     return min(_WF_CAP_MAX, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
 _TIMING = os.environ.get("YGGDRAX_B200_TIMING", "0") == "1"  # per-pass CUDA-event times
-TRAVERSAL_MODES = ("log", "two_pass", "learned", "target")
+TRAVERSAL_MODES = ("log", "two_pass", "learned", "target", "target_ordered")
 _TRAVERSAL_MODE = os.environ.get("YGGDRAX_B200_TRAVERSAL_MODE", "log")
 
 
@@ -245,10 +245,12 @@ def set_traversal_mode(mode: str) -> None:
     * ``"learned"``: one walk writing straight into rows sized by the learned
       capacity predictor (``yggdrax_b200.predictor``); rows that outgrow
       their prediction are completed from a log;
-    * ``"target"``: one warp per target node walks that node's pairs in
-      Morton order, so the rows come out in ascending order with no scatter
-      and no row sort (``ygx_target_walk``); trees with tied leaf codes use
-      ``"log"``.
+    * ``"target"``: one warp per target node walks that node's pairs
+      (``ygx_target_walk``): the rows need no scatter, only a sort;
+    * ``"target_ordered"``: the same walk in Morton order, so the rows come
+      out in ascending order with no scatter and no row sort.
+
+    Trees with tied leaf codes run the target modes as ``"log"``.
 
     Environment: ``YGGDRAX_B200_TRAVERSAL_MODE``."""
     global _TRAVERSAL_MODE
@@ -504,28 +506,31 @@ def _target_caps(total: int, nl: int, hint) -> list:
 
 
 def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_extent, leafpos32,
-                 theta, mac_type, mac, dehnen_radius_scale, root, timing, evs):
+                 theta, mac_type, mac, dehnen_radius_scale, root, timing, evs, ordered):
     """ygx_target_walk + ygx_target_walk_lists: returns the output arrays and
     stats, or None when the walk cannot serve this tree (then the caller
-    runs the log schedule)."""
+    runs the log schedule).  ordered: rows ordered by the walk itself, else
+    sorted after it."""
     lib = L.lib()
     dev = topology.parent.device
     st = L.stream_handle(dev)
     ib, idt = INDEX_BITS, INDEX_DTYPE
-    key = _hint_key(mac_type, theta, total, "target")
+    key = _hint_key(mac_type, theta, total, "target_ordered" if ordered else "target")
+    o = 1 if ordered else 0
     caps = _target_caps(total, nl, _TARGET_HINTS.get(key))
     runs = 0
     while True:
         runs += 1
         caps_np = np.asarray(caps, np.int64)
-        ws = L.workspace(lib.ygx_target_walk_workspace_size(total, nl, caps_np.ctypes.data), dev)
+        ws = L.workspace(lib.ygx_target_walk_workspace_size(total, nl, caps_np.ctypes.data, o),
+                         dev)
         stats = np.zeros(L.TSTAT_WORDS, np.uint64)
-        needs = np.zeros(12, np.uint64)
+        needs = np.zeros(14, np.uint64)
         flags = np.zeros(1, np.uint32)
         L.check(lib.ygx_target_walk(
             L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32), L.ptr(d.right32),
             L.ptr(leafpos32), L.ptr(d.parent32), L.ptr(d.level32), L.ptr(d.nbl32), total, ni,
-            root, mac, float(theta), float(dehnen_radius_scale), caps_np.ctypes.data,
+            root, mac, float(theta), float(dehnen_radius_scale), caps_np.ctypes.data, o,
             L.ptr(topology.level_offsets), num_levels, ib, stats.ctypes.data,
             needs.ctypes.data, flags.ctypes.data, L.ptr(ws), ws.numel(), st), "ygx_target_walk")
         f = int(flags[0])
@@ -570,7 +575,7 @@ def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_ext
     if timing:
         evs[2].record()
     L.check(lib.ygx_target_walk_lists(
-        total, ni, caps_np.ctypes.data, L.ptr(d.nbl32), L.ptr(d.level32),
+        total, ni, caps_np.ctypes.data, o, L.ptr(d.nbl32), L.ptr(d.level32),
         L.ptr(topology.level_offsets), num_levels, ib, P, Q, int(needs[4]), int(needs[5]),
         L.ptr(node_offsets), L.ptr(far_counts), L.ptr(level_offsets), L.ptr(sources),
         L.ptr(targets), L.ptr(target_levels), L.ptr(near_offsets), L.ptr(near_counts),
@@ -580,10 +585,12 @@ def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_ext
     if f:
         raise L.YgxError(f"target walk lists reported flags {f:#x}")
     LAST_WALK_STATS.clear()
-    LAST_WALK_STATS.update(s, mode="target", walk_runs=runs,
+    LAST_WALK_STATS.update(s, mode="target_ordered" if ordered else "target", walk_runs=runs,
                            split_list_max_chunks=int(needs[8]),
                            continuation_pieces=int(needs[7]), pieces_run=int(needs[11]),
-                           busy_fraction=int(needs[9]) / max(1, int(needs[9]) + int(needs[10])))
+                           busy_fraction=int(needs[9]) / max(1, int(needs[9]) + int(needs[10])),
+                           steps=int(needs[12]),
+                           lane_fill=int(needs[13]) / max(1, 32 * int(needs[12])))
     if P == 0:
         node_offsets.zero_()
         level_offsets.zero_()
@@ -642,10 +649,11 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     mac = _MAC_CODES[mac_type]
     root = _root_of(topology, d)
     far_raw_off = near_raw_off = None
-    if mode == "target" and not _host_of(topology).malformed and num_levels >= 2:
+    if mode in ("target", "target_ordered") and not _host_of(topology).malformed and \
+            num_levels >= 2:
         out = _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_extent,
                            leafpos32, theta, mac_type, mac, dehnen_radius_scale, root, timing,
-                           evs)
+                           evs, mode == "target_ordered")
         if out is not None:
             (s, node_offsets, far_counts, level_offsets, sources, targets, target_levels,
              near_offsets, near_counts, neighbors, nlp) = out
