@@ -307,7 +307,10 @@ __global__ void k_tw_init_nodes(int32_t total, int32_t root, int32_t* __restrict
 // the walk
 
 // Warp-collective: writes the n staged int32 entries to `pool` and records
-// the chunk (key: row | class | first id); counts the row.
+// the chunk, and counts the row.  The record's key: ordered walks, row |
+// class | first id (the chunks are sorted by it); unordered walks, row |
+// the chunk's offset within the row (taken by the count).
+template <bool kOrd>
 __device__ __forceinline__ void tw_flush_rows(const int32_t* stg, int n, int lane, int t,
                                               unsigned long long key_hi, unsigned cls_bit,
                                               int32_t* pool, unsigned long long cap,
@@ -322,13 +325,14 @@ __device__ __forceinline__ void tw_flush_rows(const int32_t* stg, int n, int lan
   if (ok) {
     for (int k = lane; k < n; k += 32) pool[off + k] = stg[k];
     if (lane == 0) {
-      keys[ri] = key_hi | cls_bit | (unsigned long long)(uint32_t)stg[0];
+      const int within = atomicAdd(cnt_row, n);
+      keys[ri] = key_hi | (kOrd ? (cls_bit | (unsigned long long)(uint32_t)stg[0])
+                                : (unsigned long long)(uint32_t)within);
       TwChunk c;
       c.off = (long long)off;
       c.cnt = n;
       c.t = t;
       recs[ri] = c;
-      atomicAdd(cnt_row, n);
     }
   } else if (lane == 0) {
     raise_flag(a.status, kFlagLogOverflow);
@@ -643,14 +647,14 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
     unsigned c_acc = 0, c_near = 0, c_ref = 0;  // this lane's decisions in this piece
     auto flush_fi = [&]() {
       const unsigned long long hi = (unsigned long long)(uint32_t)a.rank[t] << 32;
-      tw_flush_rows(W.stg_fi, n_fi, lane, t, hi, 0u, a.far_pool, a.far_cap, &a.ctl->far_cur,
+      tw_flush_rows<kOrd>(W.stg_fi, n_fi, lane, t, hi, 0u, a.far_pool, a.far_cap, &a.ctl->far_cur,
                     &al.far, a.far_keys, a.far_recs, a.far_rec_cap, &a.ctl->far_rec_cur,
                     &al.far_r, &a.far_cnt[t], a);
       n_fi = 0;
     };
     auto flush_fl = [&]() {
       const unsigned long long hi = (unsigned long long)(uint32_t)a.rank[t] << 32;
-      tw_flush_rows(W.stg_fl, n_fl, lane, t, hi, 0x80000000u, a.far_pool, a.far_cap,
+      tw_flush_rows<kOrd>(W.stg_fl, n_fl, lane, t, hi, 0x80000000u, a.far_pool, a.far_cap,
                     &a.ctl->far_cur, &al.far, a.far_keys, a.far_recs, a.far_rec_cap,
                     &a.ctl->far_rec_cur, &al.far_r, &a.far_cnt[t], a);
       n_fl = 0;
@@ -658,7 +662,7 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
     auto flush_n = [&]() {
       const int lp = a.recs[t].k.z;  // leaf position (leaf targets only)
       const unsigned long long hi = (unsigned long long)(uint32_t)lp << 32;
-      tw_flush_rows(W.stg_n, n_n, lane, t, hi, 0u, a.near_pool, a.near_cap, &a.ctl->near_cur,
+      tw_flush_rows<kOrd>(W.stg_n, n_n, lane, t, hi, 0u, a.near_pool, a.near_cap, &a.ctl->near_cur,
                     &al.near_, a.near_keys, a.near_recs, a.near_rec_cap, &a.ctl->near_rec_cur,
                     &al.near_r, &a.near_cnt[lp], a);
       n_n = 0;
@@ -1015,19 +1019,32 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Unordered rows: one warp per chunk copies its int32 entries to the row's
-// raw area (the rows are sorted afterwards).
+// Unordered rows: one warp per chunk record (any order) copies the chunk's
+// entries to the row's raw area at base[row] + the chunk's offset within
+// the row (record key: row << 32 | offset); the rows are sorted afterwards.
+// A record that does not fit its row or its pool is reported, not copied.
 __global__ void __launch_bounds__(256)
-    k_tw_copy_raw(const uint32_t* __restrict__ order, const TwChunk* __restrict__ recs, int64_t m,
-                  const int64_t* __restrict__ dest, const int32_t* __restrict__ pool,
-                  int32_t* __restrict__ raw) {
+    k_tw_copy_raw(const unsigned long long* __restrict__ keys, const TwChunk* __restrict__ recs,
+                  int64_t m, const int64_t* __restrict__ base, int64_t rows,
+                  const int32_t* __restrict__ pool, int64_t pool_cap, int32_t* __restrict__ raw,
+                  int64_t raw_cap, uint32_t* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t i = w0; i < m; i += nw) {
-    const TwChunk c = recs[order[i]];
-    const int64_t d = dest[i];
-    for (int k = lane; k < c.cnt; k += 32) raw[d + k] = pool[c.off + k];
+    const TwChunk c = recs[i];
+    if (c.cnt <= 0) continue;
+    const unsigned long long k = keys[i];
+    if ((int64_t)(k >> 32) >= rows || c.off < 0 || c.off + c.cnt > pool_cap) {
+      if (lane == 0) raise_flag(status, kFlagMalformed);
+      continue;
+    }
+    const int64_t d = base[k >> 32] + (int64_t)(k & 0xffffffffull);
+    if (d < 0 || d + c.cnt > raw_cap) {
+      if (lane == 0) raise_flag(status, kFlagMalformed);
+      continue;
+    }
+    for (int e = lane; e < c.cnt; e += 32) raw[d + e] = pool[c.off + e];
   }
 }
 
@@ -1435,50 +1452,58 @@ int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* ca
   k_tw_near_tables<<<grid_for(L + 1, 256), 256, 0, stream>>>(s.near_off, s.near_cnt, (int32_t)L,
                                                             index_bits, near_offsets, near_counts);
   YGX_CHECK_LAUNCH();
-  // rows: sort the chunk records by (row, class, first id), place them by a
-  // scan of their counts, copy
-  SortScratch sw;
-  {
-    Arena sa{(char*)s.sort_ws, 0, s.sort_ws_bytes};
-    sw = carve_sort_scratch(sa, c.far_rec > c.near_rec ? c.far_rec : c.near_rec);
-  }
-  for (int pass = 0; pass < 2; ++pass) {
-    const bool far = pass == 0;
-    const int64_t m = (int64_t)(far ? far_records : near_records);
-    if (m == 0) continue;
-    // key bits: row (rank or leaf position) << 32 | class | id
-    int64_t rows = far ? total : L;
-    int hi_bits = 1;
-    while ((1ll << hi_bits) < rows) ++hi_bits;
-    rc = onesweep_sort(reinterpret_cast<const uint64_t*>(far ? s.far_keys : s.near_keys),
-                       nullptr, m, 0, 32 + hi_bits, reinterpret_cast<uint64_t*>(s.keys_sorted),
-                       s.order, sw, false, s.status, stream);
-    if (rc) return rc;
-    k_tw_sorted_counts<<<grid_for(m, 256), 256, 0, stream>>>(s.order, far ? s.far_recs : s.near_recs,
-                                                            m, s.sorted_cnt);
-    YGX_CHECK_LAUNCH();
-    rc = exclusive_scan<int32_t>(s.sorted_cnt, m, s.dest, s.scan_tmp, stream);
-    if (rc) return rc;
-    if (ordered) {
-      k_tw_copy<<<grid_for(m * 32, 256, kNumSMs * 16), 256, 0, stream>>>(
-          s.order, far ? s.far_recs : s.near_recs, m, s.dest, far ? s.far_pool : s.near_pool,
-          index_bits, far ? sources : neighbors, far ? targets : nullptr,
-          far ? target_levels : nullptr, level32);
-    } else {
-      k_tw_copy_raw<<<grid_for(m * 32, 256, kNumSMs * 16), 256, 0, stream>>>(
-          s.order, far ? s.far_recs : s.near_recs, m, s.dest, far ? s.far_pool : s.near_pool,
-          far ? s.far_raw : s.near_raw);
-    }
-    YGX_CHECK_LAUNCH();
-  }
   if (!ordered) {
-    // every raw row sits at its final offset: sort and widen
+    // chunks straight to their rows (offsets taken by the walk), then every
+    // row sorted
+    if (far_records > 0) {
+      k_tw_copy_raw<<<grid_for((int64_t)far_records * 32, 256, kNumSMs * 16), 256, 0, stream>>>(
+          s.far_keys, s.far_recs, (int64_t)far_records, s.obl, total, s.far_pool, c.far, s.far_raw,
+          far_total, s.status);
+      YGX_CHECK_LAUNCH();
+    }
+    if (near_records > 0) {
+      k_tw_copy_raw<<<grid_for((int64_t)near_records * 32, 256, kNumSMs * 16), 256, 0, stream>>>(
+          s.near_keys, s.near_recs, (int64_t)near_records, s.near_off, L, s.near_pool, c.near_,
+          s.near_raw, near_total, s.status);
+      YGX_CHECK_LAUNCH();
+    }
     rc = row_sort_pass(s.rs, total, s.far_off_node, s.far_cnt, level32, s.far_raw, nullptr,
                        nullptr, index_bits, sources, targets, target_levels, total, stream);
     if (rc) return rc;
     rc = row_sort_pass(s.rs, L, s.near_off, s.near_cnt, nullptr, s.near_raw, nullptr, nullptr,
                        index_bits, neighbors, nullptr, nullptr, total, stream);
     if (rc) return rc;
+  } else {
+    // rows: sort the chunk records by (row, class, first id), place them by
+    // a scan of their counts, copy
+    SortScratch sw;
+    {
+      Arena sa{(char*)s.sort_ws, 0, s.sort_ws_bytes};
+      sw = carve_sort_scratch(sa, c.far_rec > c.near_rec ? c.far_rec : c.near_rec);
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+      const bool far = pass == 0;
+      const int64_t m = (int64_t)(far ? far_records : near_records);
+      if (m == 0) continue;
+      // key bits: row (rank or leaf position) << 32 | class | id
+      int64_t rows = far ? total : L;
+      int hi_bits = 1;
+      while ((1ll << hi_bits) < rows) ++hi_bits;
+      rc = onesweep_sort(reinterpret_cast<const uint64_t*>(far ? s.far_keys : s.near_keys),
+                         nullptr, m, 0, 32 + hi_bits, reinterpret_cast<uint64_t*>(s.keys_sorted),
+                         s.order, sw, false, s.status, stream);
+      if (rc) return rc;
+      k_tw_sorted_counts<<<grid_for(m, 256), 256, 0, stream>>>(
+          s.order, far ? s.far_recs : s.near_recs, m, s.sorted_cnt);
+      YGX_CHECK_LAUNCH();
+      rc = exclusive_scan<int32_t>(s.sorted_cnt, m, s.dest, s.scan_tmp, stream);
+      if (rc) return rc;
+      k_tw_copy<<<grid_for(m * 32, 256, kNumSMs * 16), 256, 0, stream>>>(
+          s.order, far ? s.far_recs : s.near_recs, m, s.dest, far ? s.far_pool : s.near_pool,
+          index_bits, far ? sources : neighbors, far ? targets : nullptr,
+          far ? target_levels : nullptr, level32);
+      YGX_CHECK_LAUNCH();
+    }
   }
   if (max_nbr > 0 && neighbor_leaf_positions && leafpos32 && L > 0) {
     k_tw_nbr_leaf_pos<<<grid_for(L * max_nbr, 256), 256, 0, stream>>>(

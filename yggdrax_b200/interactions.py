@@ -589,7 +589,8 @@ def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_ext
                            split_list_max_chunks=int(needs[8]),
                            continuation_pieces=int(needs[7]), pieces_run=int(needs[11]),
                            busy_fraction=int(needs[9]) / max(1, int(needs[9]) + int(needs[10])),
-                           steps=int(needs[12]),
+                           steps=int(needs[12]), far_records=int(needs[4]),
+                           near_records=int(needs[5]),
                            lane_fill=int(needs[13]) / max(1, 32 * int(needs[12])))
     if P == 0:
         node_offsets.zero_()
