@@ -332,21 +332,27 @@ def test_wavefront_overflow_retries_with_larger_capacity(cuda_device):
     P, M = _to_dev(pos, cuda_device), _to_dev(mass, cuda_device)
     gt, ps = yb.build_tree(P, M, leaf_size=8, return_reordered=True)[:2]
     gg = yb.compute_tree_geometry(gt, ps)
-    a = _run_walk(gt, gg, 0.6, "dehnen", 1.0)
-    peak = LAST_WALK_STATS["max_wf"]
-    assert peak > 2_000_000
-    b = _run_walk(gt, gg, 0.6, "dehnen", 1.0, wf_capacity=4)
-    assert LAST_WALK_STATS["wf_capacity"] > 4
-    assert LAST_WALK_STATS["max_wf"] == peak
+    prev = yb.get_traversal_mode()
+    yb.set_traversal_mode("log")  # the generation walk's wavefront ladder
+    try:
+        a = _run_walk(gt, gg, 0.6, "dehnen", 1.0)
+        peak = LAST_WALK_STATS["max_wf"]
+        assert peak > 2_000_000
+        b = _run_walk(gt, gg, 0.6, "dehnen", 1.0, wf_capacity=4)
+        assert LAST_WALK_STATS["wf_capacity"] > 4
+        assert LAST_WALK_STATS["max_wf"] == peak
+    finally:
+        yb.set_traversal_mode(prev)
     for f in ("far_counts", "node_offsets", "level_offsets", "sources", "targets",
               "near_counts", "near_offsets", "neighbors"):
         np.testing.assert_array_equal(_np(getattr(a, f)), _np(getattr(b, f)), err_msg=f)
 
 
-@pytest.mark.parametrize("mode", ["two_pass", "log"])
+@pytest.mark.parametrize("mode", ["two_pass", "log", "target", "target_ordered"])
 def test_traversal_modes_give_identical_lists(cuda_device, oracle, mode):
-    """The plain two-pass schedule (count walk, then a fill walk) and the
-    one-walk pair log return the same lists as the oracle."""
+    """The plain two-pass schedule (count walk, then a fill walk), the
+    one-walk pair log and the per-target walks return the same lists as the
+    oracle."""
     import yggdrax_b200 as yb
     from yggdrax_b200 import inputs
 
@@ -354,11 +360,12 @@ def test_traversal_modes_give_identical_lists(cuda_device, oracle, mode):
     P, M = _to_dev(pos, cuda_device), _to_dev(mass, cuda_device)
     gt, ps = yb.build_tree(P, M, leaf_size=16, return_reordered=True)[:2]
     gg = yb.compute_tree_geometry(gt, ps)
+    prev = yb.get_traversal_mode()
     yb.set_traversal_mode(mode)
     try:
         gi, gn = yb.build_interactions_and_neighbors(gt, gg, theta=0.5, mac_type="bh")
     finally:
-        yb.set_traversal_mode("log")
+        yb.set_traversal_mode(prev)
     ot = oracle.build_tree(pos, mass, leaf_size=16)
     og = oracle.compute_tree_geometry(ot, ot.positions_sorted)
     r = oracle.build_interactions_and_neighbors(ot, og, theta=0.5, mac_type="bh")

@@ -113,12 +113,13 @@ def _learned_lists(cuda_device, oracle, params=None, cal=None, n=120_000, seed=3
     g = yb.compute_tree_geometry(t, ps)
     if params is not None:
         predictor.set_predictor(params, cal)
+    prev = yb.get_traversal_mode()
     yb.set_traversal_mode("learned")
     try:
         gi, gn = yb.build_interactions_and_neighbors(t, g, theta=0.6, mac_type="dehnen")
         stats = dict(LAST_WALK_STATS)
     finally:
-        yb.set_traversal_mode("log")
+        yb.set_traversal_mode(prev)
         predictor.set_predictor(None)
     ot = oracle.build_tree(pos, mass, leaf_size=16)
     og = oracle.compute_tree_geometry(ot, ot.positions_sorted)

@@ -50,13 +50,14 @@ def _run(yb, gt, gg, theta, mac, budget=None, mode="target"):
     L.check(lib.ygx_tune_get(L.TUNE["target_budget"], old.ctypes.data), "ygx_tune_get")
     if budget is not None:
         L.check(lib.ygx_tune_set(L.TUNE["target_budget"], budget), "ygx_tune_set")
+    prev = yb.get_traversal_mode()
     yb.set_traversal_mode(mode)
     try:
         gi, gn, res = yb.build_interactions_and_neighbors(gt, gg, theta=theta, mac_type=mac,
                                                           return_result=True)
         stats = dict(LAST_WALK_STATS)
     finally:
-        yb.set_traversal_mode("log")
+        yb.set_traversal_mode(prev)
         L.check(lib.ygx_tune_set(L.TUNE["target_budget"], int(old[0])), "ygx_tune_set")
     return gi, gn, res, stats
 
@@ -141,8 +142,8 @@ def test_target_walk_4m_plummer_matches_log_walk(cuda_device, mode):
     yb.set_reference_limits(False)
     try:
         a, an, ares, _ = _run(yb, gt, gg, 0.6, "dehnen", mode=mode)
-        b, bn, bres = yb.build_interactions_and_neighbors(gt, gg, theta=0.6, mac_type="dehnen",
-                                                          return_result=True)
+        b, bn, bres, st = _run(yb, gt, gg, 0.6, "dehnen", mode="log")
+        assert st["mode"] == "log"
     finally:
         yb.set_reference_limits(True)
     for f in ("offsets", "counts", "sources", "targets", "level_offsets", "target_levels"):

@@ -22,6 +22,7 @@ from .interactions import (
     build_compact_far_pairs_and_leaf_neighbor_lists,
     build_interactions_and_neighbors,
     build_leaf_neighbor_lists,
+    get_traversal_mode,
     set_default_dual_tree_config,
     set_dense_neighbor_budget,
     set_reference_limits,

@@ -232,21 +232,21 @@ def _grow_wf_cap(cap: int, stats) -> int:
     return min(_WF_CAP_MAX, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
 _TIMING = os.environ.get("YGGDRAX_B200_TIMING", "0") == "1"  # per-pass CUDA-event times
 TRAVERSAL_MODES = ("log", "two_pass", "learned", "target", "target_ordered")
-_TRAVERSAL_MODE = os.environ.get("YGGDRAX_B200_TRAVERSAL_MODE", "log")
+_TRAVERSAL_MODE = os.environ.get("YGGDRAX_B200_TRAVERSAL_MODE", "target")
 
 
 def set_traversal_mode(mode: str) -> None:
     """How the exact lists are produced (all modes return identical lists):
 
-    * ``"log"`` (default): one walk that counts row entries and logs every
-      accepted / near pair once, then a scatter of the log into the rows;
+    * ``"log"``: one walk that counts row entries and logs every accepted /
+      near pair once, then a scatter of the log into the rows;
     * ``"two_pass"``: the reference's plain count-then-fill schedule, two
       walks (counts, then entries written at row cursors);
     * ``"learned"``: one walk writing straight into rows sized by the learned
       capacity predictor (``yggdrax_b200.predictor``); rows that outgrow
       their prediction are completed from a log;
-    * ``"target"``: one warp per target node walks that node's pairs
-      (``ygx_target_walk``): the rows need no scatter, only a sort;
+    * ``"target"`` (default): one warp per target node walks that node's
+      pairs (``ygx_target_walk``): the rows need no scatter, only a sort;
     * ``"target_ordered"``: the same walk in Morton order, so the rows come
       out in ascending order with no scatter and no row sort.
 
@@ -257,6 +257,11 @@ def set_traversal_mode(mode: str) -> None:
     if mode not in TRAVERSAL_MODES:
         raise ValueError(f"traversal mode must be one of {TRAVERSAL_MODES}, got {mode!r}")
     _TRAVERSAL_MODE = mode
+
+
+def get_traversal_mode() -> str:
+    """The schedule ``set_traversal_mode`` selected last."""
+    return _TRAVERSAL_MODE
 
 
 def set_dense_neighbor_budget(nbytes: Optional[int]) -> None:
