@@ -852,31 +852,50 @@ __device__ __forceinline__ void warp_sort_row(const int32_t* __restrict__ raw, i
   int32_t v[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) v[r] = sm[lane * S + r];
+  // All-ascending network: every comparator puts the minimum at the lower
+  // index, so no per-comparator direction is needed.  The first step of a
+  // k-block pairs i with i ^ (k - 1): inside a lane register r with r ^
+  // (k - 1) while k <= R, else lane l ^ (k / R - 1), register R - 1 - r.
 #pragma unroll
   for (int k = 2; k <= 32 * R; k <<= 1) {
+    if (k <= R) {
 #pragma unroll
-    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int r = 0; r < R; ++r) {
+        const int rp = r ^ (k - 1);
+        if (rp > r) {
+          const int32_t x = v[r], y = v[rp];
+          v[r] = min(x, y);
+          v[rp] = max(x, y);
+        }
+      }
+    } else {
+      const int m = (k >> LOGR) - 1;
+      const bool lower = (lane & ((k >> LOGR) >> 1)) == 0;
+      int32_t y[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) y[r] = __shfl_xor_sync(0xffffffffu, v[R - 1 - r], m);
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = lower ? min(v[r], y[r]) : max(v[r], y[r]);
+    }
+#pragma unroll
+    for (int j = k >> 2; j > 0; j >>= 1) {
       if (j < R) {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           if ((r & j) == 0) {
-            const int pr = r | j;
-            const bool up = (((lane << LOGR) + r) & k) == 0;
-            const int32_t x = v[r], y = v[pr];
-            const int32_t mn = x < y ? x : y, mx = x < y ? y : x;
-            v[r] = up ? mn : mx;
-            v[pr] = up ? mx : mn;
+            const int rp = r | j;
+            const int32_t x = v[r], y = v[rp];
+            v[r] = min(x, y);
+            v[rp] = max(x, y);
           }
         }
       } else {
         const int lj = j >> LOGR;
         const bool lower = (lane & lj) == 0;
-        const bool up = ((lane << LOGR) & k) == 0;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int32_t y = __shfl_xor_sync(0xffffffffu, v[r], lj);
-          const int32_t mn = v[r] < y ? v[r] : y, mx = v[r] < y ? y : v[r];
-          v[r] = (lower == up) ? mn : mx;
+          v[r] = lower ? min(v[r], y) : max(v[r], y);
         }
       }
     }
