@@ -339,7 +339,7 @@ def main():
                     help="skip timing the batched workload (4096 uneven point sets)")
     ap.add_argument("--roofline-only", action="store_true",
                     help="time only the sort roofline leg (for profiling it)")
-    ap.add_argument("--mode", default="target",
+    ap.add_argument("--mode", default="learned",
                     choices=["log", "two_pass", "learned", "target", "target_ordered"],
                     help="traversal schedule of the main timing (all give the same lists)")
     args = ap.parse_args()
@@ -563,7 +563,7 @@ def main():
     return 0
 
 
-def mode_timings(step, pos_d, mass_d, n, steps, barrier, main_mode: str = "target") -> dict:
+def mode_timings(step, pos_d, mass_d, n, steps, barrier, main_mode: str = "learned") -> dict:
     """Device time of the step with every traversal schedule other than the
     main one: the pair log (one walk, scatter, row sort), the plain two-pass
     traversal (count walk + fill walk, the reference's schedule), the learned

@@ -347,6 +347,15 @@ int ygx_traverse_finalize(int64_t total, int64_t num_internal, int64_t wf_capaci
  * and ygx_target_walk_lists sorts the rows.  The same `ordered` must be
  * passed to all three calls of one walk.  Well-formed single
  * trees only (nodes 0..num_internal-1 internal, root `root`).
+ * Predicted rows (unordered only; all six pointers, or none): far_rcap32
+ * (per node) / near_rcap32 (per leaf position) are row capacities
+ * (ygx_predict_caps), pad_far / pad_near their slots (ygx_target_pad), and
+ * far_raw / near_raw int32 arrays of at least the padded totals plus the
+ * extension the walk reports (YGX_TSTAT_EXT_FAR / _EXT_NEAR: the entries of
+ * the rows that outgrew their capacity).  The walk writes every chunk that
+ * fits its row's capacity in place; only the rest pass through the pools.
+ * With predicted rows stats_out also carries YGX_TSTAT_OVF_ROWS /
+ * _OVF_ENTRIES. 
  * caps (host, 8 int64): entry capacities of the far pool, near pool, split
  * lists, spill area; record capacities of far chunks, near chunks,
  * split-list chunks; continuation queue.  needs_out (host, 14 uint64): what
@@ -366,15 +375,24 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
                     const int32_t* parent32, const int32_t* level32, const int32_t* nbl32,
                     int64_t total, int64_t num_internal, int root, int mac, float theta,
                     float dehnen_radius_scale, const int64_t* caps, int ordered,
-                    const void* tree_level_offsets, int num_levels, int index_bits,
-                    uint64_t* stats_out, uint64_t* needs_out, uint32_t* flags_out, void* ws,
-                    size_t ws_bytes, cudaStream_t stream);
+                    const int32_t* far_rcap32, const int32_t* near_rcap32,
+                    const int64_t* pad_far, const int64_t* pad_near, int32_t* far_raw,
+                    int32_t* near_raw, const void* tree_level_offsets, int num_levels,
+                    int index_bits, uint64_t* stats_out, uint64_t* needs_out,
+                    uint32_t* flags_out, void* ws, size_t ws_bytes, cudaStream_t stream);
 /* After ygx_target_walk on the same workspace and capacities: the offset /
  * count tables and the rows (level-major far sources / targets /
  * target_levels, leaf-ordered near neighbours) in the index dtype, and
  * with max_nbr > 0 the dense neighbour_leaf_positions table (L x max_nbr).
- * far_records / near_records: needs_out[4] / needs_out[5] of the walk. */
+ * far_records / near_records: needs_out[4] / needs_out[5] of the walk.
+ * Unordered walks assemble and sort the rows in far_raw / near_raw (int32,
+ * capacities far_raw_cap / near_raw_cap: at least far_total / near_total, or
+ * with predicted rows the same arrays, capacities and pointers the walk had);
+ * ordered walks take NULL / 0 for all of these. */
 int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* caps, int ordered,
+                          const int32_t* far_rcap32, const int32_t* near_rcap32,
+                          const int64_t* pad_far, const int64_t* pad_near, int32_t* far_raw,
+                          int64_t far_raw_cap, int32_t* near_raw, int64_t near_raw_cap,
                           const int32_t* nbl32, const int32_t* level32,
                           const void* tree_level_offsets, int num_levels, int index_bits,
                           int64_t far_total, int64_t near_total, uint64_t far_records,
@@ -384,6 +402,14 @@ int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* ca
                           const int32_t* leafpos32, int64_t max_nbr,
                           void* neighbor_leaf_positions, void* ws, size_t ws_bytes,
                           cudaStream_t stream);
+/* Padded row slots for predicted capacities (no reference counterpart: the
+ * reference sizes rows by its count pass): pad_far[0..total] /
+ * pad_near[0..num_leaves] = exclusive sums of far_rcap32 / near_rcap32 (int64,
+ * device); sums_out (host, 2) = the padded totals.  Synchronizes the stream. */
+size_t ygx_target_pad_workspace_size(int64_t total, int64_t num_leaves);
+int ygx_target_pad(int64_t total, int64_t num_leaves, const int32_t* far_rcap32,
+                   const int32_t* near_rcap32, int64_t* pad_far, int64_t* pad_near,
+                   uint64_t* sums_out, void* ws, size_t ws_bytes, cudaStream_t stream);
 /* ---- row re-layouts ---------------------------------------------------------
  * Device forms of the jnp gathers / cumsum / nonzero the reference uses to
  * re-lay its lists.  Index arrays are in the index dtype (index_bits). */

@@ -114,9 +114,12 @@ _SIGS = {
     "ygx_gather_index": (I32, [P, I64, P, I64, I32, P, P, SZ, P]),
     "ygx_scatter_positions": (I32, [P, I32, I64, I64, P, I32, P, SZ, P]),
     "ygx_target_walk_workspace_size": (SZ, [I64, I64, P, I32]),
-    "ygx_target_walk": (I32, [P, P, P, P, P, P, P, P, P, I64, I64, I32, I32, F32, F32, P, I32, P,
-                              I32, I32, P, P, P, P, SZ, P]),
-    "ygx_target_walk_lists": (I32, [I64, I64, P, I32, P, P, P, I32, I32, I64, I64, ctypes.c_uint64,
+    "ygx_target_walk": (I32, [P, P, P, P, P, P, P, P, P, I64, I64, I32, I32, F32, F32, P, I32,
+                              P, P, P, P, P, P, P, I32, I32, P, P, P, P, SZ, P]),
+    "ygx_target_pad_workspace_size": (SZ, [I64, I64]),
+    "ygx_target_pad": (I32, [I64, I64, P, P, P, P, P, P, SZ, P]),
+    "ygx_target_walk_lists": (I32, [I64, I64, P, I32, P, P, P, P, P, I64, P, I64, P, P, P, I32, I32,
+                                    I64, I64, ctypes.c_uint64,
                                     ctypes.c_uint64, P, P, P, P, P, P, P, P, P, P, I64, P, P,
                                     SZ, P]),
     "ygx_traverse_finalize": (I32, [I64, I64, I64, I64, P, P, I32, P, P, P, P, P, P, P, P, P, P,

@@ -195,6 +195,16 @@ struct TwArgs {
   int budget;
   unsigned long long blk_entries;  // pool block (entries) per claim
   unsigned int blk_records;        // record block per claim
+  // unordered walks with predicted row capacities: a chunk that fits its
+  // row's capacity is written in place at pad[row] + its offset in the row
+  const int32_t* far_rcap;   // per node (nullptr: no prediction)
+  const int32_t* near_rcap;  // per leaf position
+  const int64_t* pad_far;    // padded row starts, per node / leaf position
+  const int64_t* pad_near;
+  int32_t* far_raw;
+  int32_t* near_raw;
+  unsigned* first_ovf_far;   // smallest in-row offset that went to the pool
+  unsigned* first_ovf_near;
 };
 
 // Takes n slots from the warp's block *b (in shared memory, touched by lane
@@ -309,7 +319,11 @@ __global__ void k_tw_init_nodes(int32_t total, int32_t root, int32_t* __restrict
 // Warp-collective: writes the n staged int32 entries to `pool` and records
 // the chunk, and counts the row.  The record's key: ordered walks, row |
 // class | first id (the chunks are sorted by it); unordered walks, row |
-// the chunk's offset within the row (taken by the count).
+// the chunk's offset within the row (taken by the count).  With a predicted
+// row (raw != nullptr) the offset is taken first and a chunk that ends within
+// the row's capacity rcap is written in place at raw[pad + offset] instead
+// (no record); the others go to the pool, and first_ovf keeps the smallest
+// offset that did.
 template <bool kOrd>
 __device__ __forceinline__ void tw_flush_rows(const int32_t* stg, int n, int lane, int t,
                                               unsigned long long key_hi, unsigned cls_bit,
@@ -317,9 +331,37 @@ __device__ __forceinline__ void tw_flush_rows(const int32_t* stg, int n, int lan
                                               unsigned long long* pool_cur, TwBlk* pb,
                                               unsigned long long* keys, TwChunk* recs,
                                               unsigned rec_cap, unsigned* rec_cur, TwBlk* rb,
-                                              int32_t* cnt_row, const TwArgs& a) {
+                                              int32_t* cnt_row, int32_t* raw, int rcap,
+                                              int64_t pad, unsigned* first_ovf,
+                                              const TwArgs& a) {
   if (n == 0) return;
   unsigned long long off = 0, ri = 0;
+  if (!kOrd && raw) {
+    int within = 0;
+    if (lane == 0) within = atomicAdd(cnt_row, n);
+    within = __shfl_sync(0xffffffffu, within, 0);
+    if ((long long)within + n <= (long long)rcap) {
+      for (int k = lane; k < n; k += 32) raw[pad + within + k] = stg[k];
+      return;
+    }
+    const bool fits = tw_take(pb, (unsigned long long)n, a.blk_entries, pool_cur, cap, lane, &off) &&
+                      tw_take(rb, 1ull, a.blk_records, rec_cur, rec_cap, lane, &ri);
+    if (fits) {
+      for (int k = lane; k < n; k += 32) pool[off + k] = stg[k];
+      if (lane == 0) {
+        keys[ri] = key_hi | (unsigned long long)(uint32_t)within;
+        TwChunk c;
+        c.off = (long long)off;
+        c.cnt = n;
+        c.t = t;
+        recs[ri] = c;
+        atomicMin(first_ovf, (unsigned)within);
+      }
+    } else if (lane == 0) {
+      raise_flag(a.status, kFlagLogOverflow);
+    }
+    return;
+  }
   const bool ok = tw_take(pb, (unsigned long long)n, a.blk_entries, pool_cur, cap, lane, &off) &&
                   tw_take(rb, 1ull, a.blk_records, rec_cur, rec_cap, lane, &ri);
   if (ok) {
@@ -645,26 +687,34 @@ __global__ void __launch_bounds__(kTwThreads, kTwBlocksPerSM) k_tw_walk(TwArgs a
     int cur = 0, stk_n = 0, steps = 0, lanes = 0;
     int n_fi = 0, n_fl = 0, n_n = 0, n_s = 0;
     unsigned c_acc = 0, c_near = 0, c_ref = 0;  // this lane's decisions in this piece
+    // far rows are keyed by level-major rank (ordered: the chunk sort
+    // places them) or by node id (unordered: offset tables per node)
     auto flush_fi = [&]() {
-      const unsigned long long hi = (unsigned long long)(uint32_t)a.rank[t] << 32;
+      const unsigned long long hi = (unsigned long long)(uint32_t)(kOrd ? a.rank[t] : t) << 32;
+      const bool in_place = !kOrd && a.far_rcap != nullptr;
       tw_flush_rows<kOrd>(W.stg_fi, n_fi, lane, t, hi, 0u, a.far_pool, a.far_cap, &a.ctl->far_cur,
                     &al.far, a.far_keys, a.far_recs, a.far_rec_cap, &a.ctl->far_rec_cur,
-                    &al.far_r, &a.far_cnt[t], a);
+                    &al.far_r, &a.far_cnt[t], in_place ? a.far_raw : nullptr,
+                    in_place ? a.far_rcap[t] : 0, in_place ? a.pad_far[t] : 0,
+                    in_place ? &a.first_ovf_far[t] : nullptr, a);
       n_fi = 0;
     };
     auto flush_fl = [&]() {
       const unsigned long long hi = (unsigned long long)(uint32_t)a.rank[t] << 32;
       tw_flush_rows<kOrd>(W.stg_fl, n_fl, lane, t, hi, 0x80000000u, a.far_pool, a.far_cap,
                     &a.ctl->far_cur, &al.far, a.far_keys, a.far_recs, a.far_rec_cap,
-                    &a.ctl->far_rec_cur, &al.far_r, &a.far_cnt[t], a);
+                    &a.ctl->far_rec_cur, &al.far_r, &a.far_cnt[t], nullptr, 0, 0, nullptr, a);
       n_fl = 0;
     };
     auto flush_n = [&]() {
       const int lp = a.recs[t].k.z;  // leaf position (leaf targets only)
       const unsigned long long hi = (unsigned long long)(uint32_t)lp << 32;
+      const bool in_place = !kOrd && a.near_rcap != nullptr;
       tw_flush_rows<kOrd>(W.stg_n, n_n, lane, t, hi, 0u, a.near_pool, a.near_cap, &a.ctl->near_cur,
                     &al.near_, a.near_keys, a.near_recs, a.near_rec_cap, &a.ctl->near_rec_cur,
-                    &al.near_r, &a.near_cnt[lp], a);
+                    &al.near_r, &a.near_cnt[lp], in_place ? a.near_raw : nullptr,
+                    in_place ? a.near_rcap[lp] : 0, in_place ? a.pad_near[lp] : 0,
+                    in_place ? &a.first_ovf_near[lp] : nullptr, a);
       n_n = 0;
     };
     auto flush_s = [&]() {
@@ -1048,6 +1098,112 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Predicted rows: per list, the rows that outgrew their capacity, the
+// entries past the capacities and the entries those rows hold (their
+// extension).  out: ovf rows, ovf entries, far extension, near extension.
+__global__ void k_tw_ext_stats(const int32_t* __restrict__ far_cnt,
+                               const int32_t* __restrict__ far_rcap, int32_t total,
+                               const int32_t* __restrict__ near_cnt,
+                               const int32_t* __restrict__ near_rcap, int32_t L,
+                               unsigned long long* __restrict__ out) {
+  unsigned long long rows = 0, past = 0, ef = 0, en = 0;
+  for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    const int32_t c = far_cnt[k], r = far_rcap[k];
+    if (c > r) {
+      ++rows;
+      past += (unsigned long long)(c - r);
+      ef += (unsigned long long)c;
+    }
+    if (k < L) {
+      const int32_t cn = near_cnt[k], rn = near_rcap[k];
+      if (cn > rn) {
+        ++rows;
+        past += (unsigned long long)(cn - rn);
+        en += (unsigned long long)cn;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    rows += __shfl_xor_sync(0xffffffffu, rows, o);
+    past += __shfl_xor_sync(0xffffffffu, past, o);
+    ef += __shfl_xor_sync(0xffffffffu, ef, o);
+    en += __shfl_xor_sync(0xffffffffu, en, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (rows) atomicAdd(&out[0], rows);
+    if (past) atomicAdd(&out[1], past);
+    if (ef) atomicAdd(&out[2], ef);
+    if (en) atomicAdd(&out[3], en);
+  }
+}
+
+// Extension length of every row: its count if it outgrew the capacity.
+__global__ void k_tw_ext_len(const int32_t* __restrict__ cnt, const int32_t* __restrict__ rcap,
+                             int32_t rows, int32_t* __restrict__ ext_len) {
+  for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < rows; k += gridDim.x * blockDim.x)
+    ext_len[k] = cnt[k] > rcap[k] ? cnt[k] : 0;
+}
+
+// Where every row's raw entries sit: its padded slot, or for a row that
+// outgrew it, its extension behind all padded slots.
+__global__ void k_tw_roff(const int32_t* __restrict__ cnt, const int32_t* __restrict__ rcap,
+                          const int64_t* __restrict__ pad, const int64_t* __restrict__ ext_off,
+                          int32_t rows, int64_t* __restrict__ roff) {
+  const int64_t pad_total = pad[rows];
+  for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < rows; k += gridDim.x * blockDim.x)
+    roff[k] = cnt[k] > rcap[k] ? pad_total + ext_off[k] : pad[k];
+}
+
+// A row that outgrew its slot: the entries written in place (offsets below
+// the first one that went to the pool) move to the front of its extension.
+// The extensions lie back to back behind all slots (ext_off: exclusive sums
+// of the rows' extension lengths, rows + 1 entries), so the copy runs over
+// blocks of 1024 extension positions, one warp per block, each finding its
+// rows by binary search: a halo row of 10^5 entries is spread over many
+// warps instead of one.
+__device__ __forceinline__ int32_t tw_row_of(const int64_t* __restrict__ ext_off, int32_t rows,
+                                             int64_t x) {
+  // last r with ext_off[r] <= x (its extension then holds x)
+  int32_t lo = 0, hi = rows;  // ext_off[0] = 0 <= x < ext_off[rows]
+  while (hi - lo > 1) {
+    const int32_t mid = (lo + hi) >> 1;
+    if (ext_off[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+__global__ void k_tw_prefix_copy(const int32_t* __restrict__ cnt, const int64_t* __restrict__ pad,
+                                 const unsigned* __restrict__ first_ovf,
+                                 const int64_t* __restrict__ ext_off, int32_t rows,
+                                 int32_t* __restrict__ raw, int64_t raw_cap,
+                                 uint32_t* __restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t ext_total = ext_off[rows], pad_total = pad[rows];
+  if (pad_total + ext_total > raw_cap) {  // reported, nothing copied
+    if (w0 == 0 && lane == 0) raise_flag(status, kFlagMalformed);
+    return;
+  }
+  for (int64_t x0 = w0 * 1024; x0 < ext_total; x0 += nw * 1024) {
+    const int64_t x1 = x0 + 1024 < ext_total ? x0 + 1024 : ext_total;
+    int64_t x = x0;
+    while (x < x1) {
+      const int32_t r = tw_row_of(ext_off, rows, x);
+      const int64_t rb = ext_off[r], re = ext_off[r + 1];
+      const int64_t seg_end = re < x1 ? re : x1;
+      const unsigned fo = first_ovf[r];
+      const int64_t P = fo < (unsigned)cnt[r] ? (int64_t)fo : (int64_t)cnt[r];
+      const int64_t src = pad[r];
+      for (int64_t xx = x + lane; xx < seg_end; xx += 32) {
+        const int64_t k = xx - rb;
+        if (k < P) raw[pad_total + xx] = raw[src + k];
+      }
+      x = seg_end > x ? seg_end : x1;  // a zero-length row cannot hold x
+    }
+  }
+}
+
 // counts in nodes_by_level order; far offsets; index-dtype tables
 __global__ void k_tw_gather(const int32_t* __restrict__ cnt, const int32_t* __restrict__ nbl,
                             int32_t m, int32_t* __restrict__ out) {
@@ -1147,10 +1303,14 @@ struct TwScratch {
   int64_t* near_off;
   void* sort_ws;
   size_t sort_ws_bytes;
-  // unordered walks: rows assembled raw, then sorted
-  int32_t* far_raw;
-  int32_t* near_raw;
+  // unordered walks: rows assembled raw (caller's arrays), then sorted
   int64_t* far_off_node;
+  unsigned* first_ovf_far;  // predicted rows
+  unsigned* first_ovf_near;
+  int32_t* ext_len;
+  int64_t* ext_off;
+  int64_t* roff_far;
+  int64_t* roff_near;
   RowSortScratch rs;
 };
 
@@ -1198,13 +1358,20 @@ static TwScratch carve_tw(Arena& a, int64_t total, int64_t L, const TwCaps& c, b
   s.near_off = a.take<int64_t>((L > 0 ? L : 1) + 1);
   s.sort_ws_bytes = onesweep_scratch_bytes(mrec) + 256;
   s.sort_ws = a.take<unsigned char>(s.sort_ws_bytes);
-  s.far_raw = s.near_raw = nullptr;
   s.far_off_node = nullptr;
+  s.first_ovf_far = s.first_ovf_near = nullptr;
+  s.ext_len = nullptr;
+  s.ext_off = s.roff_far = s.roff_near = nullptr;
   s.rs = RowSortScratch{nullptr, nullptr, nullptr, nullptr, 0};
   if (!ordered) {
-    s.far_raw = a.take<int32_t>(c.far);
-    s.near_raw = a.take<int32_t>(c.near_);
+    const int64_t mx = (total > L ? total : L) + 1;
     s.far_off_node = a.take<int64_t>(total + 1);
+    s.first_ovf_far = a.take<unsigned>(total);
+    s.first_ovf_near = a.take<unsigned>(L > 0 ? L : 1);
+    s.ext_len = a.take<int32_t>(mx);
+    s.ext_off = a.take<int64_t>(mx);
+    s.roff_far = a.take<int64_t>(total);
+    s.roff_near = a.take<int64_t>(L > 0 ? L : 1);
     s.rs = carve_row_sort(a, total, L);
   }
   return s;
@@ -1235,8 +1402,10 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
                     const int32_t* parent32, const int32_t* level32, const int32_t* nbl32,
                     int64_t total, int64_t num_internal, int root, int mac, float theta,
                     float dehnen_radius_scale, const int64_t* caps, int ordered,
-                    const void* tree_level_offsets, int num_levels, int index_bits,
-                    uint64_t* stats_out, uint64_t* needs_out,
+                    const int32_t* far_rcap32, const int32_t* near_rcap32,
+                    const int64_t* pad_far, const int64_t* pad_near, int32_t* far_raw,
+                    int32_t* near_raw, const void* tree_level_offsets, int num_levels,
+                    int index_bits, uint64_t* stats_out, uint64_t* needs_out,
                     uint32_t* flags_out, void* ws, size_t ws_bytes, cudaStream_t stream) {
   using namespace ygx;
   if (total < 3 || total > INT32_MAX || num_internal < 1 || mac < 0 || mac > 2 || !caps ||
@@ -1247,6 +1416,10 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
   if (!center || !radius || !max_extent || !left32 || !right32 || !leafpos32 || !parent32 ||
       !level32 || !nbl32 || !ws)
     return YGX_ERR_ARG;
+  const bool pred = far_rcap32 != nullptr;
+  if (pred && (ordered || !near_rcap32 || !pad_far || !pad_near || !far_raw || !near_raw))
+    return YGX_ERR_ARG;
+  if (!pred && (near_rcap32 || pad_far || pad_near || far_raw || near_raw)) return YGX_ERR_ARG;
   TwCaps c{caps[0], caps[1], caps[2], caps[3], caps[4], caps[5], caps[6], caps[7]};
   if (!caps_ok(c)) return YGX_ERR_ARG;
   if (ws_bytes < ygx_target_walk_workspace_size(total, total - num_internal, caps, ordered))
@@ -1257,6 +1430,11 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
   const size_t zero_bytes = (size_t)((char*)(s.near_cnt + (L > 0 ? L : 1)) - (char*)s.status);
   if (cudaMemsetAsync(s.status, 0, zero_bytes, stream) != cudaSuccess ||
       cudaMemsetAsync(s.q_ready, 0, sizeof(unsigned int) * c.queue, stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  if (pred && (cudaMemsetAsync(s.first_ovf_far, 0xff, sizeof(unsigned) * total, stream) !=
+                   cudaSuccess ||
+               cudaMemsetAsync(s.first_ovf_near, 0xff, sizeof(unsigned) * (L > 0 ? L : 1),
+                               stream) != cudaSuccess))
     return YGX_ERR_CUDA;
   const int32_t T = (int32_t)total, NI = (int32_t)num_internal;
   k_tw_first_leaf<<<grid_for(L, 256), 256, 0, stream>>>(parent32, left32, NI, T, s.first);
@@ -1314,6 +1492,14 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
   a.status = s.status;
   a.spin_limit = (uint32_t)g_tune.spin_limit;
   a.budget = g_tune.target_budget;
+  a.far_rcap = pred ? far_rcap32 : nullptr;
+  a.near_rcap = pred ? near_rcap32 : nullptr;
+  a.pad_far = pad_far;
+  a.pad_near = pad_near;
+  a.far_raw = far_raw;
+  a.near_raw = near_raw;
+  a.first_ovf_far = pred ? s.first_ovf_far : nullptr;
+  a.first_ovf_near = pred ? s.first_ovf_near : nullptr;
   {
     // allocation blocks: small enough that every warp's open blocks fit the
     // pools many times over, large enough to keep the global cursors quiet
@@ -1353,9 +1539,14 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
   k_tw_row_stats<<<grid_for(total, 256, kNumSMs * 4), 256, 0, stream>>>(s.far_cnt, T, s.near_cnt,
                                                                        (int32_t)L, s.rowstat);
   YGX_CHECK_LAUNCH();
+  if (pred) {
+    k_tw_ext_stats<<<grid_for(total, 256, kNumSMs * 4), 256, 0, stream>>>(
+        s.far_cnt, far_rcap32, T, s.near_cnt, near_rcap32, (int32_t)L, s.rowstat + 4);
+    YGX_CHECK_LAUNCH();
+  }
   TwCtl ctl;
   unsigned int hist[kTwHist];
-  unsigned long long rs[4];
+  unsigned long long rs[8];
   int64_t lvl_off[kTwHist / 2 + 1];
   int32_t lvl_off32[kTwHist / 2 + 1];
   const bool i64 = index_bits == 64;
@@ -1394,6 +1585,12 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
   stats_out[YGX_TSTAT_REFINE] = ctl.ref_sides / 2 + (unsigned long long)total;
   stats_out[YGX_TSTAT_MAX_WF] = mw;
   stats_out[YGX_TSTAT_GENS] = gens;
+  if (pred) {
+    stats_out[YGX_TSTAT_OVF_ROWS] = rs[4];
+    stats_out[YGX_TSTAT_OVF_ENTRIES] = rs[5];
+    stats_out[YGX_TSTAT_EXT_FAR] = rs[6];
+    stats_out[YGX_TSTAT_EXT_NEAR] = rs[7];
+  }
   // what each capacity needed (a re-run with these fits)
   needs_out[0] = ctl.far_cur;
   needs_out[1] = ctl.near_cur;
@@ -1416,6 +1613,9 @@ int ygx_target_walk(const float* center, const float* radius, const float* max_e
 // the level-major far lists and the leaf-order near lists in the index dtype,
 // with the reference's offset / count tables.
 int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* caps, int ordered,
+                          const int32_t* far_rcap32, const int32_t* near_rcap32,
+                          const int64_t* pad_far, const int64_t* pad_near, int32_t* far_raw,
+                          int64_t far_raw_cap, int32_t* near_raw, int64_t near_raw_cap,
                           const int32_t* nbl32, const int32_t* level32,
                           const void* tree_level_offsets, int num_levels, int index_bits,
                           int64_t far_total, int64_t near_total, uint64_t far_records,
@@ -1433,7 +1633,12 @@ int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* ca
   if (ws_bytes < ygx_target_walk_workspace_size(total, total - num_internal, caps, ordered))
     return YGX_ERR_ARG;
   if ((int64_t)far_records > c.far_rec || (int64_t)near_records > c.near_rec) return YGX_ERR_ARG;
-  if (!ordered && (far_total > c.far || near_total > c.near_)) return YGX_ERR_ARG;
+  const bool pred = far_rcap32 != nullptr;
+  if (ordered && (pred || far_raw || near_raw)) return YGX_ERR_ARG;
+  if (!ordered && (!far_raw || !near_raw)) return YGX_ERR_ARG;
+  if (pred && (!near_rcap32 || !pad_far || !pad_near)) return YGX_ERR_ARG;
+  if (!ordered && !pred && (far_total > far_raw_cap || near_total > near_raw_cap))
+    return YGX_ERR_ARG;
   const int64_t L = total - num_internal;
   Arena ar{(char*)ws, 0, ws_bytes};
   TwScratch s = carve_tw(ar, total, L, c, ordered != 0);
@@ -1454,24 +1659,54 @@ int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* ca
   YGX_CHECK_LAUNCH();
   if (!ordered) {
     // chunks straight to their rows (offsets taken by the walk), then every
-    // row sorted
+    // row sorted.  Rows sit at their output offsets, or with predicted
+    // capacities in their padded slots (in place since the walk) or, when
+    // they outgrew them, in an extension behind all slots.
+    const int32_t LL = (int32_t)L;
+    const int64_t* far_base = s.far_off_node;
+    const int64_t* near_base = s.near_off;
+    if (pred) {
+      for (int pass = 0; pass < 2; ++pass) {
+        const bool far = pass == 0;
+        const int32_t rows = far ? T : LL;
+        const int32_t* cnt = far ? s.far_cnt : s.near_cnt;
+        const int32_t* rcap = far ? far_rcap32 : near_rcap32;
+        const int64_t* pad = far ? pad_far : pad_near;
+        int64_t* roff = far ? s.roff_far : s.roff_near;
+        if (rows == 0) continue;
+        k_tw_ext_len<<<grid_for(rows, 256), 256, 0, stream>>>(cnt, rcap, rows, s.ext_len);
+        YGX_CHECK_LAUNCH();
+        rc = exclusive_scan<int32_t>(s.ext_len, rows, s.ext_off, s.scan_tmp, stream);
+        if (rc) return rc;
+        k_tw_roff<<<grid_for(rows, 256), 256, 0, stream>>>(cnt, rcap, pad, s.ext_off, rows, roff);
+        YGX_CHECK_LAUNCH();
+        k_tw_prefix_copy<<<kNumSMs * 8, 256, 0, stream>>>(
+            cnt, pad, far ? s.first_ovf_far : s.first_ovf_near, s.ext_off, rows,
+            far ? far_raw : near_raw, far ? far_raw_cap : near_raw_cap, s.status);
+        YGX_CHECK_LAUNCH();
+      }
+      far_base = s.roff_far;
+      near_base = s.roff_near;
+    }
     if (far_records > 0) {
       k_tw_copy_raw<<<grid_for((int64_t)far_records * 32, 256, kNumSMs * 16), 256, 0, stream>>>(
-          s.far_keys, s.far_recs, (int64_t)far_records, s.obl, total, s.far_pool, c.far, s.far_raw,
-          far_total, s.status);
+          s.far_keys, s.far_recs, (int64_t)far_records, far_base, total, s.far_pool, c.far,
+          far_raw, far_raw_cap, s.status);
       YGX_CHECK_LAUNCH();
     }
     if (near_records > 0) {
       k_tw_copy_raw<<<grid_for((int64_t)near_records * 32, 256, kNumSMs * 16), 256, 0, stream>>>(
-          s.near_keys, s.near_recs, (int64_t)near_records, s.near_off, L, s.near_pool, c.near_,
-          s.near_raw, near_total, s.status);
+          s.near_keys, s.near_recs, (int64_t)near_records, near_base, L, s.near_pool, c.near_,
+          near_raw, near_raw_cap, s.status);
       YGX_CHECK_LAUNCH();
     }
-    rc = row_sort_pass(s.rs, total, s.far_off_node, s.far_cnt, level32, s.far_raw, nullptr,
-                       nullptr, index_bits, sources, targets, target_levels, total, stream);
+    rc = row_sort_pass(s.rs, total, s.far_off_node, s.far_cnt, level32, far_raw,
+                       pred ? s.roff_far : nullptr, nullptr, index_bits, sources, targets,
+                       target_levels, total, stream);
     if (rc) return rc;
-    rc = row_sort_pass(s.rs, L, s.near_off, s.near_cnt, nullptr, s.near_raw, nullptr, nullptr,
-                       index_bits, neighbors, nullptr, nullptr, total, stream);
+    rc = row_sort_pass(s.rs, L, s.near_off, s.near_cnt, nullptr, near_raw,
+                       pred ? s.roff_near : nullptr, nullptr, index_bits, neighbors, nullptr,
+                       nullptr, total, stream);
     if (rc) return rc;
   } else {
     // rows: sort the chunk records by (row, class, first id), place them by
@@ -1511,6 +1746,40 @@ int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* ca
         neighbor_leaf_positions);
     YGX_CHECK_LAUNCH();
   }
+  return YGX_OK;
+}
+
+// Padded row slots for predicted capacities: pad_far[0..total] and
+// pad_near[0..num_leaves] = exclusive sums of far_rcap32 / near_rcap32;
+// sums_out (host, 2) = the two totals.  Synchronizes the stream.
+size_t ygx_target_pad_workspace_size(int64_t total, int64_t num_leaves) {
+  const int64_t m = total > num_leaves ? total : num_leaves;
+  return sizeof(int64_t) * ygx::scan_scratch_elems(m > 0 ? m : 1) + 256;
+}
+
+int ygx_target_pad(int64_t total, int64_t num_leaves, const int32_t* far_rcap32,
+                   const int32_t* near_rcap32, int64_t* pad_far, int64_t* pad_near,
+                   uint64_t* sums_out, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  using namespace ygx;
+  if (total < 1 || num_leaves < 1 || num_leaves > total || !far_rcap32 || !near_rcap32 ||
+      !pad_far || !pad_near || !sums_out || !ws ||
+      ws_bytes < ygx_target_pad_workspace_size(total, num_leaves))
+    return YGX_ERR_ARG;
+  if (reinterpret_cast<uintptr_t>(ws) % sizeof(int64_t)) return YGX_ERR_ARG;
+  int64_t* tmp = reinterpret_cast<int64_t*>(ws);
+  int rc = exclusive_scan<int32_t>(far_rcap32, total, pad_far, tmp, stream);
+  if (rc) return rc;
+  rc = exclusive_scan<int32_t>(near_rcap32, num_leaves, pad_near, tmp, stream);
+  if (rc) return rc;
+  int64_t sums[2];
+  if (cudaMemcpyAsync(&sums[0], pad_far + total, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                      stream) != cudaSuccess ||
+      cudaMemcpyAsync(&sums[1], pad_near + num_leaves, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                      stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return YGX_ERR_CUDA;
+  sums_out[0] = (uint64_t)sums[0];
+  sums_out[1] = (uint64_t)sums[1];
   return YGX_OK;
 }
 

@@ -232,7 +232,7 @@ def _grow_wf_cap(cap: int, stats) -> int:
     return min(_WF_CAP_MAX, max(cap * 4, 2 * int(stats[L.TSTAT["wf_need"]])))
 _TIMING = os.environ.get("YGGDRAX_B200_TIMING", "0") == "1"  # per-pass CUDA-event times
 TRAVERSAL_MODES = ("log", "two_pass", "learned", "target", "target_ordered")
-_TRAVERSAL_MODE = os.environ.get("YGGDRAX_B200_TRAVERSAL_MODE", "target")
+_TRAVERSAL_MODE = os.environ.get("YGGDRAX_B200_TRAVERSAL_MODE", "learned")
 
 
 def set_traversal_mode(mode: str) -> None:
@@ -242,11 +242,14 @@ def set_traversal_mode(mode: str) -> None:
       near pair once, then a scatter of the log into the rows;
     * ``"two_pass"``: the reference's plain count-then-fill schedule, two
       walks (counts, then entries written at row cursors);
-    * ``"learned"``: one walk writing straight into rows sized by the learned
-      capacity predictor (``yggdrax_b200.predictor``); rows that outgrow
-      their prediction are completed from a log;
-    * ``"target"`` (default): one warp per target node walks that node's
-      pairs (``ygx_target_walk``): the rows need no scatter, only a sort;
+    * ``"learned"`` (default): the per-target walk below with every row given
+      a slot sized by the learned capacity predictor
+      (``yggdrax_b200.predictor``); the walk writes every chunk that fits in
+      place, rows that outgrow their slot are completed from the rest (trees
+      the per-target walk does not serve use the generation walk writing into
+      predicted rows, completed from a log);
+    * ``"target"``: one warp per target node walks that node's pairs
+      (``ygx_target_walk``): the rows need no scatter, only a sort;
     * ``"target_ordered"``: the same walk in Morton order, so the rows come
       out in ascending order with no scatter and no row sort.
 
@@ -498,6 +501,9 @@ def _learned_walk_fill(topology, d, total, ni, nl, num_levels, center, radius, m
 # far / near / split chunk records, continuation queue).
 _TARGET_HINTS: dict = {}
 _TARGET_FALLBACK_WARNED: set = set()
+# Learned mode on the per-target walk, per (mac, theta, size octave): the far
+# / near extension entries (per tree node) the last walk needed.
+_LEARNED_TARGET_HINTS: dict = {}
 
 
 def _target_caps(total: int, nl: int, hint) -> list:
@@ -511,22 +517,57 @@ def _target_caps(total: int, nl: int, hint) -> list:
 
 
 def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_extent, leafpos32,
-                 theta, mac_type, mac, dehnen_radius_scale, root, timing, evs, ordered):
+                 theta, mac_type, mac, dehnen_radius_scale, root, timing, evs, ordered,
+                 learned=False):
     """ygx_target_walk + ygx_target_walk_lists: returns the output arrays and
     stats, or None when the walk cannot serve this tree (then the caller
     runs the log schedule).  ordered: rows ordered by the walk itself, else
-    sorted after it."""
+    sorted after it.  learned (unordered): rows get the capacity predictor's
+    slots and the walk writes every chunk that fits in place."""
     lib = L.lib()
     dev = topology.parent.device
     st = L.stream_handle(dev)
     ib, idt = INDEX_BITS, INDEX_DTYPE
-    key = _hint_key(mac_type, theta, total, "target_ordered" if ordered else "target")
+    mode_name = "learned" if learned else ("target_ordered" if ordered else "target")
+    key = _hint_key(mac_type, theta, total, mode_name)
     o = 1 if ordered else 0
     caps = _target_caps(total, nl, _TARGET_HINTS.get(key))
+    far_raw = near_raw = None
+    if learned:
+        from .predictor import default_predictor
+
+        params, cal = default_predictor(dev)
+        far_rcap = torch.empty(total, dtype=torch.int32, device=dev)
+        near_rcap = torch.empty(nl, dtype=torch.int32, device=dev)
+        L.check(lib.ygx_predict_caps(
+            L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.level32),
+            L.ptr(d.parent32), L.ptr(leafpos32), total, ni,
+            L.ptr(topology.node_ranges.contiguous()), ib, root, float(theta), mac, L.ptr(params),
+            float(cal["slack_far"]), float(cal["slack_near"]), int(cal["add"]), L.ptr(far_rcap),
+            L.ptr(near_rcap), st), "ygx_predict_caps")
+        pad_far = torch.empty(total + 1, dtype=torch.int64, device=dev)
+        pad_near = torch.empty(nl + 1, dtype=torch.int64, device=dev)
+        pws = L.workspace(lib.ygx_target_pad_workspace_size(total, nl), dev)
+        sums = np.zeros(2, np.uint64)
+        L.check(lib.ygx_target_pad(total, nl, L.ptr(far_rcap), L.ptr(near_rcap), L.ptr(pad_far),
+                                   L.ptr(pad_near), sums.ctypes.data, L.ptr(pws), pws.numel(), st),
+                "ygx_target_pad")
+        del pws
+        pf, pn = int(sums[0]), int(sums[1])
+        h = _LEARNED_TARGET_HINTS.get(key, (0.0, 0.0))
+        ext = [int(1.25 * h[0] * total), int(1.25 * h[1] * total)]
     runs = 0
     while True:
         runs += 1
         caps_np = np.asarray(caps, np.int64)
+        pred = (None,) * 6
+        if learned:
+            fr = pf + max(ext[0], pf // 16 + 4096)
+            nr = pn + max(ext[1], pn // 16 + 4096)
+            far_raw = torch.empty(fr, dtype=torch.int32, device=dev)
+            near_raw = torch.empty(nr, dtype=torch.int32, device=dev)
+            pred = (L.ptr(far_rcap), L.ptr(near_rcap), L.ptr(pad_far), L.ptr(pad_near),
+                    L.ptr(far_raw), L.ptr(near_raw))
         ws = L.workspace(lib.ygx_target_walk_workspace_size(total, nl, caps_np.ctypes.data, o),
                          dev)
         stats = np.zeros(L.TSTAT_WORDS, np.uint64)
@@ -535,7 +576,7 @@ def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_ext
         L.check(lib.ygx_target_walk(
             L.ptr(center), L.ptr(radius), L.ptr(max_extent), L.ptr(d.left32), L.ptr(d.right32),
             L.ptr(leafpos32), L.ptr(d.parent32), L.ptr(d.level32), L.ptr(d.nbl32), total, ni,
-            root, mac, float(theta), float(dehnen_radius_scale), caps_np.ctypes.data, o,
+            root, mac, float(theta), float(dehnen_radius_scale), caps_np.ctypes.data, o, *pred,
             L.ptr(topology.level_offsets), num_levels, ib, stats.ctypes.data,
             needs.ctypes.data, flags.ctypes.data, L.ptr(ws), ws.numel(), st), "ygx_target_walk")
         f = int(flags[0])
@@ -554,14 +595,24 @@ def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_ext
             if grown == caps or runs > 12:
                 raise L.YgxError(f"target walk capacities did not converge (flags {f:#x})")
             caps = grown
-            del ws
+            ws = far_raw = near_raw = None
             continue
         if f:
             raise L.YgxError(f"target walk reported flags {f:#x}")
+        if learned:
+            ef = int(stats[L.TSTAT["ext_far"]])
+            en = int(stats[L.TSTAT["ext_near"]])
+            if pf + ef > far_raw.numel() or pn + en > near_raw.numel():
+                ext = [ef, en]  # the row counts are deterministic: the re-run fits
+                ws = far_raw = near_raw = None
+                continue
         break
     prev = _TARGET_HINTS.get(key)
     cur = [int(n) / total for n in needs[:8]]
     _TARGET_HINTS[key] = cur if prev is None else [max(a, b) for a, b in zip(prev, cur)]
+    if learned:
+        _LEARNED_TARGET_HINTS[key] = (int(stats[L.TSTAT["ext_far"]]) / total,
+                                      int(stats[L.TSTAT["ext_near"]]) / total)
     if timing:
         evs[1].record()
     s = {k: int(stats[v]) for k, v in L.TSTAT.items()}
@@ -579,8 +630,13 @@ def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_ext
     nlp = torch.empty((nl, max_nbr), dtype=idt, device=dev)
     if timing:
         evs[2].record()
+    if not ordered and not learned:
+        far_raw = torch.empty(max(P, 1), dtype=torch.int32, device=dev)
+        near_raw = torch.empty(max(Q, 1), dtype=torch.int32, device=dev)
+    raw = (None, 0, None, 0) if ordered else (L.ptr(far_raw), far_raw.numel(), L.ptr(near_raw),
+                                              near_raw.numel())
     L.check(lib.ygx_target_walk_lists(
-        total, ni, caps_np.ctypes.data, o, L.ptr(d.nbl32), L.ptr(d.level32),
+        total, ni, caps_np.ctypes.data, o, *pred[:4], *raw, L.ptr(d.nbl32), L.ptr(d.level32),
         L.ptr(topology.level_offsets), num_levels, ib, P, Q, int(needs[4]), int(needs[5]),
         L.ptr(node_offsets), L.ptr(far_counts), L.ptr(level_offsets), L.ptr(sources),
         L.ptr(targets), L.ptr(target_levels), L.ptr(near_offsets), L.ptr(near_counts),
@@ -589,8 +645,14 @@ def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_ext
     f = L.read_status(ws)
     if f:
         raise L.YgxError(f"target walk lists reported flags {f:#x}")
+    far_raw = near_raw = None
     LAST_WALK_STATS.clear()
-    LAST_WALK_STATS.update(s, mode="target_ordered" if ordered else "target", walk_runs=runs,
+    if learned:
+        entries = max(1, P + Q)
+        LAST_WALK_STATS.update(padded_far=pf, padded_near=pn, over_allocation=(pf + pn) / entries,
+                               overflow_row_fraction=s["ovf_rows"] / max(1, total + nl),
+                               overflow_entry_fraction=s["ovf_entries"] / entries)
+    LAST_WALK_STATS.update(s, mode=mode_name, walk_runs=runs,
                            split_list_max_chunks=int(needs[8]),
                            continuation_pieces=int(needs[7]), pieces_run=int(needs[11]),
                            busy_fraction=int(needs[9]) / max(1, int(needs[9]) + int(needs[10])),
@@ -655,11 +717,11 @@ def _run_walk(topology, geometry, theta: float, mac_type: str, dehnen_radius_sca
     mac = _MAC_CODES[mac_type]
     root = _root_of(topology, d)
     far_raw_off = near_raw_off = None
-    if mode in ("target", "target_ordered") and not _host_of(topology).malformed and \
-            num_levels >= 2:
+    if mode in ("target", "target_ordered", "learned") and not _host_of(topology).malformed and \
+            num_levels >= 2 and not wf_capacity:
         out = _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_extent,
                            leafpos32, theta, mac_type, mac, dehnen_radius_scale, root, timing,
-                           evs, mode == "target_ordered")
+                           evs, mode == "target_ordered", learned=mode == "learned")
         if out is not None:
             (s, node_offsets, far_counts, level_offsets, sources, targets, target_levels,
              near_offsets, near_counts, neighbors, nlp) = out
