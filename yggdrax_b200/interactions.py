@@ -666,11 +666,23 @@ def _target_walk(topology, d, total, ni, nl, num_levels, center, radius, max_ext
         near_offsets, near_counts, neighbors, nlp
 
 
+_DEVICE_BYTES: dict = {}
+
+
 def _dense_table_width(max_near: int, nl: int, ib: int, dev) -> int:
     """Width of the dense neighbour_leaf_positions table, or 0 when it would
-    not fit the budget (warned once per table shape)."""
+    not fit the budget (warned once per table shape).  The free-memory query
+    behind the default budget can take milliseconds, so it is skipped when
+    the table exceeds a quarter of the whole device (then it exceeds a
+    quarter of the free memory too)."""
     dense_bytes = nl * max_near * (4 if ib == 32 else 8)
-    if dense_bytes > _dense_neighbor_budget(dev):
+    too_big = False
+    if _DENSE_BUDGET is None:
+        key = (dev.type, dev.index)
+        if key not in _DEVICE_BYTES:
+            _DEVICE_BYTES[key] = torch.cuda.get_device_properties(dev).total_memory
+        too_big = dense_bytes > _DEVICE_BYTES[key] // 4
+    if too_big or dense_bytes > _dense_neighbor_budget(dev):
         if (nl, max_near) not in _DENSE_WARNED:  # once per table shape
             _DENSE_WARNED.add((nl, max_near))
             logger.warning(

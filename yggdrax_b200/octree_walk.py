@@ -33,7 +33,7 @@ from . import _lib as L
 from .dtypes import INDEX_BITS, INDEX_DTYPE
 from .interactions import (_DEFAULT_MAX_INTERACTIONS, _DEFAULT_MAX_NEIGHBORS, _MAC_CODES,
                            DEFAULT_PAIR_QUEUE_MULTIPLIER, DualTreeRetryEvent,
-                           DualTreeTraversalConfig, _dense_neighbor_budget, _target_blocks)
+                           DualTreeTraversalConfig, _target_blocks)
 from . import interactions as _inter
 
 _OCT_REQUIRED = ("oct_valid_mask", "oct_parent", "oct_children", "oct_child_counts",
@@ -398,15 +398,7 @@ def build_octree_native_neighbor_lists(
             "ygx_scatter_positions")
     # dense (rows, longest row) table of neighbour row positions, -1 padded
     max_nbr = int(counts.max().item()) if rows else 0
-    dense_bytes = rows * max_nbr * (4 if INDEX_BITS == 32 else 8)
-    if dense_bytes > _dense_neighbor_budget(dev):
-        if (rows, max_nbr) not in _inter._DENSE_WARNED:  # once per table shape
-            _inter._DENSE_WARNED.add((rows, max_nbr))
-            _inter.logger.warning(
-                "neighbor_leaf_positions would need %.1f GiB (%d leaves x %d neighbours); "
-                "returning an empty (L, 0) table -- raise the budget with "
-                "set_dense_neighbor_budget() to build it", dense_bytes / 2**30, rows, max_nbr)
-        max_nbr = 0
+    max_nbr = _inter._dense_table_width(max_nbr, rows, INDEX_BITS, dev)
     pos = torch.full((rows, max_nbr), -1, dtype=idt, device=dev)
     if max_nbr and neighbors.numel():
         # row of every neighbour cell (rank_of_cell from the carrier compaction)
