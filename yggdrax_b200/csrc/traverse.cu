@@ -1065,11 +1065,24 @@ __global__ void __launch_bounds__(kBigThreads, 3)
     const int32_t vbase = row_base ? row_base[r] : 0;   // ids written relative to it
     const int64_t n = row_cnt[r];
     const int32_t lvl = row_level ? row_level[r] : 0;
+    // eight loads in flight per thread: a long row is otherwise a chain of
+    // dependent global round trips
+    constexpr int kU = 8;
     int32_t vmin = INT32_MAX, vmax = INT32_MIN;
-    for (int64_t k = tid; k < n; k += nt) {
-      const int32_t v = raw[roff + k];
-      vmin = v < vmin ? v : vmin;
-      vmax = v > vmax ? v : vmax;
+    for (int64_t k = tid; k < n; k += (int64_t)nt * kU) {
+      int32_t v[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int64_t kk = k + (int64_t)u * nt;
+        v[u] = kk < n ? raw[roff + kk] : INT32_MAX;
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (k + (int64_t)u * nt < n) {
+          vmin = v[u] < vmin ? v[u] : vmin;
+          vmax = v[u] > vmax ? v[u] : vmax;
+        }
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -1093,11 +1106,22 @@ __global__ void __launch_bounds__(kBigThreads, 3)
     if (swords <= kSumWords) {
       uint32_t* bm = words <= kBlockRowCap ? s_dyn : gbm;
       bool dup = false;
-      for (int64_t k = tid; k < n; k += nt) {
-        const uint32_t v = (uint32_t)(raw[roff + k] - vmin);
-        const uint32_t bit = 1u << (v & 31);
-        if (atomicOr(&bm[v >> 5], bit) & bit) dup = true;
-        atomicOr(&s_sum[v >> 10], 1u << ((v >> 5) & 31));
+      for (int64_t k = tid; k < n; k += (int64_t)nt * kU) {
+        int32_t w[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          const int64_t kk = k + (int64_t)u * nt;
+          w[u] = kk < n ? raw[roff + kk] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          if (k + (int64_t)u * nt < n) {
+            const uint32_t v = (uint32_t)(w[u] - vmin);
+            const uint32_t bit = 1u << (v & 31);
+            if (atomicOr(&bm[v >> 5], bit) & bit) dup = true;
+            atomicOr(&s_sum[v >> 10], 1u << ((v >> 5) & 31));
+          }
+        }
       }
       if (dup) s_dup = 1;
       __syncthreads();
