@@ -509,7 +509,11 @@ def main():
     # -- the same step with the other traversal schedules (same exact lists) ----
     modes = {args.mode: {"ms_per_step": t_dev * 1e3, "value": n / t_dev}}
     if not args.no_modes:
-        modes.update(mode_timings(step, pos_d, mass_d, n, args.steps, barrier, args.mode))
+        modes.update(mode_timings(step, pos_d, mass_d, n, args.steps, barrier, args.mode,
+                                  pos_h, mass_h))
+        # the main schedule's end-to-end figures (this rank), beside the others'
+        modes[args.mode]["e2e_value"] = n / t_e2e
+        modes[args.mode]["e2e_serial_value"] = n / t_e2e_serial
 
     batched = None
     if not args.no_batched:  # every rank (barriers inside), each on its share of the sets
@@ -563,13 +567,17 @@ def main():
     return 0
 
 
-def mode_timings(step, pos_d, mass_d, n, steps, barrier, main_mode: str = "learned") -> dict:
+def mode_timings(step, pos_d, mass_d, n, steps, barrier, main_mode: str = "learned",
+                 pos_h=None, mass_h=None) -> dict:
     """Device time of the step with every traversal schedule other than the
     main one: the pair log (one walk, scatter, row sort), the plain two-pass
     traversal (count walk + fill walk, the reference's schedule), the learned
     one-pass traversal (rows sized by the capacity predictor) and the
     per-target walks (rows without a scatter, then sorted; or in Morton order
-    straight from the walk), inputs resident; the median over the steps."""
+    straight from the walk), inputs resident; the median over the steps.
+    With the pinned host inputs, also each schedule's end-to-end rate through
+    the public API, serial (copy in, compute, read the counts back, all in the
+    timed region), as ``e2e_serial_value``."""
     import torch
 
     import yggdrax_b200 as yb
@@ -595,6 +603,22 @@ def mode_timings(step, pos_d, mass_d, n, steps, barrier, main_mode: str = "learn
                 per.append(a.elapsed_time(b))
             ms = float(np.median(per))
             rec = {"ms_per_step": ms, "value": n / (ms / 1e3)}
+            if pos_h is not None:
+                dev = pos_d.device
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                barrier()
+                a.record()
+                for _ in range(steps):
+                    P = pos_h.to(dev, non_blocking=True)
+                    M = mass_h.to(dev, non_blocking=True)
+                    _, _, inter, nbrs = step(P, M)
+                    inter.counts.cpu()
+                    nbrs.counts.cpu()
+                    inter = nbrs = None
+                b.record()
+                barrier()
+                rec["e2e_serial_value"] = n / (a.elapsed_time(b) / 1e3 / steps)
             if mode == "learned":
                 rec["predictor"] = {k: LAST_WALK_STATS.get(k) for k in (
                     "over_allocation", "overflow_row_fraction", "overflow_entry_fraction",

@@ -1106,16 +1106,38 @@ __global__ void __launch_bounds__(kBigThreads, 3)
     if (swords <= kSumWords) {
       uint32_t* bm = words <= kBlockRowCap ? s_dyn : gbm;
       bool dup = false;
-      for (int64_t k = tid; k < n; k += (int64_t)nt * kU) {
+      const bool dense = n >= 8 * words;
+      // trip count shared by the lanes of a warp (the loop body votes)
+      for (int64_t k = tid; k - lane < n; k += (int64_t)nt * kU) {
         int32_t w[kU];
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
           const int64_t kk = k + (int64_t)u * nt;
           w[u] = kk < n ? raw[roff + kk] : 0;
         }
+        // Dense rows (at least 8 ids per bitmap word on average, e.g. the
+        // near rows of halo leaves) have their ids in clustered runs, so the
+        // lanes of a warp mostly set bits of the same word: one atomic per
+        // word group (the group's bits ORed first; a repeated id shows as
+        // fewer bits than lanes or as a bit already set), and the summary
+        // is built by ballots afterwards.  Sparse rows set their bits and
+        // summary bits directly.
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
-          if (k + (int64_t)u * nt < n) {
+          const bool valid = k + (int64_t)u * nt < n;
+          if (dense) {
+            const unsigned act = __ballot_sync(0xffffffffu, valid);
+            if (valid) {
+              const uint32_t v = (uint32_t)(w[u] - vmin);
+              const uint32_t bit = 1u << (v & 31);
+              const unsigned peers = __match_any_sync(act, v >> 5);
+              const unsigned comb = __reduce_or_sync(peers, bit);
+              if (lane == __ffs(peers) - 1) {
+                const uint32_t old = atomicOr(&bm[v >> 5], comb);
+                if ((old & comb) != 0u || __popc(comb) != __popc(peers)) dup = true;
+              }
+            }
+          } else if (valid) {
             const uint32_t v = (uint32_t)(w[u] - vmin);
             const uint32_t bit = 1u << (v & 31);
             if (atomicOr(&bm[v >> 5], bit) & bit) dup = true;
@@ -1125,6 +1147,14 @@ __global__ void __launch_bounds__(kBigThreads, 3)
       }
       if (dup) s_dup = 1;
       __syncthreads();
+      if (dense && !s_dup) {
+        for (int64_t w0 = (int64_t)warp * 32; w0 < words; w0 += (int64_t)nwarps * 32) {
+          const int64_t ww = w0 + lane;
+          const unsigned m = __ballot_sync(0xffffffffu, ww < words && bm[ww] != 0u);
+          if (lane == 0) s_sum[w0 >> 5] = m;
+        }
+        __syncthreads();
+      }
       if (s_dup) {
         // undo the bits; the row goes to the bitonic network
         for (int64_t k = tid; k < n; k += nt) {
