@@ -61,7 +61,7 @@ enum {
                                /* before it gives up and flags YGX_FLAG_TIMEOUT          */
                                /* (0..2^24; default 2^22); not a performance knob        */
 #define YGX_TUNE_TARGET_BUDGET 7 /* steps one warp spends on a piece of a target before */
-                                 /* handing the rest to other warps (1..4096; 64)      */
+                                 /* handing the rest to other warps (1..4096; 128)     */
 
 /* traversal statistics words (host array of YGX_TSTAT_WORDS uint64) */
 #define YGX_TSTAT_WORDS 16

@@ -22,7 +22,7 @@ struct Tune {
   int row_grid_per_sm = 16;    // CTAs per SM of the short-row finalize kernels
   int sort_tile = 0;           // onesweep tile shape (index into kSortShape, sort.cuh)
   int spin_limit = 1 << 22;    // iterations of a device-side wait before it gives up
-  int target_budget = 64;      // per-target walk: warp steps per piece before a hand-off
+  int target_budget = 128;     // per-target walk: warp steps per piece before a hand-off
 };
 extern Tune g_tune;
 
