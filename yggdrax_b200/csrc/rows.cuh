@@ -12,20 +12,35 @@ struct RowSortScratch {
   int32_t* big_rows;    // stride entries
   int32_t* class_rows;  // one list of stride rows per size class
   uint32_t* bitmaps;    // one bitmap over [0, universe) per long-row CTA
-  int64_t stride;       // max(rows of any pass)
+  int64_t stride;       // rows of both tables of a pass together
 };
 
-// Carves the scratch for passes of up to max(total, L) rows whose values lie
-// in [0, total).
-RowSortScratch carve_row_sort(Arena& a, int64_t total, int64_t L);
-
-// Sorts rows[0, rows): row r has cnt[r] raw int32 values at raw + (roff ?
+// One list's rows: row r has cnt[r] raw int32 values at raw + (roff ?
 // roff[r] : off[r]) and is written, sorted, at vals + off[r] (values minus
 // rbase[r] when rbase is given); far rows also write the target r - rbase[r]
-// and lvl[r] for every entry into tgts / lvls.  Does not synchronize.
-int row_sort_pass(const RowSortScratch& s, int64_t rows, const int64_t* off, const int32_t* cnt,
-                  const int32_t* lvl, int32_t* raw, const int64_t* roff, const int32_t* rbase,
-                  int index_bits, void* vals, void* tgts, void* lvls, int64_t universe,
-                  cudaStream_t stream);
+// and lvl[r] for every entry into tgts / lvls.
+struct RowTable {
+  int64_t rows;
+  const int64_t* off;
+  const int32_t* cnt;
+  const int32_t* lvl;
+  int32_t* raw;
+  const int64_t* roff;
+  const int32_t* rbase;
+  void* vals;
+  void* tgts;
+  void* lvls;
+};
+
+// Carves the scratch for a pass over a table of `total` rows and one of `L`
+// rows whose values lie in [0, total).
+RowSortScratch carve_row_sort(Arena& a, int64_t total, int64_t L);
+
+// Sorts the rows of both tables in one pass (b.rows may be 0): one size
+// classification, one launch per size class and one long-row launch for
+// both, so the longest rows of either start first and the rest fill in
+// around them.  Does not synchronize.
+int row_sort_pass(const RowSortScratch& s, const RowTable& a, const RowTable& b, int index_bits,
+                  int64_t universe, cudaStream_t stream);
 
 }  // namespace ygx

@@ -1700,13 +1700,12 @@ int ygx_target_walk_lists(int64_t total, int64_t num_internal, const int64_t* ca
           near_raw, near_raw_cap, s.status);
       YGX_CHECK_LAUNCH();
     }
-    rc = row_sort_pass(s.rs, total, s.far_off_node, s.far_cnt, level32, far_raw,
-                       pred ? s.roff_far : nullptr, nullptr, index_bits, sources, targets,
-                       target_levels, total, stream);
-    if (rc) return rc;
-    rc = row_sort_pass(s.rs, L, s.near_off, s.near_cnt, nullptr, near_raw,
-                       pred ? s.roff_near : nullptr, nullptr, index_bits, neighbors, nullptr,
-                       nullptr, total, stream);
+    const RowTable far_rows{total, s.far_off_node, s.far_cnt, level32, far_raw,
+                            pred ? s.roff_far : nullptr, nullptr, sources, targets,
+                            target_levels};
+    const RowTable near_rows{L, s.near_off, s.near_cnt, nullptr, near_raw,
+                             pred ? s.roff_near : nullptr, nullptr, neighbors, nullptr, nullptr};
+    rc = row_sort_pass(s.rs, far_rows, near_rows, index_bits, total, stream);
     if (rc) return rc;
   } else {
     // rows: sort the chunk records by (row, class, first id), place them by

@@ -926,13 +926,15 @@ __device__ __forceinline__ void warp_sort_row(const int32_t* __restrict__ raw, i
 // CTA kernel.
 constexpr int kRowClasses = 6;  // R = 1, 2, 4, 8, 16, 32
 
-__global__ void k_rows_classify(int64_t rows, const int32_t* __restrict__ row_cnt,
-                                int32_t* __restrict__ lists, int64_t list_stride,
-                                uint32_t* __restrict__ list_n, int32_t* __restrict__ big_rows,
-                                uint32_t* __restrict__ n_big) {
+// Rows of two tables in one pass: row r < ta.rows is ta's row r, the others
+// are tb's row r - ta.rows.
+__global__ void k_rows_classify(RowTable ta, RowTable tb, int32_t* __restrict__ lists,
+                                int64_t list_stride, uint32_t* __restrict__ list_n,
+                                int32_t* __restrict__ big_rows, uint32_t* __restrict__ n_big) {
+  const int64_t rows = ta.rows + tb.rows;
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows;
        r += (int64_t)gridDim.x * blockDim.x) {
-    const int n = row_cnt[r];
+    const int n = r < ta.rows ? ta.cnt[r] : tb.cnt[r - ta.rows];
     if (n == 0) continue;
     if (n > kWarpRowCap) {
       // rows longer than kBlockRowCap from the front, the others from the
@@ -959,19 +961,19 @@ __global__ void k_rows_classify(int64_t rows, const int32_t* __restrict__ row_cn
 template <int R>
 __global__ void __launch_bounds__(256, R >= 32 ? 2 : (R >= 16 ? 3 : 4))
     k_rows_class(const int32_t* __restrict__ list, const uint32_t* __restrict__ list_n,
-                 const int64_t* __restrict__ row_off, const int32_t* __restrict__ row_cnt,
-                 const int32_t* __restrict__ row_level, const int32_t* __restrict__ raw,
-                 const int64_t* __restrict__ raw_off, const int32_t* __restrict__ row_base,
-                 int index_bits, void* vals_out, void* tgt_out, void* lvl_out) {
+                 RowTable ta, RowTable tb, int index_bits) {
   __shared__ int32_t s_rows[8][32 * (R + 1)];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t nm = *list_n;
   for (uint32_t b = blockIdx.x * 8 + w; b < nm; b += gridDim.x * 8) {
-    const int32_t r = list[b];
-    const int32_t vbase = row_base ? row_base[r] : 0;
-    warp_sort_row<R>(raw, raw_off ? raw_off[r] : row_off[r], row_off[r], row_cnt[r],
-                     index_bits, vals_out, tgt_out, lvl_out, r - vbase, vbase,
-                     row_level ? row_level[r] : 0, lane, s_rows[w]);
+    const int32_t g = list[b];
+    const bool second = g >= ta.rows;
+    const RowTable& T = second ? tb : ta;
+    const int32_t r = second ? g - (int32_t)ta.rows : g;
+    const int32_t vbase = T.rbase ? T.rbase[r] : 0;
+    warp_sort_row<R>(T.raw, T.roff ? T.roff[r] : T.off[r], T.off[r], T.cnt[r], index_bits,
+                     T.vals, T.tgts, T.lvls, r - vbase, vbase, T.lvl ? T.lvl[r] : 0, lane,
+                     s_rows[w]);
   }
 }
 
@@ -1029,11 +1031,8 @@ __device__ __forceinline__ int64_t block_excl_scan(int64_t v, int64_t* s_tmp, in
 // shared memory up to kBlockRowCap entries, else in place in global memory).
 __global__ void __launch_bounds__(kBigThreads, 3)
     k_rows_big(const int32_t* __restrict__ big_rows, uint32_t* __restrict__ n_big,
-               int64_t list_cap, const int64_t* __restrict__ row_off,
-               const int32_t* __restrict__ row_cnt, const int32_t* __restrict__ row_level,
-               int32_t* __restrict__ raw, const int64_t* __restrict__ raw_off,
-               const int32_t* __restrict__ row_base, int index_bits, void* vals_out,
-               void* tgt_out, void* lvl_out, uint32_t* __restrict__ bitmaps, int64_t universe) {
+               int64_t list_cap, RowTable ta, RowTable tb, int index_bits,
+               uint32_t* __restrict__ bitmaps, int64_t universe) {
   extern __shared__ uint32_t s_dyn[];  // kBlockRowCap words: bitmap, or a row to sort
   __shared__ uint32_t s_sum[kSumWords];
   __shared__ int32_t s_cc[kSumWords];  // per-chunk counts, then bases (< n < 2^31)
@@ -1051,15 +1050,34 @@ __global__ void __launch_bounds__(kBigThreads, 3)
   if (gwords > kBlockRowCap)
     for (int64_t w = tid; w < gwords; w += nt) gbm[w] = 0u;
   __syncthreads();
+  __shared__ RowTable s_tab;  // the current row's table (picked by thread 0)
+  __shared__ int32_t s_row;
   while (true) {
     if (tid == 0) {
-      s_item = atomicAdd(&n_big[9], 1u);
+      const uint32_t bb = atomicAdd(&n_big[9], 1u);
+      s_item = bb;
       s_dup = 0;
+      if (bb < n_long + n_mid) {
+        const int32_t g = bb < n_long ? big_rows[bb] : big_rows[list_cap - 1 - (bb - n_long)];
+        const bool second = g >= ta.rows;
+        s_tab = second ? tb : ta;
+        s_row = second ? g - (int32_t)ta.rows : g;
+      }
     }
     __syncthreads();
     const uint32_t b = s_item;
     if (b >= n_long + n_mid) break;
-    const int32_t r = b < n_long ? big_rows[b] : big_rows[list_cap - 1 - (b - n_long)];
+    const RowTable& T = s_tab;
+    const int32_t r = s_row;
+    const int64_t* __restrict__ row_off = T.off;
+    const int32_t* __restrict__ row_cnt = T.cnt;
+    const int32_t* __restrict__ row_level = T.lvl;
+    int32_t* __restrict__ raw = T.raw;
+    const int64_t* __restrict__ raw_off = T.roff;
+    const int32_t* __restrict__ row_base = T.rbase;
+    void* vals_out = T.vals;
+    void* tgt_out = T.tgts;
+    void* lvl_out = T.lvls;
     const int64_t off = row_off[r];
     const int64_t roff = raw_off ? raw_off[r] : off;  // where the raw row is read
     const int32_t vbase = row_base ? row_base[r] : 0;   // ids written relative to it
@@ -1309,7 +1327,7 @@ struct TravScratch {
   unsigned long long* near_pos;
   int64_t* scan_tmp;
   int32_t* big_rows;
-  int32_t* class_rows;  // kRowClasses lists of max(total, L) rows
+  int32_t* class_rows;  // kRowClasses lists of total + L rows
   uint32_t* bitmaps;
   int2* wf[2];
   uint32_t* region_cnt[2];
@@ -1343,7 +1361,7 @@ constexpr int kBigGrid = kNumSMs * 3;
 
 RowSortScratch carve_row_sort(Arena& a, int64_t total, int64_t L) {
   RowSortScratch s;
-  s.stride = total > L ? total : L;
+  s.stride = total + L;
   s.n_big = a.take<uint32_t>(64);
   s.big_rows = a.take<int32_t>(s.stride);
   s.class_rows = a.take<int32_t>((size_t)kRowClasses * s.stride);
@@ -1351,30 +1369,27 @@ RowSortScratch carve_row_sort(Arena& a, int64_t total, int64_t L) {
   return s;
 }
 
-int row_sort_pass(const RowSortScratch& s, int64_t rows, const int64_t* off, const int32_t* cnt,
-                  const int32_t* lvl, int32_t* raw, const int64_t* roff, const int32_t* rbase,
-                  int index_bits, void* vals, void* tgts, void* lvls, int64_t universe,
-                  cudaStream_t stream) {
+int row_sort_pass(const RowSortScratch& s, const RowTable& a, const RowTable& b, int index_bits,
+                  int64_t universe, cudaStream_t stream) {
   const int grid_small = kNumSMs * g_tune.row_grid_per_sm;
   const size_t big_smem = sizeof(int32_t) * kBlockRowCap;
   static std::atomic<uint64_t> big_attr{0};
   if (ensure_smem_limit(k_rows_big, (int)big_smem, big_attr) != cudaSuccess) return YGX_ERR_CUDA;
-  if (rows > s.stride) return YGX_ERR_ARG;
+  const int64_t rows = a.rows + b.rows;
+  if (a.rows < 0 || b.rows < 0 || rows > s.stride || rows > INT32_MAX) return YGX_ERR_ARG;
   if (cudaMemsetAsync(s.n_big, 0, 16 * sizeof(uint32_t), stream) != cudaSuccess)
     return YGX_ERR_CUDA;
-  k_rows_classify<<<grid_for(rows, 256), 256, 0, stream>>>(rows, cnt, s.class_rows, s.stride,
+  k_rows_classify<<<grid_for(rows, 256), 256, 0, stream>>>(a, b, s.class_rows, s.stride,
                                                            s.n_big + 1, s.big_rows, s.n_big);
   YGX_CHECK_LAUNCH();
 #define YGX_ROWS(C, R)                                                                        \
-  k_rows_class<R><<<grid_small, 256, 0, stream>>>(s.class_rows + (C) * s.stride, s.n_big + 1 + (C), \
-                                                  off, cnt, lvl, raw, roff, rbase, index_bits,  \
-                                                  vals, tgts, lvls);                            \
+  k_rows_class<R><<<grid_small, 256, 0, stream>>>(s.class_rows + (C) * s.stride,             \
+                                                  s.n_big + 1 + (C), a, b, index_bits);       \
   YGX_CHECK_LAUNCH();
   YGX_ROWS(0, 1) YGX_ROWS(1, 2) YGX_ROWS(2, 4) YGX_ROWS(3, 8) YGX_ROWS(4, 16) YGX_ROWS(5, 32)
 #undef YGX_ROWS
-  k_rows_big<<<kBigGrid, kBigThreads, big_smem, stream>>>(s.big_rows, s.n_big, s.stride, off, cnt,
-                                                          lvl, raw, roff, rbase, index_bits, vals,
-                                                          tgts, lvls, s.bitmaps, universe);
+  k_rows_big<<<kBigGrid, kBigThreads, big_smem, stream>>>(s.big_rows, s.n_big, s.stride, a, b,
+                                                          index_bits, s.bitmaps, universe);
   YGX_CHECK_LAUNCH();
   return YGX_OK;
 }
@@ -1403,8 +1418,8 @@ static TravScratch carve_trav(Arena& a, int64_t total, int64_t L, int64_t cap, i
   s.far_pos = a.take<unsigned long long>(total + L);
   s.near_pos = s.far_pos ? s.far_pos + total : nullptr;
   s.scan_tmp = a.take<int64_t>(scan_scratch_elems(total > L ? total : L));
-  s.big_rows = a.take<int32_t>(total > L ? total : L);
-  s.class_rows = a.take<int32_t>((size_t)kRowClasses * (total > L ? total : L));
+  s.big_rows = a.take<int32_t>(total + L);  // far and near rows sort in one pass
+  s.class_rows = a.take<int32_t>((size_t)kRowClasses * (total + L));
   s.bitmaps = a.take<uint32_t>((size_t)kBigGrid * ((total + 31) / 32));
   s.wf[0] = a.take<int2>(region_capacity(cap) * kWalkGrid);
   s.wf[1] = a.take<int2>(region_capacity(cap) * kWalkGrid);
@@ -1899,7 +1914,7 @@ int ygx_traverse_fill_predicted(int64_t total, int64_t num_internal, int64_t wf_
   if ((rc = ygx::exclusive_scan<int32_t>(s.ext_near_cnt, L, s.ext_near_off, s.scan_tmp, stream)))
     return rc;
   // moved-row lists: far rows in big_rows, near rows in class_rows (both
-  // hold max(total, L) entries and are free until the finalize); counters
+  // hold at least max(total, L) entries and are free until the finalize); counters
   // in n_big[10] / n_big[11]
   if (cudaMemsetAsync(s.n_big + 10, 0, 2 * sizeof(uint32_t), stream) != cudaSuccess)
     return YGX_ERR_CUDA;
@@ -1982,14 +1997,12 @@ static int finalize_impl(const ygx::TravScratch& s, int64_t total, int64_t L,
                          const int32_t* near_row_base, void* far_sources, void* far_targets,
                          void* target_levels, void* neighbors, void* neighbor_leaf_positions,
                          int64_t max_nbr, cudaStream_t stream) {
-  const ygx::RowSortScratch rs{s.n_big, s.big_rows, s.class_rows, s.bitmaps,
-                               total > L ? total : L};
-  int rc2 = ygx::row_sort_pass(rs, total, s.far_off, s.far_cnt, level32, far_src32, far_raw_off,
-                               far_row_base, index_bits, far_sources, far_targets, target_levels,
-                               total, stream);
-  if (rc2) return rc2;
-  rc2 = ygx::row_sort_pass(rs, L, s.near_off, s.near_cnt, nullptr, near_nbr32, near_raw_off,
-                           near_row_base, index_bits, neighbors, nullptr, nullptr, total, stream);
+  const ygx::RowSortScratch rs{s.n_big, s.big_rows, s.class_rows, s.bitmaps, total + L};
+  const ygx::RowTable far_rows{total, s.far_off, s.far_cnt, level32, far_src32, far_raw_off,
+                               far_row_base, far_sources, far_targets, target_levels};
+  const ygx::RowTable near_rows{L, s.near_off, s.near_cnt, nullptr, near_nbr32, near_raw_off,
+                                near_row_base, neighbors, nullptr, nullptr};
+  const int rc2 = ygx::row_sort_pass(rs, far_rows, near_rows, index_bits, total, stream);
   if (rc2) return rc2;
   if (neighbor_leaf_positions && max_nbr > 0) {
     ygx::k_neighbor_leaf_positions<<<ygx::grid_for(L * max_nbr, 256), 256, 0, stream>>>(
