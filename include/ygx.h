@@ -152,6 +152,16 @@ int ygx_sort_pairs_noalloc_status(uint32_t* host_flags, cudaStream_t stream);
 int ygx_reorder(const float* positions, const float* masses, const uint32_t* order, int64_t n,
                 int index_bits, float* positions_sorted, float* masses_sorted,
                 void* particle_indices, void* inverse, cudaStream_t stream);
+/* The same reorder in two steps, for random-order inputs: ygx_pack_particles
+ * writes (x, y, z, mass) float4 records (packed: n records, 16-byte aligned,
+ * caller-owned), and ygx_reorder_packed gathers one aligned record per
+ * particle (one memory sector instead of up to three).  Outputs as for
+ * ygx_reorder; any output may be NULL. */
+int ygx_pack_particles(const float* positions, const float* masses, int64_t n, void* packed,
+                       cudaStream_t stream);
+int ygx_reorder_packed(const void* packed, const uint32_t* order, int64_t n, int index_bits,
+                       float* positions_sorted, float* masses_sorted, void* particle_indices,
+                       void* inverse, cudaStream_t stream);
 
 /* ---- L1: leaf partitions -------------------------------------------------- */
 

@@ -88,6 +88,39 @@ def test_radix_build_matches_oracle(cuda_device, oracle, case, leaf_size):
     _compare_tree(gt, ot)
 
 
+def test_packed_reorder_matches_plain_reorder(cuda_device):
+    """ygx_pack_particles + ygx_reorder_packed (the build's path) give the same
+    sorted positions, masses, particle indices and inverse permutation as
+    ygx_reorder, for a random order of an uneven count."""
+    import torch
+
+    from yggdrax_b200 import _lib as L
+
+    lib = L.lib()
+    n = 70_001
+    rng = np.random.default_rng(3)
+    P = _to_dev(rng.standard_normal((n, 3)).astype(np.float32), cuda_device)
+    M = _to_dev(rng.random(n).astype(np.float32), cuda_device)
+    order = torch.randperm(n, device=cuda_device).to(torch.int32)
+    st = L.stream_handle(cuda_device)
+    outs = [[torch.empty((n, 3), dtype=torch.float32, device=cuda_device),
+             torch.empty(n, dtype=torch.float32, device=cuda_device),
+             torch.empty(n, dtype=torch.int64, device=cuda_device),
+             torch.empty(n, dtype=torch.int64, device=cuda_device)] for _ in range(2)]
+    L.check(lib.ygx_reorder(L.ptr(P), L.ptr(M), L.ptr(order), n, 64,
+                            *[L.ptr(o) for o in outs[0]], st), "ygx_reorder")
+    packed = torch.empty((n, 4), dtype=torch.float32, device=cuda_device)
+    L.check(lib.ygx_pack_particles(L.ptr(P), L.ptr(M), n, L.ptr(packed), st),
+            "ygx_pack_particles")
+    L.check(lib.ygx_reorder_packed(L.ptr(packed), L.ptr(order), n, 64,
+                                   *[L.ptr(o) for o in outs[1]], st), "ygx_reorder_packed")
+    for a, b in zip(*outs):
+        assert torch.equal(a, b)
+    # a misaligned record array is refused
+    assert lib.ygx_reorder_packed(L.ptr(packed) + 4, L.ptr(order), n, 64, None, None, None,
+                                  None, st) == 1  # YGX_ERR_ARG
+
+
 @pytest.mark.parametrize("case", ["clumps30k", "plummer40k", "collinear128", "dup64"])
 @pytest.mark.parametrize("refine", [True, False])
 def test_fixed_depth_build_matches_oracle(cuda_device, oracle, case, refine):

@@ -73,6 +73,8 @@ _SIGS = {
     "ygx_sort_pairs_noalloc": (I32, [P, P, I64, I32, I32, P, P, P]),
     "ygx_sort_pairs_noalloc_status": (I32, [P, P]),
     "ygx_reorder": (I32, [P, P, P, I64, I32, P, P, P, P, P]),
+    "ygx_pack_particles": (I32, [P, P, I64, P, P]),
+    "ygx_reorder_packed": (I32, [P, P, I64, I32, P, P, P, P, P]),
     "ygx_leaves_adaptive": (I32, [P, I64, I64, I32, P, P, P, P, P]),
     "ygx_leaves_fixed": (I32, [P, I64, I32, I32, P, P, P, P, P]),
     "ygx_refine_workspace_size": (SZ, [I64]),

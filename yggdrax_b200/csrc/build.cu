@@ -58,6 +58,53 @@ __global__ void __launch_bounds__(kReorderThreads)
   }
 }
 
+// The same reorder from particles packed as (x, y, z, mass) float4 records:
+// one aligned 16-byte gather (a single sector) per particle instead of a
+// 12-byte position that may straddle two sectors plus a 4-byte mass in a
+// third.  k_pack_particles writes the records in one coalesced pass.
+__global__ void k_pack_particles(const float* __restrict__ pos, const float* __restrict__ mass,
+                                 int64_t n, float4* __restrict__ packed) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x)
+    packed[k] = make_float4(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2], mass[k]);
+}
+
+__global__ void __launch_bounds__(kReorderThreads)
+    k_reorder_packed(const float4* __restrict__ packed, const uint32_t* __restrict__ order,
+                     int64_t n, int index_bits, float* __restrict__ pos_sorted,
+                     float* __restrict__ mass_sorted, void* __restrict__ particle_indices,
+                     void* __restrict__ inverse) {
+  constexpr int64_t kChunk = (int64_t)kReorderThreads * kReorderItems;
+  for (int64_t k0 = (int64_t)blockIdx.x * kChunk + threadIdx.x; k0 < n;
+       k0 += (int64_t)gridDim.x * kChunk) {
+    uint32_t v[kReorderItems];
+    float4 p[kReorderItems];
+#pragma unroll
+    for (int u = 0; u < kReorderItems; ++u) {
+      const int64_t k = k0 + (int64_t)u * kReorderThreads;
+      v[u] = k < n ? order[k] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < kReorderItems; ++u) {
+      const int64_t k = k0 + (int64_t)u * kReorderThreads;
+      if (k < n) p[u] = __ldg(packed + v[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < kReorderItems; ++u) {
+      const int64_t k = k0 + (int64_t)u * kReorderThreads;
+      if (k >= n) continue;
+      if (pos_sorted) {
+        pos_sorted[3 * k] = p[u].x;
+        pos_sorted[3 * k + 1] = p[u].y;
+        pos_sorted[3 * k + 2] = p[u].z;
+      }
+      if (mass_sorted) mass_sorted[k] = p[u].w;
+      if (particle_indices) store_idx(particle_indices, index_bits, k, v[u]);
+      if (inverse) store_idx(inverse, index_bits, v[u], k);
+    }
+  }
+}
+
 // _tree_impl.py:405-406: fixed-size chunks of the sorted order.
 __global__ void k_leaves_adaptive(const uint64_t* __restrict__ codes, int64_t n, int64_t leaf_size,
                                   int64_t L, int index_bits, void* starts, void* ends,
@@ -636,6 +683,32 @@ static TopoScratch carve_topo(Arena& a, int64_t L) {
 }  // namespace ygx
 
 extern "C" {
+
+int ygx_pack_particles(const float* positions, const float* masses, int64_t n, void* packed,
+                       cudaStream_t stream) {
+  if (n < 1 || !positions || !masses || !packed ||
+      (reinterpret_cast<uintptr_t>(packed) & 15u) != 0)
+    return YGX_ERR_ARG;
+  ygx::k_pack_particles<<<ygx::grid_for(n, 256), 256, 0, stream>>>(
+      positions, masses, n, reinterpret_cast<float4*>(packed));
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
+
+int ygx_reorder_packed(const void* packed, const uint32_t* order, int64_t n, int index_bits,
+                       float* positions_sorted, float* masses_sorted, void* particle_indices,
+                       void* inverse, cudaStream_t stream) {
+  if (n < 1 || !order || !packed || (reinterpret_cast<uintptr_t>(packed) & 15u) != 0 ||
+      (index_bits != 32 && index_bits != 64))
+    return YGX_ERR_ARG;
+  ygx::k_reorder_packed<<<ygx::grid_for((n + ygx::kReorderItems - 1) / ygx::kReorderItems,
+                                         ygx::kReorderThreads),
+                          ygx::kReorderThreads, 0, stream>>>(
+      reinterpret_cast<const float4*>(packed), order, n, index_bits, positions_sorted,
+      masses_sorted, particle_indices, inverse);
+  YGX_CHECK_LAUNCH();
+  return YGX_OK;
+}
 
 int ygx_reorder(const float* positions, const float* masses, const uint32_t* order, int64_t n,
                 int index_bits, float* positions_sorted, float* masses_sorted,

@@ -326,8 +326,15 @@ def _build(positions, masses, bounds, *, build_mode: str, leaf_size: int = 8,
     mass_sorted = torch.empty(n, dtype=torch.float32, device=dev)
     pidx = torch.empty(n, dtype=idt, device=dev)
     inv = torch.empty(n, dtype=idt, device=dev)
-    L.check(lib.ygx_reorder(L.ptr(pos), L.ptr(mass), L.ptr(order), n, ib, L.ptr(pos_sorted),
-                            L.ptr(mass_sorted), L.ptr(pidx), L.ptr(inv), st), "ygx_reorder")
+    # (x, y, z, mass) records: the Morton-order gather then reads one aligned
+    # 16-byte record per particle
+    packed = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    L.check(lib.ygx_pack_particles(L.ptr(pos), L.ptr(mass), n, L.ptr(packed), st),
+            "ygx_pack_particles")
+    L.check(lib.ygx_reorder_packed(L.ptr(packed), L.ptr(order), n, ib, L.ptr(pos_sorted),
+                                   L.ptr(mass_sorted), L.ptr(pidx), L.ptr(inv), st),
+            "ygx_reorder_packed")
+    del packed
 
     use_morton = build_mode == "fixed_depth"
     tree_leaf_size: Optional[int] = None
