@@ -43,6 +43,21 @@ def test_workspace_size_queries_run_without_gpu():
     assert lib.ygx_traverse_workspace_size(2047, 1024, 1 << 16, 1 << 16) > (1 << 16) * 24
 
 
+def test_packed_reorder_refuses_misaligned_records_before_launch():
+    """The packed gather reads 16-byte records; a record array off that
+    boundary is refused on the host (YGX_ERR_ARG) before any CUDA call, so
+    the check runs here without a GPU on fake, never dereferenced pointers."""
+    from yggdrax_b200 import _lib
+
+    lib = _lib.lib()
+    for addr in (0x10004, 0x10008, 0x1000C):
+        assert lib.ygx_reorder_packed(addr, 0x20000, 100, 64, None, None, None, None,
+                                      None) == 1
+    assert lib.ygx_reorder_packed(0x10000, 0x20000, 100, 48, None, None, None, None,
+                                  None) == 1  # index width
+    assert lib.ygx_reorder_packed(0x10000, None, 100, 64, None, None, None, None, None) == 1
+
+
 def test_product_does_not_import_oracle():
     pkg = os.path.join(ROOT, "yggdrax_b200")
     for dirpath, _, files in os.walk(pkg):
