@@ -48,9 +48,9 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 N_DEFAULT = 16_777_216
-# dram__bytes_read.sum + dram__bytes_write.sum of one k_onesweep launch
-# (ncu, keys = Morton codes of the Plummer input), by key count.
-SORT_PASS_DRAM_BYTES: dict = {16_777_216: 361_430_000}
+# dram__bytes_read.sum + dram__bytes_write.sum of one onesweep launch (ncu,
+# keys = Morton codes of the Plummer input), by (key count, digit bits).
+SORT_PASS_DRAM_BYTES: dict = {(16_777_216, 8): 361_430_000}
 LEAF = 32
 THETA = 0.6
 MAC = "dehnen"
@@ -261,14 +261,18 @@ def run_reference(args):
 
 def sort_roofline(codes, dev, reps: int) -> dict:
     """The build's HBM-bound kernel: the onesweep LSD sort of the Morton codes
-    (key u64 + value u32, 8-bit digits over 63 bits = 8 passes), timed with
-    CUDA events on its own stream, L2 flushed (256 MB write) before every
-    sort.  Algorithmic bytes: read key + value, write key + value (24 B per
-    key) on passes 2-8; the first pass reads no values (its values are the
-    input positions), 20 B per key; per launch the mean, 23.5 B per key."""
+    (key u64 + value u32 over 63 bits) at the digit width the autotuner chose
+    -- 8-bit digits in 8 passes (k_onesweep) or 11-bit digits in 6 passes
+    (k_onesweep_wide) -- timed with CUDA events on its own stream, L2 flushed
+    (256 MB write) before every sort; the other width is timed the same way
+    and reported beside it.  Algorithmic bytes: read key + value, write key +
+    value (24 B per key) on every pass but the first, which reads no values
+    (its values are the input positions), 20 B per key; per launch the mean
+    over the passes (23.5 B per key at 8 passes, 23.33 B at 6)."""
     import torch
 
     from yggdrax_b200 import _lib as L
+    from yggdrax_b200 import autotune
 
     lib = L.lib()
     n = int(codes.numel())
@@ -283,41 +287,47 @@ def sort_roofline(codes, dev, reps: int) -> dict:
         L.check(lib.ygx_sort_pairs(L.ptr(codes), None, n, 0, 63, L.ptr(kout), L.ptr(vout),
                                    L.ptr(wsb), wsb.numel(), st), "ygx_sort_pairs")
 
-    for _ in range(3):
-        sort_once()
-    sort_ms = []
-    for _ in range(reps):
-        flush.zero_()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        sort_once()
-        b.record(stream)
-        torch.cuda.synchronize(dev)
-        sort_ms.append(a.elapsed_time(b))
+    def timed(fn, warm):
+        for _ in range(warm):
+            fn()
+        ms = []
+        for _ in range(reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            ms.append(a.elapsed_time(b))
+        return float(np.median(ms))
+
+    chosen = autotune.current()["sort_bits"]
+    by_bits = {}
+    try:
+        for bits in (8, 11):
+            autotune.apply({"sort_bits": bits})
+            by_bits[bits] = timed(sort_once, 3)
+    finally:
+        autotune.apply({"sort_bits": chosen})
     # Library reference point: CUB's radix sort through torch.sort (stable,
     # int64 keys, int64 indices: 32 B per key per pass) on the same codes.
-    lib_ms = []
     c64 = codes.view(torch.int64)
-    for i in range(reps + 2):
-        flush.zero_()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        torch.sort(c64, stable=True)
-        b.record(stream)
-        torch.cuda.synchronize(dev)
-        if i >= 2:
-            lib_ms.append(a.elapsed_time(b))
-    passes = 8
-    sort_s = float(np.median(sort_ms)) / 1e3
+    lib_ms = timed(lambda: torch.sort(c64, stable=True), 2)
+    passes = 6 if chosen == 11 else 8
+    sort_s = by_bits[chosen] / 1e3
     bytes_per_pass = (20.0 + 24.0 * (passes - 1)) / passes * n
     achieved = bytes_per_pass / (sort_s / passes) / 1e9
     peak, peak_kind = _peaks()
-    return {"kernel": "k_onesweep (8 passes, 8-bit digits, key u64 + value u32)",
+    kernel = ("k_onesweep_wide (6 passes, 11-bit digits, key u64 + value u32)" if chosen == 11
+              else "k_onesweep (8 passes, 8-bit digits, key u64 + value u32)")
+    return {"kernel": kernel, "digit_bits": chosen, "passes": passes,
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_kind": peak_kind,
-            "traffic": SORT_PASS_DRAM_BYTES.get(n), "algorithmic_bytes_per_launch": bytes_per_pass,
+            "traffic": SORT_PASS_DRAM_BYTES.get((n, chosen)),
+            "algorithmic_bytes_per_launch": bytes_per_pass,
             "launch_ms_avg": sort_s / passes * 1e3, "n_keys": n,
-            "sort_ms": sort_s * 1e3, "torch_sort_stable_ms": float(np.median(lib_ms))}
+            "sort_ms": sort_s * 1e3, "sort_ms_by_digit_bits": by_bits,
+            "torch_sort_stable_ms": lib_ms}
 
 
 def main():

@@ -62,6 +62,9 @@ enum {
                                /* (0..2^24; default 2^22); not a performance knob        */
 #define YGX_TUNE_TARGET_BUDGET 7 /* steps one warp spends on a piece of a target before */
                                  /* handing the rest to other warps (1..4096; 128)     */
+#define YGX_TUNE_SORT_BITS 8   /* onesweep digit width: 8, or 11 (2048 bins) for every  */
+                               /* sort whose key range it covers in fewer passes        */
+                               /* (63-bit Morton codes: 6 passes instead of 8)          */
 
 /* traversal statistics words (host array of YGX_TSTAT_WORDS uint64) */
 #define YGX_TSTAT_WORDS 16
@@ -130,7 +133,7 @@ int ygx_sort_pairs(const uint64_t* keys_in, const uint32_t* values_in, int64_t n
 /* Same sort as ygx_sort_pairs, for callers that cannot allocate device
  * memory where they sort (e.g. an XLA custom-call handler without a scratch
  * request, whose framework has preallocated the GPU's memory pool): the
- * scratch lives in a 4 MiB array inside libygx.so that every GPU using the
+ * scratch lives in a 6 MiB array inside libygx.so that every GPU using the
  * library keeps until the process exits.  At most 262,144 keys per call;
  * larger n returns YGX_ERR_TOO_LARGE.  Nothing is allocated.  The first call
  * on a device looks up the array's device address (make it before any

@@ -24,13 +24,15 @@ def test_knob_table_roundtrip(tune_mod):
     from yggdrax_b200 import _lib as L
 
     tune_mod.apply({"walk_blocks": 4, "row_grid": 8, "sort_rank": 2, "sort_skew": 100,
-                    "sort_tile": 3})
+                    "sort_tile": 3, "sort_bits": 11})
     cur = tune_mod.current()
+    assert cur["sort_bits"] == 11
     assert cur["walk_blocks"] == 4 and cur["row_grid"] == 8 and cur["sort_tile"] == 3
     assert cur["sort_rank"] == 2 and cur["sort_skew"] == 100
     for knob, bad in (("walk_blocks", 1), ("walk_blocks", 7), ("refit_warps", 3),
                       ("row_grid", 12), ("sort_rank", 3), ("sort_skew", 0), ("sort_skew", 257),
-                      ("sort_tile", -1), ("sort_tile", 4)):
+                      ("sort_tile", -1), ("sort_tile", 4), ("sort_bits", 9),
+                      ("sort_bits", 16)):
         with pytest.raises(ValueError):
             tune_mod.apply({knob: bad})
         assert tune_mod.current()[knob] == cur[knob]
@@ -40,19 +42,20 @@ def test_knob_table_roundtrip(tune_mod):
 
 
 def test_search_finds_cheapest_setting(tune_mod, monkeypatch):
-    # synthetic cost: best at walk_blocks=4, refit_warps=2, row_grid=32
+    # synthetic cost: best at 11-bit digits, walk_blocks=4, refit_warps=2, row_grid=32
     def cost():
         c = tune_mod.current()
         return (10.0 + abs(c["walk_blocks"] - 4) + (c["refit_warps"] != 2) * 0.5
-                + (32 - c["row_grid"]) * 0.01)
+                + (32 - c["row_grid"]) * 0.01 + (c["sort_bits"] == 8) * 0.3)
 
     monkeypatch.setattr(tune_mod, "time_ms", lambda fn, dev, reps=3, warmup=1: cost())
-    tune_mod.apply({"walk_blocks": 6, "refit_warps": 8, "row_grid": 16})
+    tune_mod.apply({"walk_blocks": 6, "refit_warps": 8, "row_grid": 16, "sort_bits": 8})
     log = []
     best = tune_mod.tune(lambda: None, None, log=log)
     assert (best["walk_blocks"], best["refit_warps"], best["row_grid"]) == (4, 2, 32)
+    assert best["sort_bits"] == 11
     assert tune_mod.current() == best
-    assert len(log) == 1 + 3 + 2 + 3
+    assert len(log) == 1 + 1 + 3 + 2 + 3
 
 
 def test_cache_roundtrip(tune_mod, monkeypatch):

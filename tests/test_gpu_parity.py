@@ -268,22 +268,28 @@ def test_single_leaf_tree(cuda_device, oracle):
     assert int(gn.counts.sum()) == 0
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2, 3])
-def test_sort_pairs_is_stable(cuda_device, tile):
-    """Stable sort under every onesweep tile shape (3072-6144 keys per tile);
-    sizes straddle tile boundaries of each shape."""
+@pytest.mark.parametrize("tile,digit_bits", [(0, 8), (1, 8), (2, 8), (3, 8), (0, 11)])
+def test_sort_pairs_is_stable(cuda_device, tile, digit_bits):
+    """Stable sort under every onesweep tile shape (3072-6144 keys per tile)
+    and with 11-bit digits (4096-key tiles; used for 9-11, 17-22, 25-33,
+    ... bit ranges, where it cuts passes); sizes straddle tile boundaries of
+    each shape."""
     import torch
 
     from yggdrax_b200 import _lib as L
     from yggdrax_b200 import autotune
 
-    rng = np.random.default_rng(3 + tile)
+    rng = np.random.default_rng(3 + tile + digit_bits)
     saved = autotune.current()
-    autotune.apply({"sort_tile": tile})
+    autotune.apply({"sort_tile": tile, "sort_bits": digit_bits})
     try:
         for n, bits in [(1, 8), (3071, 8), (4095, 8), (4097, 16), (5121, 12), (6145, 24),
-                        (100003, 63), (300000, 20)]:
-            keys = rng.integers(0, 1 << min(bits, 62), size=n, dtype=np.uint64)
+                        (100003, 63), (300000, 20), (1, 63), (4095, 11), (4096, 9),
+                        (8193, 63), (12289, 33), (200001, 64)]:
+            keys = rng.integers(0, 1 << 63, size=n, dtype=np.uint64) * np.uint64(2) + \
+                rng.integers(0, 2, size=n, dtype=np.uint64)
+            if bits < 64:
+                keys &= np.uint64((1 << bits) - 1)
             keys[: n // 3] = keys[0]  # many ties
             k = torch.from_numpy(keys).to(cuda_device)
             ko = torch.empty_like(k)

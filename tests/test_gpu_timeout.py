@@ -47,20 +47,22 @@ def test_spin_limit_knob_range(cuda_device):
     assert int(v[0]) == DEFAULT_SPIN_LIMIT
 
 
-def test_lookback_wait_that_runs_out_reports_timeout(cuda_device):
+@pytest.mark.parametrize("digit_bits", [8, 11])
+def test_lookback_wait_that_runs_out_reports_timeout(cuda_device, digit_bits):
     import torch
 
     from yggdrax_b200 import _lib as L
 
     lib = L.lib()
     rng = np.random.default_rng(21)
-    n = 1 << 24  # 4096 tiles per pass, 8 passes
+    n = 1 << 24  # 4096 tiles per pass; 8 passes of 8-bit digits, 6 of 11-bit
     keys_np = rng.integers(0, 1 << 63, size=n, dtype=np.uint64)
     vals_np = np.arange(n, dtype=np.int32)
     keys = torch.from_numpy(keys_np).to(cuda_device)
     vals = torch.from_numpy(vals_np).to(cuda_device)
     ws = L.workspace(lib.ygx_sort_pairs_workspace_size(n), cuda_device)
     flags = []
+    L.check(lib.ygx_tune_set(L.TUNE["sort_bits"], digit_bits), "ygx_tune_set")
     L.check(lib.ygx_tune_set(L.TUNE["spin_limit"], 0), "ygx_tune_set")
     try:
         for _ in range(4):  # the first call practically always meets a wait
@@ -73,7 +75,10 @@ def test_lookback_wait_that_runs_out_reports_timeout(cuda_device):
         L.check(lib.ygx_tune_set(L.TUNE["spin_limit"], DEFAULT_SPIN_LIMIT), "ygx_tune_set")
     assert any(f & L.FLAG_TIMEOUT for f in flags), flags
     # the context is still usable and the default limit sorts correctly
-    rc, f, ko, vo = _sort(lib, L, keys, vals, ws, cuda_device)
+    try:
+        rc, f, ko, vo = _sort(lib, L, keys, vals, ws, cuda_device)
+    finally:
+        L.check(lib.ygx_tune_set(L.TUNE["sort_bits"], 8), "ygx_tune_set")
     assert rc == 0 and f == 0
     order = np.argsort(keys_np, kind="stable")
     np.testing.assert_array_equal(vo.cpu().numpy(), order.astype(np.int32))

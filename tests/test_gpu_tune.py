@@ -12,6 +12,7 @@ SETTINGS = [
     ("sort_rank", 1), ("sort_rank", 2), ("sort_skew", 1), ("sort_skew", 256),
     ("walk_blocks", 2), ("walk_blocks", 5), ("refit_warps", 2), ("refit_warps", 4),
     ("row_grid", 4), ("row_grid", 32), ("sort_tile", 1), ("sort_tile", 2), ("sort_tile", 3),
+    ("sort_bits", 11),
 ]
 
 
@@ -75,7 +76,7 @@ def test_batched_path_under_knobs(cuda_device):
     try:
         ref = run()
         for knob, v in (("walk_blocks", 2), ("sort_rank", 1), ("refit_warps", 2),
-                        ("sort_tile", 3)):
+                        ("sort_tile", 3), ("sort_bits", 11)):
             autotune.apply(dict(defaults, **{knob: v}))
             assert _same(run(), ref), (knob, v)
             autotune.apply(defaults)

@@ -7,7 +7,8 @@ array inside libygx.so, so these tests check, through the C ABI, that two
 calls in a row (sharing that array) each match the workspace-based
 ygx_sort_pairs exactly, that the array's status word reads 0 after each
 call (ygx_sort_pairs_noalloc_status), that the value-less and in-place forms
-sort stably under the default and a non-default tile shape, and that sizes
+sort stably under the default and a non-default tile shape and with 11-bit
+digits, and that sizes
 above the array's limit are refused.  This file sorts last so a failure here
 never hides another test's result.
 """
@@ -92,21 +93,22 @@ def test_noalloc_sort_rejects_sizes_above_its_limit(cuda_device):
     assert rc == YGX_ERR_TOO_LARGE
 
 
-@pytest.mark.parametrize("tile", [0, 2])
-def test_noalloc_sort_without_values_and_in_place(cuda_device, tile):
+@pytest.mark.parametrize("knob,value", [("sort_tile", 0), ("sort_tile", 2), ("sort_bits", 11)])
+def test_noalloc_sort_without_values_and_in_place(cuda_device, knob, value):
     """values_in == NULL (each value is the input position) and keys_in ==
     keys_out (the input is staged inside the shared array first), at the
-    array's key limit, under the default and one other tile shape."""
+    array's key limit, under the default and one other tile shape, and with
+    11-bit digits (a 20-bit key: two passes instead of three)."""
     import torch
 
     from yggdrax_b200 import _lib as L
 
     lib = L.lib()
     old = np.zeros(1, np.int32)
-    L.check(lib.ygx_tune_get(L.TUNE["sort_tile"], old.ctypes.data), "ygx_tune_get")
-    L.check(lib.ygx_tune_set(L.TUNE["sort_tile"], tile), "ygx_tune_set")
+    L.check(lib.ygx_tune_get(L.TUNE[knob], old.ctypes.data), "ygx_tune_get")
+    L.check(lib.ygx_tune_set(L.TUNE[knob], value), "ygx_tune_set")
     try:
-        rng = np.random.default_rng(12 + tile)
+        rng = np.random.default_rng(12 + value)
         n = MAX_KEYS
         keys_np = rng.integers(0, 1 << 20, size=n, dtype=np.uint64)  # many ties
         order = np.argsort(keys_np, kind="stable")
@@ -131,4 +133,4 @@ def test_noalloc_sort_without_values_and_in_place(cuda_device, tile):
         np.testing.assert_array_equal(kio.cpu().numpy(), keys_np[order])
         np.testing.assert_array_equal(vo2.cpu().numpy(), vals_np[order])
     finally:
-        L.check(lib.ygx_tune_set(L.TUNE["sort_tile"], int(old[0])), "ygx_tune_set")
+        L.check(lib.ygx_tune_set(L.TUNE[knob], int(old[0])), "ygx_tune_set")

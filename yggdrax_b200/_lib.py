@@ -38,7 +38,7 @@ FLAG_BAD_INPUT = 1 << 5
 FLAG_LOG_OVERFLOW = 1 << 6
 WALK_LOG = 0
 TUNE = dict(sort_rank=0, sort_skew=1, walk_blocks=2, refit_warps=3, row_grid=4, sort_tile=5,
-            spin_limit=6, target_budget=7)
+            spin_limit=6, target_budget=7, sort_bits=8)
 WALK_COUNT = 1
 
 TSTAT_WORDS = 16

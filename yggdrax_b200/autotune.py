@@ -3,14 +3,20 @@
 The library exposes a few process-wide knobs (``ygx_tune_set``): how the
 onesweep sort ranks a tile's keys (warp ballots, per-warp peer tables, or a
 per-pass choice by how concentrated the pass's digits are, with its
-threshold) and its tile shape (keys per thread, CTAs per SM), how many CTAs per SM the traversal walk runs, the warps per CTA
-of the leaf refit, and the CTAs per SM of the short-row finalize.  None of
-them changes a result.  This module measures candidate settings on the
-caller's own workload with CUDA events and keeps the fastest:
+threshold), its tile shape (keys per thread, CTAs per SM) and its digit
+width (8 bits, or 11 bits where that cuts passes: 6 instead of 8 for the
+63-bit Morton codes), how many CTAs per SM the traversal walk runs, the
+warps per CTA of the leaf refit, and the CTAs per SM of the short-row
+finalize.  None of them changes a result.  This module measures candidate
+settings on the caller's own workload with CUDA events and keeps the
+fastest:
 
-* the sort knobs on the sort of the workload's Morton codes alone (a short,
-  low-noise measurement), then
-* the other knobs one at a time (coordinate descent) on the whole step.
+* the 8-bit pass's knobs on the sort of the workload's Morton codes alone (a
+  short, low-noise measurement), then
+* the other knobs one at a time (coordinate descent) on the whole step --
+  the digit width among them, because at 8 bits the Morton encode also
+  builds the sort's digit histograms while the 11-bit sort counts its own,
+  so only the whole step compares the two fairly.
 
 Results are cached per device and workload signature in a JSON file
 (``$YGGDRAX_B200_TUNE_CACHE``, default ``~/.cache/yggdrax_b200/tune.json``)
@@ -28,10 +34,12 @@ import torch
 
 from . import _lib as L
 
-KNOBS = ("sort_rank", "sort_skew", "sort_tile", "walk_blocks", "refit_warps", "row_grid")
+KNOBS = ("sort_rank", "sort_skew", "sort_tile", "sort_bits", "walk_blocks", "refit_warps",
+         "row_grid")
 SPACE: Dict[str, tuple] = {
     "sort_rank": (0, 1, 2),
     "sort_tile": (0, 1, 2, 3),
+    "sort_bits": (8, 11),
     "sort_skew": (8, 16, 32, 64, 128),
     "walk_blocks": (3, 4, 5, 6),
     "refit_warps": (2, 4, 8),
@@ -129,7 +137,8 @@ def _sort_step(codes: torch.Tensor, dev: torch.device) -> Callable[[], None]:
 
 
 def tune(step: Callable[[], object], dev: torch.device, *, codes: Optional[torch.Tensor] = None,
-         knobs: Iterable[str] = ("walk_blocks", "refit_warps", "row_grid"), reps: int = 3,
+         knobs: Iterable[str] = ("sort_bits", "walk_blocks", "refit_warps", "row_grid"),
+         reps: int = 3,
          log: Optional[list] = None) -> dict:
     """Choose knob values for ``step`` (a callable that runs the workload
     once).  With ``codes`` (the workload's Morton codes) the sort knobs are
@@ -139,6 +148,7 @@ def tune(step: Callable[[], object], dev: torch.device, *, codes: Optional[torch
     if codes is not None:
         run = _sort_step(codes, dev)
         results = []
+        best["sort_bits"] = 8  # the rank and tile knobs shape the 8-bit pass
         for rank in SPACE["sort_rank"]:
             for skew in (SPACE["sort_skew"] if rank == 2 else (best["sort_skew"],)):
                 cfg = dict(best, sort_rank=rank, sort_skew=skew)

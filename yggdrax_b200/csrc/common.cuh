@@ -23,6 +23,7 @@ struct Tune {
   int sort_tile = 0;           // onesweep tile shape (index into kSortShape, sort.cuh)
   int spin_limit = 1 << 22;    // iterations of a device-side wait before it gives up
   int target_budget = 128;     // per-target walk: warp steps per piece before a hand-off
+  int sort_bits = 8;           // onesweep digit width: 8, or 11 where it cuts passes
 };
 extern Tune g_tune;
 

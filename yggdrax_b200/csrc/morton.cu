@@ -652,7 +652,9 @@ int ygx_encode_sort(const float* positions, int64_t n, const float* bounds_in, f
                         stream) != cudaSuccess)
       return YGX_ERR_CUDA;
   }
-  const int passes = ygx::sort_passes(0, 63);
+  // the 8-bit sort's digit histograms come out of the encode; the 11-bit
+  // sort counts its own
+  const int passes = ygx::sort_uses_wide(0, 63) ? 0 : ygx::sort_passes(0, 63);
   if (ygx::sort_scratch_reset(l.sort, n, passes, stream) != cudaSuccess) return YGX_ERR_CUDA;
   bool fused = false;
   if (!bounds_in) {

@@ -31,7 +31,7 @@ namespace ygx {
 namespace {
 
 constexpr int64_t kNoAllocMaxKeys = int64_t(1) << 18;   // 262,144 keys per call
-constexpr size_t kNoAllocBytes = size_t(4) << 20;      // 4 MiB per GPU
+constexpr size_t kNoAllocBytes = size_t(6) << 20;      // 6 MiB per GPU
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 

@@ -11,19 +11,6 @@ namespace ygx {
 
 namespace {
 
-constexpr uint32_t kFlagAgg = 1u << 30;
-constexpr uint32_t kFlagInc = 2u << 30;
-constexpr uint32_t kCountMask = (1u << 30) - 1;
-
-__device__ __forceinline__ uint32_t ld_volatile_u32(const uint32_t* p) {
-  uint32_t v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_volatile_u32(uint32_t* p, uint32_t v) {
-  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
 __global__ void k_histogram(const uint64_t* __restrict__ keys, int64_t n, int begin_bit,
                             int passes, uint32_t* __restrict__ hist) {
   __shared__ uint32_t s_hist[8 * kSortRadix];
@@ -183,6 +170,10 @@ __global__ void __launch_bounds__(kSortThreads, kBlocksPerSM)
     st_volatile_u32(&my_lb[d], kFlagInc | ((excl + total) & kCountMask));
   }
   const uint32_t glob_d = digit_offsets[d] + excl;
+  // The look-back can leave the warp's lanes diverged (each waited on its
+  // own digit); the ranking needs them converged so that the leader lanes'
+  // atomics of successive items apply in item order.
+  __syncwarp();
   // Stable warp multisplit, kRankGroup items at a time: the peer mask of
   // every item (lanes holding the same digit) from one ballot per digit bit
   // (match-any measured slower here), then one shared-memory atomic per
@@ -356,7 +347,23 @@ SortScratch carve_sort_scratch(Arena& a, int64_t n, int max_passes) {
   s.rank_mode = a.take<uint32_t>(64);
   s.keys_tmp = a.take<uint64_t>((size_t)(n > 0 ? n : 1));
   s.vals_tmp = a.take<uint32_t>((size_t)(n > 0 ? n : 1));
+  s.wcounters = s.whist = s.woffsets = nullptr;
+  s.wlook[0] = s.wlook[1] = nullptr;
+  s.wtiles = 0;
+  if (max_passes >= 2) {  // a range of 9..11 bits already takes one wide pass instead of two
+    s.wtiles = sort_tiles(n, kWideTile) > 0 ? sort_tiles(n, kWideTile) : 1;
+    s.wcounters = a.take<uint32_t>(64);
+    s.whist = a.take<uint32_t>((size_t)kWideMaxPasses * kWideRadix);
+    s.wlook[0] = a.take<uint32_t>((size_t)s.wtiles * kWideRadix);
+    s.wlook[1] = a.take<uint32_t>((size_t)s.wtiles * kWideRadix);
+    s.woffsets = a.take<uint32_t>((size_t)kWideMaxPasses * kWideRadix);
+  }
   return s;
+}
+
+bool sort_uses_wide(int begin_bit, int end_bit) {
+  return g_tune.sort_bits == kWideBits &&
+         sort_passes_wide(begin_bit, end_bit) < sort_passes(begin_bit, end_bit);
 }
 
 cudaError_t sort_scratch_reset(const SortScratch& s, int64_t n, int passes, cudaStream_t st) {
@@ -372,6 +379,9 @@ int onesweep_sort(const uint64_t* keys_in, const uint32_t* vals_in, int64_t n, i
   if (n >= (int64_t)kCountMask) return YGX_ERR_ARG;
   if (begin_bit < 0 || end_bit > 64 || end_bit <= begin_bit) return YGX_ERR_ARG;
   if (vals_in != nullptr && (const void*)vals_in == (const void*)vals_out) return YGX_ERR_ARG;
+  if (s.wlook[0] != nullptr && sort_uses_wide(begin_bit, end_bit))
+    return onesweep_sort_wide(keys_in, vals_in, n, begin_bit, end_bit, keys_out, vals_out, s,
+                              status, st);
   const int passes = sort_passes(begin_bit, end_bit);
   if (passes > 8) return YGX_ERR_ARG;
   if (!hist_ready) {

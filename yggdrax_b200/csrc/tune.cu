@@ -18,6 +18,7 @@ bool legal(int knob, int v) {
     case YGX_TUNE_SORT_TILE: return v >= 0 && v < kSortTileShapes;
     case YGX_TUNE_SPIN_LIMIT: return v >= 0 && v <= kSpinLimitMax;
     case YGX_TUNE_TARGET_BUDGET: return v >= 1 && v <= 4096;
+    case YGX_TUNE_SORT_BITS: return v == kSortRadixBits || v == kWideBits;
     default: return false;
   }
 }
@@ -31,6 +32,7 @@ int* slot(int knob) {
     case YGX_TUNE_SORT_TILE: return &g_tune.sort_tile;
     case YGX_TUNE_SPIN_LIMIT: return &g_tune.spin_limit;
     case YGX_TUNE_TARGET_BUDGET: return &g_tune.target_budget;
+    case YGX_TUNE_SORT_BITS: return &g_tune.sort_bits;
     default: return nullptr;
   }
 }
