@@ -1,5 +1,7 @@
 // Stable LSD radix sort of (uint64 key, uint32 value) pairs: one
-// "onesweep" kernel per 8-bit digit with decoupled look-back.
+// "onesweep" kernel per digit with decoupled look-back -- 8-bit digits
+// (sort.cu), or 11-bit digits where the tuning knob asks for them and they
+// cut passes (sort_wide.cu).
 #pragma once
 #include "common.cuh"
 
