@@ -58,6 +58,22 @@ def test_packed_reorder_refuses_misaligned_records_before_launch():
     assert lib.ygx_reorder_packed(0x10000, None, 100, 64, None, None, None, None, None) == 1
 
 
+def test_tune_knob_ids_match_the_header():
+    """The binding's knob table (yggdrax_b200._lib.TUNE) and the header's
+    YGX_TUNE_* numbers are kept by hand in two places; they must agree, and
+    every knob the header declares must be readable."""
+    from yggdrax_b200 import _lib
+
+    src = open(os.path.join(ROOT, "include", "ygx.h")).read()
+    header = {m.group(1).lower(): int(m.group(2))
+              for m in re.finditer(r"#define YGX_TUNE_([A-Z_]+)\s+(\d+)", src)}
+    assert header == _lib.TUNE
+    lib = _lib.lib()
+    v = ctypes.c_int(0)
+    for knob in header.values():
+        assert lib.ygx_tune_get(knob, ctypes.byref(v)) == 0
+
+
 def test_product_does_not_import_oracle():
     pkg = os.path.join(ROOT, "yggdrax_b200")
     for dirpath, _, files in os.walk(pkg):
