@@ -62,23 +62,25 @@ def test_lookback_wait_that_runs_out_reports_timeout(cuda_device, digit_bits):
     vals = torch.from_numpy(vals_np).to(cuda_device)
     ws = L.workspace(lib.ygx_sort_pairs_workspace_size(n), cuda_device)
     flags = []
+    old_bits = np.zeros(1, np.int32)
+    L.check(lib.ygx_tune_get(L.TUNE["sort_bits"], old_bits.ctypes.data), "ygx_tune_get")
     L.check(lib.ygx_tune_set(L.TUNE["sort_bits"], digit_bits), "ygx_tune_set")
-    L.check(lib.ygx_tune_set(L.TUNE["spin_limit"], 0), "ygx_tune_set")
     try:
-        for _ in range(4):  # the first call practically always meets a wait
-            rc, f, _, _ = _sort(lib, L, keys, vals, ws, cuda_device)
-            assert rc == 0  # the launch ended and the call returned
-            flags.append(f)
-            if f & L.FLAG_TIMEOUT:
-                break
-    finally:
-        L.check(lib.ygx_tune_set(L.TUNE["spin_limit"], DEFAULT_SPIN_LIMIT), "ygx_tune_set")
-    assert any(f & L.FLAG_TIMEOUT for f in flags), flags
-    # the context is still usable and the default limit sorts correctly
-    try:
+        L.check(lib.ygx_tune_set(L.TUNE["spin_limit"], 0), "ygx_tune_set")
+        try:
+            for _ in range(4):  # the first call practically always meets a wait
+                rc, f, _, _ = _sort(lib, L, keys, vals, ws, cuda_device)
+                assert rc == 0  # the launch ended and the call returned
+                flags.append(f)
+                if f & L.FLAG_TIMEOUT:
+                    break
+        finally:
+            L.check(lib.ygx_tune_set(L.TUNE["spin_limit"], DEFAULT_SPIN_LIMIT), "ygx_tune_set")
+        assert any(f & L.FLAG_TIMEOUT for f in flags), flags
+        # the context is still usable and the default limit sorts correctly
         rc, f, ko, vo = _sort(lib, L, keys, vals, ws, cuda_device)
     finally:
-        L.check(lib.ygx_tune_set(L.TUNE["sort_bits"], 8), "ygx_tune_set")
+        L.check(lib.ygx_tune_set(L.TUNE["sort_bits"], int(old_bits[0])), "ygx_tune_set")
     assert rc == 0 and f == 0
     order = np.argsort(keys_np, kind="stable")
     np.testing.assert_array_equal(vo.cpu().numpy(), order.astype(np.int32))
