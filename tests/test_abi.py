@@ -58,6 +58,34 @@ def test_packed_reorder_refuses_misaligned_records_before_launch():
     assert lib.ygx_reorder_packed(0x10000, None, 100, 64, None, None, None, None, None) == 1
 
 
+def test_sort_pairs_refuses_bad_arguments_before_launch():
+    """ygx_sort_pairs checks its arguments on the host before any CUDA call
+    (YGX_ERR_ARG = 1), under both digit widths; the pointers here are fake
+    and never dereferenced."""
+    from yggdrax_b200 import _lib
+
+    lib = _lib.lib()
+    n = 1000
+    ws_bytes = lib.ygx_sort_pairs_workspace_size(n)
+    keys, kout, vin, vout, ws = 0x100000, 0x200000, 0x300000, 0x400000, 0x500000
+    old = ctypes.c_int(0)
+    assert lib.ygx_tune_get(_lib.TUNE["sort_bits"], ctypes.byref(old)) == 0
+    try:
+        for bits in (8, 11):
+            assert lib.ygx_tune_set(_lib.TUNE["sort_bits"], bits) == 0
+            call = lib.ygx_sort_pairs
+            assert call(keys, vin, -1, 0, 63, kout, vout, ws, ws_bytes, None) == 1
+            assert call(keys, vin, n, 0, 63, kout, vout, ws, ws_bytes - 1, None) == 1
+            assert call(keys, vin, n, 0, 63, kout, vout, None, ws_bytes, None) == 1
+            assert call(keys, vin, n, 20, 20, kout, vout, ws, ws_bytes, None) == 1
+            assert call(keys, vin, n, -1, 8, kout, vout, ws, ws_bytes, None) == 1
+            assert call(keys, vin, n, 0, 65, kout, vout, ws, ws_bytes, None) == 1
+            assert call(keys, vin, n, 0, 63, kout, vin, ws, ws_bytes, None) == 1  # values alias
+            assert call(keys, vin, 0, 0, 63, kout, vout, ws, ws_bytes, None) == 0  # nothing to do
+    finally:
+        lib.ygx_tune_set(_lib.TUNE["sort_bits"], old.value)
+
+
 def test_tune_knob_ids_match_the_header():
     """The binding's knob table (yggdrax_b200._lib.TUNE) and the header's
     YGX_TUNE_* numbers are kept by hand in two places; they must agree, and
