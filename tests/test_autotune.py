@@ -58,6 +58,44 @@ def test_search_finds_cheapest_setting(tune_mod, monkeypatch):
     assert len(log) == 1 + 1 + 3 + 2 + 3
 
 
+def test_sort_stage_tunes_the_8_bit_pass_and_leaves_the_width_to_the_step(tune_mod,
+                                                                           monkeypatch):
+    # synthetic costs: the sort alone is cheapest at ranking 1 / tile shape 2;
+    # the whole step is cheapest with 11-bit digits
+    stage = {"now": "sort"}
+    seen_bits = []
+
+    def cost():
+        c = tune_mod.current()
+        if stage["now"] == "sort":
+            seen_bits.append(c["sort_bits"])
+            return 1.0 + (c["sort_rank"] != 1) * 0.2 + (c["sort_tile"] != 2) * 0.1
+        return 10.0 + (c["sort_bits"] == 8) * 0.5
+
+    def sort_step(codes, dev):
+        stage["now"] = "sort"
+        return lambda: None
+
+    def step():
+        pass
+
+    def timed(fn, dev, reps=3, warmup=1):
+        if fn is step:
+            stage["now"] = "step"
+        return cost()
+
+    monkeypatch.setattr(tune_mod, "_sort_step", sort_step)
+    monkeypatch.setattr(tune_mod, "time_ms", timed)
+    tune_mod.apply({"sort_rank": 2, "sort_tile": 0, "sort_bits": 11})
+    log = []
+    best = tune_mod.tune(step, None, codes=object(), knobs=("sort_bits",), log=log)
+    assert best["sort_rank"] == 1 and best["sort_tile"] == 2
+    assert best["sort_bits"] == 11  # chosen on the step
+    assert seen_bits and set(seen_bits) == {8}  # the sort stage measures the 8-bit pass
+    assert tune_mod.current() == best
+    assert [r["stage"] for r in log].count("sort") == len(seen_bits)
+
+
 def test_cache_roundtrip(tune_mod, monkeypatch):
     calls = []
     monkeypatch.setattr(tune_mod, "tune",
